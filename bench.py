@@ -1,0 +1,349 @@
+"""Benchmark: GDoF/s of the Newtonian residual + Jacobian apply on B200, FP64 and FP32-mixed.
+
+Workload (the at-scale operator configuration): unit cube, 64^3 hex elements, degree 3 (P=4 nodes, Q=5 Gauss points per
+direction), 5 conservative fields, ideal gas (cv=717.5, cp=1004.5, mu=1.8e-5, k=0.0257), SUPG, dt=1e-5, BDF2 shift
+3/(2 dt); state = background (P=101325, T=288, u=(10,0,0)) plus 8 seeded sinusoidal modes (|k| <= 8, 1e-3 relative).
+L-vector 7,189,057 nodes x 5 = 35,945,285 DOF; 32,768,000 quadrature points.
+
+One step = one IFunction apply (writes the residual and the stored Jacobian data) + one IJacobian action, the unit of
+work of a Newton-Krylov iteration.  value = DOF / step time (GDoF/s), whole job over N GPUs (replicas, weak scaling).
+Inputs are larger than L2 (qdata alone is 2.6 GB), so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size 64]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+METRIC = "GDoF/s residual+Jacobian apply, FP64 vs FP32-mixed, at stated FP64-oracle error"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def workload(n, P=4, Q=5):
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    mesh = prob.box_mesh((n, n, n), P)
+    basis = prob.tensor_basis(P, Q)
+    ctx = prob.newtonian_context(P - 1, cv=717.5, cp=1004.5, mu=1.8e-5, k=0.0257, stab=prob.STAB_SUPG, dt=1e-5, ijacobian_time_shift=1.5e5)
+    q = prob.multimode_state(mesh, basis, ctx.gas, seed=0)
+    rng = np.random.default_rng(1)
+    q_dot = q * 1e-3 * rng.uniform(-1, 1, q.shape)
+    dq = q * 1e-4 * rng.uniform(-1, 1, q.shape)
+    return prob, mesh, basis, ctx, q, q_dot, dq
+
+
+def algorithmic_bytes(N_L, N_q, E, P, f32=False):
+    """Per-apply algorithmic bytes: unique L-vector traffic, qdata (10 doubles) and jac_data (14 values) per point, int32
+    offsets.  IFunction reads q, q_dot, writes v; IJacobian reads dq, writes v."""
+    b_if = 8 * 3 * N_L + 8 * N_q * 10 + (4 if f32 else 8) * N_q * 14 + 4 * E * P ** 3
+    b_ij = (4 if f32 else 8) * 2 * N_L + 8 * N_q * 10 + (4 if f32 else 8) * N_q * 14 + 4 * E * P ** 3
+    return b_if, b_ij
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.count(",") >= 8]
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------------------------------------------------
+# CPU legs (oracle = the checker / baseline; never the measured product)
+
+def cpu_leg(n_sample, use_ref, reps=3):
+    """Time the reference CPU path (reference QFunctions under the libCEED-semantics oracle driver, OpenMP over element
+    colours, all host threads) on a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    if use_ref and O.ref() is None:
+        use_ref = False
+    prob, mesh, basis, ctx, q, q_dot, dq = workload(n_sample)
+    threads = os.cpu_count() or 1
+    m = O.Mesh(mesh.num_elem, basis.P, basis.Q, mesh.offsets, basis.interp1d, basis.grad1d, basis.qweight1d, colors=mesh.colors,
+               num_threads=threads)
+    qdata = O.setup_qdata(mesh.num_elem, basis.Q, mesh.x_elem)
+    jd = np.zeros(mesh.num_elem * 14 * basis.Q ** 3)
+    cb = prob.context_bytes(ctx)
+    O.apply_ifunction(m, cb, q, q_dot, qdata, jd, use_ref=use_ref)
+    O.apply_ijacobian(m, cb, dq, qdata, jd, use_ref=use_ref)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.apply_ifunction(m, cb, q, q_dot, qdata, jd, use_ref=use_ref)
+        O.apply_ijacobian(m, cb, dq, qdata, jd, use_ref=use_ref)
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+    return {"value": mesh.l_size / t / 1e9, "unit": "GDoF/s", "cores": threads, "kind": "reference" if use_ref else "port",
+            "sample": f"{n_sample}^3 elements P=4 Q=5 ({mesh.l_size} DOF), IFunction+IJacobian, median of {reps}",
+            "seconds_per_step": t}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    n_sample = args.cpu_sample
+    res = cpu_leg(n_sample, use_ref=True, reps=max(1, min(args.steps, 5)))
+    line = {"metric": METRIC, "value": res["value"], "unit": "GDoF/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["seconds_per_step"] * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"64^3 hex P=4 Q=5 Newtonian IFunction+IJacobian (bounded CPU sample {n_sample}^3)"},
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------------------------------------
+# GPU arm
+
+def run_gpu(args, rank, world):
+    import torch
+    hb = importlib.import_module("honee-4aiad_b200")
+    kern = importlib.import_module("honee-4aiad_b200.kernels")
+    ce = importlib.import_module("honee-4aiad_b200.ceed")
+    hon = importlib.import_module("honee-4aiad_b200.honee")
+    hb.lib()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    prob, mesh, basis, ctx, q, q_dot, dq = workload(args.size)
+    P, Q, E = basis.P, basis.Q, mesh.num_elem
+    N_L, N_q = mesh.l_size, E * Q ** 3
+    cb = prob.context_bytes(ctx)
+
+    op = kern.ElemOp(mesh, basis)
+    f64 = dict(dtype=torch.float64, device=dev)
+    t_q = torch.from_numpy(q).to(dev)
+    t_qd = torch.from_numpy(q_dot).to(dev)
+    t_dq = torch.from_numpy(dq).to(dev)
+    t_v = torch.empty(N_L, **f64)
+    t_jv = torch.empty(N_L, **f64)
+    t_x = torch.from_numpy(mesh.x_elem).to(dev)
+    t_qdata = torch.empty(E * 10 * Q ** 3, **f64)
+    t_jd = torch.empty(E * 14 * Q ** 3, **f64)
+    op.setup_qdata(t_x, t_qdata)
+    del t_x
+    t_jd32 = torch.empty(E * 14 * Q ** 3, dtype=torch.float32, device=dev)
+    t_dq32 = t_dq.float()
+    t_jv32 = torch.empty(N_L, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def step64():
+        op.ifunction(cb, t_q, t_qd, t_qdata, t_v, jac_data=t_jd)
+        op.ijacobian(cb, t_qdata, t_jd, t_dq, t_jv)
+
+    def step32():
+        op.ifunction(cb, t_q, t_qd, t_qdata, t_v, jac_data_f32=t_jd32)
+        op.ijacobian(cb, t_qdata, t_jd32, t_dq32, t_jv32, fp32=True)
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(k):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / k
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = t.item()
+        return ms
+
+    with ClockSampler(dev.index) as clk:
+        ms64 = timed(step64, args.steps)
+    clocks = clk.summary()
+    ms32 = timed(step32, args.steps)
+    ms_if = timed(lambda: op.ifunction(cb, t_q, t_qd, t_qdata, t_v, jac_data=t_jd), args.steps)
+    ms_ij = timed(lambda: op.ijacobian(cb, t_qdata, t_jd, t_dq, t_jv), args.steps)
+    ms_if32 = timed(lambda: op.ifunction(cb, t_q, t_qd, t_qdata, t_v, jac_data_f32=t_jd32), args.steps)
+    ms_ij32 = timed(lambda: op.ijacobian(cb, t_qdata, t_jd32, t_dq32, t_jv32, fp32=True), args.steps)
+    t_diag = torch.empty(N_L, **f64)
+    ms_diag = timed(lambda: op.diagonal(cb, t_qdata, t_jd, t_diag), max(1, min(args.steps, 3)))
+
+    # FP32 Jacobian error against the FP64 kernel on the full workload
+    step64()
+    jv64 = t_jv.clone()
+    step32()
+    err32 = (torch.linalg.vector_norm(t_jv32.double() - jv64) / torch.linalg.vector_norm(jv64)).item()
+
+    # e2e through the libCEED API with host (pinned) buffers: H2D of q, q_dot, dq and D2H of both results every step
+    ceed = ce.Ceed("/gpu/b200")
+    ops = hon.NewtonianOperators(ceed, mesh, basis, ctx)
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    h_q, h_qd, h_dq = pin(q), pin(q_dot), pin(dq)
+    h_g, h_j = pin(np.zeros(N_L)), pin(np.zeros(N_L))
+    qv, dv, gv, jvv = (ce.Vector(ceed, N_L) for _ in range(4))
+
+    def e2e_step():
+        qv.set_array_host(h_q, copy=False)
+        ops.q_dot.set_array_host(h_qd, copy=False)
+        dv.set_array_host(h_dq, copy=False)
+        gv.set_array_host(h_g, copy=False)
+        jvv.set_array_host(h_j, copy=False)
+        ops.op_ifunction.apply(qv, gv)
+        ops.op_ijacobian.apply(dv, jvv)
+        ce.L().CeedVectorSyncArray(gv.ptr, ce.CEED_MEM_HOST)
+        ce.L().CeedVectorSyncArray(jvv.ptr, ce.CEED_MEM_HOST)
+
+    ms_e2e = timed(e2e_step, max(1, min(args.steps, 5)))
+    err_e2e = float(np.linalg.norm(h_j - jv64.cpu().numpy()) / np.linalg.norm(jv64.cpu().numpy()))
+
+    # parity on a small case of the same operator against the CPU oracle (the accuracy the number is quoted at)
+    acc = parity_sample(prob, kern, torch, dev)
+
+    pk, pk_kind = peaks()
+    b_if, b_ij = algorithmic_bytes(N_L, N_q, E, P)
+    achieved_if = b_if / (ms_if * 1e-3) / 1e9
+    launches = 2 * op.num_colors * args.steps
+    line = {
+        "metric": METRIC, "value": world * N_L / (ms64 * 1e-3) / 1e9, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: background + 8 seeded sinusoidal modes (|k|<=8, 1e-3 relative)",
+        "config": {"workload": f"{args.size}^3 hex elements, P=4 Q=5, Newtonian IFunction + IJacobian (SUPG, conservative, FP64)",
+                   "dofs": N_L, "elements": E, "qpts": N_q, "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (qdata 2.6 GB, jac_data 3.7 GB per GPU); no flush"},
+        "fp32_mixed": {"value": world * N_L / (ms32 * 1e-3) / 1e9, "unit": "GDoF/s", "ms_per_step": ms32,
+                       "jacobian_rel_l2_vs_fp64": err32, "residual": "FP64", "jacobian": "FP32 (FP32 jac_data, FP64 qdata)"},
+        "breakdown_ms": {"ifunction": ms_if, "ijacobian": ms_ij, "ifunction_f32_jacdata": ms_if32, "ijacobian_f32": ms_ij32,
+                         "diagonal_f64": ms_diag},
+        "accuracy": acc,
+        "roofline": {"bound": "hbm", "kernel": "k_ifunction (fused IFunction, one launch per colour)", "achieved": achieved_if,
+                     "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved_if / pk["hbm_gbs"], "peak_source": pk_kind,
+                     "algorithmic_bytes_per_apply": b_if, "traffic": None,
+                     "ijacobian": {"achieved": b_ij / (ms_ij * 1e-3) / 1e9, "frac": b_ij / (ms_ij * 1e-3) / 1e9 / pk["hbm_gbs"]}},
+        "e2e": {"value": world * N_L / (ms_e2e * 1e-3) / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": 3 * 8 * N_L, "d2h_bytes_per_step": 2 * 8 * N_L,
+                "api": "CeedVectorSetArray(HOST, USE_POINTER) + CeedOperatorApply x2 + CeedVectorSyncArray(HOST)", "jacobian_rel_l2_vs_kernel": err_e2e},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = {k: v for k, v in cpu_leg(args.cpu_sample, use_ref=False).items() if k != "seconds_per_step"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def parity_sample(prob, kern, torch, dev):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    mesh = prob.box_mesh((6, 6, 6), 4)
+    basis = prob.tensor_basis(4, 5)
+    ctx = prob.newtonian_context(3, cv=717.5, cp=1004.5, mu=1.8e-5, k=0.0257, stab=prob.STAB_SUPG, dt=1e-5, ijacobian_time_shift=1.5e5)
+    q = prob.multimode_state(mesh, basis, ctx.gas, seed=3)
+    qd = q * 1e-3
+    dq = q * 1e-4 * np.random.default_rng(2).uniform(-1, 1, q.shape)
+    cb = prob.context_bytes(ctx)
+    m = O.Mesh(mesh.num_elem, 4, 5, mesh.offsets, basis.interp1d, basis.grad1d, basis.qweight1d, colors=mesh.colors)
+    qdata = O.setup_qdata(mesh.num_elem, 5, mesh.x_elem)
+    jd = np.zeros(mesh.num_elem * 14 * 125)
+    v_ref = O.apply_ifunction(m, cb, q, qd, qdata, jd)
+    j_ref = O.apply_ijacobian(m, cb, dq, qdata, jd)
+    op = kern.ElemOp(mesh, basis)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    tq, tqd, tdq, tqdata = T(q), T(qd), T(dq), T(qdata)
+    tv, tj = torch.empty_like(tq), torch.empty_like(tq)
+    tjd = torch.empty(mesh.num_elem * 14 * 125, dtype=torch.float64, device=dev)
+    tjd32 = torch.empty(mesh.num_elem * 14 * 125, dtype=torch.float32, device=dev)
+    op.ifunction(cb, tq, tqd, tqdata, tv, jac_data=tjd, jac_data_f32=tjd32)
+    op.ijacobian(cb, tqdata, tjd, tdq, tj)
+    tj32 = torch.empty(mesh.l_size, dtype=torch.float32, device=dev)
+    op.ijacobian(cb, tqdata, tjd32, tdq.float(), tj32, fp32=True)
+    torch.cuda.synchronize()
+    r = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    return {"case": "6^3 P=4 Q=5 same operator", "ifunction_rel_l2": r(tv.cpu().numpy(), v_ref), "ijacobian_rel_l2": r(tj.cpu().numpy(), j_ref),
+            "ijacobian_f32_rel_l2": r(tj32.double().cpu().numpy(), j_ref)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=64)
+    ap.add_argument("--cpu-sample", type=int, default=32)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank)
+        else:
+            run_gpu(args, rank, world)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1632 @@
+/* ceed_b200.c -- libCEED-compatible host layer of the B200 backend (declared in include/ceed/ceed.h).
+ *
+ * HONEE builds its operators through the libCEED C API (src/setuplibceed.c:97-340, src/qdata.c:133-190) and applies
+ * them through CeedOperatorApply / CeedOperatorApplyAdd / CeedOperatorLinearAssembleDiagonal (src/setupts.c:109,
+ * src/mat-ceed.c:1603-1700).  This file implements that object model (Ceed, CeedVector, CeedElemRestriction, CeedBasis,
+ * CeedQFunctionContext, CeedQFunction, CeedOperator, composite operators, context field labels, error handling) and,
+ * when an operator is first applied, recognises the HONEE QFunction by the kernel name in its source string
+ * ("newtonian.h:IFunction_Newtonian_Conserv" -> "IFunction_Newtonian_Conserv") and binds it to a fused sm_100a kernel
+ * (include/honee_b200.h).  An operator whose QFunction has no fused kernel fails with CEED_ERROR_UNSUPPORTED; the user
+ * function pointer is never called, so nothing runs on the CPU.
+ *
+ * Memory follows libCEED's CUDA backends: a CeedVector mirrors host and device arrays with validity flags, wraps
+ * caller arrays zero-copy with CEED_USE_POINTER (include/petsc-ceed-utils.h:127-191), and copies lazily on access.
+ * All device work is stream-ordered on the Ceed's stream (the legacy default stream unless CeedSetStream is called);
+ * host reads synchronise it.
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdbool.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ceed/ceed.h"
+#include "hb_internal.h"
+#include "honee_b200.h"
+
+#define MAX_FIELDS 16
+#define MAX_SUBS 16
+#define MAX_LABELS 16
+#define NAME_LEN 128
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* object layouts                                                                                                     */
+
+struct Ceed_private {
+  int              ref;
+  char             resource[256];
+  int              mixed;  /* 1: FP32 Jacobian action and diagonal */
+  cudaStream_t     stream;
+  CeedErrorHandler handler;
+  char             err_msg[2048];
+  double          *d_scratch; /* 1024 doubles for reductions */
+};
+
+struct CeedVector_private {
+  Ceed     ceed;
+  int      ref;
+  CeedSize length;
+  double  *h, *d;
+  int      h_own, d_own, h_valid, d_valid;
+  float   *d_f32;      /* FP32 shadow (mixed-precision jac_data) */
+  int      f32_valid;  /* shadow holds the current values */
+  int      f64_stale;  /* FP64 copies are out of date: rebuild from the shadow on access */
+};
+
+struct CeedElemRestriction_private {
+  Ceed     ceed;
+  int      ref;
+  CeedInt  num_elem, elem_size, num_comp, comp_stride;
+  CeedSize l_size;
+  int      strided;
+  CeedInt  strides[3];
+  int32_t *h_off, *d_off, *d_strides;
+  int64_t *d_tptr, *d_teidx; /* transpose CSR, built on first transpose apply */
+};
+
+struct CeedBasis_private {
+  Ceed    ceed;
+  int     ref;
+  int     dim, num_comp, P1d, Q1d, tensor;
+  double  interp1d[HB_MAX_P * HB_MAX_P], grad1d[HB_MAX_P * HB_MAX_P], qref1d[HB_MAX_P], qweight1d[HB_MAX_P];
+  double *d_B, *d_G, *d_w;
+};
+
+typedef struct {
+  char   name[NAME_LEN];
+  size_t offset, num_values;
+  int    type;
+} CtxLabel;
+
+struct CeedQFunctionContext_private {
+  Ceed                                ceed;
+  int                                 ref;
+  size_t                              size;
+  void                               *data;
+  int                                 own;
+  CeedQFunctionContextDataDestroyUser destroy;
+  int                                 nlabels;
+  CtxLabel                            labels[MAX_LABELS];
+};
+
+typedef struct {
+  char         name[NAME_LEN];
+  CeedInt      size;
+  CeedEvalMode emode;
+} QFField;
+
+struct CeedQFunction_private {
+  Ceed                 ceed;
+  int                  ref;
+  CeedInt              vlength;
+  CeedQFunctionUser    f;
+  char                 source[512], kernel[NAME_LEN];
+  int                  nin, nout;
+  QFField              in[MAX_FIELDS], out[MAX_FIELDS];
+  CeedQFunctionContext ctx;
+  CeedSize             user_flops;
+};
+
+typedef struct {
+  CeedElemRestriction r;
+  CeedBasis           b;
+  CeedVector          v;
+  int                 set;
+} OpField;
+
+enum { PLAN_NONE = 0, PLAN_SETUP, PLAN_IFUNCTION, PLAN_IJACOBIAN };
+
+struct CeedOperator_private {
+  Ceed          ceed;
+  int           ref;
+  int           composite;
+  char          name[NAME_LEN];
+  CeedQFunction qf;
+  OpField       in[MAX_FIELDS], out[MAX_FIELDS];
+  int           nsub;
+  CeedOperator  subs[MAX_SUBS];
+  /* backend plan */
+  int       plan;
+  HbElemOp *eop;
+  int       idl_coords_set;
+  float    *d_tmp_in32, *d_tmp_out32; /* mixed-precision staging of L-vectors */
+  double   *d_tmp_e;                  /* coordinate E-vector for the Setup operator */
+};
+
+struct CeedContextFieldLabel_private {
+  int    n;
+  struct {
+    CeedQFunctionContext ctx;
+    size_t               offset, num_values;
+  } ent[MAX_SUBS];
+  char name[NAME_LEN];
+};
+
+struct CeedRequest_private {
+  int unused;
+};
+
+/* sentinels */
+static struct CeedVector_private          vec_active_obj, vec_none_obj;
+static struct CeedBasis_private           basis_none_obj;
+static struct CeedElemRestriction_private rstr_none_obj;
+static struct CeedQFunction_private       qf_none_obj;
+static CeedRequest                        req_immediate_obj, req_ordered_obj;
+CeedRequest *const                        CEED_REQUEST_IMMEDIATE    = &req_immediate_obj;
+CeedRequest *const                        CEED_REQUEST_ORDERED      = &req_ordered_obj;
+const CeedInt                             CEED_STRIDES_BACKEND[3]   = {0, 0, 0};
+const CeedVector                          CEED_VECTOR_ACTIVE        = &vec_active_obj;
+const CeedVector                          CEED_VECTOR_NONE          = &vec_none_obj;
+const CeedBasis                           CEED_BASIS_NONE           = &basis_none_obj;
+const CeedElemRestriction                 CEED_ELEMRESTRICTION_NONE = &rstr_none_obj;
+const CeedQFunction                       CEED_QFUNCTION_NONE       = &qf_none_obj;
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* errors                                                                                                             */
+
+static int ceed_error(Ceed ceed, const char *file, int line, const char *func, int ecode, const char *fmt, ...) {
+  va_list args;
+  va_start(args, fmt);
+  int r = ecode;
+  if (ceed && ceed->handler) r = ceed->handler(ceed, file, line, func, ecode, fmt, &args);
+  else r = CeedErrorStore(ceed, file, line, func, ecode, fmt, &args);
+  va_end(args);
+  return r;
+}
+#define CeedError(ceed, ecode, ...) ceed_error((ceed), __FILE__, __LINE__, __func__, (ecode), __VA_ARGS__)
+#define CK(call)            \
+  do {                      \
+    int ierr_ = (call);     \
+    if (ierr_) return ierr_; \
+  } while (0)
+#define CUDA_CK(ceed, call)                                                                                          \
+  do {                                                                                                               \
+    cudaError_t cerr_ = (call);                                                                                      \
+    if (cerr_ != cudaSuccess) return CeedError((ceed), CEED_ERROR_BACKEND, "CUDA error %s in %s", cudaGetErrorString(cerr_), #call); \
+  } while (0)
+#define HB_CK(ceed, call)                                                                             \
+  do {                                                                                                \
+    int herr_ = (call);                                                                               \
+    if (herr_) return CeedError((ceed), herr_ == HB_ERROR_UNSUPPORTED ? CEED_ERROR_UNSUPPORTED : CEED_ERROR_BACKEND, \
+                                "backend call %s failed with status %d", #call, herr_);              \
+  } while (0)
+
+static char fallback_msg[2048];
+
+int CeedErrorStore(Ceed ceed, const char *filename, int line_no, const char *func, int ecode, const char *format, va_list *args) {
+  char *buf = ceed ? ceed->err_msg : fallback_msg;
+  int   n   = snprintf(buf, 2048, "%s:%d in %s(): ", filename, line_no, func);
+  if (n < 0 || n >= 2048) n = 0;
+  vsnprintf(buf + n, (size_t)(2048 - n), format, *args);
+  return ecode;
+}
+int CeedErrorReturn(Ceed ceed, const char *filename, int line_no, const char *func, int ecode, const char *format, va_list *args) {
+  return CeedErrorStore(ceed, filename, line_no, func, ecode, format, args);
+}
+int CeedErrorAbort(Ceed ceed, const char *filename, int line_no, const char *func, int ecode, const char *format, va_list *args) {
+  CeedErrorStore(ceed, filename, line_no, func, ecode, format, args);
+  fprintf(stderr, "%s\n", ceed ? ceed->err_msg : fallback_msg);
+  abort();
+  return ecode;
+}
+int CeedErrorExit(Ceed ceed, const char *filename, int line_no, const char *func, int ecode, const char *format, va_list *args) {
+  CeedErrorStore(ceed, filename, line_no, func, ecode, format, args);
+  fprintf(stderr, "%s\n", ceed ? ceed->err_msg : fallback_msg);
+  exit(ecode);
+  return ecode;
+}
+int CeedSetErrorHandler(Ceed ceed, CeedErrorHandler handler) {
+  ceed->handler = handler;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedGetErrorMessage(Ceed ceed, const char **err_msg) {
+  *err_msg = ceed ? ceed->err_msg : fallback_msg;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedResetErrorMessage(Ceed ceed, const char **err_msg) {
+  if (ceed) ceed->err_msg[0] = 0;
+  if (err_msg) *err_msg = ceed ? ceed->err_msg : fallback_msg;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* Ceed                                                                                                               */
+
+int CeedInit(const char *resource, Ceed *ceed) {
+  *ceed = NULL;
+  if (!resource) return CEED_ERROR_MAJOR;
+  int mixed = 0;
+  if (!strcmp(resource, "/gpu/b200") || !strcmp(resource, "/gpu/cuda") || !strcmp(resource, "/gpu/cuda/shared") ||
+      !strcmp(resource, "/gpu/cuda/gen") || !strcmp(resource, "/gpu/cuda/ref") || !strcmp(resource, "/gpu/b200/fp64"))
+    mixed = 0;
+  else if (!strcmp(resource, "/gpu/b200/mixed")) mixed = 1;
+  else {
+    snprintf(fallback_msg, sizeof fallback_msg, "CeedInit: resource '%s' is not provided by the B200 backend (use /gpu/b200 or /gpu/b200/mixed)",
+             resource);
+    return CEED_ERROR_UNSUPPORTED;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    snprintf(fallback_msg, sizeof fallback_msg, "CeedInit: resource '%s' needs a CUDA device and none is visible", resource);
+    return CEED_ERROR_BACKEND;
+  }
+  Ceed c = (Ceed)calloc(1, sizeof(*c));
+  c->ref   = 1;
+  c->mixed = mixed;
+  snprintf(c->resource, sizeof c->resource, "%s", resource);
+  c->stream  = NULL;
+  c->handler = CeedErrorStore;
+  if (cudaMalloc((void **)&c->d_scratch, 1024 * sizeof(double)) != cudaSuccess) {
+    free(c);
+    return CEED_ERROR_BACKEND;
+  }
+  *ceed = c;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedReferenceCopy(Ceed ceed, Ceed *ceed_copy) {
+  ceed->ref++;
+  CK(CeedDestroy(ceed_copy));
+  *ceed_copy = ceed;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedDestroy(Ceed *ceed) {
+  if (!*ceed) return CEED_ERROR_SUCCESS;
+  if (--(*ceed)->ref > 0) {
+    *ceed = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  cudaFree((*ceed)->d_scratch);
+  free(*ceed);
+  *ceed = NULL;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedGetResource(Ceed ceed, const char **resource) {
+  *resource = ceed->resource;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedGetPreferredMemType(Ceed ceed, CeedMemType *type) {
+  (void)ceed;
+  *type = CEED_MEM_DEVICE;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedIsDeterministic(Ceed ceed, bool *is_deterministic) {
+  (void)ceed;
+  *is_deterministic = true; /* coloured scatters, no atomics */
+  return CEED_ERROR_SUCCESS;
+}
+int CeedSetStream(Ceed ceed, void *handle) {
+  ceed->stream = (cudaStream_t)handle;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedGetVersion(int *major, int *minor, int *patch, bool *release) {
+  if (major) *major = CEED_VERSION_MAJOR;
+  if (minor) *minor = CEED_VERSION_MINOR;
+  if (patch) *patch = CEED_VERSION_PATCH;
+  if (release) *release = CEED_VERSION_RELEASE;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* CeedVector                                                                                                         */
+
+int CeedVectorCreate(Ceed ceed, CeedSize len, CeedVector *vec) {
+  if (len < 0) return CeedError(ceed, CEED_ERROR_DIMENSION, "negative vector length");
+  CeedVector v = (CeedVector)calloc(1, sizeof(*v));
+  v->ceed      = ceed;
+  ceed->ref++;
+  v->ref    = 1;
+  v->length = len;
+  *vec      = v;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorReferenceCopy(CeedVector vec, CeedVector *vec_copy) {
+  vec->ref++;
+  CK(CeedVectorDestroy(vec_copy));
+  *vec_copy = vec;
+  return CEED_ERROR_SUCCESS;
+}
+
+static int vec_alloc_host(CeedVector v) {
+  if (!v->h) {
+    v->h     = (double *)malloc(sizeof(double) * (size_t)(v->length ? v->length : 1));
+    v->h_own = 1;
+    if (!v->h) return CeedError(v->ceed, CEED_ERROR_MAJOR, "host allocation of %td doubles failed", v->length);
+  }
+  return CEED_ERROR_SUCCESS;
+}
+static int vec_alloc_dev(CeedVector v) {
+  if (!v->d) {
+    CUDA_CK(v->ceed, cudaMalloc((void **)&v->d, sizeof(double) * (size_t)(v->length ? v->length : 1)));
+    v->d_own = 1;
+  }
+  return CEED_ERROR_SUCCESS;
+}
+/* bring the FP64 device copy up to date from the FP32 shadow */
+static int vec_unstale(CeedVector v) {
+  if (!v->f64_stale) return CEED_ERROR_SUCCESS;
+  CK(vec_alloc_dev(v));
+  HB_CK(v->ceed, hb_vec_f32_to_f64(v->d_f32, v->d, v->length, 0, v->ceed->stream));
+  v->f64_stale = 0;
+  v->d_valid   = 1;
+  v->h_valid   = 0;
+  return CEED_ERROR_SUCCESS;
+}
+static int vec_sync_dev(CeedVector v) {
+  CK(vec_unstale(v));
+  CK(vec_alloc_dev(v));
+  if (!v->d_valid) {
+    if (!v->h_valid) return CeedError(v->ceed, CEED_ERROR_INCOMPLETE, "vector has no valid data");
+    CUDA_CK(v->ceed, cudaMemcpyAsync(v->d, v->h, sizeof(double) * (size_t)v->length, cudaMemcpyHostToDevice, v->ceed->stream));
+    CUDA_CK(v->ceed, cudaStreamSynchronize(v->ceed->stream));
+    v->d_valid = 1;
+  }
+  return CEED_ERROR_SUCCESS;
+}
+static int vec_sync_host(CeedVector v) {
+  CK(vec_unstale(v));
+  CK(vec_alloc_host(v));
+  if (!v->h_valid) {
+    if (!v->d_valid) return CeedError(v->ceed, CEED_ERROR_INCOMPLETE, "vector has no valid data");
+    CUDA_CK(v->ceed, cudaMemcpyAsync(v->h, v->d, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToHost, v->ceed->stream));
+    CUDA_CK(v->ceed, cudaStreamSynchronize(v->ceed->stream));
+    v->h_valid = 1;
+  }
+  return CEED_ERROR_SUCCESS;
+}
+/* device array for a kernel that reads the vector */
+static int vec_dev_read(CeedVector v, const double **d) {
+  CK(vec_sync_dev(v));
+  *d = v->d;
+  return CEED_ERROR_SUCCESS;
+}
+/* device array for a kernel that writes (write_only: contents may be discarded) */
+static int vec_dev_write(CeedVector v, double **d, int write_only) {
+  if (write_only) {
+    v->f64_stale = 0;
+    CK(vec_alloc_dev(v));
+  } else CK(vec_sync_dev(v));
+  v->d_valid   = 1;
+  v->h_valid   = 0;
+  v->f32_valid = 0;
+  *d           = v->d;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorSetArray(CeedVector v, CeedMemType mem_type, CeedCopyMode copy_mode, CeedScalar *array) {
+  v->f64_stale = 0;
+  v->f32_valid = 0;
+  if (mem_type == CEED_MEM_HOST) {
+    if (copy_mode == CEED_COPY_VALUES) {
+      CK(vec_alloc_host(v));
+      if (array) memcpy(v->h, array, sizeof(double) * (size_t)v->length);
+    } else {
+      if (v->h_own) free(v->h);
+      v->h     = array;
+      v->h_own = copy_mode == CEED_OWN_POINTER;
+    }
+    v->h_valid = array != NULL;
+    v->d_valid = 0;
+  } else {
+    if (copy_mode == CEED_COPY_VALUES) {
+      CK(vec_alloc_dev(v));
+      if (array) CUDA_CK(v->ceed, cudaMemcpyAsync(v->d, array, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToDevice, v->ceed->stream));
+    } else {
+      if (v->d_own) cudaFree(v->d);
+      v->d     = array;
+      v->d_own = copy_mode == CEED_OWN_POINTER;
+    }
+    v->d_valid = array != NULL;
+    v->h_valid = 0;
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorSetValue(CeedVector v, CeedScalar value) {
+  double *d;
+  CK(vec_dev_write(v, &d, 1));
+  HB_CK(v->ceed, hb_vec_set_f64(d, v->length, value, v->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorSyncArray(CeedVector v, CeedMemType mem_type) { return mem_type == CEED_MEM_HOST ? vec_sync_host(v) : vec_sync_dev(v); }
+
+int CeedVectorTakeArray(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
+  if (mem_type == CEED_MEM_HOST) {
+    if (v->h && !v->h_valid && (v->d_valid || v->f64_stale)) CK(vec_sync_host(v));
+    *array     = v->h;
+    v->h       = NULL;
+    v->h_own   = 0;
+    v->h_valid = 0;
+  } else {
+    if (v->d && !v->d_valid && (v->h_valid || v->f64_stale)) CK(vec_sync_dev(v));
+    *array     = v->d;
+    v->d       = NULL;
+    v->d_own   = 0;
+    v->d_valid = 0;
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorGetArrayRead(CeedVector v, CeedMemType mem_type, const CeedScalar **array) {
+  if (mem_type == CEED_MEM_HOST) {
+    CK(vec_sync_host(v));
+    *array = v->h;
+  } else {
+    CK(vec_sync_dev(v));
+    *array = v->d;
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorGetArray(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
+  if (mem_type == CEED_MEM_HOST) {
+    CK(vec_sync_host(v));
+    v->d_valid = 0;
+    *array     = v->h;
+  } else {
+    CK(vec_sync_dev(v));
+    v->h_valid = 0;
+    *array     = v->d;
+  }
+  v->f32_valid = 0;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorGetArrayWrite(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
+  v->f64_stale = 0;
+  v->f32_valid = 0;
+  if (mem_type == CEED_MEM_HOST) {
+    CK(vec_alloc_host(v));
+    v->h_valid = 1;
+    v->d_valid = 0;
+    *array     = v->h;
+  } else {
+    CK(vec_alloc_dev(v));
+    v->d_valid = 1;
+    v->h_valid = 0;
+    *array     = v->d;
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorRestoreArray(CeedVector v, CeedScalar **array) {
+  (void)v;
+  *array = NULL;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedVectorRestoreArrayRead(CeedVector v, const CeedScalar **array) {
+  (void)v;
+  *array = NULL;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedVectorGetLength(CeedVector v, CeedSize *length) {
+  *length = v->length;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorNorm(CeedVector v, CeedNormType type, CeedScalar *norm) {
+  const double *d;
+  CK(vec_dev_read(v, &d));
+  double r  = 0;
+  int    tp = type == CEED_NORM_1 ? 0 : (type == CEED_NORM_2 ? 1 : 2);
+  HB_CK(v->ceed, hb_vec_reduce_f64(d, NULL, v->length, tp, v->ceed->d_scratch, &r, v->ceed->stream));
+  *norm = type == CEED_NORM_2 ? sqrt(r) : r;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorCopy(CeedVector vec, CeedVector vec_copy) {
+  if (vec->length != vec_copy->length) return CeedError(vec->ceed, CEED_ERROR_INCOMPATIBLE, "vector lengths differ");
+  const double *s;
+  double       *d;
+  CK(vec_dev_read(vec, &s));
+  CK(vec_dev_write(vec_copy, &d, 1));
+  CUDA_CK(vec->ceed, cudaMemcpyAsync(d, s, sizeof(double) * (size_t)vec->length, cudaMemcpyDeviceToDevice, vec->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+int CeedVectorScale(CeedVector x, CeedScalar alpha) {
+  double *d;
+  CK(vec_dev_write(x, &d, 0));
+  HB_CK(x->ceed, hb_vec_scale_f64(d, x->length, alpha, x->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+int CeedVectorAXPY(CeedVector y, CeedScalar alpha, CeedVector x) {
+  if (x->length != y->length) return CeedError(y->ceed, CEED_ERROR_INCOMPATIBLE, "vector lengths differ");
+  const double *xd;
+  double       *yd;
+  CK(vec_dev_read(x, &xd));
+  CK(vec_dev_write(y, &yd, 0));
+  HB_CK(y->ceed, hb_vec_axpy_f64(yd, alpha, xd, y->length, y->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+int CeedVectorAXPBY(CeedVector y, CeedScalar alpha, CeedScalar beta, CeedVector x) {
+  if (x->length != y->length) return CeedError(y->ceed, CEED_ERROR_INCOMPATIBLE, "vector lengths differ");
+  const double *xd;
+  double       *yd;
+  CK(vec_dev_read(x, &xd));
+  CK(vec_dev_write(y, &yd, 0));
+  HB_CK(y->ceed, hb_vec_axpby_f64(yd, alpha, beta, xd, y->length, y->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+int CeedVectorPointwiseMult(CeedVector w, CeedVector x, CeedVector y) {
+  const double *xd, *yd;
+  double       *wd;
+  CK(vec_dev_read(x, &xd));
+  CK(vec_dev_read(y, &yd));
+  CK(vec_dev_write(w, &wd, w != x && w != y));
+  HB_CK(w->ceed, hb_vec_pointwise_mult_f64(wd, xd, yd, w->length, w->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+int CeedVectorReciprocal(CeedVector v) {
+  double *d;
+  CK(vec_dev_write(v, &d, 0));
+  HB_CK(v->ceed, hb_vec_reciprocal_f64(d, v->length, v->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedVectorDestroy(CeedVector *vec) {
+  CeedVector v = *vec;
+  if (!v || v == CEED_VECTOR_ACTIVE || v == CEED_VECTOR_NONE) {
+    *vec = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (--v->ref > 0) {
+    *vec = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (v->h_own) free(v->h);
+  if (v->d_own) cudaFree(v->d);
+  if (v->d_f32) cudaFree(v->d_f32);
+  Ceed ceed = v->ceed;
+  free(v);
+  *vec = NULL;
+  return CeedDestroy(&ceed);
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* CeedElemRestriction                                                                                                */
+
+int CeedElemRestrictionCreate(Ceed ceed, CeedInt num_elem, CeedInt elem_size, CeedInt num_comp, CeedInt comp_stride, CeedSize l_size,
+                              CeedMemType mem_type, CeedCopyMode copy_mode, const CeedInt *offsets, CeedElemRestriction *rstr) {
+  (void)copy_mode;
+  if (num_elem < 0 || elem_size < 1 || num_comp < 1) return CeedError(ceed, CEED_ERROR_DIMENSION, "invalid restriction dimensions");
+  const size_t n = (size_t)num_elem * elem_size;
+  int32_t     *h = (int32_t *)malloc(sizeof(int32_t) * (n ? n : 1));
+  if (mem_type == CEED_MEM_HOST) memcpy(h, offsets, sizeof(int32_t) * n);
+  else CUDA_CK(ceed, cudaMemcpy(h, offsets, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+  /* host-side bounds validation: every entry offset + c*comp_stride must lie in [0, l_size) */
+  const int64_t span = (int64_t)(num_comp - 1) * comp_stride;
+  for (size_t i = 0; i < n; i++)
+    if (h[i] < 0 || (int64_t)h[i] + span >= l_size) {
+      const int32_t bad = h[i];
+      free(h);
+      return CeedError(ceed, CEED_ERROR_DIMENSION, "restriction offset %d at entry %zu outside the L-vector of size %td", bad, i, l_size);
+    }
+  CeedElemRestriction r = (CeedElemRestriction)calloc(1, sizeof(*r));
+  r->ceed               = ceed;
+  ceed->ref++;
+  r->ref         = 1;
+  r->num_elem    = num_elem;
+  r->elem_size   = elem_size;
+  r->num_comp    = num_comp;
+  r->comp_stride = comp_stride;
+  r->l_size      = l_size;
+  r->h_off       = h;
+  *rstr          = r;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedElemRestrictionCreateStrided(Ceed ceed, CeedInt num_elem, CeedInt elem_size, CeedInt num_comp, CeedSize l_size, const CeedInt strides[3],
+                                     CeedElemRestriction *rstr) {
+  CeedElemRestriction r = (CeedElemRestriction)calloc(1, sizeof(*r));
+  r->ceed               = ceed;
+  ceed->ref++;
+  r->ref       = 1;
+  r->num_elem  = num_elem;
+  r->elem_size = elem_size;
+  r->num_comp  = num_comp;
+  r->l_size    = l_size;
+  r->strided   = 1;
+  if (strides == CEED_STRIDES_BACKEND) {
+    /* backend layout [elem][comp][node]: the layout the fused kernels read qdata and write jac_data in */
+    r->strides[0] = 1;
+    r->strides[1] = elem_size;
+    r->strides[2] = elem_size * num_comp;
+  } else memcpy(r->strides, strides, sizeof(r->strides));
+  const int64_t last = (int64_t)(elem_size - 1) * r->strides[0] + (int64_t)(num_comp - 1) * r->strides[1] + (int64_t)(num_elem - 1) * r->strides[2];
+  if (num_elem > 0 && (last >= l_size || last < 0)) {
+    CeedElemRestrictionDestroy(&r);
+    return CeedError(ceed, CEED_ERROR_DIMENSION, "strided restriction exceeds the L-vector size %td", l_size);
+  }
+  *rstr = r;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedElemRestrictionReferenceCopy(CeedElemRestriction rstr, CeedElemRestriction *rstr_copy) {
+  rstr->ref++;
+  CK(CeedElemRestrictionDestroy(rstr_copy));
+  *rstr_copy = rstr;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedElemRestrictionCreateVector(CeedElemRestriction r, CeedVector *l_vec, CeedVector *e_vec) {
+  if (l_vec) CK(CeedVectorCreate(r->ceed, r->l_size, l_vec));
+  if (e_vec) CK(CeedVectorCreate(r->ceed, (CeedSize)r->num_elem * r->elem_size * r->num_comp, e_vec));
+  return CEED_ERROR_SUCCESS;
+}
+
+static int rstr_upload(CeedElemRestriction r) {
+  if (r->strided) {
+    if (!r->d_strides) {
+      CUDA_CK(r->ceed, cudaMalloc((void **)&r->d_strides, sizeof(int32_t) * 3));
+      CUDA_CK(r->ceed, cudaMemcpy(r->d_strides, r->strides, sizeof(int32_t) * 3, cudaMemcpyHostToDevice));
+    }
+  } else if (!r->d_off) {
+    const size_t n = (size_t)r->num_elem * r->elem_size;
+    CUDA_CK(r->ceed, cudaMalloc((void **)&r->d_off, sizeof(int32_t) * (n ? n : 1)));
+    CUDA_CK(r->ceed, cudaMemcpy(r->d_off, r->h_off, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+/* transpose map: for each L entry, the E entries that map to it, in increasing E order (a serial scatter's order) */
+static int rstr_build_transpose(CeedElemRestriction r) {
+  if (r->d_tptr) return CEED_ERROR_SUCCESS;
+  const int64_t ne = (int64_t)r->num_elem * r->elem_size * r->num_comp;
+  int64_t      *ptr = (int64_t *)calloc((size_t)r->l_size + 1, sizeof(int64_t));
+  int64_t      *idx = (int64_t *)malloc(sizeof(int64_t) * (size_t)(ne ? ne : 1));
+  for (int64_t t = 0; t < ne; t++) {
+    const int64_t p = t % r->elem_size, rr = t / r->elem_size, c = rr % r->num_comp, el = rr / r->num_comp;
+    ptr[r->h_off[el * r->elem_size + p] + c * r->comp_stride + 1]++;
+  }
+  for (int64_t i = 0; i < r->l_size; i++) ptr[i + 1] += ptr[i];
+  int64_t *fill = (int64_t *)malloc(sizeof(int64_t) * (size_t)(r->l_size ? r->l_size : 1));
+  memcpy(fill, ptr, sizeof(int64_t) * (size_t)r->l_size);
+  /* E entries visited element by element, node by node: within one L entry this is increasing element order */
+  for (int64_t el = 0; el < r->num_elem; el++)
+    for (int64_t p = 0; p < r->elem_size; p++)
+      for (int64_t c = 0; c < r->num_comp; c++) {
+        const int64_t li = r->h_off[el * r->elem_size + p] + c * r->comp_stride;
+        idx[fill[li]++]  = (el * r->num_comp + c) * r->elem_size + p;
+      }
+  free(fill);
+  int err = 0;
+  if (cudaMalloc((void **)&r->d_tptr, sizeof(int64_t) * ((size_t)r->l_size + 1)) != cudaSuccess ||
+      cudaMalloc((void **)&r->d_teidx, sizeof(int64_t) * (size_t)(ne ? ne : 1)) != cudaSuccess ||
+      cudaMemcpy(r->d_tptr, ptr, sizeof(int64_t) * ((size_t)r->l_size + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(r->d_teidx, idx, sizeof(int64_t) * (size_t)ne, cudaMemcpyHostToDevice) != cudaSuccess)
+    err = 1;
+  free(ptr);
+  free(idx);
+  if (err) return CeedError(r->ceed, CEED_ERROR_BACKEND, "could not upload the transpose restriction map");
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedElemRestrictionApply(CeedElemRestriction r, CeedTransposeMode t_mode, CeedVector u, CeedVector ru, CeedRequest *request) {
+  (void)request;
+  CK(rstr_upload(r));
+  const double *in;
+  double       *out;
+  CK(vec_dev_read(u, &in));
+  if (t_mode == CEED_NOTRANSPOSE) {
+    CK(vec_dev_write(ru, &out, 1));
+    HB_CK(r->ceed, hb_restrict_apply(r->num_elem, r->elem_size, r->num_comp, r->comp_stride, r->strided ? NULL : r->d_off,
+                                     r->strided ? r->d_strides : NULL, in, out, r->ceed->stream));
+  } else {
+    /* libCEED semantics: the transpose adds into ru */
+    CK(vec_dev_write(ru, &out, 0));
+    if (r->strided) HB_CK(r->ceed, hb_restrict_apply_t_strided(r->num_elem, r->elem_size, r->num_comp, r->d_strides, in, out, r->ceed->stream));
+    else {
+      CK(rstr_build_transpose(r));
+      HB_CK(r->ceed, hb_restrict_apply_t_csr(r->l_size, r->d_tptr, r->d_teidx, in, out, r->ceed->stream));
+    }
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedElemRestrictionGetNumElements(CeedElemRestriction r, CeedInt *num_elem) {
+  *num_elem = r->num_elem;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedElemRestrictionGetElementSize(CeedElemRestriction r, CeedInt *elem_size) {
+  *elem_size = r->elem_size;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedElemRestrictionGetLVectorSize(CeedElemRestriction r, CeedSize *l_size) {
+  *l_size = r->l_size;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedElemRestrictionGetEVectorSize(CeedElemRestriction r, CeedSize *e_size) {
+  *e_size = (CeedSize)r->num_elem * r->elem_size * r->num_comp;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedElemRestrictionGetNumComponents(CeedElemRestriction r, CeedInt *num_comp) {
+  *num_comp = r->num_comp;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedElemRestrictionGetCompStride(CeedElemRestriction r, CeedInt *comp_stride) {
+  *comp_stride = r->comp_stride;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedElemRestrictionGetMultiplicity(CeedElemRestriction r, CeedVector mult) {
+  CeedVector e;
+  CK(CeedVectorCreate(r->ceed, (CeedSize)r->num_elem * r->elem_size * r->num_comp, &e));
+  CK(CeedVectorSetValue(e, 1.0));
+  CK(CeedVectorSetValue(mult, 0.0));
+  CK(CeedElemRestrictionApply(r, CEED_TRANSPOSE, e, mult, CEED_REQUEST_IMMEDIATE));
+  return CeedVectorDestroy(&e);
+}
+
+int CeedElemRestrictionDestroy(CeedElemRestriction *rstr) {
+  CeedElemRestriction r = *rstr;
+  if (!r || r == CEED_ELEMRESTRICTION_NONE) {
+    *rstr = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (--r->ref > 0) {
+    *rstr = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  free(r->h_off);
+  cudaFree(r->d_off);
+  cudaFree(r->d_strides);
+  cudaFree(r->d_tptr);
+  cudaFree(r->d_teidx);
+  Ceed ceed = r->ceed;
+  free(r);
+  *rstr = NULL;
+  return CeedDestroy(&ceed);
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* CeedBasis                                                                                                          */
+
+int CeedBasisCreateTensorH1(Ceed ceed, CeedInt dim, CeedInt num_comp, CeedInt P_1d, CeedInt Q_1d, const CeedScalar *interp_1d, const CeedScalar *grad_1d,
+                            const CeedScalar *q_ref_1d, const CeedScalar *q_weight_1d, CeedBasis *basis) {
+  if (dim < 1 || dim > 3 || P_1d < 1 || Q_1d < 1) return CeedError(ceed, CEED_ERROR_DIMENSION, "invalid tensor basis dimensions");
+  if (P_1d > HB_MAX_P || Q_1d > HB_MAX_P)
+    return CeedError(ceed, CEED_ERROR_UNSUPPORTED, "tensor bases with more than %d nodes or points per direction are not supported", HB_MAX_P);
+  CeedBasis b = (CeedBasis)calloc(1, sizeof(*b));
+  b->ceed     = ceed;
+  ceed->ref++;
+  b->ref      = 1;
+  b->dim      = dim;
+  b->num_comp = num_comp;
+  b->P1d      = P_1d;
+  b->Q1d      = Q_1d;
+  b->tensor   = 1;
+  memcpy(b->interp1d, interp_1d, sizeof(double) * P_1d * Q_1d);
+  memcpy(b->grad1d, grad_1d, sizeof(double) * P_1d * Q_1d);
+  if (q_ref_1d) memcpy(b->qref1d, q_ref_1d, sizeof(double) * Q_1d);
+  if (q_weight_1d) memcpy(b->qweight1d, q_weight_1d, sizeof(double) * Q_1d);
+  *basis = b;
+  return CEED_ERROR_SUCCESS;
+}
+
+static void legendre(int n, double x, double *p, double *dp) {
+  double p0 = 1, p1 = x;
+  if (n == 0) {
+    *p  = 1;
+    *dp = 0;
+    return;
+  }
+  for (int k = 2; k <= n; k++) {
+    const double p2 = ((2 * k - 1) * x * p1 - (k - 1) * p0) / k;
+    p0              = p1;
+    p1              = p2;
+  }
+  *p  = p1;
+  *dp = n * (x * p1 - p0) / (x * x - 1);
+}
+
+int CeedGaussQuadrature(CeedInt Q, CeedScalar *x, CeedScalar *w) {
+  for (int i = 0; i < Q; i++) {
+    double z = -cos(M_PI * (i + 0.75) / (Q + 0.5)), p, dp;
+    for (int it = 0; it < 100; it++) {
+      legendre(Q, z, &p, &dp);
+      const double dz = p / dp;
+      z -= dz;
+      if (fabs(dz) < 1e-16) break;
+    }
+    legendre(Q, z, &p, &dp);
+    x[i] = z;
+    if (w) w[i] = 2 / ((1 - z * z) * dp * dp);
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedLobattoQuadrature(CeedInt P, CeedScalar *x, CeedScalar *w) {
+  const int N = P - 1;
+  x[0]        = -1;
+  x[N]        = 1;
+  for (int i = 1; i < N; i++) {
+    double z = -cos(M_PI * i / N);
+    for (int it = 0; it < 100; it++) {
+      double p, dp;
+      legendre(N, z, &p, &dp);
+      const double ddp = (2 * z * dp - N * (N + 1) * p) / (1 - z * z), dz = dp / ddp;
+      z -= dz;
+      if (fabs(dz) < 1e-16) break;
+    }
+    x[i] = z;
+  }
+  if (w)
+    for (int i = 0; i <= N; i++) {
+      double p, dp;
+      legendre(N, x[i], &p, &dp);
+      w[i] = 2.0 / (N * (N + 1) * p * p);
+    }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedBasisCreateTensorH1Lagrange(Ceed ceed, CeedInt dim, CeedInt num_comp, CeedInt P, CeedInt Q, CeedQuadMode quad_mode, CeedBasis *basis) {
+  if (P > HB_MAX_P || Q > HB_MAX_P || P < 2) return CeedError(ceed, CEED_ERROR_UNSUPPORTED, "unsupported Lagrange basis size");
+  double nodes[HB_MAX_P], qx[HB_MAX_P], qw[HB_MAX_P], B[HB_MAX_P * HB_MAX_P], G[HB_MAX_P * HB_MAX_P];
+  CeedLobattoQuadrature(P, nodes, NULL);
+  if (quad_mode == CEED_GAUSS) CeedGaussQuadrature(Q, qx, qw);
+  else CeedLobattoQuadrature(Q, qx, qw);
+  for (int q = 0; q < Q; q++)
+    for (int j = 0; j < P; j++) {
+      double l = 1, dl = 0;
+      for (int m = 0; m < P; m++) {
+        if (m == j) continue;
+        const double f = (qx[q] - nodes[m]) / (nodes[j] - nodes[m]);
+        dl             = dl * f + l / (nodes[j] - nodes[m]);
+        l *= f;
+      }
+      B[q * P + j] = l;
+      G[q * P + j] = dl;
+    }
+  return CeedBasisCreateTensorH1(ceed, dim, num_comp, P, Q, B, G, qx, qw, basis);
+}
+
+int CeedBasisCreateH1(Ceed ceed, CeedElemTopology topo, CeedInt num_comp, CeedInt num_nodes, CeedInt nqpts, const CeedScalar *interp,
+                      const CeedScalar *grad, const CeedScalar *q_ref, const CeedScalar *q_weights, CeedBasis *basis) {
+  (void)topo, (void)num_comp, (void)num_nodes, (void)nqpts, (void)interp, (void)grad, (void)q_ref, (void)q_weights, (void)basis;
+  return CeedError(ceed, CEED_ERROR_UNSUPPORTED, "non-tensor H1 bases are outside the B200 backend's hex-element scope");
+}
+int CeedBasisCreateProjection(CeedBasis basis_from, CeedBasis basis_to, CeedBasis *basis_project) {
+  (void)basis_to, (void)basis_project;
+  return CeedError(basis_from->ceed, CEED_ERROR_UNSUPPORTED, "projection bases (initial-condition operators) are outside the backend scope");
+}
+
+int CeedBasisReferenceCopy(CeedBasis basis, CeedBasis *basis_copy) {
+  basis->ref++;
+  CK(CeedBasisDestroy(basis_copy));
+  *basis_copy = basis;
+  return CEED_ERROR_SUCCESS;
+}
+
+static int basis_upload(CeedBasis b) {
+  if (b->d_B) return CEED_ERROR_SUCCESS;
+  const size_t n = sizeof(double) * b->P1d * b->Q1d;
+  CUDA_CK(b->ceed, cudaMalloc((void **)&b->d_B, n));
+  CUDA_CK(b->ceed, cudaMalloc((void **)&b->d_G, n));
+  CUDA_CK(b->ceed, cudaMalloc((void **)&b->d_w, sizeof(double) * b->Q1d));
+  CUDA_CK(b->ceed, cudaMemcpy(b->d_B, b->interp1d, n, cudaMemcpyHostToDevice));
+  CUDA_CK(b->ceed, cudaMemcpy(b->d_G, b->grad1d, n, cudaMemcpyHostToDevice));
+  CUDA_CK(b->ceed, cudaMemcpy(b->d_w, b->qweight1d, sizeof(double) * b->Q1d, cudaMemcpyHostToDevice));
+  return CEED_ERROR_SUCCESS;
+}
+
+/* Layouts: nodal input/output [elem][comp][P^dim]; quadrature values [elem][comp][Q^dim], gradients
+ * [elem][dim][comp][Q^dim], weights [elem][Q^dim]. */
+int CeedBasisApply(CeedBasis b, CeedInt num_elem, CeedTransposeMode t_mode, CeedEvalMode eval_mode, CeedVector u, CeedVector v) {
+  if (eval_mode != CEED_EVAL_INTERP && eval_mode != CEED_EVAL_GRAD && eval_mode != CEED_EVAL_WEIGHT)
+    return CeedError(b->ceed, CEED_ERROR_UNSUPPORTED, "eval mode %d not supported", eval_mode);
+  CK(basis_upload(b));
+  const double *in = NULL;
+  double       *out;
+  if (eval_mode != CEED_EVAL_WEIGHT) CK(vec_dev_read(u, &in));
+  CK(vec_dev_write(v, &out, 1));
+  HB_CK(b->ceed, hb_basis_apply_generic(num_elem, b->num_comp, b->dim, b->P1d, b->Q1d, t_mode == CEED_TRANSPOSE, eval_mode, b->d_B, b->d_G, b->d_w,
+                                        in, out, b->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedBasisGetDimension(CeedBasis b, CeedInt *dim) {
+  *dim = b->dim;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedBasisGetNumComponents(CeedBasis b, CeedInt *num_comp) {
+  *num_comp = b->num_comp;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedBasisGetNumNodes(CeedBasis b, CeedInt *P) {
+  int n = 1;
+  for (int d = 0; d < b->dim; d++) n *= b->P1d;
+  *P = n;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedBasisGetNumNodes1D(CeedBasis b, CeedInt *P_1d) {
+  *P_1d = b->P1d;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedBasisGetNumQuadraturePoints(CeedBasis b, CeedInt *Q) {
+  int n = 1;
+  for (int d = 0; d < b->dim; d++) n *= b->Q1d;
+  *Q = n;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedBasisGetNumQuadraturePoints1D(CeedBasis b, CeedInt *Q_1d) {
+  *Q_1d = b->Q1d;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedBasisDestroy(CeedBasis *basis) {
+  CeedBasis b = *basis;
+  if (!b || b == CEED_BASIS_NONE) {
+    *basis = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (--b->ref > 0) {
+    *basis = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  cudaFree(b->d_B);
+  cudaFree(b->d_G);
+  cudaFree(b->d_w);
+  Ceed ceed = b->ceed;
+  free(b);
+  *basis = NULL;
+  return CeedDestroy(&ceed);
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* CeedQFunctionContext                                                                                               */
+
+int CeedQFunctionContextCreate(Ceed ceed, CeedQFunctionContext *ctx) {
+  CeedQFunctionContext c = (CeedQFunctionContext)calloc(1, sizeof(*c));
+  c->ceed                = ceed;
+  ceed->ref++;
+  c->ref = 1;
+  *ctx   = c;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionContextReferenceCopy(CeedQFunctionContext ctx, CeedQFunctionContext *ctx_copy) {
+  ctx->ref++;
+  CK(CeedQFunctionContextDestroy(ctx_copy));
+  *ctx_copy = ctx;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionContextSetData(CeedQFunctionContext ctx, CeedMemType mem_type, CeedCopyMode copy_mode, size_t size, void *data) {
+  if (mem_type != CEED_MEM_HOST) return CeedError(ctx->ceed, CEED_ERROR_UNSUPPORTED, "contexts are read from host memory at apply time");
+  if (ctx->own) free(ctx->data);
+  if (copy_mode == CEED_COPY_VALUES) {
+    ctx->data = malloc(size);
+    memcpy(ctx->data, data, size);
+    ctx->own = 1;
+  } else {
+    ctx->data = data;
+    ctx->own  = copy_mode == CEED_OWN_POINTER;
+  }
+  ctx->size = size;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionContextGetData(CeedQFunctionContext ctx, CeedMemType mem_type, void *data) {
+  if (mem_type != CEED_MEM_HOST) return CeedError(ctx->ceed, CEED_ERROR_UNSUPPORTED, "context data lives in host memory");
+  *(void **)data = ctx->data;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionContextGetDataRead(CeedQFunctionContext ctx, CeedMemType mem_type, void *data) { return CeedQFunctionContextGetData(ctx, mem_type, data); }
+int CeedQFunctionContextRestoreData(CeedQFunctionContext ctx, void *data) {
+  (void)ctx;
+  *(void **)data = NULL;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionContextRestoreDataRead(CeedQFunctionContext ctx, void *data) { return CeedQFunctionContextRestoreData(ctx, data); }
+int CeedQFunctionContextSetDataDestroy(CeedQFunctionContext ctx, CeedMemType f_mem_type, CeedQFunctionContextDataDestroyUser f) {
+  (void)f_mem_type;
+  ctx->destroy = f;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionContextRegisterDouble(CeedQFunctionContext ctx, const char *field_name, size_t field_offset, size_t num_values,
+                                       const char *field_description) {
+  (void)field_description;
+  for (int i = 0; i < ctx->nlabels; i++)
+    if (!strcmp(ctx->labels[i].name, field_name)) return CeedError(ctx->ceed, CEED_ERROR_MINOR, "context field '%s' already registered", field_name);
+  if (ctx->nlabels >= MAX_LABELS) return CeedError(ctx->ceed, CEED_ERROR_UNSUPPORTED, "too many context fields");
+  if (ctx->size && field_offset + num_values * sizeof(double) > ctx->size)
+    return CeedError(ctx->ceed, CEED_ERROR_DIMENSION, "context field '%s' exceeds the context size", field_name);
+  CtxLabel *l = &ctx->labels[ctx->nlabels++];
+  snprintf(l->name, sizeof l->name, "%s", field_name);
+  l->offset     = field_offset;
+  l->num_values = num_values;
+  l->type       = CEED_CONTEXT_FIELD_DOUBLE;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionContextGetContextSize(CeedQFunctionContext ctx, size_t *ctx_size) {
+  *ctx_size = ctx->size;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionContextDestroy(CeedQFunctionContext *ctx) {
+  CeedQFunctionContext c = *ctx;
+  if (!c) return CEED_ERROR_SUCCESS;
+  if (--c->ref > 0) {
+    *ctx = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (c->destroy) c->destroy(c->data);
+  else if (c->own) free(c->data);
+  Ceed ceed = c->ceed;
+  free(c);
+  *ctx = NULL;
+  return CeedDestroy(&ceed);
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* CeedQFunction                                                                                                      */
+
+int CeedQFunctionCreateInterior(Ceed ceed, CeedInt vec_length, CeedQFunctionUser f, const char *source, CeedQFunction *qf) {
+  if (!source) return CeedError(ceed, CEED_ERROR_INCOMPLETE, "QFunction source location is required");
+  CeedQFunction q = (CeedQFunction)calloc(1, sizeof(*q));
+  q->ceed         = ceed;
+  ceed->ref++;
+  q->ref     = 1;
+  q->vlength = vec_length;
+  q->f       = f;
+  snprintf(q->source, sizeof q->source, "%s", source);
+  const char *colon = strrchr(source, ':');
+  snprintf(q->kernel, sizeof q->kernel, "%s", colon ? colon + 1 : source);
+  *qf = q;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionReferenceCopy(CeedQFunction qf, CeedQFunction *qf_copy) {
+  qf->ref++;
+  CK(CeedQFunctionDestroy(qf_copy));
+  *qf_copy = qf;
+  return CEED_ERROR_SUCCESS;
+}
+static int qf_add(CeedQFunction qf, QFField *arr, int *n, const char *name, CeedInt size, CeedEvalMode emode) {
+  if (*n >= MAX_FIELDS) return CeedError(qf->ceed, CEED_ERROR_UNSUPPORTED, "too many QFunction fields");
+  QFField *f = &arr[(*n)++];
+  snprintf(f->name, sizeof f->name, "%s", name);
+  f->size  = size;
+  f->emode = emode;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionAddInput(CeedQFunction qf, const char *field_name, CeedInt size, CeedEvalMode eval_mode) {
+  return qf_add(qf, qf->in, &qf->nin, field_name, size, eval_mode);
+}
+int CeedQFunctionAddOutput(CeedQFunction qf, const char *field_name, CeedInt size, CeedEvalMode eval_mode) {
+  return qf_add(qf, qf->out, &qf->nout, field_name, size, eval_mode);
+}
+int CeedQFunctionSetContext(CeedQFunction qf, CeedQFunctionContext ctx) {
+  if (ctx) ctx->ref++;
+  CK(CeedQFunctionContextDestroy(&qf->ctx));
+  qf->ctx = ctx;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionGetContext(CeedQFunction qf, CeedQFunctionContext *ctx) {
+  *ctx = qf->ctx;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionSetUserFlopsEstimate(CeedQFunction qf, CeedSize flops) {
+  qf->user_flops = flops;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionGetKernelName(CeedQFunction qf, const char **kernel_name) {
+  *kernel_name = qf->kernel;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedQFunctionDestroy(CeedQFunction *qf) {
+  CeedQFunction q = *qf;
+  if (!q || q == CEED_QFUNCTION_NONE) {
+    *qf = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (--q->ref > 0) {
+    *qf = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  CeedQFunctionContextDestroy(&q->ctx);
+  Ceed ceed = q->ceed;
+  free(q);
+  *qf = NULL;
+  return CeedDestroy(&ceed);
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* CeedOperator: object model                                                                                         */
+
+int CeedOperatorCreate(Ceed ceed, CeedQFunction qf, CeedQFunction dqf, CeedQFunction dqfT, CeedOperator *op) {
+  (void)dqf, (void)dqfT;
+  if (!qf || qf == CEED_QFUNCTION_NONE) return CeedError(ceed, CEED_ERROR_INCOMPLETE, "operator needs a QFunction");
+  CeedOperator o = (CeedOperator)calloc(1, sizeof(*o));
+  o->ceed        = ceed;
+  ceed->ref++;
+  o->ref = 1;
+  qf->ref++;
+  o->qf = qf;
+  *op   = o;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorCreateComposite(Ceed ceed, CeedOperator *op) {
+  CeedOperator o = (CeedOperator)calloc(1, sizeof(*o));
+  o->ceed        = ceed;
+  ceed->ref++;
+  o->ref       = 1;
+  o->composite = 1;
+  *op          = o;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedCompositeOperatorCreate(Ceed ceed, CeedOperator *op) { return CeedOperatorCreateComposite(ceed, op); }
+int CeedOperatorReferenceCopy(CeedOperator op, CeedOperator *op_copy) {
+  op->ref++;
+  CK(CeedOperatorDestroy(op_copy));
+  *op_copy = op;
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedOperatorSetField(CeedOperator op, const char *field_name, CeedElemRestriction rstr, CeedBasis basis, CeedVector vec) {
+  if (op->composite) return CeedError(op->ceed, CEED_ERROR_INCOMPATIBLE, "cannot set a field on a composite operator");
+  OpField *f = NULL;
+  for (int i = 0; i < op->qf->nin && !f; i++)
+    if (!strcmp(op->qf->in[i].name, field_name)) f = &op->in[i];
+  for (int i = 0; i < op->qf->nout && !f; i++)
+    if (!strcmp(op->qf->out[i].name, field_name)) f = &op->out[i];
+  if (!f) return CeedError(op->ceed, CEED_ERROR_INCOMPLETE, "QFunction has no field named '%s'", field_name);
+  if (rstr && rstr != CEED_ELEMRESTRICTION_NONE) rstr->ref++;
+  if (basis && basis != CEED_BASIS_NONE) basis->ref++;
+  if (vec && vec != CEED_VECTOR_ACTIVE && vec != CEED_VECTOR_NONE) vec->ref++;
+  if (f->set) {
+    CeedElemRestrictionDestroy(&f->r);
+    CeedBasisDestroy(&f->b);
+    CeedVectorDestroy(&f->v);
+  }
+  f->r   = rstr;
+  f->b   = basis;
+  f->v   = vec;
+  f->set = 1;
+  op->plan = PLAN_NONE; /* re-plan on next apply */
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedOperatorCompositeAddSub(CeedOperator composite_op, CeedOperator sub_op) {
+  if (!composite_op->composite) return CeedError(composite_op->ceed, CEED_ERROR_MINOR, "not a composite operator");
+  if (composite_op->nsub >= MAX_SUBS) return CeedError(composite_op->ceed, CEED_ERROR_UNSUPPORTED, "too many sub-operators");
+  sub_op->ref++;
+  composite_op->subs[composite_op->nsub++] = sub_op;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedCompositeOperatorAddSub(CeedOperator composite_op, CeedOperator sub_op) { return CeedOperatorCompositeAddSub(composite_op, sub_op); }
+int CeedOperatorCompositeGetNumSub(CeedOperator op, CeedInt *num_suboperators) {
+  *num_suboperators = op->nsub;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorCompositeGetSubList(CeedOperator op, CeedOperator **sub_operators) {
+  *sub_operators = op->subs;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorSetName(CeedOperator op, const char *name) {
+  snprintf(op->name, sizeof op->name, "%s", name);
+  return CEED_ERROR_SUCCESS;
+}
+
+static int op_check_fields(CeedOperator op) {
+  for (int i = 0; i < op->qf->nin; i++)
+    if (!op->in[i].set) return CeedError(op->ceed, CEED_ERROR_INCOMPLETE, "operator field '%s' not set", op->qf->in[i].name);
+  for (int i = 0; i < op->qf->nout; i++)
+    if (!op->out[i].set) return CeedError(op->ceed, CEED_ERROR_INCOMPLETE, "operator field '%s' not set", op->qf->out[i].name);
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorCheckReady(CeedOperator op) {
+  if (op->composite) {
+    for (int i = 0; i < op->nsub; i++) CK(CeedOperatorCheckReady(op->subs[i]));
+    return CEED_ERROR_SUCCESS;
+  }
+  return op_check_fields(op);
+}
+
+static CeedElemRestriction op_active_rstr(CeedOperator op, int output) {
+  const int n = output ? op->qf->nout : op->qf->nin;
+  for (int i = 0; i < n; i++) {
+    OpField *f = output ? &op->out[i] : &op->in[i];
+    if (f->set && f->v == CEED_VECTOR_ACTIVE) return f->r;
+  }
+  return NULL;
+}
+int CeedOperatorGetActiveVectorLengths(CeedOperator op, CeedSize *input_size, CeedSize *output_size) {
+  CeedOperator o = op->composite ? (op->nsub ? op->subs[0] : NULL) : op;
+  if (!o) return CeedError(op->ceed, CEED_ERROR_INCOMPLETE, "empty composite operator");
+  CeedElemRestriction ri = op_active_rstr(o, 0), ro = op_active_rstr(o, 1);
+  if (input_size) *input_size = ri ? ri->l_size : -1;
+  if (output_size) *output_size = ro ? ro->l_size : -1;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* context labels: every QFunction context of op (or of its sub-operators) that registered field_name */
+static void label_collect(CeedOperator op, const char *name, CeedContextFieldLabel lab) {
+  if (op->composite) {
+    for (int i = 0; i < op->nsub; i++) label_collect(op->subs[i], name, lab);
+    return;
+  }
+  CeedQFunctionContext ctx = op->qf->ctx;
+  if (!ctx) return;
+  for (int k = 0; k < lab->n; k++)
+    if (lab->ent[k].ctx == ctx) return;
+  for (int i = 0; i < ctx->nlabels; i++)
+    if (!strcmp(ctx->labels[i].name, name) && lab->n < MAX_SUBS) {
+      lab->ent[lab->n].ctx        = ctx;
+      lab->ent[lab->n].offset     = ctx->labels[i].offset;
+      lab->ent[lab->n].num_values = ctx->labels[i].num_values;
+      lab->n++;
+    }
+}
+
+/* labels are owned by a small global pool so callers never free them (libCEED ties them to the operator) */
+#define LABEL_POOL 256
+static struct CeedContextFieldLabel_private label_pool[LABEL_POOL];
+static int                                  label_pool_n;
+
+int CeedOperatorGetContextFieldLabel(CeedOperator op, const char *field_name, CeedContextFieldLabel *field_label) {
+  struct CeedContextFieldLabel_private tmp;
+  memset(&tmp, 0, sizeof tmp);
+  label_collect(op, field_name, &tmp);
+  if (!tmp.n) {
+    *field_label = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  snprintf(tmp.name, sizeof tmp.name, "%s", field_name);
+  for (int i = 0; i < label_pool_n; i++)
+    if (!memcmp(&label_pool[i], &tmp, sizeof tmp)) {
+      *field_label = &label_pool[i];
+      return CEED_ERROR_SUCCESS;
+    }
+  if (label_pool_n >= LABEL_POOL) return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "too many context labels");
+  label_pool[label_pool_n] = tmp;
+  *field_label             = &label_pool[label_pool_n++];
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedOperatorSetContextDouble(CeedOperator op, CeedContextFieldLabel lab, double *values) {
+  if (!lab) return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "invalid context field label");
+  for (int k = 0; k < lab->n; k++) {
+    CeedQFunctionContext ctx = lab->ent[k].ctx;
+    memcpy((char *)ctx->data + lab->ent[k].offset, values, sizeof(double) * lab->ent[k].num_values);
+  }
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorGetContextDoubleRead(CeedOperator op, CeedContextFieldLabel lab, size_t *num_values, const double **values) {
+  if (!lab || !lab->n) return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "invalid context field label");
+  *num_values = lab->ent[0].num_values;
+  *values     = (const double *)((const char *)lab->ent[0].ctx->data + lab->ent[0].offset);
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorRestoreContextDoubleRead(CeedOperator op, CeedContextFieldLabel lab, const double **values) {
+  (void)op, (void)lab;
+  *values = NULL;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* CeedOperator: backend plans                                                                                        */
+
+static int is_tensor3(CeedBasis b, int ncomp) { return b && b != CEED_BASIS_NONE && b->tensor && b->dim == 3 && b->num_comp == ncomp; }
+
+static int plan_fail(CeedOperator op, const char *why) {
+  return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "operator '%s' (QFunction %s) has no B200 kernel: %s", op->name, op->qf->kernel, why);
+}
+
+/* element-level restriction + basis pair of the Newtonian state fields */
+static int plan_elemop(CeedOperator op, CeedElemRestriction r, CeedBasis b) {
+  if (!r || r == CEED_ELEMRESTRICTION_NONE || r->strided) return plan_fail(op, "state field needs an offset restriction");
+  if (r->num_comp != 5 || r->comp_stride != 1) return plan_fail(op, "state restriction must be 5 node-interleaved components (comp_stride 1)");
+  if (!is_tensor3(b, 5)) return plan_fail(op, "state basis must be a 3D tensor H1 basis with 5 components");
+  if (r->elem_size != b->P1d * b->P1d * b->P1d) return plan_fail(op, "restriction element size does not match the basis");
+  if (!op->eop) {
+    HB_CK(op->ceed, hb_elemop_create(r->num_elem, b->P1d, b->Q1d, r->h_off, r->l_size, b->interp1d, b->grad1d, b->qref1d, b->qweight1d, &op->eop));
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+static int check_qdata_rstr(CeedOperator op, CeedElemRestriction r, int ncomp, int Q3, const char *what) {
+  if (!r || r == CEED_ELEMRESTRICTION_NONE || !r->strided || r->num_comp != ncomp || r->elem_size != Q3)
+    return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "%s must use a strided restriction with %d components at %d points", what, ncomp, Q3);
+  if (r->strides[0] != 1 || r->strides[1] != Q3 || r->strides[2] != Q3 * ncomp)
+    return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "%s must use the backend [elem][comp][point] layout (CEED_STRIDES_BACKEND)", what);
+  return CEED_ERROR_SUCCESS;
+}
+
+/* gather the coordinate field of an input (restriction with 3 comps, P=2 basis) into an E-vector [E][3][8] */
+static int gather_coords(CeedOperator op, OpField *fx, CeedVector xvec, double **d_xe) {
+  CeedElemRestriction r = fx->r;
+  if (!r || r == CEED_ELEMRESTRICTION_NONE || r->num_comp != 3 || r->elem_size != 8 || !fx->b || fx->b == CEED_BASIS_NONE || fx->b->P1d != 2)
+    return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "coordinate field must be a trilinear (P=2) 3-component field");
+  CK(rstr_upload(r));
+  const size_t nb = sizeof(double) * 24 * (size_t)r->num_elem;
+  if (!*d_xe) CUDA_CK(op->ceed, cudaMalloc((void **)d_xe, nb));
+  const double *x;
+  CK(vec_dev_read(xvec, &x));
+  HB_CK(op->ceed, hb_restrict_apply(r->num_elem, 8, 3, r->comp_stride, r->strided ? NULL : r->d_off, r->strided ? r->d_strides : NULL, x, *d_xe,
+                                    op->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+
+static int op_plan(CeedOperator op) {
+  if (op->plan != PLAN_NONE) return CEED_ERROR_SUCCESS;
+  CK(op_check_fields(op));
+  CeedQFunction qf = op->qf;
+  const char   *k  = qf->kernel;
+  if (!strcmp(k, "Setup")) {
+    /* inputs: "dx" (GRAD of coordinates), "weight" (WEIGHT); output: qdata (NONE, strided) */
+    if (qf->nin != 2 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_GRAD || qf->in[1].emode != CEED_EVAL_WEIGHT ||
+        qf->out[0].emode != CEED_EVAL_NONE || qf->out[0].size != 10)
+      return plan_fail(op, "unexpected Setup field layout");
+    if (op->in[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "Setup expects the coordinates as the active input");
+    CeedBasis bx = op->in[0].b;
+    if (!is_tensor3(bx, 3) || bx->P1d != 2) return plan_fail(op, "Setup needs a trilinear coordinate basis");
+    CK(check_qdata_rstr(op, op->out[0].r, 10, bx->Q1d * bx->Q1d * bx->Q1d, "qdata"));
+    op->plan = PLAN_SETUP;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (!strcmp(k, "IFunction_Newtonian_Conserv")) {
+    if (qf->nin < 5 || qf->nout != 3 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[1].emode != CEED_EVAL_GRAD ||
+        qf->in[2].emode != CEED_EVAL_INTERP || qf->in[3].emode != CEED_EVAL_NONE || qf->out[0].emode != CEED_EVAL_INTERP ||
+        qf->out[1].emode != CEED_EVAL_GRAD || qf->out[2].emode != CEED_EVAL_NONE)
+      return plan_fail(op, "unexpected IFunction field layout (src/setuplibceed.c:216-230)");
+    if (qf->nin > 5) return plan_fail(op, "projected divergence of the diffusive flux is not supported");
+    if (op->in[0].v != CEED_VECTOR_ACTIVE || op->in[1].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE ||
+        op->out[1].v != CEED_VECTOR_ACTIVE)
+      return plan_fail(op, "q/Grad_q and v/Grad_v must be active");
+    if (op->in[0].r != op->in[1].r || op->in[0].r != op->in[2].r || op->in[0].r != op->out[0].r || op->in[0].r != op->out[1].r)
+      return plan_fail(op, "state fields must share one restriction");
+    if (op->in[0].b != op->in[1].b || op->in[0].b != op->in[2].b || op->in[0].b != op->out[0].b || op->in[0].b != op->out[1].b)
+      return plan_fail(op, "state fields must share one basis");
+    if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+    CK(plan_elemop(op, op->in[0].r, op->in[0].b));
+    const int Q3 = op->eop->Q * op->eop->Q * op->eop->Q;
+    CK(check_qdata_rstr(op, op->in[3].r, 10, Q3, "qdata"));
+    const int njd = qf->out[2].size;
+    if (njd != 14 && njd != 15) return plan_fail(op, "jac_data must have 14 or 15 components");
+    CK(check_qdata_rstr(op, op->out[2].r, njd, Q3, "jac_data"));
+    op->plan = PLAN_IFUNCTION;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (!strcmp(k, "IJacobian_Newtonian_Conserv")) {
+    if (qf->nin != 4 || qf->nout != 2 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[1].emode != CEED_EVAL_GRAD ||
+        qf->in[2].emode != CEED_EVAL_NONE || qf->in[3].emode != CEED_EVAL_NONE || qf->out[0].emode != CEED_EVAL_INTERP ||
+        qf->out[1].emode != CEED_EVAL_GRAD)
+      return plan_fail(op, "unexpected IJacobian field layout (src/setuplibceed.c:252-266)");
+    if (op->in[0].v != CEED_VECTOR_ACTIVE || op->in[1].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE ||
+        op->out[1].v != CEED_VECTOR_ACTIVE)
+      return plan_fail(op, "dq/Grad_dq and v/Grad_v must be active");
+    if (op->in[0].r != op->in[1].r || op->in[0].r != op->out[0].r || op->in[0].r != op->out[1].r) return plan_fail(op, "shared restriction expected");
+    if (op->in[0].b != op->in[1].b || op->in[0].b != op->out[0].b || op->in[0].b != op->out[1].b) return plan_fail(op, "shared basis expected");
+    if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+    CK(plan_elemop(op, op->in[0].r, op->in[0].b));
+    const int Q3 = op->eop->Q * op->eop->Q * op->eop->Q;
+    CK(check_qdata_rstr(op, op->in[2].r, 10, Q3, "qdata"));
+    const int njd = qf->in[3].size;
+    if (njd != 14 && njd != 15) return plan_fail(op, "jac_data must have 14 or 15 components");
+    CK(check_qdata_rstr(op, op->in[3].r, njd, Q3, "jac_data"));
+    op->plan = PLAN_IJACOBIAN;
+    return CEED_ERROR_SUCCESS;
+  }
+  return plan_fail(op, "no fused kernel for this QFunction (no CPU fallback on /gpu/b200)");
+}
+
+static int vec_f32_shadow(CeedVector v) {
+  if (!v->d_f32) CUDA_CK(v->ceed, cudaMalloc((void **)&v->d_f32, sizeof(float) * (size_t)(v->length ? v->length : 1)));
+  return CEED_ERROR_SUCCESS;
+}
+
+/* apply one non-composite operator, adding into out (out already holds what should be kept) */
+static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
+  CK(op_plan(op));
+  Ceed         ceed = op->ceed;
+  cudaStream_t s    = ceed->stream;
+  switch (op->plan) {
+    case PLAN_SETUP: {
+      CeedBasis bx = op->in[0].b;
+      CK(gather_coords(op, &op->in[0], in, &op->d_tmp_e));
+      double *qd;
+      CK(vec_dev_write(out, &qd, 0));
+      /* Setup writes (not adds) qdata: libCEED's strided output of an EVAL_NONE field is overwritten per element */
+      HB_CK(ceed, hb_setup_qdata(op->in[0].r->num_elem, bx->Q1d, bx->qref1d, bx->qweight1d, op->d_tmp_e, qd, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_IFUNCTION: {
+      const HbNewtonianContext *ctx = (const HbNewtonianContext *)op->qf->ctx->data;
+      if (ctx->idl_enable && !op->idl_coords_set) {
+        CeedVector xv = op->in[4].v;
+        if (!xv || xv == CEED_VECTOR_ACTIVE || xv == CEED_VECTOR_NONE) return plan_fail(op, "IDL needs the coordinate field 'x'");
+        CK(gather_coords(op, &op->in[4], xv, &op->eop->d_x_elem));
+        op->idl_coords_set = 1;
+      }
+      HbIFunctionIO io;
+      memset(&io, 0, sizeof io);
+      CK(vec_dev_read(in, &io.q));
+      CK(vec_dev_read(op->in[2].v, &io.q_dot));
+      CK(vec_dev_read(op->in[3].v, &io.qdata));
+      CeedVector jd = op->out[2].v;
+      if (ceed->mixed) {
+        CK(vec_f32_shadow(jd));
+        io.jac_data_f32 = jd->d_f32;
+        jd->f32_valid   = 1;
+        jd->f64_stale   = 1;
+        jd->h_valid = jd->d_valid = 0;
+      } else {
+        double *jdd;
+        CK(vec_dev_write(jd, &jdd, 1));
+        io.jac_data = jdd;
+      }
+      double *v;
+      CK(vec_dev_write(out, &v, 0));
+      io.v   = v;
+      io.add = 1;
+      HB_CK(ceed, hb_ifunction_apply(op->eop, ctx, &io, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_IJACOBIAN: {
+      const HbNewtonianContext *ctx = (const HbNewtonianContext *)op->qf->ctx->data;
+      const double             *qd;
+      CK(vec_dev_read(op->in[2].v, &qd));
+      CeedVector jd = op->in[3].v;
+      if (ceed->mixed) {
+        if (!jd->f32_valid) {
+          const double *j64;
+          CK(vec_dev_read(jd, &j64));
+          CK(vec_f32_shadow(jd));
+          HB_CK(ceed, hb_vec_f64_to_f32(j64, jd->d_f32, jd->length, 0, s));
+          jd->f32_valid = 1;
+        }
+        const int64_t n = op->eop->l_size;
+        if (!op->d_tmp_in32) {
+          CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_in32, sizeof(float) * (size_t)n));
+          CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_out32, sizeof(float) * (size_t)n));
+        }
+        const double *x;
+        double       *y;
+        CK(vec_dev_read(in, &x));
+        CK(vec_dev_write(out, &y, 0));
+        HB_CK(ceed, hb_vec_f64_to_f32(x, op->d_tmp_in32, n, 0, s));
+        HB_CK(ceed, hb_ijacobian_apply_f32(op->eop, ctx, qd, jd->d_f32, op->d_tmp_in32, op->d_tmp_out32, 0, s));
+        HB_CK(ceed, hb_vec_f32_to_f64(op->d_tmp_out32, y, n, 1, s));
+      } else {
+        const double *j64, *x;
+        double       *y;
+        CK(vec_dev_read(jd, &j64));
+        CK(vec_dev_read(in, &x));
+        CK(vec_dev_write(out, &y, 0));
+        HB_CK(ceed, hb_ijacobian_apply_f64(op->eop, ctx, qd, j64, x, y, 1, s));
+      }
+      return CEED_ERROR_SUCCESS;
+    }
+  }
+  return plan_fail(op, "unplanned operator");
+}
+
+static int op_apply_add(CeedOperator op, CeedVector in, CeedVector out) {
+  if (op->composite) {
+    for (int i = 0; i < op->nsub; i++) CK(op_apply_add_single(op->subs[i], in, out));
+    return CEED_ERROR_SUCCESS;
+  }
+  return op_apply_add_single(op, in, out);
+}
+
+int CeedOperatorApply(CeedOperator op, CeedVector in, CeedVector out, CeedRequest *request) {
+  (void)request;
+  if (out && out != CEED_VECTOR_NONE) {
+    /* Setup overwrites; everything else accumulates after zeroing */
+    int only_setup = !op->composite && (op_plan(op) == 0) && op->plan == PLAN_SETUP;
+    if (!only_setup) CK(CeedVectorSetValue(out, 0.0));
+  }
+  return op_apply_add(op, in, out);
+}
+
+int CeedOperatorApplyAdd(CeedOperator op, CeedVector in, CeedVector out, CeedRequest *request) {
+  (void)request;
+  return op_apply_add(op, in, out);
+}
+
+static int op_diag_add_single(CeedOperator op, CeedVector assembled) {
+  CK(op_plan(op));
+  if (op->plan != PLAN_IJACOBIAN) return plan_fail(op, "diagonal assembly is provided for the IJacobian operator");
+  Ceed                      ceed = op->ceed;
+  cudaStream_t              s    = ceed->stream;
+  const HbNewtonianContext *ctx  = (const HbNewtonianContext *)op->qf->ctx->data;
+  const double             *qd;
+  CK(vec_dev_read(op->in[2].v, &qd));
+  CeedVector jd = op->in[3].v;
+  double    *y;
+  if (ceed->mixed) {
+    if (!jd->f32_valid) {
+      const double *j64;
+      CK(vec_dev_read(jd, &j64));
+      CK(vec_f32_shadow(jd));
+      HB_CK(ceed, hb_vec_f64_to_f32(j64, jd->d_f32, jd->length, 0, s));
+      jd->f32_valid = 1;
+    }
+    const int64_t n = op->eop->l_size;
+    if (!op->d_tmp_out32) {
+      CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_in32, sizeof(float) * (size_t)n));
+      CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_out32, sizeof(float) * (size_t)n));
+    }
+    CK(vec_dev_write(assembled, &y, 0));
+    HB_CK(ceed, hb_diagonal_assemble_f32(op->eop, ctx, qd, jd->d_f32, op->d_tmp_out32, 0, s));
+    HB_CK(ceed, hb_vec_f32_to_f64(op->d_tmp_out32, y, n, 1, s));
+  } else {
+    const double *j64;
+    CK(vec_dev_read(jd, &j64));
+    CK(vec_dev_write(assembled, &y, 0));
+    HB_CK(ceed, hb_diagonal_assemble_f64(op->eop, ctx, qd, j64, y, 1, s));
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedOperatorLinearAssembleAddDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request) {
+  (void)request;
+  if (op->composite) {
+    for (int i = 0; i < op->nsub; i++) CK(op_diag_add_single(op->subs[i], assembled));
+    return CEED_ERROR_SUCCESS;
+  }
+  return op_diag_add_single(op, assembled);
+}
+
+int CeedOperatorLinearAssembleDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request) {
+  CK(CeedVectorSetValue(assembled, 0.0));
+  return CeedOperatorLinearAssembleAddDiagonal(op, assembled, request);
+}
+
+/* Flop estimate: sum-factorised basis (interp + collocated gradient and their transposes) plus the point-wise counts
+ * of the fused kernels (measured with the oracle's counting build: about 700 flops per IFunction point and 520 per
+ * IJacobian point at conservative variables with SUPG). */
+int CeedOperatorGetFlopsEstimate(CeedOperator op, CeedSize *flops) {
+  *flops = 0;
+  if (op->composite) {
+    for (int i = 0; i < op->nsub; i++) {
+      CeedSize f;
+      CK(CeedOperatorGetFlopsEstimate(op->subs[i], &f));
+      *flops += f;
+    }
+    return CEED_ERROR_SUCCESS;
+  }
+  CK(op_plan(op));
+  if (!op->eop) return CEED_ERROR_SUCCESS;
+  const CeedSize P = op->eop->P, Q = op->eop->Q, E = op->eop->num_elem, Q3 = Q * Q * Q;
+  const CeedSize interp = 2 * (Q * P * P * P + Q * Q * P * P + Q * Q * Q * P), deriv = 2 * 3 * Q3 * Q;
+  if (op->plan == PLAN_IFUNCTION) *flops = E * (5 * (2 * (interp + deriv)) + 5 * interp + 700 * Q3);
+  else if (op->plan == PLAN_IJACOBIAN) *flops = E * (5 * (2 * (interp + deriv)) + 520 * Q3);
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedOperatorDestroy(CeedOperator *op) {
+  CeedOperator o = *op;
+  if (!o) return CEED_ERROR_SUCCESS;
+  if (--o->ref > 0) {
+    *op = NULL;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (o->composite) {
+    for (int i = 0; i < o->nsub; i++) CeedOperatorDestroy(&o->subs[i]);
+  } else {
+    for (int i = 0; i < o->qf->nin; i++)
+      if (o->in[i].set) {
+        CeedElemRestrictionDestroy(&o->in[i].r);
+        CeedBasisDestroy(&o->in[i].b);
+        CeedVectorDestroy(&o->in[i].v);
+      }
+    for (int i = 0; i < o->qf->nout; i++)
+      if (o->out[i].set) {
+        CeedElemRestrictionDestroy(&o->out[i].r);
+        CeedBasisDestroy(&o->out[i].b);
+        CeedVectorDestroy(&o->out[i].v);
+      }
+    CeedQFunctionDestroy(&o->qf);
+  }
+  hb_elemop_destroy(o->eop);
+  cudaFree(o->d_tmp_in32);
+  cudaFree(o->d_tmp_out32);
+  cudaFree(o->d_tmp_e);
+  Ceed ceed = o->ceed;
+  free(o);
+  *op = NULL;
+  return CeedDestroy(&ceed);
+}

@@ -1,0 +1,338 @@
+// newtonian_qf.cuh -- point-wise Newtonian ideal-gas physics for the fused sm_100a kernels.
+//
+// Device restatement of the reference QFunctions, specialised to conservative state variables:
+//   IFunction_Newtonian / IFunction_Newtonian_Integrand   qfunctions/newtonian.h:205-257, newtonian_integrands.h:87-115
+//   IJacobian_Newtonian / IJacobian_Newtonian_Integrand   qfunctions/newtonian.h:272-311, newtonian_integrands.h:134-166
+//   Tau_diagPrim, Stabilization, StabilizationMatrix      qfunctions/stabilization.h:25-100
+//   state algebra and fluxes                              qfunctions/newtonian_state.h:64-89, 170-184, 425-574
+// The arithmetic is reorganised for the GPU: reciprocals of density/cv are formed once and multiplied, only the rows of
+// the linearised flux that are used are formed, and terms known to be zero (time derivative of Y, divergence of the
+// diffusive flux when its projection is off) are dropped.  The result equals the reference to rounding (a few ulp per
+// quantity); parity tests bound the operator-level difference.  Templated on the arithmetic type so the same source
+// gives the FP64 residual/Jacobian and the FP32 Jacobian of the mixed-precision solver.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "honee_b200_types.h"
+
+namespace hb {
+
+// Per-launch physical constants derived once on the host from the 184-byte context.
+template <typename T>
+struct PhysConst {
+  T mu, lambda, k, cv, inv_cv, gm1;  // gm1 = cp/cv - 1
+  T Rgas;                            // cp - cv
+  T g[3];
+  T shift;                           // ijacobian time shift
+  T Ctau_C, Ctau_M, Ctau_E, Ctau_v;
+  T dts;                             // Ctau_t / dt
+  int stab;                          // HbStabilizationType
+  int idl_enable;
+  T idl_amplitude, idl_start, idl_length, idl_pressure;
+};
+
+template <typename T>
+struct St {  // state: conservative U and primitive Y
+  T rho, m[3], E;
+  T P, u[3], T_;
+};
+
+template <typename T>
+__device__ __forceinline__ T rcp(T x) { return T(1) / x; }
+
+// StateFromU (newtonian_state.h:64-73, 379-388); also returns 1/rho and the specific energies used by the tangents.
+template <typename T>
+__device__ __forceinline__ void state_from_u(const PhysConst<T> &c, const T q[5], St<T> &s, T &inv_rho, T &etot, T &eint) {
+  s.rho = q[0];
+  s.m[0] = q[1];
+  s.m[1] = q[2];
+  s.m[2] = q[3];
+  s.E = q[4];
+  inv_rho = rcp(s.rho);
+  for (int i = 0; i < 3; i++) s.u[i] = s.m[i] * inv_rho;
+  const T ke = T(.5) * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]);
+  etot = s.E * inv_rho;
+  eint = etot - ke;
+  s.T_ = eint * c.inv_cv;
+  s.P = c.gm1 * s.rho * eint;
+}
+
+// StateFromU_fwd (newtonian_state.h:75-89, 390-400): tangent of Y for a conservative tangent dU.
+template <typename T>
+__device__ __forceinline__ void state_from_u_fwd(const PhysConst<T> &c, const St<T> &s, T inv_rho, T etot, T eint, const T dU[5], St<T> &ds) {
+  ds.rho = dU[0];
+  ds.m[0] = dU[1];
+  ds.m[1] = dU[2];
+  ds.m[2] = dU[3];
+  ds.E = dU[4];
+  for (int i = 0; i < 3; i++) ds.u[i] = (ds.m[i] - s.u[i] * ds.rho) * inv_rho;
+  const T dke = ds.u[0] * s.u[0] + ds.u[1] * s.u[1] + ds.u[2] * s.u[2];
+  const T detot = (ds.E - etot * ds.rho) * inv_rho;
+  const T deint = detot - dke;
+  ds.T_ = deint * c.inv_cv;
+  ds.P = c.gm1 * (ds.rho * eint + s.rho * deint);
+}
+
+// StateFromY_fwd (newtonian_state.h:170-184, 358-369): conservative tangent of a primitive tangent dY.
+template <typename T>
+__device__ __forceinline__ void state_from_y_fwd(const PhysConst<T> &c, const St<T> &s, T eint, const T dY[5], St<T> &ds) {
+  ds.P = dY[0];
+  ds.u[0] = dY[1];
+  ds.u[1] = dY[2];
+  ds.u[2] = dY[3];
+  ds.T_ = dY[4];
+  const T Tt = s.T_;
+  ds.rho = (dY[0] * Tt - s.P * dY[4]) / (c.Rgas * Tt * Tt);
+  for (int i = 0; i < 3; i++) ds.m[i] = ds.rho * s.u[i] + s.rho * ds.u[i];
+  const T ke = T(.5) * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]);
+  const T dke = ds.u[0] * s.u[0] + ds.u[1] * s.u[1] + ds.u[2] * s.u[2];
+  const T e_int = c.cv * Tt;
+  const T de_int = c.cv * dY[4];
+  ds.E = ds.rho * (e_int + ke) + s.rho * (de_int + dke);
+  (void)eint;
+}
+
+// Row i of the linearised inviscid flux (newtonian_state.h:433-442): dF_i for components 0..4.
+template <typename T>
+__device__ __forceinline__ void dflux_row(const St<T> &s, const St<T> &ds, int i, T r[5]) {
+  r[0] = ds.m[i];
+  for (int j = 0; j < 3; j++) r[1 + j] = ds.m[i] * s.u[j] + s.m[i] * ds.u[j] + (i == j ? ds.P : T(0));
+  r[4] = (ds.E + ds.P) * s.u[i] + (s.E + s.P) * ds.u[i];
+}
+
+// Diagonal tau (stabilization.h:67-100).
+template <typename T>
+__device__ __forceinline__ void tau_diag(const PhysConst<T> &c, const St<T> &s, const T X[3][3], T tau[3]) {
+  T g[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) g[i][j] = X[0][i] * X[0][j] + X[1][i] * X[1][j] + X[2][i] * X[2][j];
+  T ugu = 0, g2 = 0;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    ugu += s.u[i] * (g[i][0] * s.u[0] + g[i][1] * s.u[1] + g[i][2] * s.u[2]);
+#pragma unroll
+    for (int j = 0; j < 3; j++) g2 += g[i][j] * g[i][j];
+  }
+  const T tsum = s.rho * s.rho * (T(4) * c.dts * c.dts + ugu) + c.Ctau_v * c.mu * c.mu * g2;
+  const T f = sqrt(tsum);
+  const T inv_f = rcp(f);
+  tau[0] = c.Ctau_C * f / (s.rho * (g[0][0] + g[1][1] + g[2][2])) * T(0.125);
+  tau[1] = c.Ctau_M * inv_f;
+  tau[2] = c.Ctau_E * inv_f * c.inv_cv;
+}
+
+// SU/SUPG term stab[comp][dir] = dF_dir(StateFromY_fwd(tau . r)) with r the strong residual (stabilization.h:25-58).
+template <typename T>
+__device__ __forceinline__ void stabilization(const PhysConst<T> &c, const St<T> &s, T eint, const T tau[3], const St<T> gs[3],
+                                              const T Udot[5], const T body[5], T stab[5][3]) {
+  if (c.stab == HB_STAB_NONE) {
+#pragma unroll
+    for (int i = 0; i < 5; i++) stab[i][0] = stab[i][1] = stab[i][2] = 0;
+    return;
+  }
+  T r[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    T row[5];
+    dflux_row(s, gs[i], i, row);
+#pragma unroll
+    for (int j = 0; j < 5; j++) r[j] += row[j];
+  }
+  if (c.stab == HB_STAB_SUPG) {
+#pragma unroll
+    for (int j = 0; j < 5; j++) r[j] += Udot[j] - body[j];
+  }
+  const T dY[5] = {tau[0] * r[0], tau[1] * r[1], tau[1] * r[2], tau[1] * r[3], tau[2] * r[4]};
+  St<T> d;
+  state_from_y_fwd(c, s, eint, dY, d);
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    T row[5];
+    dflux_row(s, d, i, row);
+#pragma unroll
+    for (int j = 0; j < 5; j++) stab[j][i] = row[j];
+  }
+}
+
+// KM strain rate from velocity gradients gs[j].u[i] = du_i/dx_j (newtonian_state.h:509-537).
+template <typename T>
+__device__ __forceinline__ void km_strain(const St<T> gs[3], T e[6]) {
+  const T w = T(1.0 / 1.4142135623730951);  // 1/sqrt(2.) in the working precision (utils.h:240)
+  e[0] = gs[0].u[0];
+  e[1] = gs[1].u[1];
+  e[2] = gs[2].u[2];
+  e[3] = w * (gs[2].u[1] + gs[1].u[2]);
+  e[4] = w * (gs[2].u[0] + gs[0].u[2]);
+  e[5] = w * (gs[1].u[0] + gs[0].u[1]);
+}
+
+// Full stress tensor from a KM strain rate (NewtonianStress + KMUnpack, newtonian_state.h:553-558, utils.h:239-247).
+template <typename T>
+__device__ __forceinline__ void stress_full(const PhysConst<T> &c, const T e[6], T sig[3][3]) {
+  const T w = T(1.0 / 1.4142135623730951);
+  const T div = e[0] + e[1] + e[2];
+  const T ld = c.lambda * div;
+  sig[0][0] = c.mu * (T(2) * e[0] + ld);
+  sig[1][1] = c.mu * (T(2) * e[1] + ld);
+  sig[2][2] = c.mu * (T(2) * e[2] + ld);
+  sig[1][2] = sig[2][1] = w * (c.mu * (T(2) * e[3]));
+  sig[0][2] = sig[2][0] = w * (c.mu * (T(2) * e[4]));
+  sig[0][1] = sig[1][0] = w * (c.mu * (T(2) * e[5]));
+}
+
+// Physical gradient of the state (StatePhysicalGradientFromReference, newtonian_state.h:581-593):
+// gref[d][c] reference derivatives, X = dXdx; dq[c][j] = sum_k gref[k][c] X[k][j].
+template <typename T>
+__device__ __forceinline__ void physical_gradient(const PhysConst<T> &c, const St<T> &s, T inv_rho, T etot, T eint, const T gref[3][5],
+                                                  const T X[3][3], St<T> gs[3]) {
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    T dq[5];
+#pragma unroll
+    for (int cc = 0; cc < 5; cc++) dq[cc] = gref[0][cc] * X[0][j] + gref[1][cc] * X[1][j] + gref[2][cc] * X[2][j];
+    state_from_u_fwd(c, s, inv_rho, etot, eint, dq, gs[j]);
+  }
+}
+
+// IDL ramp (utils.h:287-295)
+template <typename T>
+__device__ __forceinline__ T linear_ramp(T amplitude, T length, T start, T x) {
+  if (x < start) return amplitude;
+  if (x < start + length) return amplitude * ((x - start) * (T(-1) / length) + T(1));
+  return T(0);
+}
+
+// IFunction at one quadrature point. Inputs: q[5], reference gradient gref[3][5], q_dot[5], qdata (wdetJ, X).
+// Outputs: v[5], grad_v[3][5] in reference directions (already multiplied by wdetJ X), and the 14 stored values.
+template <typename T>
+__device__ __forceinline__ void ifunction_point(const PhysConst<T> &c, const T q[5], const T gref[3][5], const T qdot[5], T wdetJ, const T X[3][3],
+                                                T x0, T v[5], T gv[3][5], T jd[15]) {
+  St<T> s;
+  T inv_rho, etot, eint;
+  state_from_u(c, q, s, inv_rho, etot, eint);
+  St<T> gs[3];
+  physical_gradient(c, s, inv_rho, etot, eint, gref, X, gs);
+
+  T e[6], sig[3][3];
+  km_strain(gs, e);
+  stress_full(c, e, sig);
+
+  // -F_total + stab, F_total[comp][dir] (newtonian_state.h:477-484), viscous energy flux (:560-565)
+  T gvi[5][3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const T Fe = -s.u[0] * sig[0][j] - s.u[1] * sig[1][j] - s.u[2] * sig[2][j] - c.k * gs[j].T_;
+    gvi[0][j] = -s.m[j];
+#pragma unroll
+    for (int kk = 0; kk < 3; kk++) gvi[1 + kk][j] = -(s.m[j] * s.u[kk] + (j == kk ? s.P : T(0)) - sig[kk][j]);
+    gvi[4][j] = -((s.E + s.P) * s.u[j] + Fe);
+  }
+  const T body[5] = {T(0), s.rho * c.g[0], s.rho * c.g[1], s.rho * c.g[2], s.m[0] * c.g[0] + s.m[1] * c.g[1] + s.m[2] * c.g[2]};
+  T vi[5];
+#pragma unroll
+  for (int j = 0; j < 5; j++) vi[j] = qdot[j] - body[j];
+
+  T tau[3], stab[5][3];
+  tau_diag(c, s, X, tau);
+  stabilization(c, s, eint, tau, gs, qdot, body, stab);
+#pragma unroll
+  for (int j = 0; j < 5; j++)
+#pragma unroll
+    for (int d = 0; d < 3; d++) gvi[j][d] += stab[j][d];
+
+  T sigma = 0;
+  if (c.idl_enable) {  // newtonian_integrands.h:38-45
+    sigma = linear_ramp(c.idl_amplitude, c.idl_length, c.idl_start, x0);
+    const T dY[5] = {(s.P - c.idl_pressure) * sigma, T(0), T(0), T(0), T(0)};
+    St<T> d;
+    state_from_y_fwd(c, s, eint, dY, d);
+    vi[0] += d.rho;
+    vi[1] += d.m[0];
+    vi[2] += d.m[1];
+    vi[3] += d.m[2];
+    vi[4] += d.E;
+  }
+#pragma unroll
+  for (int j = 0; j < 5; j++) v[j] = wdetJ * vi[j];
+#pragma unroll
+  for (int kk = 0; kk < 3; kk++)
+#pragma unroll
+    for (int j = 0; j < 5; j++) gv[kk][j] = wdetJ * (gvi[j][0] * X[kk][0] + gvi[j][1] * X[kk][1] + gvi[j][2] * X[kk][2]);
+#pragma unroll
+  for (int j = 0; j < 5; j++) jd[j] = q[j];
+#pragma unroll
+  for (int j = 0; j < 6; j++) jd[5 + j] = e[j];
+#pragma unroll
+  for (int j = 0; j < 3; j++) jd[11 + j] = tau[j];
+  jd[14] = sigma;
+}
+
+// IJacobian action at one quadrature point (jd = stored q, KM strain rate, tau [, sigma]).
+template <typename T>
+__device__ __forceinline__ void ijacobian_point(const PhysConst<T> &c, const T jd[15], const T dq[5], const T gref[3][5], T wdetJ, const T X[3][3],
+                                                T v[5], T gv[3][5]) {
+  St<T> s;
+  T inv_rho, etot, eint;
+  const T q[5] = {jd[0], jd[1], jd[2], jd[3], jd[4]};
+  state_from_u(c, q, s, inv_rho, etot, eint);
+  St<T> ds;
+  state_from_u_fwd(c, s, inv_rho, etot, eint, dq, ds);
+  St<T> gs[3];
+  physical_gradient(c, s, inv_rho, etot, eint, gref, X, gs);
+
+  T de[6], dsig[3][3], sig[3][3];
+  km_strain(gs, de);
+  stress_full(c, de, dsig);
+  const T e[6] = {jd[5], jd[6], jd[7], jd[8], jd[9], jd[10]};
+  stress_full(c, e, sig);
+
+  T gvi[5][3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    T row[5];
+    dflux_row(s, ds, j, row);
+    const T dFe = -s.u[0] * dsig[0][j] - ds.u[0] * sig[0][j] - s.u[1] * dsig[1][j] - ds.u[1] * sig[1][j] - s.u[2] * dsig[2][j] -
+                  ds.u[2] * sig[2][j] - c.k * gs[j].T_;
+    gvi[0][j] = -row[0];
+#pragma unroll
+    for (int kk = 0; kk < 3; kk++) gvi[1 + kk][j] = -(row[1 + kk] - dsig[kk][j]);
+    gvi[4][j] = -(row[4] + dFe);
+  }
+  const T dbody[5] = {T(0), ds.rho * c.g[0], ds.rho * c.g[1], ds.rho * c.g[2], ds.m[0] * c.g[0] + ds.m[1] * c.g[1] + ds.m[2] * c.g[2]};
+  T dUdot[5], vi[5];
+  const T dU[5] = {ds.rho, ds.m[0], ds.m[1], ds.m[2], ds.E};
+#pragma unroll
+  for (int j = 0; j < 5; j++) {
+    dUdot[j] = c.shift * dU[j];
+    vi[j] = dUdot[j] - dbody[j];
+  }
+  const T tau[3] = {jd[11], jd[12], jd[13]};
+  T dstab[5][3];
+  stabilization(c, s, eint, tau, gs, dUdot, dbody, dstab);
+#pragma unroll
+  for (int j = 0; j < 5; j++)
+#pragma unroll
+    for (int d = 0; d < 3; d++) gvi[j][d] += dstab[j][d];
+  if (c.idl_enable) {  // newtonian_integrands.h:58-64
+    const T sigma = jd[14];
+    const T dY[5] = {ds.P * sigma, T(0), T(0), T(0), T(0)};
+    St<T> d;
+    state_from_y_fwd(c, s, eint, dY, d);
+    vi[0] += d.rho;
+    vi[1] += d.m[0];
+    vi[2] += d.m[1];
+    vi[3] += d.m[2];
+    vi[4] += d.E;
+  }
+#pragma unroll
+  for (int j = 0; j < 5; j++) v[j] = wdetJ * vi[j];
+#pragma unroll
+  for (int kk = 0; kk < 3; kk++)
+#pragma unroll
+    for (int j = 0; j < 5; j++) gv[kk][j] = wdetJ * (gvi[j][0] * X[kk][0] + gvi[j][1] * X[kk][1] + gvi[j][2] * X[kk][2]);
+}
+
+}  // namespace hb

@@ -1,0 +1,143 @@
+"""HONEE's operator set-up for the Newtonian volume operator, written against the libCEED binding.
+
+Mirrors, call for call, what the reference does before time stepping:
+  * QDataGet (src/qdata.c:133-190): the ``Setup`` QFunction on the coordinate field -> qdata [elem][10][Q^3]
+  * SetupLibceed (src/setuplibceed.c:97-340): bases, restrictions, jac_data, the IFunction and IJacobian volume
+    operators with the field names of src/setuplibceed.c:216-266, wrapped in composite operators (:295-306)
+  * NS_NEWTONIAN_IG context registration (problems/newtonian.c:744-753): "timestep size", "ijacobian time shift",
+    "solution time" labels
+and exposes the calls the reference makes in its hot loop:
+  * IFunction_NS (src/setupts.c:78-125)      -> :meth:`NewtonianOperators.ifunction`
+  * FormIJacobian_NS (src/setupts.c:131-157) -> :meth:`NewtonianOperators.set_ijacobian_shift`
+  * MatMult_Ceed (src/mat-ceed.c:1643-1700)  -> :meth:`NewtonianOperators.ijacobian`
+  * MatGetDiagonal_Ceed (src/mat-ceed.c:1603-1634) -> :meth:`NewtonianOperators.diagonal`
+The structured box mesh stands in for DMPlex; all arithmetic happens in libceed_b200.so.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import ceed as ce
+from .problem import CONTEXT_LABELS, BoxMesh, TensorBasis, context_bytes
+
+
+def linear_coordinate_basis(Q: int, qref1d, qweight1d):
+    """P=2 Lagrange basis of the trilinear coordinate field at the solution's quadrature points."""
+    x = np.asarray(qref1d)
+    B = np.stack([0.5 * (1 - x), 0.5 * (1 + x)], axis=1)
+    G = np.tile(np.array([[-0.5, 0.5]]), (Q, 1))
+    return B, G
+
+
+class NewtonianOperators:
+    def __init__(self, ceed: ce.Ceed, mesh: BoxMesh, basis: TensorBasis, ctx, *, num_comps_jac_data=None):
+        self.ceed, self.mesh, self.basis, self.ctx = ceed, mesh, basis, ctx
+        P, Q, E = basis.P, basis.Q, mesh.num_elem
+        Q3 = Q ** 3
+        njd = num_comps_jac_data or (15 if ctx.idl_enable else 14)
+        self.num_jd = njd
+        # -- bases (src/dm-utils.c:766-879)
+        self.basis_q = ce.Basis(ceed, 3, 5, P, Q, basis.interp1d, basis.grad1d, basis.qref1d, basis.qweight1d)
+        Bx, Gx = linear_coordinate_basis(Q, basis.qref1d, basis.qweight1d)
+        self.basis_x = ce.Basis(ceed, 3, 3, 2, Q, Bx, Gx, basis.qref1d, basis.qweight1d)
+        # -- restrictions (src/dm-utils.c:83-137, :235)
+        self.rstr_q = ce.ElemRestriction(ceed, E, P ** 3, 5, 1, mesh.l_size, offsets=mesh.offsets)
+        off_x = (np.arange(E * 8, dtype=np.int64) * 3).astype(np.int32)  # element-local (periodic-safe) coordinates
+        self.rstr_x = ce.ElemRestriction(ceed, E, 8, 3, 1, E * 24, offsets=off_x)
+        self.rstr_qd = ce.ElemRestriction(ceed, E, Q3, 10, 0, E * Q3 * 10)
+        self.rstr_jd = ce.ElemRestriction(ceed, E, Q3, njd, 0, E * Q3 * njd)
+        # -- coordinates as an interleaved L-vector [elem][vertex][3]
+        x_elem = mesh.x_elem.reshape(E, 3, 8)
+        self.x_coord = ce.Vector(ceed, E * 24)
+        self.x_coord.set_array_host(np.ascontiguousarray(x_elem.transpose(0, 2, 1)).reshape(-1))
+        # -- qdata (QDataGet, src/qdata.c:153-178)
+        self.q_data = ce.Vector(ceed, E * Q3 * 10)
+        qf_setup = ce.QFunction(ceed, "setupgeo.h:Setup")
+        qf_setup.add_input("dx", 9, ce.CEED_EVAL_GRAD)
+        qf_setup.add_input("weight", 1, ce.CEED_EVAL_WEIGHT)
+        qf_setup.add_output("surface qdata", 10, ce.CEED_EVAL_NONE)
+        op_setup = ce.Operator(ceed, qf_setup)
+        op_setup.set_field("dx", self.rstr_x, self.basis_x, ceed.active)
+        op_setup.set_field("weight", ceed.rstr_none, self.basis_x, ceed.vector_none)
+        op_setup.set_field("surface qdata", self.rstr_qd, ceed.basis_none, ceed.active)
+        op_setup.apply(self.x_coord, self.q_data)
+        self.op_setup = op_setup
+        # -- context (problems/newtonian.c:744-753)
+        self.qfctx = ce.QFunctionContext(ceed, ctx)
+        for name, off in CONTEXT_LABELS.items():
+            self.qfctx.register_double(name, off, 1)
+        # -- vectors (src/setuplibceed.c:125-131)
+        self.jac_data = ce.Vector(ceed, E * Q3 * njd)
+        self.q_dot = ce.Vector(ceed, mesh.l_size)
+        # -- IFunction volume operator (src/setuplibceed.c:209-243)
+        qf_if = ce.QFunction(ceed, "newtonian.h:IFunction_Newtonian_Conserv")
+        for name, size, mode in (("q", 5, ce.CEED_EVAL_INTERP), ("Grad_q", 15, ce.CEED_EVAL_GRAD), ("q dot", 5, ce.CEED_EVAL_INTERP),
+                                 ("qdata", 10, ce.CEED_EVAL_NONE), ("x", 3, ce.CEED_EVAL_INTERP)):
+            qf_if.add_input(name, size, mode)
+        qf_if.add_output("v", 5, ce.CEED_EVAL_INTERP)
+        qf_if.add_output("Grad_v", 15, ce.CEED_EVAL_GRAD)
+        qf_if.add_output("jac_data", njd, ce.CEED_EVAL_NONE)
+        qf_if.set_context(self.qfctx)
+        op_if = ce.Operator(ceed, qf_if)
+        op_if.set_name("IFunction Domain Operator")
+        op_if.set_field("q", self.rstr_q, self.basis_q, ceed.active)
+        op_if.set_field("Grad_q", self.rstr_q, self.basis_q, ceed.active)
+        op_if.set_field("q dot", self.rstr_q, self.basis_q, self.q_dot)
+        op_if.set_field("qdata", self.rstr_qd, ceed.basis_none, self.q_data)
+        op_if.set_field("x", self.rstr_x, self.basis_x, self.x_coord)
+        op_if.set_field("v", self.rstr_q, self.basis_q, ceed.active)
+        op_if.set_field("Grad_v", self.rstr_q, self.basis_q, ceed.active)
+        op_if.set_field("jac_data", self.rstr_jd, ceed.basis_none, self.jac_data)
+        # -- IJacobian volume operator (src/setuplibceed.c:245-269)
+        qf_ij = ce.QFunction(ceed, "newtonian.h:IJacobian_Newtonian_Conserv")
+        for name, size, mode in (("dq", 5, ce.CEED_EVAL_INTERP), ("Grad_dq", 15, ce.CEED_EVAL_GRAD), ("qdata", 10, ce.CEED_EVAL_NONE),
+                                 ("jac_data", njd, ce.CEED_EVAL_NONE)):
+            qf_ij.add_input(name, size, mode)
+        qf_ij.add_output("v", 5, ce.CEED_EVAL_INTERP)
+        qf_ij.add_output("Grad_v", 15, ce.CEED_EVAL_GRAD)
+        qf_ij.set_context(self.qfctx)
+        op_ij = ce.Operator(ceed, qf_ij)
+        op_ij.set_name("IJacobian Domain Operator")
+        op_ij.set_field("dq", self.rstr_q, self.basis_q, ceed.active)
+        op_ij.set_field("Grad_dq", self.rstr_q, self.basis_q, ceed.active)
+        op_ij.set_field("qdata", self.rstr_qd, ceed.basis_none, self.q_data)
+        op_ij.set_field("jac_data", self.rstr_jd, ceed.basis_none, self.jac_data)
+        op_ij.set_field("v", self.rstr_q, self.basis_q, ceed.active)
+        op_ij.set_field("Grad_v", self.rstr_q, self.basis_q, ceed.active)
+        # -- composites (src/setuplibceed.c:295-306)
+        self.op_ifunction = ce.Operator(ceed)
+        self.op_ifunction.set_name("IFunction Composite Operator")
+        self.op_ifunction.add_sub(op_if)
+        self.op_ijacobian = ce.Operator(ceed)
+        self.op_ijacobian.set_name("IJacobian Composite Operator")
+        self.op_ijacobian.add_sub(op_ij)
+        self._vol = (op_if, op_ij, qf_if, qf_ij, qf_setup)
+
+    # ---- context updates (src/setupts.c:91-93, :141)
+    def set_time(self, t):
+        self.op_ifunction.set_context_double("solution time", [t])
+
+    def set_timestep(self, dt):
+        self.op_ifunction.set_context_double("timestep size", [dt])
+
+    def set_ijacobian_shift(self, shift):
+        self.op_ijacobian.set_context_double("ijacobian time shift", [shift])
+
+    # ---- hot-path calls
+    def ifunction(self, q: ce.Vector, q_dot: ce.Vector, g: ce.Vector):
+        """G = F(q, q_dot): HONEE points its q_dot CeedVector at the PETSc array, then applies (src/setupts.c:102-109)."""
+        q_dot.copy_to(self.q_dot) if q_dot is not self.q_dot else None
+        self.op_ifunction.apply(q, g)
+
+    def ijacobian(self, dq: ce.Vector, out: ce.Vector, add=False):
+        self.op_ijacobian.apply(dq, out, add=add)
+
+    def diagonal(self, out: ce.Vector):
+        self.op_ijacobian.assemble_diagonal(out)
+
+    def host_inputs(self):
+        """qdata as a numpy array (for checks against the oracle)."""
+        return self.q_data.to_numpy()
+
+    def context_bytes(self):
+        return context_bytes(self.ctx)

@@ -1,0 +1,106 @@
+"""ctypes binding of the kernel-level C ABI (include/honee_b200.h) on device pointers.
+
+Used by callers that manage device memory themselves -- the Newton-Krylov driver, the benchmark and the parity tests --
+with torch tensors serving only as device buffers and streams.  Every call is asynchronous on the stream it is given.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import lib as _load
+
+HB_MAX_P = 8
+
+
+class HbElemOp(C.Structure):
+    _fields_ = [("num_elem", C.c_int), ("P", C.c_int), ("Q", C.c_int), ("l_size", C.c_int64), ("d_offsets", C.c_void_p),
+                ("num_colors", C.c_int), ("h_color_ptr", C.POINTER(C.c_int32)), ("d_color_elem", C.c_void_p),
+                ("interp1d", C.c_double * 64), ("grad1d", C.c_double * 64), ("colo_grad1d", C.c_double * 64),
+                ("qref1d", C.c_double * 8), ("qweight1d", C.c_double * 8), ("d_x_elem", C.c_void_p), ("num_sms", C.c_int),
+                ("device", C.c_int)]
+
+
+class HbIFunctionIO(C.Structure):
+    _fields_ = [("q", C.c_void_p), ("q_dot", C.c_void_p), ("qdata", C.c_void_p), ("jac_data", C.c_void_p), ("jac_data_f32", C.c_void_p),
+                ("v", C.c_void_p), ("add", C.c_int)]
+
+
+def _dp(a: np.ndarray):
+    return np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _addr(t):
+    if t is None:
+        return None
+    return C.c_void_p(t.data_ptr() if hasattr(t, "data_ptr") else int(t))
+
+
+def _stream(s):
+    if s is None:
+        return None
+    return C.c_void_p(s.cuda_stream if hasattr(s, "cuda_stream") else int(s))
+
+
+class HbError(RuntimeError):
+    pass
+
+
+def _chk(code, what):
+    if code != 0:
+        raise HbError(f"{what} failed with status {code}")
+
+
+class ElemOp:
+    """Device description of the hex element operator (restriction + colouring + tensor basis)."""
+
+    def __init__(self, mesh, basis):
+        L = _load()
+        self.ptr = C.POINTER(HbElemOp)()
+        off = np.ascontiguousarray(mesh.offsets, dtype=np.int32)
+        _chk(L.hb_elemop_create(mesh.num_elem, basis.P, basis.Q, off.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int64(mesh.l_size),
+                                _dp(basis.interp1d), _dp(basis.grad1d), _dp(basis.qref1d), _dp(basis.qweight1d), C.byref(self.ptr)),
+             "hb_elemop_create")
+        self.num_elem, self.P, self.Q, self.l_size = mesh.num_elem, basis.P, basis.Q, mesh.l_size
+        self.qref1d = np.ascontiguousarray(basis.qref1d)
+        self.qweight1d = np.ascontiguousarray(basis.qweight1d)
+
+    @property
+    def num_colors(self):
+        return self.ptr.contents.num_colors
+
+    def color_sizes(self):
+        c = self.ptr.contents
+        return [c.h_color_ptr[i + 1] - c.h_color_ptr[i] for i in range(c.num_colors)]
+
+    def set_vertex_coords(self, x_elem):
+        _chk(_load().hb_elemop_set_vertex_coords(self.ptr, _dp(x_elem)), "hb_elemop_set_vertex_coords")
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                _load().hb_elemop_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    # ---- operators
+    def setup_qdata(self, x_elem_dev, qdata_dev, stream=None):
+        _chk(_load().hb_setup_qdata(self.num_elem, self.Q, _dp(self.qref1d), _dp(self.qweight1d), _addr(x_elem_dev), _addr(qdata_dev),
+                                    _stream(stream)), "hb_setup_qdata")
+
+    def ifunction(self, ctx_bytes: bytes, q, q_dot, qdata, v, jac_data=None, jac_data_f32=None, add=False, stream=None):
+        io = HbIFunctionIO(_addr(q), _addr(q_dot), _addr(qdata), _addr(jac_data), _addr(jac_data_f32), _addr(v), int(add))
+        cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        _chk(_load().hb_ifunction_apply(self.ptr, cb, C.byref(io), _stream(stream)), "hb_ifunction_apply")
+
+    def ijacobian(self, ctx_bytes: bytes, qdata, jac_data, dq, v, add=False, fp32=False, stream=None):
+        cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        fn = _load().hb_ijacobian_apply_f32 if fp32 else _load().hb_ijacobian_apply_f64
+        _chk(fn(self.ptr, cb, _addr(qdata), _addr(jac_data), _addr(dq), _addr(v), int(add), _stream(stream)), "hb_ijacobian_apply")
+
+    def diagonal(self, ctx_bytes: bytes, qdata, jac_data, diag, add=False, fp32=False, stream=None):
+        cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        fn = _load().hb_diagonal_assemble_f32 if fp32 else _load().hb_diagonal_assemble_f64
+        _chk(fn(self.ptr, cb, _addr(qdata), _addr(jac_data), _addr(diag), int(add), _stream(stream)), "hb_diagonal_assemble")

@@ -1,0 +1,315 @@
+"""Caller-side problem set-up: what HONEE's L2/L4 layers hand to the operator backend.
+
+HONEE builds its QFunction context in ``NS_NEWTONIAN_IG`` (problems/newtonian.c:573-760), its mesh with PETSc DMPlex and
+its tensor basis with PetscFE (src/dm-utils.c:387-879).  PETSc is not part of this project, so this module supplies the
+same inputs for structured hex boxes: the 184-byte ``NewtonianIdealGasContext_`` with the reference defaults, int32
+restriction offsets into a node-interleaved L-vector, the element coordinate field, and the 1D Lagrange tabulation on
+Gauss-Lobatto nodes with Gauss-Legendre quadrature.  The operator backend itself never depends on this module: it takes
+whatever offsets, bases and contexts a caller passes through the libCEED API.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# --------------------------------------------------------------------------------------------------------------------
+# QFunction context structs (byte-identical to qfunctions/newtonian_types.h:20-75)
+
+STATEVAR_CONSERVATIVE, STATEVAR_PRIMITIVE, STATEVAR_ENTROPY = 0, 1, 2
+STAB_NONE, STAB_SU, STAB_SUPG = 0, 1, 2
+
+
+class GasProperties(C.Structure):
+    _fields_ = [("lambda_", C.c_double), ("mu", C.c_double), ("k", C.c_double), ("cv", C.c_double), ("cp", C.c_double)]
+
+
+class TauCoefficients(C.Structure):
+    _fields_ = [("Ctau_t", C.c_double), ("Ctau_v", C.c_double), ("Ctau_C", C.c_double), ("Ctau_M", C.c_double), ("Ctau_E", C.c_double)]
+
+
+class NewtonianContext(C.Structure):
+    """struct NewtonianIdealGasContext_ (qfunctions/newtonian_types.h:28-47)."""
+    _fields_ = [("gas", GasProperties), ("g", C.c_double * 3), ("time", C.c_double), ("ijacobian_time_shift", C.c_double),
+                ("is_implicit", C.c_bool), ("state_var", C.c_int), ("stabilization", C.c_int), ("idl_enable", C.c_bool),
+                ("idl_pressure", C.c_double), ("idl_amplitude", C.c_double), ("idl_start", C.c_double), ("idl_length", C.c_double),
+                ("tau_coeffs", TauCoefficients), ("dt", C.c_double), ("divFdiff_method", C.c_int)]
+
+
+class StatePrimitive(C.Structure):
+    _fields_ = [("pressure", C.c_double), ("velocity", C.c_double * 3), ("temperature", C.c_double)]
+
+
+class TaylorGreenContext(C.Structure):
+    """struct TaylorGreenContext_ (qfunctions/taylorgreen.h:12-20)."""
+    _fields_ = [("reference", StatePrimitive), ("newt_ctx", NewtonianContext), ("lx", C.c_double), ("ly", C.c_double),
+                ("lz", C.c_double), ("u", C.c_double * 3)]
+
+
+assert C.sizeof(NewtonianContext) == 184
+assert NewtonianContext.time.offset == 64 and NewtonianContext.ijacobian_time_shift.offset == 72 and NewtonianContext.dt.offset == 168
+
+# Field offsets HONEE registers with CeedQFunctionContextRegisterDouble (problems/newtonian.c:747-753)
+CONTEXT_LABELS = {"timestep size": NewtonianContext.dt.offset,
+                  "ijacobian time shift": NewtonianContext.ijacobian_time_shift.offset,
+                  "solution time": NewtonianContext.time.offset}
+
+
+def newtonian_context(degree: int, *, cv=717., cp=1004., lambda_=-2. / 3., mu=1.8e-5, k=0.02638, g=(0., 0., 0.), stab=STAB_NONE,
+                      state_var=STATEVAR_CONSERVATIVE, implicit=True, dt=1.0, ijacobian_time_shift=0.0, time=0.0,
+                      Ctau_t=1.0, Ctau_v=None, Ctau_C=None, Ctau_M=None, Ctau_E=0.125, idl=None) -> NewtonianContext:
+    """Context with the defaults of problems/newtonian.c:588-613, overridable like the -cv/-cp/-mu/-k/-stab/-Ctau_* options."""
+    cv_func = (36, 60, 128)
+    ctx = NewtonianContext()
+    ctx.gas = GasProperties(lambda_, mu, k, cv, cp)
+    ctx.g[:] = list(g)
+    ctx.time = time
+    ctx.ijacobian_time_shift = ijacobian_time_shift
+    ctx.is_implicit = bool(implicit)
+    ctx.state_var = state_var
+    ctx.stabilization = stab
+    ctx.tau_coeffs = TauCoefficients(Ctau_t, cv_func[min(3, degree) - 1] if Ctau_v is None else Ctau_v,
+                                     0.25 / degree if Ctau_C is None else Ctau_C, 0.25 / degree if Ctau_M is None else Ctau_M, Ctau_E)
+    ctx.dt = dt
+    ctx.divFdiff_method = 0
+    if idl is not None:  # (decay_time, start, length, pressure), problems/newtonian.c:656-677, 722
+        decay, start, length, pressure = idl
+        ctx.idl_enable = True
+        ctx.idl_amplitude = 1.0 / decay
+        ctx.idl_start, ctx.idl_length, ctx.idl_pressure = start, length, pressure
+    return ctx
+
+
+def context_bytes(ctx) -> bytes:
+    return bytes(memoryview(ctx))
+
+
+# --------------------------------------------------------------------------------------------------------------------
+# ideal-gas state conversion used by initial conditions (qfunctions/newtonian_state.h:159-168)
+
+def conservative_from_primitive(gas: GasProperties, P, u, T):
+    R = gas.cp - gas.cv
+    rho = P / (R * T)
+    u = np.asarray(u)
+    E = rho * (gas.cv * T + 0.5 * np.sum(u * u, axis=0))
+    return np.stack([rho, rho * u[0], rho * u[1], rho * u[2], E])
+
+
+# --------------------------------------------------------------------------------------------------------------------
+# 1D tabulation
+
+def _legendre(n, x):
+    p0, p1 = np.ones_like(x), x.copy()
+    if n == 0:
+        return p0, np.zeros_like(x)
+    for kk in range(2, n + 1):
+        p0, p1 = p1, ((2 * kk - 1) * x * p1 - (kk - 1) * p0) / kk
+    dp = n * (x * p1 - p0) / (x * x - 1)
+    return p1, dp
+
+
+def gauss_legendre(Q: int):
+    x = -np.cos(np.pi * (np.arange(Q) + 0.75) / (Q + 0.5))
+    for _ in range(100):
+        p, dp = _legendre(Q, x)
+        dx = p / dp
+        x = x - dx
+        if np.max(np.abs(dx)) < 1e-16:
+            break
+    p, dp = _legendre(Q, x)
+    return x, 2.0 / ((1 - x * x) * dp * dp)
+
+
+def gauss_lobatto(P: int):
+    N = P - 1
+    x = -np.cos(np.pi * np.arange(P) / N)
+    inner = x[1:-1].copy()
+    for _ in range(100):
+        p, dp = _legendre(N, inner)
+        ddp = (2 * inner * dp - N * (N + 1) * p) / (1 - inner * inner)
+        dx = dp / ddp
+        inner = inner - dx
+        if inner.size == 0 or np.max(np.abs(dx)) < 1e-16:
+            break
+    x[1:-1] = inner
+    x[0], x[-1] = -1.0, 1.0
+    return x
+
+
+def lagrange_tabulate(nodes, pts):
+    P, Q = len(nodes), len(pts)
+    B = np.zeros((Q, P))
+    G = np.zeros((Q, P))
+    for q in range(Q):
+        for j in range(P):
+            l, dl = 1.0, 0.0
+            for m in range(P):
+                if m == j:
+                    continue
+                f = (pts[q] - nodes[m]) / (nodes[j] - nodes[m])
+                dl = dl * f + l / (nodes[j] - nodes[m])
+                l *= f
+            B[q, j], G[q, j] = l, dl
+    return B, G
+
+
+@dataclass
+class TensorBasis:
+    """Arguments of CeedBasisCreateTensorH1 (src/dm-utils.c:766-879): 1D interp/grad [Q][P], q_ref, q_weight."""
+    P: int
+    Q: int
+    interp1d: np.ndarray
+    grad1d: np.ndarray
+    qref1d: np.ndarray
+    qweight1d: np.ndarray
+    nodes1d: np.ndarray
+
+
+def tensor_basis(P: int, Q: int) -> TensorBasis:
+    nodes = gauss_lobatto(P)
+    qx, qw = gauss_legendre(Q)
+    B, G = lagrange_tabulate(nodes, qx)
+    return TensorBasis(P, Q, B, G, qx, qw, nodes)
+
+
+# --------------------------------------------------------------------------------------------------------------------
+# structured hex box
+
+@dataclass
+class BoxMesh:
+    n: tuple
+    P: int
+    periodic: tuple
+    xs: np.ndarray
+    ys: np.ndarray
+    zs: np.ndarray
+    num_elem: int = 0
+    num_nodes: int = 0
+    offsets: np.ndarray = field(default=None, repr=False)   # int32 [E][P^3], node*5
+    x_elem: np.ndarray = field(default=None, repr=False)    # [E][3][8] vertex coordinates (E-vector of the P=2 field)
+    colors: tuple = field(default=None, repr=False)         # (color_ptr, color_elem) CSR
+    node_dims: tuple = ()
+
+    @property
+    def l_size(self):
+        return 5 * self.num_nodes
+
+
+def _nodes_dim(n, P, periodic):
+    return n * (P - 1) + (0 if periodic else 1)
+
+
+def box_mesh(n, P, periodic=(False, False, False), lo=(0., 0., 0.), hi=(1., 1., 1.), planes=None, ncomp=5) -> BoxMesh:
+    """Lexicographic hex box with node-interleaved L-vector; `planes` optionally gives the vertex planes per direction."""
+    n = tuple(int(v) for v in n)
+    periodic = tuple(bool(p) for p in periodic)
+    if planes is None:
+        planes = [np.linspace(lo[d], hi[d], n[d] + 1) for d in range(3)]
+    N = tuple(_nodes_dim(n[d], P, periodic[d]) for d in range(3))
+    ex, ey, ez = np.meshgrid(np.arange(n[0]), np.arange(n[1]), np.arange(n[2]), indexing="ij")
+    ex, ey, ez = (a.transpose(2, 1, 0).reshape(-1) for a in (ex, ey, ez))  # x fastest
+    a = np.arange(P)
+    A, Bb, Cc = np.meshgrid(a, a, a, indexing="ij")
+    A, Bb, Cc = (t.transpose(2, 1, 0).reshape(-1) for t in (A, Bb, Cc))     # local node a fastest
+    i = (ex[:, None] * (P - 1) + A[None, :]) % N[0]
+    j = (ey[:, None] * (P - 1) + Bb[None, :]) % N[1]
+    k = (ez[:, None] * (P - 1) + Cc[None, :]) % N[2]
+    node = i.astype(np.int64) + N[0] * (j.astype(np.int64) + N[1] * k.astype(np.int64))
+    num_nodes = N[0] * N[1] * N[2]
+    assert num_nodes * ncomp < 2 ** 31, "int32 offsets overflow"
+    offsets = (node * ncomp).astype(np.int32).reshape(-1)
+    E = n[0] * n[1] * n[2]
+    x_elem = np.zeros((E, 3, 8))
+    for v in range(8):
+        va, vb, vc = v & 1, (v >> 1) & 1, (v >> 2) & 1
+        x_elem[:, 0, v] = planes[0][ex + va]
+        x_elem[:, 1, v] = planes[1][ey + vb]
+        x_elem[:, 2, v] = planes[2][ez + vc]
+    m = BoxMesh(n, P, periodic, np.asarray(planes[0]), np.asarray(planes[1]), np.asarray(planes[2]), E, num_nodes, offsets,
+                x_elem.reshape(-1), None, N)
+    m.colors = parity_colors(n)
+    return m
+
+
+def parity_colors(n):
+    """2x2x2 parity colouring of a lexicographic box: elements of one colour share no node (needs even counts when periodic)."""
+    ex, ey, ez = np.meshgrid(np.arange(n[0]), np.arange(n[1]), np.arange(n[2]), indexing="ij")
+    ex, ey, ez = (a.transpose(2, 1, 0).reshape(-1) for a in (ex, ey, ez))
+    color = (ex % 2) + 2 * (ey % 2) + 4 * (ez % 2)
+    order = np.argsort(color, kind="stable").astype(np.int32)
+    counts = np.bincount(color, minlength=8)
+    ptr_ = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    return ptr_, order
+
+
+def node_coordinates(mesh: BoxMesh, basis: TensorBasis):
+    """Physical coordinates [3][num_nodes] of the Lagrange nodes (for nodal initial conditions)."""
+    coords = []
+    for d, planes in enumerate((mesh.xs, mesh.ys, mesh.zs)):
+        nd = mesh.n[d]
+        Nd = mesh.node_dims[d]
+        x = np.zeros(Nd)
+        for e in range(nd):
+            h0, h1 = planes[e], planes[e + 1]
+            loc = h0 + (basis.nodes1d + 1) * 0.5 * (h1 - h0)
+            for a in range(mesh.P):
+                idx = e * (mesh.P - 1) + a
+                if idx < Nd:
+                    x[idx] = loc[a]
+        coords.append(x)
+    X, Y, Z = np.meshgrid(coords[0], coords[1], coords[2], indexing="ij")
+    return np.stack([t.transpose(2, 1, 0).reshape(-1) for t in (X, Y, Z)])
+
+
+# --------------------------------------------------------------------------------------------------------------------
+# workloads (synthetic stand-ins with the shapes and value distributions of the benchmark configurations)
+
+def gaussian_pulse_state(mesh: BoxMesh, basis: TensorBasis, gas: GasProperties, *, P0=101325., T0=288., u0=(10., 0., 0.), amp=0.01,
+                         sigma=0.1, center=(0.5, 0.5, 0.5), noise=1e-4, seed=0):
+    """3D Gaussian pressure pulse on a uniform background plus seeded uniform relative noise on all conservative fields."""
+    X = node_coordinates(mesh, basis)
+    r2 = sum((X[d] - center[d]) ** 2 for d in range(3))
+    P = P0 * (1 + amp * np.exp(-r2 / (2 * sigma ** 2)))
+    u = np.array(u0)[:, None] * np.ones_like(P)[None, :]
+    q = conservative_from_primitive(gas, P, u, T0 * np.ones_like(P))
+    rng = np.random.default_rng(seed)
+    q = q * (1 + noise * rng.uniform(-1, 1, size=q.shape))
+    return np.ascontiguousarray(q.T.reshape(-1))
+
+
+def multimode_state(mesh: BoxMesh, basis: TensorBasis, gas: GasProperties, *, P0=101325., T0=288., u0=(10., 0., 0.), modes=8,
+                    amp=1e-3, kmax=8, seed=0):
+    """Background state plus `modes` seeded sinusoidal perturbations (|k| <= kmax * 2pi) with relative amplitude `amp`."""
+    X = node_coordinates(mesh, basis)
+    rng = np.random.default_rng(seed)
+    q0 = conservative_from_primitive(gas, P0 * np.ones(X.shape[1]), np.array(u0)[:, None] * np.ones((1, X.shape[1])),
+                                     T0 * np.ones(X.shape[1]))
+    pert = np.zeros_like(q0)
+    for _ in range(modes):
+        kvec = rng.uniform(-1, 1, 3)
+        kvec *= rng.uniform(0, kmax) / max(np.linalg.norm(kvec), 1e-12)
+        phase = rng.uniform(0, 2 * np.pi, 5)
+        arg = 2 * np.pi * (kvec[0] * X[0] + kvec[1] * X[1] + kvec[2] * X[2])
+        pert += np.sin(arg[None, :] + phase[:, None])
+    q = q0 * (1 + amp * pert)
+    return np.ascontiguousarray(q.T.reshape(-1))
+
+
+def taylor_green_context(degree: int, *, L=2 * math.pi, Re=1600., Ma=0.1, rho0=1.0, V0=1.0, stab=STAB_SUPG):
+    """Taylor-Green vortex parameters in the form of examples/taylor_green_vortex.yaml (Re=1600, Ma=0.1)."""
+    cv, cp = 717., 1003.8
+    gamma = cp / cv
+    R = cp - cv
+    c = V0 / Ma
+    T0 = c * c / (gamma * R)
+    P0 = rho0 * R * T0
+    mu = rho0 * V0 * (L / (2 * math.pi)) / Re
+    Pr = 0.71
+    k = cp * mu / Pr
+    ctx = TaylorGreenContext()
+    ctx.reference = StatePrimitive(P0, (C.c_double * 3)(V0, 0., 0.), T0)
+    ctx.newt_ctx = newtonian_context(degree, cv=cv, cp=cp, mu=mu, k=k, stab=stab, Ctau_v=60, Ctau_C=0.5, Ctau_M=0.5, Ctau_E=0.5)
+    ctx.lx = ctx.ly = ctx.lz = L
+    return ctx

@@ -1,0 +1,137 @@
+/* honee_b200.h -- kernel-level C ABI of the B200 Newtonian operator backend.
+ *
+ * Plain pointers and sizes, no CUDA or torch types: device pointers are `double *` / `float *` allocated by the caller
+ * (or by the libCEED-compatible layer in ceed_b200.c), streams are passed as `void *` (a cudaStream_t, NULL = legacy
+ * default stream).  Every call is asynchronous on that stream.
+ *
+ * This is the layer the libCEED API of include/ceed/ceed.h dispatches to once it has recognised the HONEE operators;
+ * it is also exported so a caller that manages its own device memory (a solver, a test, the benchmark) can drive the
+ * fused kernels directly.  Each entry names the reference call it serves.
+ */
+#ifndef HONEE_B200_H
+#define HONEE_B200_H
+
+#include <stdint.h>
+
+#include "honee_b200_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HB_EXPORT __attribute__((visibility("default")))
+
+/* Status codes (0 = success; the values match libCEED's CEED_ERROR_* where they overlap). */
+enum {
+  HB_SUCCESS           = 0,
+  HB_ERROR_MINOR       = 1,
+  HB_ERROR_DIMENSION   = 2,
+  HB_ERROR_INCOMPLETE  = 3,
+  HB_ERROR_INCOMPATIBLE = 4,
+  HB_ERROR_ACCESS      = 5,
+  HB_ERROR_MAJOR       = -1,
+  HB_ERROR_BACKEND     = -2,
+  HB_ERROR_UNSUPPORTED = -3,
+  HB_ERROR_INVALID     = -4,
+  HB_ERROR_CUDA        = -5,
+  HB_ERROR_NOMEM       = -6,
+};
+
+#define HB_MAX_P 8
+
+/* Device-resident description of one H1 element operator on a hex mesh: restriction offsets (int32, one per element
+ * node, pointing at component 0 of a node-interleaved 5-component L-vector, comp_stride 1), an element colouring in
+ * which no two elements of one colour share an L-vector entry, and the 1D tensor basis.
+ * Replaces what libCEED builds from CeedElemRestrictionCreate (src/dm-utils.c:83-137) and CeedBasisCreateTensorH1
+ * (src/dm-utils.c:766-879). */
+typedef struct HbElemOp {
+  int            num_elem, P, Q;
+  int64_t        l_size;        /* entries of the L-vector (5 * nodes) */
+  int32_t       *d_offsets;     /* device [num_elem][P^3] */
+  int            num_colors;
+  int32_t       *h_color_ptr;   /* host CSR pointer [num_colors + 1] */
+  int32_t       *d_color_elem;  /* device element ids grouped by colour */
+  double         interp1d[HB_MAX_P * HB_MAX_P];   /* [Q][P] */
+  double         grad1d[HB_MAX_P * HB_MAX_P];     /* [Q][P] */
+  double         colo_grad1d[HB_MAX_P * HB_MAX_P];/* [Q][Q] derivative on the quadrature points: grad1d = colo * interp1d */
+  double         qref1d[HB_MAX_P], qweight1d[HB_MAX_P];
+  double        *d_x_elem;      /* device [num_elem][3][8] vertex coordinates (only needed with the IDL), may be NULL */
+  int            num_sms;
+  int            device;
+} HbElemOp;
+
+/* Build the device description from host arrays.  Validates every offset against l_size (bounds are checked on the
+ * host once, so the kernels need no per-access checks), colours the elements greedily and uploads. */
+HB_EXPORT int hb_elemop_create(int num_elem, int P, int Q, const int32_t *offsets, int64_t l_size, const double *interp1d, const double *grad1d,
+                     const double *qref1d, const double *qweight1d, HbElemOp **op);
+/* Attach trilinear vertex coordinates [num_elem][3][8] (host pointer) used by the internal damping layer. */
+HB_EXPORT int hb_elemop_set_vertex_coords(HbElemOp *op, const double *x_elem);
+HB_EXPORT int hb_elemop_destroy(HbElemOp *op);
+
+/* Inputs/outputs of one IFunction apply (device pointers). */
+typedef struct {
+  const double *q, *q_dot; /* L-vectors */
+  const double *qdata;     /* [num_elem][10][Q^3] */
+  double       *jac_data;  /* [num_elem][14 or 15][Q^3] FP64 stored values, may be NULL */
+  float        *jac_data_f32; /* same layout in FP32 for the mixed-precision Jacobian, may be NULL */
+  double       *v;         /* L-vector output */
+  int           add;       /* 0: v = F(q), 1: v += F(q) */
+} HbIFunctionIO;
+
+/* Fused IFunction_Newtonian_Conserv operator (qfunctions/newtonian.h:205-261 inside the volume operator of
+ * src/setuplibceed.c:209-243), called where HONEE calls CeedOperatorApply(op_ifunction) (src/setupts.c:109). */
+HB_EXPORT int hb_ifunction_apply(const HbElemOp *op, const void *ctx184, const HbIFunctionIO *io, void *stream);
+
+/* Fused IJacobian_Newtonian_Conserv action (qfunctions/newtonian.h:272-315, operator src/setuplibceed.c:245-269),
+ * called where MatMult_Ceed calls CeedOperatorApplyAdd (src/mat-ceed.c:1669).  FP64 and FP32 variants; the FP32 one
+ * reads the FP32 shadow of jac_data and FP32 L-vectors, qdata stays FP64 and is rounded on load. */
+HB_EXPORT int hb_ijacobian_apply_f64(const HbElemOp *op, const void *ctx184, const double *qdata, const double *jac_data, const double *dq, double *v,
+                           int add, void *stream);
+HB_EXPORT int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, const float *dq, float *v,
+                           int add, void *stream);
+
+/* Point-wise diagonal of the IJacobian operator, where MatGetDiagonal_Ceed calls CeedOperatorLinearAssembleDiagonal
+ * (src/mat-ceed.c:1603-1630). */
+HB_EXPORT int hb_diagonal_assemble_f64(const HbElemOp *op, const void *ctx184, const double *qdata, const double *jac_data, double *diag, int add,
+                             void *stream);
+HB_EXPORT int hb_diagonal_assemble_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, float *diag, int add,
+                             void *stream);
+
+/* Geometric factors of the Setup QFunction (qfunctions/setupgeo.h:42-56; driven by QDataGet, src/qdata.c:133-190) from
+ * trilinear vertex coordinates x_elem [num_elem][3][8] (device) with the Gauss rule qref1d/qweight1d (host). */
+HB_EXPORT int hb_setup_qdata(int num_elem, int Q, const double *qref1d, const double *qweight1d, const double *x_elem, double *qdata, void *stream);
+
+/* Device vector helpers used by the libCEED layer and the Newton-Krylov driver (asynchronous on `s`, except the
+ * reductions, which synchronise `s` and return the value on the host; `scratch` is a device buffer of >= 1024 doubles;
+ * reduce type 0: sum|x|, 1: sum x^2, 2: max|x|, 3: dot(x, y)). */
+HB_EXPORT int hb_vec_set_f64(double *x, int64_t n, double v, void *s);
+HB_EXPORT int hb_vec_set_f32(float *x, int64_t n, float v, void *s);
+HB_EXPORT int hb_vec_scale_f64(double *x, int64_t n, double a, void *s);
+HB_EXPORT int hb_vec_scale_f32(float *x, int64_t n, float a, void *s);
+HB_EXPORT int hb_vec_axpy_f64(double *y, double a, const double *x, int64_t n, void *s);
+HB_EXPORT int hb_vec_axpy_f32(float *y, float a, const float *x, int64_t n, void *s);
+HB_EXPORT int hb_vec_axpby_f64(double *y, double a, double b, const double *x, int64_t n, void *s);
+HB_EXPORT int hb_vec_axpby_f32(float *y, float a, float b, const float *x, int64_t n, void *s);
+HB_EXPORT int hb_vec_pointwise_mult_f64(double *w, const double *x, const double *y, int64_t n, void *s);
+HB_EXPORT int hb_vec_pointwise_mult_f32(float *w, const float *x, const float *y, int64_t n, void *s);
+HB_EXPORT int hb_vec_reciprocal_f64(double *x, int64_t n, void *s);
+HB_EXPORT int hb_vec_f64_to_f32(const double *x, float *y, int64_t n, int add, void *s);
+HB_EXPORT int hb_vec_f32_to_f64(const float *x, double *y, int64_t n, int add, void *s);
+/* type 0: sum|x|, 1: sum x^2, 2: max|x|, 3: dot(x, y); scratch: device buffer of >= 1024 doubles; synchronises s */
+HB_EXPORT int hb_vec_reduce_f64(const double *x, const double *y, int64_t n, int type, double *scratch, double *result, void *s);
+HB_EXPORT int hb_vec_reduce_f32(const float *x, const float *y, int64_t n, int type, double *scratch, double *result, void *s);
+
+HB_EXPORT int hb_restrict_apply(int num_elem, int esize, int ncomp, int cstride, const int32_t *d_off, const int32_t *d_strides, const double *l, double *e,
+                      void *s);
+HB_EXPORT int hb_restrict_apply_t_csr(int64_t l_size, const int64_t *d_ptr, const int64_t *d_eidx, const double *e, double *l, void *s);
+HB_EXPORT int hb_restrict_apply_t_strided(int num_elem, int esize, int ncomp, const int32_t *d_strides, const double *e, double *l, void *s);
+HB_EXPORT int hb_basis_apply_generic(int num_elem, int ncomp, int dim, int P, int Q, int tmode, int emode, const double *d_B, const double *d_G,
+                           const double *d_w, const double *u, double *v, void *s);
+
+/* Library identification */
+const char *hb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,142 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself (run in a container that has the reference).
+
+  python tests/golden/make_golden.py [--ref /root/reference]
+
+Outputs (committed; the GPU box has no reference tree):
+  pointwise_newtonian.npz   seeded quadrature-point inputs and the outputs of the reference's own
+                            IFunction_Newtonian_* / IJacobian_Newtonian_* QFunctions (qfunctions/newtonian.h:205-315),
+                            compiled unchanged into oracle/_ref/libhonee_ref.so by oracle/Makefile
+  taylorgreen_ke_step0.json the step-0 row of tests/output/taylorgreen_totalke.csv with the configuration that produced
+                            it (examples/navierstokes.c:222, examples/taylor_green_vortex.yaml)
+  unit_state.json           the UnitTests_Newtonian inputs and tolerances (problems/newtonian.c:947-987) with the
+                            reference's StateToQ outputs for every (A, B) pair
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import ctypes as C
+import importlib
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def seeded_points(rng, gas, Q, state_var):
+    """Perturbed states around an atmospheric background, with reference gradients and an affine-ish dXdx."""
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    P = 101325 * (1 + 0.01 * rng.uniform(-1, 1, Q))
+    T = 288 * (1 + 0.01 * rng.uniform(-1, 1, Q))
+    u = rng.uniform(-30, 30, (3, Q))
+    U = prob.conservative_from_primitive(gas, P, u, T)
+    Y = np.stack([P, u[0], u[1], u[2], T])
+    if state_var == 0:
+        q = U
+    elif state_var == 1:
+        q = Y
+    else:
+        import oracle as O
+        q = np.zeros((5, Q))
+        for i in range(Q):
+            out = (C.c_double * 5)()
+            O.ref().ref_StateToQ(C.byref(gas), (C.c_double * 5)(*Y[:, i]), 1, 2, out)
+            q[:, i] = out[:]
+    scale = np.abs(q) + 1e-3
+    grad_q = rng.normal(size=(3, 5, Q)) * scale[None] * 0.05
+    q_dot = rng.normal(size=(5, Q)) * scale * 3.0
+    h = 1 / 16.
+    dXdx = np.eye(3)[:, :, None] * (2 / h) + rng.normal(size=(3, 3, Q)) * 1.5
+    qdata = np.concatenate([rng.uniform(0.5, 1, (1, Q)) * (h / 2) ** 3, dXdx.reshape(9, Q)])
+    x = rng.uniform(0, 1, (3, Q))
+    dq = rng.normal(size=(5, Q)) * scale * 1e-3
+    grad_dq = rng.normal(size=(3, 5, Q)) * scale[None] * 1e-2
+    return q, grad_q, q_dot, qdata, x, dq, grad_dq
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={args.ref}"], check=True)
+    import oracle as O
+    R = O.ref()
+    assert R is not None, "reference QFunctions were not built"
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+
+    # ---- point-wise golden vectors
+    rng = np.random.default_rng(20240611)
+    Q = 24
+    cases = []
+    names = {0: "Conserv", 1: "Prim", 2: "Entropy"}
+    for state_var in (0, 1, 2):
+        for stab in (0, 1, 2):
+            cases.append(dict(state_var=state_var, stab=stab, idl=False))
+    cases.append(dict(state_var=0, stab=2, idl=True))
+    cases.append(dict(state_var=0, stab=2, idl=False, gravity=True))
+    arrays = {}
+    meta = []
+    for ci, cs in enumerate(cases):
+        ctx = prob.newtonian_context(3, stab=cs["stab"], state_var=cs["state_var"], dt=1e-5, ijacobian_time_shift=1.5e5,
+                                     g=(0.3, -9.81, 0.1) if cs.get("gravity") else (0., 0., 0.),
+                                     idl=(2e-3, 0.2, 0.5, 101000.) if cs["idl"] else None)
+        cb = prob.context_bytes(ctx)
+        njd = 15 if cs["idl"] else 14
+        q, gq, qd, qdata, x, dq, gdq = seeded_points(rng, ctx.gas, Q, cs["state_var"])
+        ins = [np.ascontiguousarray(a) for a in (q, gq, qd, qdata, x)]
+        v = np.zeros((5, Q)); gv = np.zeros((3, 5, Q)); jd = np.zeros((njd, Q))
+        assert O.call_qf(getattr(R, f"ref_IFunction_Newtonian_{names[cs['state_var']]}"), cb, Q, ins, [v, gv, jd]) == 0
+        jv = np.zeros((5, Q)); jgv = np.zeros((3, 5, Q))
+        jins = [np.ascontiguousarray(a) for a in (dq, gdq, qdata, jd)]
+        assert O.call_qf(getattr(R, f"ref_IJacobian_Newtonian_{names[cs['state_var']]}"), cb, Q, jins, [jv, jgv]) == 0
+        for k, a in dict(ctx=np.frombuffer(cb, dtype=np.uint8), q=q, grad_q=gq, q_dot=qd, qdata=qdata, x=x, v=v, grad_v=gv, jac_data=jd, dq=dq,
+                         grad_dq=gdq, jv=jv, jgrad_v=jgv).items():
+            arrays[f"c{ci}_{k}"] = a
+        meta.append(dict(cs, njd=njd, qf=names[cs["state_var"]]))
+    arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    arrays["Q"] = np.array(Q)
+    np.savez_compressed(os.path.join(HERE, "pointwise_newtonian.npz"), **arrays)
+
+    # ---- Taylor-Green KE step 0 (tests/output/taylorgreen_totalke.csv)
+    rows = [r for r in csv.reader(open(os.path.join(args.ref, "tests/output/taylorgreen_totalke.csv"))) if r and not r[0].startswith("#")]
+    header, first = rows[0], rows[1]
+    ke = {h: float(v) for h, v in zip(header, first)}
+    ke.update(dict(source="tests/output/taylorgreen_totalke.csv (step 0)", faces=[2, 2, 2], degree=2, P=3, Q=3, box=[0, 6.283185307179586],
+                   periodic=True, reference_velocity=[1, 0, 0], reference_temperature=0.2490535963, reference_pressure=71.42857143,
+                   mu=0.000625, k=0.8836267606, cv=717, cp=1003.8, csv_rtol=1e-9, csv_ztol=3e-10))
+    json.dump(ke, open(os.path.join(HERE, "taylorgreen_ke_step0.json"), "w"), indent=1)
+
+    # ---- UnitTests_Newtonian inputs (problems/newtonian.c:947-987) and reference StateToQ outputs
+    ctx = prob.newtonian_context(2)
+    gas = ctx.gas
+    T, rho, ub = 200., 1.2, 40.
+    gamma = gas.cp / gas.cv
+    Pp = (gamma - 1) * rho * gas.cv * T
+    u = [ub, ub * 1.1, ub * 1.2]
+    ek = 0.5 * sum(a * a for a in u)
+    ei = gas.cv * T
+    ent = np.log(Pp) - gamma * np.log(rho)
+    rp = rho / Pp
+    Y0 = [Pp, *u, T]
+    U0 = [rho, rho * u[0], rho * u[1], rho * u[2], rho * (ek + ei)]
+    V0 = [(gamma - ent) / (gamma - 1) - rp * ek, rp * u[0], rp * u[1], rp * u[2], -rp]
+    conv = {}
+    for a, A0 in ((0, U0), (1, Y0), (2, V0)):
+        for b in (0, 1, 2):
+            out = (C.c_double * 5)()
+            R.ref_StateToQ(C.byref(gas), (C.c_double * 5)(*A0), a, b, out)
+            conv[f"{a}->{b}"] = list(out)
+    json.dump(dict(Y0=Y0, U0=U0, V0=V0, rtol_roundtrip="20*DBL_EPSILON", rtol_fwd=5e-6, fd_eps=4e-7, state_to_q=conv,
+                   source="problems/newtonian.c:947-987"), open(os.path.join(HERE, "unit_state.json"), "w"), indent=1)
+    print("wrote", os.listdir(HERE))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,183 @@
+"""GPU parity: the fused sm_100a operators, reached through the libCEED C API, against the CPU oracle.
+
+Tolerances: restriction maps bit-exact; FP64 residual, Jacobian action and diagonal within
+1e-12 relative L2 of the oracle; geometric factors within 1e-14; the FP32 (mixed-precision) Jacobian action and
+diagonal within 2e-6 relative L2 (single-precision arithmetic on FP64 geometry).
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from helpers import O, case, oracle_ifunction, oracle_mesh, prob, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+ce = importlib.import_module("honee-4aiad_b200.ceed")
+hon = importlib.import_module("honee-4aiad_b200.honee")
+
+TOL64 = 1e-12
+TOL32 = 2e-6
+
+CASES = {
+    # config-1 shape: 3D Gaussian pulse, degree 2 (P=3, Q=3), SUPG
+    "cfg1_P3Q3": dict(n=(8, 8, 8), P=3, Q=3),
+    # config-2 shape at reduced size: degree 3 with q_extra 1 (P=4, Q=5), multi-mode state
+    "cfg2_P4Q5": dict(n=(6, 5, 4), P=4, Q=5, state="modes"),
+    # config-3 shape: periodic, degree 4 with q_extra 1 (P=5, Q=6)
+    "cfg3_P5Q6_periodic": dict(n=(4, 4, 4), P=5, Q=6, periodic=(1, 1, 1), state="modes"),
+    "su_gravity_P4Q4": dict(n=(3, 3, 3), P=4, Q=4, stab=prob.STAB_SU, g=(0.5, -9.81, 0.2)),
+    "nostab_P3Q4": dict(n=(3, 4, 2), P=3, Q=4, stab=prob.STAB_NONE),
+    "idl_P3Q3": dict(n=(6, 3, 3), P=3, Q=3, idl=(2e-3, 0.2, 0.5, 101000.0)),
+}
+
+
+def _setup(name, resource="/gpu/b200"):
+    kw = dict(CASES[name])
+    mesh, basis, ctx, q, qd = case(**kw)
+    ceed = ce.Ceed(resource)
+    ops = hon.NewtonianOperators(ceed, mesh, basis, ctx)
+    qv = ce.Vector(ceed, mesh.l_size)
+    qv.set_array_host(q)
+    ops.q_dot.set_array_host(qd)
+    g = ce.Vector(ceed, mesh.l_size)
+    return mesh, basis, ctx, q, qd, ceed, ops, qv, g
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_ifunction_ijacobian_diagonal_fp64(name):
+    mesh, basis, ctx, q, qd, ceed, ops, qv, g = _setup(name)
+    v_ref, jd_ref, qdata_ref, m = oracle_ifunction(mesh, basis, ctx, q, qd)
+    # geometric factors (Setup QFunction)
+    assert rel_l2(ops.q_data.to_numpy(), qdata_ref) < 1e-14
+    # residual
+    ops.ifunction(qv, ops.q_dot, g)
+    v = g.to_numpy()
+    assert rel_l2(v, v_ref) < TOL64, rel_l2(v, v_ref)
+    assert rel_l2(ops.jac_data.to_numpy(), jd_ref) < TOL64
+    # Jacobian action
+    cb = prob.context_bytes(ctx)
+    dq = np.random.default_rng(3).normal(size=q.shape) * np.abs(q) * 1e-4
+    dv = ce.Vector(ceed, mesh.l_size)
+    dv.set_array_host(dq)
+    jv = ce.Vector(ceed, mesh.l_size)
+    ops.ijacobian(dv, jv)
+    j_ref = O.apply_ijacobian(m, cb, dq, qdata_ref, jd_ref, num_jd=ops.num_jd)
+    assert rel_l2(jv.to_numpy(), j_ref) < TOL64, rel_l2(jv.to_numpy(), j_ref)
+    # ApplyAdd accumulates
+    ops.ijacobian(dv, jv, add=True)
+    assert rel_l2(jv.to_numpy(), 2 * j_ref) < TOL64
+    # diagonal
+    if mesh.num_elem <= 216:
+        d = ce.Vector(ceed, mesh.l_size)
+        ops.diagonal(d)
+        d_ref = O.assemble_diagonal(m, cb, qdata_ref, jd_ref, mesh.l_size, num_jd=ops.num_jd)
+        assert rel_l2(d.to_numpy(), d_ref) < TOL64, rel_l2(d.to_numpy(), d_ref)
+
+
+@pytest.mark.parametrize("name", ["cfg1_P3Q3", "cfg2_P4Q5", "cfg3_P5Q6_periodic"])
+def test_mixed_precision_jacobian(name):
+    mesh, basis, ctx, q, qd, ceed, ops, qv, g = _setup(name, "/gpu/b200/mixed")
+    v_ref, jd_ref, qdata_ref, m = oracle_ifunction(mesh, basis, ctx, q, qd)
+    ops.ifunction(qv, ops.q_dot, g)
+    assert rel_l2(g.to_numpy(), v_ref) < TOL64  # the residual stays FP64
+    cb = prob.context_bytes(ctx)
+    dq = np.random.default_rng(4).normal(size=q.shape) * np.abs(q) * 1e-4
+    dv = ce.Vector(ceed, mesh.l_size)
+    dv.set_array_host(dq)
+    jv = ce.Vector(ceed, mesh.l_size)
+    ops.ijacobian(dv, jv)
+    j_ref = O.apply_ijacobian(m, cb, dq, qdata_ref, jd_ref)
+    err = rel_l2(jv.to_numpy(), j_ref)
+    assert err < TOL32, err
+    d = ce.Vector(ceed, mesh.l_size)
+    ops.diagonal(d)
+    d_ref = O.assemble_diagonal(m, cb, qdata_ref, jd_ref, mesh.l_size)
+    assert rel_l2(d.to_numpy(), d_ref) < TOL32
+
+
+def test_context_labels_update_the_kernels():
+    """FormIJacobian_NS sets "ijacobian time shift" by label before the Krylov solve (src/setupts.c:141)."""
+    mesh, basis, ctx, q, qd, ceed, ops, qv, g = _setup("cfg1_P3Q3")
+    ops.ifunction(qv, ops.q_dot, g)
+    dq = np.random.default_rng(5).normal(size=q.shape) * np.abs(q) * 1e-4
+    dv = ce.Vector(ceed, mesh.l_size)
+    dv.set_array_host(dq)
+    jv = ce.Vector(ceed, mesh.l_size)
+    ops.set_ijacobian_shift(12345.0)
+    assert ops.op_ijacobian.get_context_double("ijacobian time shift") == [12345.0]
+    ops.ijacobian(dv, jv)
+    ctx2 = prob.newtonian_context(2)
+    import ctypes as C
+    C.memmove(C.addressof(ctx2), C.addressof(ctx), C.sizeof(ctx))
+    _, jd_ref, qdata_ref, m = oracle_ifunction(mesh, basis, ctx2, q, qd)
+    ctx2.ijacobian_time_shift = 12345.0
+    j_ref = O.apply_ijacobian(m, prob.context_bytes(ctx2), dq, qdata_ref, jd_ref)
+    assert rel_l2(jv.to_numpy(), j_ref) < TOL64
+
+
+def test_restriction_maps_bit_exact():
+    mesh = prob.box_mesh((3, 2, 2), 4, periodic=(1, 0, 1))
+    ceed = ce.Ceed("/gpu/b200")
+    r = ce.ElemRestriction(ceed, mesh.num_elem, 64, 5, 1, mesh.l_size, offsets=mesh.offsets)
+    lv, ev = r.create_vectors()
+    rng = np.random.default_rng(8)
+    l = rng.normal(size=mesh.l_size)
+    lv.set_array_host(l)
+    r.apply(False, lv, ev)
+    e = ev.to_numpy()
+    e_ref = np.zeros_like(e)
+    O.lib().oracle_restrict(mesh.num_elem, 64, 5, 1, O.ptr(mesh.offsets), O.ptr(l), O.ptr(e_ref))
+    np.testing.assert_array_equal(e, e_ref)
+    lv.set_value(0.0)
+    r.apply(True, ev, lv)
+    lt_ref = np.zeros(mesh.l_size)
+    O.lib().oracle_restrict_t(mesh.num_elem, 64, 5, 1, O.ptr(mesh.offsets), O.ptr(e_ref), O.ptr(lt_ref))
+    np.testing.assert_array_equal(lv.to_numpy(), lt_ref)
+
+
+def test_colouring_is_conflict_free():
+    kern = importlib.import_module("honee-4aiad_b200.kernels")
+    mesh = prob.box_mesh((6, 4, 4), 4, periodic=(1, 0, 1))
+    basis = prob.tensor_basis(4, 5)
+    op = kern.ElemOp(mesh, basis)
+    assert op.num_colors == 8 and sum(op.color_sizes()) == mesh.num_elem
+
+
+def test_unsupported_qfunction_fails_loudly():
+    ceed = ce.Ceed("/gpu/b200")
+    mesh = prob.box_mesh((1, 1, 1), 3)
+    basis = prob.tensor_basis(3, 3)
+    b = ce.Basis(ceed, 3, 5, 3, 3, basis.interp1d, basis.grad1d, basis.qref1d, basis.qweight1d)
+    r = ce.ElemRestriction(ceed, 1, 27, 5, 1, mesh.l_size, offsets=mesh.offsets)
+    qf = ce.QFunction(ceed, "newtonian.h:RHSFunction_Newtonian")
+    qf.add_input("q", 5, ce.CEED_EVAL_INTERP)
+    qf.add_output("v", 5, ce.CEED_EVAL_INTERP)
+    op = ce.Operator(ceed, qf)
+    op.set_field("q", r, b, ceed.active)
+    op.set_field("v", r, b, ceed.active)
+    x = ce.Vector(ceed, mesh.l_size)
+    x.set_value(1.0)
+    y = ce.Vector(ceed, mesh.l_size)
+    with pytest.raises(ce.CeedError) as ei:
+        op.apply(x, y)
+    assert ei.value.code == ce.CEED_ERROR_UNSUPPORTED and "no CPU fallback" in str(ei.value)
+
+
+def test_direct_kernel_abi_matches_ceed_path():
+    """The kernel ABI on caller-managed device buffers (torch tensors) equals the libCEED path."""
+    import torch
+    kern = importlib.import_module("honee-4aiad_b200.kernels")
+    mesh, basis, ctx, q, qd, ceed, ops, qv, g = _setup("cfg2_P4Q5")
+    ops.ifunction(qv, ops.q_dot, g)
+    v_ceed = g.to_numpy()
+    op = kern.ElemOp(mesh, basis)
+    dev = torch.device("cuda:0")
+    tq = torch.from_numpy(q).to(dev)
+    tqd = torch.from_numpy(qd).to(dev)
+    tqdata = torch.from_numpy(ops.q_data.to_numpy()).to(dev)
+    tv = torch.zeros_like(tq)
+    tjd = torch.zeros(mesh.num_elem * 14 * basis.Q ** 3, dtype=torch.float64, device=dev)
+    op.ifunction(prob.context_bytes(ctx), tq, tqd, tqdata, tv, jac_data=tjd)
+    torch.cuda.synchronize()
+    assert rel_l2(tv.cpu().numpy(), v_ceed) < 1e-15
