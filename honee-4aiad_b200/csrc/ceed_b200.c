@@ -555,6 +555,7 @@ int CeedVectorAXPBY(CeedVector y, CeedScalar alpha, CeedScalar beta, CeedVector 
   return CEED_ERROR_SUCCESS;
 }
 int CeedVectorPointwiseMult(CeedVector w, CeedVector x, CeedVector y) {
+  if (x->length != w->length || y->length != w->length) return CeedError(w->ceed, CEED_ERROR_INCOMPATIBLE, "vector lengths differ");
   const double *xd, *yd;
   double       *wd;
   CK(vec_dev_read(x, &xd));
@@ -638,7 +639,13 @@ int CeedElemRestrictionCreateStrided(Ceed ceed, CeedInt num_elem, CeedInt elem_s
     r->strides[0] = 1;
     r->strides[1] = elem_size;
     r->strides[2] = elem_size * num_comp;
-  } else memcpy(r->strides, strides, sizeof(r->strides));
+  } else {
+    memcpy(r->strides, strides, sizeof(r->strides));
+    if (strides[0] < 0 || strides[1] < 0 || strides[2] < 0) {
+      CeedElemRestrictionDestroy(&r);
+      return CeedError(ceed, CEED_ERROR_DIMENSION, "negative restriction strides are not supported");
+    }
+  }
   const int64_t last = (int64_t)(elem_size - 1) * r->strides[0] + (int64_t)(num_comp - 1) * r->strides[1] + (int64_t)(num_elem - 1) * r->strides[2];
   if (num_elem > 0 && (last >= l_size || last < 0)) {
     CeedElemRestrictionDestroy(&r);
@@ -710,6 +717,10 @@ static int rstr_build_transpose(CeedElemRestriction r) {
 
 int CeedElemRestrictionApply(CeedElemRestriction r, CeedTransposeMode t_mode, CeedVector u, CeedVector ru, CeedRequest *request) {
   (void)request;
+  const CeedSize e_size = (CeedSize)r->num_elem * r->elem_size * r->num_comp;
+  const CeedSize in_len = t_mode == CEED_NOTRANSPOSE ? r->l_size : e_size, out_len = t_mode == CEED_NOTRANSPOSE ? e_size : r->l_size;
+  if (u->length < in_len || ru->length < out_len)
+    return CeedError(r->ceed, CEED_ERROR_DIMENSION, "restriction apply vectors too short (need %td in, %td out)", in_len, out_len);
   CK(rstr_upload(r));
   const double *in;
   double       *out;
@@ -921,6 +932,13 @@ int CeedBasisApply(CeedBasis b, CeedInt num_elem, CeedTransposeMode t_mode, Ceed
   if (eval_mode != CEED_EVAL_INTERP && eval_mode != CEED_EVAL_GRAD && eval_mode != CEED_EVAL_WEIGHT)
     return CeedError(b->ceed, CEED_ERROR_UNSUPPORTED, "eval mode %d not supported", eval_mode);
   CK(basis_upload(b));
+  CeedSize Pn = 1, Qn = 1;
+  for (int d = 0; d < b->dim; d++) Pn *= b->P1d, Qn *= b->Q1d;
+  const CeedSize nq = (CeedSize)num_elem * b->num_comp * (eval_mode == CEED_EVAL_GRAD ? b->dim : 1) * Qn, np = (CeedSize)num_elem * b->num_comp * Pn;
+  const CeedSize need_in = eval_mode == CEED_EVAL_WEIGHT ? 0 : (t_mode == CEED_TRANSPOSE ? nq : np);
+  const CeedSize need_out = eval_mode == CEED_EVAL_WEIGHT ? (CeedSize)num_elem * Qn : (t_mode == CEED_TRANSPOSE ? np : nq);
+  if ((need_in && (!u || u == CEED_VECTOR_NONE || u->length < need_in)) || v->length < need_out)
+    return CeedError(b->ceed, CEED_ERROR_DIMENSION, "basis apply vectors too short (need %td in, %td out)", need_in, need_out);
   const double *in = NULL;
   double       *out;
   if (eval_mode != CEED_EVAL_WEIGHT) CK(vec_dev_read(u, &in));
@@ -1417,6 +1435,13 @@ static int vec_f32_shadow(CeedVector v) {
   return CEED_ERROR_SUCCESS;
 }
 
+/* every vector a planned operator touches must be at least as long as its restriction says (device safety) */
+static int need_len(CeedOperator op, CeedVector v, CeedSize n, const char *what) {
+  if (!v || v == CEED_VECTOR_ACTIVE || v == CEED_VECTOR_NONE || v->length < n)
+    return CeedError(op->ceed, CEED_ERROR_DIMENSION, "operator '%s': %s vector missing or shorter than %td", op->name, what, n);
+  return CEED_ERROR_SUCCESS;
+}
+
 /* apply one non-composite operator, adding into out (out already holds what should be kept) */
 static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
   CK(op_plan(op));
@@ -1425,6 +1450,8 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
   switch (op->plan) {
     case PLAN_SETUP: {
       CeedBasis bx = op->in[0].b;
+      CK(need_len(op, in, op->in[0].r->l_size, "coordinate"));
+      CK(need_len(op, out, op->out[0].r->l_size, "qdata"));
       CK(gather_coords(op, &op->in[0], in, &op->d_tmp_e));
       double *qd;
       CK(vec_dev_write(out, &qd, 0));
@@ -1434,6 +1461,13 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
     }
     case PLAN_IFUNCTION: {
       const HbNewtonianContext *ctx = (const HbNewtonianContext *)op->qf->ctx->data;
+      if ((ctx->idl_enable ? 15 : 14) != op->qf->out[2].size)
+        return plan_fail(op, "jac_data must have 15 components with the IDL enabled and 14 without (problems/newtonian.c:756-757)");
+      CK(need_len(op, in, op->eop->l_size, "input"));
+      CK(need_len(op, out, op->eop->l_size, "output"));
+      CK(need_len(op, op->in[2].v, op->eop->l_size, "q dot"));
+      CK(need_len(op, op->in[3].v, op->in[3].r->l_size, "qdata"));
+      CK(need_len(op, op->out[2].v, op->out[2].r->l_size, "jac_data"));
       if (ctx->idl_enable && !op->idl_coords_set) {
         CeedVector xv = op->in[4].v;
         if (!xv || xv == CEED_VECTOR_ACTIVE || xv == CEED_VECTOR_NONE) return plan_fail(op, "IDL needs the coordinate field 'x'");
@@ -1466,6 +1500,12 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
     }
     case PLAN_IJACOBIAN: {
       const HbNewtonianContext *ctx = (const HbNewtonianContext *)op->qf->ctx->data;
+      if ((ctx->idl_enable ? 15 : 14) != op->qf->in[3].size)
+        return plan_fail(op, "jac_data must have 15 components with the IDL enabled and 14 without (problems/newtonian.c:756-757)");
+      CK(need_len(op, in, op->eop->l_size, "input"));
+      CK(need_len(op, out, op->eop->l_size, "output"));
+      CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
+      CK(need_len(op, op->in[3].v, op->in[3].r->l_size, "jac_data"));
       const double             *qd;
       CK(vec_dev_read(op->in[2].v, &qd));
       CeedVector jd = op->in[3].v;
@@ -1529,6 +1569,11 @@ int CeedOperatorApplyAdd(CeedOperator op, CeedVector in, CeedVector out, CeedReq
 static int op_diag_add_single(CeedOperator op, CeedVector assembled) {
   CK(op_plan(op));
   if (op->plan != PLAN_IJACOBIAN) return plan_fail(op, "diagonal assembly is provided for the IJacobian operator");
+  CK(need_len(op, assembled, op->eop->l_size, "diagonal"));
+  CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
+  CK(need_len(op, op->in[3].v, op->in[3].r->l_size, "jac_data"));
+  if ((((const HbNewtonianContext *)op->qf->ctx->data)->idl_enable ? 15 : 14) != op->qf->in[3].size)
+    return plan_fail(op, "jac_data component count does not match the IDL setting");
   Ceed                      ceed = op->ceed;
   cudaStream_t              s    = ceed->stream;
   const HbNewtonianContext *ctx  = (const HbNewtonianContext *)op->qf->ctx->data;

@@ -132,7 +132,8 @@ __global__ void k_basis(int num_elem, int ncomp, int dim, int P, int Q, int tmod
   const int nd = emode == 2 ? dim : 1;
   int64_t nout;
   if (emode == 16) nout = (int64_t)num_elem * Qn;
-  else nout = (int64_t)num_elem * ncomp * nd * (tmode ? Pn : Qn);
+  else if (tmode) nout = (int64_t)num_elem * ncomp * Pn;  // transpose sums over the nd gradient directions
+  else nout = (int64_t)num_elem * ncomp * nd * Qn;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nout; t += (int64_t)gridDim.x * blockDim.x) {
     if (emode == 16) {
       int q = (int)(t % Qn), w = 1;
@@ -281,7 +282,7 @@ int hb_basis_apply_generic(int num_elem, int ncomp, int dim, int P, int Q, int t
     Pn *= P;
     Qn *= Q;
   }
-  const int64_t n = (int64_t)num_elem * ncomp * (emode == 2 ? dim : 1) * (tmode ? Pn : Qn);
+  const int64_t n = emode == 16 ? (int64_t)num_elem * Qn : (tmode ? (int64_t)num_elem * ncomp * Pn : (int64_t)num_elem * ncomp * (emode == 2 ? dim : 1) * Qn);
   k_basis<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(num_elem, ncomp, dim, P, Q, tmode, emode, d_B, d_G, d_w, u, v);
   return rc();
 }
