@@ -214,6 +214,10 @@ def run_gpu(args, rank, world):
         ms64 = timed(step64, args.steps)
     clocks = clk.summary()
     ms32 = timed(step32, args.steps)
+    if args.only_kernels:
+        if rank == 0:
+            print(json.dumps({"ms_per_step_f64": ms64, "ms_per_step_f32": ms32, "gdofs_f64": N_L / ms64 / 1e6, "clocks": clocks}), flush=True)
+        return
     ms_if = timed(lambda: op.ifunction(cb, t_q, t_qd, t_qdata, t_v, jac_data=t_jd), args.steps)
     ms_ij = timed(lambda: op.ijacobian(cb, t_qdata, t_jd, t_dq, t_jv), args.steps)
     ms_if32 = timed(lambda: op.ifunction(cb, t_q, t_qd, t_qdata, t_v, jac_data_f32=t_jd32), args.steps)
@@ -324,6 +328,7 @@ def main():
     ap.add_argument("--size", type=int, default=64)
     ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only-kernels", action="store_true", help="time the fused kernels only (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

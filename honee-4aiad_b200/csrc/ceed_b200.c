@@ -1454,7 +1454,7 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
       CK(need_len(op, out, op->out[0].r->l_size, "qdata"));
       CK(gather_coords(op, &op->in[0], in, &op->d_tmp_e));
       double *qd;
-      CK(vec_dev_write(out, &qd, 0));
+      CK(vec_dev_write(out, &qd, 1));
       /* Setup writes (not adds) qdata: libCEED's strided output of an EVAL_NONE field is overwritten per element */
       HB_CK(ceed, hb_setup_qdata(op->in[0].r->num_elem, bx->Q1d, bx->qref1d, bx->qweight1d, op->d_tmp_e, qd, s));
       return CEED_ERROR_SUCCESS;
