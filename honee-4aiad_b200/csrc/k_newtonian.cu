@@ -116,6 +116,32 @@ struct QRef {
   double x[kMaxP];
 };
 
+// L2 prefetch of the 16-byte-aligned part of [p, p + bytes) with one bulk (TMA-engine) request; issued by one thread.
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, size_t bytes) {
+  const uintptr_t a = (uintptr_t)p, lo = (a + 15) & ~(uintptr_t)15, hi = (a + bytes) & ~(uintptr_t)15;
+  if (hi > lo) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// Warm L2 with the next element's node values (all L-vectors it gathers or scatter-adds) and its per-point data.
+template <int P, typename TL>
+__device__ __forceinline__ void prefetch_element(const int32_t *__restrict__ offsets, int e, const TL *const *vecs, int nvec, const void *blk0,
+                                                 size_t bytes0, const void *blk1, size_t bytes1) {
+  constexpr int P3 = P * P * P;
+  if (threadIdx.x < P3) {
+    const int64_t o = __ldg(offsets + (int64_t)e * P3 + threadIdx.x);
+    for (int v = 0; v < nvec; v++) {
+      const char *a = (const char *)(vecs[v] + o);
+      prefetch_l2(a);
+      prefetch_l2(a + 5 * sizeof(TL) - 1);
+    }
+  } else if (threadIdx.x == P3) {
+    if (blk0) prefetch_l2_bulk(blk0, bytes0);
+    if (blk1) prefetch_l2_bulk(blk1, bytes1);
+  }
+}
+
 // ---------------------------------------------------------------------------------------------------------------------
 // Forward: gather NV input L-vectors (5 comps each) and produce interp [NV*5][Q3] and, for the first vector, the
 // reference gradient [3][5][Q3].  Shared layout (doubles or T): sN [NV*5][P3], s1 [NV*5][P][P][Q], s2 [NV*5][P][Q][Q].
@@ -302,15 +328,22 @@ struct IfunctionPtrs {
 };
 
 template <int P, int Q>
-__global__ void __launch_bounds__(nthreads_for<double>(Q), 2) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p) {
+__global__ void __launch_bounds__(nthreads_for<double>(Q), 3) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p) {
   constexpr int NT = nthreads_for<double>(Q);
   using L = SmemLayout<P, Q>;
   extern __shared__ __align__(16) double smem[];
   double *sN = smem, *s1 = sN + L::nN, *s2 = s1 + L::n1, *sU = s2 + L::n2, *sG = sU + L::nU;
   double *sD = sU + 5 * L::Q3;  // interp of q_dot
   const double *lin[2] = {p.q, p.q_dot};
+  const double *pre[3] = {p.q, p.q_dot, p.v};
   for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
     const int e = a.elems[idx];
+    if (idx == blockIdx.x)
+      prefetch_element<P, double>(a.offsets, e, pre, 3, a.qdata + (int64_t)e * 10 * L::Q3, sizeof(double) * 10 * L::Q3, nullptr, 0);
+    if (idx + gridDim.x < a.n_elems) {
+      const int en = a.elems[idx + gridDim.x];
+      prefetch_element<P, double>(a.offsets, en, pre, 3, a.qdata + (int64_t)en * 10 * L::Q3, sizeof(double) * 10 * L::Q3, nullptr, 0);
+    }
     forward<P, Q, 2, NT, double, double>(a, e, lin, sN, s1, s2, sU, sG);
     const int q = threadIdx.x;
     if (q < L::Q3) {
@@ -363,7 +396,7 @@ struct IjacobianPtrs {
 };
 
 template <int P, int Q, typename T>
-__global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
+__global__ void __launch_bounds__(nthreads_for<T>(Q), 3) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
   constexpr int NT = nthreads_for<T>(Q);
   using L = SmemLayout<P, Q>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -371,8 +404,18 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_ijacobian(const ElemA
   T *sN = smem, *s1 = sN + L::nN, *s2 = s1 + L::n1, *sU = s2 + L::n2, *sG = sU + L::nU;
   T *sW1 = sU + 5 * L::Q3;
   const T *lin[1] = {p.dq};
+  const T *pre[2] = {p.dq, p.v};
+  const size_t jbytes = sizeof(T) * (size_t)a.num_jd * L::Q3;
   for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
     const int e = a.elems[idx];
+    if (idx == blockIdx.x)
+      prefetch_element<P, T>(a.offsets, e, pre, 2, a.qdata + (int64_t)e * 10 * L::Q3, sizeof(double) * 10 * L::Q3,
+                             p.jac_data + (int64_t)e * a.num_jd * L::Q3, jbytes);
+    if (idx + gridDim.x < a.n_elems) {
+      const int en = a.elems[idx + gridDim.x];
+      prefetch_element<P, T>(a.offsets, en, pre, 2, a.qdata + (int64_t)en * 10 * L::Q3, sizeof(double) * 10 * L::Q3,
+                             p.jac_data + (int64_t)en * a.num_jd * L::Q3, jbytes);
+    }
     forward<P, Q, 1, NT, T, T>(a, e, lin, sN, s1, s2, sU, sG);
     const int q = threadIdx.x;
     if (q < L::Q3) {
@@ -634,7 +677,7 @@ static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, c
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<double> a = make_args<double>(op, ctx, io->qdata, c);
     if (a.n_elems == 0) continue;
-    k_ifunction<P, Q><<<grid_for(op, a.n_elems, 2), nthreads_for<double>(Q), sm, s>>>(a, p);
+    k_ifunction<P, Q><<<grid_for(op, a.n_elems, 3), nthreads_for<double>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
@@ -648,7 +691,7 @@ static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, c
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
-    k_ijacobian<P, Q, T><<<grid_for(op, a.n_elems, 2), nthreads_for<T>(Q), sm, s>>>(a, p);
+    k_ijacobian<P, Q, T><<<grid_for(op, a.n_elems, 3), nthreads_for<T>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
