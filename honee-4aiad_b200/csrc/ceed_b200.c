@@ -43,6 +43,8 @@ struct Ceed_private {
   CeedErrorHandler handler;
   char             err_msg[2048];
   double          *d_scratch; /* 1024 doubles for reductions */
+  HbElemOp        *ops[64];   /* element operators whose kernel status words are checked at host synchronisation */
+  int              nops;
 };
 
 struct CeedVector_private {
@@ -369,6 +371,30 @@ static int vec_sync_dev(CeedVector v) {
   }
   return CEED_ERROR_SUCCESS;
 }
+/* Kernels never trap: a bounded wait that gives up sets a status word.  Surface it at the next host synchronisation. */
+static int ceed_check_status(Ceed ceed) {
+  for (int i = 0; i < ceed->nops; i++) {
+    int st = 0;
+    if (cudaMemcpy(&st, ceed->ops[i]->d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return CeedError(ceed, CEED_ERROR_BACKEND, "could not read the kernel status word");
+    if (st) {
+      cudaMemset(ceed->ops[i]->d_status, 0, sizeof(int));
+      return CeedError(ceed, CEED_ERROR_BACKEND, "a fused kernel abandoned a bounded wait (status %d); its output is incomplete", st);
+    }
+  }
+  return CEED_ERROR_SUCCESS;
+}
+static void ceed_register_op(Ceed ceed, HbElemOp *op) {
+  if (ceed->nops < 64) ceed->ops[ceed->nops++] = op;
+}
+static void ceed_unregister_op(Ceed ceed, HbElemOp *op) {
+  for (int i = 0; i < ceed->nops; i++)
+    if (ceed->ops[i] == op) {
+      ceed->ops[i] = ceed->ops[--ceed->nops];
+      return;
+    }
+}
+
 static int vec_sync_host(CeedVector v) {
   CK(vec_unstale(v));
   CK(vec_alloc_host(v));
@@ -377,6 +403,7 @@ static int vec_sync_host(CeedVector v) {
     CUDA_CK(v->ceed, cudaMemcpyAsync(v->h, v->d, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToHost, v->ceed->stream));
     CUDA_CK(v->ceed, cudaStreamSynchronize(v->ceed->stream));
     v->h_valid = 1;
+    CK(ceed_check_status(v->ceed));
   }
   return CEED_ERROR_SUCCESS;
 }
@@ -517,6 +544,7 @@ int CeedVectorNorm(CeedVector v, CeedNormType type, CeedScalar *norm) {
   double r  = 0;
   int    tp = type == CEED_NORM_1 ? 0 : (type == CEED_NORM_2 ? 1 : 2);
   HB_CK(v->ceed, hb_vec_reduce_f64(d, NULL, v->length, tp, v->ceed->d_scratch, &r, v->ceed->stream));
+  CK(ceed_check_status(v->ceed));
   *norm = type == CEED_NORM_2 ? sqrt(r) : r;
   return CEED_ERROR_SUCCESS;
 }
@@ -1340,6 +1368,7 @@ static int plan_elemop(CeedOperator op, CeedElemRestriction r, CeedBasis b) {
   if (r->elem_size != b->P1d * b->P1d * b->P1d) return plan_fail(op, "restriction element size does not match the basis");
   if (!op->eop) {
     HB_CK(op->ceed, hb_elemop_create(r->num_elem, b->P1d, b->Q1d, r->h_off, r->l_size, b->interp1d, b->grad1d, b->qref1d, b->qweight1d, &op->eop));
+    ceed_register_op(op->ceed, op->eop);
   }
   return CEED_ERROR_SUCCESS;
 }
@@ -1666,6 +1695,7 @@ int CeedOperatorDestroy(CeedOperator *op) {
       }
     CeedQFunctionDestroy(&o->qf);
   }
+  if (o->eop) ceed_unregister_op(o->ceed, o->eop);
   hb_elemop_destroy(o->eop);
   cudaFree(o->d_tmp_in32);
   cudaFree(o->d_tmp_out32);

@@ -39,7 +39,16 @@ static int color_elements(int num_elem, int elem_size, const int32_t *offsets, i
     }
     color[e] = (uint8_t)c;
     if (c + 1 > ncol) ncol = c + 1;
-    for (int p = 0; p < elem_size; p++) mask[o[p]] |= (uint64_t)1 << c;
+    for (int p = 0; p < elem_size; p++) {
+      /* colour c was free on all of e's nodes, so a bit already set here means e lists this node twice (a periodic
+       * direction with one element); its scatter would then race with itself */
+      if (mask[o[p]] & ((uint64_t)1 << c)) {
+        free(mask);
+        free(color);
+        return HB_ERROR_UNSUPPORTED;
+      }
+      mask[o[p]] |= (uint64_t)1 << c;
+    }
   }
   free(mask);
   int32_t *ptr = (int32_t *)calloc((size_t)ncol + 1, sizeof(int32_t));
@@ -126,8 +135,11 @@ int hb_elemop_create(int num_elem, int P, int Q, const int32_t *offsets, int64_t
     cudaDeviceGetAttribute(&op->num_sms, cudaDevAttrMultiProcessorCount, op->device);
     if (op->num_sms <= 0) op->num_sms = 148;
     const size_t nb_off = sizeof(int32_t) * (size_t)num_elem * P3, nb_col = sizeof(int32_t) * (size_t)num_elem;
-    if (cudaMalloc((void **)&op->d_offsets, nb_off) != cudaSuccess || cudaMalloc((void **)&op->d_color_elem, nb_col) != cudaSuccess)
+    if (cudaMalloc((void **)&op->d_offsets, nb_off) != cudaSuccess || cudaMalloc((void **)&op->d_color_elem, nb_col) != cudaSuccess ||
+        cudaMalloc((void **)&op->d_status, sizeof(int)) != cudaSuccess)
       err = HB_ERROR_NOMEM;
+    else if (cudaMemset(op->d_status, 0, sizeof(int)) != cudaSuccess)
+      err = HB_ERROR_CUDA;
     else if (cudaMemcpy(op->d_offsets, offsets, nb_off, cudaMemcpyHostToDevice) != cudaSuccess ||
              cudaMemcpy(op->d_color_elem, color_elem, nb_col, cudaMemcpyHostToDevice) != cudaSuccess)
       err = HB_ERROR_CUDA;
@@ -148,8 +160,17 @@ int hb_elemop_set_vertex_coords(HbElemOp *op, const double *x_elem) {
   return cudaMemcpy(op->d_x_elem, x_elem, nb, cudaMemcpyHostToDevice) == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
+int hb_elemop_status(HbElemOp *op, int *status, int clear) {
+  if (!op || !status) return HB_ERROR_INVALID;
+  if (cudaDeviceSynchronize() != cudaSuccess) return HB_ERROR_CUDA;
+  if (cudaMemcpy(status, op->d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return HB_ERROR_CUDA;
+  if (clear && *status && cudaMemset(op->d_status, 0, sizeof(int)) != cudaSuccess) return HB_ERROR_CUDA;
+  return HB_SUCCESS;
+}
+
 int hb_elemop_destroy(HbElemOp *op) {
   if (!op) return HB_SUCCESS;
+  if (op->d_status) cudaFree(op->d_status);
   if (op->d_offsets) cudaFree(op->d_offsets);
   if (op->d_color_elem) cudaFree(op->d_color_elem);
   if (op->d_x_elem) cudaFree(op->d_x_elem);

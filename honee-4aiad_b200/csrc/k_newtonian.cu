@@ -17,6 +17,7 @@
 
 #include "honee_b200.h"
 #include "newtonian_qf.cuh"
+#include "pipeline.cuh"
 
 namespace hb {
 
@@ -33,6 +34,8 @@ template <typename T>
 __host__ __device__ constexpr int nthreads_for(int Q) {
   return ((Q * Q * Q + 31) / 32) * 32;
 }
+// resident CTAs per SM the register budget is tuned for (65536 registers / (threads * CTAs))
+__host__ __device__ constexpr int min_blocks_for(int Q) { return Q <= 5 ? 3 : (Q == 6 ? 2 : 1); }
 
 // ---------------------------------------------------------------------------------------------------------------------
 // fibre passes over shared-memory tensors.  All arrays are [comp][n2][n1][n0] with n0 fastest.
@@ -88,6 +91,7 @@ struct ElemArgs {
   const double *qdata;     // [E][10][Q^3]
   const double *x_elem;    // [E][3][8] vertex coordinates (IDL only), may be null
   int num_jd;              // 14 or 15
+  int *status;             // device error word: bit 0 = a bounded wait gave up
 };
 
 template <typename T>
@@ -116,52 +120,56 @@ struct QRef {
   double x[kMaxP];
 };
 
-// L2 prefetch of the 16-byte-aligned part of [p, p + bytes) with one bulk (TMA-engine) request; issued by one thread.
-__device__ __forceinline__ void prefetch_l2_bulk(const void *p, size_t bytes) {
-  const uintptr_t a = (uintptr_t)p, lo = (a + 15) & ~(uintptr_t)15, hi = (a + bytes) & ~(uintptr_t)15;
-  if (hi > lo) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");
-}
-
-__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
-// Warm L2 with the next element's node values (all L-vectors it gathers or scatter-adds) and its per-point data.
-template <int P, typename TL>
-__device__ __forceinline__ void prefetch_element(const int32_t *__restrict__ offsets, int e, const TL *const *vecs, int nvec, const void *blk0,
-                                                 size_t bytes0, const void *blk1, size_t bytes1) {
-  constexpr int P3 = P * P * P;
-  if (threadIdx.x < P3) {
-    const int64_t o = __ldg(offsets + (int64_t)e * P3 + threadIdx.x);
-    for (int v = 0; v < nvec; v++) {
-      const char *a = (const char *)(vecs[v] + o);
-      prefetch_l2(a);
-      prefetch_l2(a + 5 * sizeof(TL) - 1);
-    }
-  } else if (threadIdx.x == P3) {
-    if (blk0) prefetch_l2_bulk(blk0, bytes0);
-    if (blk1) prefetch_l2_bulk(blk1, bytes1);
-  }
-}
-
 // ---------------------------------------------------------------------------------------------------------------------
-// Forward: gather NV input L-vectors (5 comps each) and produce interp [NV*5][Q3] and, for the first vector, the
-// reference gradient [3][5][Q3].  Shared layout (doubles or T): sN [NV*5][P3], s1 [NV*5][P][P][Q], s2 [NV*5][P][Q][Q].
-template <int P, int Q, int NV, int NT, typename T, typename TL>
-__device__ __forceinline__ void forward(const ElemArgs<T> &a, int e, const TL *const *l_in, T *sN, T *s1, T *s2, T *sU, T *sG) {
-  constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
-  constexpr int NC = NV * 5;
-  const int32_t *off = a.offsets + (int64_t)e * P3;
+// Element pipeline.  Per CTA, elements are processed one after another; while element e is computed, the data of the
+// next element e' of the same colour is already being copied into shared memory:
+//   * its node values (state, time derivative) by cp.async, issued once the first fibre pass has consumed e's values
+//   * its per-point blocks (qdata, stored Jacobian data) by TMA bulk copies on an mbarrier, issued after e's point-wise
+//     phase has consumed e's blocks
+//   * the current values of the output L-vector at its nodes by cp.async, issued after e's scatter
+// so each element starts with all its inputs resident.  Elements of one colour share no node, so the output values
+// gathered ahead are still current when the element scatters (a plain store of old + contribution, no atomics).
+
+// Gather NV L-vectors (5 interleaved comps each) at element e's nodes into comp-major sN [NV*5][P3].
+template <int P, int NV, int NT, typename T, typename TL>
+__device__ __forceinline__ void gather_async(const int32_t *__restrict__ offsets, int e, const TL *const *l_in, T *sN) {
+  constexpr int P3 = P * P * P;
+  static_assert(sizeof(T) == sizeof(TL), "staged copies keep the L-vector precision");
+  const int32_t *off = offsets + (int64_t)e * P3;
   for (int t = threadIdx.x; t < P3 * 5; t += NT) {
     const int p = t / 5, c = t % 5;
     const int64_t o = __ldg(off + p) + c;
 #pragma unroll
-    for (int v = 0; v < NV; v++) sN[(v * 5 + c) * P3 + p] = T(l_in[v][o]);
+    for (int v = 0; v < NV; v++) {
+      if (sizeof(T) == 8) cp_async8(&sN[(v * 5 + c) * P3 + p], l_in[v] + o);
+      else cp_async4(&sN[(v * 5 + c) * P3 + p], l_in[v] + o);
+    }
   }
+}
+
+// Gather the output L-vector at element e's nodes, node-major sV [P3][5] (the layout of the scatter).
+template <int P, int NT, typename T>
+__device__ __forceinline__ void gather_out_async(const int32_t *__restrict__ offsets, int e, const T *l_out, T *sV) {
+  constexpr int P3 = P * P * P;
+  const int32_t *off = offsets + (int64_t)e * P3;
+  for (int t = threadIdx.x; t < P3 * 5; t += NT) {
+    const int64_t o = __ldg(off + t / 5) + t % 5;
+    if (sizeof(T) == 8) cp_async8(&sV[t], l_out + o);
+    else cp_async4(&sV[t], l_out + o);
+  }
+}
+
+// Forward passes after the gather: sN -> (x) s1 -> (y) s2 -> (z) interp sU [NV*5][Q3] and, for the first vector, the
+// z derivative; then x/y derivatives.  `after_x` runs once sN is consumed (issues the next element's gather).
+template <int P, int Q, int NV, int NT, typename T, typename AfterX>
+__device__ __forceinline__ void forward_passes(const Basis1D<T> &bas, const T *sN, T *s1, T *s2, T *sU, T *sG, AfterX after_x) {
+  constexpr int Q2 = Q * Q, Q3 = Q2 * Q;
+  constexpr int NC = NV * 5;
+  pass0<NC * P * P, P, Q, false, NT>(sN, s1, bas.B, P);
   __syncthreads();
-  pass0<NC * P * P, P, Q, false, NT>(sN, s1, a.basis.B, P);
+  after_x();
+  pass1<NC, P, Q, P, Q, false, NT>(s1, s2, bas.B, P);
   __syncthreads();
-  pass1<NC, P, Q, P, Q, false, NT>(s1, s2, a.basis.B, P);
-  __syncthreads();
-  // z pass: interpolate along z and, for the first vector, differentiate along z on the quadrature grid
   for (int f = threadIdx.x; f < NC * Q2; f += NT) {
     const int yx = f % Q2, c = f / Q2;
     T in[P], val[Q];
@@ -171,7 +179,7 @@ __device__ __forceinline__ void forward(const ElemArgs<T> &a, int e, const TL *c
     for (int k = 0; k < Q; k++) {
       T s = 0;
 #pragma unroll
-      for (int cz = 0; cz < P; cz++) s += a.basis.B[k * P + cz] * in[cz];
+      for (int cz = 0; cz < P; cz++) s += bas.B[k * P + cz] * in[cz];
       val[k] = s;
       sU[c * Q3 + k * Q2 + yx] = s;
     }
@@ -180,28 +188,18 @@ __device__ __forceinline__ void forward(const ElemArgs<T> &a, int e, const TL *c
       for (int k = 0; k < Q; k++) {
         T s = 0;
 #pragma unroll
-        for (int l = 0; l < Q; l++) s += a.basis.D[k * Q + l] * val[l];
+        for (int l = 0; l < Q; l++) s += bas.D[k * Q + l] * val[l];
         sG[(2 * 5 + c) * Q3 + k * Q2 + yx] = s;
       }
     }
   }
   __syncthreads();
-  // x and y derivatives of the first vector on the quadrature grid
   for (int f = threadIdx.x; f < 2 * 5 * Q2; f += NT) {
     const int dir = f / (5 * Q2), r = f % (5 * Q2), c = r / Q2, rem = r % Q2;
-    const T *src;
-    T *dst;
-    int stride;
-    if (dir == 0) {  // fibre along x at (k,j) = rem
-      src = sU + c * Q3 + rem * Q;
-      dst = sG + (0 * 5 + c) * Q3 + rem * Q;
-      stride = 1;
-    } else {  // fibre along y at (k, i): rem = k*Q + i
-      const int k = rem / Q, i = rem % Q;
-      src = sU + c * Q3 + k * Q2 + i;
-      dst = sG + (1 * 5 + c) * Q3 + k * Q2 + i;
-      stride = Q;
-    }
+    const int base = dir == 0 ? rem * Q : (rem / Q) * Q2 + (rem % Q);
+    const int stride = dir == 0 ? 1 : Q;
+    const T *src = sU + c * Q3 + base;
+    T *dst = sG + (dir * 5 + c) * Q3 + base;
     T val[Q];
 #pragma unroll
     for (int l = 0; l < Q; l++) val[l] = src[l * stride];
@@ -209,29 +207,23 @@ __device__ __forceinline__ void forward(const ElemArgs<T> &a, int e, const TL *c
     for (int k = 0; k < Q; k++) {
       T s = 0;
 #pragma unroll
-      for (int l = 0; l < Q; l++) s += a.basis.D[k * Q + l] * val[l];
+      for (int l = 0; l < Q; l++) s += bas.D[k * Q + l] * val[l];
       dst[k * stride] = s;
     }
   }
   __syncthreads();
 }
 
-// Transpose: v [5][Q3] (in sU) and grad_v [3][5][Q3] (in sG) back to the element nodes, then scatter-add into l_out.
-// Scratch: sW1 [5][Q3], sW2 [5][Q3], sT2 [5][P][Q][Q], sT1 [5][P][P][Q], sF [P3][5].
-template <int P, int Q, int NT, typename T, typename TL>
-__device__ __forceinline__ void transpose_scatter(const ElemArgs<T> &a, int e, TL *l_out, const T *sU, const T *sG, T *sW1, T *sW2, T *sT2, T *sT1,
-                                                  T *sF) {
-  constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
+// Transpose of the point values v [5][Q3] (sU) and reference-direction fluxes [3][5][Q3] (sG) back to the element
+// nodes, node-major sF [P3][5].  Scratch: sW1 [5][Q3], sW2 [5][Q3], sT2 [5][P][Q][Q], sT1 [5][P][P][Q]; sT1 may alias
+// sG (free once the z pass is done), sF may alias sW2.
+template <int P, int Q, int NT, typename T>
+__device__ __forceinline__ void transpose_passes(const Basis1D<T> &bas, const T *sU, const T *sG, T *sW1, T *sW2, T *sT2, T *sT1, T *sF) {
+  constexpr int Q2 = Q * Q, Q3 = Q2 * Q;
   for (int f = threadIdx.x; f < 2 * 5 * Q2; f += NT) {
     const int dir = f / (5 * Q2), r = f % (5 * Q2), c = r / Q2, rem = r % Q2;
-    int base, stride;
-    if (dir == 0) {
-      base = rem * Q;
-      stride = 1;
-    } else {
-      base = (rem / Q) * Q2 + (rem % Q);
-      stride = Q;
-    }
+    const int base = dir == 0 ? rem * Q : (rem / Q) * Q2 + (rem % Q);
+    const int stride = dir == 0 ? 1 : Q;
     const T *g = sG + (dir * 5 + c) * Q3 + base;
     T gv[Q];
 #pragma unroll
@@ -243,7 +235,7 @@ __device__ __forceinline__ void transpose_scatter(const ElemArgs<T> &a, int e, T
       for (int i = 0; i < Q; i++) {
         T s = v[i];
 #pragma unroll
-        for (int l = 0; l < Q; l++) s += a.basis.D[l * Q + i] * gv[l];
+        for (int l = 0; l < Q; l++) s += bas.D[l * Q + i] * gv[l];
         w[i] = s;
       }
     } else {
@@ -252,7 +244,7 @@ __device__ __forceinline__ void transpose_scatter(const ElemArgs<T> &a, int e, T
       for (int j = 0; j < Q; j++) {
         T s = 0;
 #pragma unroll
-        for (int l = 0; l < Q; l++) s += a.basis.D[l * Q + j] * gv[l];
+        for (int l = 0; l < Q; l++) s += bas.D[l * Q + j] * gv[l];
         w[j * Q] = s;
       }
     }
@@ -267,21 +259,20 @@ __device__ __forceinline__ void transpose_scatter(const ElemArgs<T> &a, int e, T
     for (int k = 0; k < Q; k++) {
       T s = sW1[c * Q3 + k * Q2 + yx] + sW2[c * Q3 + k * Q2 + yx];
 #pragma unroll
-      for (int l = 0; l < Q; l++) s += a.basis.D[l * Q + k] * gz[l];
+      for (int l = 0; l < Q; l++) s += bas.D[l * Q + k] * gz[l];
       w[k] = s;
     }
 #pragma unroll
     for (int cz = 0; cz < P; cz++) {
       T s = 0;
 #pragma unroll
-      for (int k = 0; k < Q; k++) s += a.basis.B[k * P + cz] * w[k];
+      for (int k = 0; k < Q; k++) s += bas.B[k * P + cz] * w[k];
       sT2[(c * P + cz) * Q2 + yx] = s;
     }
   }
   __syncthreads();
-  pass1<5, P, Q, Q, P, true, NT>(sT2, sT1, a.basis.B, P);
+  pass1<5, P, Q, Q, P, true, NT>(sT2, sT1, bas.B, P);
   __syncthreads();
-  // x pass writes node-major [p][c] for a coalesced scatter
   for (int f = threadIdx.x; f < 5 * P * P; f += NT) {
     const int c = f / (P * P), zb = f % (P * P);
     T in[Q];
@@ -291,29 +282,51 @@ __device__ __forceinline__ void transpose_scatter(const ElemArgs<T> &a, int e, T
     for (int pa = 0; pa < P; pa++) {
       T s = 0;
 #pragma unroll
-      for (int i = 0; i < Q; i++) s += a.basis.B[i * P + pa] * in[i];
+      for (int i = 0; i < Q; i++) s += bas.B[i * P + pa] * in[i];
       sF[(zb * P + pa) * 5 + c] = s;
     }
   }
   __syncthreads();
-  const int32_t *off = a.offsets + (int64_t)e * P3;
+}
+
+// out[o] = old + contribution; elements of one colour share no node, so `old` (gathered ahead) is current.
+template <int P, int NT, typename T>
+__device__ __forceinline__ void scatter_store(const int32_t *__restrict__ offsets, int e, const T *sV, const T *sF, T *l_out) {
+  constexpr int P3 = P * P * P;
+  const int32_t *off = offsets + (int64_t)e * P3;
   for (int t = threadIdx.x; t < P3 * 5; t += NT) {
-    const int p = t / 5, c = t % 5;
-    const int64_t o = __ldg(off + p) + c;
-    l_out[o] += TL(sF[t]);
+    const int64_t o = __ldg(off + t / 5) + t % 5;
+    l_out[o] = sV[t] + sF[t];
   }
 }
 
-template <int P, int Q>
-struct SmemLayout {
+// Shared-memory plan (in units of T unless noted):
+//   sN  [NV*5][P3]      staged node values of the element being computed / the next one
+//   sV  [P3][5]         staged output values at the element's nodes
+//   s1  [NV*5][P][P][Q] x-pass output; later sT2 (transpose scratch)
+//   s2  [NV*5][P][Q][Q] y-pass output; later w2 and the final node values
+//   sU  [10][Q3]        interpolated values (q, then q_dot or w1); point-wise outputs v in place
+//   sG  [15][Q3]        reference gradients; point-wise fluxes in place; later sT1
+//   sJD [15][Q3]        staged stored Jacobian data (IJacobian only)
+//   sQD [10][Q3] double staged qdata
+template <int P, int Q, int NV, typename T, bool JD>
+struct Plan {
   static constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
-  // forward buffers for up to two input vectors
-  static constexpr int nN = 10 * P3, n1 = 10 * P * P * Q, n2 = 10 * P * Q2;
-  static constexpr int nU = 10 * Q3, nG = 15 * Q3;
-  static constexpr int total = nN + n1 + n2 + nU + nG;
-  static_assert(5 * P * Q2 <= nN, "sT2 fits in sN");
-  static_assert(5 * P * P * Q <= n1, "sT1 fits in s1");
-  static_assert(5 * Q3 <= n2 || 5 * Q3 <= nN + n1, "w2 fits");
+  static constexpr int cmax(int x, int y) { return x > y ? x : y; }
+  static constexpr int nN = NV * 5 * P3, nV = 5 * P3, nU = 10 * Q3, nG = 15 * Q3;
+  static constexpr int n1 = cmax(NV * 5 * P * P * Q, 5 * P * Q2);          // x-pass output, then sT2
+  static constexpr int n2 = cmax(cmax(NV * 5 * P * Q2, 5 * Q3), 5 * P3);   // y-pass output, then w2 and node values
+  static constexpr int nJD = JD ? 15 * Q3 : 0;
+  static constexpr int kAl = 16 / (int)sizeof(T);
+  static constexpr int pad(int n) { return (n + kAl - 1) / kAl * kAl; }  // every buffer 16-byte aligned (bulk copies)
+  static constexpr int oN = 0, oV = pad(oN + nN), o1 = pad(oV + nV), o2 = pad(o1 + n1), oU = pad(o2 + n2), oG = pad(oU + nU),
+                       oJD = pad(oG + nG), end_T = pad(oJD + nJD);
+  static constexpr size_t qd_offset_bytes = ((size_t)end_T * sizeof(T) + 15) & ~(size_t)15;
+  static constexpr size_t bytes = qd_offset_bytes + sizeof(double) * 10 * Q3 + 16;  // + mbarrier
+  static_assert(5 * P * Q2 <= n1, "sT2 fits in s1");
+  static_assert(5 * Q3 <= n2, "w2 fits in s2");
+  static_assert(5 * P3 <= n2, "final node values fit in s2");
+  static_assert(5 * P * P * Q <= nG, "sT1 fits in sG");
 };
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -325,64 +338,117 @@ struct IfunctionPtrs {
   float *jac_f32;     // [E][num_jd][Q3] single-precision shadow for the mixed-precision Jacobian, may be null
   double *v;
   QRef qref;
+  int qdata_tma;      // qdata blocks can be bulk-copied (16-byte aligned base)
 };
 
 template <int P, int Q>
-__global__ void __launch_bounds__(nthreads_for<double>(Q), 3) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p) {
+__global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p) {
   constexpr int NT = nthreads_for<double>(Q);
-  using L = SmemLayout<P, Q>;
-  extern __shared__ __align__(16) double smem[];
-  double *sN = smem, *s1 = sN + L::nN, *s2 = s1 + L::n1, *sU = s2 + L::n2, *sG = sU + L::nU;
-  double *sD = sU + 5 * L::Q3;  // interp of q_dot
+  using L = Plan<P, Q, 2, double, false>;
+  constexpr int Q3 = L::Q3;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sm = reinterpret_cast<double *>(smem_raw);
+  double *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
+  double *sD = sU + 5 * Q3;
+  double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + sizeof(double) * 10 * Q3);
+  __shared__ int s_bail;
   const double *lin[2] = {p.q, p.q_dot};
-  const double *pre[3] = {p.q, p.q_dot, p.v};
-  for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
+  const unsigned qd_bytes = sizeof(double) * 10 * Q3;
+
+  if (threadIdx.x == 0) {
+    mbar_init(mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_bail = 0;
+  }
+  __syncthreads();
+  int idx = blockIdx.x;
+  if (idx >= a.n_elems) return;
+  // prologue: stage the first element
+  {
+    const int e0 = a.elems[idx];
+    gather_async<P, 2, NT, double, double>(a.offsets, e0, lin, sN);
+    gather_out_async<P, NT, double>(a.offsets, e0, p.v, sV);
+    cp_async_commit();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
+    stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+    cp_async_commit();
+  }
+  unsigned phase = 0;
+  for (; idx < a.n_elems; idx += gridDim.x) {
     const int e = a.elems[idx];
-    if (idx == blockIdx.x)
-      prefetch_element<P, double>(a.offsets, e, pre, 3, a.qdata + (int64_t)e * 10 * L::Q3, sizeof(double) * 10 * L::Q3, nullptr, 0);
-    if (idx + gridDim.x < a.n_elems) {
-      const int en = a.elems[idx + gridDim.x];
-      prefetch_element<P, double>(a.offsets, en, pre, 3, a.qdata + (int64_t)en * 10 * L::Q3, sizeof(double) * 10 * L::Q3, nullptr, 0);
+    const int nidx = idx + gridDim.x;
+    const int en = nidx < a.n_elems ? a.elems[nidx] : -1;
+    cp_async_wait_all();
+    if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
+      s_bail = 1;
+      atomicOr(a.status, 1);
     }
-    forward<P, Q, 2, NT, double, double>(a, e, lin, sN, s1, s2, sU, sG);
+    __syncthreads();
+    if (s_bail) break;
+    phase ^= 1;
+    if (en >= 0 && threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, qd_bytes);
+    forward_passes<P, Q, 2, NT, double>(a.basis, sN, s1, s2, sU, sG, [&]() {
+      if (en >= 0) {
+        gather_async<P, 2, NT, double, double>(a.offsets, en, lin, sN);
+        cp_async_commit();
+      }
+    });
     const int q = threadIdx.x;
-    if (q < L::Q3) {
+    if (q < Q3) {
       double qi[5], qd[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5], jd[15];
 #pragma unroll
       for (int c = 0; c < 5; c++) {
-        qi[c] = sU[c * L::Q3 + q];
-        qd[c] = sD[c * L::Q3 + q];
+        qi[c] = sU[c * Q3 + q];
+        qd[c] = sD[c * Q3 + q];
 #pragma unroll
-        for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * L::Q3 + q];
+        for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
-      load_qdata(a.qdata + (int64_t)e * 10 * L::Q3, L::Q3, q, wdetJ, X);
+      wdetJ = sQD[q];
+#pragma unroll
+      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = sQD[(1 + k) * Q3 + q];
       double x0 = 0;
       if (a.pc.idl_enable) x0 = qpt_x0<Q>(a.x_elem + (int64_t)e * 24, p.qref.x, q % Q, (q / Q) % Q, q / (Q * Q));
       ifunction_point<double>(a.pc, qi, gref, qd, wdetJ, X, x0, v, gv, jd);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
-        sU[c * L::Q3 + q] = v[c];
+        sU[c * Q3 + q] = v[c];
 #pragma unroll
-        for (int d = 0; d < 3; d++) sG[(d * 5 + c) * L::Q3 + q] = gv[d][c];
+        for (int d = 0; d < 3; d++) sG[(d * 5 + c) * Q3 + q] = gv[d][c];
       }
       if (p.jac_data) {
-        double *jdp = p.jac_data + (int64_t)e * a.num_jd * L::Q3 + q;
+        double *jdp = p.jac_data + (int64_t)e * a.num_jd * Q3 + q;
 #pragma unroll
-        for (int c = 0; c < 14; c++) jdp[c * L::Q3] = jd[c];
-        if (a.num_jd > 14) jdp[14 * L::Q3] = jd[14];
+        for (int c = 0; c < 14; c++) jdp[c * Q3] = jd[c];
+        if (a.num_jd > 14) jdp[14 * Q3] = jd[14];
       }
       if (p.jac_f32) {
-        float *jdp = p.jac_f32 + (int64_t)e * a.num_jd * L::Q3 + q;
+        float *jdp = p.jac_f32 + (int64_t)e * a.num_jd * Q3 + q;
 #pragma unroll
-        for (int c = 0; c < 14; c++) jdp[c * L::Q3] = float(jd[c]);
-        if (a.num_jd > 14) jdp[14 * L::Q3] = float(jd[14]);
+        for (int c = 0; c < 14; c++) jdp[c * Q3] = float(jd[c]);
+        if (a.num_jd > 14) jdp[14 * Q3] = float(jd[14]);
       }
     }
     __syncthreads();
-    // transpose scratch: w1 in the q_dot interp slot, w2 in s2, sT2 in sN, sT1 in s1, final node values in s2
-    transpose_scatter<P, Q, NT, double, double>(a, e, p.v, sU, sG, sD, s2, sN, s1, s2);
+    if (en >= 0) {  // sQD consumed: stage the next element's qdata
+      if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
+      }
+      stage_block<double, NT>(sQD, a.qdata + (int64_t)en * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+      cp_async_commit();
+    }
+    // transpose scratch: w1 in the q_dot slot, w2 and the node values in s2, sT2 in s1, sT1 in sG
+    transpose_passes<P, Q, NT, double>(a.basis, sU, sG, sD, s2, s1, sG, s2);
+    scatter_store<P, NT, double>(a.offsets, e, sV, s2, p.v);
     __syncthreads();
+    if (en >= 0) {
+      gather_out_async<P, NT, double>(a.offsets, en, p.v, sV);
+      cp_async_commit();
+    }
   }
+  cp_async_wait_all();
+  if (s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);  // let an outstanding bulk copy land before exit
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -393,56 +459,111 @@ struct IjacobianPtrs {
   const T *dq;
   const T *jac_data;  // [E][num_jd][Q3]
   T *v;
+  int qdata_tma, jd_tma;
 };
 
 template <int P, int Q, typename T>
-__global__ void __launch_bounds__(nthreads_for<T>(Q), 3) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
+__global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
   constexpr int NT = nthreads_for<T>(Q);
-  using L = SmemLayout<P, Q>;
+  using L = Plan<P, Q, 1, T, true>;
+  constexpr int Q3 = L::Q3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *smem = reinterpret_cast<T *>(smem_raw);
-  T *sN = smem, *s1 = sN + L::nN, *s2 = s1 + L::n1, *sU = s2 + L::n2, *sG = sU + L::nU;
-  T *sW1 = sU + 5 * L::Q3;
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  T *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG, *sJD = sm + L::oJD;
+  T *sW1 = sU + 5 * Q3;
+  double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + sizeof(double) * 10 * Q3);
+  __shared__ int s_bail;
   const T *lin[1] = {p.dq};
-  const T *pre[2] = {p.dq, p.v};
-  const size_t jbytes = sizeof(T) * (size_t)a.num_jd * L::Q3;
-  for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
+  const unsigned qd_bytes = sizeof(double) * 10 * Q3;
+  const int njd = a.num_jd;
+  const unsigned jd_bytes = (unsigned)(sizeof(T) * njd * Q3);
+  const unsigned tx = (p.qdata_tma ? qd_bytes : 0) + (p.jd_tma ? jd_bytes : 0);
+
+  if (threadIdx.x == 0) {
+    mbar_init(mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_bail = 0;
+  }
+  __syncthreads();
+  int idx = blockIdx.x;
+  if (idx >= a.n_elems) return;
+  {
+    const int e0 = a.elems[idx];
+    gather_async<P, 1, NT, T, T>(a.offsets, e0, lin, sN);
+    gather_out_async<P, NT, T>(a.offsets, e0, p.v, sV);
+    cp_async_commit();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, tx);
+    stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+    stage_block<T, NT>(sJD, p.jac_data + (int64_t)e0 * njd * Q3, njd * Q3, p.jd_tma, mbar);
+    cp_async_commit();
+  }
+  unsigned phase = 0;
+  for (; idx < a.n_elems; idx += gridDim.x) {
     const int e = a.elems[idx];
-    if (idx == blockIdx.x)
-      prefetch_element<P, T>(a.offsets, e, pre, 2, a.qdata + (int64_t)e * 10 * L::Q3, sizeof(double) * 10 * L::Q3,
-                             p.jac_data + (int64_t)e * a.num_jd * L::Q3, jbytes);
-    if (idx + gridDim.x < a.n_elems) {
-      const int en = a.elems[idx + gridDim.x];
-      prefetch_element<P, T>(a.offsets, en, pre, 2, a.qdata + (int64_t)en * 10 * L::Q3, sizeof(double) * 10 * L::Q3,
-                             p.jac_data + (int64_t)en * a.num_jd * L::Q3, jbytes);
+    const int nidx = idx + gridDim.x;
+    const int en = nidx < a.n_elems ? a.elems[nidx] : -1;
+    cp_async_wait_all();
+    if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
+      s_bail = 1;
+      atomicOr(a.status, 1);
     }
-    forward<P, Q, 1, NT, T, T>(a, e, lin, sN, s1, s2, sU, sG);
+    __syncthreads();
+    if (s_bail) break;
+    phase ^= 1;
+    if (en >= 0 && threadIdx.x == 0) {
+      prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, qd_bytes);
+      prefetch_l2_bulk(p.jac_data + (int64_t)en * njd * Q3, jd_bytes);
+    }
+    forward_passes<P, Q, 1, NT, T>(a.basis, sN, s1, s2, sU, sG, [&]() {
+      if (en >= 0) {
+        gather_async<P, 1, NT, T, T>(a.offsets, en, lin, sN);
+        cp_async_commit();
+      }
+    });
     const int q = threadIdx.x;
-    if (q < L::Q3) {
+    if (q < Q3) {
       T dq[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5], jd[15];
 #pragma unroll
       for (int c = 0; c < 5; c++) {
-        dq[c] = sU[c * L::Q3 + q];
+        dq[c] = sU[c * Q3 + q];
 #pragma unroll
-        for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * L::Q3 + q];
+        for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
-      const T *jdp = p.jac_data + (int64_t)e * a.num_jd * L::Q3 + q;
 #pragma unroll
-      for (int c = 0; c < 14; c++) jd[c] = jdp[c * L::Q3];
-      jd[14] = a.num_jd > 14 ? jdp[14 * L::Q3] : T(0);
-      load_qdata(a.qdata + (int64_t)e * 10 * L::Q3, L::Q3, q, wdetJ, X);
+      for (int c = 0; c < 14; c++) jd[c] = sJD[c * Q3 + q];
+      jd[14] = njd > 14 ? sJD[14 * Q3 + q] : T(0);
+      wdetJ = T(sQD[q]);
+#pragma unroll
+      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = T(sQD[(1 + k) * Q3 + q]);
       ijacobian_point<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
-        sU[c * L::Q3 + q] = v[c];
+        sU[c * Q3 + q] = v[c];
 #pragma unroll
-        for (int d = 0; d < 3; d++) sG[(d * 5 + c) * L::Q3 + q] = gv[d][c];
+        for (int d = 0; d < 3; d++) sG[(d * 5 + c) * Q3 + q] = gv[d][c];
       }
     }
     __syncthreads();
-    transpose_scatter<P, Q, NT, T, T>(a, e, p.v, sU, sG, sW1, s2, sN, s1, s2);
+    if (en >= 0) {
+      if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(mbar, tx);
+      }
+      stage_block<double, NT>(sQD, a.qdata + (int64_t)en * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+      stage_block<T, NT>(sJD, p.jac_data + (int64_t)en * njd * Q3, njd * Q3, p.jd_tma, mbar);
+      cp_async_commit();
+    }
+    transpose_passes<P, Q, NT, T>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
+    scatter_store<P, NT, T>(a.offsets, e, sV, s2, p.v);
     __syncthreads();
+    if (en >= 0) {
+      gather_out_async<P, NT, T>(a.offsets, en, p.v, sV);
+      cp_async_commit();
+    }
   }
+  cp_async_wait_all();
+  if (s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -649,11 +770,15 @@ static ElemArgs<T> make_args(const HbElemOp *op, const HbNewtonianContext &ctx, 
   a.qdata = qdata;
   a.x_elem = op->d_x_elem;
   a.num_jd = ctx.idl_enable ? 15 : 14;
+  a.status = op->d_status;
   return a;
 }
 
-static int grid_for(const HbElemOp *op, int n_elems, int ctas_per_sm) {
-  const int g = op->num_sms * ctas_per_sm;
+template <typename K>
+static int grid_for(const HbElemOp *op, int n_elems, K kernel, int nthreads, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nthreads, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  const int g = op->num_sms * per_sm;
   return n_elems < g ? n_elems : g;
 }
 
@@ -665,7 +790,8 @@ static size_t smem_bytes(int P, int Q) {
 
 template <int P, int Q>
 static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
-  const size_t sm = smem_bytes<double>(P, Q);
+  using L = Plan<P, Q, 2, double, false>;
+  const size_t sm = L::bytes;
   cudaFuncSetAttribute(k_ifunction<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   IfunctionPtrs p;
   p.q = io->q;
@@ -674,10 +800,11 @@ static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, c
   p.jac_f32 = io->jac_data_f32;
   p.v = io->v;
   for (int i = 0; i < kMaxP; i++) p.qref.x[i] = i < Q ? op->qref1d[i] : 0;
+  p.qdata_tma = ((uintptr_t)io->qdata % 16) == 0;
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<double> a = make_args<double>(op, ctx, io->qdata, c);
     if (a.n_elems == 0) continue;
-    k_ifunction<P, Q><<<grid_for(op, a.n_elems, 3), nthreads_for<double>(Q), sm, s>>>(a, p);
+    k_ifunction<P, Q><<<grid_for(op, a.n_elems, k_ifunction<P, Q>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
@@ -685,13 +812,20 @@ static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, c
 template <int P, int Q, typename T>
 static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v,
                             cudaStream_t s) {
-  const size_t sm = smem_bytes<T>(P, Q);
+  using L = Plan<P, Q, 1, T, true>;
+  const size_t sm = L::bytes;
   cudaFuncSetAttribute(k_ijacobian<P, Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  IjacobianPtrs<T> p{dq, jd, v};
+  IjacobianPtrs<T> p;
+  p.dq = dq;
+  p.jac_data = jd;
+  p.v = v;
+  const int njd = ctx.idl_enable ? 15 : 14;
+  p.qdata_tma = ((uintptr_t)qdata % 16) == 0;
+  p.jd_tma = ((uintptr_t)jd % 16) == 0 && (sizeof(T) * njd * L::Q3) % 16 == 0;
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
-    k_ijacobian<P, Q, T><<<grid_for(op, a.n_elems, 3), nthreads_for<T>(Q), sm, s>>>(a, p);
+    k_ijacobian<P, Q, T><<<grid_for(op, a.n_elems, k_ijacobian<P, Q, T>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
@@ -709,14 +843,14 @@ static int launch_diagonal(const HbElemOp *op, const HbNewtonianContext &ctx, co
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
-    k_diagonal<P, Q, T><<<grid_for(op, a.n_elems, 2), nthreads_for<T>(Q), sm, s>>>(a, p);
+    k_diagonal<P, Q, T><<<grid_for(op, a.n_elems, k_diagonal<P, Q, T>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
 // (P, Q) pairs compiled: polynomial degree 1..5 with q_extra 0 or 1 (Q = P or P + 1); the benchmark configurations use
-// (3,3), (4,5) and (5,6).  P=2 with Q=3 is left out because its transpose scratch would not fit the forward buffers.
-#define HB_PQ_LIST(X) X(2, 2) X(3, 3) X(3, 4) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7)
+// (3,3), (4,5) and (5,6).
+#define HB_PQ_LIST(X) X(2, 2) X(2, 3) X(3, 3) X(3, 4) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7)
 
 }  // namespace hb
 

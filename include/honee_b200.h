@@ -58,6 +58,7 @@ typedef struct HbElemOp {
   double        *d_x_elem;      /* device [num_elem][3][8] vertex coordinates (only needed with the IDL), may be NULL */
   int            num_sms;
   int            device;
+  int           *d_status;      /* device error word written by the kernels (bit 0: a bounded wait gave up) */
 } HbElemOp;
 
 /* Build the device description from host arrays.  Validates every offset against l_size (bounds are checked on the
@@ -67,6 +68,9 @@ HB_EXPORT int hb_elemop_create(int num_elem, int P, int Q, const int32_t *offset
 /* Attach trilinear vertex coordinates [num_elem][3][8] (host pointer) used by the internal damping layer. */
 HB_EXPORT int hb_elemop_set_vertex_coords(HbElemOp *op, const double *x_elem);
 HB_EXPORT int hb_elemop_destroy(HbElemOp *op);
+/* Read (synchronising the device) and optionally clear the kernels' error word.  The fused kernels never trap: a wait
+ * that gives up records bit 0 here and the kernel returns early, leaving its output incomplete. */
+HB_EXPORT int hb_elemop_status(HbElemOp *op, int *status, int clear);
 
 /* Inputs/outputs of one IFunction apply (device pointers). */
 typedef struct {
