@@ -101,19 +101,14 @@ __device__ __forceinline__ void load_qdata(const double *__restrict__ qd, int Q3
   for (int k = 0; k < 9; k++) X[k / 3][k % 3] = T(__ldg(qd + (1 + k) * Q3 + q));
 }
 
-// x coordinate of quadrature point (i,j,k) from the element's vertex coordinates (trilinear coordinate field).
+// x coordinate of quadrature point (i,j,k) from the element's vertex coordinates (trilinear coordinate field); scalar
+// code only, so nothing is placed in local memory.
 template <int Q>
 __device__ __forceinline__ double qpt_x0(const double *__restrict__ xe, const double *qref, int i, int j, int k) {
-  const double xi[3] = {qref[i], qref[j], qref[k]};
-  double s = 0;
-#pragma unroll
-  for (int v = 0; v < 8; v++) {
-    double w = 1;
-#pragma unroll
-    for (int d = 0; d < 3; d++) w *= ((v >> d) & 1) ? 0.5 * (1 + xi[d]) : 0.5 * (1 - xi[d]);
-    s += w * __ldg(xe + v);
-  }
-  return s;
+  const double lx = 0.5 * (1 - qref[i]), hx = 0.5 * (1 + qref[i]), ly = 0.5 * (1 - qref[j]), hy = 0.5 * (1 + qref[j]);
+  const double lz = 0.5 * (1 - qref[k]), hz = 0.5 * (1 + qref[k]);
+  return lz * (ly * (lx * __ldg(xe + 0) + hx * __ldg(xe + 1)) + hy * (lx * __ldg(xe + 2) + hx * __ldg(xe + 3))) +
+         hz * (ly * (lx * __ldg(xe + 4) + hx * __ldg(xe + 5)) + hy * (lx * __ldg(xe + 6) + hx * __ldg(xe + 7)));
 }
 
 struct QRef {
@@ -130,44 +125,88 @@ struct QRef {
 // so each element starts with all its inputs resident.  Elements of one colour share no node, so the output values
 // gathered ahead are still current when the element scatters (a plain store of old + contribution, no atomics).
 
-// Gather NV L-vectors (5 interleaved comps each) at element e's nodes into comp-major sN [NV*5][P3].
-template <int P, int NV, int NT, typename T, typename TL>
-__device__ __forceinline__ void gather_async(const int32_t *__restrict__ offsets, int e, const TL *const *l_in, T *sN) {
-  constexpr int P3 = P * P * P;
-  static_assert(sizeof(T) == sizeof(TL), "staged copies keep the L-vector precision");
-  const int32_t *off = offsets + (int64_t)e * P3;
-  for (int t = threadIdx.x; t < P3 * 5; t += NT) {
-    const int p = t / 5, c = t % 5;
-    const int64_t o = __ldg(off + p) + c;
+// Offsets of the entries a thread handles in a 5-component node gather/scatter: entries t = threadIdx.x + j*NT
+// (node t/5, component t%5).  They are loaded into registers one element ahead (so no gather waits on them) and kept in
+// shared memory for the scatter and the output gather, so they are not live across the point-wise phase.  L-vector
+// indices fit in int32 (checked on the host).
+template <int P, int NT>
+struct EntryOffsets {
+  static constexpr int P3 = P * P * P, NJ = (5 * P3 + NT - 1) / NT;
+  int32_t o[NJ];
+  __device__ __forceinline__ void load(const int32_t *__restrict__ offsets, int e) {
+    const int32_t *off = offsets + (int64_t)e * P3;
 #pragma unroll
-    for (int v = 0; v < NV; v++) {
-      if (sizeof(T) == 8) cp_async8(&sN[(v * 5 + c) * P3 + p], l_in[v] + o);
-      else cp_async4(&sN[(v * 5 + c) * P3 + p], l_in[v] + o);
+    for (int j = 0; j < NJ; j++) {
+      const int t = threadIdx.x + j * NT;
+      o[j] = t < 5 * P3 ? __ldg(off + t / 5) + t % 5 : 0;
+    }
+  }
+  __device__ __forceinline__ void store(int32_t *sO) const {
+#pragma unroll
+    for (int j = 0; j < NJ; j++) {
+      const int t = threadIdx.x + j * NT;
+      if (t < 5 * P3) sO[t] = o[j];
+    }
+  }
+};
+
+// Row stride of the staged node values: P rounded up to an odd number so the x pass reads without bank conflicts.
+template <int P>
+__host__ __device__ constexpr int padded_row() { return P | 1; }
+
+// Gather NV L-vectors at one element's nodes into comp-major sN [NV*5][P][P][PX] (x rows padded to PX).
+template <int P, int NV, int NT, typename T>
+__device__ __forceinline__ void gather_async(const EntryOffsets<P, NT> &eo, const T *l0, const T *l1, T *sN) {
+  constexpr int P3 = P * P * P, PX = padded_row<P>(), PS = P * P * PX;
+#pragma unroll
+  for (int j = 0; j < EntryOffsets<P, NT>::NJ; j++) {
+    const int t = threadIdx.x + j * NT;
+    if (t < 5 * P3) {
+      const int p = t / 5, c = t % 5, srow = (p / P) * PX + p % P;
+      if (sizeof(T) == 8) cp_async8(&sN[c * PS + srow], l0 + eo.o[j]);
+      else cp_async4(&sN[c * PS + srow], l0 + eo.o[j]);
+      if (NV > 1) {
+        if (sizeof(T) == 8) cp_async8(&sN[(5 + c) * PS + srow], l1 + eo.o[j]);
+        else cp_async4(&sN[(5 + c) * PS + srow], l1 + eo.o[j]);
+      }
     }
   }
 }
 
-// Gather the output L-vector at element e's nodes, node-major sV [P3][5] (the layout of the scatter).
+// Gather the output L-vector at one element's nodes, node-major sV [P3][5] (the layout of the scatter); sO holds the
+// element's entry offsets (EntryOffsets::store).
 template <int P, int NT, typename T>
-__device__ __forceinline__ void gather_out_async(const int32_t *__restrict__ offsets, int e, const T *l_out, T *sV) {
+__device__ __forceinline__ void gather_out_async(const int32_t *sO, const T *l_out, T *sV) {
   constexpr int P3 = P * P * P;
-  const int32_t *off = offsets + (int64_t)e * P3;
-  for (int t = threadIdx.x; t < P3 * 5; t += NT) {
-    const int64_t o = __ldg(off + t / 5) + t % 5;
-    if (sizeof(T) == 8) cp_async8(&sV[t], l_out + o);
-    else cp_async4(&sV[t], l_out + o);
+  for (int t = threadIdx.x; t < 5 * P3; t += NT) {
+    if (sizeof(T) == 8) cp_async8(&sV[t], l_out + sO[t]);
+    else cp_async4(&sV[t], l_out + sO[t]);
   }
 }
 
-// Forward passes after the gather: sN -> (x) s1 -> (y) s2 -> (z) interp sU [NV*5][Q3] and, for the first vector, the
-// z derivative; then x/y derivatives.  `after_x` runs once sN is consumed (issues the next element's gather).
-template <int P, int Q, int NV, int NT, typename T, typename AfterX>
-__device__ __forceinline__ void forward_passes(const Basis1D<T> &bas, const T *sN, T *s1, T *s2, T *sU, T *sG, AfterX after_x) {
+// x pass from the padded staging rows: sN [NC][P*P][PX] -> s1 [NC][P*P][Q]
+template <int P, int Q, int NC, int NT, typename T>
+__device__ __forceinline__ void pass_x_staged(const Basis1D<T> &bas, const T *sN, T *s1) {
+  constexpr int PX = padded_row<P>();
+  for (int f = threadIdx.x; f < NC * P * P; f += NT) {
+    T x[P];
+#pragma unroll
+    for (int a = 0; a < P; a++) x[a] = sN[f * PX + a];
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+      T s = 0;
+#pragma unroll
+      for (int a = 0; a < P; a++) s += bas.B[i * P + a] * x[a];
+      s1[f * Q + i] = s;
+    }
+  }
+}
+
+// Forward passes after the x pass: s1 -> (y) s2 -> (z) interp sU [NC][Q3] and, for the first vector, the z
+// derivative; then x/y derivatives of the first vector on the quadrature grid.
+template <int P, int Q, int NC, int NT, typename T>
+__device__ __forceinline__ void forward_yz(const Basis1D<T> &bas, const T *s1, T *s2, T *sU, T *sG) {
   constexpr int Q2 = Q * Q, Q3 = Q2 * Q;
-  constexpr int NC = NV * 5;
-  pass0<NC * P * P, P, Q, false, NT>(sN, s1, bas.B, P);
-  __syncthreads();
-  after_x();
   pass1<NC, P, Q, P, Q, false, NT>(s1, s2, bas.B, P);
   __syncthreads();
   for (int f = threadIdx.x; f < NC * Q2; f += NT) {
@@ -291,17 +330,13 @@ __device__ __forceinline__ void transpose_passes(const Basis1D<T> &bas, const T 
 
 // out[o] = old + contribution; elements of one colour share no node, so `old` (gathered ahead) is current.
 template <int P, int NT, typename T>
-__device__ __forceinline__ void scatter_store(const int32_t *__restrict__ offsets, int e, const T *sV, const T *sF, T *l_out) {
+__device__ __forceinline__ void scatter_store(const int32_t *sO, const T *sV, const T *sF, T *l_out) {
   constexpr int P3 = P * P * P;
-  const int32_t *off = offsets + (int64_t)e * P3;
-  for (int t = threadIdx.x; t < P3 * 5; t += NT) {
-    const int64_t o = __ldg(off + t / 5) + t % 5;
-    l_out[o] = sV[t] + sF[t];
-  }
+  for (int t = threadIdx.x; t < 5 * P3; t += NT) l_out[sO[t]] = sV[t] + sF[t];
 }
 
 // Shared-memory plan (in units of T unless noted):
-//   sN  [NV*5][P3]      staged node values of the element being computed / the next one
+//   sN  [NV*5][P][P][PX] staged node values (x rows padded to odd PX) of the element being computed / the next one
 //   sV  [P3][5]         staged output values at the element's nodes
 //   s1  [NV*5][P][P][Q] x-pass output; later sT2 (transpose scratch)
 //   s2  [NV*5][P][Q][Q] y-pass output; later w2 and the final node values
@@ -313,7 +348,7 @@ template <int P, int Q, int NV, typename T, bool JD>
 struct Plan {
   static constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
   static constexpr int cmax(int x, int y) { return x > y ? x : y; }
-  static constexpr int nN = NV * 5 * P3, nV = 5 * P3, nU = 10 * Q3, nG = 15 * Q3;
+  static constexpr int nN = NV * 5 * P * P * padded_row<P>(), nV = 5 * P3, nU = 10 * Q3, nG = 15 * Q3;
   static constexpr int n1 = cmax(NV * 5 * P * P * Q, 5 * P * Q2);          // x-pass output, then sT2
   static constexpr int n2 = cmax(cmax(NV * 5 * P * Q2, 5 * Q3), 5 * P3);   // y-pass output, then w2 and node values
   static constexpr int nJD = JD ? 15 * Q3 : 0;
@@ -353,7 +388,8 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
   double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + sizeof(double) * 10 * Q3);
   __shared__ int s_bail;
-  const double *lin[2] = {p.q, p.q_dot};
+  __shared__ double s_qref[kMaxP];
+  __shared__ int32_t sO[2][5 * L::P3];  // entry offsets of the current / next element
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
 
   if (threadIdx.x == 0) {
@@ -361,15 +397,22 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_bail = 0;
   }
+  if (threadIdx.x == 0) {  // constant indices: indexing the parameter array with threadIdx would copy it to local memory
+#pragma unroll
+    for (int i = 0; i < kMaxP; i++) s_qref[i] = p.qref.x[i];
+  }
   __syncthreads();
   int idx = blockIdx.x;
   if (idx >= a.n_elems) return;
-  // prologue: stage the first element
-  {
+  int buf = 0;
+  {  // prologue: stage the first element
     const int e0 = a.elems[idx];
-    gather_async<P, 2, NT, double, double>(a.offsets, e0, lin, sN);
-    gather_out_async<P, NT, double>(a.offsets, e0, p.v, sV);
-    cp_async_commit();
+    EntryOffsets<P, NT> eo;
+    eo.load(a.offsets, e0);
+    eo.store(sO[0]);
+    gather_async<P, 2, NT, double>(eo, p.q, p.q_dot, sN);
+    __syncthreads();
+    gather_out_async<P, NT, double>(sO[0], p.v, sV);
     if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
     stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
     cp_async_commit();
@@ -379,6 +422,8 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
     const int e = a.elems[idx];
     const int nidx = idx + gridDim.x;
     const int en = nidx < a.n_elems ? a.elems[nidx] : -1;
+    EntryOffsets<P, NT> nxt;
+    if (en >= 0) nxt.load(a.offsets, en);
     cp_async_wait_all();
     if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
       s_bail = 1;
@@ -388,12 +433,14 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
     if (s_bail) break;
     phase ^= 1;
     if (en >= 0 && threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, qd_bytes);
-    forward_passes<P, Q, 2, NT, double>(a.basis, sN, s1, s2, sU, sG, [&]() {
-      if (en >= 0) {
-        gather_async<P, 2, NT, double, double>(a.offsets, en, lin, sN);
-        cp_async_commit();
-      }
-    });
+    pass_x_staged<P, Q, 10, NT, double>(a.basis, sN, s1);
+    __syncthreads();
+    if (en >= 0) {  // sN consumed: stage the next element's node values
+      gather_async<P, 2, NT, double>(nxt, p.q, p.q_dot, sN);
+      cp_async_commit();
+      nxt.store(sO[buf ^ 1]);
+    }
+    forward_yz<P, Q, 10, NT, double>(a.basis, s1, s2, sU, sG);
     const int q = threadIdx.x;
     if (q < Q3) {
       double qi[5], qd[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5], jd[15];
@@ -408,7 +455,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
 #pragma unroll
       for (int k = 0; k < 9; k++) X[k / 3][k % 3] = sQD[(1 + k) * Q3 + q];
       double x0 = 0;
-      if (a.pc.idl_enable) x0 = qpt_x0<Q>(a.x_elem + (int64_t)e * 24, p.qref.x, q % Q, (q / Q) % Q, q / (Q * Q));
+      if (a.pc.idl_enable) x0 = qpt_x0<Q>(a.x_elem + (int64_t)e * 24, s_qref, q % Q, (q / Q) % Q, q / (Q * Q));
       ifunction_point<double>(a.pc, qi, gref, qd, wdetJ, X, x0, v, gv, jd);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
@@ -440,10 +487,11 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
     }
     // transpose scratch: w1 in the q_dot slot, w2 and the node values in s2, sT2 in s1, sT1 in sG
     transpose_passes<P, Q, NT, double>(a.basis, sU, sG, sD, s2, s1, sG, s2);
-    scatter_store<P, NT, double>(a.offsets, e, sV, s2, p.v);
+    scatter_store<P, NT, double>(sO[buf], sV, s2, p.v);
     __syncthreads();
+    buf ^= 1;
     if (en >= 0) {
-      gather_out_async<P, NT, double>(a.offsets, en, p.v, sV);
+      gather_out_async<P, NT, double>(sO[buf], p.v, sV);
       cp_async_commit();
     }
   }
@@ -474,7 +522,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
   double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + sizeof(double) * 10 * Q3);
   __shared__ int s_bail;
-  const T *lin[1] = {p.dq};
+  __shared__ int32_t sO[2][5 * L::P3];  // entry offsets of the current / next element
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
   const int njd = a.num_jd;
   const unsigned jd_bytes = (unsigned)(sizeof(T) * njd * Q3);
@@ -488,11 +536,15 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
   __syncthreads();
   int idx = blockIdx.x;
   if (idx >= a.n_elems) return;
+  int buf = 0;
   {
     const int e0 = a.elems[idx];
-    gather_async<P, 1, NT, T, T>(a.offsets, e0, lin, sN);
-    gather_out_async<P, NT, T>(a.offsets, e0, p.v, sV);
-    cp_async_commit();
+    EntryOffsets<P, NT> eo;
+    eo.load(a.offsets, e0);
+    eo.store(sO[0]);
+    gather_async<P, 1, NT, T>(eo, p.dq, p.dq, sN);
+    __syncthreads();
+    gather_out_async<P, NT, T>(sO[0], p.v, sV);
     if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, tx);
     stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
     stage_block<T, NT>(sJD, p.jac_data + (int64_t)e0 * njd * Q3, njd * Q3, p.jd_tma, mbar);
@@ -500,9 +552,10 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
   }
   unsigned phase = 0;
   for (; idx < a.n_elems; idx += gridDim.x) {
-    const int e = a.elems[idx];
     const int nidx = idx + gridDim.x;
     const int en = nidx < a.n_elems ? a.elems[nidx] : -1;
+    EntryOffsets<P, NT> nxt;
+    if (en >= 0) nxt.load(a.offsets, en);
     cp_async_wait_all();
     if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
       s_bail = 1;
@@ -515,12 +568,14 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
       prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, qd_bytes);
       prefetch_l2_bulk(p.jac_data + (int64_t)en * njd * Q3, jd_bytes);
     }
-    forward_passes<P, Q, 1, NT, T>(a.basis, sN, s1, s2, sU, sG, [&]() {
-      if (en >= 0) {
-        gather_async<P, 1, NT, T, T>(a.offsets, en, lin, sN);
-        cp_async_commit();
-      }
-    });
+    pass_x_staged<P, Q, 5, NT, T>(a.basis, sN, s1);
+    __syncthreads();
+    if (en >= 0) {
+      gather_async<P, 1, NT, T>(nxt, p.dq, p.dq, sN);
+      cp_async_commit();
+      nxt.store(sO[buf ^ 1]);
+    }
+    forward_yz<P, Q, 5, NT, T>(a.basis, s1, s2, sU, sG);
     const int q = threadIdx.x;
     if (q < Q3) {
       T dq[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5], jd[15];
@@ -555,10 +610,11 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
       cp_async_commit();
     }
     transpose_passes<P, Q, NT, T>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
-    scatter_store<P, NT, T>(a.offsets, e, sV, s2, p.v);
+    scatter_store<P, NT, T>(sO[buf], sV, s2, p.v);
     __syncthreads();
+    buf ^= 1;
     if (en >= 0) {
-      gather_out_async<P, NT, T>(a.offsets, en, p.v, sV);
+      gather_out_async<P, NT, T>(sO[buf], p.v, sV);
       cp_async_commit();
     }
   }
