@@ -169,7 +169,9 @@ const CeedQFunction                       CEED_QFUNCTION_NONE       = &qf_none_o
 /* ------------------------------------------------------------------------------------------------------------------ */
 /* errors                                                                                                             */
 
-static int ceed_error(Ceed ceed, const char *file, int line, const char *func, int ecode, const char *fmt, ...) {
+/* CeedErrorImpl: route an error through the Ceed's handler (CeedErrorStore by default, as HONEE installs it,
+ * examples/navierstokes.c:66); the CeedError macro of the public header calls this. */
+int CeedErrorImpl(Ceed ceed, const char *file, int line, const char *func, int ecode, const char *fmt, ...) {
   va_list args;
   va_start(args, fmt);
   int r = ecode;
@@ -178,7 +180,6 @@ static int ceed_error(Ceed ceed, const char *file, int line, const char *func, i
   va_end(args);
   return r;
 }
-#define CeedError(ceed, ecode, ...) ceed_error((ceed), __FILE__, __LINE__, __func__, (ecode), __VA_ARGS__)
 #define CK(call)            \
   do {                      \
     int ierr_ = (call);     \
@@ -1091,6 +1092,10 @@ int CeedQFunctionContextGetContextSize(CeedQFunctionContext ctx, size_t *ctx_siz
   *ctx_size = ctx->size;
   return CEED_ERROR_SUCCESS;
 }
+int CeedQFunctionContextReference(CeedQFunctionContext ctx) {
+  ctx->ref++;
+  return CEED_ERROR_SUCCESS;
+}
 int CeedQFunctionContextDestroy(CeedQFunctionContext *ctx) {
   CeedQFunctionContext c = *ctx;
   if (!c) return CEED_ERROR_SUCCESS;
@@ -1704,4 +1709,174 @@ int CeedOperatorDestroy(CeedOperator *op) {
   free(o);
   *op = NULL;
   return CeedDestroy(&ceed);
+}
+
+/* ------------------------------------------------------------------------------------------------------------------ */
+/* Accessors, views and the assembly entry points HONEE links against (src/mat-ceed.c, src/misc.c, src/petsc_ops.c)      */
+
+int CeedGetGitVersion(const char **git_version) {
+  *git_version = "honee-b200";
+  return CEED_ERROR_SUCCESS;
+}
+Ceed CeedObjectReturnCeed(CeedObject obj) { return obj ? *(Ceed *)obj : NULL; }
+int  CeedVectorGetCeed(CeedVector vec, Ceed *ceed) {
+  *ceed = NULL;
+  return CeedReferenceCopy(vec->ceed, ceed);
+}
+Ceed CeedVectorReturnCeed(CeedVector vec) { return vec->ceed; }
+int  CeedElemRestrictionGetCeed(CeedElemRestriction rstr, Ceed *ceed) {
+  *ceed = NULL;
+  return CeedReferenceCopy(rstr->ceed, ceed);
+}
+Ceed CeedElemRestrictionReturnCeed(CeedElemRestriction rstr) { return rstr->ceed; }
+Ceed CeedBasisReturnCeed(CeedBasis basis) { return basis->ceed; }
+int  CeedOperatorGetCeed(CeedOperator op, Ceed *ceed) {
+  *ceed = NULL;
+  return CeedReferenceCopy(op->ceed, ceed);
+}
+Ceed CeedOperatorReturnCeed(CeedOperator op) { return op->ceed; }
+int  CeedOperatorIsComposite(CeedOperator op, bool *is_composite) {
+  *is_composite = op->composite != 0;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorGetContext(CeedOperator op, CeedQFunctionContext *ctx) {
+  *ctx = NULL;
+  if (op->composite) return CeedError(op->ceed, CEED_ERROR_INCOMPATIBLE, "composite operators have no single context");
+  if (op->qf->ctx) return CeedQFunctionContextReferenceCopy(op->qf->ctx, ctx);
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedQFunctionCreateIdentity(Ceed ceed, CeedInt size, CeedEvalMode in_mode, CeedEvalMode out_mode, CeedQFunction *qf) {
+  CK(CeedQFunctionCreateInterior(ceed, 1, NULL, "Identity", qf));
+  CK(CeedQFunctionAddInput(*qf, "input", size, in_mode));
+  return CeedQFunctionAddOutput(*qf, "output", size, out_mode);
+}
+
+/* Operator fields are addressed through a handle encoding (operator, field index); the layout is private to this file. */
+struct CeedOperatorField_private {
+  CeedOperator op;
+  int          out, index;
+};
+#define FIELD_POOL 1024
+static struct CeedOperatorField_private field_pool[FIELD_POOL];
+static int                              field_pool_n;
+
+int CeedOperatorGetFieldByName(CeedOperator op, const char *field_name, CeedOperatorField *op_field) {
+  *op_field = NULL;
+  if (op->composite) return CeedError(op->ceed, CEED_ERROR_INCOMPATIBLE, "composite operators have no fields");
+  for (int o = 0; o < 2; o++) {
+    const int n = o ? op->qf->nout : op->qf->nin;
+    for (int i = 0; i < n; i++) {
+      const char *nm = o ? op->qf->out[i].name : op->qf->in[i].name;
+      if (strcmp(nm, field_name)) continue;
+      for (int k = 0; k < field_pool_n; k++)
+        if (field_pool[k].op == op && field_pool[k].out == o && field_pool[k].index == i) {
+          *op_field = &field_pool[k];
+          return CEED_ERROR_SUCCESS;
+        }
+      if (field_pool_n >= FIELD_POOL) return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "too many operator field handles");
+      field_pool[field_pool_n] = (struct CeedOperatorField_private){op, o, i};
+      *op_field                = &field_pool[field_pool_n++];
+      return CEED_ERROR_SUCCESS;
+    }
+  }
+  return CeedError(op->ceed, CEED_ERROR_INCOMPLETE, "operator has no field named '%s'", field_name);
+}
+static OpField *field_of(CeedOperatorField f) { return f->out ? &f->op->out[f->index] : &f->op->in[f->index]; }
+int CeedOperatorFieldGetElemRestriction(CeedOperatorField op_field, CeedElemRestriction *rstr) {
+  *rstr = field_of(op_field)->r;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorFieldGetVector(CeedOperatorField op_field, CeedVector *vec) {
+  *vec = field_of(op_field)->v;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorFieldGetData(CeedOperatorField op_field, const char **field_name, CeedElemRestriction *rstr, CeedBasis *basis, CeedVector *vec) {
+  OpField *f = field_of(op_field);
+  if (field_name) *field_name = op_field->out ? op_field->op->qf->out[op_field->index].name : op_field->op->qf->in[op_field->index].name;
+  if (rstr) *rstr = f->r;
+  if (basis) *basis = f->b;
+  if (vec) *vec = f->v;
+  return CEED_ERROR_SUCCESS;
+}
+
+static int view_tabs_default;
+int CeedOperatorSetNumViewTabs(CeedOperator op, CeedInt num_tabs) {
+  (void)op;
+  view_tabs_default = num_tabs;
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorGetNumViewTabs(CeedOperator op, CeedInt *num_tabs) {
+  (void)op;
+  *num_tabs = view_tabs_default;
+  return CEED_ERROR_SUCCESS;
+}
+static void op_view(CeedOperator op, FILE *stream, int terse, int depth) {
+  const int tabs = view_tabs_default + depth;
+  for (int t = 0; t < tabs; t++) fputs("  ", stream);
+  if (op->composite) {
+    fprintf(stream, "Composite CeedOperator '%s' (%d sub-operators) on %s\n", op->name, op->nsub, op->ceed->resource);
+    for (int i = 0; i < op->nsub; i++) op_view(op->subs[i], stream, terse, depth + 1);
+    return;
+  }
+  fprintf(stream, "CeedOperator '%s': QFunction %s, %d inputs, %d outputs, backend plan %s\n", op->name, op->qf->kernel, op->qf->nin,
+          op->qf->nout,
+          op->plan == PLAN_IFUNCTION   ? "fused IFunction"
+          : op->plan == PLAN_IJACOBIAN ? "fused IJacobian"
+          : op->plan == PLAN_SETUP     ? "qdata setup"
+                                       : "not planned");
+  if (terse) return;
+  for (int o = 0; o < 2; o++)
+    for (int i = 0; i < (o ? op->qf->nout : op->qf->nin); i++) {
+      const QFField *qf = o ? &op->qf->out[i] : &op->qf->in[i];
+      for (int t = 0; t < tabs + 1; t++) fputs("  ", stream);
+      fprintf(stream, "%s field '%s': size %d, eval mode %d\n", o ? "output" : "input", qf->name, qf->size, qf->emode);
+    }
+}
+int CeedOperatorView(CeedOperator op, FILE *stream) {
+  op_view(op, stream, 0, 0);
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorViewTerse(CeedOperator op, FILE *stream) {
+  op_view(op, stream, 1, 0);
+  return CEED_ERROR_SUCCESS;
+}
+int CeedOperatorSetQFunctionAssemblyDataUpdateNeeded(CeedOperator op, bool needs_data_update) {
+  (void)op, (void)needs_data_update; /* the diagonal is linearised on the fly from the stored Jacobian data */
+  return CEED_ERROR_SUCCESS;
+}
+
+#define ASSEMBLY_UNSUPPORTED(op) \
+  CeedError((op)->ceed, CEED_ERROR_UNSUPPORTED, "assembled (COO) and point-block operators are not provided by /gpu/b200 (matrix-free only)")
+int CeedOperatorLinearAssembleSymbolic(CeedOperator op, CeedSize *num_entries, CeedInt **rows, CeedInt **cols) {
+  (void)num_entries, (void)rows, (void)cols;
+  return ASSEMBLY_UNSUPPORTED(op);
+}
+int CeedOperatorLinearAssemble(CeedOperator op, CeedVector values) {
+  (void)values;
+  return ASSEMBLY_UNSUPPORTED(op);
+}
+int CeedOperatorLinearAssembleGetNumEntries(CeedOperator op, CeedSize *num_entries) {
+  (void)num_entries;
+  return ASSEMBLY_UNSUPPORTED(op);
+}
+int CeedOperatorLinearAssemblePointBlockDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request) {
+  (void)assembled, (void)request;
+  return ASSEMBLY_UNSUPPORTED(op);
+}
+int CeedOperatorLinearAssemblePointBlockDiagonalSymbolic(CeedOperator op, CeedSize *num_entries, CeedInt **rows, CeedInt **cols) {
+  (void)num_entries, (void)rows, (void)cols;
+  return ASSEMBLY_UNSUPPORTED(op);
+}
+int CeedOperatorGetOperatorAssemblyData(CeedOperator op, CeedOperatorAssemblyData *data) {
+  (void)data;
+  return ASSEMBLY_UNSUPPORTED(op);
+}
+int CeedOperatorAssemblyDataGetBases(CeedOperatorAssemblyData data, CeedInt *num_active_bases_in, CeedBasis **active_bases_in,
+                                     const CeedScalar ***assembled_bases_in, CeedInt *num_active_bases_out, CeedBasis **active_bases_out,
+                                     const CeedScalar ***assembled_bases_out) {
+  (void)data, (void)num_active_bases_in, (void)active_bases_in, (void)assembled_bases_in, (void)num_active_bases_out, (void)active_bases_out,
+      (void)assembled_bases_out;
+  snprintf(fallback_msg, sizeof fallback_msg, "operator assembly data is not provided by /gpu/b200");
+  return CEED_ERROR_UNSUPPORTED;
 }

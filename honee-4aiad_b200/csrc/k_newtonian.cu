@@ -13,11 +13,32 @@
 // src/mat-ceed.c:1618,1669 on the operators built in src/setuplibceed.c:209-269.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "honee_b200.h"
 #include "newtonian_qf.cuh"
 #include "pipeline.cuh"
+
+// Optional per-phase cycle accounting of the fused kernels (debug builds with -DHB_PHASE_TIMING only): thread 0 of
+// every CTA adds the clock64() deltas of each phase to hb_phase_cycles[].
+#ifdef HB_PHASE_TIMING
+__device__ unsigned long long hb_phase_cycles[16];
+#define HB_PT_DECL unsigned long long hb_t0 = clock64(), hb_acc[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+#define HB_PT(k)                             \
+  if (threadIdx.x == 0) {                    \
+    const unsigned long long t1 = clock64(); \
+    hb_acc[k] += t1 - hb_t0;                 \
+    hb_t0 = t1;                              \
+  }
+#define HB_PT_FLUSH(base) \
+  if (threadIdx.x == 0)   \
+    for (int k = 0; k < 16; k++) atomicAdd(&hb_phase_cycles[(base) + k], hb_acc[k]);
+#else
+#define HB_PT_DECL
+#define HB_PT(k)
+#define HB_PT_FLUSH(base)
+#endif
 
 namespace hb {
 
@@ -35,7 +56,7 @@ __host__ __device__ constexpr int nthreads_for(int Q) {
   return ((Q * Q * Q + 31) / 32) * 32;
 }
 // resident CTAs per SM the register budget is tuned for (65536 registers / (threads * CTAs))
-__host__ __device__ constexpr int min_blocks_for(int Q) { return Q <= 5 ? 3 : (Q == 6 ? 2 : 1); }
+__host__ __device__ constexpr int min_blocks_for(int Q, bool staged = true) { return Q <= 5 ? (staged ? 3 : 4) : (Q == 6 ? 2 : 1); }
 
 // ---------------------------------------------------------------------------------------------------------------------
 // fibre passes over shared-memory tensors.  All arrays are [comp][n2][n1][n0] with n0 fastest.
@@ -344,20 +365,21 @@ __device__ __forceinline__ void scatter_store(const int32_t *sO, const T *sV, co
 //   sG  [15][Q3]        reference gradients; point-wise fluxes in place; later sT1
 //   sJD [15][Q3]        staged stored Jacobian data (IJacobian only)
 //   sQD [10][Q3] double staged qdata
-template <int P, int Q, int NV, typename T, bool JD>
+template <int P, int Q, int NV, typename T, bool JD, bool ST = true>
 struct Plan {
   static constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
   static constexpr int cmax(int x, int y) { return x > y ? x : y; }
   static constexpr int nN = NV * 5 * P * P * padded_row<P>(), nV = 5 * P3, nU = 10 * Q3, nG = 15 * Q3;
   static constexpr int n1 = cmax(NV * 5 * P * P * Q, 5 * P * Q2);          // x-pass output, then sT2
   static constexpr int n2 = cmax(cmax(NV * 5 * P * Q2, 5 * Q3), 5 * P3);   // y-pass output, then w2 and node values
-  static constexpr int nJD = JD ? 15 * Q3 : 0;
+  static constexpr int nJD = (JD && ST) ? 15 * Q3 : 0;
   static constexpr int kAl = 16 / (int)sizeof(T);
   static constexpr int pad(int n) { return (n + kAl - 1) / kAl * kAl; }  // every buffer 16-byte aligned (bulk copies)
   static constexpr int oN = 0, oV = pad(oN + nN), o1 = pad(oV + nV), o2 = pad(o1 + n1), oU = pad(o2 + n2), oG = pad(oU + nU),
                        oJD = pad(oG + nG), end_T = pad(oJD + nJD);
   static constexpr size_t qd_offset_bytes = ((size_t)end_T * sizeof(T) + 15) & ~(size_t)15;
-  static constexpr size_t bytes = qd_offset_bytes + sizeof(double) * 10 * Q3 + 16;  // + mbarrier
+  static constexpr size_t mbar_offset = qd_offset_bytes + (ST ? sizeof(double) * 10 * Q3 : 0);  // staged qdata precedes it
+  static constexpr size_t bytes = mbar_offset + 16;
   static_assert(5 * P * Q2 <= n1, "sT2 fits in s1");
   static_assert(5 * Q3 <= n2, "w2 fits in s2");
   static_assert(5 * P3 <= n2, "final node values fit in s2");
@@ -376,17 +398,17 @@ struct IfunctionPtrs {
   int qdata_tma;      // qdata blocks can be bulk-copied (16-byte aligned base)
 };
 
-template <int P, int Q>
-__global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p) {
+template <int P, int Q, bool ST>
+__global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p) {
   constexpr int NT = nthreads_for<double>(Q);
-  using L = Plan<P, Q, 2, double, false>;
+  using L = Plan<P, Q, 2, double, false, ST>;
   constexpr int Q3 = L::Q3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sm = reinterpret_cast<double *>(smem_raw);
   double *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
   double *sD = sU + 5 * Q3;
   double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + sizeof(double) * 10 * Q3);
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::mbar_offset);
   __shared__ int s_bail;
   __shared__ double s_qref[kMaxP];
   __shared__ int32_t sO[2][5 * L::P3];  // entry offsets of the current / next element
@@ -411,39 +433,55 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
     eo.load(a.offsets, e0);
     eo.store(sO[0]);
     gather_async<P, 2, NT, double>(eo, p.q, p.q_dot, sN);
+    if constexpr (ST) {
+      if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
+      stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+    } else if (threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)e0 * 10 * Q3, qd_bytes);
+    cp_async_commit();
     __syncthreads();
     gather_out_async<P, NT, double>(sO[0], p.v, sV);
-    if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
-    stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
     cp_async_commit();
   }
   unsigned phase = 0;
+  // element ids and entry offsets are read two elements ahead so no global load latency sits on the critical path
+  const int G = gridDim.x;
+  int ecur = a.elems[idx];
+  int en = idx + G < a.n_elems ? a.elems[idx + G] : -1;
+  int en2 = idx + 2 * G < a.n_elems ? a.elems[idx + 2 * G] : -1;
+  EntryOffsets<P, NT> nxt, nxt2;
+  if (en >= 0) nxt.load(a.offsets, en);
+  HB_PT_DECL
   for (; idx < a.n_elems; idx += gridDim.x) {
-    const int e = a.elems[idx];
-    const int nidx = idx + gridDim.x;
-    const int en = nidx < a.n_elems ? a.elems[nidx] : -1;
-    EntryOffsets<P, NT> nxt;
-    if (en >= 0) nxt.load(a.offsets, en);
-    cp_async_wait_all();
-    if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
+    const int e = ecur;
+    const int en3 = idx + 3 * G < a.n_elems ? a.elems[idx + 3 * G] : -1;  // used one iteration later
+    if (en2 >= 0) nxt2.load(a.offsets, en2);
+    HB_PT(7)
+    // everything but the most recent group (the output gather, only needed at the scatter) has landed
+    cp_async_wait_group<1>();
+    HB_PT(8)
+    if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
       s_bail = 1;
       atomicOr(a.status, 1);
     }
+    HB_PT(9)
     __syncthreads();
     if (s_bail) break;
     phase ^= 1;
+    HB_PT(0)
     if (en >= 0 && threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, qd_bytes);
     pass_x_staged<P, Q, 10, NT, double>(a.basis, sN, s1);
     __syncthreads();
+    HB_PT(1)
     if (en >= 0) {  // sN consumed: stage the next element's node values
       gather_async<P, 2, NT, double>(nxt, p.q, p.q_dot, sN);
       cp_async_commit();
       nxt.store(sO[buf ^ 1]);
     }
     forward_yz<P, Q, 10, NT, double>(a.basis, s1, s2, sU, sG);
+    HB_PT(2)
     const int q = threadIdx.x;
     if (q < Q3) {
-      double qi[5], qd[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5], jd[15];
+      double qi[5], qd[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5];
 #pragma unroll
       for (int c = 0; c < 5; c++) {
         qi[c] = sU[c * Q3 + q];
@@ -451,52 +489,68 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
 #pragma unroll
         for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
-      wdetJ = sQD[q];
+      const double *qdp = ST ? sQD : a.qdata + (int64_t)e * 10 * Q3;
+      wdetJ = qdp[q];
 #pragma unroll
-      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = sQD[(1 + k) * Q3 + q];
+      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = qdp[(1 + k) * Q3 + q];
       double x0 = 0;
       if (a.pc.idl_enable) x0 = qpt_x0<Q>(a.x_elem + (int64_t)e * 24, s_qref, q % Q, (q / Q) % Q, q / (Q * Q));
-      ifunction_point<double>(a.pc, qi, gref, qd, wdetJ, X, x0, v, gv, jd);
+      // stored Jacobian values go to global memory as soon as they are known (FP64 and/or the FP32 shadow)
+      double *jd64 = p.jac_data ? p.jac_data + (int64_t)e * a.num_jd * Q3 + q : nullptr;
+      float *jd32 = p.jac_f32 ? p.jac_f32 + (int64_t)e * a.num_jd * Q3 + q : nullptr;
+      const int njd = a.num_jd;
+      auto emit = [=](int k, double val) {
+        if (k < njd) {
+          if (jd64) jd64[k * Q3] = val;
+          if (jd32) jd32[k * Q3] = float(val);
+        }
+      };
+      ifunction_point_stream<double>(a.pc, qi, gref, qd, wdetJ, X, x0, v, gv, emit);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
         sU[c * Q3 + q] = v[c];
 #pragma unroll
         for (int d = 0; d < 3; d++) sG[(d * 5 + c) * Q3 + q] = gv[d][c];
       }
-      if (p.jac_data) {
-        double *jdp = p.jac_data + (int64_t)e * a.num_jd * Q3 + q;
-#pragma unroll
-        for (int c = 0; c < 14; c++) jdp[c * Q3] = jd[c];
-        if (a.num_jd > 14) jdp[14 * Q3] = jd[14];
-      }
-      if (p.jac_f32) {
-        float *jdp = p.jac_f32 + (int64_t)e * a.num_jd * Q3 + q;
-#pragma unroll
-        for (int c = 0; c < 14; c++) jdp[c * Q3] = float(jd[c]);
-        if (a.num_jd > 14) jdp[14 * Q3] = float(jd[14]);
-      }
     }
     __syncthreads();
+    HB_PT(3)
     if (en >= 0) {  // sQD consumed: stage the next element's qdata
-      if (threadIdx.x == 0) {
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
+      if constexpr (ST) {
+        if (threadIdx.x == 0) {
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
+        }
+        stage_block<double, NT>(sQD, a.qdata + (int64_t)en * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
       }
-      stage_block<double, NT>(sQD, a.qdata + (int64_t)en * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
       cp_async_commit();
     }
     // transpose scratch: w1 in the q_dot slot, w2 and the node values in s2, sT2 in s1, sT1 in sG
+    HB_PT(4)
     transpose_passes<P, Q, NT, double>(a.basis, sU, sG, sD, s2, s1, sG, s2);
+    HB_PT(5)
+    if (en >= 0) cp_async_wait_group<2>();  // the output gather, committed before this element's two stagings
+    else cp_async_wait_group<0>();
+    HB_PT(10)
+    __syncthreads();
+    HB_PT(11)
     scatter_store<P, NT, double>(sO[buf], sV, s2, p.v);
+    HB_PT(12)
     __syncthreads();
     buf ^= 1;
     if (en >= 0) {
       gather_out_async<P, NT, double>(sO[buf], p.v, sV);
       cp_async_commit();
     }
+    ecur = en;
+    en = en2;
+    en2 = en3;
+    nxt = nxt2;
+    HB_PT(6)
   }
+  HB_PT_FLUSH(0)
   cp_async_wait_all();
-  if (s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);  // let an outstanding bulk copy land before exit
+  if (ST && s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);  // let an outstanding bulk copy land before exit
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -510,17 +564,17 @@ struct IjacobianPtrs {
   int qdata_tma, jd_tma;
 };
 
-template <int P, int Q, typename T>
-__global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
+template <int P, int Q, typename T, bool ST>
+__global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST)) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
   constexpr int NT = nthreads_for<T>(Q);
-  using L = Plan<P, Q, 1, T, true>;
+  using L = Plan<P, Q, 1, T, true, ST>;
   constexpr int Q3 = L::Q3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
   T *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG, *sJD = sm + L::oJD;
   T *sW1 = sU + 5 * Q3;
   double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + sizeof(double) * 10 * Q3);
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::mbar_offset);
   __shared__ int s_bail;
   __shared__ int32_t sO[2][5 * L::P3];  // entry offsets of the current / next element
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
@@ -543,21 +597,34 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
     eo.load(a.offsets, e0);
     eo.store(sO[0]);
     gather_async<P, 1, NT, T>(eo, p.dq, p.dq, sN);
+    if constexpr (ST) {
+      if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, tx);
+      stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+      stage_block<T, NT>(sJD, p.jac_data + (int64_t)e0 * njd * Q3, njd * Q3, p.jd_tma, mbar);
+    } else if (threadIdx.x == 0) {
+      prefetch_l2_bulk(a.qdata + (int64_t)e0 * 10 * Q3, qd_bytes);
+      prefetch_l2_bulk(p.jac_data + (int64_t)e0 * njd * Q3, jd_bytes);
+    }
+    cp_async_commit();
     __syncthreads();
     gather_out_async<P, NT, T>(sO[0], p.v, sV);
-    if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, tx);
-    stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
-    stage_block<T, NT>(sJD, p.jac_data + (int64_t)e0 * njd * Q3, njd * Q3, p.jd_tma, mbar);
     cp_async_commit();
   }
   unsigned phase = 0;
+  // element ids and entry offsets are read two elements ahead so no global load latency sits on the critical path
+  const int G = gridDim.x;
+  int ecur = a.elems[idx];
+  int en = idx + G < a.n_elems ? a.elems[idx + G] : -1;
+  int en2 = idx + 2 * G < a.n_elems ? a.elems[idx + 2 * G] : -1;
+  EntryOffsets<P, NT> nxt, nxt2;
+  if (en >= 0) nxt.load(a.offsets, en);
   for (; idx < a.n_elems; idx += gridDim.x) {
-    const int nidx = idx + gridDim.x;
-    const int en = nidx < a.n_elems ? a.elems[nidx] : -1;
-    EntryOffsets<P, NT> nxt;
-    if (en >= 0) nxt.load(a.offsets, en);
-    cp_async_wait_all();
-    if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
+    const int e = ecur;
+    const int en3 = idx + 3 * G < a.n_elems ? a.elems[idx + 3 * G] : -1;  // used one iteration later
+    if (en2 >= 0) nxt2.load(a.offsets, en2);
+    // everything but the most recent group (the output gather, only needed at the scatter) has landed
+    cp_async_wait_group<1>();
+    if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
       s_bail = 1;
       atomicOr(a.status, 1);
     }
@@ -585,13 +652,15 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
 #pragma unroll
         for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
+      const T *jdp = ST ? sJD : p.jac_data + (int64_t)e * njd * Q3;
+      const double *qdp = ST ? sQD : a.qdata + (int64_t)e * 10 * Q3;
 #pragma unroll
-      for (int c = 0; c < 14; c++) jd[c] = sJD[c * Q3 + q];
-      jd[14] = njd > 14 ? sJD[14 * Q3 + q] : T(0);
-      wdetJ = T(sQD[q]);
+      for (int c = 0; c < 14; c++) jd[c] = jdp[c * Q3 + q];
+      jd[14] = njd > 14 ? jdp[14 * Q3 + q] : T(0);
+      wdetJ = T(qdp[q]);
 #pragma unroll
-      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = T(sQD[(1 + k) * Q3 + q]);
-      ijacobian_point<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
+      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = T(qdp[(1 + k) * Q3 + q]);
+      ijacobian_point_stream<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
         sU[c * Q3 + q] = v[c];
@@ -601,15 +670,20 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
     }
     __syncthreads();
     if (en >= 0) {
-      if (threadIdx.x == 0) {
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(mbar, tx);
+      if constexpr (ST) {
+        if (threadIdx.x == 0) {
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(mbar, tx);
+        }
+        stage_block<double, NT>(sQD, a.qdata + (int64_t)en * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+        stage_block<T, NT>(sJD, p.jac_data + (int64_t)en * njd * Q3, njd * Q3, p.jd_tma, mbar);
       }
-      stage_block<double, NT>(sQD, a.qdata + (int64_t)en * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
-      stage_block<T, NT>(sJD, p.jac_data + (int64_t)en * njd * Q3, njd * Q3, p.jd_tma, mbar);
       cp_async_commit();
     }
     transpose_passes<P, Q, NT, T>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
+    if (en >= 0) cp_async_wait_group<2>();
+    else cp_async_wait_group<0>();
+    __syncthreads();
     scatter_store<P, NT, T>(sO[buf], sV, s2, p.v);
     __syncthreads();
     buf ^= 1;
@@ -617,9 +691,13 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q)) k_ijaco
       gather_out_async<P, NT, T>(sO[buf], p.v, sV);
       cp_async_commit();
     }
+    ecur = en;
+    en = en2;
+    en2 = en3;
+    nxt = nxt2;
   }
   cp_async_wait_all();
-  if (s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);
+  if (ST && s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -645,8 +723,22 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemAr
   T *sT1 = sA + 10 * Q3;       // [Q][Q][P]  after x contraction
   T *sT2 = sT1 + Q2 * P;       // [Q][P][P]  after y contraction
   T *sOut = sT2 + Q * P * P;   // [5][P3]
-  // product-matrix selectors for the 10 (m,n) combinations: number of x/y/z derivatives (0: B*B, 1: B*G, 2: G*G)
-  // combo order: II, IGx, IGy, IGz, GxGx, GyGy, GzGz, GxGy, GxGz, GyGz
+  // squared basis rows: W[s][i][p] for s = 0: B*B, 1: B*G, 2: G*G (shared copies: no parameter arrays indexed at run time)
+  __shared__ T sW[3][kMaxP * kMaxP];
+  for (int t = threadIdx.x; t < Q * P; t += NT) {
+    T b = 0, g = 0;
+#pragma unroll
+    for (int i = 0; i < Q * P; i++)
+      if (i == t) {
+        b = a.basis.B[i];
+        g = p.G1[i];
+      }
+    sW[0][t] = b * b;
+    sW[1][t] = b * g;
+    sW[2][t] = g * g;
+  }
+  __syncthreads();
+  // combo order: II, IGx, IGy, IGz, GxGx, GyGy, GzGz, GxGy, GxGz, GyGz; selectors = number of derivatives per direction
   constexpr int cx[10] = {0, 1, 0, 0, 2, 0, 0, 1, 1, 0};
   constexpr int cy[10] = {0, 0, 1, 0, 0, 2, 0, 1, 0, 1};
   constexpr int cz[10] = {0, 0, 0, 1, 0, 0, 2, 0, 1, 1};
@@ -662,16 +754,25 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemAr
         jd[14] = a.num_jd > 14 ? jdp[14 * Q3] : T(0);
         load_qdata(a.qdata + (int64_t)e * 10 * Q3, Q3, q, wdetJ, X);
         T A[4][4];
-#pragma unroll 1
+#pragma unroll
         for (int n = 0; n < 4; n++) {
           T dq[5] = {0, 0, 0, 0, 0}, gref[3][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}}, v[5], gv[3][5];
-          if (n == 0) dq[c] = 1;
-          else gref[n - 1][c] = 1;
-          ijacobian_point<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
-          A[0][n] = v[c];
-          A[1][n] = gv[0][c];
-          A[2][n] = gv[1][c];
-          A[3][n] = gv[2][c];
+#pragma unroll
+          for (int k = 0; k < 5; k++) {
+            if (n == 0 && k == c) dq[k] = 1;
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+              if (n == d + 1 && k == c) gref[d][k] = 1;
+          }
+          ijacobian_point_stream<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
+#pragma unroll
+          for (int k = 0; k < 5; k++)
+            if (k == c) {
+              A[0][n] = v[k];
+              A[1][n] = gv[0][k];
+              A[2][n] = gv[1][k];
+              A[3][n] = gv[2][k];
+            }
         }
         sA[0 * Q3 + q] = A[0][0];
         sA[1 * Q3 + q] = A[0][1] + A[1][0];
@@ -688,16 +789,12 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemAr
       __syncthreads();
 #pragma unroll
       for (int m = 0; m < 10; m++) {
-        // x: T1[k][j][pa] = sum_i X(i,pa) A[k][j][i]
-        for (int f = threadIdx.x; f < Q2 * P; f += NT) {
+        const T *Wx = sW[cx[m]], *Wy = sW[cy[m]], *Wz = sW[cz[m]];
+        for (int f = threadIdx.x; f < Q2 * P; f += NT) {  // x: T1[k][j][pa] = sum_i Wx(i,pa) A[k][j][i]
           const int pa = f % P, kj = f / P;
           T s = 0;
 #pragma unroll
-          for (int i = 0; i < Q; i++) {
-            const T b = a.basis.B[i * P + pa], g = p.G1[i * P + pa];
-            const T w = cx[m] == 0 ? b * b : (cx[m] == 1 ? b * g : g * g);
-            s += w * sA[m * Q3 + kj * Q + i];
-          }
+          for (int i = 0; i < Q; i++) s += Wx[i * P + pa] * sA[m * Q3 + kj * Q + i];
           sT1[kj * P + pa] = s;
         }
         __syncthreads();
@@ -705,11 +802,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemAr
           const int pa = f % P, pb = (f / P) % P, k = f / (P * P);
           T s = 0;
 #pragma unroll
-          for (int j = 0; j < Q; j++) {
-            const T b = a.basis.B[j * P + pb], g = p.G1[j * P + pb];
-            const T w = cy[m] == 0 ? b * b : (cy[m] == 1 ? b * g : g * g);
-            s += w * sT1[(k * Q + j) * P + pa];
-          }
+          for (int j = 0; j < Q; j++) s += Wy[j * P + pb] * sT1[(k * Q + j) * P + pa];
           sT2[(k * P + pb) * P + pa] = s;
         }
         __syncthreads();
@@ -717,11 +810,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemAr
           const int pab = f % (P * P), pc_ = f / (P * P);
           T s = 0;
 #pragma unroll
-          for (int k = 0; k < Q; k++) {
-            const T b = a.basis.B[k * P + pc_], g = p.G1[k * P + pc_];
-            const T w = cz[m] == 0 ? b * b : (cz[m] == 1 ? b * g : g * g);
-            s += w * sT2[k * P * P + pab];
-          }
+          for (int k = 0; k < Q; k++) s += Wz[k * P + pc_] * sT2[k * P * P + pab];
           sOut[c * P3 + f] += s;
         }
         __syncthreads();
@@ -844,11 +933,11 @@ static size_t smem_bytes(int P, int Q) {
   return sizeof(T) * (size_t)(10 * P3 + 10 * P * P * Q + 10 * P * Q * Q + 10 * Q3 + 15 * Q3);
 }
 
-template <int P, int Q>
-static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
-  using L = Plan<P, Q, 2, double, false>;
+template <int P, int Q, bool ST>
+static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
+  using L = Plan<P, Q, 2, double, false, ST>;
   const size_t sm = L::bytes;
-  cudaFuncSetAttribute(k_ifunction<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_ifunction<P, Q, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   IfunctionPtrs p;
   p.q = io->q;
   p.q_dot = io->q_dot;
@@ -860,17 +949,23 @@ static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, c
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<double> a = make_args<double>(op, ctx, io->qdata, c);
     if (a.n_elems == 0) continue;
-    k_ifunction<P, Q><<<grid_for(op, a.n_elems, k_ifunction<P, Q>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p);
+    k_ifunction<P, Q, ST><<<grid_for(op, a.n_elems, k_ifunction<P, Q, ST>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
-template <int P, int Q, typename T>
-static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v,
-                            cudaStream_t s) {
-  using L = Plan<P, Q, 1, T, true>;
+template <int P, int Q>
+static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
+  // staged per-point data (TMA, 3 CTAs/SM) measured faster than direct loads at 4 CTAs/SM with spills
+  return launch_ifunction_v<P, Q, true>(op, ctx, io, s);
+}
+
+template <int P, int Q, typename T, bool ST>
+static int launch_ijacobian_v(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v,
+                              cudaStream_t s) {
+  using L = Plan<P, Q, 1, T, true, ST>;
   const size_t sm = L::bytes;
-  cudaFuncSetAttribute(k_ijacobian<P, Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_ijacobian<P, Q, T, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   IjacobianPtrs<T> p;
   p.dq = dq;
   p.jac_data = jd;
@@ -881,9 +976,15 @@ static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, c
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
-    k_ijacobian<P, Q, T><<<grid_for(op, a.n_elems, k_ijacobian<P, Q, T>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
+    k_ijacobian<P, Q, T, ST><<<grid_for(op, a.n_elems, k_ijacobian<P, Q, T, ST>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+
+template <int P, int Q, typename T>
+static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v,
+                            cudaStream_t s) {
+  return launch_ijacobian_v<P, Q, T, true>(op, ctx, qdata, jd, dq, v, s);
 }
 
 template <int P, int Q, typename T>
@@ -1009,3 +1110,15 @@ extern "C" int hb_setup_qdata(int num_elem, int Q, const double *qref1d, const d
   k_setup_qdata<<<(unsigned)((n + bs - 1) / bs), bs, 0, (cudaStream_t)stream>>>(num_elem, Q, x_elem, r, w, qdata);
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
+
+#ifdef HB_PHASE_TIMING
+extern "C" HB_EXPORT int hb_debug_phase_cycles(unsigned long long *out, int reset) {
+  if (cudaDeviceSynchronize() != cudaSuccess) return HB_ERROR_CUDA;
+  if (cudaMemcpyFromSymbol(out, hb_phase_cycles, sizeof(unsigned long long) * 16) != cudaSuccess) return HB_ERROR_CUDA;
+  if (reset) {
+    unsigned long long z[16] = {0};
+    cudaMemcpyToSymbol(hb_phase_cycles, z, sizeof z);
+  }
+  return HB_SUCCESS;
+}
+#endif

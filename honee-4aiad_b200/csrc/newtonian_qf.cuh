@@ -336,3 +336,216 @@ __device__ __forceinline__ void ijacobian_point(const PhysConst<T> &c, const T j
 }
 
 }  // namespace hb
+
+namespace hb {
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Streaming forms of the point-wise IFunction / IJacobian used by the fused kernels.  Same arithmetic as
+// ifunction_point / ijacobian_point, reordered so few values are live at once: each physical-gradient direction j is
+// folded into the strong residual, the velocity-gradient column and the temperature gradient as soon as it is formed,
+// the fluxes are projected onto the reference directions one physical direction at a time, and stored Jacobian values
+// are handed to `emit` (index, value) as soon as they are known.
+
+// gradient direction j of the state: dq_j = sum_k gref[k][.] X[k][j] -> tangent state
+template <typename T>
+__device__ __forceinline__ void gradient_dir(const PhysConst<T> &c, const St<T> &s, T inv_rho, T etot, T eint, const T gref[3][5], const T X[3][3],
+                                             int j, St<T> &g) {
+  T dq[5];
+#pragma unroll
+  for (int cc = 0; cc < 5; cc++) dq[cc] = gref[0][cc] * X[0][j] + gref[1][cc] * X[1][j] + gref[2][cc] * X[2][j];
+  state_from_u_fwd(c, s, inv_rho, etot, eint, dq, g);
+}
+
+template <typename T, typename Emit>
+__device__ __forceinline__ void ifunction_point_stream(const PhysConst<T> &c, const T q[5], const T gref[3][5], const T qdot[5], T wdetJ,
+                                                       const T X[3][3], T x0, T v[5], T gv[3][5], Emit emit) {
+  St<T> s;
+  T inv_rho, etot, eint;
+  state_from_u(c, q, s, inv_rho, etot, eint);
+  // strong convective residual, velocity gradient G[i][j] = du_i/dx_j, temperature gradient
+  T r[5] = {0, 0, 0, 0, 0}, G[3][3], gT[3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    St<T> g;
+    gradient_dir(c, s, inv_rho, etot, eint, gref, X, j, g);
+    if (c.stab != HB_STAB_NONE) {
+      T row[5];
+      dflux_row(s, g, j, row);
+#pragma unroll
+      for (int k = 0; k < 5; k++) r[k] += row[k];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) G[i][j] = g.u[i];
+    gT[j] = g.T_;
+  }
+  // KM strain rate (newtonian_state.h:523-532) and stress
+  const T w = T(1.0 / 1.4142135623730951);
+  T e[6];
+  e[0] = G[0][0];
+  e[1] = G[1][1];
+  e[2] = G[2][2];
+  e[3] = w * (G[1][2] + G[2][1]);
+  e[4] = w * (G[0][2] + G[2][0]);
+  e[5] = w * (G[0][1] + G[1][0]);
+#pragma unroll
+  for (int k = 0; k < 5; k++) emit(k, q[k]);
+#pragma unroll
+  for (int k = 0; k < 6; k++) emit(5 + k, e[k]);
+  T sig[3][3];
+  stress_full(c, e, sig);
+  // tau and the stabilisation state perturbation
+  T tau[3];
+  tau_diag(c, s, X, tau);
+#pragma unroll
+  for (int k = 0; k < 3; k++) emit(11 + k, tau[k]);
+  const T body[5] = {T(0), s.rho * c.g[0], s.rho * c.g[1], s.rho * c.g[2], s.m[0] * c.g[0] + s.m[1] * c.g[1] + s.m[2] * c.g[2]};
+  St<T> d;
+  const bool stab = c.stab != HB_STAB_NONE;
+  if (stab) {
+    if (c.stab == HB_STAB_SUPG) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) r[k] += qdot[k] - body[k];
+    }
+    const T dY[5] = {tau[0] * r[0], tau[1] * r[1], tau[1] * r[2], tau[1] * r[3], tau[2] * r[4]};
+    state_from_y_fwd(c, s, eint, dY, d);
+  }
+  T vi[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) vi[k] = qdot[k] - body[k];
+  T sigma = 0;
+  if (c.idl_enable) {
+    sigma = linear_ramp(c.idl_amplitude, c.idl_length, c.idl_start, x0);
+    const T dY[5] = {(s.P - c.idl_pressure) * sigma, T(0), T(0), T(0), T(0)};
+    St<T> di;
+    state_from_y_fwd(c, s, eint, dY, di);
+    vi[0] += di.rho;
+    vi[1] += di.m[0];
+    vi[2] += di.m[1];
+    vi[3] += di.m[2];
+    vi[4] += di.E;
+  }
+  emit(14, sigma);
+#pragma unroll
+  for (int k = 0; k < 5; k++) v[k] = wdetJ * vi[k];
+  // per physical direction j: gvi[.][j] = -F_total[.][j] + stab[.][j]; project onto reference directions
+#pragma unroll
+  for (int kk = 0; kk < 3; kk++)
+#pragma unroll
+    for (int k = 0; k < 5; k++) gv[kk][k] = 0;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const T Fe = -s.u[0] * sig[0][j] - s.u[1] * sig[1][j] - s.u[2] * sig[2][j] - c.k * gT[j];
+    T col[5];
+    col[0] = -s.m[j];
+#pragma unroll
+    for (int kk = 0; kk < 3; kk++) col[1 + kk] = -(s.m[j] * s.u[kk] + (j == kk ? s.P : T(0)) - sig[kk][j]);
+    col[4] = -((s.E + s.P) * s.u[j] + Fe);
+    if (stab) {
+      T row[5];
+      dflux_row(s, d, j, row);
+#pragma unroll
+      for (int k = 0; k < 5; k++) col[k] += row[k];
+    }
+#pragma unroll
+    for (int kk = 0; kk < 3; kk++) {
+      const T xw = wdetJ * X[kk][j];
+#pragma unroll
+      for (int k = 0; k < 5; k++) gv[kk][k] += col[k] * xw;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void ijacobian_point_stream(const PhysConst<T> &c, const T jd[15], const T dq[5], const T gref[3][5], T wdetJ,
+                                                       const T X[3][3], T v[5], T gv[3][5]) {
+  St<T> s;
+  T inv_rho, etot, eint;
+  const T q[5] = {jd[0], jd[1], jd[2], jd[3], jd[4]};
+  state_from_u(c, q, s, inv_rho, etot, eint);
+  St<T> ds;
+  state_from_u_fwd(c, s, inv_rho, etot, eint, dq, ds);
+  T r[5] = {0, 0, 0, 0, 0}, G[3][3], gT[3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    St<T> g;
+    gradient_dir(c, s, inv_rho, etot, eint, gref, X, j, g);
+    if (c.stab != HB_STAB_NONE) {
+      T row[5];
+      dflux_row(s, g, j, row);
+#pragma unroll
+      for (int k = 0; k < 5; k++) r[k] += row[k];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) G[i][j] = g.u[i];
+    gT[j] = g.T_;
+  }
+  const T w = T(1.0 / 1.4142135623730951);
+  T de[6];
+  de[0] = G[0][0];
+  de[1] = G[1][1];
+  de[2] = G[2][2];
+  de[3] = w * (G[1][2] + G[2][1]);
+  de[4] = w * (G[0][2] + G[2][0]);
+  de[5] = w * (G[0][1] + G[1][0]);
+  T dsig[3][3], sig[3][3];
+  stress_full(c, de, dsig);
+  const T e[6] = {jd[5], jd[6], jd[7], jd[8], jd[9], jd[10]};
+  stress_full(c, e, sig);
+  const T dbody[5] = {T(0), ds.rho * c.g[0], ds.rho * c.g[1], ds.rho * c.g[2], ds.m[0] * c.g[0] + ds.m[1] * c.g[1] + ds.m[2] * c.g[2]};
+  T vi[5];
+  const T dU[5] = {ds.rho, ds.m[0], ds.m[1], ds.m[2], ds.E};
+  St<T> d;
+  const bool stab = c.stab != HB_STAB_NONE;
+  if (stab) {
+    if (c.stab == HB_STAB_SUPG) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) r[k] += c.shift * dU[k] - dbody[k];
+    }
+    const T dY[5] = {jd[11] * r[0], jd[12] * r[1], jd[12] * r[2], jd[12] * r[3], jd[13] * r[4]};
+    state_from_y_fwd(c, s, eint, dY, d);
+  }
+#pragma unroll
+  for (int k = 0; k < 5; k++) vi[k] = c.shift * dU[k] - dbody[k];
+  if (c.idl_enable) {
+    const T dY[5] = {ds.P * jd[14], T(0), T(0), T(0), T(0)};
+    St<T> di;
+    state_from_y_fwd(c, s, eint, dY, di);
+    vi[0] += di.rho;
+    vi[1] += di.m[0];
+    vi[2] += di.m[1];
+    vi[3] += di.m[2];
+    vi[4] += di.E;
+  }
+#pragma unroll
+  for (int k = 0; k < 5; k++) v[k] = wdetJ * vi[k];
+#pragma unroll
+  for (int kk = 0; kk < 3; kk++)
+#pragma unroll
+    for (int k = 0; k < 5; k++) gv[kk][k] = 0;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    T row[5];
+    dflux_row(s, ds, j, row);
+    const T dFe = -s.u[0] * dsig[0][j] - ds.u[0] * sig[0][j] - s.u[1] * dsig[1][j] - ds.u[1] * sig[1][j] - s.u[2] * dsig[2][j] -
+                  ds.u[2] * sig[2][j] - c.k * gT[j];
+    T col[5];
+    col[0] = -row[0];
+#pragma unroll
+    for (int kk = 0; kk < 3; kk++) col[1 + kk] = -(row[1 + kk] - dsig[kk][j]);
+    col[4] = -(row[4] + dFe);
+    if (stab) {
+      T srow[5];
+      dflux_row(s, d, j, srow);
+#pragma unroll
+      for (int k = 0; k < 5; k++) col[k] += srow[k];
+    }
+#pragma unroll
+    for (int kk = 0; kk < 3; kk++) {
+      const T xw = wdetJ * X[kk][j];
+#pragma unroll
+      for (int k = 0; k < 5; k++) gv[kk][k] += col[k] * xw;
+    }
+  }
+}
+
+}  // namespace hb

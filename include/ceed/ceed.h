@@ -36,12 +36,7 @@ extern "C" {
    (CEED_VERSION_MAJOR > major ||            \
     (CEED_VERSION_MAJOR == major && (CEED_VERSION_MINOR > minor || (CEED_VERSION_MINOR == minor && CEED_VERSION_PATCH >= patch)))))
 
-typedef int32_t   CeedInt;
-typedef int8_t    CeedInt8;
-typedef ptrdiff_t CeedSize;
-typedef double    CeedScalar;
-#define CEED_SCALAR_TYPE CEED_SCALAR_FP64
-#define CEED_EPSILON 0x1p-52
+#include "ceed/types.h"
 
 typedef struct Ceed_private                 *Ceed;
 typedef struct CeedRequest_private          *CeedRequest;
@@ -54,45 +49,13 @@ typedef struct CeedOperatorField_private    *CeedOperatorField;
 typedef struct CeedQFunctionContext_private *CeedQFunctionContext;
 typedef struct CeedContextFieldLabel_private *CeedContextFieldLabel;
 typedef struct CeedOperator_private         *CeedOperator;
+typedef struct CeedObject_private           *CeedObject; /* every object starts with its Ceed, so any handle casts to this */
+typedef struct CeedOperatorAssemblyData_private *CeedOperatorAssemblyData;
 
 typedef int (*CeedQFunctionUser)(void *ctx, const CeedInt Q, const CeedScalar *const *in, CeedScalar *const *out);
 typedef int (*CeedQFunctionContextDataDestroyUser)(void *data);
 typedef int (*CeedErrorHandler)(Ceed, const char *, int, const char *, int, const char *, va_list *);
 
-typedef enum {
-  CEED_ERROR_SUCCESS      = 0,
-  CEED_ERROR_MINOR        = 1,
-  CEED_ERROR_DIMENSION    = 2,
-  CEED_ERROR_INCOMPLETE   = 3,
-  CEED_ERROR_INCOMPATIBLE = 4,
-  CEED_ERROR_ACCESS       = 5,
-  CEED_ERROR_MAJOR        = -1,
-  CEED_ERROR_BACKEND      = -2,
-  CEED_ERROR_UNSUPPORTED  = -3,
-} CeedErrorType;
-
-typedef enum { CEED_MEM_HOST, CEED_MEM_DEVICE } CeedMemType;
-typedef enum { CEED_COPY_VALUES, CEED_USE_POINTER, CEED_OWN_POINTER } CeedCopyMode;
-typedef enum { CEED_NORM_1, CEED_NORM_2, CEED_NORM_MAX } CeedNormType;
-typedef enum { CEED_NOTRANSPOSE, CEED_TRANSPOSE } CeedTransposeMode;
-typedef enum {
-  CEED_EVAL_NONE   = 0,
-  CEED_EVAL_INTERP = 1,
-  CEED_EVAL_GRAD   = 2,
-  CEED_EVAL_DIV    = 4,
-  CEED_EVAL_CURL   = 8,
-  CEED_EVAL_WEIGHT = 16,
-} CeedEvalMode;
-typedef enum { CEED_GAUSS = 0, CEED_GAUSS_LOBATTO = 1 } CeedQuadMode;
-typedef enum {
-  CEED_TOPOLOGY_LINE     = 1 << 16 | 0,
-  CEED_TOPOLOGY_TRIANGLE = 2 << 16 | 1,
-  CEED_TOPOLOGY_QUAD     = 2 << 16 | 2,
-  CEED_TOPOLOGY_TET      = 3 << 16 | 3,
-  CEED_TOPOLOGY_PYRAMID  = 3 << 16 | 4,
-  CEED_TOPOLOGY_PRISM    = 3 << 16 | 5,
-  CEED_TOPOLOGY_HEX      = 3 << 16 | 6,
-} CeedElemTopology;
 typedef enum { CEED_CONTEXT_FIELD_DOUBLE = 1, CEED_CONTEXT_FIELD_INT32 = 2, CEED_CONTEXT_FIELD_BOOL = 3 } CeedContextFieldType;
 
 CEED_EXTERN CeedRequest *const        CEED_REQUEST_IMMEDIATE;
@@ -120,6 +83,10 @@ CEED_EXTERN int CeedErrorReturn(Ceed ceed, const char *filename, int line_no, co
 CEED_EXTERN int CeedErrorStore(Ceed ceed, const char *filename, int line_no, const char *func, int ecode, const char *format, va_list *args);
 CEED_EXTERN int CeedErrorAbort(Ceed ceed, const char *filename, int line_no, const char *func, int ecode, const char *format, va_list *args);
 CEED_EXTERN int CeedErrorExit(Ceed ceed, const char *filename, int line_no, const char *func, int ecode, const char *format, va_list *args);
+CEED_EXTERN int CeedGetGitVersion(const char **git_version);
+CEED_EXTERN int CeedErrorImpl(Ceed ceed, const char *filename, int line_no, const char *func, int ecode, const char *format, ...);
+#define CeedError(ceed, ecode, ...) (CeedErrorImpl((ceed), __FILE__, __LINE__, __func__, (ecode), __VA_ARGS__) ?: (ecode))
+CEED_EXTERN Ceed CeedObjectReturnCeed(CeedObject obj);
 
 /* ---- CeedVector (include/petsc-ceed-utils.h:127-219 zero-copy wrapping, src/qdata.c:42-45, src/mat-ceed.c) ---- */
 CEED_EXTERN int CeedVectorCreate(Ceed ceed, CeedSize len, CeedVector *vec);
@@ -141,6 +108,8 @@ CEED_EXTERN int CeedVectorAXPY(CeedVector y, CeedScalar alpha, CeedVector x);
 CEED_EXTERN int CeedVectorAXPBY(CeedVector y, CeedScalar alpha, CeedScalar beta, CeedVector x);
 CEED_EXTERN int CeedVectorPointwiseMult(CeedVector w, CeedVector x, CeedVector y);
 CEED_EXTERN int CeedVectorReciprocal(CeedVector vec);
+CEED_EXTERN int CeedVectorGetCeed(CeedVector vec, Ceed *ceed);
+CEED_EXTERN Ceed CeedVectorReturnCeed(CeedVector vec);
 CEED_EXTERN int CeedVectorDestroy(CeedVector *vec);
 
 /* ---- CeedElemRestriction (src/dm-utils.c:83-137, :235, src/setuplibceed.c:121-129) ---- */
@@ -158,6 +127,8 @@ CEED_EXTERN int CeedElemRestrictionGetEVectorSize(CeedElemRestriction rstr, Ceed
 CEED_EXTERN int CeedElemRestrictionGetNumComponents(CeedElemRestriction rstr, CeedInt *num_comp);
 CEED_EXTERN int CeedElemRestrictionGetCompStride(CeedElemRestriction rstr, CeedInt *comp_stride);
 CEED_EXTERN int CeedElemRestrictionGetMultiplicity(CeedElemRestriction rstr, CeedVector mult);
+CEED_EXTERN int CeedElemRestrictionGetCeed(CeedElemRestriction rstr, Ceed *ceed);
+CEED_EXTERN Ceed CeedElemRestrictionReturnCeed(CeedElemRestriction rstr);
 CEED_EXTERN int CeedElemRestrictionDestroy(CeedElemRestriction *rstr);
 
 /* ---- CeedBasis (src/dm-utils.c:766-879) ---- */
@@ -176,6 +147,7 @@ CEED_EXTERN int CeedBasisGetNumNodes(CeedBasis basis, CeedInt *P);
 CEED_EXTERN int CeedBasisGetNumNodes1D(CeedBasis basis, CeedInt *P_1d);
 CEED_EXTERN int CeedBasisGetNumQuadraturePoints(CeedBasis basis, CeedInt *Q);
 CEED_EXTERN int CeedBasisGetNumQuadraturePoints1D(CeedBasis basis, CeedInt *Q_1d);
+CEED_EXTERN Ceed CeedBasisReturnCeed(CeedBasis basis);
 CEED_EXTERN int CeedBasisDestroy(CeedBasis *basis);
 CEED_EXTERN int CeedLobattoQuadrature(CeedInt Q, CeedScalar *q_ref_1d, CeedScalar *q_weight_1d);
 CEED_EXTERN int CeedGaussQuadrature(CeedInt Q, CeedScalar *q_ref_1d, CeedScalar *q_weight_1d);
@@ -192,6 +164,7 @@ CEED_EXTERN int CeedQFunctionContextSetDataDestroy(CeedQFunctionContext ctx, Cee
 CEED_EXTERN int CeedQFunctionContextRegisterDouble(CeedQFunctionContext ctx, const char *field_name, size_t field_offset, size_t num_values,
                                                    const char *field_description);
 CEED_EXTERN int CeedQFunctionContextGetContextSize(CeedQFunctionContext ctx, size_t *ctx_size);
+CEED_EXTERN int CeedQFunctionContextReference(CeedQFunctionContext ctx);
 CEED_EXTERN int CeedQFunctionContextDestroy(CeedQFunctionContext *ctx);
 
 /* ---- CeedQFunction (src/setuplibceed.c:209-266, src/qdata.c:153-170) ---- */
@@ -203,6 +176,7 @@ CEED_EXTERN int CeedQFunctionSetContext(CeedQFunction qf, CeedQFunctionContext c
 CEED_EXTERN int CeedQFunctionGetContext(CeedQFunction qf, CeedQFunctionContext *ctx);
 CEED_EXTERN int CeedQFunctionSetUserFlopsEstimate(CeedQFunction qf, CeedSize flops);
 CEED_EXTERN int CeedQFunctionGetKernelName(CeedQFunction qf, const char **kernel_name);
+CEED_EXTERN int CeedQFunctionCreateIdentity(Ceed ceed, CeedInt size, CeedEvalMode in_mode, CeedEvalMode out_mode, CeedQFunction *qf);
 CEED_EXTERN int CeedQFunctionDestroy(CeedQFunction *qf);
 
 /* ---- CeedOperator (src/setuplibceed.c:209-318, src/setupts.c:109, src/mat-ceed.c:1603-1700, src/petsc_ops.c:232-234) ---- */
@@ -227,6 +201,31 @@ CEED_EXTERN int CeedOperatorApplyAdd(CeedOperator op, CeedVector in, CeedVector 
 CEED_EXTERN int CeedOperatorLinearAssembleDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request);
 CEED_EXTERN int CeedOperatorLinearAssembleAddDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request);
 CEED_EXTERN int CeedOperatorGetFlopsEstimate(CeedOperator op, CeedSize *flops);
+CEED_EXTERN int CeedOperatorGetCeed(CeedOperator op, Ceed *ceed);
+CEED_EXTERN Ceed CeedOperatorReturnCeed(CeedOperator op);
+CEED_EXTERN int CeedOperatorIsComposite(CeedOperator op, bool *is_composite);
+CEED_EXTERN int CeedOperatorGetContext(CeedOperator op, CeedQFunctionContext *ctx);
+CEED_EXTERN int CeedOperatorGetFieldByName(CeedOperator op, const char *field_name, CeedOperatorField *op_field);
+CEED_EXTERN int CeedOperatorFieldGetElemRestriction(CeedOperatorField op_field, CeedElemRestriction *rstr);
+CEED_EXTERN int CeedOperatorFieldGetVector(CeedOperatorField op_field, CeedVector *vec);
+CEED_EXTERN int CeedOperatorFieldGetData(CeedOperatorField op_field, const char **field_name, CeedElemRestriction *rstr, CeedBasis *basis,
+                                         CeedVector *vec);
+CEED_EXTERN int CeedOperatorView(CeedOperator op, FILE *stream);
+CEED_EXTERN int CeedOperatorViewTerse(CeedOperator op, FILE *stream);
+CEED_EXTERN int CeedOperatorSetNumViewTabs(CeedOperator op, CeedInt num_tabs);
+CEED_EXTERN int CeedOperatorGetNumViewTabs(CeedOperator op, CeedInt *num_tabs);
+CEED_EXTERN int CeedOperatorSetQFunctionAssemblyDataUpdateNeeded(CeedOperator op, bool needs_data_update);
+/* Full (COO) assembly and point-block diagonals are not provided on /gpu/b200 (assembled matrices are not matrix-free; the
+ * point-block Jacobi preconditioner is listed as next): these return CEED_ERROR_UNSUPPORTED. */
+CEED_EXTERN int CeedOperatorLinearAssembleSymbolic(CeedOperator op, CeedSize *num_entries, CeedInt **rows, CeedInt **cols);
+CEED_EXTERN int CeedOperatorLinearAssemble(CeedOperator op, CeedVector values);
+CEED_EXTERN int CeedOperatorLinearAssembleGetNumEntries(CeedOperator op, CeedSize *num_entries);
+CEED_EXTERN int CeedOperatorLinearAssemblePointBlockDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request);
+CEED_EXTERN int CeedOperatorLinearAssemblePointBlockDiagonalSymbolic(CeedOperator op, CeedSize *num_entries, CeedInt **rows, CeedInt **cols);
+CEED_EXTERN int CeedOperatorGetOperatorAssemblyData(CeedOperator op, CeedOperatorAssemblyData *data);
+CEED_EXTERN int CeedOperatorAssemblyDataGetBases(CeedOperatorAssemblyData data, CeedInt *num_active_bases_in, CeedBasis **active_bases_in,
+                                                 const CeedScalar ***assembled_bases_in, CeedInt *num_active_bases_out,
+                                                 CeedBasis **active_bases_out, const CeedScalar ***assembled_bases_out);
 CEED_EXTERN int CeedOperatorDestroy(CeedOperator *op);
 
 #ifdef __cplusplus
