@@ -274,7 +274,10 @@ def run_gpu(args, rank, world):
         "accuracy": acc,
         "roofline": {"bound": "hbm", "kernel": "k_ifunction (fused IFunction, one launch per colour)", "achieved": achieved_if,
                      "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved_if / pk["hbm_gbs"], "peak_source": pk_kind,
-                     "algorithmic_bytes_per_apply": b_if, "traffic": None,
+                     "algorithmic_bytes_per_apply": b_if, "algorithmic_bytes_per_launch": b_if / op.num_colors,
+                     "traffic": IF_DRAM_BYTES_PER_ELEM * E / op.num_colors,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 4096-element k_ifunction launch "
+                                       "(32^3, P=4 Q=5), scaled by the elements of one launch here",
                      "ijacobian": {"achieved": b_ij / (ms_ij * 1e-3) / 1e9, "frac": b_ij / (ms_ij * 1e-3) / 1e9 / pk["hbm_gbs"]}},
         "e2e": {"value": world * N_L / (ms_e2e * 1e-3) / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": 3 * 8 * N_L, "d2h_bytes_per_step": 2 * 8 * N_L,
                 "api": "CeedVectorSetArray(HOST, USE_POINTER) + CeedOperatorApply x2 + CeedVectorSyncArray(HOST)", "jacobian_rel_l2_vs_kernel": err_e2e},
@@ -285,6 +288,11 @@ def run_gpu(args, rank, world):
         line["cpu_baseline"] = {k: v for k, v in cpu_leg(args.cpu_sample, use_ref=False).items() if k != "seconds_per_step"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# DRAM bytes (read + write) per element of one k_ifunction<4,5> launch, from an ncu capture of a 4,096-element colour
+# launch at 32^3: 90.25 MB read + 28.65 MB written.
+IF_DRAM_BYTES_PER_ELEM = (90.252032e6 + 28.651008e6) / 4096
 
 
 def parity_sample(prob, kern, torch, dev):

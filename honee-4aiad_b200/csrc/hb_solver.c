@@ -1,0 +1,346 @@
+/* hb_solver.c -- implicit time loop on the GPU: BDF1/BDF2 + Newton + right-preconditioned GMRES with a Jacobi
+ * preconditioner, in FP64 or mixed precision.
+ *
+ * This is the caller side of the hot path.  HONEE drives the same operators through PETSc: TSBDF (src/setupts.c:343) calls
+ * IFunction_NS (src/setupts.c:78-125) for the residual F(t, q, alpha q + z), FormIJacobian_NS (src/setupts.c:131-157) sets the
+ * "ijacobian time shift" alpha, KSP (GMRES) applies MatMult_Ceed (src/mat-ceed.c:1643-1700) and PCJacobi uses
+ * MatGetDiagonal_Ceed (src/mat-ceed.c:1603-1634).  PETSc is not part of this project, so the loop is restated here in C on
+ * device buffers with the fused kernels of include/honee_b200.h.
+ *
+ * Mixed precision (the `jacobian_fp32` option): the Newton residual, the Newton update and its norm stay FP64; the IFunction
+ * also writes the stored Jacobian data in FP32, and the Krylov basis, the Jacobian actions and the Jacobi diagonal are FP32
+ * with FP64 accumulation of every inner product.  The Newton iteration converges to the same FP64 residual tolerance; only
+ * the Krylov solve is less exact per step.
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "honee_b200.h"
+
+#define MAXK HB_GMRES_MAX_BASIS
+
+struct HbTimeStepper {
+  const HbElemOp    *op;
+  HbNewtonianContext ctx;
+  const double      *qdata;
+  HbSolverOptions    o;
+  int64_t            n;
+  int                njd, steps_taken;
+  double             t;
+  cudaStream_t       s;
+  /* FP64 state */
+  double *q, *q_prev, *q_prev2, *z, *qdot, *res, *jd64, *d_partial, *d_dots, *scratch;
+  /* Krylov (FP32 or FP64) */
+  void  *V, *w, *zvec, *diag, *jd32, *y_work;
+  float *res32;
+  double *delta;
+};
+
+#define CUCK(x)                                \
+  do {                                         \
+    if ((x) != cudaSuccess) return HB_ERROR_CUDA; \
+  } while (0)
+#define HBCK(x)          \
+  do {                   \
+    int e_ = (x);        \
+    if (e_) return e_;   \
+  } while (0)
+
+void hb_solver_default_options(HbSolverOptions *o) {
+  memset(o, 0, sizeof *o);
+  o->dt            = 1e-5;
+  o->bdf_order     = 2;
+  o->newton_rtol   = 1e-8;
+  o->newton_atol   = 1e-30;
+  o->newton_max_it = 20;
+  o->ksp_rtol      = 1e-5; /* PETSc's KSP default */
+  o->ksp_max_it    = 200;
+  o->gmres_restart = 30;
+  o->pc_jacobi     = 1;
+  o->jacobian_fp32 = 0;
+}
+
+static size_t ksz(const HbTimeStepper *ts) { return ts->o.jacobian_fp32 ? sizeof(float) : sizeof(double); }
+
+int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, const HbSolverOptions *opts, void *stream, HbTimeStepper **out) {
+  *out = NULL;
+  if (!op || !ctx184 || !d_qdata || !opts) return HB_ERROR_INVALID;
+  if (opts->gmres_restart < 1 || opts->gmres_restart + 1 > MAXK || opts->dt <= 0 || (opts->bdf_order != 1 && opts->bdf_order != 2))
+    return HB_ERROR_INVALID;
+  HbTimeStepper *ts = (HbTimeStepper *)calloc(1, sizeof *ts);
+  if (!ts) return HB_ERROR_NOMEM;
+  ts->op = op;
+  memcpy(&ts->ctx, ctx184, sizeof ts->ctx);
+  ts->qdata = d_qdata;
+  ts->o     = *opts;
+  ts->n     = op->l_size;
+  ts->njd   = ts->ctx.idl_enable ? 15 : 14;
+  ts->s     = (cudaStream_t)stream;
+  const size_t nb = sizeof(double) * (size_t)ts->n, Q3 = (size_t)op->Q * op->Q * op->Q, njd = (size_t)ts->njd * op->num_elem * Q3;
+  const int m = ts->o.gmres_restart;
+  int err = 0;
+  err |= cudaMalloc((void **)&ts->q, nb) | cudaMalloc((void **)&ts->q_prev, nb) | cudaMalloc((void **)&ts->q_prev2, nb);
+  err |= cudaMalloc((void **)&ts->z, nb) | cudaMalloc((void **)&ts->qdot, nb) | cudaMalloc((void **)&ts->res, nb) | cudaMalloc((void **)&ts->delta, nb);
+  err |= cudaMalloc((void **)&ts->d_partial, sizeof(double) * 512 * MAXK) | cudaMalloc((void **)&ts->d_dots, sizeof(double) * MAXK);
+  err |= cudaMalloc((void **)&ts->scratch, sizeof(double) * 1024);
+  err |= cudaMalloc(&ts->V, ksz(ts) * (size_t)ts->n * (m + 1)) | cudaMalloc(&ts->w, ksz(ts) * (size_t)ts->n);
+  err |= cudaMalloc(&ts->zvec, ksz(ts) * (size_t)ts->n) | cudaMalloc(&ts->diag, ksz(ts) * (size_t)ts->n);
+  if (ts->o.jacobian_fp32) err |= cudaMalloc(&ts->jd32, sizeof(float) * njd) | cudaMalloc((void **)&ts->res32, sizeof(float) * (size_t)ts->n);
+  else err |= cudaMalloc((void **)&ts->jd64, sizeof(double) * njd);
+  if (err) {
+    hb_ts_destroy(ts);
+    return HB_ERROR_NOMEM;
+  }
+  *out = ts;
+  return HB_SUCCESS;
+}
+
+int hb_ts_destroy(HbTimeStepper *ts) {
+  if (!ts) return HB_SUCCESS;
+  void *p[] = {ts->q, ts->q_prev, ts->q_prev2, ts->z, ts->qdot, ts->res, ts->delta, ts->d_partial, ts->d_dots, ts->scratch,
+               ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64};
+  for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
+    if (p[i]) cudaFree(p[i]);
+  free(ts);
+  return HB_SUCCESS;
+}
+
+int hb_ts_set_state(HbTimeStepper *ts, const double *d_q, double t) {
+  CUCK(cudaMemcpyAsync(ts->q, d_q, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s));
+  ts->t           = t;
+  ts->steps_taken = 0;
+  return HB_SUCCESS;
+}
+
+int hb_ts_get_state(HbTimeStepper *ts, double *d_q, double *t) {
+  CUCK(cudaMemcpyAsync(d_q, ts->q, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s));
+  if (t) *t = ts->t;
+  return HB_SUCCESS;
+}
+
+const void *hb_ts_context(HbTimeStepper *ts) { return &ts->ctx; }
+
+/* ---- small helpers on the Krylov precision ---- */
+static int kv_norm2(HbTimeStepper *ts, const void *x, double *nrm) {
+  double r;
+  if (ts->o.jacobian_fp32) HBCK(hb_vec_reduce_f32((const float *)x, NULL, ts->n, 1, ts->scratch, &r, ts->s));
+  else HBCK(hb_vec_reduce_f64((const double *)x, NULL, ts->n, 1, ts->scratch, &r, ts->s));
+  *nrm = sqrt(r);
+  return HB_SUCCESS;
+}
+static void *kv_col(HbTimeStepper *ts, int j) { return (char *)ts->V + ksz(ts) * (size_t)ts->n * j; }
+static int kv_scale(HbTimeStepper *ts, void *x, double a) {
+  return ts->o.jacobian_fp32 ? hb_vec_scale_f32((float *)x, ts->n, (float)a, ts->s) : hb_vec_scale_f64((double *)x, ts->n, a, ts->s);
+}
+static int kv_copy(HbTimeStepper *ts, void *dst, const void *src) {
+  return cudaMemcpyAsync(dst, src, ksz(ts) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s) == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+/* y = J x (the IJacobian operator at the current linearisation point) */
+static int kv_jac(HbTimeStepper *ts, const void *x, void *y) {
+  if (ts->o.jacobian_fp32) return hb_ijacobian_apply_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (const float *)x, (float *)y, 0, ts->s);
+  return hb_ijacobian_apply_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, (const double *)x, (double *)y, 0, ts->s);
+}
+/* z = M^-1 x (Jacobi) or copy */
+static int kv_pc(HbTimeStepper *ts, const void *x, void *z) {
+  if (!ts->o.pc_jacobi) return kv_copy(ts, z, x);
+  if (ts->o.jacobian_fp32) return hb_vec_pointwise_mult_f32((float *)z, (const float *)ts->diag, (const float *)x, ts->n, ts->s);
+  return hb_vec_pointwise_mult_f64((double *)z, (const double *)ts->diag, (const double *)x, ts->n, ts->s);
+}
+static int kv_multidot(HbTimeStepper *ts, int k, const void *w, double *h) {
+  if (ts->o.jacobian_fp32) HBCK(hb_krylov_multidot_f32((const float *)ts->V, ts->n, k, (const float *)w, ts->n, ts->d_partial, ts->d_dots, ts->s));
+  else HBCK(hb_krylov_multidot_f64((const double *)ts->V, ts->n, k, (const double *)w, ts->n, ts->d_partial, ts->d_dots, ts->s));
+  CUCK(cudaMemcpyAsync(h, ts->d_dots, sizeof(double) * k, cudaMemcpyDeviceToHost, ts->s));
+  CUCK(cudaStreamSynchronize(ts->s));
+  return HB_SUCCESS;
+}
+static int kv_multiaxpy(HbTimeStepper *ts, void *w, int k, const double *c) {
+  if (ts->o.jacobian_fp32) return hb_krylov_multiaxpy_f32((float *)w, (const float *)ts->V, ts->n, k, c, ts->n, ts->s);
+  return hb_krylov_multiaxpy_f64((double *)w, (const double *)ts->V, ts->n, k, c, ts->n, ts->s);
+}
+
+/* Jacobi diagonal at the current linearisation point, stored inverted */
+static int assemble_pc(HbTimeStepper *ts) {
+  if (!ts->o.pc_jacobi) return HB_SUCCESS;
+  if (ts->o.jacobian_fp32) {
+    HBCK(hb_diagonal_assemble_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (float *)ts->diag, 0, ts->s));
+    /* invert in FP64 (delta is free before the Krylov solve), store FP32 */
+    HBCK(hb_vec_f32_to_f64((const float *)ts->diag, ts->delta, ts->n, 0, ts->s));
+    HBCK(hb_vec_reciprocal_f64(ts->delta, ts->n, ts->s));
+    return hb_vec_f64_to_f32(ts->delta, (float *)ts->diag, ts->n, 0, ts->s);
+  }
+  HBCK(hb_diagonal_assemble_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, (double *)ts->diag, 0, ts->s));
+  return hb_vec_reciprocal_f64((double *)ts->diag, ts->n, ts->s);
+}
+
+/* GMRES(m), right preconditioned, classical Gram-Schmidt with one re-orthogonalisation (CGS2); solves J delta = -res
+ * (res FP64) to relative tolerance ksp_rtol.  delta (FP64) receives the solution. */
+static int gmres(HbTimeStepper *ts, int *its_out, double *rnorm_out) {
+  const int m = ts->o.gmres_restart;
+  double    H[MAXK + 1][MAXK], cs[MAXK], sn[MAXK], g[MAXK + 1], hcol[MAXK], h2[MAXK], y[MAXK];
+  int       its = 0;
+  HBCK(hb_vec_set_f64(ts->delta, ts->n, 0.0, ts->s));
+  /* r0 = -res (x0 = 0) */
+  void *v0 = kv_col(ts, 0);
+  if (ts->o.jacobian_fp32) HBCK(hb_vec_f64_to_f32(ts->res, (float *)v0, ts->n, 0, ts->s));
+  else HBCK(cudaMemcpyAsync(v0, ts->res, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s) == cudaSuccess ? 0 : HB_ERROR_CUDA);
+  HBCK(kv_scale(ts, v0, -1.0));
+  double beta0;
+  HBCK(kv_norm2(ts, v0, &beta0));
+  double beta = beta0;
+  if (beta0 == 0) {
+    *its_out   = 0;
+    *rnorm_out = 0;
+    return HB_SUCCESS;
+  }
+  const double target = ts->o.ksp_rtol * beta0;
+  while (its < ts->o.ksp_max_it) {
+    HBCK(kv_scale(ts, kv_col(ts, 0), 1.0 / beta));
+    memset(g, 0, sizeof g);
+    g[0]  = beta;
+    int k = 0;
+    for (; k < m && its < ts->o.ksp_max_it; k++, its++) {
+      HBCK(kv_pc(ts, kv_col(ts, k), ts->zvec));
+      HBCK(kv_jac(ts, ts->zvec, ts->w));
+      /* CGS2 */
+      HBCK(kv_multidot(ts, k + 1, ts->w, hcol));
+      for (int i = 0; i <= k; i++) y[i] = -hcol[i];
+      HBCK(kv_multiaxpy(ts, ts->w, k + 1, y));
+      HBCK(kv_multidot(ts, k + 1, ts->w, h2));
+      for (int i = 0; i <= k; i++) {
+        y[i] = -h2[i];
+        hcol[i] += h2[i];
+      }
+      HBCK(kv_multiaxpy(ts, ts->w, k + 1, y));
+      double hn;
+      HBCK(kv_norm2(ts, ts->w, &hn));
+      for (int i = 0; i <= k; i++) H[i][k] = hcol[i];
+      H[k + 1][k] = hn;
+      if (hn > 0) {
+        HBCK(kv_copy(ts, kv_col(ts, k + 1), ts->w));
+        HBCK(kv_scale(ts, kv_col(ts, k + 1), 1.0 / hn));
+      }
+      /* apply the previous Givens rotations, then a new one */
+      for (int i = 0; i < k; i++) {
+        const double a = H[i][k], b = H[i + 1][k];
+        H[i][k]         = cs[i] * a + sn[i] * b;
+        H[i + 1][k]     = -sn[i] * a + cs[i] * b;
+      }
+      const double a = H[k][k], b = H[k + 1][k], r = hypot(a, b);
+      cs[k]    = r > 0 ? a / r : 1;
+      sn[k]    = r > 0 ? b / r : 0;
+      H[k][k]  = r;
+      H[k + 1][k] = 0;
+      g[k + 1] = -sn[k] * g[k];
+      g[k]     = cs[k] * g[k];
+      if (fabs(g[k + 1]) <= target || hn == 0) {
+        k++;
+        its++;
+        break;
+      }
+    }
+    /* y = H^-1 g (upper triangular k x k) ; delta += M^-1 V y */
+    for (int i = k - 1; i >= 0; i--) {
+      double s = g[i];
+      for (int j = i + 1; j < k; j++) s -= H[i][j] * y[j];
+      y[i] = s / H[i][i];
+    }
+    if (ts->o.jacobian_fp32) {
+      HBCK(hb_vec_set_f32((float *)ts->w, ts->n, 0.0f, ts->s));
+      HBCK(hb_krylov_multiaxpy_f32((float *)ts->w, (const float *)ts->V, ts->n, k, y, ts->n, ts->s));
+      HBCK(kv_pc(ts, ts->w, ts->zvec));
+      HBCK(hb_vec_f32_to_f64((const float *)ts->zvec, ts->delta, ts->n, 1, ts->s));
+    } else {
+      HBCK(hb_vec_set_f64((double *)ts->w, ts->n, 0.0, ts->s));
+      HBCK(hb_krylov_multiaxpy_f64((double *)ts->w, (const double *)ts->V, ts->n, k, y, ts->n, ts->s));
+      HBCK(kv_pc(ts, ts->w, ts->zvec));
+      HBCK(hb_vec_axpy_f64(ts->delta, 1.0, (const double *)ts->zvec, ts->n, ts->s));
+    }
+    beta = fabs(g[k]);
+    if (beta <= target || its >= ts->o.ksp_max_it) break;
+    /* restart: r = -res - J delta, in the Krylov precision */
+    void *r = kv_col(ts, 0);
+    if (ts->o.jacobian_fp32) {
+      HBCK(hb_vec_f64_to_f32(ts->delta, (float *)ts->zvec, ts->n, 0, ts->s));
+      HBCK(kv_jac(ts, ts->zvec, r));
+      HBCK(hb_vec_f64_to_f32(ts->res, (float *)ts->w, ts->n, 0, ts->s));
+      HBCK(hb_vec_axpby_f32((float *)r, -1.0f, -1.0f, (const float *)ts->w, ts->n, ts->s)); /* r = -res - J delta */
+    } else {
+      HBCK(kv_jac(ts, ts->delta, r));
+      HBCK(hb_vec_axpby_f64((double *)r, -1.0, -1.0, ts->res, ts->n, ts->s));
+    }
+    HBCK(kv_norm2(ts, r, &beta));
+  }
+  *its_out   = its;
+  *rnorm_out = beta / beta0;
+  return HB_SUCCESS;
+}
+
+int hb_ts_step(HbTimeStepper *ts, HbStepStats *st) {
+  memset(st, 0, sizeof *st);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, ts->s);
+  const double dt  = ts->o.dt;
+  const int    bdf = (ts->o.bdf_order == 2 && ts->steps_taken >= 1) ? 2 : 1;
+  double       alpha;
+  /* history: q_prev2 <- q_prev, q_prev <- q (the initial Newton guess is the previous state) */
+  if (bdf == 2) CUCK(cudaMemcpyAsync(ts->q_prev2, ts->q_prev, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s));
+  CUCK(cudaMemcpyAsync(ts->q_prev, ts->q, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s));
+  if (bdf == 1) { /* q_dot = (q - q_n)/dt */
+    alpha = 1.0 / dt;
+    HBCK(hb_vec_combine_f64(ts->q_prev, NULL, -1.0 / dt, 0.0, ts->z, ts->n, ts->s));
+  } else { /* q_dot = (3 q - 4 q_n + q_{n-1}) / (2 dt) */
+    alpha = 1.5 / dt;
+    HBCK(hb_vec_combine_f64(ts->q_prev, ts->q_prev2, -2.0 / dt, 0.5 / dt, ts->z, ts->n, ts->s));
+  }
+  ts->ctx.dt                   = dt;
+  ts->ctx.ijacobian_time_shift = alpha;
+  ts->ctx.time                 = ts->t + dt;
+  double r0 = 0, rn = 0;
+  int    it = 0, ksp_total = 0, converged = 0;
+  for (; it <= ts->o.newton_max_it; it++) {
+    HBCK(hb_bdf_qdot(ts->q, ts->z, alpha, ts->qdot, ts->n, ts->s));
+    HbIFunctionIO io = {ts->q, ts->qdot, ts->qdata, ts->o.jacobian_fp32 ? NULL : ts->jd64, ts->o.jacobian_fp32 ? (float *)ts->jd32 : NULL, ts->res, 0};
+    HBCK(hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s));
+    double r2;
+    HBCK(hb_vec_reduce_f64(ts->res, NULL, ts->n, 1, ts->scratch, &r2, ts->s));
+    rn = sqrt(r2);
+    if (it == 0) r0 = rn;
+    if (!isfinite(rn)) {
+      st->converged_reason = -1; /* diverged: non-finite residual (src/setupts.c:232-249 checks for NaN the same way) */
+      break;
+    }
+    if (rn <= ts->o.newton_rtol * r0 || rn <= ts->o.newton_atol) {
+      converged = 1;
+      break;
+    }
+    if (it == ts->o.newton_max_it) break;
+    if (it == 0 || ts->o.pc_every_newton) HBCK(assemble_pc(ts));
+    int    kits;
+    double krel;
+    HBCK(gmres(ts, &kits, &krel));
+    ksp_total += kits;
+    HBCK(hb_vec_axpy_f64(ts->q, 1.0, ts->delta, ts->n, ts->s));
+  }
+  cudaEventRecord(e1, ts->s);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  st->newton_its = it;
+  st->ksp_its    = ksp_total;
+  st->res0       = r0;
+  st->res_final  = rn;
+  st->seconds    = ms * 1e-3;
+  if (st->converged_reason == 0) st->converged_reason = converged ? 1 : -2;
+  ts->t += dt;
+  ts->steps_taken++;
+  int status = 0;
+  HBCK(hb_elemop_status((HbElemOp *)ts->op, &status, 1));
+  return status ? HB_ERROR_BACKEND : HB_SUCCESS;
+}

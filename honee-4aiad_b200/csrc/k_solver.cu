@@ -1,0 +1,328 @@
+// k_solver.cu -- device kernels of the implicit time loop: Krylov block operations (multi-dot, multi-axpy) in FP32 or FP64
+// with FP64 accumulation, the BDF time-derivative update, and the total-kinetic-energy / CFL monitors.
+//
+// Monitors restate qfunctions/monitor_totalkineticenergy.h:8-39 (summed as src/monitor_totalkineticenergy.c:134-163) and
+// qfunctions/monitor_cfl.h:9-46 with numerics.h:24-29 (min/max times dt, src/monitor_cfl.c:140-164).  Reductions are
+// two-stage with fixed block order, so results are deterministic.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "honee_b200.h"
+#include "newtonian_qf.cuh"
+
+namespace {
+
+constexpr int kBS = 256;
+constexpr int kMaxK = HB_GMRES_MAX_BASIS;
+constexpr int kRedBlocks = 512;
+
+inline unsigned nblocks(int64_t n) {
+  const int64_t b = (n + kBS - 1) / kBS;
+  return (unsigned)(b > 148 * 32 ? 148 * 32 : (b < 1 ? 1 : b));
+}
+
+// h[i] = sum_e V[i][e] w[e], i < k; per-block partials [kRedBlocks][kMaxK]
+template <typename T>
+__global__ void __launch_bounds__(kBS) k_multidot(const T *__restrict__ V, int64_t ldv, int k, const T *__restrict__ w, int64_t n, double *partial) {
+  __shared__ double sh[kMaxK][kBS / 32];
+  double acc[kMaxK];
+#pragma unroll
+  for (int i = 0; i < kMaxK; i++) acc[i] = 0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const double we = (double)w[e];
+#pragma unroll
+    for (int i = 0; i < kMaxK; i++)
+      if (i < k) acc[i] += (double)V[i * ldv + e] * we;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < kMaxK; i++) {
+    if (i >= k) break;
+    double v = acc[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[i][warp] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < k; i += blockDim.x) {
+    double s = 0;
+    for (int wi = 0; wi < kBS / 32; wi++) s += sh[i][wi];
+    partial[blockIdx.x * kMaxK + i] = s;
+  }
+}
+
+__global__ void k_multidot_final(const double *partial, int nblk, int k, double *out) {
+  const int i = blockIdx.x;  // one block per output
+  __shared__ double sh[kBS];
+  double s = 0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partial[b * kMaxK + i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && i < k) out[i] = sh[0];
+}
+
+struct Coefs {
+  double c[kMaxK];
+};
+
+// w[e] += sum_{i<k} c[i] V[i][e]
+template <typename T, typename TW>
+__global__ void __launch_bounds__(kBS) k_multiaxpy(TW *__restrict__ w, const T *__restrict__ V, int64_t ldv, int k, Coefs c, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0;
+#pragma unroll
+    for (int i = 0; i < kMaxK; i++)
+      if (i < k) s += c.c[i] * (double)V[i * ldv + e];
+    w[e] = TW((double)w[e] + s);
+  }
+}
+
+// q_dot = alpha q + z
+__global__ void k_bdf_qdot(const double *__restrict__ q, const double *__restrict__ z, double alpha, double *__restrict__ qdot, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) qdot[e] = alpha * q[e] + z[e];
+}
+
+// z = a q1 + b q2 (history combination of the BDF formula)
+__global__ void k_combine(const double *__restrict__ q1, const double *__restrict__ q2, double a, double b, double *__restrict__ z, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    z[e] = a * q1[e] + (q2 ? b * q2[e] : 0.0);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Monitors: one CTA per element (not a hot path), direct tensor evaluation of q and its reference gradient at each point.
+
+struct MonBasis {
+  double B[HB_MAX_P * HB_MAX_P], G[HB_MAX_P * HB_MAX_P];
+};
+
+__device__ void eval_point(const double *sN, int P, int Q, const MonBasis &b, int qp, double qi[5], double gref[3][5]) {
+  const int i = qp % Q, j = (qp / Q) % Q, k = qp / (Q * Q);
+  for (int c = 0; c < 5; c++) {
+    qi[c] = 0;
+    gref[0][c] = gref[1][c] = gref[2][c] = 0;
+  }
+  for (int pc = 0; pc < P; pc++)
+    for (int pb = 0; pb < P; pb++)
+      for (int pa = 0; pa < P; pa++) {
+        const int p = (pc * P + pb) * P + pa;
+        const double bx = b.B[i * P + pa], by = b.B[j * P + pb], bz = b.B[k * P + pc];
+        const double gx = b.G[i * P + pa], gy = b.G[j * P + pb], gz = b.G[k * P + pc];
+        for (int c = 0; c < 5; c++) {
+          const double u = sN[p * 5 + c];
+          qi[c] += bx * by * bz * u;
+          gref[0][c] += gx * by * bz * u;
+          gref[1][c] += bx * gy * bz * u;
+          gref[2][c] += bx * by * gz * u;
+        }
+      }
+}
+
+// per-element partial sums of the five kinetic-energy integrands [num_elem][5]
+__global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, const double *__restrict__ q, const double *__restrict__ qdata,
+                             hb::PhysConst<double> pc, MonBasis b, double *__restrict__ elem_sums) {
+  extern __shared__ double sm[];
+  const int e = blockIdx.x, P3 = P * P * P, Q3 = Q * Q * Q;
+  double *sN = sm, *red = sm + 5 * P3;
+  for (int t = threadIdx.x; t < 5 * P3; t += blockDim.x) sN[t] = q[offsets[(int64_t)e * P3 + t / 5] + t % 5];
+  __syncthreads();
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int qp = threadIdx.x; qp < Q3; qp += blockDim.x) {
+    double qi[5], gref[3][5], X[3][3];
+    eval_point(sN, P, Q, b, qp, qi, gref);
+    const double *qd = qdata + (int64_t)e * 10 * Q3;
+    const double wdetJ = qd[qp];
+    for (int kk = 0; kk < 9; kk++) X[kk / 3][kk % 3] = qd[(1 + kk) * Q3 + qp];
+    hb::St<double> s;
+    double inv_rho, etot, eint;
+    hb::state_from_u(pc, qi, s, inv_rho, etot, eint);
+    hb::St<double> gs[3];
+    hb::physical_gradient(pc, s, inv_rho, etot, eint, gref, X, gs);
+    double e6[6], S[3][3];
+    hb::km_strain(gs, e6);
+    const double w = 1.0 / 1.4142135623730951;
+    S[0][0] = e6[0];
+    S[1][1] = e6[1];
+    S[2][2] = e6[2];
+    S[1][2] = S[2][1] = w * e6[3];
+    S[0][2] = S[2][0] = w * e6[4];
+    S[0][1] = S[1][0] = w * e6[5];
+    const double div = e6[0] + e6[1] + e6[2];
+    double SS = 0;
+    for (int a = 0; a < 3; a++)
+      for (int c = 0; c < 3; c++) SS += S[a][c] * S[a][c];
+    const double w0 = gs[2].u[1] - gs[1].u[2], w1 = gs[0].u[2] - gs[2].u[0], w2 = gs[1].u[0] - gs[0].u[1];
+    acc[0] += wdetJ * 0.5 * s.rho * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]);
+    acc[1] += wdetJ * -2 * pc.mu * SS;
+    acc[2] += wdetJ * -pc.lambda * pc.mu * div * div;
+    acc[3] += wdetJ * s.P * div;
+    acc[4] += wdetJ * pc.mu * (w0 * w0 + w1 * w1 + w2 * w2);
+  }
+  for (int c = 0; c < 5; c++) red[c * blockDim.x + threadIdx.x] = acc[c];
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double s = 0;
+    for (int t = 0; t < (int)blockDim.x; t++) s += red[threadIdx.x * blockDim.x + t];
+    elem_sums[(int64_t)e * 5 + threadIdx.x] = s;
+  }
+}
+
+// per-element min/max over points of sqrt(u . g u) with g = 0.25 dXdx^T dXdx
+__global__ void k_monitor_cfl(int P, int Q, const int32_t *__restrict__ offsets, const double *__restrict__ q, const double *__restrict__ qdata,
+                              hb::PhysConst<double> pc, MonBasis b, double *__restrict__ elem_minmax) {
+  extern __shared__ double sm[];
+  const int e = blockIdx.x, P3 = P * P * P, Q3 = Q * Q * Q;
+  double *sN = sm, *red = sm + 5 * P3;
+  for (int t = threadIdx.x; t < 5 * P3; t += blockDim.x) sN[t] = q[offsets[(int64_t)e * P3 + t / 5] + t % 5];
+  __syncthreads();
+  double mn = 1e300, mx = -1e300;
+  for (int qp = threadIdx.x; qp < Q3; qp += blockDim.x) {
+    double qi[5], gref[3][5], X[3][3], g[3][3];
+    eval_point(sN, P, Q, b, qp, qi, gref);
+    const double *qd = qdata + (int64_t)e * 10 * Q3;
+    for (int kk = 0; kk < 9; kk++) X[kk / 3][kk % 3] = qd[(1 + kk) * Q3 + qp];
+    hb::St<double> s;
+    double inv_rho, etot, eint;
+    hb::state_from_u(pc, qi, s, inv_rho, etot, eint);
+    for (int a = 0; a < 3; a++)
+      for (int c = 0; c < 3; c++) g[a][c] = 0.25 * (X[0][a] * X[0][c] + X[1][a] * X[1][c] + X[2][a] * X[2][c]);
+    double ugu = 0;
+    for (int a = 0; a < 3; a++) ugu += s.u[a] * (g[a][0] * s.u[0] + g[a][1] * s.u[1] + g[a][2] * s.u[2]);
+    const double cfl = sqrt(ugu);
+    mn = fmin(mn, cfl);
+    mx = fmax(mx, cfl);
+  }
+  red[threadIdx.x] = mn;
+  red[blockDim.x + threadIdx.x] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 1e300, c = -1e300;
+    for (int t = 0; t < (int)blockDim.x; t++) {
+      a = fmin(a, red[t]);
+      c = fmax(c, red[blockDim.x + t]);
+    }
+    elem_minmax[(int64_t)e * 2] = a;
+    elem_minmax[(int64_t)e * 2 + 1] = c;
+  }
+}
+
+inline int rc() { return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA; }
+
+}  // namespace
+
+extern "C" {
+
+int hb_krylov_multidot_f64(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_partial, double *d_out, void *s) {
+  if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
+  k_multidot<double><<<kRedBlocks, kBS, 0, (cudaStream_t)s>>>(V, ldv, k, w, n, d_partial);
+  k_multidot_final<<<k, kBS, 0, (cudaStream_t)s>>>(d_partial, kRedBlocks, k, d_out);
+  return rc();
+}
+int hb_krylov_multidot_f32(const float *V, int64_t ldv, int k, const float *w, int64_t n, double *d_partial, double *d_out, void *s) {
+  if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
+  k_multidot<float><<<kRedBlocks, kBS, 0, (cudaStream_t)s>>>(V, ldv, k, w, n, d_partial);
+  k_multidot_final<<<k, kBS, 0, (cudaStream_t)s>>>(d_partial, kRedBlocks, k, d_out);
+  return rc();
+}
+int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, const double *c, int64_t n, void *s) {
+  if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
+  Coefs cf;
+  memset(&cf, 0, sizeof cf);
+  memcpy(cf.c, c, sizeof(double) * k);
+  k_multiaxpy<double, double><<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, V, ldv, k, cf, n);
+  return rc();
+}
+int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s) {
+  if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
+  Coefs cf;
+  memset(&cf, 0, sizeof cf);
+  memcpy(cf.c, c, sizeof(double) * k);
+  k_multiaxpy<float, float><<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, V, ldv, k, cf, n);
+  return rc();
+}
+int hb_krylov_multiaxpy_f32_to_f64(double *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s) {
+  if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
+  Coefs cf;
+  memset(&cf, 0, sizeof cf);
+  memcpy(cf.c, c, sizeof(double) * k);
+  k_multiaxpy<float, double><<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, V, ldv, k, cf, n);
+  return rc();
+}
+int hb_bdf_qdot(const double *q, const double *z, double alpha, double *qdot, int64_t n, void *s) {
+  k_bdf_qdot<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(q, z, alpha, qdot, n);
+  return rc();
+}
+int hb_vec_combine_f64(const double *q1, const double *q2, double a, double b, double *z, int64_t n, void *s) {
+  k_combine<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(q1, q2, a, b, z, n);
+  return rc();
+}
+
+static hb::PhysConst<double> phys_of(const void *ctx184) {
+  HbNewtonianContext c;
+  memcpy(&c, ctx184, sizeof c);
+  hb::PhysConst<double> p;
+  memset(&p, 0, sizeof p);
+  p.mu = c.gas.mu;
+  p.lambda = c.gas.lambda;
+  p.k = c.gas.k;
+  p.cv = c.gas.cv;
+  p.inv_cv = 1.0 / c.gas.cv;
+  p.gm1 = c.gas.cp / c.gas.cv - 1;
+  p.Rgas = c.gas.cp - c.gas.cv;
+  return p;
+}
+
+static MonBasis mon_basis(const HbElemOp *op) {
+  MonBasis b;
+  memset(&b, 0, sizeof b);
+  memcpy(b.B, op->interp1d, sizeof(double) * op->P * op->Q);
+  memcpy(b.G, op->grad1d, sizeof(double) * op->P * op->Q);
+  return b;
+}
+
+// Kinetic-energy monitor sums (not divided by the volume); d_scratch >= 5 * num_elem doubles; synchronises the stream.
+int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *d_scratch, double sums[5], void *s) {
+  const int P3 = op->P * op->P * op->P;
+  const int nt = 128;
+  const size_t sm = sizeof(double) * (5 * P3 + 5 * nt);
+  k_monitor_ke<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), mon_basis(op), d_scratch);
+  if (rc()) return HB_ERROR_CUDA;
+  double *h = (double *)malloc(sizeof(double) * 5 * (size_t)op->num_elem);
+  if (!h) return HB_ERROR_NOMEM;
+  int err = cudaMemcpyAsync(h, d_scratch, sizeof(double) * 5 * (size_t)op->num_elem, cudaMemcpyDeviceToHost, (cudaStream_t)s) != cudaSuccess ||
+            cudaStreamSynchronize((cudaStream_t)s) != cudaSuccess;
+  for (int c = 0; c < 5; c++) sums[c] = 0;
+  for (int64_t e = 0; e < op->num_elem; e++)
+    for (int c = 0; c < 5; c++) sums[c] += h[e * 5 + c];
+  free(h);
+  return err ? HB_ERROR_CUDA : HB_SUCCESS;
+}
+
+// CFL monitor: min and max over points of dt * sqrt(u . g u); d_scratch >= 2 * num_elem doubles; synchronises.
+int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double dt, double *d_scratch, double minmax[2],
+                   void *s) {
+  const int P3 = op->P * op->P * op->P;
+  const int nt = 128;
+  const size_t sm = sizeof(double) * (5 * P3 + 2 * nt);
+  k_monitor_cfl<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), mon_basis(op), d_scratch);
+  if (rc()) return HB_ERROR_CUDA;
+  double *h = (double *)malloc(sizeof(double) * 2 * (size_t)op->num_elem);
+  if (!h) return HB_ERROR_NOMEM;
+  int err = cudaMemcpyAsync(h, d_scratch, sizeof(double) * 2 * (size_t)op->num_elem, cudaMemcpyDeviceToHost, (cudaStream_t)s) != cudaSuccess ||
+            cudaStreamSynchronize((cudaStream_t)s) != cudaSuccess;
+  double mn = 1e300, mx = -1e300;
+  for (int64_t e = 0; e < op->num_elem; e++) {
+    mn = fmin(mn, h[2 * e]);
+    mx = fmax(mx, h[2 * e + 1]);
+  }
+  free(h);
+  minmax[0] = mn * dt;
+  minmax[1] = mx * dt;
+  return err ? HB_ERROR_CUDA : HB_SUCCESS;
+}
+
+}  // extern "C"

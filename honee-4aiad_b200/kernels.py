@@ -19,7 +19,7 @@ class HbElemOp(C.Structure):
                 ("num_colors", C.c_int), ("h_color_ptr", C.POINTER(C.c_int32)), ("d_color_elem", C.c_void_p),
                 ("interp1d", C.c_double * 64), ("grad1d", C.c_double * 64), ("colo_grad1d", C.c_double * 64),
                 ("qref1d", C.c_double * 8), ("qweight1d", C.c_double * 8), ("d_x_elem", C.c_void_p), ("num_sms", C.c_int),
-                ("device", C.c_int)]
+                ("device", C.c_int), ("d_status", C.c_void_p)]
 
 
 class HbIFunctionIO(C.Structure):

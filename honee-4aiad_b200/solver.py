@@ -1,0 +1,105 @@
+"""ctypes binding of the implicit time loop (hb_ts_* in include/honee_b200.h) and the device monitors.
+
+The loop restates what HONEE asks of PETSc for the Newtonian problem (TSBDF, SNES Newton, KSP GMRES, PC Jacobi:
+src/setupts.c:333-480) on device buffers: every residual is the fused IFunction, every Krylov product the fused IJacobian,
+the preconditioner the fused diagonal.  `jacobian_fp32=True` selects the mixed-precision solve (FP32 Krylov basis,
+Jacobian data and diagonal; FP64 residual, update and inner-product accumulation).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import lib as _load
+from .kernels import _addr, _chk, _stream
+
+
+class HbSolverOptions(C.Structure):
+    _fields_ = [("dt", C.c_double), ("bdf_order", C.c_int), ("newton_rtol", C.c_double), ("newton_atol", C.c_double),
+                ("newton_max_it", C.c_int), ("ksp_rtol", C.c_double), ("ksp_max_it", C.c_int), ("gmres_restart", C.c_int),
+                ("pc_jacobi", C.c_int), ("pc_every_newton", C.c_int), ("jacobian_fp32", C.c_int)]
+
+
+class HbStepStats(C.Structure):
+    _fields_ = [("newton_its", C.c_int), ("ksp_its", C.c_int), ("converged_reason", C.c_int), ("res0", C.c_double),
+                ("res_final", C.c_double), ("seconds", C.c_double)]
+
+
+@dataclass
+class StepStats:
+    newton_its: int
+    ksp_its: int
+    converged_reason: int
+    res0: float
+    res_final: float
+    seconds: float
+
+
+def default_options(**kw) -> HbSolverOptions:
+    o = HbSolverOptions()
+    _load().hb_solver_default_options(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class TimeStepper:
+    """BDF time stepper over one ElemOp (kernels.ElemOp); device state is a torch tensor or a raw device address."""
+
+    def __init__(self, elemop, ctx_bytes: bytes, qdata, options: HbSolverOptions | None = None, stream=None, **kw):
+        L = _load()
+        self.options = options if options is not None else default_options(**kw)
+        self._ctx = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        self._op = elemop  # keeps the element operator alive
+        self._stream = _stream(stream)
+        self.ptr = C.c_void_p()
+        _chk(L.hb_ts_create(elemop.ptr, self._ctx, _addr(qdata), C.byref(self.options), self._stream, C.byref(self.ptr)), "hb_ts_create")
+
+    def set_state(self, q, t=0.0):
+        _chk(_load().hb_ts_set_state(self.ptr, _addr(q), C.c_double(t)), "hb_ts_set_state")
+
+    def get_state(self, q) -> float:
+        t = C.c_double()
+        _chk(_load().hb_ts_get_state(self.ptr, _addr(q), C.byref(t)), "hb_ts_get_state")
+        return t.value
+
+    def step(self) -> StepStats:
+        s = HbStepStats()
+        _chk(_load().hb_ts_step(self.ptr, C.byref(s)), "hb_ts_step")
+        return StepStats(s.newton_its, s.ksp_its, s.converged_reason, s.res0, s.res_final, s.seconds)
+
+    def context_bytes(self) -> bytes:
+        L = _load()
+        L.hb_ts_context.restype = C.c_void_p
+        return C.string_at(L.hb_ts_context(self.ptr), len(self._ctx))
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                _load().hb_ts_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+
+def monitor_ke(elemop, ctx_bytes: bytes, q, qdata, scratch, stream=None) -> np.ndarray:
+    """Kinetic-energy integrand sums (TotalKineticEnergy, StrainDissipation, DivergenceDissipation, VolumeExpansion,
+    MuVorticity2), not yet divided by the domain volume.  scratch: >= 5 * num_elem doubles on the device."""
+    sums = np.zeros(5)
+    cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+    _chk(_load().hb_monitor_ke(elemop.ptr, cb, _addr(q), _addr(qdata), _addr(scratch), sums.ctypes.data_as(C.POINTER(C.c_double)),
+                               _stream(stream)), "hb_monitor_ke")
+    return sums
+
+
+def monitor_cfl(elemop, ctx_bytes: bytes, q, qdata, dt, scratch, stream=None) -> tuple[float, float]:
+    """(min, max) over quadrature points of dt * sqrt(u . g u), g = 0.25 dXdx^T dXdx.  scratch: >= 2 * num_elem doubles."""
+    mm = np.zeros(2)
+    cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+    _chk(_load().hb_monitor_cfl(elemop.ptr, cb, _addr(q), _addr(qdata), C.c_double(dt), _addr(scratch),
+                                mm.ctypes.data_as(C.POINTER(C.c_double)), _stream(stream)), "hb_monitor_cfl")
+    return float(mm[0]), float(mm[1])

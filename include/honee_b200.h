@@ -132,6 +132,55 @@ HB_EXPORT int hb_restrict_apply_t_strided(int num_elem, int esize, int ncomp, co
 HB_EXPORT int hb_basis_apply_generic(int num_elem, int ncomp, int dim, int P, int Q, int tmode, int emode, const double *d_B, const double *d_G,
                            const double *d_w, const double *u, double *v, void *s);
 
+/* ---- Implicit time loop (the caller of the hot path; PETSc TSBDF + SNES + KSP GMRES + PCJacobi in HONEE,
+ *      src/setupts.c:78-157, :333-480; src/mat-ceed.c:1603-1700) ---- */
+#define HB_GMRES_MAX_BASIS 32
+
+typedef struct {
+  double dt;              /* time step */
+  int    bdf_order;       /* 1 or 2 (the first step of BDF2 is BDF1, as TSBDF starts) */
+  double newton_rtol, newton_atol;
+  int    newton_max_it;
+  double ksp_rtol;        /* GMRES relative tolerance */
+  int    ksp_max_it, gmres_restart;
+  int    pc_jacobi;       /* 1: Jacobi from the assembled diagonal, 0: none */
+  int    pc_every_newton; /* 0: diagonal once per time step (lagged), 1: every Newton iteration */
+  int    jacobian_fp32;   /* mixed precision: FP32 Krylov basis, Jacobian action and diagonal; FP64 residual and update */
+} HbSolverOptions;
+
+typedef struct {
+  int    newton_its, ksp_its, converged_reason; /* 1 converged, -1 non-finite residual, -2 iteration limit */
+  double res0, res_final, seconds;
+} HbStepStats;
+
+typedef struct HbTimeStepper HbTimeStepper;
+
+HB_EXPORT void hb_solver_default_options(HbSolverOptions *o);
+/* ctx184 is copied; its dt / ijacobian_time_shift / time fields are set every step like HONEE's context labels. */
+HB_EXPORT int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, const HbSolverOptions *opts, void *stream,
+                           HbTimeStepper **ts);
+HB_EXPORT int hb_ts_set_state(HbTimeStepper *ts, const double *d_q, double t);
+HB_EXPORT int hb_ts_get_state(HbTimeStepper *ts, double *d_q, double *t);
+HB_EXPORT int hb_ts_step(HbTimeStepper *ts, HbStepStats *stats);
+HB_EXPORT const void *hb_ts_context(HbTimeStepper *ts);
+HB_EXPORT int hb_ts_destroy(HbTimeStepper *ts);
+
+/* Krylov block operations (FP64 accumulation): out[i] = V_i . w for i < k (d_partial: 512*HB_GMRES_MAX_BASIS doubles),
+ * w += sum_i c_i V_i */
+HB_EXPORT int hb_krylov_multidot_f64(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_partial, double *d_out, void *s);
+HB_EXPORT int hb_krylov_multidot_f32(const float *V, int64_t ldv, int k, const float *w, int64_t n, double *d_partial, double *d_out, void *s);
+HB_EXPORT int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
+HB_EXPORT int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
+HB_EXPORT int hb_krylov_multiaxpy_f32_to_f64(double *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
+HB_EXPORT int hb_bdf_qdot(const double *q, const double *z, double alpha, double *qdot, int64_t n, void *s);
+HB_EXPORT int hb_vec_combine_f64(const double *q1, const double *q2, double a, double b, double *z, int64_t n, void *s);
+
+/* Monitors (src/monitor_totalkineticenergy.c:134-163, src/monitor_cfl.c:140-164): kinetic-energy integrand sums (not divided
+ * by the volume; d_scratch >= 5*num_elem doubles) and dt * min/max CFL (d_scratch >= 2*num_elem doubles).  Synchronise. */
+HB_EXPORT int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *d_scratch, double sums[5], void *s);
+HB_EXPORT int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double dt, double *d_scratch,
+                             double minmax[2], void *s);
+
 /* Library identification */
 const char *hb_version(void);
 

@@ -74,3 +74,20 @@ def test_elemop_rejects_out_of_range_offsets(hb, prob):
     code = L.hb_elemop_create(1, 2, 2, bad.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int64(mesh.l_size), kern._dp(basis.interp1d),
                               kern._dp(basis.grad1d), kern._dp(basis.qref1d), kern._dp(basis.qweight1d), C.byref(p))
     assert code == -4 and not p  # HB_ERROR_INVALID, nothing allocated
+
+
+def test_solver_options_defaults_and_validation_on_host():
+    """Defaults mirror the PETSc settings HONEE's BDF runs use; invalid options are refused before any device work."""
+    import ctypes as C
+    S = importlib.import_module("honee-4aiad_b200.solver")
+    K = importlib.import_module("honee-4aiad_b200.kernels")
+    o = S.default_options()
+    assert o.bdf_order == 2 and o.ksp_rtol == 1e-5 and o.gmres_restart == 30 and o.pc_jacobi == 1 and o.jacobian_fp32 == 0
+    L = importlib.import_module("honee-4aiad_b200").lib()
+    fake = K.HbElemOp()
+    ctx = C.create_string_buffer(184)
+    ts = C.c_void_p()
+    for bad in (dict(gmres_restart=0), dict(gmres_restart=32), dict(bdf_order=3), dict(dt=0.0)):
+        ob = S.default_options(**bad)
+        assert L.hb_ts_create(C.byref(fake), ctx, C.c_void_p(16), C.byref(ob), None, C.byref(ts)) == -4, bad
+        assert not ts.value
