@@ -229,17 +229,26 @@ def box_mesh(n, P, periodic=(False, False, False), lo=(0., 0., 0.), hi=(1., 1., 
         x_elem[:, 2, v] = planes[2][ez + vc]
     m = BoxMesh(n, P, periodic, np.asarray(planes[0]), np.asarray(planes[1]), np.asarray(planes[2]), E, num_nodes, offsets,
                 x_elem.reshape(-1), None, N)
-    m.colors = parity_colors(n)
+    m.colors = parity_colors(n, periodic)
     return m
 
 
-def parity_colors(n):
-    """2x2x2 parity colouring of a lexicographic box: elements of one colour share no node (needs even counts when periodic)."""
+def parity_colors(n, periodic=(False, False, False)):
+    """Parity colouring of a lexicographic box: elements of one colour share no node.  Per direction the colour is the
+    element index mod 2; along a periodic direction with an odd element count the last element touches the first, so it
+    takes a third colour there (up to 3x3x3 classes)."""
     ex, ey, ez = np.meshgrid(np.arange(n[0]), np.arange(n[1]), np.arange(n[2]), indexing="ij")
-    ex, ey, ez = (a.transpose(2, 1, 0).reshape(-1) for a in (ex, ey, ez))
-    color = (ex % 2) + 2 * (ey % 2) + 4 * (ez % 2)
+    idx = [a.transpose(2, 1, 0).reshape(-1) for a in (ex, ey, ez)]
+    per = []
+    for d in range(3):
+        c = idx[d] % 2
+        if periodic[d] and n[d] % 2 == 1 and n[d] > 1:
+            c = np.where(idx[d] == n[d] - 1, 2, c)
+        per.append(c)
+    color = per[0] + 3 * (per[1] + 3 * per[2])
+    _, color = np.unique(color, return_inverse=True)
     order = np.argsort(color, kind="stable").astype(np.int32)
-    counts = np.bincount(color, minlength=8)
+    counts = np.bincount(color)
     ptr_ = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
     return ptr_, order
 

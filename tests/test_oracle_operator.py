@@ -140,3 +140,17 @@ def test_diagonal_matches_brute_force():
         e = np.zeros(mesh.l_size); e[i] = 1
         brute[i] = O.apply_ijacobian(m, cb, e, qdata, jd)[i]
     assert rel_l2(d, brute) < 1e-13
+
+
+@pytest.mark.parametrize("n,periodic", [((5, 5, 5), (1, 1, 1)), ((3, 4, 5), (1, 0, 1)), ((2, 3, 2), (0, 0, 0)), ((4, 4, 4), (1, 1, 1))])
+def test_box_colouring_is_conflict_free(n, periodic):
+    """The oracle's threaded scatter relies on the colouring: elements of one colour share no L-vector node."""
+    mesh = prob.box_mesh(n, 3, periodic=periodic)
+    ptr_, order = mesh.colors
+    off = mesh.offsets.reshape(mesh.num_elem, -1)
+    assert sorted(order.tolist()) == list(range(mesh.num_elem))
+    for c in range(len(ptr_) - 1):
+        nodes = off[order[ptr_[c]:ptr_[c + 1]]]
+        per_elem = [np.unique(r) for r in nodes]
+        allnodes = np.concatenate(per_elem)
+        assert len(np.unique(allnodes)) == len(allnodes), (c, n, periodic)
