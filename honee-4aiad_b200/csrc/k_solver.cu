@@ -5,6 +5,8 @@
 // qfunctions/monitor_cfl.h:9-46 with numerics.h:24-29 (min/max times dt, src/monitor_cfl.c:140-164).  Reductions are
 // two-stage with fixed block order, so results are deterministic.
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -214,6 +216,36 @@ inline int rc() { return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERR
 
 }  // namespace
 
+// ---------------------------------------------------------------------------------------------------------------------
+// Fixed device scratch for hb_krylov_multidot_f64_static: the per-block partial sums of k_multidot, [kRedBlocks][kMaxK]
+// doubles = 512 x 32 x 8 B = 128 KiB, the most any k <= HB_GMRES_MAX_BASIS needs.  Every entry the final pass reads is
+// written earlier in the same call by k_multidot, so nothing in it has to start at zero.  One copy per device and per
+// loaded module: calls that overlap on one device (two streams, or two host threads without ordering) race on it.
+static __device__ __align__(256) double g_multidot_scratch[kRedBlocks * kMaxK];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::atomic<double *> g_multidot_scratch_addr[kMaxDevices];
+
+// Address of g_multidot_scratch on the current device, looked up once per device (with that device current) on the first
+// call there.  The lookup may load this module on the device, so the first call on each device belongs before any
+// stream capture starts.
+int multidot_scratch(double **p) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return HB_ERROR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return HB_ERROR_UNSUPPORTED;
+  double *a = g_multidot_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!a) {
+    void *sym = nullptr;
+    if (cudaGetSymbolAddress(&sym, g_multidot_scratch) != cudaSuccess || !sym) return HB_ERROR_CUDA;
+    a = (double *)sym;
+    g_multidot_scratch_addr[dev].store(a, std::memory_order_release);
+  }
+  *p = a;
+  return HB_SUCCESS;
+}
+}  // namespace
+
 extern "C" {
 
 int hb_krylov_multidot_f64(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_partial, double *d_out, void *s) {
@@ -226,6 +258,22 @@ int hb_krylov_multidot_f32(const float *V, int64_t ldv, int k, const float *w, i
   if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
   k_multidot<float><<<kRedBlocks, kBS, 0, (cudaStream_t)s>>>(V, ldv, k, w, n, d_partial);
   k_multidot_final<<<k, kBS, 0, (cudaStream_t)s>>>(d_partial, kRedBlocks, k, d_out);
+  return rc();
+}
+
+// hb_krylov_multidot_f64 without the caller's partial-sum buffer: the same two kernels, with the partials in the fixed
+// device scratch above.  For callers that have no device work buffer to give and must not create one per call: an inner
+// product requested through a vector-library callback that carries only the vectors (a cudaMalloc/cudaFree pair there
+// would synchronise the whole device on every Krylov iteration), or a solver that commits all device memory to its Krylov
+// basis at set-up and allocates nothing afterwards.  k above HB_GMRES_MAX_BASIS would need more partials than the scratch
+// holds and is refused with HB_ERROR_INVALID before anything is launched.
+int hb_krylov_multidot_f64_static(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_out, void *s) {
+  if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
+  double *partial = nullptr;
+  const int e = multidot_scratch(&partial);
+  if (e) return e;
+  k_multidot<double><<<kRedBlocks, kBS, 0, (cudaStream_t)s>>>(V, ldv, k, w, n, partial);
+  k_multidot_final<<<k, kBS, 0, (cudaStream_t)s>>>(partial, kRedBlocks, k, d_out);
   return rc();
 }
 int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, const double *c, int64_t n, void *s) {

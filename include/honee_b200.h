@@ -169,6 +169,13 @@ HB_EXPORT int hb_ts_destroy(HbTimeStepper *ts);
  * w += sum_i c_i V_i */
 HB_EXPORT int hb_krylov_multidot_f64(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_partial, double *d_out, void *s);
 HB_EXPORT int hb_krylov_multidot_f32(const float *V, int64_t ldv, int k, const float *w, int64_t n, double *d_partial, double *d_out, void *s);
+/* hb_krylov_multidot_f64 that allocates nothing and takes no work buffer: the partial sums live in a fixed 128 KiB device
+ * array inside this library (room for k <= HB_GMRES_MAX_BASIS; larger k returns HB_ERROR_INVALID, nothing launched).
+ * No counterpart in the reference (PETSc's VecMDot owns its work space); it exists for callers that cannot hand over a
+ * device buffer, such as a vector-library inner-product callback.  The first call on each device looks the array up
+ * and belongs before any stream capture; calls that overlap on one device (different streams or host threads) race on
+ * the shared array and must be serialised by the caller. */
+HB_EXPORT int hb_krylov_multidot_f64_static(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_out, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f32_to_f64(double *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
