@@ -61,6 +61,7 @@ void hb_solver_default_options(HbSolverOptions *o) {
   o->gmres_restart = 30;
   o->pc_jacobi     = 1;
   o->jacobian_fp32 = 0;
+  o->cgs_refine    = 0; /* KSPGMRESSetCGSRefinementType default: never */
 }
 
 static size_t ksz(const HbTimeStepper *ts) { return ts->o.jacobian_fp32 ? sizeof(float) : sizeof(double); }
@@ -175,7 +176,8 @@ static int assemble_pc(HbTimeStepper *ts) {
   return hb_vec_reciprocal_f64((double *)ts->diag, ts->n, ts->s);
 }
 
-/* GMRES(m), right preconditioned, classical Gram-Schmidt with one re-orthogonalisation (CGS2); solves J delta = -res
+/* GMRES(m), right preconditioned, classical Gram-Schmidt (PETSc's KSPGMRES default, refinement "never") or CGS2 with
+ * `cgs_refine`; solves J delta = -res
  * (res FP64) to relative tolerance ksp_rtol.  delta (FP64) receives the solution. */
 static int gmres(HbTimeStepper *ts, int *its_out, double *rnorm_out) {
   const int m = ts->o.gmres_restart;
@@ -204,16 +206,18 @@ static int gmres(HbTimeStepper *ts, int *its_out, double *rnorm_out) {
     for (; k < m && its < ts->o.ksp_max_it; k++, its++) {
       HBCK(kv_pc(ts, kv_col(ts, k), ts->zvec));
       HBCK(kv_jac(ts, ts->zvec, ts->w));
-      /* CGS2 */
+      /* classical Gram-Schmidt, optionally with one refinement pass (CGS2) */
       HBCK(kv_multidot(ts, k + 1, ts->w, hcol));
       for (int i = 0; i <= k; i++) y[i] = -hcol[i];
       HBCK(kv_multiaxpy(ts, ts->w, k + 1, y));
-      HBCK(kv_multidot(ts, k + 1, ts->w, h2));
-      for (int i = 0; i <= k; i++) {
-        y[i] = -h2[i];
-        hcol[i] += h2[i];
+      if (ts->o.cgs_refine) {
+        HBCK(kv_multidot(ts, k + 1, ts->w, h2));
+        for (int i = 0; i <= k; i++) {
+          y[i] = -h2[i];
+          hcol[i] += h2[i];
+        }
+        HBCK(kv_multiaxpy(ts, ts->w, k + 1, y));
       }
-      HBCK(kv_multiaxpy(ts, ts->w, k + 1, y));
       double hn;
       HBCK(kv_norm2(ts, ts->w, &hn));
       for (int i = 0; i <= k; i++) H[i][k] = hcol[i];

@@ -55,8 +55,11 @@ template <typename T>
 __host__ __device__ constexpr int nthreads_for(int Q) {
   return ((Q * Q * Q + 31) / 32) * 32;
 }
-// resident CTAs per SM the register budget is tuned for (65536 registers / (threads * CTAs))
-__host__ __device__ constexpr int min_blocks_for(int Q, bool staged = true) { return Q <= 5 ? (staged ? 3 : 4) : (Q == 6 ? 2 : 1); }
+// resident CTAs per SM the register budget is tuned for (65536 registers / (threads * CTAs)); the FP32 Jacobian holds
+// half the point-wise state in registers and fits four CTAs (121 registers, no spills at P=4, Q=5)
+__host__ __device__ constexpr int min_blocks_for(int Q, bool staged = true, int elem_bytes = 8) {
+  return Q <= 5 ? (elem_bytes == 4 ? 4 : (staged ? 3 : 4)) : (Q == 6 ? 2 : 1);
+}
 
 // ---------------------------------------------------------------------------------------------------------------------
 // fibre passes over shared-memory tensors.  All arrays are [comp][n2][n1][n0] with n0 fastest.
@@ -79,22 +82,37 @@ __device__ __forceinline__ void pass0(const T *__restrict__ in, T *__restrict__ 
   }
 }
 
-// along n1: in [NC][N2][NIN][N0] -> out [NC][N2][NOUT][N0]
+// along n1: in [NC][N2][NIN][N0] -> out [NC][N2][NOUT][N0].  Each thread takes two fibres (f and f + NT) per round, loads
+// both before computing either, so the two dot-product chains overlap; a missing second fibre recomputes the first and
+// skips its store.
 template <int NC, int N2, int N0, int NIN, int NOUT, bool TR, int NT, typename T>
 __device__ __forceinline__ void pass1(const T *__restrict__ in, T *__restrict__ out, const T *__restrict__ M, int ldm) {
-  for (int f = threadIdx.x; f < NC * N2 * N0; f += NT) {
-    const int x = f % N0, cz = f / N0;
-    const T *src = in + cz * NIN * N0 + x;
-    T *dst = out + cz * NOUT * N0 + x;
-    T v[NIN];
+  constexpr int NF = NC * N2 * N0;
+  constexpr bool TWO = NF > NT;  // one round of one fibre per thread covers the pass otherwise
+#pragma unroll 1
+  for (int f0 = threadIdx.x; f0 < NF; f0 += (TWO ? 2 : 1) * NT) {
+    const bool h1 = TWO && f0 + NT < NF;
+    const int f1 = h1 ? f0 + NT : f0;
+    const int x0 = f0 % N0, cz0 = f0 / N0, x1 = f1 % N0, cz1 = f1 / N0;
+    const T *src0 = in + cz0 * NIN * N0 + x0, *src1 = in + cz1 * NIN * N0 + x1;
+    T v0[NIN], v1[NIN];
 #pragma unroll
-    for (int a = 0; a < NIN; a++) v[a] = src[a * N0];
+    for (int a = 0; a < NIN; a++) {
+      v0[a] = src0[a * N0];
+      if constexpr (TWO) v1[a] = src1[a * N0];
+    }
+    T *dst0 = out + cz0 * NOUT * N0 + x0, *dst1 = out + cz1 * NOUT * N0 + x1;
 #pragma unroll
     for (int i = 0; i < NOUT; i++) {
-      T s = 0;
+      T s0 = 0, s1 = 0;
 #pragma unroll
-      for (int a = 0; a < NIN; a++) s += (TR ? M[a * ldm + i] : M[i * ldm + a]) * v[a];
-      dst[i * N0] = s;
+      for (int a = 0; a < NIN; a++) {
+        const T m = TR ? M[a * ldm + i] : M[i * ldm + a];
+        s0 += m * v0[a];
+        if constexpr (TWO) s1 += m * v1[a];
+      }
+      dst0[i * N0] = s0;
+      if (TWO && h1) dst1[i * N0] = s1;
     }
   }
 }
@@ -148,25 +166,27 @@ struct QRef {
 
 // Offsets of the entries a thread handles in a 5-component node gather/scatter: entries t = threadIdx.x + j*NT
 // (node t/5, component t%5).  They are loaded into registers one element ahead (so no gather waits on them) and kept in
-// shared memory for the scatter and the output gather, so they are not live across the point-wise phase.  L-vector
-// indices fit in int32 (checked on the host).
+// shared memory for the scatter and the output gather, so they are not live across the point-wise phase.  load() only
+// issues the loads: the registers hold the node offsets as loaded and the component is added where they are used, so no
+// instruction waits for the load until the next element starts.  L-vector indices fit in int32 (checked on the host).
 template <int P, int NT>
 struct EntryOffsets {
   static constexpr int P3 = P * P * P, NJ = (5 * P3 + NT - 1) / NT;
-  int32_t o[NJ];
+  int32_t o[NJ];  // node offset (node * 5) of entry threadIdx.x + j*NT
   __device__ __forceinline__ void load(const int32_t *__restrict__ offsets, int e) {
     const int32_t *off = offsets + (int64_t)e * P3;
 #pragma unroll
     for (int j = 0; j < NJ; j++) {
       const int t = threadIdx.x + j * NT;
-      o[j] = t < 5 * P3 ? __ldg(off + t / 5) + t % 5 : 0;
+      if (t < 5 * P3) o[j] = __ldg(off + t / 5);
     }
   }
+  __device__ __forceinline__ int32_t entry(int j) const { return o[j] + (int)((threadIdx.x + j * NT) % 5); }
   __device__ __forceinline__ void store(int32_t *sO) const {
 #pragma unroll
     for (int j = 0; j < NJ; j++) {
       const int t = threadIdx.x + j * NT;
-      if (t < 5 * P3) sO[t] = o[j];
+      if (t < 5 * P3) sO[t] = entry(j);
     }
   }
 };
@@ -184,11 +204,12 @@ __device__ __forceinline__ void gather_async(const EntryOffsets<P, NT> &eo, cons
     const int t = threadIdx.x + j * NT;
     if (t < 5 * P3) {
       const int p = t / 5, c = t % 5, srow = (p / P) * PX + p % P;
-      if (sizeof(T) == 8) cp_async8(&sN[c * PS + srow], l0 + eo.o[j]);
-      else cp_async4(&sN[c * PS + srow], l0 + eo.o[j]);
+      const int32_t o = eo.o[j] + c;
+      if (sizeof(T) == 8) cp_async8(&sN[c * PS + srow], l0 + o);
+      else cp_async4(&sN[c * PS + srow], l0 + o);
       if (NV > 1) {
-        if (sizeof(T) == 8) cp_async8(&sN[(5 + c) * PS + srow], l1 + eo.o[j]);
-        else cp_async4(&sN[(5 + c) * PS + srow], l1 + eo.o[j]);
+        if (sizeof(T) == 8) cp_async8(&sN[(5 + c) * PS + srow], l1 + o);
+        else cp_async4(&sN[(5 + c) * PS + srow], l1 + o);
       }
     }
   }
@@ -205,70 +226,117 @@ __device__ __forceinline__ void gather_out_async(const int32_t *sO, const T *l_o
   }
 }
 
-// x pass from the padded staging rows: sN [NC][P*P][PX] -> s1 [NC][P*P][Q]
+// x pass from the padded staging rows: sN [NC][P*P][PX] -> s1 [NC][P*P][Q] (two fibres per thread and round)
 template <int P, int Q, int NC, int NT, typename T>
 __device__ __forceinline__ void pass_x_staged(const Basis1D<T> &bas, const T *sN, T *s1) {
-  constexpr int PX = padded_row<P>();
-  for (int f = threadIdx.x; f < NC * P * P; f += NT) {
-    T x[P];
+  constexpr int PX = padded_row<P>(), NF = NC * P * P;
+  constexpr bool TWO = NF > NT;
+#pragma unroll 1
+  for (int f0 = threadIdx.x; f0 < NF; f0 += (TWO ? 2 : 1) * NT) {
+    const bool h1 = TWO && f0 + NT < NF;
+    const int f1 = h1 ? f0 + NT : f0;
+    T x0[P], x1[P];
 #pragma unroll
-    for (int a = 0; a < P; a++) x[a] = sN[f * PX + a];
+    for (int a = 0; a < P; a++) {
+      x0[a] = sN[f0 * PX + a];
+      if constexpr (TWO) x1[a] = sN[f1 * PX + a];
+    }
 #pragma unroll
     for (int i = 0; i < Q; i++) {
-      T s = 0;
+      T s0 = 0, s1v = 0;
 #pragma unroll
-      for (int a = 0; a < P; a++) s += bas.B[i * P + a] * x[a];
-      s1[f * Q + i] = s;
+      for (int a = 0; a < P; a++) {
+        s0 += bas.B[i * P + a] * x0[a];
+        if constexpr (TWO) s1v += bas.B[i * P + a] * x1[a];
+      }
+      s1[f0 * Q + i] = s0;
+      if (TWO && h1) s1[f1 * Q + i] = s1v;
     }
   }
 }
 
 // Forward passes after the x pass: s1 -> (y) s2 -> (z) interp sU [NC][Q3] and, for the first vector, the z
-// derivative; then x/y derivatives of the first vector on the quadrature grid.
+// derivative; then x/y derivatives of the first vector on the quadrature grid.  Two fibres per thread and round.
 template <int P, int Q, int NC, int NT, typename T>
 __device__ __forceinline__ void forward_yz(const Basis1D<T> &bas, const T *s1, T *s2, T *sU, T *sG) {
   constexpr int Q2 = Q * Q, Q3 = Q2 * Q;
   pass1<NC, P, Q, P, Q, false, NT>(s1, s2, bas.B, P);
   __syncthreads();
-  for (int f = threadIdx.x; f < NC * Q2; f += NT) {
-    const int yx = f % Q2, c = f / Q2;
-    T in[P], val[Q];
+  constexpr bool TWO = NC * Q2 > NT;
+  constexpr bool D1 = TWO && NT / Q2 < 5;  // a second fibre can belong to the first vector (needs its z derivative)
+#pragma unroll 1
+  for (int f0 = threadIdx.x; f0 < NC * Q2; f0 += (TWO ? 2 : 1) * NT) {
+    const bool h1 = TWO && f0 + NT < NC * Q2;
+    const int f1 = h1 ? f0 + NT : f0;
+    const int yx0 = f0 % Q2, c0 = f0 / Q2, yx1 = f1 % Q2, c1 = f1 / Q2;
+    T in0[P], in1[P], val0[Q], val1[Q];
 #pragma unroll
-    for (int cz = 0; cz < P; cz++) in[cz] = s2[(c * P + cz) * Q2 + yx];
+    for (int cz = 0; cz < P; cz++) {
+      in0[cz] = s2[(c0 * P + cz) * Q2 + yx0];
+      if constexpr (TWO) in1[cz] = s2[(c1 * P + cz) * Q2 + yx1];
+    }
 #pragma unroll
     for (int k = 0; k < Q; k++) {
-      T s = 0;
+      T a0 = 0, a1 = 0;
 #pragma unroll
-      for (int cz = 0; cz < P; cz++) s += bas.B[k * P + cz] * in[cz];
-      val[k] = s;
-      sU[c * Q3 + k * Q2 + yx] = s;
+      for (int cz = 0; cz < P; cz++) {
+        a0 += bas.B[k * P + cz] * in0[cz];
+        if constexpr (TWO) a1 += bas.B[k * P + cz] * in1[cz];
+      }
+      val0[k] = a0;
+      val1[k] = a1;
+      sU[c0 * Q3 + k * Q2 + yx0] = a0;
+      if (TWO && h1) sU[c1 * Q3 + k * Q2 + yx1] = a1;
     }
-    if (c < 5) {
+    // z derivative of the first vector (components 0-4)
+    if (c0 < 5) {
 #pragma unroll
       for (int k = 0; k < Q; k++) {
-        T s = 0;
+        T d0 = 0;
 #pragma unroll
-        for (int l = 0; l < Q; l++) s += bas.D[k * Q + l] * val[l];
-        sG[(2 * 5 + c) * Q3 + k * Q2 + yx] = s;
+        for (int l = 0; l < Q; l++) d0 += bas.D[k * Q + l] * val0[l];
+        sG[(2 * 5 + c0) * Q3 + k * Q2 + yx0] = d0;
+      }
+    }
+    if (D1 && h1 && c1 < 5) {
+#pragma unroll
+      for (int k = 0; k < Q; k++) {
+        T d1 = 0;
+#pragma unroll
+        for (int l = 0; l < Q; l++) d1 += bas.D[k * Q + l] * val1[l];
+        sG[(2 * 5 + c1) * Q3 + k * Q2 + yx1] = d1;
       }
     }
   }
   __syncthreads();
-  for (int f = threadIdx.x; f < 2 * 5 * Q2; f += NT) {
-    const int dir = f / (5 * Q2), r = f % (5 * Q2), c = r / Q2, rem = r % Q2;
-    const int base = dir == 0 ? rem * Q : (rem / Q) * Q2 + (rem % Q);
-    const int stride = dir == 0 ? 1 : Q;
-    const T *src = sU + c * Q3 + base;
-    T *dst = sG + (dir * 5 + c) * Q3 + base;
-    T val[Q];
+  constexpr int NXY = 2 * 5 * Q2;
+  constexpr bool TWO_XY = NXY > NT;
+#pragma unroll 1
+  for (int f0 = threadIdx.x; f0 < NXY; f0 += (TWO_XY ? 2 : 1) * NT) {
+    const bool h1 = TWO_XY && f0 + NT < NXY;
+    const int f1 = h1 ? f0 + NT : f0;
+    const int dir0 = f0 / (5 * Q2), r0 = f0 % (5 * Q2), cc0 = r0 / Q2, rem0 = r0 % Q2;
+    const int dir1 = f1 / (5 * Q2), r1 = f1 % (5 * Q2), cc1 = r1 / Q2, rem1 = r1 % Q2;
+    const int base0 = dir0 == 0 ? rem0 * Q : (rem0 / Q) * Q2 + (rem0 % Q), st0 = dir0 == 0 ? 1 : Q;
+    const int base1 = dir1 == 0 ? rem1 * Q : (rem1 / Q) * Q2 + (rem1 % Q), st1 = dir1 == 0 ? 1 : Q;
+    const T *src0 = sU + cc0 * Q3 + base0, *src1 = sU + cc1 * Q3 + base1;
+    T *dst0 = sG + (dir0 * 5 + cc0) * Q3 + base0, *dst1 = sG + (dir1 * 5 + cc1) * Q3 + base1;
+    T v0[Q], v1[Q];
 #pragma unroll
-    for (int l = 0; l < Q; l++) val[l] = src[l * stride];
+    for (int l = 0; l < Q; l++) {
+      v0[l] = src0[l * st0];
+      if constexpr (TWO_XY) v1[l] = src1[l * st1];
+    }
 #pragma unroll
     for (int k = 0; k < Q; k++) {
-      T s = 0;
+      T d0 = 0, d1 = 0;
 #pragma unroll
-      for (int l = 0; l < Q; l++) s += bas.D[k * Q + l] * val[l];
-      dst[k * stride] = s;
+      for (int l = 0; l < Q; l++) {
+        d0 += bas.D[k * Q + l] * v0[l];
+        if constexpr (TWO_XY) d1 += bas.D[k * Q + l] * v1[l];
+      }
+      dst0[k * st0] = d0;
+      if (TWO_XY && h1) dst1[k * st1] = d1;
     }
   }
   __syncthreads();
@@ -276,37 +344,44 @@ __device__ __forceinline__ void forward_yz(const Basis1D<T> &bas, const T *s1, T
 
 // Transpose of the point values v [5][Q3] (sU) and reference-direction fluxes [3][5][Q3] (sG) back to the element
 // nodes, node-major sF [P3][5].  Scratch: sW1 [5][Q3], sW2 [5][Q3], sT2 [5][P][Q][Q], sT1 [5][P][P][Q]; sT1 may alias
-// sG (free once the z pass is done), sF may alias sW2.
+// sG (free once the z pass is done), sF may alias sW2.  Two fibres per thread and round where a pass has more fibres
+// than threads.
 template <int P, int Q, int NT, typename T>
 __device__ __forceinline__ void transpose_passes(const Basis1D<T> &bas, const T *sU, const T *sG, T *sW1, T *sW2, T *sT2, T *sT1, T *sF) {
-  constexpr int Q2 = Q * Q, Q3 = Q2 * Q;
-  for (int f = threadIdx.x; f < 2 * 5 * Q2; f += NT) {
-    const int dir = f / (5 * Q2), r = f % (5 * Q2), c = r / Q2, rem = r % Q2;
-    const int base = dir == 0 ? rem * Q : (rem / Q) * Q2 + (rem % Q);
-    const int stride = dir == 0 ? 1 : Q;
-    const T *g = sG + (dir * 5 + c) * Q3 + base;
-    T gv[Q];
+  constexpr int Q2 = Q * Q, Q3 = Q2 * Q, NXY = 2 * 5 * Q2;
+  constexpr bool TWO = NXY > NT;
+#pragma unroll 1
+  for (int f0 = threadIdx.x; f0 < NXY; f0 += (TWO ? 2 : 1) * NT) {
+    const bool h1 = TWO && f0 + NT < NXY;
+    const int f1 = h1 ? f0 + NT : f0;
+    const int dir0 = f0 / (5 * Q2), r0 = f0 % (5 * Q2), c0 = r0 / Q2, rem0 = r0 % Q2;
+    const int dir1 = f1 / (5 * Q2), r1 = f1 % (5 * Q2), c1 = r1 / Q2, rem1 = r1 % Q2;
+    const int base0 = dir0 == 0 ? rem0 * Q : (rem0 / Q) * Q2 + (rem0 % Q), st0 = dir0 == 0 ? 1 : Q;
+    const int base1 = dir1 == 0 ? rem1 * Q : (rem1 / Q) * Q2 + (rem1 % Q), st1 = dir1 == 0 ? 1 : Q;
+    const T *g0 = sG + (dir0 * 5 + c0) * Q3 + base0, *g1 = sG + (dir1 * 5 + c1) * Q3 + base1;
+    // x direction adds the point values (w1 = v + D^T g_x); y direction starts from zero (w2 = D^T g_y)
+    const T *v0 = sU + c0 * Q3 + base0, *v1 = sU + c1 * Q3 + base1;
+    T *w0 = (dir0 == 0 ? sW1 : sW2) + c0 * Q3 + base0, *w1 = (dir1 == 0 ? sW1 : sW2) + c1 * Q3 + base1;
+    T gv0[Q], gv1[Q], b0[Q], b1[Q];
 #pragma unroll
-    for (int l = 0; l < Q; l++) gv[l] = g[l * stride];
-    if (dir == 0) {
-      const T *v = sU + c * Q3 + base;
-      T *w = sW1 + c * Q3 + base;
-#pragma unroll
-      for (int i = 0; i < Q; i++) {
-        T s = v[i];
-#pragma unroll
-        for (int l = 0; l < Q; l++) s += bas.D[l * Q + i] * gv[l];
-        w[i] = s;
+    for (int l = 0; l < Q; l++) {
+      gv0[l] = g0[l * st0];
+      b0[l] = dir0 == 0 ? v0[l] : T(0);
+      if constexpr (TWO) {
+        gv1[l] = g1[l * st1];
+        b1[l] = dir1 == 0 ? v1[l] : T(0);
       }
-    } else {
-      T *w = sW2 + c * Q3 + base;
+    }
 #pragma unroll
-      for (int j = 0; j < Q; j++) {
-        T s = 0;
+    for (int i = 0; i < Q; i++) {
+      T s0 = b0[i], s1 = TWO ? b1[i] : T(0);
 #pragma unroll
-        for (int l = 0; l < Q; l++) s += bas.D[l * Q + j] * gv[l];
-        w[j * Q] = s;
+      for (int l = 0; l < Q; l++) {
+        s0 += bas.D[l * Q + i] * gv0[l];
+        if constexpr (TWO) s1 += bas.D[l * Q + i] * gv1[l];
       }
+      w0[i * st0] = s0;
+      if (TWO && h1) w1[i * st1] = s1;
     }
   }
   __syncthreads();
@@ -453,7 +528,8 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
   HB_PT_DECL
   for (; idx < a.n_elems; idx += gridDim.x) {
     const int e = ecur;
-    const int en3 = idx + 3 * G < a.n_elems ? a.elems[idx + 3 * G] : -1;  // used one iteration later
+    int en3 = -1;  // used one iteration later: a predicated load, so nothing waits for it here
+    if (idx + 3 * G < a.n_elems) en3 = __ldg(a.elems + idx + 3 * G);
     if (en2 >= 0) nxt2.load(a.offsets, en2);
     HB_PT(7)
     // everything but the most recent group (the output gather, only needed at the scatter) has landed
@@ -565,7 +641,7 @@ struct IjacobianPtrs {
 };
 
 template <int P, int Q, typename T, bool ST>
-__global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST)) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
+__global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int)sizeof(T))) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
   constexpr int NT = nthreads_for<T>(Q);
   using L = Plan<P, Q, 1, T, true, ST>;
   constexpr int Q3 = L::Q3;
@@ -620,7 +696,8 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST)) k_i
   if (en >= 0) nxt.load(a.offsets, en);
   for (; idx < a.n_elems; idx += gridDim.x) {
     const int e = ecur;
-    const int en3 = idx + 3 * G < a.n_elems ? a.elems[idx + 3 * G] : -1;  // used one iteration later
+    int en3 = -1;  // used one iteration later: a predicated load, so nothing waits for it here
+    if (idx + 3 * G < a.n_elems) en3 = __ldg(a.elems + idx + 3 * G);
     if (en2 >= 0) nxt2.load(a.offsets, en2);
     // everything but the most recent group (the output gather, only needed at the scatter) has landed
     cp_async_wait_group<1>();

@@ -306,6 +306,26 @@ def multimode_state(mesh: BoxMesh, basis: TensorBasis, gas: GasProperties, *, P0
     return np.ascontiguousarray(q.T.reshape(-1))
 
 
+def taylor_green_state(mesh: BoxMesh, basis: TensorBasis, tg: "TaylorGreenContext") -> np.ndarray:
+    """Nodal Taylor-Green vortex initial state (conservative, node-interleaved), as ICsTaylorGreen computes it
+    (qfunctions/taylorgreen.h:23-50): coordinates scaled by 2 pi / L, pressure with its cos(2 z + 2) factor, velocity
+    amplitude |reference velocity| plus the context's mean velocity u, uniform reference temperature."""
+    X = node_coordinates(mesh, basis)
+    gas = tg.newt_ctx.gas
+    R = gas.cp - gas.cv
+    ref = tg.reference
+    V0 = math.sqrt(sum(ref.velocity[i] ** 2 for i in range(3)))
+    rho0 = ref.pressure / (ref.temperature * R)
+    x = X[0] * (2 * math.pi / tg.lx)
+    y = X[1] * (2 * math.pi / tg.ly)
+    z = X[2] * (2 * math.pi / tg.lz)
+    P = ref.pressure + (rho0 * V0 * V0 / 16) * (np.cos(2 * x) + np.cos(2 * y)) * np.cos(2 * z + 2)
+    u = np.stack([tg.u[0] + V0 * np.sin(x) * np.cos(y) * np.cos(z), tg.u[1] - V0 * np.cos(x) * np.sin(y) * np.cos(z),
+                  tg.u[2] + 0 * x])
+    q = conservative_from_primitive(gas, P, u, ref.temperature * np.ones_like(P))
+    return np.ascontiguousarray(q.T.reshape(-1))
+
+
 def taylor_green_context(degree: int, *, L=2 * math.pi, Re=1600., Ma=0.1, rho0=1.0, V0=1.0, stab=STAB_SUPG):
     """Taylor-Green vortex parameters in the form of examples/taylor_green_vortex.yaml (Re=1600, Ma=0.1)."""
     cv, cp = 717., 1003.8

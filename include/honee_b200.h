@@ -146,6 +146,7 @@ typedef struct {
   int    pc_jacobi;       /* 1: Jacobi from the assembled diagonal, 0: none */
   int    pc_every_newton; /* 0: diagonal once per time step (lagged), 1: every Newton iteration */
   int    jacobian_fp32;   /* mixed precision: FP32 Krylov basis, Jacobian action and diagonal; FP64 residual and update */
+  int    cgs_refine;      /* 0: classical Gram-Schmidt once (PETSc default), 1: a second pass every iteration (CGS2) */
 } HbSolverOptions;
 
 typedef struct {

@@ -161,3 +161,27 @@ def test_monitor_cfl_uniform_flow_on_anisotropic_box():
     mn, mx = S.monitor_cfl(op, prob.context_bytes(ctx), torch.from_numpy(q).to(_dev()), qdata, dt, scratch)
     expect = dt * np.sqrt(np.sum((u * np.array(n)) ** 2))  # element size 1/n_i, metric 0.25 dXdx^T dXdx = diag(n_i^2)
     assert mn == pytest.approx(expect, rel=1e-12) and mx == pytest.approx(expect, rel=1e-12)
+
+
+def test_taylor_green_driver_fp64_and_mixed_monitors_agree():
+    """Short Taylor-Green run through the time-stepping driver: Newton converges every step in both precisions, the
+    kinetic energy decays, and the mixed-precision monitors follow the FP64 ones."""
+    NS = importlib.import_module("honee-4aiad_b200.navierstokes")
+    r64 = NS.run("taylor_green", faces=4, degree=3, steps=4, cfl=1.0, mixed=False)
+    r32 = NS.run("taylor_green", faces=4, degree=3, steps=4, cfl=1.0, mixed=True)
+    ke = [row["TotalKineticEnergy"] for row in r64.rows]
+    assert all(b < a for a, b in zip(ke, ke[1:])), ke
+    assert abs(ke[0] - 0.125) < 0.01  # V0^2/8 for the Taylor-Green velocity field, up to discretisation error
+    d = NS.compare(r64, r32)
+    assert d["TotalKineticEnergy"] < 1e-8 and d["StrainDissipation"] < 1e-6, d
+    assert r64.rows[-1]["maxcfl"] > 0
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_cgs_refinement_gives_the_same_step(fp32):
+    mesh, basis, ctx, q0, op, qdata = _problem(n=(3, 3, 3), dt=1e-4)
+    kw = dict(dt=1e-4, bdf_order=1, newton_rtol=1e-9, jacobian_fp32=fp32)
+    qa, _, (sa,), _ = _run(op, ctx, qdata, q0, 1, cgs_refine=0, **kw)
+    qb, _, (sb,), _ = _run(op, ctx, qdata, q0, 1, cgs_refine=1, **kw)
+    assert sa.converged_reason == 1 and sb.converged_reason == 1
+    assert rel_l2(qa - q0, qb - q0) < 1e-6

@@ -154,3 +154,16 @@ def test_box_colouring_is_conflict_free(n, periodic):
         per_elem = [np.unique(r) for r in nodes]
         allnodes = np.concatenate(per_elem)
         assert len(np.unique(allnodes)) == len(allnodes), (c, n, periodic)
+
+
+def test_taylor_green_state_matches_reference_initial_condition():
+    """The product's nodal TG initial state equals the reference ICsTaylorGreen QFunction run by the oracle."""
+    L = 2 * np.pi
+    mesh = prob.box_mesh((3, 3, 3), 5, periodic=(1, 1, 1), hi=(L, L, L))
+    basis = prob.tensor_basis(5, 6)
+    tg = prob.taylor_green_context(4)
+    tg.u[0], tg.u[1], tg.u[2] = 0.1, -0.2, 0.05
+    X = prob.node_coordinates(mesh, basis)
+    qn = np.zeros((5, X.shape[1]))
+    O.call_qf(O.lib().oracle_qf_ics_taylorgreen, bytes(memoryview(tg)), X.shape[1], [np.ascontiguousarray(X)], [qn])
+    np.testing.assert_allclose(prob.taylor_green_state(mesh, basis, tg), qn.T.reshape(-1), rtol=1e-14, atol=0)
