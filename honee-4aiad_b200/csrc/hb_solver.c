@@ -27,7 +27,7 @@ struct HbTimeStepper {
   HbNewtonianContext ctx;
   const double      *qdata;
   HbSolverOptions    o;
-  int64_t            n;
+  int64_t            n, ldv; /* ldv: row stride of the Krylov basis, n rounded up so every row starts 16-byte aligned */
   int                njd, steps_taken;
   double             t;
   cudaStream_t       s;
@@ -78,6 +78,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
   ts->qdata = d_qdata;
   ts->o     = *opts;
   ts->n     = op->l_size;
+  ts->ldv   = (op->l_size + 3) & ~(int64_t)3;
   ts->njd   = ts->ctx.idl_enable ? 15 : 14;
   ts->s     = (cudaStream_t)stream;
   const size_t nb = sizeof(double) * (size_t)ts->n, Q3 = (size_t)op->Q * op->Q * op->Q, njd = (size_t)ts->njd * op->num_elem * Q3;
@@ -87,7 +88,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
   err |= cudaMalloc((void **)&ts->z, nb) | cudaMalloc((void **)&ts->qdot, nb) | cudaMalloc((void **)&ts->res, nb) | cudaMalloc((void **)&ts->delta, nb);
   err |= cudaMalloc((void **)&ts->d_partial, sizeof(double) * 512 * MAXK) | cudaMalloc((void **)&ts->d_dots, sizeof(double) * MAXK);
   err |= cudaMalloc((void **)&ts->scratch, sizeof(double) * 1024);
-  err |= cudaMalloc(&ts->V, ksz(ts) * (size_t)ts->n * (m + 1)) | cudaMalloc(&ts->w, ksz(ts) * (size_t)ts->n);
+  err |= cudaMalloc(&ts->V, ksz(ts) * (size_t)ts->ldv * (m + 1)) | cudaMalloc(&ts->w, ksz(ts) * (size_t)ts->n);
   err |= cudaMalloc(&ts->zvec, ksz(ts) * (size_t)ts->n) | cudaMalloc(&ts->diag, ksz(ts) * (size_t)ts->n);
   if (ts->o.jacobian_fp32) err |= cudaMalloc(&ts->jd32, sizeof(float) * njd) | cudaMalloc((void **)&ts->res32, sizeof(float) * (size_t)ts->n);
   else err |= cudaMalloc((void **)&ts->jd64, sizeof(double) * njd);
@@ -132,7 +133,7 @@ static int kv_norm2(HbTimeStepper *ts, const void *x, double *nrm) {
   *nrm = sqrt(r);
   return HB_SUCCESS;
 }
-static void *kv_col(HbTimeStepper *ts, int j) { return (char *)ts->V + ksz(ts) * (size_t)ts->n * j; }
+static void *kv_col(HbTimeStepper *ts, int j) { return (char *)ts->V + ksz(ts) * (size_t)ts->ldv * j; }
 static int kv_scale(HbTimeStepper *ts, void *x, double a) {
   return ts->o.jacobian_fp32 ? hb_vec_scale_f32((float *)x, ts->n, (float)a, ts->s) : hb_vec_scale_f64((double *)x, ts->n, a, ts->s);
 }
@@ -151,15 +152,15 @@ static int kv_pc(HbTimeStepper *ts, const void *x, void *z) {
   return hb_vec_pointwise_mult_f64((double *)z, (const double *)ts->diag, (const double *)x, ts->n, ts->s);
 }
 static int kv_multidot(HbTimeStepper *ts, int k, const void *w, double *h) {
-  if (ts->o.jacobian_fp32) HBCK(hb_krylov_multidot_f32((const float *)ts->V, ts->n, k, (const float *)w, ts->n, ts->d_partial, ts->d_dots, ts->s));
-  else HBCK(hb_krylov_multidot_f64((const double *)ts->V, ts->n, k, (const double *)w, ts->n, ts->d_partial, ts->d_dots, ts->s));
+  if (ts->o.jacobian_fp32) HBCK(hb_krylov_multidot_f32((const float *)ts->V, ts->ldv, k, (const float *)w, ts->n, ts->d_partial, ts->d_dots, ts->s));
+  else HBCK(hb_krylov_multidot_f64((const double *)ts->V, ts->ldv, k, (const double *)w, ts->n, ts->d_partial, ts->d_dots, ts->s));
   CUCK(cudaMemcpyAsync(h, ts->d_dots, sizeof(double) * k, cudaMemcpyDeviceToHost, ts->s));
   CUCK(cudaStreamSynchronize(ts->s));
   return HB_SUCCESS;
 }
 static int kv_multiaxpy(HbTimeStepper *ts, void *w, int k, const double *c) {
-  if (ts->o.jacobian_fp32) return hb_krylov_multiaxpy_f32((float *)w, (const float *)ts->V, ts->n, k, c, ts->n, ts->s);
-  return hb_krylov_multiaxpy_f64((double *)w, (const double *)ts->V, ts->n, k, c, ts->n, ts->s);
+  if (ts->o.jacobian_fp32) return hb_krylov_multiaxpy_f32((float *)w, (const float *)ts->V, ts->ldv, k, c, ts->n, ts->s);
+  return hb_krylov_multiaxpy_f64((double *)w, (const double *)ts->V, ts->ldv, k, c, ts->n, ts->s);
 }
 
 /* Jacobi diagonal at the current linearisation point, stored inverted */
@@ -253,12 +254,12 @@ static int gmres(HbTimeStepper *ts, int *its_out, double *rnorm_out) {
     }
     if (ts->o.jacobian_fp32) {
       HBCK(hb_vec_set_f32((float *)ts->w, ts->n, 0.0f, ts->s));
-      HBCK(hb_krylov_multiaxpy_f32((float *)ts->w, (const float *)ts->V, ts->n, k, y, ts->n, ts->s));
+      HBCK(hb_krylov_multiaxpy_f32((float *)ts->w, (const float *)ts->V, ts->ldv, k, y, ts->n, ts->s));
       HBCK(kv_pc(ts, ts->w, ts->zvec));
       HBCK(hb_vec_f32_to_f64((const float *)ts->zvec, ts->delta, ts->n, 1, ts->s));
     } else {
       HBCK(hb_vec_set_f64((double *)ts->w, ts->n, 0.0, ts->s));
-      HBCK(hb_krylov_multiaxpy_f64((double *)ts->w, (const double *)ts->V, ts->n, k, y, ts->n, ts->s));
+      HBCK(hb_krylov_multiaxpy_f64((double *)ts->w, (const double *)ts->V, ts->ldv, k, y, ts->n, ts->s));
       HBCK(kv_pc(ts, ts->w, ts->zvec));
       HBCK(hb_vec_axpy_f64(ts->delta, 1.0, (const double *)ts->zvec, ts->n, ts->s));
     }

@@ -84,6 +84,147 @@ __global__ void __launch_bounds__(kBS) k_multiaxpy(TW *__restrict__ w, const T *
   }
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// Vectorised forms of the two block operations, used when every basis row and w start on a 16-byte boundary: each
+// thread moves 16 bytes per vector and step (2 doubles or 4 floats), and the basis size K is a template parameter, so
+// the accumulators stay in registers and no predicated slots are issued.  These are pure streams over K + 1 (multi-dot)
+// or K + 2 (multi-axpy) vectors and run at the HBM rate in either precision.
+
+template <typename T>
+__device__ __forceinline__ void ld16(const T *__restrict__ p, T (&x)[16 / sizeof(T)]) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    x[0] = v.x;
+    x[1] = v.y;
+  } else {
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+    x[0] = v.x;
+    x[1] = v.y;
+    x[2] = v.z;
+    x[3] = v.w;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void st16(T *__restrict__ p, const T (&x)[16 / sizeof(T)]) {
+  if constexpr (sizeof(T) == 8) *reinterpret_cast<double2 *>(p) = make_double2(x[0], x[1]);
+  else *reinterpret_cast<float4 *>(p) = make_float4(x[0], x[1], x[2], x[3]);
+}
+
+// partial[block][i] = sum over this block's elements of V[i][e] w[e], i < K (FP64 accumulation)
+template <typename T, int K>
+__global__ void __launch_bounds__(kBS) k_multidot_vec(const T *__restrict__ V, int64_t ldv, const T *__restrict__ w, int64_t n, double *partial) {
+  constexpr int VW = 16 / sizeof(T);
+  __shared__ double sh[K][kBS / 32];
+  double acc[K];
+#pragma unroll
+  for (int i = 0; i < K; i++) acc[i] = 0;
+  const int64_t nv = n / VW;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nv; j += (int64_t)gridDim.x * blockDim.x) {
+    T wv[VW];
+    ld16(w + j * VW, wv);
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+      T x[VW];
+      ld16(V + i * ldv + j * VW, x);
+#pragma unroll
+      for (int u = 0; u < VW; u++) acc[i] += (double)x[u] * (double)wv[u];
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - nv * VW) {  // the last n mod VW elements
+    const int64_t e = nv * VW + threadIdx.x;
+    const double we = (double)w[e];
+#pragma unroll
+    for (int i = 0; i < K; i++) acc[i] += (double)V[i * ldv + e] * we;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+    double v = acc[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[i][warp] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < K; i += blockDim.x) {
+    double s = 0;
+    for (int wi = 0; wi < kBS / 32; wi++) s += sh[i][wi];
+    partial[blockIdx.x * kMaxK + i] = s;
+  }
+}
+
+// w[e] += sum_{i<K} c[i] V[i][e] (w and V of one precision; the sum in FP64)
+template <typename T, int K>
+__global__ void __launch_bounds__(kBS) k_multiaxpy_vec(T *__restrict__ w, const T *__restrict__ V, int64_t ldv, Coefs c, int64_t n) {
+  constexpr int VW = 16 / sizeof(T);
+  const int64_t nv = n / VW;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nv; j += (int64_t)gridDim.x * blockDim.x) {
+    T wv[VW];
+    ld16(w + j * VW, wv);
+    double s[VW];
+#pragma unroll
+    for (int u = 0; u < VW; u++) s[u] = (double)wv[u];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+      T x[VW];
+      ld16(V + i * ldv + j * VW, x);
+#pragma unroll
+      for (int u = 0; u < VW; u++) s[u] += c.c[i] * (double)x[u];
+    }
+#pragma unroll
+    for (int u = 0; u < VW; u++) wv[u] = T(s[u]);
+    st16(w + j * VW, wv);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - nv * VW) {
+    const int64_t e = nv * VW + threadIdx.x;
+    double s = (double)w[e];
+#pragma unroll
+    for (int i = 0; i < K; i++) s += c.c[i] * (double)V[i * ldv + e];
+    w[e] = T(s);
+  }
+}
+
+#define HB_BASIS_SIZES(X)                                                                                               \
+  X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20) X(21) \
+  X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29) X(30) X(31) X(32)
+static_assert(kMaxK == 32, "HB_BASIS_SIZES lists every basis size up to the maximum");
+
+template <typename T>
+inline bool vec_ok(const T *V, int64_t ldv, const void *w) {
+  return ((uintptr_t)V % 16 == 0) && ((uintptr_t)w % 16 == 0) && ((ldv * (int64_t)sizeof(T)) % 16 == 0);
+}
+
+// out[i] = V_i . w for i < k through the per-block partials (kRedBlocks x kMaxK doubles)
+template <typename T>
+void launch_multidot(const T *V, int64_t ldv, int k, const T *w, int64_t n, double *partial, double *out, cudaStream_t s) {
+  if (vec_ok(V, ldv, w)) {
+    switch (k) {
+#define HB_MDOT_CASE(KK) \
+  case KK: k_multidot_vec<T, KK><<<kRedBlocks, kBS, 0, s>>>(V, ldv, w, n, partial); break;
+      HB_BASIS_SIZES(HB_MDOT_CASE)
+#undef HB_MDOT_CASE
+    }
+  } else {
+    k_multidot<T><<<kRedBlocks, kBS, 0, s>>>(V, ldv, k, w, n, partial);
+  }
+  k_multidot_final<<<k, kBS, 0, s>>>(partial, kRedBlocks, k, out);
+}
+
+template <typename T>
+void launch_multiaxpy(T *w, const T *V, int64_t ldv, int k, const Coefs &c, int64_t n, cudaStream_t s) {
+  if (vec_ok(V, ldv, w)) {
+    const int64_t nv = n / (16 / (int64_t)sizeof(T));
+    const unsigned g = (unsigned)(nv / kBS + 1 > 148 * 16 ? 148 * 16 : nv / kBS + 1);
+    switch (k) {
+#define HB_MAXPY_CASE(KK) \
+  case KK: k_multiaxpy_vec<T, KK><<<g, kBS, 0, s>>>(w, V, ldv, c, n); break;
+      HB_BASIS_SIZES(HB_MAXPY_CASE)
+#undef HB_MAXPY_CASE
+    }
+  } else {
+    k_multiaxpy<T, T><<<nblocks(n), kBS, 0, s>>>(w, V, ldv, k, c, n);
+  }
+}
+
 // q_dot = alpha q + z
 __global__ void k_bdf_qdot(const double *__restrict__ q, const double *__restrict__ z, double alpha, double *__restrict__ qdot, int64_t n) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) qdot[e] = alpha * q[e] + z[e];
@@ -250,18 +391,16 @@ extern "C" {
 
 int hb_krylov_multidot_f64(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_partial, double *d_out, void *s) {
   if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
-  k_multidot<double><<<kRedBlocks, kBS, 0, (cudaStream_t)s>>>(V, ldv, k, w, n, d_partial);
-  k_multidot_final<<<k, kBS, 0, (cudaStream_t)s>>>(d_partial, kRedBlocks, k, d_out);
+  launch_multidot<double>(V, ldv, k, w, n, d_partial, d_out, (cudaStream_t)s);
   return rc();
 }
 int hb_krylov_multidot_f32(const float *V, int64_t ldv, int k, const float *w, int64_t n, double *d_partial, double *d_out, void *s) {
   if (k < 1 || k > kMaxK) return HB_ERROR_INVALID;
-  k_multidot<float><<<kRedBlocks, kBS, 0, (cudaStream_t)s>>>(V, ldv, k, w, n, d_partial);
-  k_multidot_final<<<k, kBS, 0, (cudaStream_t)s>>>(d_partial, kRedBlocks, k, d_out);
+  launch_multidot<float>(V, ldv, k, w, n, d_partial, d_out, (cudaStream_t)s);
   return rc();
 }
 
-// hb_krylov_multidot_f64 without the caller's partial-sum buffer: the same two kernels, with the partials in the fixed
+// hb_krylov_multidot_f64 without the caller's partial-sum buffer: the same kernels, with the partials in the fixed
 // device scratch above.  For callers that have no device work buffer to give and must not create one per call: an inner
 // product requested through a vector-library callback that carries only the vectors (a cudaMalloc/cudaFree pair there
 // would synchronise the whole device on every Krylov iteration), or a solver that commits all device memory to its Krylov
@@ -272,8 +411,7 @@ int hb_krylov_multidot_f64_static(const double *V, int64_t ldv, int k, const dou
   double *partial = nullptr;
   const int e = multidot_scratch(&partial);
   if (e) return e;
-  k_multidot<double><<<kRedBlocks, kBS, 0, (cudaStream_t)s>>>(V, ldv, k, w, n, partial);
-  k_multidot_final<<<k, kBS, 0, (cudaStream_t)s>>>(partial, kRedBlocks, k, d_out);
+  launch_multidot<double>(V, ldv, k, w, n, partial, d_out, (cudaStream_t)s);
   return rc();
 }
 int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, const double *c, int64_t n, void *s) {
@@ -281,7 +419,7 @@ int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, cons
   Coefs cf;
   memset(&cf, 0, sizeof cf);
   memcpy(cf.c, c, sizeof(double) * k);
-  k_multiaxpy<double, double><<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, V, ldv, k, cf, n);
+  launch_multiaxpy<double>(w, V, ldv, k, cf, n, (cudaStream_t)s);
   return rc();
 }
 int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s) {
@@ -289,7 +427,7 @@ int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const 
   Coefs cf;
   memset(&cf, 0, sizeof cf);
   memcpy(cf.c, c, sizeof(double) * k);
-  k_multiaxpy<float, float><<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, V, ldv, k, cf, n);
+  launch_multiaxpy<float>(w, V, ldv, k, cf, n, (cudaStream_t)s);
   return rc();
 }
 int hb_krylov_multiaxpy_f32_to_f64(double *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s) {
