@@ -284,10 +284,32 @@ def run_gpu(args, rank, world):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if not args.no_timeloop:
+        line["timeloop"] = timeloop_leg(args.timeloop_steps)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_leg(args.cpu_sample, use_ref=False).items() if k != "seconds_per_step"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def timeloop_leg(steps):
+    """Implicit BDF2 steps of the mixed-precision configuration (Taylor-Green, periodic [0, 2 pi]^3, 32^3 elements, P=5 Q=6,
+    10,485,760 DOF, acoustic CFL 1) in FP64 and in mixed precision: time-steps per second after the first (BDF1) step, with
+    the Newton/GMRES iteration counts and the largest relative difference of the monitors between the two runs."""
+    NS = importlib.import_module("honee-4aiad_b200.navierstokes")
+    out = {"workload": "Taylor-Green 32^3 hex, P=5 Q=6, periodic, Re 1600, Ma 0.1, acoustic CFL 1, BDF2 + Newton + GMRES(30) + Jacobi",
+           "steps": steps}
+    runs = {}
+    for tag, mixed in (("fp64", False), ("mixed", True)):
+        r = NS.run("taylor_green", faces=32, degree=4, steps=steps, cfl=1.0, mixed=mixed, monitor_every=steps)
+        runs[tag] = r
+        out[tag] = {"steps_per_s": r.steps_per_second(), "newton_its": [s.newton_its for s in r.stats],
+                    "ksp_its": [s.ksp_its for s in r.stats], "final_rel_residual": max(s.res_final / s.res0 for s in r.stats)}
+    out["dofs"] = runs["fp64"].dofs
+    out["dt"] = runs["fp64"].dt
+    out["mixed_speedup"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+    out["mixed_vs_fp64_monitor_rel_diff"] = NS.compare(runs["fp64"], runs["mixed"])
+    return out
 
 
 # DRAM bytes (read + write) per element of one k_ifunction<4,5> launch, from an ncu capture of a 4,096-element colour
@@ -337,6 +359,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--only-kernels", action="store_true", help="time the fused kernels only (profiling runs)")
+    ap.add_argument("--no-timeloop", action="store_true", help="skip the implicit time-loop leg")
+    ap.add_argument("--timeloop-steps", type=int, default=5)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
