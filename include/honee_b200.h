@@ -189,6 +189,37 @@ HB_EXPORT int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double
 HB_EXPORT int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double dt, double *d_scratch,
                              double minmax[2], void *s);
 
+/* ---- Learned subgrid-stress closure (the data-driven SGS model of qfunctions/sgs_dd_model.h, sgs_dd_utils.h,
+ *      grid_anisotropy_tensor.h; problems/sgs_dd_model.c:561-737).  The reference evaluates a trained network; here the
+ *      network is also trained on the GPU from filtered fine-grid data. ---- */
+typedef struct {
+  int   hidden1, hidden2;   /* hidden widths: 20, 20 (two layers) or 20, 0 (one layer, the reference's 6-20-6 form) */
+  float leaky_alpha;        /* negative slope of the activation; 0 = ReLU (the reference default) */
+  float out_bounds[6][2];   /* min-max bounds {lo, hi} that de-normalise the 6 outputs (OutScaling.dat) */
+} HbMlpDesc;
+
+/* Parameter count of the network (W1, b1, [W2, b2,] W3, b3; W row-major [out][in]); negative: unsupported shape. */
+HB_EXPORT int hb_mlp_num_params(const HbMlpDesc *d);
+/* One training step, FP32: MSE over `batch` samples of X/Y ([n][6] each, device), drawn with replacement by a hash of
+ * (seed, step) or taken from idx[batch] when idx is not NULL; then Adam (beta 0.9/0.999, eps 1e-8) at learning rate lr
+ * on w with moments m, v (step is 1-based).  lr == 0: gradient only (d_grad receives it, w/m/v untouched).
+ * d_work >= ceil(batch/256) * (num_params + 1) floats; d_loss[0] = the batch loss; d_grad (optional) = the gradient. */
+HB_EXPORT int hb_mlp_train_step(const HbMlpDesc *d, float *w, float *m, float *v, const float *X, const float *Y, int64_t n, const int32_t *idx,
+                                int batch, uint64_t seed, int step, float lr, float *d_work, float *d_loss, float *d_grad, void *s);
+/* Batch inference Y = net(X), [n][6] FP32 on the device. */
+HB_EXPORT int hb_mlp_forward(const HbMlpDesc *d, const float *w, const float *X, float *Y, int64_t n, void *s);
+/* Point-wise maps (FP64, arrays of n points on the device): the anisotropy tensor (KM) and width from dXdx [n][9]; the
+ * model inputs, eigenframe E [n][9] and |G A| from the velocity gradient G [n][9] (G[i][j] = du_i/dx_j), A, delta and
+ * the kinematic viscosity; the physical stress (KM) from normalised outputs. */
+HB_EXPORT int hb_sgs_anisotropy(int64_t n, const double *dXdx, double *kmA, double *delta, void *s);
+HB_EXPORT int hb_sgs_inputs(int64_t n, const double *G, const double *kmA, const double *delta, const double *nu, double *inputs, double *E,
+                            double *gmag, void *s);
+HB_EXPORT int hb_sgs_stress(int64_t n, const double *out_n, const double *delta, const double *E, const double *gmag, const float bounds[12],
+                            double *km_tau, void *s);
+/* Column-wise min/max of training targets Y [n][6] (d_work >= 3072 floats; synchronises), and the min-max map to [0, 1]. */
+HB_EXPORT int hb_sgs_target_bounds(const float *Y, int64_t n, float *d_work, float bounds[12], void *s);
+HB_EXPORT int hb_sgs_normalize_targets(float *Y, int64_t n, const float bounds[12], void *s);
+
 /* Library identification */
 const char *hb_version(void);
 

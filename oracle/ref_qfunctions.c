@@ -8,10 +8,15 @@
  */
 #include <ceed/types.h>
 
+#include "differential_filter.h"
+#include "grid_anisotropy_tensor.h"
 #include "monitor_totalkineticenergy.h"
 #include "newtonian.h"
 #include "setupgeo.h"
+#include "sgs_dd_model.h"
 #include "taylorgreen.h"
+
+#include <stddef.h>
 
 #define EXPORT __attribute__((visibility("default")))
 typedef const CeedScalar *const *In;
@@ -52,3 +57,39 @@ EXPORT void ref_StateToQ_fwd(const NewtonianIGProperties *gas, const CeedScalar 
 }
 EXPORT int ref_context_size(void) { return (int)sizeof(struct NewtonianIdealGasContext_); }
 EXPORT int ref_setup_context_size(void) { return (int)sizeof(struct SetupContext_); }
+
+/* Data-driven SGS closure and its training data (sgs_dd_model.h, sgs_dd_training.h, grid_anisotropy_tensor.h) and the
+ * differential filter (differential_filter.h). */
+EXPORT int ref_ComputeSgsDDNodal_Conserv(void *c, CeedInt Q, In in, Out out) { return ComputeSgsDDNodal_Conserv(c, Q, in, out); }
+EXPORT int ref_AnisotropyTensorCollocate(void *c, CeedInt Q, In in, Out out) { return AnisotropyTensorCollocate(c, Q, in, out); }
+EXPORT int ref_IFunction_NodalSgs_Conserv(void *c, CeedInt Q, In in, Out out) { return IFunction_NodalSgs_Conserv(c, Q, in, out); }
+EXPORT int ref_DifferentialFilter_RHS_Conserv(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_RHS_Conserv(c, Q, in, out); }
+EXPORT int ref_DifferentialFilter_LHS_11(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_LHS_11(c, Q, in, out); }
+EXPORT int ref_DifferentialFilter_LHS_1(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_LHS_1(c, Q, in, out); }
+/* ComputeSgsDDInputs / ComputeSgsDDOutputs / DataDrivenInference on single points */
+EXPORT void ref_ComputeSgsDDInputs(const CeedScalar grad_velo[3][3], const CeedScalar km_A_ij[6], CeedScalar delta, CeedScalar nu,
+                                   CeedScalar evec[3][3], CeedScalar inputs[6], CeedScalar *gmag) {
+  ComputeSgsDDInputs(grad_velo, km_A_ij, delta, nu, evec, inputs, gmag);
+}
+EXPORT void ref_ComputeSgsDDOutputs(CeedScalar outputs[6], CeedScalar delta, const CeedScalar evec[3][3], const CeedScalar bounds[6][2],
+                                    CeedScalar gmag, CeedScalar km_sgs[6]) {
+  ComputeSgsDDOutputs(outputs, delta, evec, bounds, gmag, km_sgs);
+}
+EXPORT void ref_DataDrivenInference(const CeedScalar *inputs, CeedScalar *outputs, void *ctx) { DataDrivenInference(inputs, outputs, ctx); }
+EXPORT int  ref_Diagonalize3(CeedScalar A[3][3], CeedScalar eval[3], CeedScalar evec[3][3], int sweeps) {
+  CeedInt work[3] = {0};
+  return Diagonalize3(A, eval, evec, work, SORT_DECREASING_EVALS, true, sweeps);
+}
+/* struct layouts the tests build contexts with: {sizeof, offsetof(newt_ctx), offsetof(offsets), offsetof(data)} */
+EXPORT void ref_sgs_dd_ctx_layout(size_t out[4]) {
+  out[0] = sizeof(struct SgsDDContext_);
+  out[1] = offsetof(struct SgsDDContext_, newt_ctx);
+  out[2] = offsetof(struct SgsDDContext_, offsets);
+  out[3] = offsetof(struct SgsDDContext_, data);
+}
+EXPORT void ref_diff_filter_ctx_layout(size_t out[4]) {
+  out[0] = sizeof(struct DifferentialFilterContext_);
+  out[1] = offsetof(struct DifferentialFilterContext_, newt_ctx);
+  out[2] = offsetof(struct DifferentialFilterContext_, kernel_scaling);
+  out[3] = offsetof(struct DifferentialFilterContext_, damping_function);
+}
