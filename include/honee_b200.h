@@ -11,6 +11,7 @@
 #ifndef HONEE_B200_H
 #define HONEE_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #include "honee_b200_types.h"
@@ -219,6 +220,32 @@ HB_EXPORT int hb_sgs_stress(int64_t n, const double *out_n, const double *delta,
 /* Column-wise min/max of training targets Y [n][6] (d_work >= 3072 floats; synchronises), and the min-max map to [0, 1]. */
 HB_EXPORT int hb_sgs_target_bounds(const float *Y, int64_t n, float *d_work, float bounds[12], void *s);
 HB_EXPORT int hb_sgs_normalize_targets(float *Y, int64_t n, const float bounds[12], void *s);
+
+/* ---- Differential filter (src/differential_filter.c, qfunctions/differential_filter.h) and SGS training pairs ---- */
+typedef struct {
+  int    grid_based_width;  /* 1: width tensor from the element anisotropy tensor (-diff_filter_grid_based_width), 0: identity */
+  double width_scaling[3];  /* -diff_filter_width_scaling (default 1, 1, 1) */
+  double kernel_scaling;    /* -diff_filter_kernel_scaling (default 0.1) */
+} HbFilterOptions;
+
+/* y = (M + K_alpha) x for nc node-interleaved fields on the element operator's mesh (DifferentialFilter_LHS_N). */
+HB_EXPORT int hb_filter_apply(const HbElemOp *op, int nc, const HbFilterOptions *o, const double *qdata, const double *x, double *y, void *s);
+/* The operator's diagonal, one value per node (the same for every field), and its reciprocal expanded to nc fields. */
+HB_EXPORT int hb_filter_diagonal(const HbElemOp *op, const HbFilterOptions *o, const double *qdata, double *diag, void *s);
+HB_EXPORT int hb_filter_jacobi(const double *diag, int64_t nodes, int nc, double *dinv, void *s);
+/* rhs [node][11] = int phi (P, u, T, uu_xx, uu_yy, uu_zz, uu_yz, uu_xz, uu_xy) of the conservative state q
+ * (DifferentialFilter_RHS_Conserv). */
+HB_EXPORT int hb_filter_rhs(const HbElemOp *op, const void *ctx184, const double *qdata, const double *q, double *rhs, void *s);
+/* CG + point Jacobi to relative natural-norm tolerance rtol; work >= hb_filter_work_doubles(op, nc) doubles.  Returns
+ * HB_ERROR_INCOMPLETE when max_it was reached. */
+HB_EXPORT size_t hb_filter_work_doubles(const HbElemOp *op, int nc);
+HB_EXPORT int hb_filter_solve(const HbElemOp *op, int nc, const HbFilterOptions *o, const double *qdata, const double *b, double *x, double rtol,
+                              int max_it, double *work, int *its, double *rel_norm, void *s);
+/* Training pairs at every quadrature point (X: model inputs, Y: filtered stress in the model's output frame scaled by
+ * delta^2 |G A|^2, [num_elem * Q^3][6] FP32) from filtered fields [node][11] (qfunctions/sgs_dd_training.h:22-56 with
+ * the stress taken into the model frame); width_scale = filter width / this mesh's element width. */
+HB_EXPORT int hb_sgs_training_pairs(const HbElemOp *op, const void *ctx184, const double *qdata, const double *filtered, double width_scale, float *X,
+                                    float *Y, void *s);
 
 /* Library identification */
 const char *hb_version(void);

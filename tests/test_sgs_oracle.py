@@ -112,3 +112,58 @@ def test_oracle_equals_reference_library_on_fresh_points():
         R.ref_Diagonalize3(Mc.ctypes.data_as(dp), ev.ctypes.data_as(dp), Ev.ctypes.data_as(dp), 5)
         np.testing.assert_array_equal(e2, ev)
         np.testing.assert_array_equal(E2, Ev)
+
+
+def _filter_ctx(R, newt: bytes, grid_based, ws, ks):
+    import ctypes as C
+    lay = (C.c_size_t * 4)()
+    R.ref_diff_filter_ctx_layout(lay)
+    size, o_newt, o_ks, o_damp = lay[:]
+    buf = bytearray(size)
+    buf[0] = 1 if grid_based else 0
+    np.frombuffer(buf, dtype=np.float64, count=3, offset=8)[:] = ws           # width_scaling follows the bool
+    np.frombuffer(buf, dtype=np.float64, count=1, offset=o_ks)[:] = ks
+    np.frombuffer(buf, dtype=np.int32, count=1, offset=o_damp)[:] = 0         # DIFF_FILTER_DAMP_NONE
+    buf[o_newt:o_newt + len(newt)] = newt
+    return bytes(buf)
+
+
+@pytest.mark.parametrize("grid_based", [False, True])
+def test_filter_pointwise_forms_match_reference(grid_based):
+    import oracle as O
+    import filter_oracle as FO
+    R = O.ref()
+    if R is None:
+        pytest.skip("oracle/_ref not built")
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    rng = np.random.default_rng(31)
+    n, N = 64, 11
+    ctx = prob.newtonian_context(2, cv=717.5, cp=1004.5, mu=1.8e-5, k=0.0257)
+    ws, ks = np.array([1.5, 0.7, 2.0]), 0.1
+    cb = _filter_ctx(R, prob.context_bytes(ctx), grid_based, ws, ks)
+    q = rng.normal(0, 1, (N, n))
+    gq = rng.normal(0, 1, (3 * N, n))
+    dXdx = np.stack([np.diag(rng.uniform(5, 50, 3)) + rng.normal(0, 2, (3, 3)) for _ in range(n)])
+    qdata = np.zeros((10, n))
+    qdata[0] = rng.uniform(0.5, 2, n)
+    qdata[1:] = dXdx.reshape(n, 9).T
+    Aij = np.zeros((7, n))
+    O.call_qf(R.ref_AnisotropyTensorCollocate, None, n, [np.ascontiguousarray(qdata)], [Aij])
+    v = np.zeros((N, n))
+    gv = np.zeros((3 * N, n))
+    O.call_qf(R.ref_DifferentialFilter_LHS_11, cb, n, [q, gq, Aij, np.zeros((3, n)), np.ascontiguousarray(qdata)], [v, gv])
+    for i in range(n):
+        al = FO.alpha_at(dXdx[i], grid_based, ws, ks)
+        vv, gg = FO.lhs_point(q[:, i], gq[:, i].reshape(3, N), dXdx[i], qdata[0, i], al)
+        np.testing.assert_allclose(vv, v[:, i], rtol=1e-14)
+        np.testing.assert_allclose(gg, gv[:, i].reshape(3, N), rtol=1e-11, atol=1e-12 * np.abs(gg).max())
+    # right-hand side integrand: wdetJ * (P, u, T, u_i u_j)
+    P = 101325 * (1 + 0.01 * rng.uniform(-1, 1, n))
+    T = 288 * (1 + 0.01 * rng.uniform(-1, 1, n))
+    u = rng.uniform(-20, 20, (3, n))
+    qc = prob.conservative_from_primitive(ctx.gas, P, u, T)
+    v0, v1 = np.zeros((5, n)), np.zeros((6, n))
+    O.call_qf(R.ref_DifferentialFilter_RHS_Conserv, cb, n, [np.ascontiguousarray(qc), np.ascontiguousarray(qdata)], [v0, v1])
+    w = qdata[0]
+    np.testing.assert_allclose(v0, w * np.stack([P, u[0], u[1], u[2], T]), rtol=1e-12)
+    np.testing.assert_allclose(v1, w * np.stack([u[0] ** 2, u[1] ** 2, u[2] ** 2, u[1] * u[2], u[0] * u[2], u[0] * u[1]]), rtol=1e-11)
