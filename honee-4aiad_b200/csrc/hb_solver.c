@@ -37,6 +37,9 @@ struct HbTimeStepper {
   void  *V, *w, *zvec, *diag, *jd32, *y_work;
   float *res32;
   double *delta;
+  /* optional learned closure fused into the residual (host copy of the weights) */
+  HbMlpDesc sgs_desc;
+  float    *sgs_w;
 };
 
 #define CUCK(x)                                \
@@ -106,6 +109,7 @@ int hb_ts_destroy(HbTimeStepper *ts) {
                ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64};
   for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
     if (p[i]) cudaFree(p[i]);
+  free(ts->sgs_w);
   free(ts);
   return HB_SUCCESS;
 }
@@ -124,6 +128,20 @@ int hb_ts_get_state(HbTimeStepper *ts, double *d_q, double *t) {
 }
 
 const void *hb_ts_context(HbTimeStepper *ts) { return &ts->ctx; }
+
+int hb_ts_set_sgs(HbTimeStepper *ts, const HbMlpDesc *d, const float *h_weights) {
+  if (!ts) return HB_ERROR_INVALID;
+  free(ts->sgs_w);
+  ts->sgs_w = NULL;
+  if (!d || !h_weights) return HB_SUCCESS; /* closure off */
+  const int np = hb_mlp_num_params(d);
+  if (np < 0) return np;
+  ts->sgs_w = (float *)malloc(sizeof(float) * (size_t)np);
+  if (!ts->sgs_w) return HB_ERROR_NOMEM;
+  memcpy(ts->sgs_w, h_weights, sizeof(float) * (size_t)np);
+  ts->sgs_desc = *d;
+  return HB_SUCCESS;
+}
 
 /* ---- small helpers on the Krylov precision ---- */
 static int kv_norm2(HbTimeStepper *ts, const void *x, double *nrm) {
@@ -310,7 +328,8 @@ int hb_ts_step(HbTimeStepper *ts, HbStepStats *st) {
   for (; it <= ts->o.newton_max_it; it++) {
     HBCK(hb_bdf_qdot(ts->q, ts->z, alpha, ts->qdot, ts->n, ts->s));
     HbIFunctionIO io = {ts->q, ts->qdot, ts->qdata, ts->o.jacobian_fp32 ? NULL : ts->jd64, ts->o.jacobian_fp32 ? (float *)ts->jd32 : NULL, ts->res, 0};
-    HBCK(hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s));
+    if (ts->sgs_w) HBCK(hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io, &ts->sgs_desc, ts->sgs_w, ts->s));
+    else HBCK(hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s));
     double r2;
     HBCK(hb_vec_reduce_f64(ts->res, NULL, ts->n, 1, ts->scratch, &r2, ts->s));
     rn = sqrt(r2);

@@ -19,6 +19,7 @@
 #include "honee_b200.h"
 #include "newtonian_qf.cuh"
 #include "pipeline.cuh"
+#include "sgs.cuh"
 
 // Optional per-phase cycle accounting of the fused kernels (debug builds with -DHB_PHASE_TIMING only): thread 0 of
 // every CTA adds the clock64() deltas of each phase to hb_phase_cycles[].
@@ -462,6 +463,60 @@ struct Plan {
 };
 
 // ---------------------------------------------------------------------------------------------------------------------
+// Learned SGS closure fused into the residual (qfunctions/sgs_dd_model.h:65-98 and :205-241 evaluated at the quadrature
+// points instead of through a nodal projection): velocity gradient -> anisotropy-frame features -> FP32 network (weights
+// in the kernel's parameter space, read through the constant cache) -> de-normalised SGS stress -> its flux, added to the
+// reference-direction fluxes.  SGS = 1: one hidden layer of 20 (the reference's model), 2: two hidden layers of 20.
+
+template <int SGS>
+struct SgsArg {
+  int unused;
+};
+template <>
+struct SgsArg<1> {
+  float w[sgs::MlpShape<20, 0>::size];
+  float alpha;
+  float b[6][2];
+};
+template <>
+struct SgsArg<2> {
+  float w[sgs::MlpShape<20, 20>::size];
+  float alpha;
+  float b[6][2];
+};
+
+template <int SGS>
+__device__ __forceinline__ void sgs_add(const PhysConst<double> &c, const double q[5], const double gref[3][5], double wdetJ, const double X[3][3],
+                                        const SgsArg<SGS> &sg, double gv[3][5]) {
+  St<double> st;
+  double inv_rho, etot, eint;
+  state_from_u(c, q, st, inv_rho, etot, eint);
+  St<double> gs[3];
+  physical_gradient(c, st, inv_rho, etot, eint, gref, X, gs);
+  double G[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) G[i][j] = gs[j].u[i];
+  double kmA[6], delta, E[3][3], in[6], gmag;
+  sgs::anisotropy(X, kmA, delta);
+  sgs::inputs(G, kmA, delta, c.mu * inv_rho, E, in, gmag);
+  float xf[6], yf[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) xf[k] = (float)in[k];
+  sgs::mlp_forward<20, SGS == 2 ? 20 : 0>(sg.w, sg.alpha, xf, yf);
+  double y[6], km[6], F[5][3];
+#pragma unroll
+  for (int k = 0; k < 6; k++) y[k] = (double)yf[k];
+  sgs::outputs_to_stress(y, delta, E, sg.b, gmag, km);
+  sgs::flux(st.u, km, F);
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+#pragma unroll
+    for (int k = 0; k < 5; k++) gv[d][k] -= wdetJ * (X[d][0] * F[k][0] + X[d][1] * F[k][1] + X[d][2] * F[k][2]);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
 // IFunction
 
 struct IfunctionPtrs {
@@ -473,8 +528,9 @@ struct IfunctionPtrs {
   int qdata_tma;      // qdata blocks can be bulk-copied (16-byte aligned base)
 };
 
-template <int P, int Q, bool ST>
-__global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p) {
+template <int P, int Q, bool ST, int SGS = 0>
+__global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p,
+                                                                                               const SgsArg<SGS> sg) {
   constexpr int NT = nthreads_for<double>(Q);
   using L = Plan<P, Q, 2, double, false, ST>;
   constexpr int Q3 = L::Q3;
@@ -582,6 +638,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
         }
       };
       ifunction_point_stream<double>(a.pc, qi, gref, qd, wdetJ, X, x0, v, gv, emit);
+      if constexpr (SGS > 0) sgs_add<SGS>(a.pc, qi, gref, wdetJ, X, sg, gv);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
         sU[c * Q3 + q] = v[c];
@@ -1010,11 +1067,12 @@ static size_t smem_bytes(int P, int Q) {
   return sizeof(T) * (size_t)(10 * P3 + 10 * P * P * Q + 10 * P * Q * Q + 10 * Q3 + 15 * Q3);
 }
 
-template <int P, int Q, bool ST>
-static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
+template <int P, int Q, bool ST, int SGS = 0>
+static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s,
+                              const SgsArg<SGS> &sg = SgsArg<SGS>{}) {
   using L = Plan<P, Q, 2, double, false, ST>;
   const size_t sm = L::bytes;
-  cudaFuncSetAttribute(k_ifunction<P, Q, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_ifunction<P, Q, ST, SGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   IfunctionPtrs p;
   p.q = io->q;
   p.q_dot = io->q_dot;
@@ -1026,11 +1084,11 @@ static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx,
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<double> a = make_args<double>(op, ctx, io->qdata, c);
     if (a.n_elems == 0) continue;
-    k_ifunction<P, Q, ST><<<grid_for(op, a.n_elems, k_ifunction<P, Q, ST>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p);
+    k_ifunction<P, Q, ST, SGS><<<grid_for(op, a.n_elems, k_ifunction<P, Q, ST, SGS>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p,
+                                                                                                                                               sg);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
-
 template <int P, int Q>
 static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
   // staged per-point data (TMA, 3 CTAs/SM) measured faster than direct loads at 4 CTAs/SM with spills
@@ -1085,6 +1143,8 @@ static int launch_diagonal(const HbElemOp *op, const HbNewtonianContext &ctx, co
 // (P, Q) pairs compiled: polynomial degree 1..5 with q_extra 0 or 1 (Q = P or P + 1); the benchmark configurations use
 // (3,3), (4,5) and (5,6).
 #define HB_PQ_LIST(X) X(2, 2) X(2, 3) X(3, 3) X(3, 4) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7)
+// bases the residual with the fused SGS closure is built for (the coarse LES runs at degree 2 and 3)
+#define HB_SGS_PQ_LIST(X) X(3, 3) X(3, 4) X(4, 5)
 
 }  // namespace hb
 
@@ -1108,6 +1168,45 @@ extern "C" int hb_ifunction_apply(const HbElemOp *op, const void *ctx184, const 
   if (op->P == PP && op->Q == QQ) return launch_ifunction<PP, QQ>(op, ctx, io, s);
   HB_PQ_LIST(HB_CASE)
 #undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+
+template <int SGS>
+static int fill_sgs(const HbMlpDesc *d, const float *w, SgsArg<SGS> &sg) {
+  const int np = hb_mlp_num_params(d);
+  if (np != (int)(sizeof sg.w / sizeof sg.w[0])) return HB_ERROR_INVALID;
+  memcpy(sg.w, w, sizeof sg.w);
+  sg.alpha = d->leaky_alpha;
+  memcpy(sg.b, d->out_bounds, sizeof sg.b);
+  return HB_SUCCESS;
+}
+
+extern "C" int hb_ifunction_apply_sgs(const HbElemOp *op, const void *ctx184, const HbIFunctionIO *io, const HbMlpDesc *d, const float *h_weights,
+                                      void *stream) {
+  int err = check_op(op);
+  if (err) return err;
+  if (!d || !h_weights || d->hidden1 != 20 || (d->hidden2 != 0 && d->hidden2 != 20)) return HB_ERROR_INVALID;
+  HbNewtonianContext ctx;
+  memcpy(&ctx, ctx184, sizeof ctx);
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE || ctx.divFdiff_method != HB_DIV_DIFF_FLUX_PROJ_NONE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.idl_enable && !op->d_x_elem) return HB_ERROR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!io->add && cudaMemsetAsync(io->v, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
+  if (d->hidden2 == 20) {
+    SgsArg<2> sg;
+    if ((err = fill_sgs<2>(d, h_weights, sg))) return err;
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_ifunction_v<PP, QQ, true, 2>(op, ctx, io, s, sg);
+    HB_SGS_PQ_LIST(HB_CASE)
+#undef HB_CASE
+  } else {
+    SgsArg<1> sg;
+    if ((err = fill_sgs<1>(d, h_weights, sg))) return err;
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_ifunction_v<PP, QQ, true, 1>(op, ctx, io, s, sg);
+    HB_SGS_PQ_LIST(HB_CASE)
+#undef HB_CASE
+  }
   return HB_ERROR_UNSUPPORTED;
 }
 

@@ -95,6 +95,14 @@ class ElemOp:
         cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
         _chk(_load().hb_ifunction_apply(self.ptr, cb, C.byref(io), _stream(stream)), "hb_ifunction_apply")
 
+    def ifunction_sgs(self, ctx_bytes: bytes, q, q_dot, qdata, v, desc, weights, jac_data=None, jac_data_f32=None, add=False, stream=None):
+        """IFunction with the learned closure fused in (desc: sgs.HbMlpDesc, weights: float32 host array)."""
+        io = HbIFunctionIO(_addr(q), _addr(q_dot), _addr(qdata), _addr(jac_data), _addr(jac_data_f32), _addr(v), int(add))
+        cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        _chk(_load().hb_ifunction_apply_sgs(self.ptr, cb, C.byref(io), C.byref(desc), w.ctypes.data_as(C.POINTER(C.c_float)), _stream(stream)),
+             "hb_ifunction_apply_sgs")
+
     def ijacobian(self, ctx_bytes: bytes, qdata, jac_data, dq, v, add=False, fp32=False, stream=None):
         cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
         fn = _load().hb_ijacobian_apply_f32 if fp32 else _load().hb_ijacobian_apply_f64

@@ -72,6 +72,15 @@ class TimeStepper:
         _chk(_load().hb_ts_step(self.ptr, C.byref(s)), "hb_ts_step")
         return StepStats(s.newton_its, s.ksp_its, s.converged_reason, s.res0, s.res_final, s.seconds)
 
+    def set_sgs(self, desc=None, weights=None):
+        """Fuse the learned closure (sgs.HbMlpDesc, float32 weights) into the residual, or remove it (no arguments)."""
+        if desc is None:
+            _chk(_load().hb_ts_set_sgs(self.ptr, None, None), "hb_ts_set_sgs")
+            return
+        self._sgs_w = np.ascontiguousarray(weights, dtype=np.float32)
+        self._sgs_desc = desc
+        _chk(_load().hb_ts_set_sgs(self.ptr, C.byref(desc), self._sgs_w.ctypes.data_as(C.POINTER(C.c_float))), "hb_ts_set_sgs")
+
     def context_bytes(self) -> bytes:
         L = _load()
         L.hb_ts_context.restype = C.c_void_p

@@ -207,6 +207,14 @@ HB_EXPORT int hb_mlp_num_params(const HbMlpDesc *d);
  * d_work >= ceil(batch/256) * (num_params + 1) floats; d_loss[0] = the batch loss; d_grad (optional) = the gradient. */
 HB_EXPORT int hb_mlp_train_step(const HbMlpDesc *d, float *w, float *m, float *v, const float *X, const float *Y, int64_t n, const int32_t *idx,
                                 int batch, uint64_t seed, int step, float lr, float *d_work, float *d_loss, float *d_grad, void *s);
+/* IFunction with the closure fused in at every quadrature point: hb_ifunction_apply plus the SGS flux of the network
+ * (weights: host array of hb_mlp_num_params floats, copied into the launch; bounds and activation from d).  Built for
+ * P, Q = (3, 3), (3, 4), (4, 5); the Jacobian operators do not include the closure (nor does the reference's). */
+HB_EXPORT int hb_ifunction_apply_sgs(const HbElemOp *op, const void *ctx184, const HbIFunctionIO *io, const HbMlpDesc *d, const float *h_weights,
+                                     void *stream);
+/* Attach (or with d == NULL detach) the closure to a time stepper: its residual becomes hb_ifunction_apply_sgs with these
+ * weights (copied); the Krylov Jacobian stays the Newtonian one. */
+HB_EXPORT int hb_ts_set_sgs(HbTimeStepper *ts, const HbMlpDesc *d, const float *h_weights);
 /* Batch inference Y = net(X), [n][6] FP32 on the device. */
 HB_EXPORT int hb_mlp_forward(const HbMlpDesc *d, const float *w, const float *X, float *Y, int64_t n, void *s);
 /* Point-wise maps (FP64, arrays of n points on the device): the anisotropy tensor (KM) and width from dXdx [n][9]; the

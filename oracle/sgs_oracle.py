@@ -185,3 +185,44 @@ def reference_layout_to_flat(b1, b2, w1_file, w2_file):
     W1 = np.asarray(w1_file).reshape(6, 20).T
     W2 = np.asarray(w2_file).reshape(20, 6).T
     return np.concatenate([W1.reshape(-1), np.asarray(b1)[:20], W2.reshape(-1), np.asarray(b2)[:6]])
+
+
+def residual_contribution(mesh, basis, qdata, q, gas, params, h1, h2, bounds, alpha=0.0, float32_net=True):
+    """Nodal residual contribution of the closure's flux (IFunction_NodalSgs, sgs_dd_model.h:219-241, with the stress of
+    ComputeSgsDD_Fused evaluated at the quadrature points).  float32_net rounds the network's inputs, weights and
+    outputs to float32 the way the CUDA kernel evaluates it (FP64 everywhere else)."""
+    import filter_oracle as FO
+    P, Q = basis.P, basis.Q
+    Q3 = Q ** 3
+    Bq, D = FO.tensor_ops(basis.interp1d, basis.grad1d, P, Q)
+    nodes = mesh.offsets.reshape(mesh.num_elem, -1) // 5
+    qe = np.asarray(q).reshape(-1, 5)[nodes]
+    U = np.einsum("qp,epc->eqc", Bq, qe)
+    Gr = np.stack([np.einsum("qp,epc->eqc", Dr, qe) for Dr in D], axis=2)      # [E][Q3][3 dirs][5]
+    qd = np.asarray(qdata).reshape(mesh.num_elem, 10, Q3)
+    w32 = np.asarray(params, dtype=np.float32).astype(np.float64) if float32_net else np.asarray(params, dtype=np.float64)
+    out = np.zeros((mesh.num_nodes, 5))
+    for e in range(mesh.num_elem):
+        gv = np.zeros((Q3, 3, 5))
+        for k in range(Q3):
+            X = qd[e, 1:, k].reshape(3, 3)
+            rho, m = U[e, k, 0], U[e, k, 1:4]
+            u = m / rho
+            du_ref = (Gr[e, k][:, 1:4] - np.outer(Gr[e, k][:, 0], u)) / rho   # [dir][comp] d u / d xi
+            G = du_ref.T @ X
+            kmA, delta = anisotropy(X)
+            x, E, g = inputs(G, kmA, delta, gas.mu / rho)
+            if float32_net:
+                x = x.astype(np.float32).astype(np.float64)
+            y, _, _ = forward(w32, h1, h2, x[None, :], alpha)
+            if float32_net:
+                y = y.astype(np.float32).astype(np.float64)
+            km = outputs_to_stress(y[0], delta, E, np.asarray(bounds, dtype=np.float32).astype(np.float64), g)
+            tau = km_unpack(km)
+            F = np.zeros((5, 3))
+            F[1:4] = tau
+            F[4] = u @ tau
+            gv[k] = -qd[e, 0, k] * (X @ F.T)          # [dir][comp]
+        ye = sum(D[r].T @ gv[:, r, :] for r in range(3))
+        np.add.at(out, nodes[e], ye)
+    return out.reshape(-1)

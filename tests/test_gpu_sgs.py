@@ -131,3 +131,41 @@ def test_target_bounds_and_normalisation():
     yn = ty.cpu().numpy()
     assert yn.min() >= 0 and yn.max() <= 1.0000001
     np.testing.assert_allclose(yn, (Y - b[:, 0]) / (b[:, 1] - b[:, 0]), rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("model", ["reference_6_20_6", "xavier_6_20_20_6"])
+def test_residual_with_fused_closure_matches_oracle(model):
+    """IFunction with the closure minus IFunction without it equals the closure's flux contribution computed by the
+    oracle (FP32 network, FP64 elsewhere: 1e-5 relative)."""
+    import torch
+    from helpers import prob, rel_l2
+    import filter_oracle  # noqa: F401  (used by the oracle contribution)
+    K = importlib.import_module("honee-4aiad_b200.kernels")
+    L = 2 * np.pi
+    mesh = prob.box_mesh((3, 3, 3), 3, periodic=(1, 1, 1), hi=(L, L, L))
+    basis = prob.tensor_basis(3, 4)
+    tg = prob.taylor_green_context(2)
+    tg.u[0], tg.u[1], tg.u[2] = 0.2, 0.1, 0.3
+    q = prob.taylor_green_state(mesh, basis, tg)
+    ctx = tg.newt_ctx
+    ctx.dt, ctx.ijacobian_time_shift = 0.01, 150.0
+    cb = prob.context_bytes(ctx)
+    if model == "reference_6_20_6":
+        d, w = S.desc(20, 0, 0.0, GOLD["bounds"]), GOLD["weights"].astype(np.float32)
+    else:
+        d = S.desc(20, 20, 0.0, np.array([-1, 1] * 6, dtype=np.float64) * 0.5)
+        w = S.xavier_init(d, seed=8)
+    op = K.ElemOp(mesh, basis)
+    x = torch.from_numpy(np.ascontiguousarray(mesh.x_elem)).to("cuda:0")
+    qdata = torch.zeros(mesh.num_elem * 10 * basis.Q ** 3, dtype=torch.float64, device="cuda:0")
+    op.setup_qdata(x, qdata)
+    tq = torch.from_numpy(q).to("cuda:0")
+    tqd = torch.zeros_like(tq)
+    v0, v1 = torch.empty_like(tq), torch.empty_like(tq)
+    op.ifunction(cb, tq, tqd, qdata, v0)
+    op.ifunction_sgs(cb, tq, tqd, qdata, v1, d, w)
+    torch.cuda.synchronize()
+    got = (v1 - v0).cpu().numpy()
+    ref = SO.residual_contribution(mesh, basis, qdata.cpu().numpy(), q, ctx.gas, w, d.hidden1, d.hidden2, np.array(d.out_bounds[:]))
+    assert np.linalg.norm(ref) > 0
+    assert rel_l2(got, ref) < 1e-5, rel_l2(got, ref)
