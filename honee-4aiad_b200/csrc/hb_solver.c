@@ -37,9 +37,11 @@ struct HbTimeStepper {
   void  *V, *w, *zvec, *diag, *jd32, *y_work;
   float *res32;
   double *delta;
-  /* optional learned closure fused into the residual (host copy of the weights) */
+  /* optional learned closure fused into the residual (host copy of the weights); with sgs_lagged its contribution is
+   * evaluated once per step at the previous state and added to every Newton residual */
   HbMlpDesc sgs_desc;
   float    *sgs_w;
+  double   *sgs_res;
 };
 
 #define CUCK(x)                                \
@@ -65,6 +67,7 @@ void hb_solver_default_options(HbSolverOptions *o) {
   o->pc_jacobi     = 1;
   o->jacobian_fp32 = 0;
   o->cgs_refine    = 0; /* KSPGMRESSetCGSRefinementType default: never */
+  o->sgs_lagged    = 1;
 }
 
 static size_t ksz(const HbTimeStepper *ts) { return ts->o.jacobian_fp32 ? sizeof(float) : sizeof(double); }
@@ -110,6 +113,7 @@ int hb_ts_destroy(HbTimeStepper *ts) {
   for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
     if (p[i]) cudaFree(p[i]);
   free(ts->sgs_w);
+  if (ts->sgs_res) cudaFree(ts->sgs_res);
   free(ts);
   return HB_SUCCESS;
 }
@@ -138,6 +142,7 @@ int hb_ts_set_sgs(HbTimeStepper *ts, const HbMlpDesc *d, const float *h_weights)
   if (np < 0) return np;
   ts->sgs_w = (float *)malloc(sizeof(float) * (size_t)np);
   if (!ts->sgs_w) return HB_ERROR_NOMEM;
+  if (!ts->sgs_res && cudaMalloc((void **)&ts->sgs_res, sizeof(double) * (size_t)ts->n) != cudaSuccess) return HB_ERROR_NOMEM;
   memcpy(ts->sgs_w, h_weights, sizeof(float) * (size_t)np);
   ts->sgs_desc = *d;
   return HB_SUCCESS;
@@ -323,13 +328,23 @@ int hb_ts_step(HbTimeStepper *ts, HbStepStats *st) {
   ts->ctx.dt                   = dt;
   ts->ctx.ijacobian_time_shift = alpha;
   ts->ctx.time                 = ts->t + dt;
+  const int sgs_lag = ts->sgs_w && ts->o.sgs_lagged;
+  if (sgs_lag) { /* closure contribution at the previous state: F_sgs(q_n) - F(q_n), independent of q_dot */
+    HBCK(hb_vec_set_f64(ts->qdot, ts->n, 0.0, ts->s)); /* any finite q_dot; it cancels in the difference */
+    HbIFunctionIO io_a = {ts->q, ts->qdot, ts->qdata, NULL, NULL, ts->sgs_res, 0};
+    HbIFunctionIO io_b = {ts->q, ts->qdot, ts->qdata, NULL, NULL, ts->delta, 0};
+    HBCK(hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io_a, &ts->sgs_desc, ts->sgs_w, ts->s));
+    HBCK(hb_ifunction_apply(ts->op, &ts->ctx, &io_b, ts->s));
+    HBCK(hb_vec_axpy_f64(ts->sgs_res, -1.0, ts->delta, ts->n, ts->s));
+  }
   double r0 = 0, rn = 0;
   int    it = 0, ksp_total = 0, converged = 0;
   for (; it <= ts->o.newton_max_it; it++) {
     HBCK(hb_bdf_qdot(ts->q, ts->z, alpha, ts->qdot, ts->n, ts->s));
     HbIFunctionIO io = {ts->q, ts->qdot, ts->qdata, ts->o.jacobian_fp32 ? NULL : ts->jd64, ts->o.jacobian_fp32 ? (float *)ts->jd32 : NULL, ts->res, 0};
-    if (ts->sgs_w) HBCK(hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io, &ts->sgs_desc, ts->sgs_w, ts->s));
+    if (ts->sgs_w && !sgs_lag) HBCK(hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io, &ts->sgs_desc, ts->sgs_w, ts->s));
     else HBCK(hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s));
+    if (sgs_lag) HBCK(hb_vec_axpy_f64(ts->res, 1.0, ts->sgs_res, ts->n, ts->s));
     double r2;
     HBCK(hb_vec_reduce_f64(ts->res, NULL, ts->n, 1, ts->scratch, &r2, ts->s));
     rn = sqrt(r2);

@@ -242,6 +242,19 @@ __global__ void k_sgs_pairs(int P, int Q, const int32_t *__restrict__ offsets, c
   }
 }
 
+// conservative state (rho, rho u, E) of filtered fields (P, u, T, ...) [node][11], rho = P / (R T)
+__global__ void k_filtered_state(const double *__restrict__ f, int64_t nodes, double cv, double R, double *__restrict__ q) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+    const double *g = f + i * 11;
+    const double rho = g[0] / (R * g[4]);
+    q[i * 5 + 0] = rho;
+    q[i * 5 + 1] = rho * g[1];
+    q[i * 5 + 2] = rho * g[2];
+    q[i * 5 + 3] = rho * g[3];
+    q[i * 5 + 4] = rho * (cv * g[4] + 0.5 * (g[1] * g[1] + g[2] * g[2] + g[3] * g[3]));
+  }
+}
+
 __global__ void k_expand_recip(const double *__restrict__ d, int64_t nodes, int nc, double *__restrict__ dinv) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes * nc; i += (int64_t)gridDim.x * blockDim.x) dinv[i] = 1.0 / d[i / nc];
 }
@@ -324,6 +337,14 @@ int hb_filter_rhs(const HbElemOp *op, const void *ctx184, const double *qdata, c
 int hb_filter_jacobi(const double *diag, int64_t nodes, int nc, double *dinv, void *stream) {
   if (!diag || !dinv || nodes < 0 || nc < 1) return HB_ERROR_INVALID;
   if (nodes) k_expand_recip<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(diag, nodes, nc, dinv);
+  return rc();
+}
+
+int hb_filtered_state(const double *filtered, int64_t nodes, const void *ctx184, double *q, void *stream) {
+  if (!filtered || !ctx184 || !q || nodes < 0) return HB_ERROR_INVALID;
+  HbNewtonianContext c;
+  memcpy(&c, ctx184, sizeof c);
+  if (nodes) k_filtered_state<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(filtered, nodes, c.gas.cv, c.gas.cp - c.gas.cv, q);
   return rc();
 }
 

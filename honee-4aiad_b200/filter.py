@@ -65,6 +65,10 @@ class DifferentialFilter:
         its, rel = self.solve(b, x, 11, rtol, max_it)
         return x, its, rel
 
+    def conservative(self, filtered, q):
+        """Conservative state [node][5] of filtered fields (to run the monitors on the filtered solution)."""
+        _chk(_load().hb_filtered_state(_addr(filtered), C.c_int64(self.nodes), self.ctx, _addr(q), _stream(self.stream)), "hb_filtered_state")
+
     def training_pairs(self, filtered, width_scale, X, Y):
         _chk(_load().hb_sgs_training_pairs(self.op.ptr, self.ctx, _addr(self.qdata), _addr(filtered), C.c_double(width_scale), _addr(X), _addr(Y),
                                            _stream(self.stream)), "hb_sgs_training_pairs")

@@ -1,0 +1,239 @@
+"""Learned-closure coarse LES of the decaying Taylor-Green vortex, end to end on one GPU.
+
+  1. fine run: the plain method (no closure) on `fine_faces`^3 elements, snapshots of the state every `snap_every`
+     coarse steps' worth of time
+  2. each snapshot through the differential filter (filter width = the coarse element size: grid-based width, width
+     scaling = fine/coarse element ratio, kernel scaling 0.1 as src/differential_filter.c defaults) and into training
+     pairs at the fine quadrature points (model inputs of the filtered velocity gradient, the filtered stress
+     u_i u_j - u_i u_j in the model's output frame)
+  3. min-max normalisation of the targets (their bounds become the model's de-normalisation bounds, OutScaling), the
+     network (6-20-20-6, ReLU, Xavier init from a seed) trained with Adam on the GPU by this package's kernels
+  4. two coarse runs on `coarse_faces`^3 elements from the filtered initial state (the coarse nodes are a subset of the
+     fine ones for these nested meshes, so the filtered fine field is injected): without the closure, and with the
+     trained network in the residual (evaluated once per step at the previous state, hb_ts_set_sgs)
+  5. both compared with the filtered fine solution through the kinetic-energy monitor (total KE and the resolved strain
+     dissipation), with the GPU time of each run
+
+    python -m honee-4aiad_b200.les [--fine-faces 96 --coarse-faces 24 --degree 2 --t-end 2.0 ...]
+
+Everything on the device is a kernel of this package (operators, Krylov, filter, training, inference); torch tensors are
+the buffers.  Time steps are the BDF2 time loop of hb_solver.c at acoustic CFL `cfl` on each mesh's node spacing, the
+fine step a divisor of the coarse step so the snapshots fall on coarse step boundaries.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+
+import numpy as np
+
+from . import filter as FL
+from . import kernels as K
+from . import problem as prob
+from . import sgs as SG
+from . import solver as S
+
+
+class TGMesh:
+    """Periodic Taylor-Green box with its element operator, geometric factors and monitors."""
+
+    def __init__(self, faces, degree, q_extra=1, device="cuda:0"):
+        import torch
+        self.torch = torch
+        L = 2 * math.pi
+        self.faces, self.P, self.Q = faces, degree + 1, degree + 1 + q_extra
+        self.mesh = prob.box_mesh((faces,) * 3, self.P, periodic=(1, 1, 1), hi=(L, L, L))
+        self.basis = prob.tensor_basis(self.P, self.Q)
+        self.tg = prob.taylor_green_context(degree)
+        self.ctx = self.tg.newt_ctx
+        self.cb = prob.context_bytes(self.ctx)
+        self.op = K.ElemOp(self.mesh, self.basis)
+        dev = torch.device(device)
+        self.dev = dev
+        x = torch.from_numpy(np.ascontiguousarray(self.mesh.x_elem)).to(dev)
+        self.qdata = torch.empty(self.mesh.num_elem * 10 * self.Q ** 3, dtype=torch.float64, device=dev)
+        self.op.setup_qdata(x, self.qdata)
+        self.scratch = torch.empty(5 * self.mesh.num_elem, dtype=torch.float64, device=dev)
+        self.volume = L ** 3
+        gas = self.ctx.gas
+        self.wave_speed = 1.0 + math.sqrt(gas.cp / gas.cv * (gas.cp - gas.cv) * self.tg.reference.temperature)
+        self.h_node = L / (faces * (self.P - 1))
+
+    def initial_state(self):
+        return self.torch.from_numpy(prob.taylor_green_state(self.mesh, self.basis, self.tg)).to(self.dev)
+
+    def ke(self, q):
+        s = S.monitor_ke(self.op, self.cb, q, self.qdata, self.scratch) / self.volume
+        return {"TotalKineticEnergy": float(s[0]), "StrainDissipation": float(s[1]), "MuVorticity2": float(s[4])}
+
+
+def run_steps(m: TGMesh, dt, n_steps, every, mixed=True, sgs=None, on_snapshot=None, q0=None):
+    """BDF2 steps from q0 (default: the Taylor-Green initial condition); calls on_snapshot(k, q) every `every` steps
+    (and at step 0).  Returns the monitor rows and the summed step time (CUDA events inside hb_ts_step)."""
+    ts = S.TimeStepper(m.op, m.cb, m.qdata, dt=dt, bdf_order=2, jacobian_fp32=int(mixed))
+    if sgs is not None:
+        ts.set_sgs(*sgs)
+    q = m.initial_state() if q0 is None else q0.clone()
+    ts.set_state(q, 0.0)
+    rows, seconds = [], 0.0
+    rows.append({"time": 0.0, **m.ke(q)})
+    if on_snapshot:
+        on_snapshot(0, q)
+    for k in range(1, n_steps + 1):
+        st = ts.step()
+        if st.converged_reason != 1:
+            raise RuntimeError(f"step {k}: Newton did not converge ({st})")
+        seconds += st.seconds
+        if k % every == 0:
+            ts.get_state(q)
+            rows.append({"time": k * dt, **m.ke(q)})
+            if on_snapshot:
+                on_snapshot(k // every, q)
+    return rows, seconds
+
+
+def _max_rel_err(rows, ref, key, scale, from_start=False):
+    """max over the monitored times after t = 0 of |a - b| / scale; from_start compares the changes since t = 0."""
+    n = min(len(rows), len(ref))
+    a0, b0 = (rows[0][key], ref[0][key]) if from_start else (0.0, 0.0)
+    return max(abs((rows[k][key] - a0) - (ref[k][key] - b0)) for k in range(1, n)) / scale
+
+
+def study(fine_faces=96, coarse_faces=24, degree=2, t_end=2.0, snaps=4, cfl=1.0, train_steps=4000, batch=65536, lr=1e-3, seed=0,
+          clip=1e-3, log=None):
+    import torch
+
+    def say(**kw):
+        if log:
+            print(json.dumps(kw), file=log, flush=True)
+
+    if fine_faces % coarse_faces:
+        raise ValueError("the fine element count must be a multiple of the coarse one")
+    ratio = fine_faces // coarse_faces
+    coarse = TGMesh(coarse_faces, degree)
+    dt_c = cfl * coarse.h_node / coarse.wave_speed
+    every_c = max(1, int(round(t_end / dt_c / snaps)))
+    n_c = every_c * snaps
+    dt_f, n_f, every_f = dt_c / ratio, n_c * ratio, every_c * ratio
+    out = {"fine_faces": fine_faces, "coarse_faces": coarse_faces, "degree": degree, "dt_fine": dt_f, "dt_coarse": dt_c, "steps_fine": n_f,
+           "steps_coarse": n_c, "t_end": n_c * dt_c, "snapshots": snaps}
+
+    # 1-2. fine run, filtered snapshots, training pairs
+    fine = TGMesh(fine_faces, degree)
+    out["dofs_fine"], out["dofs_coarse"] = fine.mesh.l_size, coarse.mesh.l_size
+    filt = FL.DifferentialFilter(fine.op, fine.qdata, fine.cb, grid_based_width=True, width_scaling=(float(ratio),) * 3, kernel_scaling=0.1)
+    nq = fine.mesh.num_elem * fine.Q ** 3
+    Xs, Ys, ref_rows = [], [], []
+    t_filter = [0.0]
+    q_inject = [None]
+
+    def on_snap(k, q):
+        t0 = time.perf_counter()
+        fbar, its, rel = filt.filter_state(q)
+        qf = torch.empty(fine.mesh.l_size, dtype=torch.float64, device=fine.dev)
+        filt.conservative(fbar, qf)
+        ref_rows.append({"time": k * every_f * dt_f, **fine.ke(qf), "filter_cg_its": its})
+        if k == 0:  # the coarse runs start from the filtered initial state, injected at the shared nodes
+            Nf = fine.mesh.node_dims[0]
+            q_inject[0] = qf.view(Nf, Nf, Nf, 5)[::ratio, ::ratio, ::ratio, :].contiguous().view(-1)
+        if k > 0:
+            X = torch.empty(nq, 6, dtype=torch.float32, device=fine.dev)
+            Y = torch.empty_like(X)
+            filt.training_pairs(fbar, float(ratio), X, Y)
+            Xs.append(X)
+            Ys.append(Y)
+        torch.cuda.synchronize()
+        t_filter[0] += time.perf_counter() - t0
+        say(stage="fine snapshot", k=k, **ref_rows[-1])
+
+    rows_f, sec_f = run_steps(fine, dt_f, n_f, every_f, mixed=True, on_snapshot=on_snap)
+    out["fine"] = {"gpu_seconds": sec_f, "rows": rows_f}
+    out["filtered_fine"] = ref_rows
+    out["filter_seconds"] = t_filter[0]
+    del fine, filt
+    torch.cuda.empty_cache()
+
+    # 3. targets: drop non-finite rows, clip to the [clip, 1 - clip] quantiles per column, min-max normalise; train
+    X = torch.cat(Xs)
+    Y = torch.cat(Ys)
+    del Xs, Ys
+    keep = torch.isfinite(X).all(1) & torch.isfinite(Y).all(1)
+    X, Y = X[keep].contiguous(), Y[keep].contiguous()
+    g = torch.Generator(device=X.device).manual_seed(seed)
+    sub = Y[torch.randint(0, Y.shape[0], (min(Y.shape[0], 1_000_000),), device=Y.device, generator=g)]
+    lo = torch.quantile(sub, clip, dim=0)
+    hi = torch.quantile(sub, 1 - clip, dim=0)
+    Y = torch.maximum(torch.minimum(Y, hi), lo).contiguous()
+    bounds = np.stack([lo.cpu().numpy(), hi.cpu().numpy()], 1).reshape(12).astype(np.float64)
+    SG.normalize_targets(Y, bounds)
+    d = SG.desc(20, 20, 0.0, bounds)
+    tr = SG.Trainer(d, SG.xavier_init(d, seed), batch=batch, lr=lr, seed=seed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = tr.train(X, Y, train_steps, log_every=max(1, train_steps // 10))
+    torch.cuda.synchronize()
+    out["training"] = {"samples": int(X.shape[0]), "steps": train_steps, "batch": batch, "lr": lr, "seconds": time.perf_counter() - t0,
+                       "loss": hist, "bounds": bounds.tolist()}
+    say(stage="trained", **{k: v for k, v in out["training"].items() if k != "bounds"})
+    weights = tr.params()
+    out["weights"] = weights.tolist()
+    del X, Y, tr
+    torch.cuda.empty_cache()
+
+    # 4. coarse runs without and with the closure
+    rows_c0, sec_c0 = run_steps(coarse, dt_c, n_c, every_c, mixed=True, q0=q_inject[0])
+    try:
+        rows_c1, sec_c1 = run_steps(coarse, dt_c, n_c, every_c, mixed=True, sgs=(d, weights), q0=q_inject[0])
+        diverged = None
+    except RuntimeError as e:
+        rows_c1, sec_c1, diverged = [], float("nan"), str(e)
+    out["coarse_plain"] = {"gpu_seconds": sec_c0, "rows": rows_c0}
+    out["coarse_closure"] = {"gpu_seconds": sec_c1, "rows": rows_c1, "diverged": diverged}
+
+    # 5. errors against the filtered fine solution at the snapshot times
+    ke0 = ref_rows[0]["TotalKineticEnergy"]
+    eps_scale = max(abs(r["StrainDissipation"]) for r in ref_rows)
+    res = {}
+    for name, rows in (("plain", rows_c0), ("closure", rows_c1)):
+        if len(rows) < 2:
+            continue
+        res[name] = {"ke_err": _max_rel_err(rows, ref_rows, "TotalKineticEnergy", ke0),
+                     "ke_decay_err": _max_rel_err(rows, ref_rows, "TotalKineticEnergy", max(ke0 - r["TotalKineticEnergy"] for r in ref_rows),
+                                                  from_start=True),
+                     "dissipation_err": _max_rel_err(rows, ref_rows, "StrainDissipation", eps_scale)}
+    out["errors_vs_filtered_fine"] = res
+    out["cost_ratio_fine_over_closure"] = sec_f / sec_c1 if sec_c1 == sec_c1 and sec_c1 > 0 else None
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="learned-closure coarse LES of the Taylor-Green vortex")
+    ap.add_argument("--fine-faces", type=int, default=96)
+    ap.add_argument("--coarse-faces", type=int, default=24)
+    ap.add_argument("--degree", type=int, default=2)
+    ap.add_argument("--t-end", type=float, default=2.0)
+    ap.add_argument("--snaps", type=int, default=4)
+    ap.add_argument("--cfl", type=float, default=1.0)
+    ap.add_argument("--train-steps", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=None, help="write the full result (monitor rows, loss history, weights) as JSON here")
+    a = ap.parse_args(argv)
+    res = study(a.fine_faces, a.coarse_faces, a.degree, a.t_end, a.snaps, a.cfl, a.train_steps, a.batch, a.lr, a.seed, log=sys.stderr)
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(res, f)
+    summary = {k: v for k, v in res.items() if k not in ("weights", "fine", "coarse_plain", "coarse_closure", "filtered_fine", "training")}
+    summary["fine_gpu_seconds"] = res["fine"]["gpu_seconds"]
+    summary["coarse_plain_gpu_seconds"] = res["coarse_plain"]["gpu_seconds"]
+    summary["coarse_closure_gpu_seconds"] = res["coarse_closure"]["gpu_seconds"]
+    summary["final_loss"] = res["training"]["loss"][-1]
+    print(json.dumps(summary), flush=True)
+
+
+if __name__ == "__main__":
+    main()

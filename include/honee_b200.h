@@ -148,6 +148,8 @@ typedef struct {
   int    pc_every_newton; /* 0: diagonal once per time step (lagged), 1: every Newton iteration */
   int    jacobian_fp32;   /* mixed precision: FP32 Krylov basis, Jacobian action and diagonal; FP64 residual and update */
   int    cgs_refine;      /* 0: classical Gram-Schmidt once (PETSc default), 1: a second pass every iteration (CGS2) */
+  int    sgs_lagged;      /* with a closure attached: 1 (default) evaluate it at the previous state, explicitly, so Newton
+                             converges with the Newtonian Jacobian; 0 implicit (the Jacobian then omits its derivative) */
 } HbSolverOptions;
 
 typedef struct {
@@ -249,6 +251,8 @@ HB_EXPORT int hb_filter_rhs(const HbElemOp *op, const void *ctx184, const double
 HB_EXPORT size_t hb_filter_work_doubles(const HbElemOp *op, int nc);
 HB_EXPORT int hb_filter_solve(const HbElemOp *op, int nc, const HbFilterOptions *o, const double *qdata, const double *b, double *x, double rtol,
                               int max_it, double *work, int *its, double *rel_norm, void *s);
+/* Conservative state [node][5] of filtered fields [node][11] (rho = P / (R T)), e.g. to monitor the filtered solution. */
+HB_EXPORT int hb_filtered_state(const double *filtered, int64_t nodes, const void *ctx184, double *q, void *s);
 /* Training pairs at every quadrature point (X: model inputs, Y: filtered stress in the model's output frame scaled by
  * delta^2 |G A|^2, [num_elem * Q^3][6] FP32) from filtered fields [node][11] (qfunctions/sgs_dd_training.h:22-56 with
  * the stress taken into the model frame); width_scale = filter width / this mesh's element width. */

@@ -1,0 +1,21 @@
+"""End-to-end GPU test of the learned closure (the BASELINE learned-closure workflow at reduced size): a fine plain run,
+differential filter, training pairs, GPU training of the 6-20-20-6 network, and two coarse runs from the filtered
+initial state.  The closure must beat the closure-free coarse run against the filtered fine solution on the kinetic
+energy decay and on the resolved dissipation, at lower GPU cost than the fine run."""
+import importlib
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_learned_closure_beats_the_plain_coarse_run():
+    les = importlib.import_module("honee-4aiad_b200.les")
+    r = les.study(fine_faces=24, coarse_faces=6, degree=2, t_end=1.0, snaps=4, train_steps=800, batch=16384, lr=1e-3, seed=0)
+    assert r["coarse_closure"]["diverged"] is None
+    e = r["errors_vs_filtered_fine"]
+    assert e["closure"]["ke_decay_err"] < 0.5 * e["plain"]["ke_decay_err"], e
+    assert e["closure"]["ke_err"] < e["plain"]["ke_err"], e
+    assert e["closure"]["dissipation_err"] < e["plain"]["dissipation_err"], e
+    assert r["training"]["loss"][-1][1] < 0.1 * r["training"]["loss"][0][1]
+    assert r["fine"]["gpu_seconds"] > r["coarse_closure"]["gpu_seconds"]
