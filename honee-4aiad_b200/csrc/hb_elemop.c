@@ -16,7 +16,7 @@ const char *hb_version(void) { return "honee-b200 0.1 (sm_100a)"; }
 
 /* Greedy first-fit colouring: element e takes the lowest colour not used by any element sharing one of its offsets.
  * For lexicographically numbered boxes this yields the 2x2x2 parity colouring (8 colours). */
-static int color_elements(int num_elem, int elem_size, const int32_t *offsets, int64_t l_size, int32_t **color_ptr_out, int32_t **color_elem_out,
+int hb_internal_color_elements(int num_elem, int elem_size, const int32_t *offsets, int64_t l_size, int32_t **color_ptr_out, int32_t **color_elem_out,
                           int *num_colors_out) {
   uint64_t *mask  = (uint64_t *)calloc((size_t)l_size, sizeof(uint64_t));
   uint8_t  *color = (uint8_t *)malloc((size_t)num_elem);
@@ -129,7 +129,7 @@ int hb_elemop_create(int num_elem, int P, int Q, const int32_t *offsets, int64_t
   if (qweight1d) memcpy(op->qweight1d, qweight1d, sizeof(double) * Q);
   int err = collocated_derivative(P, Q, interp1d, grad1d, op->colo_grad1d);
   int32_t *color_elem = NULL;
-  if (!err) err = color_elements(num_elem, P3, offsets, l_size, &op->h_color_ptr, &color_elem, &op->num_colors);
+  if (!err) err = hb_internal_color_elements(num_elem, P3, offsets, l_size, &op->h_color_ptr, &color_elem, &op->num_colors);
   if (!err) {
     cudaGetDevice(&op->device);
     cudaDeviceGetAttribute(&op->num_sms, cudaDevAttrMultiProcessorCount, op->device);

@@ -42,6 +42,8 @@ struct HbTimeStepper {
   HbMlpDesc sgs_desc;
   float    *sgs_w;
   double   *sgs_res;
+  /* matrix-free (finite-difference) Jacobian action: perturbed state, rate and residual */
+  double *qp, *qdp, *rp;
 };
 
 #define CUCK(x)                                \
@@ -68,6 +70,7 @@ void hb_solver_default_options(HbSolverOptions *o) {
   o->jacobian_fp32 = 0;
   o->cgs_refine    = 0; /* KSPGMRESSetCGSRefinementType default: never */
   o->sgs_lagged    = 1;
+  o->jfnk          = 0;
 }
 
 static size_t ksz(const HbTimeStepper *ts) { return ts->o.jacobian_fp32 ? sizeof(float) : sizeof(double); }
@@ -77,6 +80,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
   if (!op || !ctx184 || !d_qdata || !opts) return HB_ERROR_INVALID;
   if (opts->gmres_restart < 1 || opts->gmres_restart + 1 > MAXK || opts->dt <= 0 || (opts->bdf_order != 1 && opts->bdf_order != 2))
     return HB_ERROR_INVALID;
+  if (opts->jfnk && opts->jacobian_fp32) return HB_ERROR_INVALID; /* the difference quotient needs FP64 Krylov vectors */
   HbTimeStepper *ts = (HbTimeStepper *)calloc(1, sizeof *ts);
   if (!ts) return HB_ERROR_NOMEM;
   ts->op = op;
@@ -98,6 +102,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
   err |= cudaMalloc(&ts->zvec, ksz(ts) * (size_t)ts->n) | cudaMalloc(&ts->diag, ksz(ts) * (size_t)ts->n);
   if (ts->o.jacobian_fp32) err |= cudaMalloc(&ts->jd32, sizeof(float) * njd) | cudaMalloc((void **)&ts->res32, sizeof(float) * (size_t)ts->n);
   else err |= cudaMalloc((void **)&ts->jd64, sizeof(double) * njd);
+  if (ts->o.jfnk) err |= cudaMalloc((void **)&ts->qp, nb) | cudaMalloc((void **)&ts->qdp, nb) | cudaMalloc((void **)&ts->rp, nb);
   if (err) {
     hb_ts_destroy(ts);
     return HB_ERROR_NOMEM;
@@ -109,7 +114,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
 int hb_ts_destroy(HbTimeStepper *ts) {
   if (!ts) return HB_SUCCESS;
   void *p[] = {ts->q, ts->q_prev, ts->q_prev2, ts->z, ts->qdot, ts->res, ts->delta, ts->d_partial, ts->d_dots, ts->scratch,
-               ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64};
+               ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64, ts->qp, ts->qdp, ts->rp};
   for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
     if (p[i]) cudaFree(p[i]);
   free(ts->sgs_w);
@@ -164,7 +169,33 @@ static int kv_copy(HbTimeStepper *ts, void *dst, const void *src) {
   return cudaMemcpyAsync(dst, src, ksz(ts) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s) == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 /* y = J x (the IJacobian operator at the current linearisation point) */
+/* residual F(q, q_dot) of the current model (with the closure when attached and not lagged), without Jacobian data */
+static int residual(HbTimeStepper *ts, const double *q, const double *qdot, double *out, double *jd64, float *jd32) {
+  HbIFunctionIO io = {q, qdot, ts->qdata, jd64, jd32, out, 0};
+  if (ts->sgs_w && !(ts->o.sgs_lagged && !ts->o.jfnk)) return hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io, &ts->sgs_desc, ts->sgs_w, ts->s);
+  return hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s);
+}
+
+/* y = J x by a forward difference of the full residual (PETSc's -snes_mf_operator form): the state moves by eps x and its
+ * rate by shift * eps x; eps = sqrt(DBL_EPSILON) (1 + |q|) / |x|.  ts->res holds F at the current Newton iterate. */
+static int jac_fd(HbTimeStepper *ts, const double *x, double *y) {
+  double xx, qq;
+  HBCK(hb_vec_reduce_f64(x, NULL, ts->n, 1, ts->scratch, &xx, ts->s));
+  if (xx == 0) return hb_vec_set_f64(y, ts->n, 0.0, ts->s);
+  HBCK(hb_vec_reduce_f64(ts->q, NULL, ts->n, 1, ts->scratch, &qq, ts->s));
+  const double eps = 1.4901161193847656e-08 * (1 + sqrt(qq)) / sqrt(xx);
+  CUCK(cudaMemcpyAsync(ts->qp, ts->q, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s));
+  CUCK(cudaMemcpyAsync(ts->qdp, ts->qdot, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s));
+  HBCK(hb_vec_axpy_f64(ts->qp, eps, x, ts->n, ts->s));
+  HBCK(hb_vec_axpy_f64(ts->qdp, ts->ctx.ijacobian_time_shift * eps, x, ts->n, ts->s));
+  HBCK(residual(ts, ts->qp, ts->qdp, ts->rp, NULL, NULL));
+  CUCK(cudaMemcpyAsync(y, ts->rp, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s));
+  HBCK(hb_vec_axpby_f64(y, -1.0 / eps, 1.0 / eps, ts->res, ts->n, ts->s)); /* y = (F(q + eps x) - F(q)) / eps */
+  return HB_SUCCESS;
+}
+
 static int kv_jac(HbTimeStepper *ts, const void *x, void *y) {
+  if (ts->o.jfnk) return jac_fd(ts, (const double *)x, (double *)y);
   if (ts->o.jacobian_fp32) return hb_ijacobian_apply_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (const float *)x, (float *)y, 0, ts->s);
   return hb_ijacobian_apply_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, (const double *)x, (double *)y, 0, ts->s);
 }
@@ -328,7 +359,7 @@ int hb_ts_step(HbTimeStepper *ts, HbStepStats *st) {
   ts->ctx.dt                   = dt;
   ts->ctx.ijacobian_time_shift = alpha;
   ts->ctx.time                 = ts->t + dt;
-  const int sgs_lag = ts->sgs_w && ts->o.sgs_lagged;
+  const int sgs_lag = ts->sgs_w && ts->o.sgs_lagged && !ts->o.jfnk;
   if (sgs_lag) { /* closure contribution at the previous state: F_sgs(q_n) - F(q_n), independent of q_dot */
     HBCK(hb_vec_set_f64(ts->qdot, ts->n, 0.0, ts->s)); /* any finite q_dot; it cancels in the difference */
     HbIFunctionIO io_a = {ts->q, ts->qdot, ts->qdata, NULL, NULL, ts->sgs_res, 0};
@@ -342,8 +373,7 @@ int hb_ts_step(HbTimeStepper *ts, HbStepStats *st) {
   for (; it <= ts->o.newton_max_it; it++) {
     HBCK(hb_bdf_qdot(ts->q, ts->z, alpha, ts->qdot, ts->n, ts->s));
     HbIFunctionIO io = {ts->q, ts->qdot, ts->qdata, ts->o.jacobian_fp32 ? NULL : ts->jd64, ts->o.jacobian_fp32 ? (float *)ts->jd32 : NULL, ts->res, 0};
-    if (ts->sgs_w && !sgs_lag) HBCK(hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io, &ts->sgs_desc, ts->sgs_w, ts->s));
-    else HBCK(hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s));
+    HBCK(residual(ts, io.q, io.q_dot, io.v, io.jac_data, io.jac_data_f32));
     if (sgs_lag) HBCK(hb_vec_axpy_f64(ts->res, 1.0, ts->sgs_res, ts->n, ts->s));
     double r2;
     HBCK(hb_vec_reduce_f64(ts->res, NULL, ts->n, 1, ts->scratch, &r2, ts->s));

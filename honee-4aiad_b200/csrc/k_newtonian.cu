@@ -477,12 +477,14 @@ struct SgsArg<1> {
   float w[sgs::MlpShape<20, 0>::size];
   float alpha;
   float b[6][2];
+  int clamp, no_backscatter;
 };
 template <>
 struct SgsArg<2> {
   float w[sgs::MlpShape<20, 20>::size];
   float alpha;
   float b[6][2];
+  int clamp, no_backscatter;
 };
 
 template <int SGS>
@@ -507,8 +509,21 @@ __device__ __forceinline__ void sgs_add(const PhysConst<double> &c, const double
   sgs::mlp_forward<20, SGS == 2 ? 20 : 0>(sg.w, sg.alpha, xf, yf);
   double y[6], km[6], F[5][3];
 #pragma unroll
-  for (int k = 0; k < 6; k++) y[k] = (double)yf[k];
+  for (int k = 0; k < 6; k++) y[k] = sg.clamp ? fmin(fmax((double)yf[k], 0.0), 1.0) : (double)yf[k];
   sgs::outputs_to_stress(y, delta, E, sg.b, gmag, km);
+  if (sg.no_backscatter) {  // tau : S > 0 feeds energy to the resolved scales: keep only the isotropic part there
+    double tau[3][3], ts = 0;
+    sgs::km_unpack(km, tau);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) ts += tau[i][j] * 0.5 * (G[i][j] + G[j][i]);
+    if (ts > 0) {
+      const double iso = (km[0] + km[1] + km[2]) / 3;
+      km[0] = km[1] = km[2] = iso;
+      km[3] = km[4] = km[5] = 0;
+    }
+  }
   sgs::flux(st.u, km, F);
 #pragma unroll
   for (int d = 0; d < 3; d++)
@@ -1178,6 +1193,8 @@ static int fill_sgs(const HbMlpDesc *d, const float *w, SgsArg<SGS> &sg) {
   memcpy(sg.w, w, sizeof sg.w);
   sg.alpha = d->leaky_alpha;
   memcpy(sg.b, d->out_bounds, sizeof sg.b);
+  sg.clamp = d->clamp_outputs;
+  sg.no_backscatter = d->no_backscatter;
   return HB_SUCCESS;
 }
 

@@ -10,7 +10,7 @@
      network (6-20-20-6, ReLU, Xavier init from a seed) trained with Adam on the GPU by this package's kernels
   4. two coarse runs on `coarse_faces`^3 elements from the filtered initial state (the coarse nodes are a subset of the
      fine ones for these nested meshes, so the filtered fine field is injected): without the closure, and with the
-     trained network in the residual (evaluated once per step at the previous state, hb_ts_set_sgs)
+     trained network in the residual (hb_ts_set_sgs), implicit with matrix-free Krylov products by default
   5. both compared with the filtered fine solution through the kinetic-energy monitor (total KE and the resolved strain
      dissipation), with the GPU time of each run
 
@@ -70,10 +70,10 @@ class TGMesh:
         return {"TotalKineticEnergy": float(s[0]), "StrainDissipation": float(s[1]), "MuVorticity2": float(s[4])}
 
 
-def run_steps(m: TGMesh, dt, n_steps, every, mixed=True, sgs=None, on_snapshot=None, q0=None):
+def run_steps(m: TGMesh, dt, n_steps, every, mixed=True, sgs=None, on_snapshot=None, q0=None, **opts):
     """BDF2 steps from q0 (default: the Taylor-Green initial condition); calls on_snapshot(k, q) every `every` steps
     (and at step 0).  Returns the monitor rows and the summed step time (CUDA events inside hb_ts_step)."""
-    ts = S.TimeStepper(m.op, m.cb, m.qdata, dt=dt, bdf_order=2, jacobian_fp32=int(mixed))
+    ts = S.TimeStepper(m.op, m.cb, m.qdata, dt=dt, bdf_order=2, jacobian_fp32=int(mixed), **opts)
     if sgs is not None:
         ts.set_sgs(*sgs)
     q = m.initial_state() if q0 is None else q0.clone()
@@ -103,7 +103,15 @@ def _max_rel_err(rows, ref, key, scale, from_start=False):
 
 
 def study(fine_faces=96, coarse_faces=24, degree=2, t_end=2.0, snaps=4, cfl=1.0, train_steps=4000, batch=65536, lr=1e-3, seed=0,
-          clip=1e-3, log=None):
+          clip=1e-3, implicit_closure=False, coarse_substeps=1, cache=None, clamp_outputs=False, no_backscatter=True, log=None):
+    """implicit_closure: the closure inside Newton with matrix-free Krylov products (FP64); by default it is evaluated once
+    per step at the previous state (explicit, mixed-precision Krylov).  coarse_substeps divides the coarse step of both
+    coarse runs.  cache: a directory where the fine-run products (filtered monitors, injected initial state, trained
+    model) are stored after stages 1-3 and reused by later calls with the same fine configuration.  clamp_outputs and
+    no_backscatter select the inference limiters of the fused closure (HbMlpDesc; both off = the reference's evaluation).
+    Backscatter limiting is on by default: without it the trained closure fed energy into the resolved scales of the 24^3
+    Taylor-Green run and the run diverged near t = 1.5 at every time step tried."""
+    import os
     import torch
 
     def say(**kw):
@@ -121,6 +129,45 @@ def study(fine_faces=96, coarse_faces=24, degree=2, t_end=2.0, snaps=4, cfl=1.0,
     out = {"fine_faces": fine_faces, "coarse_faces": coarse_faces, "degree": degree, "dt_fine": dt_f, "dt_coarse": dt_c, "steps_fine": n_f,
            "steps_coarse": n_c, "t_end": n_c * dt_c, "snapshots": snaps}
 
+    key = f"tg_f{fine_faces}_c{coarse_faces}_d{degree}_t{t_end}_s{snaps}_cfl{cfl}_n{train_steps}_b{batch}_seed{seed}"
+    cpath = os.path.join(cache, key + ".npz") if cache else None
+    if cpath and os.path.exists(cpath):
+        z = np.load(cpath, allow_pickle=False)
+        saved = json.loads(str(z["meta"]))
+        out.update(saved)
+        ref_rows, weights, bounds = saved["filtered_fine"], z["weights"], z["bounds"]
+        q_inject = [torch.from_numpy(z["q_inject"]).to(coarse.dev)]
+        sec_f = saved["fine"]["gpu_seconds"]
+        say(stage="loaded fine run and model", path=cpath)
+    else:
+        ref_rows, weights, bounds, q_inject, sec_f, d = _fine_and_train(out, coarse, fine_faces, degree, ratio, dt_f, n_f, every_f, clip, seed, batch,
+                                                                      lr, train_steps, say)
+        if cpath:
+            os.makedirs(cache, exist_ok=True)
+            meta = {k: out[k] for k in ("fine", "filtered_fine", "filter_seconds", "training", "dofs_fine", "dofs_coarse")}
+            np.savez(cpath, meta=json.dumps(meta), weights=weights, bounds=bounds, q_inject=q_inject[0].cpu().numpy())
+    out["weights"] = np.asarray(weights).tolist()
+
+    d = SG.desc(20, 20, 0.0, bounds, clamp_outputs=clamp_outputs, no_backscatter=no_backscatter)
+    out["limiters"] = {"clamp_outputs": bool(clamp_outputs), "no_backscatter": bool(no_backscatter)}
+
+    # 4. coarse runs without and with the closure (same step, from the same filtered initial state)
+    dt_cs, n_cs, every_cs = dt_c / coarse_substeps, n_c * coarse_substeps, every_c * coarse_substeps
+    out["coarse_dt"], out["coarse_steps"] = dt_cs, n_cs
+    rows_c0, sec_c0 = run_steps(coarse, dt_cs, n_cs, every_cs, mixed=True, q0=q_inject[0])
+    try:
+        rows_c1, sec_c1 = run_steps(coarse, dt_cs, n_cs, every_cs, mixed=not implicit_closure, sgs=(d, np.asarray(weights, dtype=np.float32)),
+                                    q0=q_inject[0], jfnk=int(implicit_closure))
+        diverged = None
+    except RuntimeError as e:
+        rows_c1, sec_c1, diverged = [], float("nan"), str(e)
+    out["coarse_plain"] = {"gpu_seconds": sec_c0, "rows": rows_c0}
+    out["coarse_closure"] = {"gpu_seconds": sec_c1, "rows": rows_c1, "diverged": diverged, "implicit": bool(implicit_closure)}
+    return _compare(out, ref_rows, rows_c0, rows_c1, sec_f, sec_c1)
+
+
+def _fine_and_train(out, coarse, fine_faces, degree, ratio, dt_f, n_f, every_f, clip, seed, batch, lr, train_steps, say):
+    import torch
     # 1-2. fine run, filtered snapshots, training pairs
     fine = TGMesh(fine_faces, degree)
     out["dofs_fine"], out["dofs_coarse"] = fine.mesh.l_size, coarse.mesh.l_size
@@ -179,21 +226,13 @@ def study(fine_faces=96, coarse_faces=24, degree=2, t_end=2.0, snaps=4, cfl=1.0,
                        "loss": hist, "bounds": bounds.tolist()}
     say(stage="trained", **{k: v for k, v in out["training"].items() if k != "bounds"})
     weights = tr.params()
-    out["weights"] = weights.tolist()
     del X, Y, tr
     torch.cuda.empty_cache()
+    return ref_rows, weights, bounds, q_inject, sec_f, d
 
-    # 4. coarse runs without and with the closure
-    rows_c0, sec_c0 = run_steps(coarse, dt_c, n_c, every_c, mixed=True, q0=q_inject[0])
-    try:
-        rows_c1, sec_c1 = run_steps(coarse, dt_c, n_c, every_c, mixed=True, sgs=(d, weights), q0=q_inject[0])
-        diverged = None
-    except RuntimeError as e:
-        rows_c1, sec_c1, diverged = [], float("nan"), str(e)
-    out["coarse_plain"] = {"gpu_seconds": sec_c0, "rows": rows_c0}
-    out["coarse_closure"] = {"gpu_seconds": sec_c1, "rows": rows_c1, "diverged": diverged}
 
-    # 5. errors against the filtered fine solution at the snapshot times
+def _compare(out, ref_rows, rows_c0, rows_c1, sec_f, sec_c1):
+    """errors of both coarse runs against the filtered fine solution at the snapshot times"""
     ke0 = ref_rows[0]["TotalKineticEnergy"]
     eps_scale = max(abs(r["StrainDissipation"]) for r in ref_rows)
     res = {}
@@ -221,9 +260,16 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--coarse-substeps", type=int, default=1, help="divide the coarse time step of both coarse runs")
+    ap.add_argument("--implicit-closure", action="store_true", help="closure inside Newton with matrix-free Krylov products")
+    ap.add_argument("--cache", default=None, help="directory to keep / reuse the fine run and the trained model")
+    ap.add_argument("--clamp-outputs", action="store_true", help="limit the network outputs to the training range")
+    ap.add_argument("--backscatter", action="store_true", help="keep the model's stress where tau : S > 0 (the reference's evaluation)")
     ap.add_argument("--out", default=None, help="write the full result (monitor rows, loss history, weights) as JSON here")
     a = ap.parse_args(argv)
-    res = study(a.fine_faces, a.coarse_faces, a.degree, a.t_end, a.snaps, a.cfl, a.train_steps, a.batch, a.lr, a.seed, log=sys.stderr)
+    res = study(a.fine_faces, a.coarse_faces, a.degree, a.t_end, a.snaps, a.cfl, a.train_steps, a.batch, a.lr, a.seed,
+                implicit_closure=a.implicit_closure, coarse_substeps=a.coarse_substeps, cache=a.cache, clamp_outputs=a.clamp_outputs,
+                no_backscatter=not a.backscatter, log=sys.stderr)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(res, f)

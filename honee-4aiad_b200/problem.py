@@ -342,3 +342,54 @@ def taylor_green_context(degree: int, *, L=2 * math.pi, Re=1600., Ma=0.1, rho0=1
     ctx.newt_ctx = newtonian_context(degree, cv=cv, cp=cp, mu=mu, k=k, stab=stab, Ctau_v=60, Ctau_C=0.5, Ctau_M=0.5, Ctau_E=0.5)
     ctx.lx = ctx.ly = ctx.lz = L
     return ctx
+
+
+# --------------------------------------------------------------------------------------------------------------------
+# boundary faces of a box mesh and the free-stream context
+
+_FACE_AXES = {  # side -> (normal axis, at upper end, tangent axis X0, tangent axis X1) with cross(X0, X1) outward
+    "x-": (0, False, 2, 1), "x+": (0, True, 1, 2),
+    "y-": (1, False, 0, 2), "y+": (1, True, 2, 0),
+    "z-": (2, False, 1, 0), "z+": (2, True, 0, 1),
+}
+
+
+def box_faces(mesh: BoxMesh, basis: TensorBasis, sides=None):
+    """Boundary faces of the non-periodic sides: offsets [F][P^2] (node * 5, face-tensor order, X0 fastest), node
+    coordinates [F][3][P^2] and the side name of each face.  The face parameterisation makes the normal of
+    cross(dx/dX0, dx/dX1) point out of the box."""
+    if sides is None:
+        sides = [s for s, (ax, _, _, _) in _FACE_AXES.items() if not mesh.periodic[ax]]
+    P, n, N = mesh.P, mesh.n, mesh.node_dims
+    X = node_coordinates(mesh, basis)
+    offs, xs, names = [], [], []
+    a = np.arange(P)
+    for side in sides:
+        ax, upper, t0, t1 = _FACE_AXES[side]
+        if mesh.periodic[ax]:
+            raise ValueError(f"side {side} is periodic")
+        e_ax = n[ax] - 1 if upper else 0
+        l_ax = P - 1 if upper else 0
+        for e1 in range(n[t1]):
+            for e0 in range(n[t0]):
+                idx = [None, None, None]
+                idx[ax] = np.full((P, P), e_ax * (P - 1) + l_ax)
+                idx[t0] = (e0 * (P - 1) + a)[None, :] * np.ones((P, 1), dtype=int)   # [b][a], a along X0 (fastest)
+                idx[t1] = (e1 * (P - 1) + a)[:, None] * np.ones((1, P), dtype=int)
+                idx = [(np.asarray(v) % N[d]).reshape(-1) for d, v in enumerate(idx)]
+                node = idx[0] + N[0] * (idx[1] + N[1] * idx[2])
+                offs.append(node * 5)
+                xs.append(X[:, node])
+                names.append(side)
+    return np.ascontiguousarray(np.array(offs, dtype=np.int32)), np.ascontiguousarray(np.array(xs)), names
+
+
+def freestream_context(newt: NewtonianContext, P, u, T) -> bytes:
+    """FreestreamContext_ bytes (bc_freestream_type.h): the Newtonian context and the exterior State (U, Y)."""
+    gas = newt.gas
+    R = gas.cp - gas.cv
+    rho = P / (R * T)
+    u = np.asarray(u, dtype=np.float64)
+    U = np.array([rho, rho * u[0], rho * u[1], rho * u[2], rho * (gas.cv * T + 0.5 * u @ u)])
+    Y = np.array([P, u[0], u[1], u[2], T])
+    return bytes(memoryview(newt)) + U.tobytes() + Y.tobytes()

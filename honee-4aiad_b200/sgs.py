@@ -20,11 +20,13 @@ from .kernels import _addr, _chk, _stream
 
 
 class HbMlpDesc(C.Structure):
-    _fields_ = [("hidden1", C.c_int), ("hidden2", C.c_int), ("leaky_alpha", C.c_float), ("out_bounds", C.c_float * 12)]
+    _fields_ = [("hidden1", C.c_int), ("hidden2", C.c_int), ("leaky_alpha", C.c_float), ("out_bounds", C.c_float * 12),
+                ("clamp_outputs", C.c_int), ("no_backscatter", C.c_int)]
 
 
-def desc(hidden1=20, hidden2=20, alpha=0.0, bounds=None) -> HbMlpDesc:
+def desc(hidden1=20, hidden2=20, alpha=0.0, bounds=None, clamp_outputs=False, no_backscatter=False) -> HbMlpDesc:
     d = HbMlpDesc(hidden1, hidden2, alpha)
+    d.clamp_outputs, d.no_backscatter = int(clamp_outputs), int(no_backscatter)
     b = np.zeros(12) if bounds is None else np.asarray(bounds, dtype=np.float64).reshape(12)
     for i in range(12):
         d.out_bounds[i] = float(b[i])

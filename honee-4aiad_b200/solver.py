@@ -20,7 +20,7 @@ class HbSolverOptions(C.Structure):
     _fields_ = [("dt", C.c_double), ("bdf_order", C.c_int), ("newton_rtol", C.c_double), ("newton_atol", C.c_double),
                 ("newton_max_it", C.c_int), ("ksp_rtol", C.c_double), ("ksp_max_it", C.c_int), ("gmres_restart", C.c_int),
                 ("pc_jacobi", C.c_int), ("pc_every_newton", C.c_int), ("jacobian_fp32", C.c_int), ("cgs_refine", C.c_int),
-                ("sgs_lagged", C.c_int)]
+                ("sgs_lagged", C.c_int), ("jfnk", C.c_int)]
 
 
 class HbStepStats(C.Structure):

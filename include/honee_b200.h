@@ -150,6 +150,8 @@ typedef struct {
   int    cgs_refine;      /* 0: classical Gram-Schmidt once (PETSc default), 1: a second pass every iteration (CGS2) */
   int    sgs_lagged;      /* with a closure attached: 1 (default) evaluate it at the previous state, explicitly, so Newton
                              converges with the Newtonian Jacobian; 0 implicit (the Jacobian then omits its derivative) */
+  int    jfnk;            /* 1: Krylov products by a forward difference of the full residual (closure included, implicit);
+                             FP64 only; the Jacobi preconditioner stays the Newtonian diagonal */
 } HbSolverOptions;
 
 typedef struct {
@@ -199,6 +201,9 @@ typedef struct {
   int   hidden1, hidden2;   /* hidden widths: 20, 20 (two layers) or 20, 0 (one layer, the reference's 6-20-6 form) */
   float leaky_alpha;        /* negative slope of the activation; 0 = ReLU (the reference default) */
   float out_bounds[6][2];   /* min-max bounds {lo, hi} that de-normalise the 6 outputs (OutScaling.dat) */
+  int   clamp_outputs;      /* inference in the residual: 1 limits the normalised outputs to [0, 1] (the training range) */
+  int   no_backscatter;     /* inference in the residual: 1 drops the deviatoric stress where it would feed energy to the
+                               resolved scales (tau : S > 0); both 0 = the reference's evaluation */
 } HbMlpDesc;
 
 /* Parameter count of the network (W1, b1, [W2, b2,] W3, b3; W row-major [out][in]); negative: unsupported shape. */
@@ -258,6 +263,41 @@ HB_EXPORT int hb_filtered_state(const double *filtered, int64_t nodes, const voi
  * the stress taken into the model frame); width_scale = filter width / this mesh's element width. */
 HB_EXPORT int hb_sgs_training_pairs(const HbElemOp *op, const void *ctx184, const double *qdata, const double *filtered, double width_scale, float *X,
                                     float *Y, void *s);
+
+/* ---- Free-stream boundary condition (qfunctions/bc_freestream.h, riemann_solver.h; problems/bc_freestream.c): the
+ *      face sub-operators of the composite IFunction / IJacobian on the boundary faces of the mesh ---- */
+typedef struct HbFaceOp {
+  int      num_faces, P, Q;
+  int64_t  l_size;
+  int32_t *d_offsets;      /* device [num_faces][P^2], node * 5 of the volume L-vector, face-tensor order */
+  int      num_colors;
+  int32_t *h_color_ptr;    /* host [num_colors + 1] */
+  int32_t *d_color_elem;   /* device face ids grouped by colour */
+  double   interp1d[HB_MAX_P * HB_MAX_P], grad1d[HB_MAX_P * HB_MAX_P], qweight1d[HB_MAX_P];
+  int      device;
+} HbFaceOp;
+
+/* FreestreamContext_ (qfunctions/bc_freestream_type.h): the Newtonian context and the exterior State (U then Y). */
+typedef struct {
+  HbNewtonianContext newt;
+  double             S_infty_U[5]; /* rho, rho u (3), E */
+  double             S_infty_Y[5]; /* P, u (3), T */
+} HbFreestreamContext;
+
+HB_EXPORT int hb_faceop_create(int num_faces, int P, int Q, const int32_t *offsets, int64_t l_size, const double *interp1d, const double *grad1d,
+                               const double *qweight1d, HbFaceOp **op);
+HB_EXPORT int hb_faceop_destroy(HbFaceOp *op);
+/* Face geometric factors (SetupBoundary, setupgeo.h:100-117) [F][10][Q^2] from the face nodes' coordinates x_nodes
+ * [F][3][P^2] (device): w detJb, unit normal, dX/dx (2 x 3).  The normal is the cross product of the two face tangents
+ * in face-tensor order; the face node order decides its orientation (outward for the box faces of problem.py). */
+HB_EXPORT int hb_face_setup_qdata(const HbFaceOp *op, const double *x_nodes, double *qdata_sur, void *s);
+/* v += int phi wdetJb F(q, S_infty, n), F = HLL (flux_type 0) or HLLC (1); jac_data_sur [F][5][Q^2] (may be NULL) = q at
+ * the points (Freestream, bc_freestream.h:14-48). */
+HB_EXPORT int hb_freestream_apply(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *q, double *jac_data_sur,
+                                  double *v, void *s);
+/* v += int phi wdetJb dF(q; dq) with the exterior state fixed (Freestream_Jacobian, bc_freestream.h:75-114). */
+HB_EXPORT int hb_freestream_jacobian_apply(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
+                                           const double *dq, double *v, void *s);
 
 /* Library identification */
 const char *hb_version(void);

@@ -8,6 +8,7 @@
  */
 #include <ceed/types.h>
 
+#include "bc_freestream.h"
 #include "differential_filter.h"
 #include "grid_anisotropy_tensor.h"
 #include "monitor_totalkineticenergy.h"
@@ -93,3 +94,11 @@ EXPORT void ref_diff_filter_ctx_layout(size_t out[4]) {
   out[2] = offsetof(struct DifferentialFilterContext_, kernel_scaling);
   out[3] = offsetof(struct DifferentialFilterContext_, damping_function);
 }
+
+/* Free-stream boundary condition (bc_freestream.h) and face geometric factors (setupgeo.h:SetupBoundary). */
+EXPORT int ref_Freestream_Conserv_HLL(void *c, CeedInt Q, In in, Out out) { return Freestream_Conserv_HLL(c, Q, in, out); }
+EXPORT int ref_Freestream_Conserv_HLLC(void *c, CeedInt Q, In in, Out out) { return Freestream_Conserv_HLLC(c, Q, in, out); }
+EXPORT int ref_Freestream_Jacobian_Conserv_HLL(void *c, CeedInt Q, In in, Out out) { return Freestream_Jacobian_Conserv_HLL(c, Q, in, out); }
+EXPORT int ref_Freestream_Jacobian_Conserv_HLLC(void *c, CeedInt Q, In in, Out out) { return Freestream_Jacobian_Conserv_HLLC(c, Q, in, out); }
+EXPORT int ref_SetupBoundary(void *c, CeedInt Q, In in, Out out) { return SetupBoundary(c, Q, in, out); }
+EXPORT int ref_freestream_ctx_size(void) { return (int)sizeof(struct FreestreamContext_); }

@@ -1,0 +1,82 @@
+"""CPU checks of the free-stream boundary oracle (oracle/face_oracle.py) against the reference's own QFunctions: the
+golden fixture tests/golden/face_points.npz (made by make_face_golden.py from oracle/_ref) covering every HLL / HLLC
+branch, the face geometric factors, and finite differences of the restated flux."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import face_oracle as FO  # noqa: E402
+
+G = np.load(os.path.join(ROOT, "tests", "golden", "face_points.npz"))
+U_INF = None
+
+
+def _ext():
+    cv, cp = float(G["cv"]), float(G["cp"])
+    u = G["u_inf"]
+    rho = float(G["P_inf"]) / ((cp - cv) * float(G["T_inf"]))
+    U = np.array([rho, rho * u[0], rho * u[1], rho * u[2], rho * (cv * float(G["T_inf"]) + 0.5 * u @ u)])
+    Y = np.array([float(G["P_inf"]), u[0], u[1], u[2], float(G["T_inf"])])
+    return U, Y, cv, cp
+
+
+@pytest.mark.parametrize("name", ["HLL", "HLLC"])
+def test_flux_and_jacobian_match_reference(name):
+    U, Y, cv, cp = _ext()
+    q, qd = G["q"], G["qdata"]
+    n = q.shape[1]
+    s = FO.state_from_U(q, cv, cp)
+    F = FO.riemann(s, FO.exterior(U, Y, n), qd[1:4], cv, cp, hllc=name == "HLLC")
+    np.testing.assert_allclose(qd[0] * F, G[f"v_{name}"], rtol=1e-11, atol=1e-9)
+    np.testing.assert_array_equal(G[f"jac_{name}"], q)
+    ds = FO.state_from_U_fwd(s, G[f"dq_{name}"], cv, cp)
+    zero = FO.St(np.zeros(n), np.zeros((3, n)), np.zeros(n), np.zeros(n), np.zeros((3, n)), np.zeros(n))
+    dF = FO.riemann(s, FO.exterior(U, Y, n), qd[1:4], cv, cp, hllc=name == "HLLC", dL=ds, dR=zero)
+    np.testing.assert_allclose(qd[0] * dF, G[f"dv_{name}"], rtol=1e-9, atol=1e-7 * np.abs(G[f"dv_{name}"]).max())
+
+
+def test_riemann_branches_all_exercised():
+    U, Y, cv, cp = _ext()
+    q, qd = G["q"], G["qdata"]
+    s = FO.state_from_U(q, cv, cp)
+    R = FO.exterior(U, Y, q.shape[1])
+    uL, uR = (s.u * qd[1:4]).sum(0), (R.u * qd[1:4]).sum(0)
+    sl, sr = FO.speeds(s, uL, R, uR, cv, cp / cv)
+    assert (sl >= 0).any() and (sr <= 0).any() and ((sl < 0) & (sr > 0)).any()
+
+
+@pytest.mark.parametrize("name", ["HLL", "HLLC"])
+def test_flux_tangent_matches_finite_differences(name):
+    U, Y, cv, cp = _ext()
+    q, qd = G["q"], G["qdata"]
+    n = q.shape[1]
+    dq = G[f"dq_{name}"] * 1e-3
+    s = FO.state_from_U(q, cv, cp)
+    zero = FO.St(np.zeros(n), np.zeros((3, n)), np.zeros(n), np.zeros(n), np.zeros((3, n)), np.zeros(n))
+    dF = FO.riemann(s, FO.exterior(U, Y, n), qd[1:4], cv, cp, hllc=name == "HLLC", dL=FO.state_from_U_fwd(s, dq, cv, cp), dR=zero)
+    Fp = FO.riemann(FO.state_from_U(q + dq, cv, cp), FO.exterior(U, Y, n), qd[1:4], cv, cp, hllc=name == "HLLC")
+    Fm = FO.riemann(FO.state_from_U(q - dq, cv, cp), FO.exterior(U, Y, n), qd[1:4], cv, cp, hllc=name == "HLLC")
+    fd = (Fp - Fm) / 2
+    ok = np.abs(fd - dF).max(0) <= 1e-4 * (np.abs(fd).max(0) + 1e-6)
+    assert ok.mean() > 0.95  # points sitting on a branch switch are not differentiable there
+
+
+def test_face_qdata_matches_reference():
+    J, w = G["J"], G["w"]
+    n = w.size
+    # one "face" per point: P = Q = 1 style evaluation via the formula on dx/dX directly
+    J0, J1 = J[0], J[1]
+    N = np.cross(J0.T, J1.T).T
+    detJb = np.linalg.norm(N, axis=0)
+    ref = G["qdata_sur"]
+    np.testing.assert_allclose(ref[0], w * detJb, rtol=1e-13)
+    np.testing.assert_allclose(ref[1:4], N / detJb, rtol=1e-12, atol=1e-14)
+    a, c, b = (J0 * J0).sum(0), (J1 * J1).sum(0), (J0 * J1).sum(0)
+    det = a * c - b * b
+    inv = np.array([[c / det, -b / det], [-b / det, a / det]])
+    dXdx = np.stack([inv[i, 0] * J0 + inv[i, 1] * J1 for i in range(2)])  # [2][3][n]
+    np.testing.assert_allclose(ref[4:], dXdx.reshape(6, n), rtol=1e-10, atol=1e-12)

@@ -185,3 +185,14 @@ def test_cgs_refinement_gives_the_same_step(fp32):
     qb, _, (sb,), _ = _run(op, ctx, qdata, q0, 1, cgs_refine=1, **kw)
     assert sa.converged_reason == 1 and sb.converged_reason == 1
     assert rel_l2(qa - q0, qb - q0) < 1e-6
+
+
+def test_matrix_free_jacobian_newton_reaches_the_same_state():
+    mesh, basis, ctx, q0, op, qdata = _problem(n=(3, 3, 3), dt=1e-4)
+    kw = dict(dt=1e-4, bdf_order=1, newton_rtol=1e-9)
+    qa, _, (sa,), _ = _run(op, ctx, qdata, q0, 1, **kw)
+    qb, _, (sb,), _ = _run(op, ctx, qdata, q0, 1, jfnk=1, **kw)
+    assert sa.converged_reason == 1 and sb.converged_reason == 1, (sa, sb)
+    assert rel_l2(qb - q0, qa - q0) < 1e-6
+    with pytest.raises(K.HbError):
+        S.TimeStepper(op, prob.context_bytes(ctx), qdata, jfnk=1, jacobian_fp32=1)
