@@ -44,6 +44,12 @@ struct HbTimeStepper {
   double   *sgs_res;
   /* matrix-free (finite-difference) Jacobian action: perturbed state, rate and residual */
   double *qp, *qdp, *rp;
+  /* optional free-stream boundary faces: residual and Jacobian sub-operators of the composite */
+  const HbFaceOp *bc;
+  unsigned char   bc_ctx[sizeof(HbFreestreamContext)];
+  int             bc_flux;
+  const double   *bc_qdata;
+  double         *bc_jac;
 };
 
 #define CUCK(x)                                \
@@ -119,6 +125,7 @@ int hb_ts_destroy(HbTimeStepper *ts) {
     if (p[i]) cudaFree(p[i]);
   free(ts->sgs_w);
   if (ts->sgs_res) cudaFree(ts->sgs_res);
+  if (ts->bc_jac) cudaFree(ts->bc_jac);
   free(ts);
   return HB_SUCCESS;
 }
@@ -137,6 +144,21 @@ int hb_ts_get_state(HbTimeStepper *ts, double *d_q, double *t) {
 }
 
 const void *hb_ts_context(HbTimeStepper *ts) { return &ts->ctx; }
+
+int hb_ts_set_freestream(HbTimeStepper *ts, const HbFaceOp *faces, const void *ctx264, int flux_type, const double *qdata_sur) {
+  if (!ts) return HB_ERROR_INVALID;
+  if (ts->bc_jac) cudaFree(ts->bc_jac);
+  ts->bc_jac = NULL;
+  ts->bc     = NULL;
+  if (!faces) return HB_SUCCESS; /* boundary off */
+  if (!ctx264 || !qdata_sur || (flux_type != 0 && flux_type != 1) || faces->l_size != ts->n) return HB_ERROR_INVALID;
+  if (cudaMalloc((void **)&ts->bc_jac, sizeof(double) * 5 * (size_t)faces->num_faces * faces->Q * faces->Q) != cudaSuccess) return HB_ERROR_NOMEM;
+  memcpy(ts->bc_ctx, ctx264, sizeof ts->bc_ctx);
+  ts->bc       = faces;
+  ts->bc_flux  = flux_type;
+  ts->bc_qdata = qdata_sur;
+  return HB_SUCCESS;
+}
 
 int hb_ts_set_sgs(HbTimeStepper *ts, const HbMlpDesc *d, const float *h_weights) {
   if (!ts) return HB_ERROR_INVALID;
@@ -172,8 +194,11 @@ static int kv_copy(HbTimeStepper *ts, void *dst, const void *src) {
 /* residual F(q, q_dot) of the current model (with the closure when attached and not lagged), without Jacobian data */
 static int residual(HbTimeStepper *ts, const double *q, const double *qdot, double *out, double *jd64, float *jd32) {
   HbIFunctionIO io = {q, qdot, ts->qdata, jd64, jd32, out, 0};
-  if (ts->sgs_w && !(ts->o.sgs_lagged && !ts->o.jfnk)) return hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io, &ts->sgs_desc, ts->sgs_w, ts->s);
-  return hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s);
+  if (ts->sgs_w && !(ts->o.sgs_lagged && !ts->o.jfnk)) HBCK(hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io, &ts->sgs_desc, ts->sgs_w, ts->s));
+  else HBCK(hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s));
+  /* boundary faces add their flux; the state at the face points is kept only for the Newton iterate's Jacobian */
+  if (ts->bc) HBCK(hb_freestream_apply(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, q, (jd64 || jd32) ? ts->bc_jac : NULL, out, ts->s));
+  return HB_SUCCESS;
 }
 
 /* y = J x by a forward difference of the full residual (PETSc's -snes_mf_operator form): the state moves by eps x and its
@@ -196,8 +221,14 @@ static int jac_fd(HbTimeStepper *ts, const double *x, double *y) {
 
 static int kv_jac(HbTimeStepper *ts, const void *x, void *y) {
   if (ts->o.jfnk) return jac_fd(ts, (const double *)x, (double *)y);
-  if (ts->o.jacobian_fp32) return hb_ijacobian_apply_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (const float *)x, (float *)y, 0, ts->s);
-  return hb_ijacobian_apply_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, (const double *)x, (double *)y, 0, ts->s);
+  if (ts->o.jacobian_fp32) {
+    HBCK(hb_ijacobian_apply_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (const float *)x, (float *)y, 0, ts->s));
+    if (ts->bc) HBCK(hb_freestream_jacobian_apply_f32(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, (const float *)x, (float *)y, ts->s));
+    return HB_SUCCESS;
+  }
+  HBCK(hb_ijacobian_apply_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, (const double *)x, (double *)y, 0, ts->s));
+  if (ts->bc) HBCK(hb_freestream_jacobian_apply(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, (const double *)x, (double *)y, ts->s));
+  return HB_SUCCESS;
 }
 /* z = M^-1 x (Jacobi) or copy */
 static int kv_pc(HbTimeStepper *ts, const void *x, void *z) {

@@ -113,12 +113,14 @@ __global__ void k_freestream(int P, int Q, const int32_t *__restrict__ offsets, 
 }
 
 // v += wdetJb * dF(q; dq) with the exterior state fixed (Freestream_Jacobian, bc_freestream.h:75-114)
+// T: precision of dq and v (the state math stays FP64); FP32 serves the mixed-precision Krylov solve
+template <typename T>
 __global__ void k_freestream_jac(int P, int Q, const int32_t *__restrict__ offsets, const int32_t *__restrict__ faces, FaceBasis b,
                                  hb::PhysConst<double> pc, Exterior ex, const double *__restrict__ qd, const double *__restrict__ jac,
-                                 const double *__restrict__ dq, double *__restrict__ v) {
+                                 const T *__restrict__ dq, T *__restrict__ v) {
   __shared__ double sN[5][kMaxP2], sF[5][kMaxQ2];
   const int f = faces[blockIdx.x], t = threadIdx.x, P2 = P * P, Q2 = Q * Q;
-  for (int i = t; i < 5 * P2; i += blockDim.x) sN[i % 5][i / 5] = dq[offsets[(int64_t)f * P2 + i / 5] + i % 5];
+  for (int i = t; i < 5 * P2; i += blockDim.x) sN[i % 5][i / 5] = (double)dq[offsets[(int64_t)f * P2 + i / 5] + i % 5];
   __syncthreads();
   if (t < Q2) {
     const int q0 = t % Q, q1 = t / Q;
@@ -146,7 +148,7 @@ __global__ void k_freestream_jac(int P, int Q, const int32_t *__restrict__ offse
     const int p = i / 5, c = i % 5;
     double acc = 0;
     for (int k = 0; k < Q2; k++) acc += b2(b, P, k % Q, k / Q, p % P, p / P) * sF[c][k];
-    v[offsets[(int64_t)f * P2 + p] + c] += acc;
+    v[offsets[(int64_t)f * P2 + p] + c] = (T)((double)v[offsets[(int64_t)f * P2 + p] + c] + acc);
   }
 }
 
@@ -179,6 +181,25 @@ int unpack_ctx(const void *ctx264, hb::PhysConst<double> &pc, Exterior &ex) {
   memcpy(ex.U, c.S_infty_U, sizeof ex.U);
   memcpy(ex.Y, c.S_infty_Y, sizeof ex.Y);
   return HB_SUCCESS;
+}
+
+template <typename T>
+int freestream_jac(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur, const T *dq, T *v,
+                          void *stream) {
+  if (!op || !ctx264 || !qdata_sur || !jac_data_sur || !dq || !v || (flux_type != 0 && flux_type != 1)) return HB_ERROR_INVALID;
+  hb::PhysConst<double> pc;
+  Exterior ex;
+  int err = unpack_ctx(ctx264, pc, ex);
+  if (err) return err;
+  ex.hllc = flux_type == 1;
+  const FaceBasis b = fbasis(op);
+  for (int c = 0; c < op->num_colors; c++) {
+    const int n = op->h_color_ptr[c + 1] - op->h_color_ptr[c];
+    if (n)
+      k_freestream_jac<T><<<n, nthreads(op), 0, (cudaStream_t)stream>>>(op->P, op->Q, op->d_offsets, op->d_color_elem + op->h_color_ptr[c], b, pc,
+                                                                         ex, qdata_sur, jac_data_sur, dq, v);
+  }
+  return rc();
 }
 
 }  // namespace
@@ -256,20 +277,12 @@ int hb_freestream_apply(const HbFaceOp *op, const void *ctx264, int flux_type, c
 
 int hb_freestream_jacobian_apply(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
                                  const double *dq, double *v, void *stream) {
-  if (!op || !ctx264 || !qdata_sur || !jac_data_sur || !dq || !v || (flux_type != 0 && flux_type != 1)) return HB_ERROR_INVALID;
-  hb::PhysConst<double> pc;
-  Exterior ex;
-  int err = unpack_ctx(ctx264, pc, ex);
-  if (err) return err;
-  ex.hllc = flux_type == 1;
-  const FaceBasis b = fbasis(op);
-  for (int c = 0; c < op->num_colors; c++) {
-    const int n = op->h_color_ptr[c + 1] - op->h_color_ptr[c];
-    if (n)
-      k_freestream_jac<<<n, nthreads(op), 0, (cudaStream_t)stream>>>(op->P, op->Q, op->d_offsets, op->d_color_elem + op->h_color_ptr[c], b, pc,
-                                                                      ex, qdata_sur, jac_data_sur, dq, v);
-  }
-  return rc();
+  return freestream_jac<double>(op, ctx264, flux_type, qdata_sur, jac_data_sur, dq, v, stream);
+}
+
+int hb_freestream_jacobian_apply_f32(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
+                                     const float *dq, float *v, void *stream) {
+  return freestream_jac<float>(op, ctx264, flux_type, qdata_sur, jac_data_sur, dq, v, stream);
 }
 
 }  // extern "C"

@@ -112,3 +112,48 @@ class ElemOp:
         cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
         fn = _load().hb_diagonal_assemble_f32 if fp32 else _load().hb_diagonal_assemble_f64
         _chk(fn(self.ptr, cb, _addr(qdata), _addr(jac_data), _addr(diag), int(add), _stream(stream)), "hb_diagonal_assemble")
+
+
+class HbFaceOp(C.Structure):
+    _fields_ = [("num_faces", C.c_int), ("P", C.c_int), ("Q", C.c_int), ("l_size", C.c_int64), ("d_offsets", C.c_void_p), ("num_colors", C.c_int),
+                ("h_color_ptr", C.POINTER(C.c_int32)), ("d_color_elem", C.c_void_p), ("interp1d", C.c_double * 64), ("grad1d", C.c_double * 64),
+                ("qweight1d", C.c_double * 8), ("device", C.c_int)]
+
+
+class FaceOp:
+    """Boundary faces of a volume mesh (problem.box_faces) with the free-stream boundary condition."""
+
+    HLL, HLLC = 0, 1
+
+    def __init__(self, offsets, l_size, basis, x_nodes):
+        import torch
+        L = _load()
+        self.ptr = C.POINTER(HbFaceOp)()
+        off = np.ascontiguousarray(offsets, dtype=np.int32)
+        self.num_faces, self.P2 = off.shape
+        _chk(L.hb_faceop_create(self.num_faces, basis.P, basis.Q, off.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int64(l_size), _dp(basis.interp1d),
+                                _dp(basis.grad1d), _dp(basis.qweight1d), C.byref(self.ptr)), "hb_faceop_create")
+        self.Q = basis.Q
+        dev = torch.device("cuda:0")
+        xn = torch.from_numpy(np.ascontiguousarray(x_nodes, dtype=np.float64)).to(dev)
+        self.qdata = torch.empty(self.num_faces * 10 * self.Q ** 2, dtype=torch.float64, device=dev)
+        _chk(L.hb_face_setup_qdata(self.ptr, _addr(xn), _addr(self.qdata), None), "hb_face_setup_qdata")
+        self.jac = torch.empty(self.num_faces * 5 * self.Q ** 2, dtype=torch.float64, device=dev)
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                _load().hb_faceop_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    def freestream(self, ctx264: bytes, q, v, flux_type=1, stream=None):
+        cb = C.create_string_buffer(bytes(ctx264), len(ctx264))
+        _chk(_load().hb_freestream_apply(self.ptr, cb, C.c_int(flux_type), _addr(self.qdata), _addr(q), _addr(self.jac), _addr(v), _stream(stream)),
+             "hb_freestream_apply")
+
+    def freestream_jacobian(self, ctx264: bytes, dq, v, flux_type=1, stream=None):
+        cb = C.create_string_buffer(bytes(ctx264), len(ctx264))
+        _chk(_load().hb_freestream_jacobian_apply(self.ptr, cb, C.c_int(flux_type), _addr(self.qdata), _addr(self.jac), _addr(dq), _addr(v),
+                                                  _stream(stream)), "hb_freestream_jacobian_apply")

@@ -73,6 +73,14 @@ class TimeStepper:
         _chk(_load().hb_ts_step(self.ptr, C.byref(s)), "hb_ts_step")
         return StepStats(s.newton_its, s.ksp_its, s.converged_reason, s.res0, s.res_final, s.seconds)
 
+    def set_freestream(self, faceop=None, ctx264: bytes = b"", flux_type=1):
+        """Add the free-stream boundary (kernels.FaceOp, FreestreamContext bytes, 0 HLL / 1 HLLC), or remove it."""
+        if faceop is None:
+            _chk(_load().hb_ts_set_freestream(self.ptr, None, None, 0, None), "hb_ts_set_freestream")
+            return
+        self._bc = (faceop, C.create_string_buffer(bytes(ctx264), len(ctx264)))
+        _chk(_load().hb_ts_set_freestream(self.ptr, faceop.ptr, self._bc[1], C.c_int(flux_type), _addr(faceop.qdata)), "hb_ts_set_freestream")
+
     def set_sgs(self, desc=None, weights=None):
         """Fuse the learned closure (sgs.HbMlpDesc, float32 weights) into the residual, or remove it (no arguments)."""
         if desc is None:

@@ -298,6 +298,13 @@ HB_EXPORT int hb_freestream_apply(const HbFaceOp *op, const void *ctx264, int fl
 /* v += int phi wdetJb dF(q; dq) with the exterior state fixed (Freestream_Jacobian, bc_freestream.h:75-114). */
 HB_EXPORT int hb_freestream_jacobian_apply(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
                                            const double *dq, double *v, void *s);
+/* the same with FP32 dq and v (state and flux math in FP64), for the mixed-precision Krylov solve */
+HB_EXPORT int hb_freestream_jacobian_apply_f32(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur,
+                                               const double *jac_data_sur, const float *dq, float *v, void *s);
+
+/* Attach (faces != NULL) or detach the free-stream boundary to a time stepper: its flux joins every residual and its
+ * tangent every Krylov product (FP32 in mixed precision); the Jacobi diagonal stays the volume one. */
+HB_EXPORT int hb_ts_set_freestream(HbTimeStepper *ts, const HbFaceOp *faces, const void *ctx264, int flux_type, const double *qdata_sur);
 
 /* Library identification */
 const char *hb_version(void);

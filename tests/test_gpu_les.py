@@ -11,7 +11,8 @@ pytestmark = pytest.mark.gpu
 
 def test_learned_closure_beats_the_plain_coarse_run():
     les = importlib.import_module("honee-4aiad_b200.les")
-    r = les.study(fine_faces=24, coarse_faces=6, degree=2, t_end=1.0, snaps=4, train_steps=800, batch=16384, lr=1e-3, seed=0)
+    # the model as the reference evaluates it (no limiter); at this size the coarse run with it stays stable
+    r = les.study(fine_faces=24, coarse_faces=6, degree=2, t_end=1.0, snaps=4, train_steps=800, batch=16384, lr=1e-3, seed=0, no_backscatter=False)
     assert r["coarse_closure"]["diverged"] is None
     e = r["errors_vs_filtered_fine"]
     assert e["closure"]["ke_decay_err"] < 0.5 * e["plain"]["ke_decay_err"], e
