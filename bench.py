@@ -152,6 +152,21 @@ def run_reference(args, rank):
 # ----------------------------------------------------------------------------------------------------------------------
 # GPU arm
 
+def max_over_ranks(ms, world, device):
+    """The job's time for one step: the slowest rank's (replicas run the same work; the job ends with the last one)."""
+    if world > 1:
+        import torch
+        t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return t.item()
+    return ms
+
+
+def job_gdofs(world, dofs_per_rank, ms):
+    """Whole-job throughput of `world` replicas, each doing dofs_per_rank per step, in GDoF/s."""
+    return world * dofs_per_rank / (ms * 1e-3) / 1e9
+
+
 def run_gpu(args, rank, world):
     import torch
     hb = importlib.import_module("honee-4aiad_b200")
@@ -203,12 +218,7 @@ def run_gpu(args, rank, world):
             fn()
         b.record()
         torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / k
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = t.item()
-        return ms
+        return max_over_ranks(a.elapsed_time(b) / k, world, dev)
 
     with ClockSampler(dev.index) as clk:
         ms64 = timed(step64, args.steps)
@@ -261,13 +271,13 @@ def run_gpu(args, rank, world):
     achieved_if = b_if / (ms_if * 1e-3) / 1e9
     launches = 2 * op.num_colors * args.steps
     line = {
-        "metric": METRIC, "value": world * N_L / (ms64 * 1e-3) / 1e9, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": job_gdofs(world, N_L, ms64), "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: background + 8 seeded sinusoidal modes (|k|<=8, 1e-3 relative)",
         "config": {"workload": f"{args.size}^3 hex elements, P=4 Q=5, Newtonian IFunction + IJacobian (SUPG, conservative, FP64)",
                    "dofs": N_L, "elements": E, "qpts": N_q, "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (qdata 2.6 GB, jac_data 3.7 GB per GPU); no flush"},
-        "fp32_mixed": {"value": world * N_L / (ms32 * 1e-3) / 1e9, "unit": "GDoF/s", "ms_per_step": ms32,
+        "fp32_mixed": {"value": job_gdofs(world, N_L, ms32), "unit": "GDoF/s", "ms_per_step": ms32,
                        "jacobian_rel_l2_vs_fp64": err32, "residual": "FP64", "jacobian": "FP32 (FP32 jac_data, FP64 qdata)"},
         "breakdown_ms": {"ifunction": ms_if, "ijacobian": ms_ij, "ifunction_f32_jacdata": ms_if32, "ijacobian_f32": ms_ij32,
                          "diagonal_f64": ms_diag},
@@ -279,7 +289,7 @@ def run_gpu(args, rank, world):
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 4096-element k_ifunction launch "
                                        "(32^3, P=4 Q=5), scaled by the elements of one launch here",
                      "ijacobian": {"achieved": b_ij / (ms_ij * 1e-3) / 1e9, "frac": b_ij / (ms_ij * 1e-3) / 1e9 / pk["hbm_gbs"]}},
-        "e2e": {"value": world * N_L / (ms_e2e * 1e-3) / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": 3 * 8 * N_L, "d2h_bytes_per_step": 2 * 8 * N_L,
+        "e2e": {"value": job_gdofs(world, N_L, ms_e2e), "unit": "GDoF/s", "h2d_bytes_per_step": 3 * 8 * N_L, "d2h_bytes_per_step": 2 * 8 * N_L,
                 "api": "CeedVectorSetArray(HOST, USE_POINTER) + CeedOperatorApply x2 + CeedVectorSyncArray(HOST)", "jacobian_rel_l2_vs_kernel": err_e2e},
         "gpu_launches": launches,
         "clocks": clocks,
