@@ -119,7 +119,7 @@ typedef struct {
   int                 set;
 } OpField;
 
-enum { PLAN_NONE = 0, PLAN_SETUP, PLAN_IFUNCTION, PLAN_IJACOBIAN };
+enum { PLAN_NONE = 0, PLAN_SETUP, PLAN_IFUNCTION, PLAN_IJACOBIAN, PLAN_SETUP_SUR, PLAN_FREESTREAM, PLAN_FREESTREAM_JAC };
 
 struct CeedOperator_private {
   Ceed          ceed;
@@ -136,6 +136,8 @@ struct CeedOperator_private {
   int       idl_coords_set;
   float    *d_tmp_in32, *d_tmp_out32; /* mixed-precision staging of L-vectors */
   double   *d_tmp_e;                  /* coordinate E-vector for the Setup operator */
+  HbFaceOp *fop;                      /* boundary-face sub-operators */
+  int       flux_type;                /* 0 HLL, 1 HLLC */
 };
 
 struct CeedContextFieldLabel_private {
@@ -1235,7 +1237,16 @@ int CeedOperatorSetField(CeedOperator op, const char *field_name, CeedElemRestri
   f->b   = basis;
   f->v   = vec;
   f->set = 1;
-  op->plan = PLAN_NONE; /* re-plan on next apply */
+  /* re-plan on next apply, with kernels built from the new fields */
+  op->plan = PLAN_NONE;
+  if (op->eop) {
+    ceed_unregister_op(op->ceed, op->eop);
+    hb_elemop_destroy(op->eop);
+    op->eop            = NULL;
+    op->idl_coords_set = 0;
+  }
+  hb_faceop_destroy(op->fop);
+  op->fop = NULL;
   return CEED_ERROR_SUCCESS;
 }
 
@@ -1360,6 +1371,7 @@ int CeedOperatorRestoreContextDoubleRead(CeedOperator op, CeedContextFieldLabel 
 /* CeedOperator: backend plans                                                                                        */
 
 static int is_tensor3(CeedBasis b, int ncomp) { return b && b != CEED_BASIS_NONE && b->tensor && b->dim == 3 && b->num_comp == ncomp; }
+static int is_tensor2(CeedBasis b, int ncomp) { return b && b != CEED_BASIS_NONE && b->tensor && b->dim == 2 && b->num_comp == ncomp; }
 
 static int plan_fail(CeedOperator op, const char *why) {
   return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "operator '%s' (QFunction %s) has no B200 kernel: %s", op->name, op->qf->kernel, why);
@@ -1386,18 +1398,85 @@ static int check_qdata_rstr(CeedOperator op, CeedElemRestriction r, int ncomp, i
   return CEED_ERROR_SUCCESS;
 }
 
-/* gather the coordinate field of an input (restriction with 3 comps, P=2 basis) into an E-vector [E][3][8] */
-static int gather_coords(CeedOperator op, OpField *fx, CeedVector xvec, double **d_xe) {
+/* every vector a planned operator touches must be at least as long as its restriction says (device safety) */
+static int need_len(CeedOperator op, CeedVector v, CeedSize n, const char *what) {
+  if (!v || v == CEED_VECTOR_ACTIVE || v == CEED_VECTOR_NONE || v->length < n)
+    return CeedError(op->ceed, CEED_ERROR_DIMENSION, "operator '%s': %s vector missing or shorter than %td", op->name, what, n);
+  return CEED_ERROR_SUCCESS;
+}
+
+/* gather the coordinate field of an input (restriction with 3 comps, basis of P nodes per direction, elem_size nodes
+ * per element) into an E-vector [E][3][elem_size] */
+static int gather_coords_n(CeedOperator op, OpField *fx, CeedVector xvec, int P, int elem_size, double **d_xe) {
   CeedElemRestriction r = fx->r;
-  if (!r || r == CEED_ELEMRESTRICTION_NONE || r->num_comp != 3 || r->elem_size != 8 || !fx->b || fx->b == CEED_BASIS_NONE || fx->b->P1d != 2)
-    return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "coordinate field must be a trilinear (P=2) 3-component field");
+  if (!r || r == CEED_ELEMRESTRICTION_NONE || r->num_comp != 3 || r->elem_size != elem_size || !fx->b || fx->b == CEED_BASIS_NONE ||
+      fx->b->P1d != P)
+    return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "coordinate field must be a 3-component field with %d nodes per direction", P);
+  CK(need_len(op, xvec, r->l_size, "coordinate"));
   CK(rstr_upload(r));
-  const size_t nb = sizeof(double) * 24 * (size_t)r->num_elem;
+  const size_t nb = sizeof(double) * 3 * elem_size * (size_t)r->num_elem;
   if (!*d_xe) CUDA_CK(op->ceed, cudaMalloc((void **)d_xe, nb));
   const double *x;
   CK(vec_dev_read(xvec, &x));
-  HB_CK(op->ceed, hb_restrict_apply(r->num_elem, 8, 3, r->comp_stride, r->strided ? NULL : r->d_off, r->strided ? r->d_strides : NULL, x, *d_xe,
-                                    op->ceed->stream));
+  HB_CK(op->ceed, hb_restrict_apply(r->num_elem, elem_size, 3, r->comp_stride, r->strided ? NULL : r->d_off, r->strided ? r->d_strides : NULL, x,
+                                    *d_xe, op->ceed->stream));
+  return CEED_ERROR_SUCCESS;
+}
+
+/* the trilinear (P=2) volume coordinate field: E-vector [E][3][8] */
+static int gather_coords(CeedOperator op, OpField *fx, CeedVector xvec, double **d_xe) { return gather_coords_n(op, fx, xvec, 2, 8, d_xe); }
+
+/* The free-stream boundary sub-operators HONEE adds to its composites (HoneeBCCreateIFunctionQF / HoneeBCCreateIJacobianQF
+ * and HoneeBCAddIFunctionOp / HoneeBCAddIJacobianOp, src/boundary_condition.c:276-470; QFunctions of
+ * qfunctions/bc_freestream.h:54-138).  Inputs "q"/"dq" (INTERP), "Grad_q"/"Grad_dq" (GRAD, unused by the flux),
+ * "surface qdata" (NONE, 10), "x" (INTERP, unused); IFunction outputs "v" (INTERP) and, for implicit runs, "surface
+ * jacobian data" (NONE, 5); the IJacobian reads that data as its fifth input.  Returns the flux type through the name. */
+static int freestream_kernel(const char *k, int *jacobian, int *flux_type) {
+  static const struct {
+    const char *name;
+    int         jac, flux;
+  } tab[] = {{"Freestream_Conserv_HLL", 0, 0},
+             {"Freestream_Conserv_HLLC", 0, 1},
+             {"Freestream_Jacobian_Conserv_HLL", 1, 0},
+             {"Freestream_Jacobian_Conserv_HLLC", 1, 1}};
+  for (size_t i = 0; i < sizeof tab / sizeof tab[0]; i++)
+    if (!strcmp(k, tab[i].name)) {
+      *jacobian  = tab[i].jac;
+      *flux_type = tab[i].flux;
+      return 1;
+    }
+  return 0;
+}
+
+static int plan_freestream(CeedOperator op, int jacobian, int flux_type) {
+  CeedQFunction qf = op->qf;
+  const int     nin = jacobian ? 5 : 4, nout = jacobian ? 1 : (qf->nout == 2 ? 2 : 1);
+  if (qf->nin != nin || qf->nout != nout || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[0].size != 5 || qf->in[1].emode != CEED_EVAL_GRAD ||
+      qf->in[2].emode != CEED_EVAL_NONE || qf->in[2].size != 10 || qf->in[3].emode != CEED_EVAL_INTERP || qf->out[0].emode != CEED_EVAL_INTERP ||
+      qf->out[0].size != 5 || (jacobian && (qf->in[4].emode != CEED_EVAL_NONE || qf->in[4].size != 5)) ||
+      (nout == 2 && (qf->out[1].emode != CEED_EVAL_NONE || qf->out[1].size != 5)))
+    return plan_fail(op, "unexpected free-stream field layout (src/boundary_condition.c:276-364)");
+  if (op->in[0].v != CEED_VECTOR_ACTIVE || op->in[1].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE)
+    return plan_fail(op, "the state and test fields must be active");
+  CeedElemRestriction r = op->in[0].r;
+  CeedBasis           b = op->in[0].b;
+  if (op->in[1].r != r || op->out[0].r != r || op->in[1].b != b || op->out[0].b != b) return plan_fail(op, "state fields must share one face restriction and basis");
+  if (!r || r == CEED_ELEMRESTRICTION_NONE || r->strided || r->num_comp != 5 || r->comp_stride != 1)
+    return plan_fail(op, "face restriction must be 5 node-interleaved components (comp_stride 1) with offsets");
+  if (!is_tensor2(b, 5) || r->elem_size != b->P1d * b->P1d) return plan_fail(op, "face basis must be a 2D tensor H1 basis with 5 components");
+  if (!qf->ctx || qf->ctx->size != sizeof(HbFreestreamContext)) return plan_fail(op, "context must be the 264-byte FreestreamContext_");
+  if (((const HbFreestreamContext *)qf->ctx->data)->newt.state_var != HB_STATEVAR_CONSERVATIVE)
+    return plan_fail(op, "free-stream context must use conservative variables");
+  const int Q2 = b->Q1d * b->Q1d;
+  CK(check_qdata_rstr(op, op->in[2].r, 10, Q2, "surface qdata"));
+  if (jacobian) CK(check_qdata_rstr(op, op->in[4].r, 5, Q2, "surface jacobian data"));
+  if (nout == 2) CK(check_qdata_rstr(op, op->out[1].r, 5, Q2, "surface jacobian data"));
+  if (!op->fop) {
+    int rc = hb_faceop_create(r->num_elem, b->P1d, b->Q1d, r->h_off, r->l_size, b->interp1d, b->grad1d, b->qweight1d, &op->fop);
+    if (rc) return CeedError(op->ceed, CEED_ERROR_BACKEND, "face operator creation failed (%d): offsets outside the L-vector or sizes too large", rc);
+  }
+  op->flux_type = flux_type;
+  op->plan      = jacobian ? PLAN_FREESTREAM_JAC : PLAN_FREESTREAM;
   return CEED_ERROR_SUCCESS;
 }
 
@@ -1461,18 +1540,26 @@ static int op_plan(CeedOperator op) {
     op->plan = PLAN_IJACOBIAN;
     return CEED_ERROR_SUCCESS;
   }
+  if (!strcmp(k, "SetupBoundary")) {
+    /* inputs "dx" (GRAD of the face coordinates), "weight" (WEIGHT); output "surface qdata" (NONE, 10, strided) --
+     * QDataBoundaryGet, src/qdata.c:228-261 */
+    if (qf->nin != 2 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_GRAD || qf->in[1].emode != CEED_EVAL_WEIGHT ||
+        qf->out[0].emode != CEED_EVAL_NONE || qf->out[0].size != 10)
+      return plan_fail(op, "unexpected SetupBoundary field layout (src/qdata.c:251-255)");
+    if (op->in[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "SetupBoundary expects the face coordinates as the active input");
+    CeedBasis bx = op->in[0].b;
+    if (!is_tensor2(bx, 3)) return plan_fail(op, "SetupBoundary needs a 2D tensor coordinate basis with 3 components");
+    CK(check_qdata_rstr(op, op->out[0].r, 10, bx->Q1d * bx->Q1d, "surface qdata"));
+    op->plan = PLAN_SETUP_SUR;
+    return CEED_ERROR_SUCCESS;
+  }
+  int jacobian, flux_type;
+  if (freestream_kernel(k, &jacobian, &flux_type)) return plan_freestream(op, jacobian, flux_type);
   return plan_fail(op, "no fused kernel for this QFunction (no CPU fallback on /gpu/b200)");
 }
 
 static int vec_f32_shadow(CeedVector v) {
   if (!v->d_f32) CUDA_CK(v->ceed, cudaMalloc((void **)&v->d_f32, sizeof(float) * (size_t)(v->length ? v->length : 1)));
-  return CEED_ERROR_SUCCESS;
-}
-
-/* every vector a planned operator touches must be at least as long as its restriction says (device safety) */
-static int need_len(CeedOperator op, CeedVector v, CeedSize n, const char *what) {
-  if (!v || v == CEED_VECTOR_ACTIVE || v == CEED_VECTOR_NONE || v->length < n)
-    return CeedError(op->ceed, CEED_ERROR_DIMENSION, "operator '%s': %s vector missing or shorter than %td", op->name, what, n);
   return CEED_ERROR_SUCCESS;
 }
 
@@ -1491,6 +1578,48 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
       CK(vec_dev_write(out, &qd, 1));
       /* Setup writes (not adds) qdata: libCEED's strided output of an EVAL_NONE field is overwritten per element */
       HB_CK(ceed, hb_setup_qdata(op->in[0].r->num_elem, bx->Q1d, bx->qref1d, bx->qweight1d, op->d_tmp_e, qd, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_SETUP_SUR: {
+      CeedBasis bx = op->in[0].b;
+      CK(need_len(op, out, op->out[0].r->l_size, "surface qdata"));
+      CK(gather_coords_n(op, &op->in[0], in, bx->P1d, bx->P1d * bx->P1d, &op->d_tmp_e));
+      double *qd;
+      CK(vec_dev_write(out, &qd, 1));
+      HB_CK(ceed, hb_face_setup_qdata_nodes(op->in[0].r->num_elem, bx->P1d, bx->Q1d, bx->interp1d, bx->grad1d, bx->qweight1d, op->d_tmp_e, qd, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_FREESTREAM: {
+      /* FP64 in both precisions: the boundary is O(E^(2/3)) of the work; in the mixed run its jac data stays FP64 */
+      const int64_t n = op->fop->l_size;
+      CK(need_len(op, in, n, "input"));
+      CK(need_len(op, out, n, "output"));
+      CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "surface qdata"));
+      const double *q, *qd;
+      double       *jd = NULL, *v;
+      CK(vec_dev_read(in, &q));
+      CK(vec_dev_read(op->in[2].v, &qd));
+      if (op->qf->nout == 2) {
+        CK(need_len(op, op->out[1].v, op->out[1].r->l_size, "surface jacobian data"));
+        CK(vec_dev_write(op->out[1].v, &jd, 1));
+      }
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_freestream_apply(op->fop, op->qf->ctx->data, op->flux_type, qd, q, jd, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_FREESTREAM_JAC: {
+      const int64_t n = op->fop->l_size;
+      CK(need_len(op, in, n, "input"));
+      CK(need_len(op, out, n, "output"));
+      CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "surface qdata"));
+      CK(need_len(op, op->in[4].v, op->in[4].r->l_size, "surface jacobian data"));
+      const double *dq, *qd, *jd;
+      double       *v;
+      CK(vec_dev_read(in, &dq));
+      CK(vec_dev_read(op->in[2].v, &qd));
+      CK(vec_dev_read(op->in[4].v, &jd));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_freestream_jacobian_apply(op->fop, op->qf->ctx->data, op->flux_type, qd, jd, dq, v, s));
       return CEED_ERROR_SUCCESS;
     }
     case PLAN_IFUNCTION: {
@@ -1589,7 +1718,7 @@ int CeedOperatorApply(CeedOperator op, CeedVector in, CeedVector out, CeedReques
   (void)request;
   if (out && out != CEED_VECTOR_NONE) {
     /* Setup overwrites; everything else accumulates after zeroing */
-    int only_setup = !op->composite && (op_plan(op) == 0) && op->plan == PLAN_SETUP;
+    int only_setup = !op->composite && (op_plan(op) == 0) && (op->plan == PLAN_SETUP || op->plan == PLAN_SETUP_SUR);
     if (!only_setup) CK(CeedVectorSetValue(out, 0.0));
   }
   return op_apply_add(op, in, out);
@@ -1602,7 +1731,19 @@ int CeedOperatorApplyAdd(CeedOperator op, CeedVector in, CeedVector out, CeedReq
 
 static int op_diag_add_single(CeedOperator op, CeedVector assembled) {
   CK(op_plan(op));
-  if (op->plan != PLAN_IJACOBIAN) return plan_fail(op, "diagonal assembly is provided for the IJacobian operator");
+  if (op->plan == PLAN_FREESTREAM_JAC) {
+    CK(need_len(op, assembled, op->fop->l_size, "diagonal"));
+    CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "surface qdata"));
+    CK(need_len(op, op->in[4].v, op->in[4].r->l_size, "surface jacobian data"));
+    const double *qd, *jd;
+    double       *y;
+    CK(vec_dev_read(op->in[2].v, &qd));
+    CK(vec_dev_read(op->in[4].v, &jd));
+    CK(vec_dev_write(assembled, &y, 0));
+    HB_CK(op->ceed, hb_freestream_diagonal(op->fop, op->qf->ctx->data, op->flux_type, qd, jd, y, op->ceed->stream));
+    return CEED_ERROR_SUCCESS;
+  }
+  if (op->plan != PLAN_IJACOBIAN) return plan_fail(op, "diagonal assembly is provided for the IJacobian operators (volume and free-stream faces)");
   CK(need_len(op, assembled, op->eop->l_size, "diagonal"));
   CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
   CK(need_len(op, op->in[3].v, op->in[3].r->l_size, "jac_data"));
@@ -1702,6 +1843,7 @@ int CeedOperatorDestroy(CeedOperator *op) {
   }
   if (o->eop) ceed_unregister_op(o->ceed, o->eop);
   hb_elemop_destroy(o->eop);
+  hb_faceop_destroy(o->fop);
   cudaFree(o->d_tmp_in32);
   cudaFree(o->d_tmp_out32);
   cudaFree(o->d_tmp_e);
@@ -1824,6 +1966,9 @@ static void op_view(CeedOperator op, FILE *stream, int terse, int depth) {
           op->plan == PLAN_IFUNCTION   ? "fused IFunction"
           : op->plan == PLAN_IJACOBIAN ? "fused IJacobian"
           : op->plan == PLAN_SETUP     ? "qdata setup"
+          : op->plan == PLAN_SETUP_SUR ? "surface qdata setup"
+          : op->plan == PLAN_FREESTREAM ? "free-stream faces"
+          : op->plan == PLAN_FREESTREAM_JAC ? "free-stream faces Jacobian"
                                        : "not planned");
   if (terse) return;
   for (int o = 0; o < 2; o++)

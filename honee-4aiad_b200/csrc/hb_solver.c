@@ -255,10 +255,12 @@ static int assemble_pc(HbTimeStepper *ts) {
     HBCK(hb_diagonal_assemble_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (float *)ts->diag, 0, ts->s));
     /* invert in FP64 (delta is free before the Krylov solve), store FP32 */
     HBCK(hb_vec_f32_to_f64((const float *)ts->diag, ts->delta, ts->n, 0, ts->s));
+    if (ts->bc) HBCK(hb_freestream_diagonal(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, ts->delta, ts->s));
     HBCK(hb_vec_reciprocal_f64(ts->delta, ts->n, ts->s));
     return hb_vec_f64_to_f32(ts->delta, (float *)ts->diag, ts->n, 0, ts->s);
   }
   HBCK(hb_diagonal_assemble_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, (double *)ts->diag, 0, ts->s));
+  if (ts->bc) HBCK(hb_freestream_diagonal(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, (double *)ts->diag, ts->s));
   return hb_vec_reciprocal_f64((double *)ts->diag, ts->n, ts->s);
 }
 

@@ -152,6 +152,46 @@ __global__ void k_freestream_jac(int P, int Q, const int32_t *__restrict__ offse
   }
 }
 
+// diag += sum over the face's points of B_p^2 wdetJb dF_c/dU_c: the diagonal of the operator above, each point's
+// Jacobian column c taken by the forward tangent with dU = e_c (libCEED diagonal assembly of Freestream_Jacobian)
+__global__ void k_freestream_diag(int P, int Q, const int32_t *__restrict__ offsets, const int32_t *__restrict__ faces, FaceBasis b,
+                                  hb::PhysConst<double> pc, Exterior ex, const double *__restrict__ qd, const double *__restrict__ jac,
+                                  double *__restrict__ diag) {
+  __shared__ double sD[5][kMaxQ2];
+  const int f = faces[blockIdx.x], t = threadIdx.x, P2 = P * P, Q2 = Q * Q;
+  if (t < Q2) {
+    double U[5];
+    for (int c = 0; c < 5; c++) U[c] = jac[((int64_t)f * 5 + c) * Q2 + t];
+    hb::St<double> s, sx, dsx;
+    double inv_rho, etot, eint;
+    hb::state_from_u(pc, U, s, inv_rho, etot, eint);
+    exterior_state(ex, sx);
+    memset(&dsx, 0, sizeof dsx);
+    const double *qf = qd + (int64_t)f * 10 * Q2;
+    const double wdetJb = qf[t], n[3] = {qf[Q2 + t], qf[2 * Q2 + t], qf[3 * Q2 + t]};
+#pragma unroll
+    for (int c = 0; c < 5; c++) {  // unrolled: c indexes registers, not a local array
+      double dU[5] = {0, 0, 0, 0, 0}, dF[5];
+      dU[c] = 1.0;
+      hb::St<double> ds;
+      hb::state_from_u_fwd(pc, s, inv_rho, etot, eint, dU, ds);
+      if (ex.hllc) hb::riemann::hllc_flux_fwd(ex.gamma, ex.cv, s, ds, sx, dsx, n, dF);
+      else hb::riemann::hll_flux_fwd(ex.gamma, ex.cv, s, ds, sx, dsx, n, dF);
+      sD[c][t] = wdetJb * dF[c];
+    }
+  }
+  __syncthreads();
+  for (int i = t; i < 5 * P2; i += blockDim.x) {
+    const int p = i / 5, c = i % 5;
+    double acc = 0;
+    for (int k = 0; k < Q2; k++) {
+      const double w = b2(b, P, k % Q, k / Q, p % P, p / P);
+      acc += w * w * sD[c][k];
+    }
+    diag[offsets[(int64_t)f * P2 + p] + c] += acc;
+  }
+}
+
 FaceBasis fbasis(const HbFaceOp *op) {
   FaceBasis b;
   memset(&b, 0, sizeof b);
@@ -252,8 +292,22 @@ int hb_faceop_destroy(HbFaceOp *op) {
 }
 
 int hb_face_setup_qdata(const HbFaceOp *op, const double *x_nodes, double *qdata_sur, void *stream) {
-  if (!op || !x_nodes || !qdata_sur) return HB_ERROR_INVALID;
-  k_face_setup<<<op->num_faces, (op->Q * op->Q + 31) / 32 * 32, 0, (cudaStream_t)stream>>>(op->P, op->Q, fbasis(op), x_nodes, qdata_sur);
+  if (!op) return HB_ERROR_INVALID;
+  return hb_face_setup_qdata_nodes(op->num_faces, op->P, op->Q, op->interp1d, op->grad1d, op->qweight1d, x_nodes, qdata_sur, stream);
+}
+
+int hb_face_setup_qdata_nodes(int num_faces, int P, int Q, const double *interp1d, const double *grad1d, const double *qweight1d,
+                              const double *x_nodes, double *qdata_sur, void *stream) {
+  if (num_faces < 0 || P < 2 || Q < 1 || P > HB_MAX_P || Q > HB_MAX_P || Q * Q > kMaxQ2 || !interp1d || !grad1d || !qweight1d || !x_nodes ||
+      !qdata_sur)
+    return HB_ERROR_INVALID;
+  if (num_faces == 0) return HB_SUCCESS;
+  FaceBasis b;
+  memset(&b, 0, sizeof b);
+  memcpy(b.B, interp1d, sizeof(double) * P * Q);
+  memcpy(b.G, grad1d, sizeof(double) * P * Q);
+  memcpy(b.w, qweight1d, sizeof(double) * Q);
+  k_face_setup<<<num_faces, (Q * Q + 31) / 32 * 32, 0, (cudaStream_t)stream>>>(P, Q, b, x_nodes, qdata_sur);
   return rc();
 }
 
@@ -278,6 +332,24 @@ int hb_freestream_apply(const HbFaceOp *op, const void *ctx264, int flux_type, c
 int hb_freestream_jacobian_apply(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
                                  const double *dq, double *v, void *stream) {
   return freestream_jac<double>(op, ctx264, flux_type, qdata_sur, jac_data_sur, dq, v, stream);
+}
+
+int hb_freestream_diagonal(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur, double *diag,
+                           void *stream) {
+  if (!op || !ctx264 || !qdata_sur || !jac_data_sur || !diag || (flux_type != 0 && flux_type != 1)) return HB_ERROR_INVALID;
+  hb::PhysConst<double> pc;
+  Exterior ex;
+  int err = unpack_ctx(ctx264, pc, ex);
+  if (err) return err;
+  ex.hllc = flux_type == 1;
+  const FaceBasis b = fbasis(op);
+  for (int c = 0; c < op->num_colors; c++) {
+    const int n = op->h_color_ptr[c + 1] - op->h_color_ptr[c];
+    if (n)
+      k_freestream_diag<<<n, nthreads(op), 0, (cudaStream_t)stream>>>(op->P, op->Q, op->d_offsets, op->d_color_elem + op->h_color_ptr[c], b, pc, ex,
+                                                                      qdata_sur, jac_data_sur, diag);
+  }
+  return rc();
 }
 
 int hb_freestream_jacobian_apply_f32(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,

@@ -11,14 +11,20 @@ and exposes the calls the reference makes in its hot loop:
   * FormIJacobian_NS (src/setupts.c:131-157) -> :meth:`NewtonianOperators.set_ijacobian_shift`
   * MatMult_Ceed (src/mat-ceed.c:1643-1700)  -> :meth:`NewtonianOperators.ijacobian`
   * MatGetDiagonal_Ceed (src/mat-ceed.c:1603-1634) -> :meth:`NewtonianOperators.diagonal`
+and, for the free-stream boundary (problems/bc_freestream.c:112-190), the face sub-operators the reference adds to both
+composites: QDataBoundaryGet (src/qdata.c:228-270, ``SetupBoundary``), HoneeBCAddIFunctionOp / HoneeBCAddIJacobianOp
+(src/boundary_condition.c:371-470) with the QFunctions of HoneeBCCreateIFunctionQF / HoneeBCCreateIJacobianQF
+(:276-364) -> :meth:`NewtonianOperators.add_freestream`.
 The structured box mesh stands in for DMPlex; all arithmetic happens in libceed_b200.so.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from . import ceed as ce
-from .problem import CONTEXT_LABELS, BoxMesh, TensorBasis, context_bytes
+from .problem import CONTEXT_LABELS, BoxMesh, TensorBasis, box_faces, context_bytes, freestream_context
 
 
 def linear_coordinate_basis(Q: int, qref1d, qweight1d):
@@ -112,6 +118,92 @@ class NewtonianOperators:
         self.op_ijacobian.set_name("IJacobian Composite Operator")
         self.op_ijacobian.add_sub(op_ij)
         self._vol = (op_if, op_ij, qf_if, qf_ij, qf_setup)
+        self.op_ifunction_volume, self.op_ijacobian_volume = op_if, op_ij
+        self.boundaries = []
+
+    # ---- boundary faces
+    def add_freestream(self, P_inf, u_inf, T_inf, *, riemann="hllc", sides=None, implicit=True):
+        """Free-stream condition on the non-periodic box sides: face restriction and 2D basis of the state, the bilinear
+        face coordinate field, surface qdata from ``SetupBoundary``, and the ``Freestream_[Jacobian_]Conserv_HLL[C]`` sub-
+        operators joined to the IFunction and IJacobian composites (num_comps_jac_data 5 for implicit runs,
+        problems/bc_freestream.c:175)."""
+        ceed, mesh, basis = self.ceed, self.mesh, self.basis
+        P, Q = basis.P, basis.Q
+        off, xn, names = box_faces(mesh, basis, sides)
+        F = off.shape[0]
+        Q2 = Q * Q
+        flux = {"hll": "HLL", "hllc": "HLLC"}[riemann]
+        # -- face restriction and basis of the state (DMPlexCeedElemRestrictionCreate / DMPlexCeedBasisCreate at the face height)
+        rstr_q = ce.ElemRestriction(ceed, F, P * P, 5, 1, mesh.l_size, offsets=off)
+        basis_q = ce.Basis(ceed, 2, 5, P, Q, basis.interp1d, basis.grad1d, basis.qref1d, basis.qweight1d)
+        # -- bilinear face coordinates (DMPlexCeedCoordinateCreateField at the face height): the face's corner nodes
+        corners = [0, P - 1, P * (P - 1), P * P - 1]
+        x_face = np.ascontiguousarray(xn[:, :, corners].transpose(0, 2, 1)).reshape(-1)      # [F][vertex][3]
+        x_coord = ce.Vector(ceed, F * 12)
+        x_coord.set_array_host(x_face)
+        rstr_x = ce.ElemRestriction(ceed, F, 4, 3, 1, F * 12, offsets=(np.arange(F * 4, dtype=np.int64) * 3).astype(np.int32))
+        Bx, Gx = linear_coordinate_basis(Q, basis.qref1d, basis.qweight1d)
+        basis_x = ce.Basis(ceed, 2, 3, 2, Q, Bx, Gx, basis.qref1d, basis.qweight1d)
+        # -- surface qdata (QDataBoundaryGet)
+        rstr_qd = ce.ElemRestriction(ceed, F, Q2, 10, 0, F * Q2 * 10)
+        q_data = ce.Vector(ceed, F * Q2 * 10)
+        qf_setup = ce.QFunction(ceed, "setupgeo.h:SetupBoundary")
+        qf_setup.add_input("dx", 6, ce.CEED_EVAL_GRAD)
+        qf_setup.add_input("weight", 1, ce.CEED_EVAL_WEIGHT)
+        qf_setup.add_output("surface qdata", 10, ce.CEED_EVAL_NONE)
+        op_setup = ce.Operator(ceed, qf_setup)
+        op_setup.set_field("dx", rstr_x, basis_x, ceed.active)
+        op_setup.set_field("weight", ceed.rstr_none, basis_x, ceed.vector_none)
+        op_setup.set_field("surface qdata", rstr_qd, ceed.basis_none, ceed.active)
+        op_setup.apply(x_coord, q_data)
+        # -- context: FreestreamContext_ (the Newtonian context and the exterior State)
+        fs_bytes = freestream_context(self.ctx, P_inf, u_inf, T_inf)
+        fs_ctx = ce.QFunctionContext(ceed, (ctypes.c_char * len(fs_bytes)).from_buffer_copy(fs_bytes))
+        njd = 5 if implicit else 0
+        rstr_jd = ce.ElemRestriction(ceed, F, Q2, 5, 0, F * Q2 * 5) if njd else None
+        jac_data = ce.Vector(ceed, F * Q2 * 5) if njd else None
+        # -- IFunction face sub-operator
+        qf_if = ce.QFunction(ceed, f"bc_freestream.h:Freestream_Conserv_{flux}")
+        for name, size, mode in (("q", 5, ce.CEED_EVAL_INTERP), ("Grad_q", 10, ce.CEED_EVAL_GRAD), ("surface qdata", 10, ce.CEED_EVAL_NONE),
+                                 ("x", 3, ce.CEED_EVAL_INTERP)):
+            qf_if.add_input(name, size, mode)
+        qf_if.add_output("v", 5, ce.CEED_EVAL_INTERP)
+        if njd:
+            qf_if.add_output("surface jacobian data", njd, ce.CEED_EVAL_NONE)
+        qf_if.set_context(fs_ctx)
+        op_if = ce.Operator(ceed, qf_if)
+        op_if.set_name("Freestream IFunction")
+        op_if.set_field("q", rstr_q, basis_q, ceed.active)
+        op_if.set_field("Grad_q", rstr_q, basis_q, ceed.active)
+        op_if.set_field("surface qdata", rstr_qd, ceed.basis_none, q_data)
+        op_if.set_field("x", rstr_x, basis_x, x_coord)
+        op_if.set_field("v", rstr_q, basis_q, ceed.active)
+        if njd:
+            op_if.set_field("surface jacobian data", rstr_jd, ceed.basis_none, jac_data)
+        self.op_ifunction.add_sub(op_if)
+        op_ij = None
+        if njd:
+            qf_ij = ce.QFunction(ceed, f"bc_freestream.h:Freestream_Jacobian_Conserv_{flux}")
+            for name, size, mode in (("dq", 5, ce.CEED_EVAL_INTERP), ("Grad_dq", 10, ce.CEED_EVAL_GRAD),
+                                     ("surface qdata", 10, ce.CEED_EVAL_NONE), ("x", 3, ce.CEED_EVAL_INTERP),
+                                     ("surface jacobian data", njd, ce.CEED_EVAL_NONE)):
+                qf_ij.add_input(name, size, mode)
+            qf_ij.add_output("v", 5, ce.CEED_EVAL_INTERP)
+            qf_ij.set_context(fs_ctx)
+            op_ij = ce.Operator(ceed, qf_ij)
+            op_ij.set_name("Freestream IJacobian")
+            op_ij.set_field("dq", rstr_q, basis_q, ceed.active)
+            op_ij.set_field("Grad_dq", rstr_q, basis_q, ceed.active)
+            op_ij.set_field("surface qdata", rstr_qd, ceed.basis_none, q_data)
+            op_ij.set_field("x", rstr_x, basis_x, x_coord)
+            op_ij.set_field("surface jacobian data", rstr_jd, ceed.basis_none, jac_data)
+            op_ij.set_field("v", rstr_q, basis_q, ceed.active)
+            self.op_ijacobian.add_sub(op_ij)
+        bc = dict(offsets=off, x_nodes=xn, sides=names, q_data=q_data, jac_data=jac_data, ctx_bytes=fs_bytes, op_ifunction=op_if,
+                  op_ijacobian=op_ij, hllc=flux == "HLLC",
+                  _keep=(rstr_q, basis_q, x_coord, rstr_x, basis_x, rstr_qd, qf_setup, op_setup, fs_ctx, rstr_jd, qf_if))
+        self.boundaries.append(bc)
+        return bc
 
     # ---- context updates (src/setupts.c:91-93, :141)
     def set_time(self, t):

@@ -291,6 +291,10 @@ HB_EXPORT int hb_faceop_destroy(HbFaceOp *op);
  * [F][3][P^2] (device): w detJb, unit normal, dX/dx (2 x 3).  The normal is the cross product of the two face tangents
  * in face-tensor order; the face node order decides its orientation (outward for the box faces of problem.py). */
 HB_EXPORT int hb_face_setup_qdata(const HbFaceOp *op, const double *x_nodes, double *qdata_sur, void *s);
+/* The same geometric factors for any face coordinate basis (P coordinate nodes per direction, e.g. the bilinear P = 2
+ * field DMPlexCeedCoordinateCreateField gives HONEE's surface Setup operator, src/qdata.c:228-261): x_nodes [F][3][P^2]. */
+HB_EXPORT int hb_face_setup_qdata_nodes(int num_faces, int P, int Q, const double *interp1d, const double *grad1d, const double *qweight1d,
+                                        const double *x_nodes, double *qdata_sur, void *s);
 /* v += int phi wdetJb F(q, S_infty, n), F = HLL (flux_type 0) or HLLC (1); jac_data_sur [F][5][Q^2] (may be NULL) = q at
  * the points (Freestream, bc_freestream.h:14-48). */
 HB_EXPORT int hb_freestream_apply(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *q, double *jac_data_sur,
@@ -298,12 +302,16 @@ HB_EXPORT int hb_freestream_apply(const HbFaceOp *op, const void *ctx264, int fl
 /* v += int phi wdetJb dF(q; dq) with the exterior state fixed (Freestream_Jacobian, bc_freestream.h:75-114). */
 HB_EXPORT int hb_freestream_jacobian_apply(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
                                            const double *dq, double *v, void *s);
+/* diag += the diagonal of that Jacobian (what CeedOperatorLinearAssembleAddDiagonal gives for the Freestream_Jacobian
+ * sub-operator): per face node p and component c, sum over points of B_p^2 wdetJb dF_c/dU_c. */
+HB_EXPORT int hb_freestream_diagonal(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
+                                     double *diag, void *s);
 /* the same with FP32 dq and v (state and flux math in FP64), for the mixed-precision Krylov solve */
 HB_EXPORT int hb_freestream_jacobian_apply_f32(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur,
                                                const double *jac_data_sur, const float *dq, float *v, void *s);
 
-/* Attach (faces != NULL) or detach the free-stream boundary to a time stepper: its flux joins every residual and its
- * tangent every Krylov product (FP32 in mixed precision); the Jacobi diagonal stays the volume one. */
+/* Attach (faces != NULL) or detach the free-stream boundary to a time stepper: its flux joins every residual, its
+ * tangent every Krylov product (FP32 in mixed precision) and its diagonal the Jacobi preconditioner (FP64). */
 HB_EXPORT int hb_ts_set_freestream(HbTimeStepper *ts, const HbFaceOp *faces, const void *ctx264, int flux_type, const double *qdata_sur);
 
 /* Library identification */

@@ -200,3 +200,27 @@ def freestream_apply(offsets, interp1d, P, Q, qdata_sur, q, U_inf, Y_inf, cv, cp
         for p in range(P * P):
             out[offsets[f, p]:offsets[f, p] + 5] += contrib[p]
     return out
+
+
+def freestream_diagonal(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, cv, cp, hllc=True, l_size=None):
+    """Diagonal of the free-stream Jacobian as an L-vector: for face node p and component c, the sum over the face's
+    points of B_p^2 wdetJb dF_c/dU_c, the column of the point Jacobian taken by the forward tangent with dU = e_c (the
+    libCEED diagonal assembly of the Freestream_Jacobian operator, bc_freestream.h:75-114, summed over faces)."""
+    B = np.asarray(interp1d).reshape(Q, P)
+    Bq = np.einsum("jb,ia->jiba", B, B).reshape(Q * Q, P * P)
+    F = offsets.shape[0]
+    out = np.zeros(l_size if l_size is not None else int(offsets.max()) + 5)
+    zero = St(*(np.zeros(Q * Q) if k not in (1, 4) else np.zeros((3, Q * Q)) for k in range(6)))
+    for f in range(F):
+        s = state_from_U(jac[f], cv, cp)
+        n = qdata_sur[f, 1:4]
+        D = np.zeros((5, Q * Q))
+        for c in range(5):
+            dU = np.zeros((5, Q * Q))
+            dU[c] = 1.0
+            ds = state_from_U_fwd(s, dU, cv, cp)
+            D[c] = qdata_sur[f, 0] * riemann(s, exterior(U_inf, Y_inf, Q * Q), n, cv, cp, hllc, dL=ds, dR=zero)[c]
+        contrib = (Bq.T ** 2) @ D.T                                          # [P2][5]
+        for p in range(P * P):
+            out[offsets[f, p]:offsets[f, p] + 5] += contrib[p]
+    return out

@@ -80,3 +80,28 @@ def test_face_qdata_matches_reference():
     inv = np.array([[c / det, -b / det], [-b / det, a / det]])
     dXdx = np.stack([inv[i, 0] * J0 + inv[i, 1] * J1 for i in range(2)])  # [2][3][n]
     np.testing.assert_allclose(ref[4:], dXdx.reshape(6, n), rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("hllc", [False, True])
+def test_face_diagonal_is_the_oracle_jacobian_diagonal(hllc):
+    """freestream_diagonal equals e_i^T J e_i of the oracle's face Jacobian (itself pinned to the reference's
+    Freestream_Jacobian above), on a small box with every side a free-stream face."""
+    import importlib
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    U, Y, cv, cp = _ext()
+    mesh = prob.box_mesh((2, 1, 1), 3)
+    basis = prob.tensor_basis(3, 3)
+    gas = prob.GasProperties(cv=cv, cp=cp)
+    q = prob.gaussian_pulse_state(mesh, basis, gas, seed=2)
+    off, xn, _ = prob.box_faces(mesh, basis)
+    qd = FO.face_qdata(basis.interp1d, basis.grad1d, basis.qweight1d, 3, 3, xn)
+    B = np.asarray(basis.interp1d).reshape(3, 3)
+    Bq = np.einsum("jb,ia->jiba", B, B).reshape(9, 9)
+    jac = np.stack([(Bq @ q.reshape(-1, 5)[off[f] // 5]).T for f in range(off.shape[0])])
+    d = FO.freestream_diagonal(off, basis.interp1d, 3, 3, qd, jac, U, Y, cv, cp, hllc=hllc, l_size=mesh.l_size)
+    rng = np.random.default_rng(1)
+    for i in rng.choice(np.unique(off.reshape(-1)), 12, replace=False) + rng.integers(0, 5, 12):
+        e = np.zeros(mesh.l_size)
+        e[i] = 1.0
+        col = FO.freestream_apply(off, basis.interp1d, 3, 3, qd, q, U, Y, cv, cp, hllc=hllc, dq=e, jac=jac)
+        assert abs(col[i] - d[i]) <= 1e-12 * np.abs(d).max()
