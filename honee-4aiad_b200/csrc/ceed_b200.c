@@ -119,7 +119,7 @@ typedef struct {
   int                 set;
 } OpField;
 
-enum { PLAN_NONE = 0, PLAN_SETUP, PLAN_IFUNCTION, PLAN_IJACOBIAN, PLAN_SETUP_SUR, PLAN_FREESTREAM, PLAN_FREESTREAM_JAC };
+enum { PLAN_NONE = 0, PLAN_SETUP, PLAN_IFUNCTION, PLAN_IJACOBIAN, PLAN_SETUP_SUR, PLAN_FREESTREAM, PLAN_FREESTREAM_JAC, PLAN_RHS, PLAN_MASS };
 
 struct CeedOperator_private {
   Ceed          ceed;
@@ -137,6 +137,7 @@ struct CeedOperator_private {
   float    *d_tmp_in32, *d_tmp_out32; /* mixed-precision staging of L-vectors */
   double   *d_tmp_e;                  /* coordinate E-vector for the Setup operator */
   HbFaceOp *fop;                      /* boundary-face sub-operators */
+  double   *d_zero, *d_tmp_rhs;       /* explicit right-hand side: zero rate and the residual it is negated from */
   int       flux_type;                /* 0 HLL, 1 HLLC */
 };
 
@@ -1247,6 +1248,14 @@ int CeedOperatorSetField(CeedOperator op, const char *field_name, CeedElemRestri
   }
   hb_faceop_destroy(op->fop);
   op->fop = NULL;
+  /* work buffers sized by the old fields */
+  cudaFree(op->d_zero);
+  cudaFree(op->d_tmp_rhs);
+  cudaFree(op->d_tmp_in32);
+  cudaFree(op->d_tmp_out32);
+  cudaFree(op->d_tmp_e);
+  op->d_zero = op->d_tmp_rhs = op->d_tmp_e = NULL;
+  op->d_tmp_in32 = op->d_tmp_out32 = NULL;
   return CEED_ERROR_SUCCESS;
 }
 
@@ -1540,6 +1549,38 @@ static int op_plan(CeedOperator op) {
     op->plan = PLAN_IJACOBIAN;
     return CEED_ERROR_SUCCESS;
   }
+  if (!strcmp(k, "RHSFunction_Newtonian")) {
+    /* explicit right-hand side (src/setuplibceed.c:179-205): q (INTERP), Grad_q (GRAD), qdata (NONE, 10), x (INTERP) ->
+     * v (INTERP), Grad_v (GRAD) */
+    if (qf->nin != 4 || qf->nout != 2 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[1].emode != CEED_EVAL_GRAD ||
+        qf->in[2].emode != CEED_EVAL_NONE || qf->in[3].emode != CEED_EVAL_INTERP || qf->out[0].emode != CEED_EVAL_INTERP ||
+        qf->out[1].emode != CEED_EVAL_GRAD)
+      return plan_fail(op, qf->nin > 4 ? "projected divergence of the diffusive flux is not supported"
+                                       : "unexpected RHSFunction field layout (src/setuplibceed.c:185-192)");
+    if (op->in[0].v != CEED_VECTOR_ACTIVE || op->in[1].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE ||
+        op->out[1].v != CEED_VECTOR_ACTIVE)
+      return plan_fail(op, "q/Grad_q and v/Grad_v must be active");
+    if (op->in[0].r != op->in[1].r || op->in[0].r != op->out[0].r || op->in[0].r != op->out[1].r) return plan_fail(op, "shared restriction expected");
+    if (op->in[0].b != op->in[1].b || op->in[0].b != op->out[0].b || op->in[0].b != op->out[1].b) return plan_fail(op, "shared basis expected");
+    if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+    CK(plan_elemop(op, op->in[0].r, op->in[0].b));
+    CK(check_qdata_rstr(op, op->in[2].r, 10, op->eop->Q * op->eop->Q * op->eop->Q, "qdata"));
+    op->plan = PLAN_RHS;
+    return CEED_ERROR_SUCCESS;
+  }
+  if (!strcmp(k, "Mass_5")) {
+    /* HoneeMassQFunctionCreate (src/honee-mass.c:20-60) on the state fields: u (INTERP), qdata (NONE) -> v (INTERP) */
+    if (qf->nin != 2 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[0].size != 5 || qf->in[1].emode != CEED_EVAL_NONE ||
+        qf->out[0].emode != CEED_EVAL_INTERP || qf->out[0].size != 5)
+      return plan_fail(op, "unexpected Mass_5 field layout (src/setuplibceed.c:40-45)");
+    if (op->in[0].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "u and v must be active");
+    if (op->in[0].r != op->out[0].r || op->in[0].b != op->out[0].b) return plan_fail(op, "u and v must share restriction and basis");
+    CK(plan_elemop(op, op->in[0].r, op->in[0].b));
+    CK(check_qdata_rstr(op, op->in[1].r, qf->in[1].size, op->eop->Q * op->eop->Q * op->eop->Q, "qdata"));
+    if (qf->in[1].size != 10) return plan_fail(op, "mass qdata must be the 10-component volume qdata");
+    op->plan = PLAN_MASS;
+    return CEED_ERROR_SUCCESS;
+  }
   if (!strcmp(k, "SetupBoundary")) {
     /* inputs "dx" (GRAD of the face coordinates), "weight" (WEIGHT); output "surface qdata" (NONE, 10, strided) --
      * QDataBoundaryGet, src/qdata.c:228-261 */
@@ -1620,6 +1661,50 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
       CK(vec_dev_read(op->in[4].v, &jd));
       CK(vec_dev_write(out, &v, 0));
       HB_CK(ceed, hb_freestream_jacobian_apply(op->fop, op->qf->ctx->data, op->flux_type, qd, jd, dq, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_RHS: {
+      /* RHS(q) = -F(q, q_dot = 0): the IFunction kernel at zero rate, negated into the output */
+      const HbNewtonianContext *ctx = (const HbNewtonianContext *)op->qf->ctx->data;
+      const int64_t             n   = op->eop->l_size;
+      CK(need_len(op, in, n, "input"));
+      CK(need_len(op, out, n, "output"));
+      CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
+      if (ctx->idl_enable && !op->idl_coords_set) {
+        CeedVector xv = op->in[3].v;
+        if (!xv || xv == CEED_VECTOR_ACTIVE || xv == CEED_VECTOR_NONE) return plan_fail(op, "IDL needs the coordinate field 'x'");
+        CK(gather_coords(op, &op->in[3], xv, &op->eop->d_x_elem));
+        op->idl_coords_set = 1;
+      }
+      if (!op->d_zero) {
+        CUDA_CK(ceed, cudaMalloc((void **)&op->d_zero, sizeof(double) * (size_t)n));
+        CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_rhs, sizeof(double) * (size_t)n));
+        CUDA_CK(ceed, cudaMemsetAsync(op->d_zero, 0, sizeof(double) * (size_t)n, s));
+      }
+      HbIFunctionIO io;
+      memset(&io, 0, sizeof io);
+      CK(vec_dev_read(in, &io.q));
+      CK(vec_dev_read(op->in[2].v, &io.qdata));
+      io.q_dot = op->d_zero;
+      io.v     = op->d_tmp_rhs;
+      io.add   = 0;
+      HB_CK(ceed, hb_ifunction_apply(op->eop, ctx, &io, s));
+      double *v;
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_vec_axpy_f64(v, -1.0, op->d_tmp_rhs, n, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_MASS: {
+      const int64_t n = op->eop->l_size;
+      CK(need_len(op, in, n, "input"));
+      CK(need_len(op, out, n, "output"));
+      CK(need_len(op, op->in[1].v, op->in[1].r->l_size, "qdata"));
+      const double *u, *qd;
+      double       *v;
+      CK(vec_dev_read(in, &u));
+      CK(vec_dev_read(op->in[1].v, &qd));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_mass_apply(op->eop, qd, u, v, 1, s));
       return CEED_ERROR_SUCCESS;
     }
     case PLAN_IFUNCTION: {
@@ -1743,7 +1828,18 @@ static int op_diag_add_single(CeedOperator op, CeedVector assembled) {
     HB_CK(op->ceed, hb_freestream_diagonal(op->fop, op->qf->ctx->data, op->flux_type, qd, jd, y, op->ceed->stream));
     return CEED_ERROR_SUCCESS;
   }
-  if (op->plan != PLAN_IJACOBIAN) return plan_fail(op, "diagonal assembly is provided for the IJacobian operators (volume and free-stream faces)");
+  if (op->plan == PLAN_MASS) {
+    CK(need_len(op, assembled, op->eop->l_size, "diagonal"));
+    CK(need_len(op, op->in[1].v, op->in[1].r->l_size, "qdata"));
+    const double *qd;
+    double       *y;
+    CK(vec_dev_read(op->in[1].v, &qd));
+    CK(vec_dev_write(assembled, &y, 0));
+    HB_CK(op->ceed, hb_mass_diagonal(op->eop, qd, y, 1, op->ceed->stream));
+    return CEED_ERROR_SUCCESS;
+  }
+  if (op->plan != PLAN_IJACOBIAN)
+    return plan_fail(op, "diagonal assembly is provided for the IJacobian operators (volume and free-stream faces) and the mass operator");
   CK(need_len(op, assembled, op->eop->l_size, "diagonal"));
   CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
   CK(need_len(op, op->in[3].v, op->in[3].r->l_size, "jac_data"));
@@ -1812,7 +1908,8 @@ int CeedOperatorGetFlopsEstimate(CeedOperator op, CeedSize *flops) {
   if (!op->eop) return CEED_ERROR_SUCCESS;
   const CeedSize P = op->eop->P, Q = op->eop->Q, E = op->eop->num_elem, Q3 = Q * Q * Q;
   const CeedSize interp = 2 * (Q * P * P * P + Q * Q * P * P + Q * Q * Q * P), deriv = 2 * 3 * Q3 * Q;
-  if (op->plan == PLAN_IFUNCTION) *flops = E * (5 * (2 * (interp + deriv)) + 5 * interp + 700 * Q3);
+  if (op->plan == PLAN_IFUNCTION || op->plan == PLAN_RHS) *flops = E * (5 * (2 * (interp + deriv)) + 5 * interp + 700 * Q3);
+  else if (op->plan == PLAN_MASS) *flops = E * (5 * 2 * interp + 5 * Q3);
   else if (op->plan == PLAN_IJACOBIAN) *flops = E * (5 * (2 * (interp + deriv)) + 520 * Q3);
   return CEED_ERROR_SUCCESS;
 }
@@ -1844,6 +1941,8 @@ int CeedOperatorDestroy(CeedOperator *op) {
   if (o->eop) ceed_unregister_op(o->ceed, o->eop);
   hb_elemop_destroy(o->eop);
   hb_faceop_destroy(o->fop);
+  cudaFree(o->d_zero);
+  cudaFree(o->d_tmp_rhs);
   cudaFree(o->d_tmp_in32);
   cudaFree(o->d_tmp_out32);
   cudaFree(o->d_tmp_e);
@@ -1969,6 +2068,8 @@ static void op_view(CeedOperator op, FILE *stream, int terse, int depth) {
           : op->plan == PLAN_SETUP_SUR ? "surface qdata setup"
           : op->plan == PLAN_FREESTREAM ? "free-stream faces"
           : op->plan == PLAN_FREESTREAM_JAC ? "free-stream faces Jacobian"
+          : op->plan == PLAN_RHS       ? "explicit right-hand side"
+          : op->plan == PLAN_MASS      ? "mass"
                                        : "not planned");
   if (terse) return;
   for (int o = 0; o < 2; o++)

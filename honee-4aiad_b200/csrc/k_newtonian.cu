@@ -1155,6 +1155,146 @@ static int launch_diagonal(const HbElemOp *op, const HbNewtonianContext &ctx, co
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// Mass operator of the explicit path (Mass_N with N = 5, qfunctions/mass.h:19-26, on the state restriction and basis:
+// src/setuplibceed.c:15-53): v += B^T (wdetJ .* (B u)) per component, and its diagonal sum_q B_p(q)^2 wdetJ_q.
+// Memory-bound (the state read once, the output read-modify-written once, one of the ten qdata components read), so
+// one CTA per element of a colour: node-interleaved gather staged in shared memory, then the three 1D contractions per
+// direction for all five components at once, qdata read as one contiguous Q^3 block.
+constexpr int kMassThreads = 256;
+
+template <int P, int Q>
+__device__ __forceinline__ void mass_basis_to_smem(const Basis1D<double> &bas, double *sB, bool squared) {
+  for (int t = threadIdx.x; t < Q * P; t += kMassThreads) {
+    double b = 0;
+#pragma unroll
+    for (int i = 0; i < Q * P; i++)  // compile-time indices: the parameter array stays in the constant bank
+      if (i == t) b = bas.B[i];
+    sB[t] = squared ? b * b : b;
+  }
+}
+
+template <int P, int Q>
+__global__ void __launch_bounds__(kMassThreads) k_mass(const ElemArgs<double> a, const double *__restrict__ u, double *__restrict__ v) {
+  constexpr int NT = kMassThreads, P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q, P2Q = P2 * Q, PQ2 = P * Q2;
+  __shared__ double sB[Q * P];
+  __shared__ double sX[5 * Q3], sY[5 * Q3];  // ping-pong; Q >= P so Q^3 bounds every intermediate
+  mass_basis_to_smem<P, Q>(a.basis, sB, false);
+  for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
+    const int e = a.elems[idx];
+    const int32_t *off = a.offsets + (int64_t)e * P3;
+    for (int i = threadIdx.x; i < 5 * P3; i += NT) sX[(i % 5) * P3 + i / 5] = u[off[i / 5] + i % 5];
+    __syncthreads();
+    for (int f = threadIdx.x; f < 5 * P2Q; f += NT) {  // x: [c][pc][pb][qi]
+      const int qi = f % Q, pcb = (f / Q) % P2, c = f / P2Q;
+      double s = 0;
+#pragma unroll
+      for (int i = 0; i < P; i++) s += sB[qi * P + i] * sX[c * P3 + pcb * P + i];
+      sY[f] = s;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 5 * PQ2; f += NT) {  // y: [c][pc][qj][qi]
+      const int qi = f % Q, qj = (f / Q) % Q, pc = (f / Q2) % P, c = f / PQ2;
+      double s = 0;
+#pragma unroll
+      for (int j = 0; j < P; j++) s += sB[qj * P + j] * sY[c * P2Q + (pc * P + j) * Q + qi];
+      sX[f] = s;
+    }
+    __syncthreads();
+    const double *wq = a.qdata + (int64_t)e * 10 * Q3;  // component 0: w detJ
+    for (int f = threadIdx.x; f < 5 * Q3; f += NT) {  // z, times w detJ: [c][qk][qj][qi]
+      const int qji = f % Q2, qk = (f / Q2) % Q, c = f / Q3;
+      double s = 0;
+#pragma unroll
+      for (int k = 0; k < P; k++) s += sB[qk * P + k] * sX[c * PQ2 + k * Q2 + qji];
+      sY[f] = s * __ldg(wq + qk * Q2 + qji);
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 5 * PQ2; f += NT) {  // z^T: [c][pc][qj][qi]
+      const int qji = f % Q2, pc = (f / Q2) % P, c = f / PQ2;
+      double s = 0;
+#pragma unroll
+      for (int k = 0; k < Q; k++) s += sB[k * P + pc] * sY[c * Q3 + k * Q2 + qji];
+      sX[f] = s;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 5 * P2Q; f += NT) {  // y^T: [c][pc][pb][qi]
+      const int qi = f % Q, pb = (f / Q) % P, pc = (f / (Q * P)) % P, c = f / P2Q;
+      double s = 0;
+#pragma unroll
+      for (int j = 0; j < Q; j++) s += sB[j * P + pb] * sX[c * PQ2 + (pc * Q + j) * Q + qi];
+      sY[f] = s;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 5 * P3; f += NT) {  // x^T and the scatter, components fastest (node-interleaved)
+      const int c = f % 5, p = f / 5, pa = p % P, pcb = p / P;
+      double s = 0;
+#pragma unroll
+      for (int i = 0; i < Q; i++) s += sB[i * P + pa] * sY[c * P2Q + pcb * Q + i];
+      v[off[p] + c] += s;
+    }
+    // the next gather writes sX, last read before the barrier above; the x^T pass reads sY, next written after a barrier
+  }
+}
+
+template <int P, int Q>
+__global__ void __launch_bounds__(kMassThreads) k_mass_diag(const ElemArgs<double> a, double *__restrict__ diag) {
+  constexpr int NT = kMassThreads, P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q;
+  __shared__ double sW[Q * P];  // B^2
+  __shared__ double sX[Q3], sY[Q3];
+  mass_basis_to_smem<P, Q>(a.basis, sW, true);
+  for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
+    const int e = a.elems[idx];
+    const double *wq = a.qdata + (int64_t)e * 10 * Q3;
+    for (int q = threadIdx.x; q < Q3; q += NT) sX[q] = __ldg(wq + q);
+    __syncthreads();
+    for (int f = threadIdx.x; f < P * Q2; f += NT) {  // [pc][qj][qi]
+      const int qji = f % Q2, pc = f / Q2;
+      double s = 0;
+#pragma unroll
+      for (int k = 0; k < Q; k++) s += sW[k * P + pc] * sX[k * Q2 + qji];
+      sY[f] = s;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < P2 * Q; f += NT) {  // [pc][pb][qi]
+      const int qi = f % Q, pb = (f / Q) % P, pc = f / (Q * P);
+      double s = 0;
+#pragma unroll
+      for (int j = 0; j < Q; j++) s += sW[j * P + pb] * sY[(pc * Q + j) * Q + qi];
+      sX[f] = s;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 5 * P3; f += NT) {
+      const int c = f % 5, p = f / 5, pa = p % P, pcb = p / P;
+      double s = 0;
+#pragma unroll
+      for (int i = 0; i < Q; i++) s += sW[i * P + pa] * sX[pcb * Q + i];
+      diag[a.offsets[(int64_t)e * P3 + p] + c] += s;
+    }
+    __syncthreads();
+  }
+}
+
+template <int P, int Q>
+static int launch_mass(const HbElemOp *op, const double *qdata, const double *u, double *v, bool diagonal, cudaStream_t s) {
+  for (int c = 0; c < op->num_colors; c++) {
+    ElemArgs<double> a;
+    memset(&a, 0, sizeof a);
+    a.offsets = op->d_offsets;
+    a.elems = op->d_color_elem + op->h_color_ptr[c];
+    a.n_elems = op->h_color_ptr[c + 1] - op->h_color_ptr[c];
+    fill_basis<double>(op, a.basis);
+    a.qdata = qdata;
+    a.status = op->d_status;
+    if (a.n_elems == 0) continue;
+    if (diagonal)
+      k_mass_diag<P, Q><<<grid_for(op, a.n_elems, k_mass_diag<P, Q>, kMassThreads, 0), kMassThreads, 0, s>>>(a, v);
+    else
+      k_mass<P, Q><<<grid_for(op, a.n_elems, k_mass<P, Q>, kMassThreads, 0), kMassThreads, 0, s>>>(a, u, v);
+  }
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+
 // (P, Q) pairs compiled: polynomial degree 1..5 with q_extra 0 or 1 (Q = P or P + 1); the benchmark configurations use
 // (3,3), (4,5) and (5,6).
 #define HB_PQ_LIST(X) X(2, 2) X(2, 3) X(3, 3) X(3, 4) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7)
@@ -1315,3 +1455,29 @@ extern "C" HB_EXPORT int hb_debug_phase_cycles(unsigned long long *out, int rese
   return HB_SUCCESS;
 }
 #endif
+
+extern "C" int hb_mass_apply(const HbElemOp *op, const double *qdata, const double *u, double *v, int add, void *stream) {
+  int err = check_op(op);
+  if (err) return err;
+  if (!qdata || !u || !v) return HB_ERROR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!add && cudaMemsetAsync(v, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_mass<PP, QQ>(op, qdata, u, v, false, s);
+  HB_PQ_LIST(HB_CASE)
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+
+extern "C" int hb_mass_diagonal(const HbElemOp *op, const double *qdata, double *diag, int add, void *stream) {
+  int err = check_op(op);
+  if (err) return err;
+  if (!qdata || !diag) return HB_ERROR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!add && cudaMemsetAsync(diag, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_mass<PP, QQ>(op, qdata, NULL, diag, true, s);
+  HB_PQ_LIST(HB_CASE)
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}

@@ -121,6 +121,43 @@ class NewtonianOperators:
         self.op_ifunction_volume, self.op_ijacobian_volume = op_if, op_ij
         self.boundaries = []
 
+    # ---- explicit path (src/setuplibceed.c:179-205 for the RHS operator, :15-53 for the mass operator of CreateKSPMass)
+    def add_explicit(self):
+        """The RHSFunction_Newtonian volume operator (fields q, Grad_q, qdata, x -> v, Grad_v) in an "RHS" composite and the
+        Mass_5 operator on the state fields, as SetupLibceed builds them for -ts_type rk."""
+        ceed = self.ceed
+        qf_rhs = ce.QFunction(ceed, "newtonian.h:RHSFunction_Newtonian")
+        for name, size, mode in (("q", 5, ce.CEED_EVAL_INTERP), ("Grad_q", 15, ce.CEED_EVAL_GRAD), ("qdata", 10, ce.CEED_EVAL_NONE),
+                                 ("x", 3, ce.CEED_EVAL_INTERP)):
+            qf_rhs.add_input(name, size, mode)
+        qf_rhs.add_output("v", 5, ce.CEED_EVAL_INTERP)
+        qf_rhs.add_output("Grad_v", 15, ce.CEED_EVAL_GRAD)
+        qf_rhs.set_context(self.qfctx)
+        op_rhs_vol = ce.Operator(ceed, qf_rhs)
+        op_rhs_vol.set_field("q", self.rstr_q, self.basis_q, ceed.active)
+        op_rhs_vol.set_field("Grad_q", self.rstr_q, self.basis_q, ceed.active)
+        op_rhs_vol.set_field("qdata", self.rstr_qd, ceed.basis_none, self.q_data)
+        op_rhs_vol.set_field("x", self.rstr_x, self.basis_x, self.x_coord)
+        op_rhs_vol.set_field("v", self.rstr_q, self.basis_q, ceed.active)
+        op_rhs_vol.set_field("Grad_v", self.rstr_q, self.basis_q, ceed.active)
+        self.op_rhs = ce.Operator(ceed)
+        self.op_rhs.set_name("RHS Composite Operator")
+        self.op_rhs.add_sub(op_rhs_vol)
+        qf_mass = ce.QFunction(ceed, "mass.h:Mass_5")
+        qf_mass.add_input("u", 5, ce.CEED_EVAL_INTERP)
+        qf_mass.add_input("qdata", 10, ce.CEED_EVAL_NONE)
+        qf_mass.add_output("v", 5, ce.CEED_EVAL_INTERP)
+        self.op_mass = ce.Operator(ceed, qf_mass)
+        self.op_mass.set_name("RHS Mass Operator")
+        self.op_mass.set_field("u", self.rstr_q, self.basis_q, ceed.active)
+        self.op_mass.set_field("qdata", self.rstr_qd, ceed.basis_none, self.q_data)
+        self.op_mass.set_field("v", self.rstr_q, self.basis_q, ceed.active)
+        self._explicit = (op_rhs_vol, qf_rhs, qf_mass)
+
+    def rhs(self, q: ce.Vector, g: ce.Vector):
+        """R = RHS(q) before the mass solve (ApplyCeedOperatorLocalToGlobal in RHS_NS, src/setupts.c:50)."""
+        self.op_rhs.apply(q, g)
+
     # ---- boundary faces
     def add_freestream(self, P_inf, u_inf, T_inf, *, riemann="hllc", sides=None, implicit=True):
         """Free-stream condition on the non-periodic box sides: face restriction and 2D basis of the state, the bilinear

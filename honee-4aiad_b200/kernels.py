@@ -114,6 +114,14 @@ class ElemOp:
         _chk(fn(self.ptr, cb, _addr(qdata), _addr(jac_data), _addr(diag), int(add), _stream(stream)), "hb_diagonal_assemble")
 
 
+    def mass(self, qdata, u, v, add=False, stream=None):
+        """v (+)= M u, the Mass_5 operator of the explicit path."""
+        _chk(_load().hb_mass_apply(self.ptr, _addr(qdata), _addr(u), _addr(v), int(add), _stream(stream)), "hb_mass_apply")
+
+    def mass_diagonal(self, qdata, diag, add=False, stream=None):
+        _chk(_load().hb_mass_diagonal(self.ptr, _addr(qdata), _addr(diag), int(add), _stream(stream)), "hb_mass_diagonal")
+
+
 class HbFaceOp(C.Structure):
     _fields_ = [("num_faces", C.c_int), ("P", C.c_int), ("Q", C.c_int), ("l_size", C.c_int64), ("d_offsets", C.c_void_p), ("num_colors", C.c_int),
                 ("h_color_ptr", C.POINTER(C.c_int32)), ("d_color_elem", C.c_void_p), ("interp1d", C.c_double * 64), ("grad1d", C.c_double * 64),

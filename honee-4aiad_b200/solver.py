@@ -104,6 +104,100 @@ class TimeStepper:
             pass
 
 
+# ---- explicit time loop (hb_explicit_*): HONEE's -ts_type rk path, RHS_NS with the mass KSP (src/setupts.c:31-75)
+RK_MAX_STAGES = 6
+
+# PETSc TSRK tableaux by -ts_rk_type name: (A, b, c), published Butcher tables
+RK_TABLEAUX = {
+    "1fe": ([[0.0]], [1.0], [0.0]),
+    "2a": ([[0, 0], [1.0, 0]], [0.5, 0.5], [0, 1.0]),
+    "3": ([[0, 0, 0], [0.5, 0, 0], [-1.0, 2.0, 0]], [1 / 6, 2 / 3, 1 / 6], [0, 0.5, 1.0]),
+    "3bs": ([[0, 0, 0, 0], [0.5, 0, 0, 0], [0, 0.75, 0, 0], [2 / 9, 1 / 3, 4 / 9, 0]], [2 / 9, 1 / 3, 4 / 9, 0], [0, 0.5, 0.75, 1.0]),
+    "4": ([[0, 0, 0, 0], [0.5, 0, 0, 0], [0, 0.5, 0, 0], [0, 0, 1.0, 0]], [1 / 6, 1 / 3, 1 / 3, 1 / 6], [0, 0.5, 0.5, 1.0]),
+}
+
+
+class HbExplicitOptions(C.Structure):
+    _fields_ = [("dt", C.c_double), ("rk_stages", C.c_int), ("rk_a", C.c_double * (RK_MAX_STAGES * RK_MAX_STAGES)),
+                ("rk_b", C.c_double * RK_MAX_STAGES), ("rk_c", C.c_double * RK_MAX_STAGES), ("mass_ksp", C.c_int),
+                ("mass_pc_rowsum", C.c_int), ("mass_rtol", C.c_double), ("mass_atol", C.c_double), ("mass_max_it", C.c_int),
+                ("mass_restart", C.c_int)]
+
+
+class HbExplicitStats(C.Structure):
+    _fields_ = [("mass_its", C.c_int), ("converged_reason", C.c_int), ("seconds", C.c_double)]
+
+
+def explicit_options(*, dt, rk_type="4", mass_ksp="preonly", pc_jacobi="rowsum", rtol=1e-5, atol=1e-50, max_it=10000,
+                     restart=30) -> HbExplicitOptions:
+    """Options in HONEE's vocabulary: -ts_rk_type, -mass_ksp_type preonly|gmres, -mass_pc_jacobi_type rowsum|diagonal."""
+    o = HbExplicitOptions()
+    _load().hb_explicit_default_options(C.byref(o))
+    A, b, c = RK_TABLEAUX[rk_type]
+    o.dt = dt
+    o.rk_stages = len(b)
+    for i in range(RK_MAX_STAGES * RK_MAX_STAGES):
+        o.rk_a[i] = 0.0
+    for i, row in enumerate(A):
+        for j, a in enumerate(row):
+            o.rk_a[i * RK_MAX_STAGES + j] = a
+    for i in range(RK_MAX_STAGES):
+        o.rk_b[i] = b[i] if i < len(b) else 0.0
+        o.rk_c[i] = c[i] if i < len(c) else 0.0
+    o.mass_ksp = {"preonly": 0, "gmres": 1}[mass_ksp]
+    o.mass_pc_rowsum = {"rowsum": 1, "diagonal": 0}[pc_jacobi]
+    o.mass_rtol, o.mass_atol, o.mass_max_it, o.mass_restart = rtol, atol, max_it, restart
+    return o
+
+
+@dataclass
+class ExplicitStats:
+    mass_its: int
+    converged_reason: int
+    seconds: float
+
+
+class ExplicitStepper:
+    """Explicit RK time stepper over one ElemOp: q_{n+1} from the tableau with G = M^-1 RHS(q) (RHS_NS)."""
+
+    def __init__(self, elemop, ctx_bytes: bytes, qdata, options: HbExplicitOptions | None = None, stream=None, **kw):
+        L = _load()
+        self.options = options if options is not None else explicit_options(**kw)
+        self._ctx = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        self._op = elemop
+        self._stream = _stream(stream)
+        self.ptr = C.c_void_p()
+        _chk(L.hb_explicit_create(elemop.ptr, self._ctx, _addr(qdata), C.byref(self.options), self._stream, C.byref(self.ptr)),
+             "hb_explicit_create")
+
+    def set_state(self, q, t=0.0):
+        _chk(_load().hb_explicit_set_state(self.ptr, _addr(q), C.c_double(t)), "hb_explicit_set_state")
+
+    def get_state(self, q) -> float:
+        t = C.c_double()
+        _chk(_load().hb_explicit_get_state(self.ptr, _addr(q), C.byref(t)), "hb_explicit_get_state")
+        return t.value
+
+    def rhs(self, q, g, t=0.0) -> tuple[int, int]:
+        """g = M^-1 RHS(q) at time t; returns (mass-solve iterations, converged reason)."""
+        its, reason = C.c_int(), C.c_int()
+        _chk(_load().hb_explicit_rhs(self.ptr, _addr(q), C.c_double(t), _addr(g), C.byref(its), C.byref(reason)), "hb_explicit_rhs")
+        return its.value, reason.value
+
+    def step(self) -> ExplicitStats:
+        s = HbExplicitStats()
+        _chk(_load().hb_explicit_step(self.ptr, C.byref(s)), "hb_explicit_step")
+        return ExplicitStats(s.mass_its, s.converged_reason, s.seconds)
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                _load().hb_explicit_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+
 def monitor_ke(elemop, ctx_bytes: bytes, q, qdata, scratch, stream=None) -> np.ndarray:
     """Kinetic-energy integrand sums (TotalKineticEnergy, StrainDissipation, DivergenceDissipation, VolumeExpansion,
     MuVorticity2), not yet divided by the domain volume.  scratch: >= 5 * num_elem doubles on the device."""

@@ -171,6 +171,49 @@ HB_EXPORT int hb_ts_step(HbTimeStepper *ts, HbStepStats *stats);
 HB_EXPORT const void *hb_ts_context(HbTimeStepper *ts);
 HB_EXPORT int hb_ts_destroy(HbTimeStepper *ts);
 
+/* ---- Explicit time loop (HONEE's -ts_type rk path: RHS_NS, src/setupts.c:31-75, with the mass-matrix KSP of
+ *      CreateKSPMass, src/setuplibceed.c:15-93; PETSc TSRK and KSP restated here) ---- */
+
+/* Mass operator (Mass_N, N = 5: qfunctions/mass.h:19-26) on the state restriction and basis: v (+)= M u, and its
+ * diagonal (what MatGetDiagonal_Ceed gives PCJacobi "diagonal"; the row sums of PCJacobi "rowsum" are M applied to ones). */
+HB_EXPORT int hb_mass_apply(const HbElemOp *op, const double *qdata, const double *u, double *v, int add, void *stream);
+HB_EXPORT int hb_mass_diagonal(const HbElemOp *op, const double *qdata, double *diag, int add, void *stream);
+
+#define HB_RK_MAX_STAGES 6
+typedef struct {
+  double dt;
+  /* explicit Butcher tableau (TSRK): stages s <= HB_RK_MAX_STAGES, a row-major s x s (strictly lower), b, c */
+  int    rk_stages;
+  double rk_a[HB_RK_MAX_STAGES * HB_RK_MAX_STAGES], rk_b[HB_RK_MAX_STAGES], rk_c[HB_RK_MAX_STAGES];
+  /* mass solve: 0 = "lumped" (KSPPREONLY + PCJacobi row sum, HONEE's default, src/setuplibceed.c:81-87),
+   *             1 = KSPGMRES, left-preconditioned by PCJacobi, preconditioned residual norm (PETSc's GMRES defaults) */
+  int    mass_ksp;
+  int    mass_pc_rowsum; /* Jacobi from the row sums (1) or from the diagonal (0, -mass_pc_jacobi_type diagonal) */
+  double mass_rtol, mass_atol;
+  int    mass_max_it, mass_restart;
+} HbExplicitOptions;
+
+typedef struct {
+  int    mass_its;        /* Krylov iterations of the step's mass solves (0 when lumped) */
+  int    converged_reason; /* 1 every mass solve converged, -1 non-finite, -2 iteration limit */
+  double seconds;
+} HbExplicitStats;
+
+typedef struct HbExplicitStepper HbExplicitStepper;
+
+/* Classical 4-stage RK (TSRK4), lumped mass, PETSc's KSP defaults (rtol 1e-5, atol 1e-50, 10000 its, restart 30). */
+HB_EXPORT void hb_explicit_default_options(HbExplicitOptions *o);
+/* ctx184 is copied; "timestep size" and "solution time" are set per stage like RHS_NS does (src/setupts.c:40-46). */
+HB_EXPORT int hb_explicit_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, const HbExplicitOptions *opts, void *stream,
+                                 HbExplicitStepper **ex);
+HB_EXPORT int hb_explicit_set_state(HbExplicitStepper *ex, const double *d_q, double t);
+HB_EXPORT int hb_explicit_get_state(HbExplicitStepper *ex, double *d_q, double *t);
+/* G = M^-1 RHS(q) with RHS = RHSFunction_Newtonian (qfunctions/newtonian.h:133-202), the explicit right-hand side of
+ * one call of RHS_NS; *its receives the mass-solve iterations and *converged_reason 1, -1 or -2 (either may be NULL). */
+HB_EXPORT int hb_explicit_rhs(HbExplicitStepper *ex, const double *d_q, double t, double *d_g, int *its, int *converged_reason);
+HB_EXPORT int hb_explicit_step(HbExplicitStepper *ex, HbExplicitStats *stats);
+HB_EXPORT int hb_explicit_destroy(HbExplicitStepper *ex);
+
 /* Krylov block operations (FP64 accumulation): out[i] = V_i . w for i < k (d_partial: 512*HB_GMRES_MAX_BASIS doubles),
  * w += sum_i c_i V_i */
 HB_EXPORT int hb_krylov_multidot_f64(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_partial, double *d_out, void *s);

@@ -987,6 +987,79 @@ static void linear_basis(int Q, double *Bx, double *Gx, double *w) {
   }
 }
 
+/* ---- explicit path: RHSFunction_Newtonian (qfunctions/newtonian.h:133-202) and Mass_N (qfunctions/mass.h:19-26) ---- */
+/* The IFunction integrand (newtonian.h:205-257) at q_dot = 0 is v = -wdetJ body (+ the damping-layer residual) and
+ * grad v = wdetJ dXdx (-F_total + stab) with the SUPG strong residual evaluated at U_dot = 0, which is exactly the negative
+ * of the RHS integrand (v = wdetJ body - damping, grad v = wdetJ dXdx (F_total - stab), U_dot = 0). */
+int oracle_qf_rhs_conserv(void *ctx, int Q, const double *const *in, double *const *out) {
+  double *zero = (double *)calloc((size_t)5 * Q, sizeof(double)), *jd = (double *)malloc(sizeof(double) * HB_JAC_DATA_COMPS_IDL * Q);
+  if (!zero || !jd) {
+    free(zero);
+    free(jd);
+    return 1;
+  }
+  const double *in_if[5]  = {in[0], in[1], zero, in[2], in[3]};
+  double       *out_if[3] = {out[0], out[1], jd};
+  const int     err       = oracle_qf_ifunction_conserv(ctx, Q, in_if, out_if);
+  for (int i = 0; i < 5 * Q; i++) out[0][i] = -out[0][i];
+  for (int i = 0; i < 15 * Q; i++) out[1][i] = -out[1][i];
+  free(zero);
+  free(jd);
+  return err;
+}
+
+static void rhs_elem(const OracleMesh *m, int64_t e, void *user, double *s, int *err) {
+  ApplyArgs *a  = (ApplyArgs *)user;
+  const int  P3 = m->P * m->P * m->P, Q3 = m->Q * m->Q * m->Q;
+  double *ue = s, *qi = ue + 5 * P3, *gq = qi + 5 * Q3, *v = gq + 15 * Q3 + 5 * Q3, *gv = v + 5 * Q3, *ve = gv + 15 * Q3;
+  double *xz = ve + 5 * P3;
+  elem_eval(m, e, a->q, ue, qi, gq);
+  if (!a->x_q) memset(xz, 0, sizeof(double) * 3 * Q3);
+  const double *in[4]  = {qi, gq, a->qdata + e * 10 * Q3, a->x_q ? a->x_q + e * 3 * Q3 : xz};
+  double       *out[2] = {v, gv};
+  if (a->qf(a->ctx, Q3, in, out)) *err = 1;
+  elem_scatter(m, e, v, gv, ve, a->v);
+}
+
+int oracle_apply_rhs(const OracleMesh *m, OracleQF qf, void *ctx, const double *q, const double *qdata, const double *x_q, double *v,
+                     int64_t l_size) {
+  ApplyArgs a = {qf, ctx, q, NULL, qdata, x_q, NULL, NULL, v, 14};
+  int       err = 0;
+  memset(v, 0, sizeof(double) * l_size);
+  for_each_elem(m, rhs_elem, &a, apply_scratch(m), &err);
+  return err;
+}
+
+int oracle_qf_mass(void *ctx, int Q, const double *const *in, double *const *out) {
+  (void)ctx;
+  for (int j = 0; j < 5; j++)
+    for (int i = 0; i < Q; i++) out[0][j * Q + i] = in[1][i] * in[0][j * Q + i];
+  return 0;
+}
+
+static void mass_elem(const OracleMesh *m, int64_t e, void *user, double *s, int *err) {
+  ApplyArgs    *a = (ApplyArgs *)user;
+  const int     P = m->P, Q = m->Q, P3 = P * P * P, Q3 = Q * Q * Q;
+  const double *B = m->interp1d;
+  double *ue = s, *ui = ue + 5 * P3, *v = ui + 5 * Q3, *ve = v + 5 * Q3;
+  elem_eval(m, e, a->q, ue, ui, NULL);
+  const double *in[2]  = {ui, a->qdata + e * 10 * Q3};
+  double       *out[1] = {v};
+  if (a->qf(NULL, Q3, in, out)) *err = 1;
+  memset(ve, 0, sizeof(double) * 5 * P3);
+  for (int c = 0; c < 5; c++) tensor_apply_t(P, Q, B, B, B, &v[c * Q3], &ve[c * P3]);
+  for (int c = 0; c < 5; c++)
+    for (int p = 0; p < P3; p++) a->v[m->offsets[e * P3 + p] + c] += ve[c * P3 + p];
+}
+
+int oracle_apply_mass(const OracleMesh *m, OracleQF qf, const double *u, const double *qdata, double *v, int64_t l_size) {
+  ApplyArgs a = {qf, NULL, u, NULL, qdata, NULL, NULL, NULL, v, 0};
+  int       err = 0;
+  memset(v, 0, sizeof(double) * l_size);
+  for_each_elem(m, mass_elem, &a, apply_scratch(m), &err);
+  return err;
+}
+
 int oracle_setup_qdata(int num_elem, int Q, const double *x_elem, double *qdata) {
   const int Q3 = Q * Q * Q;
   double    B[32], G[32], w1[16];

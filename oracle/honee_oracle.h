@@ -92,6 +92,18 @@ int oracle_apply_ijacobian(const OracleMesh *m, OracleQF qf, void *ctx, const do
  * QFunction at each quadrature point with unit inputs, then contract with the squared basis rows. diag overwritten. */
 int oracle_assemble_diagonal(const OracleMesh *m, OracleQF qf, void *ctx, const double *qdata, const double *jac_data, int num_jd,
                              double *diag, int64_t l_size);
+/* Explicit path.  RHSFunction_Newtonian (qfunctions/newtonian.h:133-202) applied as an operator: inputs q (INTERP),
+ * Grad_q (GRAD), qdata, x; outputs v (INTERP) and Grad_v (GRAD) (src/setuplibceed.c:179-205).  v is overwritten. */
+int oracle_apply_rhs(const OracleMesh *m, OracleQF qf, void *ctx, const double *q, const double *qdata, const double *x_q, double *v,
+                     int64_t l_size);
+/* The restatement of RHSFunction_Newtonian: the IFunction integrand at q_dot = 0 with the sign reversed (same in/out
+ * layout as the reference QFunction). */
+int oracle_qf_rhs_conserv(void *ctx, int Q, const double *const *in, double *const *out);
+/* Mass operator (Mass_N, N = 5, qfunctions/mass.h:19-26; src/setuplibceed.c:15-53): v = M u through the QFunction qf
+ * (in: u [5][Q], qdata [10][Q]; out: v [5][Q]) -- oracle_qf_mass or the reference's Mass_5.  v is overwritten. */
+int oracle_apply_mass(const OracleMesh *m, OracleQF qf, const double *u, const double *qdata, double *v, int64_t l_size);
+int oracle_qf_mass(void *ctx, int Q, const double *const *in, double *const *out);
+
 /* Geometric factors: qdata [elem][10][Q^3] from vertex coordinates x_elem [elem][3][8] (P=2 linear coordinate basis
  * with the same Gauss rule; src/qdata.c:133-190, qfunctions/setupgeo.h:42-56). */
 int oracle_setup_qdata(int num_elem, int Q, const double *x_elem, double *qdata);

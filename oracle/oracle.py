@@ -59,6 +59,10 @@ def _declare(L):
                  "oracle_qf_setup", "oracle_qf_monitor_ke_conserv", "oracle_qf_ics_taylorgreen"):
         getattr(L, name).restype = C.c_int
     L.oracle_apply_ifunction.restype = C.c_int
+    L.oracle_apply_rhs.restype = C.c_int
+    L.oracle_apply_mass.restype = C.c_int
+    L.oracle_qf_rhs_conserv.restype = C.c_int
+    L.oracle_qf_mass.restype = C.c_int
     L.oracle_apply_ijacobian.restype = C.c_int
     L.oracle_assemble_diagonal.restype = C.c_int
     L.oracle_box_num_nodes.restype = C.c_int64
@@ -156,6 +160,27 @@ def assemble_diagonal(mesh: Mesh, ctx: bytes, qdata, jac_data, l_size, num_jd=14
     if err:
         raise RuntimeError("oracle diagonal failed")
     return d
+
+
+def apply_rhs(mesh: Mesh, ctx: bytes, q, qdata, x_q=None, use_ref=False):
+    """RHSFunction_Newtonian as an operator (restatement, or the reference QFunction with use_ref)."""
+    L = lib()
+    fn = qf("ref_RHSFunction_Newtonian" if use_ref else "oracle_qf_rhs_conserv", use_ref)
+    v = np.zeros_like(q)
+    cbuf = C.create_string_buffer(bytes(ctx), len(ctx))
+    if L.oracle_apply_rhs(C.byref(mesh.c), fn, cbuf, ptr(q), ptr(qdata), ptr(x_q), ptr(v), C.c_int64(v.size)):
+        raise RuntimeError("oracle RHS failed")
+    return v
+
+
+def apply_mass(mesh: Mesh, u, qdata, use_ref=False):
+    """v = M u with the Mass_5 QFunction (restatement, or the reference's with use_ref)."""
+    L = lib()
+    fn = qf("ref_Mass_5" if use_ref else "oracle_qf_mass", use_ref)
+    v = np.zeros_like(u)
+    if L.oracle_apply_mass(C.byref(mesh.c), fn, ptr(u), ptr(qdata), ptr(v), C.c_int64(v.size)):
+        raise RuntimeError("oracle mass failed")
+    return v
 
 
 def setup_qdata(num_elem, Q, x_elem):

@@ -11,6 +11,7 @@
 #include "bc_freestream.h"
 #include "differential_filter.h"
 #include "grid_anisotropy_tensor.h"
+#include "mass.h"
 #include "monitor_totalkineticenergy.h"
 #include "newtonian.h"
 #include "setupgeo.h"
@@ -30,6 +31,8 @@ EXPORT int ref_IJacobian_Newtonian_Conserv(void *c, CeedInt Q, In in, Out out) {
 EXPORT int ref_IJacobian_Newtonian_Prim(void *c, CeedInt Q, In in, Out out) { return IJacobian_Newtonian_Prim(c, Q, in, out); }
 EXPORT int ref_IJacobian_Newtonian_Entropy(void *c, CeedInt Q, In in, Out out) { return IJacobian_Newtonian_Entropy(c, Q, in, out); }
 EXPORT int ref_Setup(void *c, CeedInt Q, In in, Out out) { return Setup(c, Q, in, out); }
+EXPORT int ref_RHSFunction_Newtonian(void *c, CeedInt Q, In in, Out out) { return RHSFunction_Newtonian(c, Q, in, out); }
+EXPORT int ref_Mass_5(void *c, CeedInt Q, In in, Out out) { return Mass_5(c, Q, in, out); }
 EXPORT int ref_MonitorTotalKineticEnergy_Conserv(void *c, CeedInt Q, In in, Out out) { return MonitorTotalKineticEnergy_Conserv(c, Q, in, out); }
 EXPORT int ref_ICsTaylorGreen(void *c, CeedInt Q, In in, Out out) { return ICsTaylorGreen(c, Q, in, out); }
 

@@ -10,6 +10,10 @@ Outputs (committed; the GPU box has no reference tree):
                             it (examples/navierstokes.c:222, examples/taylor_green_vortex.yaml)
   unit_state.json           the UnitTests_Newtonian inputs and tolerances (problems/newtonian.c:947-987) with the
                             reference's StateToQ outputs for every (A, B) pair
+  taylorgreen_rk4.npz       every row of tests/output/taylorgreen_totalke.csv (steps 0, 2, 3 of the explicit RK4 run of
+                            examples/navierstokes.c:222) and the final state of that run, tests/output/taylor-green.bin
+                            (HONEE binary format, src/honee-file.c:194-217: int32 token, int32 step, float64 time, then a
+                            PETSc Vec: int32 class id, int32 length, big-endian float64 values in DMPlex order)
 """
 from __future__ import annotations
 
@@ -112,6 +116,20 @@ def main():
                    periodic=True, reference_velocity=[1, 0, 0], reference_temperature=0.2490535963, reference_pressure=71.42857143,
                    mu=0.000625, k=0.8836267606, cv=717, cp=1003.8, csv_rtol=1e-9, csv_ztol=3e-10))
     json.dump(ke, open(os.path.join(HERE, "taylorgreen_ke_step0.json"), "w"), indent=1)
+
+    # ---- Taylor-Green explicit RK4 run: every KE row and the final state (tests/output/taylor-green.bin)
+    names = header[2:]
+    table = np.array([[float(v) for v in r] for r in rows[1:]])
+    raw = open(os.path.join(args.ref, "tests/output/taylor-green.bin"), "rb").read()
+    token, step = np.frombuffer(raw[:8], dtype=">i4")
+    t_final = np.frombuffer(raw[8:16], dtype=">f8")[0]
+    classid, length = np.frombuffer(raw[16:24], dtype=">i4")
+    state = np.frombuffer(raw[24:24 + 8 * int(length)], dtype=">f8").astype(np.float64)
+    assert len(raw) == 24 + 8 * int(length) and int(token) == 0x0CEEDF32 and int(classid) == 1211214
+    np.savez_compressed(os.path.join(HERE, "taylorgreen_rk4.npz"), ke_steps=table[:, 0].astype(np.int64), ke_times=table[:, 1],
+                        ke=table[:, 2:], ke_names=np.array(names), final_step=np.int64(step), final_time=np.float64(t_final),
+                        final_state=state, dt=np.float64(2e-3), tableau=np.array("4"), mass_ksp=np.array("gmres"),
+                        mass_pc_jacobi=np.array("diagonal"), source=np.array("tests/output/taylorgreen_totalke.csv, tests/output/taylor-green.bin"))
 
     # ---- UnitTests_Newtonian inputs (problems/newtonian.c:947-987) and reference StateToQ outputs
     ctx = prob.newtonian_context(2)
