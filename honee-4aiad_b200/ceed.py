@@ -297,6 +297,21 @@ class Operator(_Obj):
     def assemble_diagonal(self, out: Vector):
         self.ceed.chk(L().CeedOperatorLinearAssembleDiagonal(self.ptr, out.ptr, self.ceed.request_immediate))
 
+    def assemble_point_block_diagonal(self, out: Vector):
+        self.ceed.chk(L().CeedOperatorLinearAssemblePointBlockDiagonal(self.ptr, out.ptr, self.ceed.request_immediate))
+
+    def point_block_symbolic(self):
+        """(rows, cols) of CeedOperatorLinearAssemblePointBlockDiagonalSymbolic as numpy arrays (the C arrays are freed)."""
+        n = C.c_int64()
+        rows, cols = C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)()
+        self.ceed.chk(L().CeedOperatorLinearAssemblePointBlockDiagonalSymbolic(self.ptr, C.byref(n), C.byref(rows), C.byref(cols)))
+        r = np.ctypeslib.as_array(rows, shape=(n.value,)).copy()
+        c = np.ctypeslib.as_array(cols, shape=(n.value,)).copy()
+        libc = C.CDLL(None)
+        libc.free(C.cast(rows, C.c_void_p))
+        libc.free(C.cast(cols, C.c_void_p))
+        return r, c
+
     def context_label(self, name):
         lab = _vp()
         self.ceed.chk(L().CeedOperatorGetContextFieldLabel(self.ptr, name.encode(), C.byref(lab)))

@@ -138,6 +138,7 @@ struct CeedOperator_private {
   double   *d_tmp_e;                  /* coordinate E-vector for the Setup operator */
   HbFaceOp *fop;                      /* boundary-face sub-operators */
   double   *d_zero, *d_tmp_rhs;       /* explicit right-hand side: zero rate and the residual it is negated from */
+  float    *d_tmp_pb32;               /* mixed-precision point blocks before they are widened into the FP64 output */
   int       flux_type;                /* 0 HLL, 1 HLLC */
 };
 
@@ -1254,6 +1255,8 @@ int CeedOperatorSetField(CeedOperator op, const char *field_name, CeedElemRestri
   cudaFree(op->d_tmp_in32);
   cudaFree(op->d_tmp_out32);
   cudaFree(op->d_tmp_e);
+  cudaFree(op->d_tmp_pb32);
+  op->d_tmp_pb32 = NULL;
   op->d_zero = op->d_tmp_rhs = op->d_tmp_e = NULL;
   op->d_tmp_in32 = op->d_tmp_out32 = NULL;
   return CEED_ERROR_SUCCESS;
@@ -1943,6 +1946,7 @@ int CeedOperatorDestroy(CeedOperator *op) {
   hb_faceop_destroy(o->fop);
   cudaFree(o->d_zero);
   cudaFree(o->d_tmp_rhs);
+  cudaFree(o->d_tmp_pb32);
   cudaFree(o->d_tmp_in32);
   cudaFree(o->d_tmp_out32);
   cudaFree(o->d_tmp_e);
@@ -2106,13 +2110,114 @@ int CeedOperatorLinearAssembleGetNumEntries(CeedOperator op, CeedSize *num_entri
   (void)num_entries;
   return ASSEMBLY_UNSUPPORTED(op);
 }
-int CeedOperatorLinearAssemblePointBlockDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request) {
-  (void)assembled, (void)request;
-  return ASSEMBLY_UNSUPPORTED(op);
+/* Point-block diagonal (MatCEED's COO assembly for PCVPBJACOBI, src/mat-ceed.c:76-153): per node of the active
+ * node-interleaved L-vector a row-major 5 x 5 block [component out][component in]; values[(node * 5 + i) * 5 + j].  The
+ * symbolic call returns the matching COO rows/cols (malloc'd; the caller frees them with free(), as HONEE's
+ * IntArrayCeedToPetsc does). */
+static int pb_rstr(CeedOperator op, CeedElemRestriction *r) {
+  CeedOperator o = op;
+  while (o->composite) {
+    if (o->nsub < 1) return CeedError(op->ceed, CEED_ERROR_INCOMPLETE, "composite operator '%s' has no sub-operators", op->name);
+    o = o->subs[0];
+  }
+  *r = op_active_rstr(o, 0);
+  if (!*r || (*r)->num_comp != 5 || (*r)->comp_stride != 1 || (*r)->strided)
+    return CeedError(op->ceed, CEED_ERROR_UNSUPPORTED, "point blocks need the 5-component node-interleaved active restriction");
+  return CEED_ERROR_SUCCESS;
 }
+
+static int op_pbdiag_add_single(CeedOperator op, CeedVector assembled) {
+  CK(op_plan(op));
+  Ceed         ceed = op->ceed;
+  cudaStream_t s    = ceed->stream;
+  double      *y;
+  switch (op->plan) {
+    case PLAN_FREESTREAM_JAC: {
+      CK(need_len(op, assembled, 5 * op->fop->l_size, "point-block"));
+      CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "surface qdata"));
+      CK(need_len(op, op->in[4].v, op->in[4].r->l_size, "surface jacobian data"));
+      const double *qd, *jd;
+      CK(vec_dev_read(op->in[2].v, &qd));
+      CK(vec_dev_read(op->in[4].v, &jd));
+      CK(vec_dev_write(assembled, &y, 0));
+      HB_CK(ceed, hb_freestream_point_block_diagonal(op->fop, op->qf->ctx->data, op->flux_type, qd, jd, y, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_MASS: {
+      CK(need_len(op, assembled, 5 * op->eop->l_size, "point-block"));
+      CK(need_len(op, op->in[1].v, op->in[1].r->l_size, "qdata"));
+      const double *qd;
+      CK(vec_dev_read(op->in[1].v, &qd));
+      CK(vec_dev_write(assembled, &y, 0));
+      HB_CK(ceed, hb_mass_point_block_diagonal(op->eop, qd, y, 1, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_IJACOBIAN: break;
+    default: return plan_fail(op, "point-block assembly is provided for the IJacobian operators (volume and free-stream faces) and the mass operator");
+  }
+  const HbNewtonianContext *ctx = (const HbNewtonianContext *)op->qf->ctx->data;
+  if ((ctx->idl_enable ? 15 : 14) != op->qf->in[3].size) return plan_fail(op, "jac_data component count does not match the IDL setting");
+  const int64_t n = op->eop->l_size;
+  CK(need_len(op, assembled, 5 * n, "point-block"));
+  CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
+  CK(need_len(op, op->in[3].v, op->in[3].r->l_size, "jac_data"));
+  const double *qd;
+  CK(vec_dev_read(op->in[2].v, &qd));
+  CeedVector jd = op->in[3].v;
+  if (ceed->mixed) {
+    if (!jd->f32_valid) {
+      const double *j64;
+      CK(vec_dev_read(jd, &j64));
+      CK(vec_f32_shadow(jd));
+      HB_CK(ceed, hb_vec_f64_to_f32(j64, jd->d_f32, jd->length, 0, s));
+      jd->f32_valid = 1;
+    }
+    if (!op->d_tmp_pb32) CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_pb32, sizeof(float) * 5 * (size_t)n));
+    CK(vec_dev_write(assembled, &y, 0));
+    HB_CK(ceed, hb_point_block_diagonal_f32(op->eop, ctx, qd, jd->d_f32, op->d_tmp_pb32, 0, s));
+    HB_CK(ceed, hb_vec_f32_to_f64(op->d_tmp_pb32, y, 5 * n, 1, s));
+  } else {
+    const double *j64;
+    CK(vec_dev_read(jd, &j64));
+    CK(vec_dev_write(assembled, &y, 0));
+    HB_CK(ceed, hb_point_block_diagonal_f64(op->eop, ctx, qd, j64, y, 1, s));
+  }
+  return CEED_ERROR_SUCCESS;
+}
+
+int CeedOperatorLinearAssembleAddPointBlockDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request) {
+  (void)request;
+  if (op->composite) {
+    for (int i = 0; i < op->nsub; i++) CK(op_pbdiag_add_single(op->subs[i], assembled));
+    return CEED_ERROR_SUCCESS;
+  }
+  return op_pbdiag_add_single(op, assembled);
+}
+
+int CeedOperatorLinearAssemblePointBlockDiagonal(CeedOperator op, CeedVector assembled, CeedRequest *request) {
+  CK(CeedVectorSetValue(assembled, 0.0));
+  return CeedOperatorLinearAssembleAddPointBlockDiagonal(op, assembled, request);
+}
+
 int CeedOperatorLinearAssemblePointBlockDiagonalSymbolic(CeedOperator op, CeedSize *num_entries, CeedInt **rows, CeedInt **cols) {
-  (void)num_entries, (void)rows, (void)cols;
-  return ASSEMBLY_UNSUPPORTED(op);
+  CeedElemRestriction r;
+  CK(pb_rstr(op, &r));
+  const CeedSize nodes = r->l_size / 5, ne = nodes * 25;
+  CeedInt *ro = (CeedInt *)malloc(sizeof(CeedInt) * (size_t)ne), *co = (CeedInt *)malloc(sizeof(CeedInt) * (size_t)ne);
+  if (!ro || !co) {
+    free(ro);
+    free(co);
+    return CeedError(op->ceed, CEED_ERROR_MAJOR, "out of host memory for %td point-block entries", ne);
+  }
+  for (CeedSize k = 0; k < ne; k++) {
+    const CeedSize node = k / 25;
+    ro[k] = (CeedInt)(node * 5 + (k / 5) % 5);
+    co[k] = (CeedInt)(node * 5 + k % 5);
+  }
+  *num_entries = ne;
+  *rows        = ro;
+  *cols        = co;
+  return CEED_ERROR_SUCCESS;
 }
 int CeedOperatorGetOperatorAssemblyData(CeedOperator op, CeedOperatorAssemblyData *data) {
   (void)data;

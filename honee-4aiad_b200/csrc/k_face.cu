@@ -153,11 +153,14 @@ __global__ void k_freestream_jac(int P, int Q, const int32_t *__restrict__ offse
 }
 
 // diag += sum over the face's points of B_p^2 wdetJb dF_c/dU_c: the diagonal of the operator above, each point's
-// Jacobian column c taken by the forward tangent with dU = e_c (libCEED diagonal assembly of Freestream_Jacobian)
+// Jacobian column c taken by the forward tangent with dU = e_c (libCEED diagonal assembly of Freestream_Jacobian).
+// FULL: the whole 5 x 5 point block, out[(node * 5 + i) * 5 + j] += sum B_p^2 wdetJb dF_i/dU_j (point-block assembly).
+template <bool FULL>
 __global__ void k_freestream_diag(int P, int Q, const int32_t *__restrict__ offsets, const int32_t *__restrict__ faces, FaceBasis b,
                                   hb::PhysConst<double> pc, Exterior ex, const double *__restrict__ qd, const double *__restrict__ jac,
                                   double *__restrict__ diag) {
-  __shared__ double sD[5][kMaxQ2];
+  constexpr int NC = FULL ? 25 : 5;
+  __shared__ double sD[NC][kMaxQ2];
   const int f = faces[blockIdx.x], t = threadIdx.x, P2 = P * P, Q2 = Q * Q;
   if (t < Q2) {
     double U[5];
@@ -177,18 +180,24 @@ __global__ void k_freestream_diag(int P, int Q, const int32_t *__restrict__ offs
       hb::state_from_u_fwd(pc, s, inv_rho, etot, eint, dU, ds);
       if (ex.hllc) hb::riemann::hllc_flux_fwd(ex.gamma, ex.cv, s, ds, sx, dsx, n, dF);
       else hb::riemann::hll_flux_fwd(ex.gamma, ex.cv, s, ds, sx, dsx, n, dF);
-      sD[c][t] = wdetJb * dF[c];
+      if (FULL) {
+#pragma unroll
+        for (int i = 0; i < 5; i++) sD[i * 5 + c][t] = wdetJb * dF[i];
+      } else {
+        sD[c][t] = wdetJb * dF[c];
+      }
     }
   }
   __syncthreads();
-  for (int i = t; i < 5 * P2; i += blockDim.x) {
-    const int p = i / 5, c = i % 5;
+  for (int i = t; i < NC * P2; i += blockDim.x) {
+    const int p = i / NC, c = i % NC;
     double acc = 0;
     for (int k = 0; k < Q2; k++) {
       const double w = b2(b, P, k % Q, k / Q, p % P, p / P);
       acc += w * w * sD[c][k];
     }
-    diag[offsets[(int64_t)f * P2 + p] + c] += acc;
+    const int64_t o = offsets[(int64_t)f * P2 + p];
+    diag[FULL ? o * 5 + c : o + c] += acc;  // FULL: c = i * 5 + j
   }
 }
 
@@ -334,8 +343,8 @@ int hb_freestream_jacobian_apply(const HbFaceOp *op, const void *ctx264, int flu
   return freestream_jac<double>(op, ctx264, flux_type, qdata_sur, jac_data_sur, dq, v, stream);
 }
 
-int hb_freestream_diagonal(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur, double *diag,
-                           void *stream) {
+static int freestream_diag(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur, double *diag,
+                           void *stream, bool full) {
   if (!op || !ctx264 || !qdata_sur || !jac_data_sur || !diag || (flux_type != 0 && flux_type != 1)) return HB_ERROR_INVALID;
   hb::PhysConst<double> pc;
   Exterior ex;
@@ -345,11 +354,26 @@ int hb_freestream_diagonal(const HbFaceOp *op, const void *ctx264, int flux_type
   const FaceBasis b = fbasis(op);
   for (int c = 0; c < op->num_colors; c++) {
     const int n = op->h_color_ptr[c + 1] - op->h_color_ptr[c];
-    if (n)
-      k_freestream_diag<<<n, nthreads(op), 0, (cudaStream_t)stream>>>(op->P, op->Q, op->d_offsets, op->d_color_elem + op->h_color_ptr[c], b, pc, ex,
-                                                                      qdata_sur, jac_data_sur, diag);
+    if (!n) continue;
+    const int nt = nthreads(op); /* >= Q^2 for the point phase; the block scatter strides over its 25 P^2 entries */
+    if (full)
+      k_freestream_diag<true><<<n, nt, 0, (cudaStream_t)stream>>>(op->P, op->Q, op->d_offsets, op->d_color_elem + op->h_color_ptr[c], b, pc, ex,
+                                                                  qdata_sur, jac_data_sur, diag);
+    else
+      k_freestream_diag<false><<<n, nt, 0, (cudaStream_t)stream>>>(op->P, op->Q, op->d_offsets, op->d_color_elem + op->h_color_ptr[c], b, pc, ex,
+                                                                   qdata_sur, jac_data_sur, diag);
   }
   return rc();
+}
+
+int hb_freestream_diagonal(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur, double *diag,
+                           void *stream) {
+  return freestream_diag(op, ctx264, flux_type, qdata_sur, jac_data_sur, diag, stream, false);
+}
+
+int hb_freestream_point_block_diagonal(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
+                                       double *out, void *stream) {
+  return freestream_diag(op, ctx264, flux_type, qdata_sur, jac_data_sur, out, stream, true);
 }
 
 int hb_freestream_jacobian_apply_f32(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,

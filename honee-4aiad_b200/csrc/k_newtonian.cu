@@ -975,6 +975,143 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemAr
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
+// Point-block diagonal of the IJacobian operator with batched contractions.
+//
+// The element matrix restricted to a node p and components (i out, j in) is
+//   sum_q sum_{a,b} phi_a(p,q) A_q[(a,i),(b,j)] phi_b(p,q),   a, b in {value, d/dX0, d/dX1, d/dX2}
+// with A_q the linearised point function (20 x 20, the columns taken by forward products with unit inputs).  phi_a phi_b is
+// symmetric in (a,b), so the ten combinations {a,b} carry A[(a,i),(b,j)] + A[(b,i),(a,j)] (one term when a = b), and each is
+// a tensor product of per-direction squared-basis rows (B B, B G or G G).  A round covers one input component j and NI
+// output components: the point phase accumulates the NI x 10 combination arrays in shared memory, one thread per point,
+// then three batched passes contract them all, and the last pass sums the ten combinations before the coloured scatter.
+// This is libCEED's point-block semantics (CeedOperatorLinearAssemblePointBlockDiagonal: a 5 x 5 block
+// [component out][component in] per node, what MatCEED hands PCVPBJACOBI, src/mat-ceed.c:76-153).  Like k_diagonal the
+// cost is the 20 forward products per point; the batched contraction keeps the 25 blocks at about 2.5x the diagonal.
+__host__ __device__ constexpr int blockdiag_ni(int P, int Q, int elem_bytes) {
+  // the largest output-component group whose combination arrays [NI*10][Q^3] and first-pass buffer [NI*10][Q^2 P] fit
+  return (50 * (Q * Q * Q + Q * Q * P) * elem_bytes <= 200 * 1024)   ? 5
+         : (30 * (Q * Q * Q + Q * Q * P) * elem_bytes <= 200 * 1024) ? 3
+         : (20 * (Q * Q * Q + Q * Q * P) * elem_bytes <= 200 * 1024) ? 2
+                                                                     : 1;
+}
+template <int P, int Q, typename T>
+constexpr size_t blockdiag_smem() {
+  return sizeof(T) * (size_t)blockdiag_ni(P, Q, sizeof(T)) * 10 * (Q * Q * Q + Q * Q * P);
+}
+
+__device__ __forceinline__ int combo_sel(int m, int d) {
+  // derivatives in direction d of combination m (order: II, IGx, IGy, IGz, GxGx, GyGy, GzGz, GxGy, GxGz, GyGz)
+  if (d == 0) return (m == 1 || m == 7 || m == 8) ? 1 : (m == 4 ? 2 : 0);
+  if (d == 1) return (m == 2 || m == 7 || m == 9) ? 1 : (m == 5 ? 2 : 0);
+  return (m == 3 || m == 8 || m == 9) ? 1 : (m == 6 ? 2 : 0);
+}
+__host__ __device__ constexpr int combo_of(int a, int b) {
+  // unordered pair {a, b} of {value, Gx, Gy, Gz} -> combination index
+  return a > b ? combo_of(b, a)
+               : (a == b ? (a == 0 ? 0 : 3 + a) : (a == 0 ? b : (a == 1 ? (b == 2 ? 7 : 8) : 9)));
+}
+
+template <int P, int Q, typename T>
+__global__ void __launch_bounds__(nthreads_for<T>(Q), 1) k_blockdiag(const ElemArgs<T> a, const DiagArgs<T> p) {
+  constexpr int NT = nthreads_for<T>(Q);
+  constexpr int P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q, Q2P = Q2 * P, QP2 = Q * P2;
+  constexpr int NI = blockdiag_ni(P, Q, sizeof(T)), NA = NI * 10, NG = (5 + NI - 1) / NI;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sA = reinterpret_cast<T *>(smem_raw);  // [NA][Q3]; after the second pass [NA][Q][P][P]
+  T *sY = sA + NA * Q3;                     // [NA][Q][Q][P]
+  __shared__ T sW[3][kMaxP * kMaxP];        // B*B, B*G, G*G  [Q][P]
+  for (int t = threadIdx.x; t < Q * P; t += NT) {
+    T b = 0, g = 0;
+#pragma unroll
+    for (int i = 0; i < Q * P; i++)
+      if (i == t) {
+        b = a.basis.B[i];
+        g = p.G1[i];
+      }
+    sW[0][t] = b * b;
+    sW[1][t] = b * g;
+    sW[2][t] = g * g;
+  }
+  __syncthreads();
+  constexpr int kRounds = 5 * NG;
+  for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
+    const int e = a.elems[idx];
+    const int32_t *off = a.offsets + (int64_t)e * P3;
+    for (int r = 0; r < kRounds; r++) {
+      const int j_in = r / NG, i0 = (r % NG) * NI;  // input component j_in, output components [i0, i0 + NI)
+      const int q = threadIdx.x;
+      if (q < Q3) {
+        T jd[15], wdetJ, X[3][3];
+        const T *jdp = p.jac_data + (int64_t)e * a.num_jd * Q3 + q;
+#pragma unroll
+        for (int k = 0; k < 14; k++) jd[k] = jdp[k * Q3];
+        jd[14] = a.num_jd > 14 ? jdp[14 * Q3] : T(0);
+        load_qdata(a.qdata + (int64_t)e * 10 * Q3, Q3, q, wdetJ, X);
+        for (int t = 0; t < NA; t++) sA[t * Q3 + q] = 0;
+        {
+          const int jj = j_in;
+#pragma unroll
+          for (int n = 0; n < 4; n++) {
+            T dq[5] = {0, 0, 0, 0, 0}, gref[3][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}}, v[5], gv[3][5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+              if (n == 0 && k == jj) dq[k] = 1;
+#pragma unroll
+              for (int d = 0; d < 3; d++)
+                if (n == d + 1 && k == jj) gref[d][k] = 1;
+            }
+            ijacobian_point_stream<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+              if (k < i0 || k >= i0 + NI) continue;
+              T *row = sA + (k - i0) * 10 * Q3 + q;
+              // A[(mo, k), (n, jj)] for mo = value, Gx, Gy, Gz
+              row[combo_of(0, n) * Q3] += v[k];
+              row[combo_of(1, n) * Q3] += gv[0][k];
+              row[combo_of(2, n) * Q3] += gv[1][k];
+              row[combo_of(3, n) * Q3] += gv[2][k];
+            }
+          }
+        }
+      }
+      __syncthreads();
+      for (int f = threadIdx.x; f < NA * Q2P; f += NT) {  // x: [a][k][j][pa]
+        const int t = f / Q2P, rem = f % Q2P, pa = rem % P, kj = rem / P;
+        const T *W = sW[combo_sel(t % 10, 0)];
+        T acc = 0;
+#pragma unroll
+        for (int i = 0; i < Q; i++) acc += W[i * P + pa] * sA[t * Q3 + kj * Q + i];
+        sY[f] = acc;
+      }
+      __syncthreads();
+      for (int f = threadIdx.x; f < NA * QP2; f += NT) {  // y: [a][k][pb][pa]
+        const int t = f / QP2, rem = f % QP2, pa = rem % P, pb = (rem / P) % P, k = rem / P2;
+        const T *W = sW[combo_sel(t % 10, 1)];
+        T acc = 0;
+#pragma unroll
+        for (int j = 0; j < Q; j++) acc += W[j * P + pb] * sY[t * Q2P + (k * Q + j) * P + pa];
+        sA[f] = acc;
+      }
+      __syncthreads();
+      for (int f = threadIdx.x; f < NI * P3; f += NT) {  // z, summed over the ten combinations, and the scatter
+        const int il = f / P3, pp = f % P3, pab = pp % P2, pc_ = pp / P2;
+        const int i = i0 + il;
+        if (i >= 5) continue;
+        T acc = 0;
+#pragma unroll
+        for (int m = 0; m < 10; m++) {
+          const T *W = sW[combo_sel(m, 2)];
+#pragma unroll
+          for (int k = 0; k < Q; k++) acc += W[k * P + pc_] * sA[(il * 10 + m) * QP2 + k * P2 + pab];
+        }
+        p.diag[(int64_t)__ldg(off + pp) * 5 + i * 5 + j_in] += acc;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
 // Geometric factors (qfunctions/setupgeo.h:42-56, utils.h:201-216): trilinear coordinates -> w detJ, dX/dx.
 
 __global__ void k_setup_qdata(int num_elem, int Q, const double *__restrict__ x_elem, QRef qref, QRef qw, double *__restrict__ qdata) {
@@ -1238,7 +1375,7 @@ __global__ void __launch_bounds__(kMassThreads) k_mass(const ElemArgs<double> a,
 }
 
 template <int P, int Q>
-__global__ void __launch_bounds__(kMassThreads) k_mass_diag(const ElemArgs<double> a, double *__restrict__ diag) {
+__global__ void __launch_bounds__(kMassThreads) k_mass_diag(const ElemArgs<double> a, double *__restrict__ diag, int block) {
   constexpr int NT = kMassThreads, P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q;
   __shared__ double sW[Q * P];  // B^2
   __shared__ double sX[Q3], sY[Q3];
@@ -1269,14 +1406,15 @@ __global__ void __launch_bounds__(kMassThreads) k_mass_diag(const ElemArgs<doubl
       double s = 0;
 #pragma unroll
       for (int i = 0; i < Q; i++) s += sW[i * P + pa] * sX[pcb * Q + i];
-      diag[a.offsets[(int64_t)e * P3 + p] + c] += s;
+      const int64_t o = a.offsets[(int64_t)e * P3 + p];
+      diag[block ? o * 5 + c * 6 : o + c] += s;  // block: entry (c, c) of the node's 5 x 5 block
     }
     __syncthreads();
   }
 }
 
 template <int P, int Q>
-static int launch_mass(const HbElemOp *op, const double *qdata, const double *u, double *v, bool diagonal, cudaStream_t s) {
+static int launch_mass(const HbElemOp *op, const double *qdata, const double *u, double *v, bool diagonal, cudaStream_t s, int block = 0) {
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<double> a;
     memset(&a, 0, sizeof a);
@@ -1288,9 +1426,26 @@ static int launch_mass(const HbElemOp *op, const double *qdata, const double *u,
     a.status = op->d_status;
     if (a.n_elems == 0) continue;
     if (diagonal)
-      k_mass_diag<P, Q><<<grid_for(op, a.n_elems, k_mass_diag<P, Q>, kMassThreads, 0), kMassThreads, 0, s>>>(a, v);
+      k_mass_diag<P, Q><<<grid_for(op, a.n_elems, k_mass_diag<P, Q>, kMassThreads, 0), kMassThreads, 0, s>>>(a, v, block);
     else
       k_mass<P, Q><<<grid_for(op, a.n_elems, k_mass<P, Q>, kMassThreads, 0), kMassThreads, 0, s>>>(a, u, v);
+  }
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+
+template <int P, int Q, typename T>
+static int launch_blockdiag(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, T *out, cudaStream_t s) {
+  const size_t sm = blockdiag_smem<P, Q, T>();
+  if (cudaFuncSetAttribute(k_blockdiag<P, Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
+  DiagArgs<T> p;
+  p.jac_data = jd;
+  p.diag = out;
+  memset(p.G1, 0, sizeof p.G1);
+  for (int i = 0; i < Q * P; i++) p.G1[i] = T(op->grad1d[i]);
+  for (int c = 0; c < op->num_colors; c++) {
+    ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
+    if (a.n_elems == 0) continue;
+    k_blockdiag<P, Q, T><<<grid_for(op, a.n_elems, k_blockdiag<P, Q, T>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
@@ -1477,6 +1632,48 @@ extern "C" int hb_mass_diagonal(const HbElemOp *op, const double *qdata, double 
   if (!add && cudaMemsetAsync(diag, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
 #define HB_CASE(PP, QQ) \
   if (op->P == PP && op->Q == QQ) return launch_mass<PP, QQ>(op, qdata, NULL, diag, true, s);
+  HB_PQ_LIST(HB_CASE)
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+
+// Point-block diagonal of the IJacobian operator: out[(node * 5 + i) * 5 + j] (+)= d v_(node,i) / d dq_(node,j), i.e. one
+// row-major 5 x 5 block per node of the node-interleaved L-vector (out holds l_size * 5 values).
+template <typename T>
+static int pbdiag_dispatch(const HbElemOp *op, const void *ctx184, const double *qdata, const T *jac_data, T *out, int add, void *stream) {
+  int err = check_op(op);
+  if (err) return err;
+  if (!ctx184 || !qdata || !jac_data || !out) return HB_ERROR_INVALID;
+  HbNewtonianContext ctx;
+  memcpy(&ctx, ctx184, sizeof ctx);
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!add && cudaMemsetAsync(out, 0, sizeof(T) * (size_t)op->l_size * 5, s) != cudaSuccess) return HB_ERROR_CUDA;
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_blockdiag<PP, QQ, T>(op, ctx, qdata, jac_data, out, s);
+  HB_PQ_LIST(HB_CASE)
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+
+extern "C" int hb_point_block_diagonal_f64(const HbElemOp *op, const void *ctx184, const double *qdata, const double *jac_data, double *out, int add,
+                                           void *stream) {
+  return pbdiag_dispatch<double>(op, ctx184, qdata, jac_data, out, add, stream);
+}
+extern "C" int hb_point_block_diagonal_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, float *out, int add,
+                                           void *stream) {
+  return pbdiag_dispatch<float>(op, ctx184, qdata, jac_data, out, add, stream);
+}
+
+// the mass operator's point blocks: its diagonal on the diagonal of each node's 5 x 5 block (the components decouple)
+extern "C" int hb_mass_point_block_diagonal(const HbElemOp *op, const double *qdata, double *out, int add, void *stream) {
+  int err = check_op(op);
+  if (err) return err;
+  if (!qdata || !out) return HB_ERROR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!add && cudaMemsetAsync(out, 0, sizeof(double) * op->l_size * 5, s) != cudaSuccess) return HB_ERROR_CUDA;
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_mass<PP, QQ>(op, qdata, NULL, out, true, s, 1);
   HB_PQ_LIST(HB_CASE)
 #undef HB_CASE
   return HB_ERROR_UNSUPPORTED;

@@ -113,6 +113,11 @@ class ElemOp:
         fn = _load().hb_diagonal_assemble_f32 if fp32 else _load().hb_diagonal_assemble_f64
         _chk(fn(self.ptr, cb, _addr(qdata), _addr(jac_data), _addr(diag), int(add), _stream(stream)), "hb_diagonal_assemble")
 
+    def point_block_diagonal(self, ctx_bytes: bytes, qdata, jac_data, out, add=False, fp32=False, stream=None):
+        """out[(node * 5 + i) * 5 + j] (+)= the node's 5 x 5 block of the IJacobian (5 * l_size values)."""
+        cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        fn = _load().hb_point_block_diagonal_f32 if fp32 else _load().hb_point_block_diagonal_f64
+        _chk(fn(self.ptr, cb, _addr(qdata), _addr(jac_data), _addr(out), int(add), _stream(stream)), "hb_point_block_diagonal")
 
     def mass(self, qdata, u, v, add=False, stream=None):
         """v (+)= M u, the Mass_5 operator of the explicit path."""
@@ -120,6 +125,9 @@ class ElemOp:
 
     def mass_diagonal(self, qdata, diag, add=False, stream=None):
         _chk(_load().hb_mass_diagonal(self.ptr, _addr(qdata), _addr(diag), int(add), _stream(stream)), "hb_mass_diagonal")
+
+    def mass_point_block_diagonal(self, qdata, out, add=False, stream=None):
+        _chk(_load().hb_mass_point_block_diagonal(self.ptr, _addr(qdata), _addr(out), int(add), _stream(stream)), "hb_mass_point_block_diagonal")
 
 
 class HbFaceOp(C.Structure):
@@ -160,6 +168,12 @@ class FaceOp:
         cb = C.create_string_buffer(bytes(ctx264), len(ctx264))
         _chk(_load().hb_freestream_apply(self.ptr, cb, C.c_int(flux_type), _addr(self.qdata), _addr(q), _addr(self.jac), _addr(v), _stream(stream)),
              "hb_freestream_apply")
+
+    def freestream_point_block(self, ctx264: bytes, out, flux_type=1, stream=None):
+        """out[(node * 5 + i) * 5 + j] += the face Jacobian's 5 x 5 node blocks (after freestream() stored the face state)."""
+        cb = C.create_string_buffer(bytes(ctx264), len(ctx264))
+        _chk(_load().hb_freestream_point_block_diagonal(self.ptr, cb, C.c_int(flux_type), _addr(self.qdata), _addr(self.jac), _addr(out),
+                                                        _stream(stream)), "hb_freestream_point_block_diagonal")
 
     def freestream_jacobian(self, ctx264: bytes, dq, v, flux_type=1, stream=None):
         cb = C.create_string_buffer(bytes(ctx264), len(ctx264))

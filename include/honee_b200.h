@@ -101,6 +101,13 @@ HB_EXPORT int hb_diagonal_assemble_f64(const HbElemOp *op, const void *ctx184, c
                              void *stream);
 HB_EXPORT int hb_diagonal_assemble_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, float *diag, int add,
                              void *stream);
+/* Point-block diagonal of the IJacobian operator (CeedOperatorLinearAssemblePointBlockDiagonal, what MatCEED assembles for
+ * -pc_type vpbjacobi, src/mat-ceed.c:76-153): out[(node * 5 + i) * 5 + j] (+)= dv_(node,i) / ddq_(node,j), a row-major
+ * 5 x 5 block per node of the node-interleaved L-vector; out holds 5 * l_size values. */
+HB_EXPORT int hb_point_block_diagonal_f64(const HbElemOp *op, const void *ctx184, const double *qdata, const double *jac_data, double *out, int add,
+                                          void *stream);
+HB_EXPORT int hb_point_block_diagonal_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, float *out, int add,
+                                          void *stream);
 
 /* Geometric factors of the Setup QFunction (qfunctions/setupgeo.h:42-56; driven by QDataGet, src/qdata.c:133-190) from
  * trilinear vertex coordinates x_elem [num_elem][3][8] (device) with the Gauss rule qref1d/qweight1d (host). */
@@ -178,6 +185,8 @@ HB_EXPORT int hb_ts_destroy(HbTimeStepper *ts);
  * diagonal (what MatGetDiagonal_Ceed gives PCJacobi "diagonal"; the row sums of PCJacobi "rowsum" are M applied to ones). */
 HB_EXPORT int hb_mass_apply(const HbElemOp *op, const double *qdata, const double *u, double *v, int add, void *stream);
 HB_EXPORT int hb_mass_diagonal(const HbElemOp *op, const double *qdata, double *diag, int add, void *stream);
+/* its point blocks (5 * l_size values, row-major 5 x 5 per node): the diagonal on each block's diagonal, zeros elsewhere */
+HB_EXPORT int hb_mass_point_block_diagonal(const HbElemOp *op, const double *qdata, double *out, int add, void *stream);
 
 #define HB_RK_MAX_STAGES 6
 typedef struct {
@@ -349,6 +358,9 @@ HB_EXPORT int hb_freestream_jacobian_apply(const HbFaceOp *op, const void *ctx26
  * sub-operator): per face node p and component c, sum over points of B_p^2 wdetJb dF_c/dU_c. */
 HB_EXPORT int hb_freestream_diagonal(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur, const double *jac_data_sur,
                                      double *diag, void *s);
+/* out[(node * 5 + i) * 5 + j] += the 5 x 5 point block of that Jacobian (sum over points of B_p^2 wdetJb dF_i/dU_j) */
+HB_EXPORT int hb_freestream_point_block_diagonal(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur,
+                                                 const double *jac_data_sur, double *out, void *s);
 /* the same with FP32 dq and v (state and flux math in FP64), for the mixed-precision Krylov solve */
 HB_EXPORT int hb_freestream_jacobian_apply_f32(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur,
                                                const double *jac_data_sur, const float *dq, float *v, void *s);

@@ -224,3 +224,27 @@ def freestream_diagonal(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, c
         for p in range(P * P):
             out[offsets[f, p]:offsets[f, p] + 5] += contrib[p]
     return out
+
+
+def freestream_point_block(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, cv, cp, hllc=True, l_size=None):
+    """5 x 5 point blocks of the free-stream Jacobian, out[(node * 5 + i) * 5 + j] = sum over a node's face points of
+    B_p^2 wdetJb dF_i/dU_j (the point-block assembly of the Freestream_Jacobian operator, summed over faces)."""
+    B = np.asarray(interp1d).reshape(Q, P)
+    Bq = np.einsum("jb,ia->jiba", B, B).reshape(Q * Q, P * P)
+    n_l = l_size if l_size is not None else int(offsets.max()) + 5
+    out = np.zeros(5 * n_l)
+    zero = St(*(np.zeros(Q * Q) if k not in (1, 4) else np.zeros((3, Q * Q)) for k in range(6)))
+    for f in range(offsets.shape[0]):
+        s = state_from_U(jac[f], cv, cp)
+        n = qdata_sur[f, 1:4]
+        D = np.zeros((5, 5, Q * Q))                                             # [i][j][point]
+        for j in range(5):
+            dU = np.zeros((5, Q * Q))
+            dU[j] = 1.0
+            ds = state_from_U_fwd(s, dU, cv, cp)
+            D[:, j] = qdata_sur[f, 0] * riemann(s, exterior(U_inf, Y_inf, Q * Q), n, cv, cp, hllc, dL=ds, dR=zero)
+        contrib = np.einsum("kp,ijk->pij", Bq ** 2, D)                          # [P2][5][5]
+        for p in range(P * P):
+            o = offsets[f, p] * 5
+            out[o:o + 25] += contrib[p].reshape(-1)
+    return out

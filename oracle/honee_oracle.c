@@ -975,6 +975,61 @@ int oracle_assemble_diagonal(const OracleMesh *m, OracleQF qf, void *ctx, const 
   return err;
 }
 
+/* ---- point-block diagonal (libCEED CeedOperatorLinearAssemblePointBlockDiagonal semantics): per node a row-major
+ * 5 x 5 block [component out][component in], out[(node * 5 + i) * 5 + j], from the same linearised QFunction ---- */
+static void point_block_elem(const OracleMesh *m, int64_t e, void *user, double *s, int *err) {
+  ApplyArgs    *a  = (ApplyArgs *)user;
+  const int     P = m->P, Q = m->Q, P3 = P * P * P, Q3 = Q * Q * Q;
+  const double *B = m->interp1d, *G = m->grad1d;
+  double       *be = s; /* [P3][5][5] */
+  memset(be, 0, sizeof(double) * 25 * P3);
+  for (int qp = 0; qp < Q3; qp++) {
+    const int qi = qp % Q, qj = (qp / Q) % Q, qk = qp / (Q * Q);
+    double A[20][20], qd[10], jd[HB_JAC_DATA_COMPS_IDL];
+    for (int c = 0; c < 10; c++) qd[c] = a->qdata[(e * 10 + c) * Q3 + qp];
+    for (int c = 0; c < a->num_jd; c++) jd[c] = a->jd_in[(e * a->num_jd + c) * Q3 + qp];
+    for (int j = 0; j < 20; j++) {
+      double dq[5] = {0}, gdq[15] = {0}, v[5], gv[15];
+      if (j < 5) dq[j] = 1;
+      else gdq[j - 5] = 1;
+      const double *in[4]  = {dq, gdq, qd, jd};
+      double       *out[2] = {v, gv};
+      if (a->qf(a->ctx, 1, in, out)) *err = 1;
+      for (int i = 0; i < 5; i++) A[i][j] = v[i];
+      for (int i = 0; i < 15; i++) A[5 + i][j] = gv[i];
+    }
+    for (int p = 0; p < P3; p++) {
+      const int pa = p % P, pb = (p / P) % P, pc = p / (P * P);
+      const double bx = B[qi * P + pa], by = B[qj * P + pb], bz = B[qk * P + pc];
+      const double gx = G[qi * P + pa], gy = G[qj * P + pb], gz = G[qk * P + pc];
+      const double phi[4] = {bx * by * bz, gx * by * bz, bx * gy * bz, bx * by * gz};
+      for (int ci = 0; ci < 5; ci++)
+        for (int cj = 0; cj < 5; cj++) {
+          double acc = 0;
+          for (int mo = 0; mo < 4; mo++) {
+            const int io = mo == 0 ? ci : 5 + (mo - 1) * 5 + ci;
+            for (int mi = 0; mi < 4; mi++) {
+              const int ii = mi == 0 ? cj : 5 + (mi - 1) * 5 + cj;
+              acc += phi[mo] * A[io][ii] * phi[mi];
+            }
+          }
+          be[(p * 5 + ci) * 5 + cj] += acc;
+        }
+    }
+  }
+  for (int p = 0; p < P3; p++)
+    for (int k = 0; k < 25; k++) a->v[(int64_t)m->offsets[e * P3 + p] * 5 + k] += be[p * 25 + k];
+}
+
+int oracle_assemble_point_block(const OracleMesh *m, OracleQF qf, void *ctx, const double *qdata, const double *jac_data, int num_jd, double *out,
+                                int64_t l_size) {
+  ApplyArgs a = {qf, ctx, NULL, NULL, qdata, NULL, jac_data, NULL, out, num_jd};
+  int       err = 0;
+  memset(out, 0, sizeof(double) * 5 * l_size);
+  for_each_elem(m, point_block_elem, &a, (size_t)25 * m->P * m->P * m->P, &err);
+  return err;
+}
+
 /* ---- geometric factors ---- */
 static void linear_basis(int Q, double *Bx, double *Gx, double *w) {
   double x[16];

@@ -104,6 +104,11 @@ int oracle_qf_rhs_conserv(void *ctx, int Q, const double *const *in, double *con
 int oracle_apply_mass(const OracleMesh *m, OracleQF qf, const double *u, const double *qdata, double *v, int64_t l_size);
 int oracle_qf_mass(void *ctx, int Q, const double *const *in, double *const *out);
 
+/* Point-block diagonal of the IJacobian operator (CeedOperatorLinearAssemblePointBlockDiagonal semantics): a row-major
+ * 5 x 5 block per node, out[(node * 5 + i) * 5 + j] (5 * l_size values), overwritten. */
+int oracle_assemble_point_block(const OracleMesh *m, OracleQF qf, void *ctx, const double *qdata, const double *jac_data, int num_jd, double *out,
+                                int64_t l_size);
+
 /* Geometric factors: qdata [elem][10][Q^3] from vertex coordinates x_elem [elem][3][8] (P=2 linear coordinate basis
  * with the same Gauss rule; src/qdata.c:133-190, qfunctions/setupgeo.h:42-56). */
 int oracle_setup_qdata(int num_elem, int Q, const double *x_elem, double *qdata);

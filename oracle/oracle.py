@@ -65,6 +65,7 @@ def _declare(L):
     L.oracle_qf_mass.restype = C.c_int
     L.oracle_apply_ijacobian.restype = C.c_int
     L.oracle_assemble_diagonal.restype = C.c_int
+    L.oracle_assemble_point_block.restype = C.c_int
     L.oracle_box_num_nodes.restype = C.c_int64
 
 
@@ -181,6 +182,17 @@ def apply_mass(mesh: Mesh, u, qdata, use_ref=False):
     if L.oracle_apply_mass(C.byref(mesh.c), fn, ptr(u), ptr(qdata), ptr(v), C.c_int64(v.size)):
         raise RuntimeError("oracle mass failed")
     return v
+
+
+def assemble_point_block(mesh: Mesh, ctx: bytes, qdata, jac_data, l_size, num_jd=14, qf_name=None, use_ref=False):
+    """Row-major 5 x 5 blocks per node, [(node * 5 + i) * 5 + j], of the IJacobian operator."""
+    L = lib()
+    fn = qf(qf_name or ("ref_IJacobian_Newtonian_Conserv" if use_ref else "oracle_qf_ijacobian_conserv"), use_ref)
+    out = np.zeros(5 * l_size)
+    cbuf = C.create_string_buffer(bytes(ctx), len(ctx))
+    if L.oracle_assemble_point_block(C.byref(mesh.c), fn, cbuf, ptr(qdata), ptr(jac_data), C.c_int(num_jd), ptr(out), C.c_int64(l_size)):
+        raise RuntimeError("oracle point-block assembly failed")
+    return out
 
 
 def setup_qdata(num_elem, Q, x_elem):
