@@ -45,6 +45,10 @@ struct HbTimeStepper {
   /* matrix-free (finite-difference) Jacobian action: perturbed state, rate and residual */
   double *qp, *qdp, *rp;
   /* optional free-stream boundary faces: residual and Jacobian sub-operators of the composite */
+  /* point-block Jacobi (pc_jacobi 2): FP64 blocks, inverted in place (FP64) or into pb32 (mixed precision) */
+  double *pb64;
+  float  *pb32;
+  int    *d_sing;
   const HbFaceOp *bc;
   unsigned char   bc_ctx[sizeof(HbFreestreamContext)];
   int             bc_flux;
@@ -87,6 +91,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
   if (opts->gmres_restart < 1 || opts->gmres_restart + 1 > MAXK || opts->dt <= 0 || (opts->bdf_order != 1 && opts->bdf_order != 2))
     return HB_ERROR_INVALID;
   if (opts->jfnk && opts->jacobian_fp32) return HB_ERROR_INVALID; /* the difference quotient needs FP64 Krylov vectors */
+  if (opts->pc_jacobi < 0 || opts->pc_jacobi > 2) return HB_ERROR_INVALID;
   HbTimeStepper *ts = (HbTimeStepper *)calloc(1, sizeof *ts);
   if (!ts) return HB_ERROR_NOMEM;
   ts->op = op;
@@ -109,6 +114,10 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
   if (ts->o.jacobian_fp32) err |= cudaMalloc(&ts->jd32, sizeof(float) * njd) | cudaMalloc((void **)&ts->res32, sizeof(float) * (size_t)ts->n);
   else err |= cudaMalloc((void **)&ts->jd64, sizeof(double) * njd);
   if (ts->o.jfnk) err |= cudaMalloc((void **)&ts->qp, nb) | cudaMalloc((void **)&ts->qdp, nb) | cudaMalloc((void **)&ts->rp, nb);
+  if (ts->o.pc_jacobi == 2) {
+    err |= cudaMalloc((void **)&ts->pb64, 5 * nb) | cudaMalloc((void **)&ts->d_sing, sizeof(int));
+    if (ts->o.jacobian_fp32) err |= cudaMalloc((void **)&ts->pb32, 5 * sizeof(float) * (size_t)ts->n);
+  }
   if (err) {
     hb_ts_destroy(ts);
     return HB_ERROR_NOMEM;
@@ -120,7 +129,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
 int hb_ts_destroy(HbTimeStepper *ts) {
   if (!ts) return HB_SUCCESS;
   void *p[] = {ts->q, ts->q_prev, ts->q_prev2, ts->z, ts->qdot, ts->res, ts->delta, ts->d_partial, ts->d_dots, ts->scratch,
-               ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64, ts->qp, ts->qdp, ts->rp};
+               ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64, ts->qp, ts->qdp, ts->rp, ts->pb64, ts->pb32, ts->d_sing};
   for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
     if (p[i]) cudaFree(p[i]);
   free(ts->sgs_w);
@@ -233,6 +242,10 @@ static int kv_jac(HbTimeStepper *ts, const void *x, void *y) {
 /* z = M^-1 x (Jacobi) or copy */
 static int kv_pc(HbTimeStepper *ts, const void *x, void *z) {
   if (!ts->o.pc_jacobi) return kv_copy(ts, z, x);
+  if (ts->o.pc_jacobi == 2) {
+    if (ts->o.jacobian_fp32) return hb_pb_apply_f32(ts->pb32, (const float *)x, (float *)z, ts->n / 5, ts->s);
+    return hb_pb_apply_f64(ts->pb64, (const double *)x, (double *)z, ts->n / 5, ts->s);
+  }
   if (ts->o.jacobian_fp32) return hb_vec_pointwise_mult_f32((float *)z, (const float *)ts->diag, (const float *)x, ts->n, ts->s);
   return hb_vec_pointwise_mult_f64((double *)z, (const double *)ts->diag, (const double *)x, ts->n, ts->s);
 }
@@ -248,9 +261,26 @@ static int kv_multiaxpy(HbTimeStepper *ts, void *w, int k, const double *c) {
   return hb_krylov_multiaxpy_f64((double *)w, (const double *)ts->V, ts->ldv, k, c, ts->n, ts->s);
 }
 
-/* Jacobi diagonal at the current linearisation point, stored inverted */
-static int assemble_pc(HbTimeStepper *ts) {
+/* Jacobi diagonal (or point blocks) at the current linearisation point, stored inverted; *failed: a point block had no
+ * pivot (PETSc reports the same as a failed preconditioner set-up) */
+static int assemble_pc(HbTimeStepper *ts, int *failed) {
+  *failed = 0;
   if (!ts->o.pc_jacobi) return HB_SUCCESS;
+  if (ts->o.pc_jacobi == 2) {
+    const int64_t nodes = ts->n / 5;
+    int           sing  = 0;
+    if (ts->o.jacobian_fp32) {
+      HBCK(hb_point_block_diagonal_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, ts->pb32, 0, ts->s));
+      HBCK(hb_vec_f32_to_f64(ts->pb32, ts->pb64, 5 * ts->n, 0, ts->s));
+    } else {
+      HBCK(hb_point_block_diagonal_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, ts->pb64, 0, ts->s));
+    }
+    if (ts->bc) HBCK(hb_freestream_point_block_diagonal(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, ts->pb64, ts->s));
+    if (ts->o.jacobian_fp32) HBCK(hb_pb_invert_f64_to_f32(ts->pb64, ts->pb32, nodes, ts->d_sing, &sing, ts->s));
+    else HBCK(hb_pb_invert_f64(ts->pb64, ts->pb64, nodes, ts->d_sing, &sing, ts->s));
+    *failed = sing > 0;
+    return HB_SUCCESS;
+  }
   if (ts->o.jacobian_fp32) {
     HBCK(hb_diagonal_assemble_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (float *)ts->diag, 0, ts->s));
     /* invert in FP64 (delta is free before the Krylov solve), store FP32 */
@@ -421,7 +451,14 @@ int hb_ts_step(HbTimeStepper *ts, HbStepStats *st) {
       break;
     }
     if (it == ts->o.newton_max_it) break;
-    if (it == 0 || ts->o.pc_every_newton) HBCK(assemble_pc(ts));
+    if (it == 0 || ts->o.pc_every_newton) {
+      int pc_failed;
+      HBCK(assemble_pc(ts, &pc_failed));
+      if (pc_failed) {
+        st->converged_reason = -3;
+        break;
+      }
+    }
     int    kits;
     double krel;
     HBCK(gmres(ts, &kits, &krel));

@@ -387,6 +387,87 @@ int multidot_scratch(double **p) {
 }
 }  // namespace
 
+namespace {
+
+// ---- point-block Jacobi (PCVPBJACOBI on the 5 x 5 node blocks): invert each block once per preconditioner set-up, apply
+// y = B^-1 x per node in the Krylov precision.  One thread per node; the set-up kernel is Gauss-Jordan with partial
+// pivoting in FP64 (a block whose pivot vanishes or is not finite is counted in *singular and replaced by the identity).
+template <typename TO>
+__global__ void __launch_bounds__(kBS) k_pb_invert(const double *in, TO *out, int64_t nodes, int *singular) {  // in may equal out
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nodes; b += (int64_t)gridDim.x * blockDim.x) {
+    double A[5][10];
+#pragma unroll
+    for (int i = 0; i < 5; i++)
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        A[i][j]     = in[b * 25 + i * 5 + j];
+        A[i][5 + j] = i == j ? 1.0 : 0.0;
+      }
+    bool ok = true;
+    for (int c = 0; c < 5 && ok; c++) {
+      int pr = c;
+      for (int r = c + 1; r < 5; r++)
+        if (fabs(A[r][c]) > fabs(A[pr][c])) pr = r;
+      if (!(fabs(A[pr][c]) > 0.0) || !isfinite(A[pr][c])) {
+        ok = false;
+        break;
+      }
+      if (pr != c)
+        for (int j = 0; j < 10; j++) {
+          const double t = A[c][j];
+          A[c][j]         = A[pr][j];
+          A[pr][j]        = t;
+        }
+      const double inv = 1.0 / A[c][c];
+      for (int j = 0; j < 10; j++) A[c][j] *= inv;
+      for (int r = 0; r < 5; r++)
+        if (r != c) {
+          const double f = A[r][c];
+          for (int j = 0; j < 10; j++) A[r][j] -= f * A[c][j];
+        }
+    }
+    if (!ok) atomicAdd(singular, 1);
+#pragma unroll
+    for (int i = 0; i < 5; i++)
+#pragma unroll
+      for (int j = 0; j < 5; j++) out[b * 25 + i * 5 + j] = (TO)(ok ? A[i][5 + j] : (i == j ? 1.0 : 0.0));
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBS) k_pb_apply(const T *__restrict__ inv, const T *__restrict__ x, T *__restrict__ y, int64_t nodes) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nodes; b += (int64_t)gridDim.x * blockDim.x) {
+    T xv[5], yv[5];
+#pragma unroll
+    for (int j = 0; j < 5; j++) xv[j] = x[b * 5 + j];
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+      T acc = 0;
+#pragma unroll
+      for (int j = 0; j < 5; j++) acc += inv[b * 25 + i * 5 + j] * xv[j];
+      yv[i] = acc;
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++) y[b * 5 + i] = yv[i];
+  }
+}
+
+template <typename TO>
+int pb_invert(const double *blocks, TO *inv, int64_t nodes, int *d_singular, int *h_singular, void *s) {
+  cudaStream_t st = (cudaStream_t)s;
+  if (!blocks || !inv || !d_singular || nodes < 0) return HB_ERROR_INVALID;
+  if (cudaMemsetAsync(d_singular, 0, sizeof(int), st) != cudaSuccess) return HB_ERROR_CUDA;
+  if (nodes) k_pb_invert<TO><<<nblocks(nodes), kBS, 0, st>>>(blocks, inv, nodes, d_singular);
+  if (cudaGetLastError() != cudaSuccess) return HB_ERROR_CUDA;
+  if (h_singular) {
+    if (cudaMemcpyAsync(h_singular, d_singular, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+      return HB_ERROR_CUDA;
+  }
+  return HB_SUCCESS;
+}
+
+}  // namespace
+
 extern "C" {
 
 int hb_krylov_multidot_f64(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_partial, double *d_out, void *s) {
@@ -509,6 +590,23 @@ int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, cons
   minmax[0] = mn * dt;
   minmax[1] = mx * dt;
   return err ? HB_ERROR_CUDA : HB_SUCCESS;
+}
+
+int hb_pb_invert_f64(const double *blocks, double *inv, int64_t nodes, int *d_singular, int *h_singular, void *s) {
+  return pb_invert<double>(blocks, inv, nodes, d_singular, h_singular, s);
+}
+int hb_pb_invert_f64_to_f32(const double *blocks, float *inv, int64_t nodes, int *d_singular, int *h_singular, void *s) {
+  return pb_invert<float>(blocks, inv, nodes, d_singular, h_singular, s);
+}
+int hb_pb_apply_f64(const double *inv, const double *x, double *y, int64_t nodes, void *s) {
+  if (!inv || !x || !y || x == y) return HB_ERROR_INVALID;
+  if (nodes) k_pb_apply<double><<<nblocks(nodes), kBS, 0, (cudaStream_t)s>>>(inv, x, y, nodes);
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+int hb_pb_apply_f32(const float *inv, const float *x, float *y, int64_t nodes, void *s) {
+  if (!inv || !x || !y || x == y) return HB_ERROR_INVALID;
+  if (nodes) k_pb_apply<float><<<nblocks(nodes), kBS, 0, (cudaStream_t)s>>>(inv, x, y, nodes);
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
 }  // extern "C"

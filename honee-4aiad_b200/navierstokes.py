@@ -135,11 +135,14 @@ def main(argv=None):
     ap.add_argument("--both", action="store_true", help="run FP64 and mixed and compare the monitors")
     ap.add_argument("--monitor-every", type=int, default=10)
     ap.add_argument("--csv", default=None, help="write the monitor rows of each run here (suffix _fp64 / _mixed)")
+    ap.add_argument("--pc-type", default="jacobi", choices=["none", "jacobi", "vpbjacobi"], help="-pc_type of the Newton-Krylov solve")
     args = ap.parse_args(argv)
+    pc = {"none": 0, "jacobi": 1, "vpbjacobi": 2}[args.pc_type]
     variants = [False, True] if args.both else [args.mixed]
     runs = {}
     for mixed in variants:
-        r = run(args.problem, args.faces, args.degree, args.q_extra, args.steps, args.dt, args.cfl, mixed, args.monitor_every, log=sys.stderr)
+        r = run(args.problem, args.faces, args.degree, args.q_extra, args.steps, args.dt, args.cfl, mixed, args.monitor_every,
+                options={"pc_jacobi": pc}, log=sys.stderr)
         runs[mixed] = r
         tag = "mixed" if mixed else "fp64"
         if args.csv:

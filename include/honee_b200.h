@@ -151,7 +151,8 @@ typedef struct {
   int    newton_max_it;
   double ksp_rtol;        /* GMRES relative tolerance */
   int    ksp_max_it, gmres_restart;
-  int    pc_jacobi;       /* 1: Jacobi from the assembled diagonal, 0: none */
+  int    pc_jacobi;       /* 1: Jacobi from the assembled diagonal (-pc_type jacobi), 2: point-block Jacobi on the 5 x 5 node
+                             blocks (-pc_type vpbjacobi), 0: none */
   int    pc_every_newton; /* 0: diagonal once per time step (lagged), 1: every Newton iteration */
   int    jacobian_fp32;   /* mixed precision: FP32 Krylov basis, Jacobian action and diagonal; FP64 residual and update */
   int    cgs_refine;      /* 0: classical Gram-Schmidt once (PETSc default), 1: a second pass every iteration (CGS2) */
@@ -162,7 +163,8 @@ typedef struct {
 } HbSolverOptions;
 
 typedef struct {
-  int    newton_its, ksp_its, converged_reason; /* 1 converged, -1 non-finite residual, -2 iteration limit */
+  int    newton_its, ksp_its, converged_reason; /* 1 converged, -1 non-finite residual, -2 iteration limit,
+                                                   -3 preconditioner set-up failed (a singular point block) */
   double res0, res_final, seconds;
 } HbStepStats;
 
@@ -237,6 +239,14 @@ HB_EXPORT int hb_krylov_multidot_f64_static(const double *V, int64_t ldv, int k,
 HB_EXPORT int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f32_to_f64(double *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
+/* Point-block Jacobi (PCVPBJACOBI on 5 x 5 node blocks, row-major, as hb_point_block_diagonal_* writes them): invert every
+ * block in FP64 with partial pivoting (inv may equal blocks for the FP64 form); blocks with a vanishing pivot become the
+ * identity and are counted in *d_singular (a device int), copied to *h_singular when that is not NULL (synchronises s).
+ * Apply: y = B^-1 x per node (x and y must differ). */
+HB_EXPORT int hb_pb_invert_f64(const double *blocks, double *inv, int64_t nodes, int *d_singular, int *h_singular, void *s);
+HB_EXPORT int hb_pb_invert_f64_to_f32(const double *blocks, float *inv, int64_t nodes, int *d_singular, int *h_singular, void *s);
+HB_EXPORT int hb_pb_apply_f64(const double *inv, const double *x, double *y, int64_t nodes, void *s);
+HB_EXPORT int hb_pb_apply_f32(const float *inv, const float *x, float *y, int64_t nodes, void *s);
 HB_EXPORT int hb_bdf_qdot(const double *q, const double *z, double alpha, double *qdot, int64_t n, void *s);
 HB_EXPORT int hb_vec_combine_f64(const double *q1, const double *q2, double a, double b, double *z, int64_t n, void *s);
 
