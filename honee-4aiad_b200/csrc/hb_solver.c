@@ -45,6 +45,10 @@ struct HbTimeStepper {
   /* matrix-free (finite-difference) Jacobian action: perturbed state, rate and residual */
   double *qp, *qdp, *rp;
   /* optional free-stream boundary faces: residual and Jacobian sub-operators of the composite */
+  /* essential DOFs: L-vector indices and values (device) */
+  int32_t *ess_idx;
+  double  *ess_val, *ess_one;
+  int64_t  ess_n;
   /* point-block Jacobi (pc_jacobi 2): FP64 blocks, inverted in place (FP64) or into pb32 (mixed precision) */
   double *pb64;
   float  *pb32;
@@ -135,12 +139,16 @@ int hb_ts_destroy(HbTimeStepper *ts) {
   free(ts->sgs_w);
   if (ts->sgs_res) cudaFree(ts->sgs_res);
   if (ts->bc_jac) cudaFree(ts->bc_jac);
+  if (ts->ess_idx) cudaFree(ts->ess_idx);
+  if (ts->ess_val) cudaFree(ts->ess_val);
+  if (ts->ess_one) cudaFree(ts->ess_one);
   free(ts);
   return HB_SUCCESS;
 }
 
 int hb_ts_set_state(HbTimeStepper *ts, const double *d_q, double t) {
   CUCK(cudaMemcpyAsync(ts->q, d_q, sizeof(double) * (size_t)ts->n, cudaMemcpyDeviceToDevice, ts->s));
+  if (ts->ess_n) HBCK(hb_constrain_set_f64(ts->q, ts->ess_idx, ts->ess_val, ts->ess_n, ts->s)); /* boundary values inserted */
   ts->t           = t;
   ts->steps_taken = 0;
   return HB_SUCCESS;
@@ -167,6 +175,30 @@ int hb_ts_set_freestream(HbTimeStepper *ts, const HbFaceOp *faces, const void *c
   ts->bc_flux  = flux_type;
   ts->bc_qdata = qdata_sur;
   return HB_SUCCESS;
+}
+
+int hb_ts_set_essential(HbTimeStepper *ts, const int32_t *h_idx, const double *h_val, int64_t n) {
+  if (!ts || n < 0 || (n && !h_idx)) return HB_ERROR_INVALID;
+  for (int64_t i = 0; i < n; i++)
+    if (h_idx[i] < 0 || h_idx[i] >= ts->n) return HB_ERROR_INVALID;
+  if (ts->ess_idx) cudaFree(ts->ess_idx);
+  if (ts->ess_val) cudaFree(ts->ess_val);
+  if (ts->ess_one) cudaFree(ts->ess_one);
+  ts->ess_idx = NULL;
+  ts->ess_val = ts->ess_one = NULL;
+  ts->ess_n   = 0;
+  if (!n) return HB_SUCCESS;
+  if (cudaMalloc((void **)&ts->ess_idx, sizeof(int32_t) * (size_t)n) != cudaSuccess ||
+      cudaMalloc((void **)&ts->ess_val, sizeof(double) * (size_t)n) != cudaSuccess ||
+      cudaMalloc((void **)&ts->ess_one, sizeof(double) * (size_t)n) != cudaSuccess)
+    return HB_ERROR_NOMEM;
+  HBCK(hb_vec_set_f64(ts->ess_one, n, 1.0, ts->s));
+  CUCK(cudaMemcpy(ts->ess_idx, h_idx, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice));
+  if (h_val) CUCK(cudaMemcpy(ts->ess_val, h_val, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice));
+  else CUCK(cudaMemset(ts->ess_val, 0, sizeof(double) * (size_t)n));
+  ts->ess_n = n;
+  /* the current state takes the boundary values */
+  return hb_constrain_set_f64(ts->q, ts->ess_idx, ts->ess_val, n, ts->s);
 }
 
 int hb_ts_set_sgs(HbTimeStepper *ts, const HbMlpDesc *d, const float *h_weights) {
@@ -202,11 +234,15 @@ static int kv_copy(HbTimeStepper *ts, void *dst, const void *src) {
 /* y = J x (the IJacobian operator at the current linearisation point) */
 /* residual F(q, q_dot) of the current model (with the closure when attached and not lagged), without Jacobian data */
 static int residual(HbTimeStepper *ts, const double *q, const double *qdot, double *out, double *jd64, float *jd32) {
+  /* constrained DOFs: the rate is zero there (PETSc never writes them into the local rate vector) */
+  if (ts->ess_n) HBCK(hb_constrain_set_f64((double *)qdot, ts->ess_idx, NULL, ts->ess_n, ts->s));
   HbIFunctionIO io = {q, qdot, ts->qdata, jd64, jd32, out, 0};
   if (ts->sgs_w && !(ts->o.sgs_lagged && !ts->o.jfnk)) HBCK(hb_ifunction_apply_sgs(ts->op, &ts->ctx, &io, &ts->sgs_desc, ts->sgs_w, ts->s));
   else HBCK(hb_ifunction_apply(ts->op, &ts->ctx, &io, ts->s));
   /* boundary faces add their flux; the state at the face points is kept only for the Newton iterate's Jacobian */
   if (ts->bc) HBCK(hb_freestream_apply(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, q, (jd64 || jd32) ? ts->bc_jac : NULL, out, ts->s));
+  /* constrained rows are not part of the system (DMLocalToGlobal drops them) */
+  if (ts->ess_n) HBCK(hb_constrain_set_f64(out, ts->ess_idx, NULL, ts->ess_n, ts->s));
   return HB_SUCCESS;
 }
 
@@ -233,10 +269,12 @@ static int kv_jac(HbTimeStepper *ts, const void *x, void *y) {
   if (ts->o.jacobian_fp32) {
     HBCK(hb_ijacobian_apply_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (const float *)x, (float *)y, 0, ts->s));
     if (ts->bc) HBCK(hb_freestream_jacobian_apply_f32(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, (const float *)x, (float *)y, ts->s));
+    if (ts->ess_n) HBCK(hb_constrain_set_f32((float *)y, ts->ess_idx, NULL, ts->ess_n, ts->s));
     return HB_SUCCESS;
   }
   HBCK(hb_ijacobian_apply_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, (const double *)x, (double *)y, 0, ts->s));
   if (ts->bc) HBCK(hb_freestream_jacobian_apply(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, (const double *)x, (double *)y, ts->s));
+  if (ts->ess_n) HBCK(hb_constrain_set_f64((double *)y, ts->ess_idx, NULL, ts->ess_n, ts->s));
   return HB_SUCCESS;
 }
 /* z = M^-1 x (Jacobi) or copy */
@@ -276,6 +314,7 @@ static int assemble_pc(HbTimeStepper *ts, int *failed) {
       HBCK(hb_point_block_diagonal_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, ts->pb64, 0, ts->s));
     }
     if (ts->bc) HBCK(hb_freestream_point_block_diagonal(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, ts->pb64, ts->s));
+    if (ts->ess_n) HBCK(hb_pb_constrain(ts->pb64, ts->ess_idx, ts->ess_n, ts->s));
     if (ts->o.jacobian_fp32) HBCK(hb_pb_invert_f64_to_f32(ts->pb64, ts->pb32, nodes, ts->d_sing, &sing, ts->s));
     else HBCK(hb_pb_invert_f64(ts->pb64, ts->pb64, nodes, ts->d_sing, &sing, ts->s));
     *failed = sing > 0;
@@ -286,11 +325,13 @@ static int assemble_pc(HbTimeStepper *ts, int *failed) {
     /* invert in FP64 (delta is free before the Krylov solve), store FP32 */
     HBCK(hb_vec_f32_to_f64((const float *)ts->diag, ts->delta, ts->n, 0, ts->s));
     if (ts->bc) HBCK(hb_freestream_diagonal(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, ts->delta, ts->s));
+    if (ts->ess_n) HBCK(hb_constrain_set_f64(ts->delta, ts->ess_idx, ts->ess_one, ts->ess_n, ts->s)); /* identity rows */
     HBCK(hb_vec_reciprocal_f64(ts->delta, ts->n, ts->s));
     return hb_vec_f64_to_f32(ts->delta, (float *)ts->diag, ts->n, 0, ts->s);
   }
   HBCK(hb_diagonal_assemble_f64(ts->op, &ts->ctx, ts->qdata, ts->jd64, (double *)ts->diag, 0, ts->s));
   if (ts->bc) HBCK(hb_freestream_diagonal(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, (double *)ts->diag, ts->s));
+  if (ts->ess_n) HBCK(hb_constrain_set_f64((double *)ts->diag, ts->ess_idx, ts->ess_one, ts->ess_n, ts->s)); /* identity rows */
   return hb_vec_reciprocal_f64((double *)ts->diag, ts->n, ts->s);
 }
 
@@ -438,6 +479,7 @@ int hb_ts_step(HbTimeStepper *ts, HbStepStats *st) {
     HbIFunctionIO io = {ts->q, ts->qdot, ts->qdata, ts->o.jacobian_fp32 ? NULL : ts->jd64, ts->o.jacobian_fp32 ? (float *)ts->jd32 : NULL, ts->res, 0};
     HBCK(residual(ts, io.q, io.q_dot, io.v, io.jac_data, io.jac_data_f32));
     if (sgs_lag) HBCK(hb_vec_axpy_f64(ts->res, 1.0, ts->sgs_res, ts->n, ts->s));
+    if (sgs_lag && ts->ess_n) HBCK(hb_constrain_set_f64(ts->res, ts->ess_idx, NULL, ts->ess_n, ts->s));
     double r2;
     HBCK(hb_vec_reduce_f64(ts->res, NULL, ts->n, 1, ts->scratch, &r2, ts->s));
     rn = sqrt(r2);

@@ -1450,9 +1450,9 @@ static int launch_blockdiag(const HbElemOp *op, const HbNewtonianContext &ctx, c
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
-// (P, Q) pairs compiled: polynomial degree 1..5 with q_extra 0 or 1 (Q = P or P + 1); the benchmark configurations use
-// (3,3), (4,5) and (5,6).
-#define HB_PQ_LIST(X) X(2, 2) X(2, 3) X(3, 3) X(3, 4) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7)
+// (P, Q) pairs compiled: polynomial degree 1..5 with q_extra 0 or 1 (Q = P or P + 1), and q_extra 2 for degrees 1 and 2
+// (the channel example's q_extra 2); the benchmark configurations use (3,3), (4,5) and (5,6).
+#define HB_PQ_LIST(X) X(2, 2) X(2, 3) X(2, 4) X(3, 3) X(3, 4) X(3, 5) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7)
 // bases the residual with the fused SGS closure is built for (the coarse LES runs at degree 2 and 3)
 #define HB_SGS_PQ_LIST(X) X(3, 3) X(3, 4) X(4, 5)
 

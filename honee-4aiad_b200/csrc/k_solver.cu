@@ -466,6 +466,26 @@ int pb_invert(const double *blocks, TO *inv, int64_t nodes, int *d_singular, int
   return HB_SUCCESS;
 }
 
+// ---- essential (Dirichlet) DOFs: the constrained entries of the node-interleaved L-vector, which PETSc's DMPlex section
+// removes from the global system (the values are inserted into the local state, DMPlexInsertBoundaryValues)
+template <typename T>
+__global__ void k_constrain_set(T *__restrict__ x, const int32_t *__restrict__ idx, const double *__restrict__ val, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[idx[i]] = val ? (T)val[i] : T(0);
+}
+// rows and columns of the constrained components become those of the identity in their node's 5 x 5 block (two threads of
+// one node only ever write the same value to an entry they share)
+__global__ void k_pb_constrain(double *__restrict__ blocks, const int32_t *__restrict__ idx, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t node = idx[i] / 5, c = idx[i] % 5;
+    double *b = blocks + node * 25;
+    for (int k = 0; k < 5; k++) {
+      b[c * 5 + k] = 0.0;
+      b[k * 5 + c] = 0.0;
+    }
+    b[c * 6] = 1.0;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -606,6 +626,22 @@ int hb_pb_apply_f64(const double *inv, const double *x, double *y, int64_t nodes
 int hb_pb_apply_f32(const float *inv, const float *x, float *y, int64_t nodes, void *s) {
   if (!inv || !x || !y || x == y) return HB_ERROR_INVALID;
   if (nodes) k_pb_apply<float><<<nblocks(nodes), kBS, 0, (cudaStream_t)s>>>(inv, x, y, nodes);
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+
+int hb_constrain_set_f64(double *x, const int32_t *idx, const double *val, int64_t n, void *s) {
+  if (n < 0 || (n && (!x || !idx))) return HB_ERROR_INVALID;
+  if (n) k_constrain_set<double><<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(x, idx, val, n);
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+int hb_constrain_set_f32(float *x, const int32_t *idx, const double *val, int64_t n, void *s) {
+  if (n < 0 || (n && (!x || !idx))) return HB_ERROR_INVALID;
+  if (n) k_constrain_set<float><<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(x, idx, val, n);
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+int hb_pb_constrain(double *blocks, const int32_t *idx, int64_t n, void *s) {
+  if (n < 0 || (n && (!blocks || !idx))) return HB_ERROR_INVALID;
+  if (n) k_pb_constrain<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(blocks, idx, n);
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 

@@ -345,6 +345,58 @@ def taylor_green_context(degree: int, *, L=2 * math.pi, Re=1600., Ma=0.1, rho0=1
 
 
 # --------------------------------------------------------------------------------------------------------------------
+# channel flow (problems/channel.c:73-150, qfunctions/channel.h): Poiseuille initial state, body force, no-slip walls
+
+class ChannelContext(C.Structure):
+    """struct ChannelContext_ (qfunctions/channel.h:13-22)."""
+    _fields_ = [("implicit", C.c_bool), ("theta0", C.c_double), ("P0", C.c_double), ("umax", C.c_double), ("center", C.c_double),
+                ("H", C.c_double), ("B", C.c_double), ("newt_ctx", NewtonianContext)]
+
+
+def channel_context(newt: NewtonianContext, lo, hi, *, umax=10.0, theta0=300.0, P0=1.0e5, body_force_scale=1.0, implicit=True):
+    """NS_CHANNEL (problems/channel.c:73-137): half-height H and centre from the box's y extent, body force
+    B = scale * 2 umax mu / H^2 applied as the gravity g = (B / rho0, 0, 0) of the Newtonian context (rho0 = P0 / (R theta0))."""
+    H = 0.5 * (hi[1] - lo[1])
+    center = H + lo[1]
+    gas = newt.gas
+    B = body_force_scale * 2 * umax * gas.mu / (H * H)
+    rho = P0 / ((gas.cp - gas.cv) * theta0)
+    newt.g[:] = [B / rho, 0.0, 0.0]
+    return ChannelContext(bool(implicit), theta0, P0, umax, center, H, B, newt)
+
+
+def channel_state(mesh: BoxMesh, basis: TensorBasis, ch: ChannelContext) -> np.ndarray:
+    """ICsChannel (qfunctions/channel.h:24-73) at the nodes: pressure P0, velocity umax (1 - ((y - c)/H)^2) along x, temperature
+    theta0 (1 + Pr Ec / 3 (1 - ((y - c)/H)^4)) with Pr = mu / (cp k) and Ec = umax^2 / (cp theta0) as the reference writes them."""
+    X = node_coordinates(mesh, basis)
+    gas = ch.newt_ctx.gas
+    eta = (X[1] - ch.center) / ch.H
+    Pr = gas.mu / (gas.cp * gas.k)
+    Ec = ch.umax ** 2 / (gas.cp * ch.theta0)
+    theta = ch.theta0 * (1 + (Pr * Ec / 3) * (1 - eta ** 4))
+    u = np.stack([ch.umax * (1 - eta ** 2), 0 * eta, 0 * eta])
+    q = conservative_from_primitive(gas, ch.P0 * np.ones_like(eta), u, theta)
+    return np.ascontiguousarray(q.T.reshape(-1))
+
+
+def box_essential(mesh: BoxMesh, sides: dict):
+    """Essential DOFs of box sides: {"y-": (1, 2, 3), ...} -> sorted unique L-vector indices node * 5 + component (the
+    bc_*_essential_comps of HONEE's options; PETSc's box face sets 1/2 are z-/z+, 3/4 y-/y+, 5/6 x+/x-)."""
+    N = mesh.node_dims
+    ijk = np.stack(np.meshgrid(np.arange(N[0]), np.arange(N[1]), np.arange(N[2]), indexing="ij"), axis=-1).reshape(-1, 3)
+    node = ijk[:, 0] + N[0] * (ijk[:, 1] + N[1] * ijk[:, 2])
+    idx = []
+    for side, comps in sides.items():
+        ax = "xyz".index(side[0])
+        if mesh.periodic[ax]:
+            raise ValueError(f"side {side} is periodic")
+        at = ijk[:, ax] == (N[ax] - 1 if side[1] == "+" else 0)
+        for c in comps:
+            idx.append(node[at] * 5 + c)
+    return np.unique(np.concatenate(idx)).astype(np.int32)
+
+
+# --------------------------------------------------------------------------------------------------------------------
 # boundary faces of a box mesh and the free-stream context
 
 _FACE_AXES = {  # side -> (normal axis, at upper end, tangent axis X0, tangent axis X1) with cross(X0, X1) outward

@@ -81,6 +81,17 @@ class TimeStepper:
         self._bc = (faceop, C.create_string_buffer(bytes(ctx264), len(ctx264)))
         _chk(_load().hb_ts_set_freestream(self.ptr, faceop.ptr, self._bc[1], C.c_int(flux_type), _addr(faceop.qdata)), "hb_ts_set_freestream")
 
+    def set_essential(self, idx=None, values=None):
+        """Strong Dirichlet DOFs (L-vector indices node * 5 + component, values default 0), or none (no arguments)."""
+        L = _load()
+        if idx is None or len(idx) == 0:
+            _chk(L.hb_ts_set_essential(self.ptr, None, None, C.c_int64(0)), "hb_ts_set_essential")
+            return
+        i = np.ascontiguousarray(idx, dtype=np.int32)
+        v = None if values is None else np.ascontiguousarray(values, dtype=np.float64)
+        _chk(L.hb_ts_set_essential(self.ptr, i.ctypes.data_as(C.POINTER(C.c_int32)), None if v is None else v.ctypes.data_as(C.POINTER(C.c_double)),
+                                   C.c_int64(i.size)), "hb_ts_set_essential")
+
     def set_sgs(self, desc=None, weights=None):
         """Fuse the learned closure (sgs.HbMlpDesc, float32 weights) into the residual, or remove it (no arguments)."""
         if desc is None:

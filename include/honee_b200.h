@@ -247,6 +247,12 @@ HB_EXPORT int hb_pb_invert_f64(const double *blocks, double *inv, int64_t nodes,
 HB_EXPORT int hb_pb_invert_f64_to_f32(const double *blocks, float *inv, int64_t nodes, int *d_singular, int *h_singular, void *s);
 HB_EXPORT int hb_pb_apply_f64(const double *inv, const double *x, double *y, int64_t nodes, void *s);
 HB_EXPORT int hb_pb_apply_f32(const float *inv, const float *x, float *y, int64_t nodes, void *s);
+/* Essential (Dirichlet) DOFs, given as indices idx[n] into the node-interleaved L-vector (node * 5 + component): x[idx[i]] =
+ * val[i] (0 when val is NULL); hb_pb_constrain turns the constrained rows and columns of the 5 x 5 node blocks into those
+ * of the identity, so a block preconditioner leaves constrained entries at zero. */
+HB_EXPORT int hb_constrain_set_f64(double *x, const int32_t *idx, const double *val, int64_t n, void *s);
+HB_EXPORT int hb_constrain_set_f32(float *x, const int32_t *idx, const double *val, int64_t n, void *s);
+HB_EXPORT int hb_pb_constrain(double *blocks, const int32_t *idx, int64_t n, void *s);
 HB_EXPORT int hb_bdf_qdot(const double *q, const double *z, double alpha, double *qdot, int64_t n, void *s);
 HB_EXPORT int hb_vec_combine_f64(const double *q1, const double *q2, double a, double b, double *z, int64_t n, void *s);
 
@@ -375,6 +381,11 @@ HB_EXPORT int hb_freestream_point_block_diagonal(const HbFaceOp *op, const void 
 HB_EXPORT int hb_freestream_jacobian_apply_f32(const HbFaceOp *op, const void *ctx264, int flux_type, const double *qdata_sur,
                                                const double *jac_data_sur, const float *dq, float *v, void *s);
 
+/* Essential boundary conditions (strong Dirichlet values, as HONEE's bc_*_essential_comps / essential_values insert them
+ * through DMPlexInsertBoundaryValues, src/setupts.c:16-25, with the DOFs removed from the global system): h_idx[n] L-vector
+ * indices (node * 5 + component) and their values (NULL: zero).  The state takes the values, the rate is zero there, and
+ * the residual, the Jacobian rows and the preconditioner act only on the free DOFs.  n = 0 removes them. */
+HB_EXPORT int hb_ts_set_essential(HbTimeStepper *ts, const int32_t *h_idx, const double *h_val, int64_t n);
 /* Attach (faces != NULL) or detach the free-stream boundary to a time stepper: its flux joins every residual, its
  * tangent every Krylov product (FP32 in mixed precision) and its diagonal the Jacobi preconditioner (FP64). */
 HB_EXPORT int hb_ts_set_freestream(HbTimeStepper *ts, const HbFaceOp *faces, const void *ctx264, int flux_type, const double *qdata_sur);

@@ -10,6 +10,8 @@ Outputs (committed; the GPU box has no reference tree):
                             it (examples/navierstokes.c:222, examples/taylor_green_vortex.yaml)
   unit_state.json           the UnitTests_Newtonian inputs and tolerances (problems/newtonian.c:947-987) with the
                             reference's StateToQ outputs for every (A, B) pair
+  channel_be5.npz           the free DOFs of the final state of the "Channel" run (examples/navierstokes.c:252:
+                            examples/channel.yaml, 5 x 5 x 1 faces, 5 backward-Euler steps), tests/output/channel.bin
   taylorgreen_rk4.npz       every row of tests/output/taylorgreen_totalke.csv (steps 0, 2, 3 of the explicit RK4 run of
                             examples/navierstokes.c:222) and the final state of that run, tests/output/taylor-green.bin
                             (HONEE binary format, src/honee-file.c:194-217: int32 token, int32 step, float64 time, then a
@@ -130,6 +132,18 @@ def main():
                         ke=table[:, 2:], ke_names=np.array(names), final_step=np.int64(step), final_time=np.float64(t_final),
                         final_state=state, dt=np.float64(2e-3), tableau=np.array("4"), mass_ksp=np.array("gmres"),
                         mass_pc_jacobi=np.array("diagonal"), source=np.array("tests/output/taylorgreen_totalke.csv, tests/output/taylor-green.bin"))
+
+    # ---- Channel run (examples/navierstokes.c:252): free DOFs of the final state
+    raw = open(os.path.join(args.ref, "tests/output/channel.bin"), "rb").read()
+    token, step = np.frombuffer(raw[:8], dtype=">i4")
+    t_final = np.frombuffer(raw[8:16], dtype=">f8")[0]
+    classid, length = np.frombuffer(raw[16:24], dtype=">i4")
+    assert len(raw) == 24 + 8 * int(length) and int(classid) == 1211214
+    np.savez_compressed(os.path.join(HERE, "channel_be5.npz"), final_step=np.int64(step), final_time=np.float64(t_final),
+                        free_state=np.frombuffer(raw[24:], dtype=">f8").astype(np.float64), faces=np.array([5, 5, 1]), degree=np.int64(1),
+                        q_extra=np.int64(2), box_hi=np.array([0.01, 0.01, 0.001]), mu=np.float64(0.01), umax=np.float64(40.0),
+                        dt=np.float64(5e-6), steps=np.int64(5), essential=np.array("y-:1,2,3 y+:1,2,3 z-:3 z+:3"), compare_atol=np.float64(2e-11),
+                        source=np.array("tests/output/channel.bin (examples/navierstokes.c:252, examples/channel.yaml)"))
 
     # ---- UnitTests_Newtonian inputs (problems/newtonian.c:947-987) and reference StateToQ outputs
     ctx = prob.newtonian_context(2)

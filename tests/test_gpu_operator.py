@@ -150,7 +150,7 @@ def test_unsupported_qfunction_fails_loudly():
     basis = prob.tensor_basis(3, 3)
     b = ce.Basis(ceed, 3, 5, 3, 3, basis.interp1d, basis.grad1d, basis.qref1d, basis.qweight1d)
     r = ce.ElemRestriction(ceed, 1, 27, 5, 1, mesh.l_size, offsets=mesh.offsets)
-    qf = ce.QFunction(ceed, "newtonian.h:RHSFunction_Newtonian")
+    qf = ce.QFunction(ceed, "advection.h:RHSFunction_Advection")
     qf.add_input("q", 5, ce.CEED_EVAL_INTERP)
     qf.add_output("v", 5, ce.CEED_EVAL_INTERP)
     op = ce.Operator(ceed, qf)
