@@ -119,7 +119,7 @@ typedef struct {
   int                 set;
 } OpField;
 
-enum { PLAN_NONE = 0, PLAN_SETUP, PLAN_IFUNCTION, PLAN_IJACOBIAN, PLAN_SETUP_SUR, PLAN_FREESTREAM, PLAN_FREESTREAM_JAC, PLAN_RHS, PLAN_MASS };
+enum { PLAN_NONE = 0, PLAN_SETUP, PLAN_IFUNCTION, PLAN_IJACOBIAN, PLAN_SETUP_SUR, PLAN_FREESTREAM, PLAN_FREESTREAM_JAC, PLAN_RHS, PLAN_MASS, PLAN_MASS_STAB };
 
 struct CeedOperator_private {
   Ceed          ceed;
@@ -1584,6 +1584,23 @@ static int op_plan(CeedOperator op) {
     op->plan = PLAN_MASS;
     return CEED_ERROR_SUCCESS;
   }
+  if (!strcmp(k, "MassFunction_Newtonian_Conserv")) {
+    /* CreateKSPMassOperator_NewtonianStabilized (problems/newtonian.c:212-265): q_dot (active, INTERP), q (passive, INTERP),
+     * qdata (NONE) -> v (INTERP), Grad_v (GRAD) */
+    if (qf->nin != 3 || qf->nout != 2 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[1].emode != CEED_EVAL_INTERP ||
+        qf->in[2].emode != CEED_EVAL_NONE || qf->in[2].size != 10 || qf->out[0].emode != CEED_EVAL_INTERP || qf->out[1].emode != CEED_EVAL_GRAD)
+      return plan_fail(op, "unexpected stabilized-mass field layout (problems/newtonian.c:244-256)");
+    if (op->in[0].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE || op->out[1].v != CEED_VECTOR_ACTIVE)
+      return plan_fail(op, "q_dot, v and Grad_v must be active");
+    if (!op->in[1].v || op->in[1].v == CEED_VECTOR_ACTIVE || op->in[1].v == CEED_VECTOR_NONE) return plan_fail(op, "the state q must be a passive vector");
+    if (op->in[0].r != op->in[1].r || op->in[0].r != op->out[0].r || op->in[0].r != op->out[1].r) return plan_fail(op, "shared restriction expected");
+    if (op->in[0].b != op->in[1].b || op->in[0].b != op->out[0].b || op->in[0].b != op->out[1].b) return plan_fail(op, "shared basis expected");
+    if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+    CK(plan_elemop(op, op->in[0].r, op->in[0].b));
+    CK(check_qdata_rstr(op, op->in[2].r, 10, op->eop->Q * op->eop->Q * op->eop->Q, "qdata"));
+    op->plan = PLAN_MASS_STAB;
+    return CEED_ERROR_SUCCESS;
+  }
   if (!strcmp(k, "SetupBoundary")) {
     /* inputs "dx" (GRAD of the face coordinates), "weight" (WEIGHT); output "surface qdata" (NONE, 10, strided) --
      * QDataBoundaryGet, src/qdata.c:228-261 */
@@ -1648,7 +1665,15 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
         CK(vec_dev_write(op->out[1].v, &jd, 1));
       }
       CK(vec_dev_write(out, &v, 0));
-      HB_CK(ceed, hb_freestream_apply(op->fop, op->qf->ctx->data, op->flux_type, qd, q, jd, v, s));
+      if (((const HbFreestreamContext *)op->qf->ctx->data)->newt.is_implicit) {
+        HB_CK(ceed, hb_freestream_apply(op->fop, op->qf->ctx->data, op->flux_type, qd, q, jd, v, s));
+      } else {
+        /* explicit (RHS) form: the QFunction returns -wdetJb F (bc_freestream.h:45-48) */
+        if (!op->d_tmp_rhs) CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_rhs, sizeof(double) * (size_t)n));
+        CUDA_CK(ceed, cudaMemsetAsync(op->d_tmp_rhs, 0, sizeof(double) * (size_t)n, s));
+        HB_CK(ceed, hb_freestream_apply(op->fop, op->qf->ctx->data, op->flux_type, qd, q, NULL, op->d_tmp_rhs, s));
+        HB_CK(ceed, hb_vec_axpy_f64(v, -1.0, op->d_tmp_rhs, n, s));
+      }
       return CEED_ERROR_SUCCESS;
     }
     case PLAN_FREESTREAM_JAC: {
@@ -1695,6 +1720,21 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
       double *v;
       CK(vec_dev_write(out, &v, 0));
       HB_CK(ceed, hb_vec_axpy_f64(v, -1.0, op->d_tmp_rhs, n, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_MASS_STAB: {
+      const int64_t n = op->eop->l_size;
+      CK(need_len(op, in, n, "input"));
+      CK(need_len(op, out, n, "output"));
+      CK(need_len(op, op->in[1].v, n, "state"));
+      CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
+      const double *u, *qs, *qd;
+      double       *v;
+      CK(vec_dev_read(in, &u));
+      CK(vec_dev_read(op->in[1].v, &qs));
+      CK(vec_dev_read(op->in[2].v, &qd));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_mass_stab_apply(op->eop, op->qf->ctx->data, qd, qs, u, v, 1, s));
       return CEED_ERROR_SUCCESS;
     }
     case PLAN_MASS: {
@@ -1829,6 +1869,18 @@ static int op_diag_add_single(CeedOperator op, CeedVector assembled) {
     CK(vec_dev_read(op->in[4].v, &jd));
     CK(vec_dev_write(assembled, &y, 0));
     HB_CK(op->ceed, hb_freestream_diagonal(op->fop, op->qf->ctx->data, op->flux_type, qd, jd, y, op->ceed->stream));
+    return CEED_ERROR_SUCCESS;
+  }
+  if (op->plan == PLAN_MASS_STAB) {
+    CK(need_len(op, assembled, op->eop->l_size, "diagonal"));
+    CK(need_len(op, op->in[1].v, op->eop->l_size, "state"));
+    CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
+    const double *qs, *qd;
+    double       *y;
+    CK(vec_dev_read(op->in[1].v, &qs));
+    CK(vec_dev_read(op->in[2].v, &qd));
+    CK(vec_dev_write(assembled, &y, 0));
+    HB_CK(op->ceed, hb_mass_stab_diagonal(op->eop, op->qf->ctx->data, qd, qs, y, 1, op->ceed->stream));
     return CEED_ERROR_SUCCESS;
   }
   if (op->plan == PLAN_MASS) {
@@ -2074,6 +2126,7 @@ static void op_view(CeedOperator op, FILE *stream, int terse, int depth) {
           : op->plan == PLAN_FREESTREAM_JAC ? "free-stream faces Jacobian"
           : op->plan == PLAN_RHS       ? "explicit right-hand side"
           : op->plan == PLAN_MASS      ? "mass"
+          : op->plan == PLAN_MASS_STAB ? "stabilized mass"
                                        : "not planned");
   if (terse) return;
   for (int o = 0; o < 2; o++)

@@ -4,7 +4,9 @@
  * HONEE's explicit path (-ts_type rk): RHS_NS (src/setupts.c:31-75) applies the RHSFunction_Newtonian operator
  * (qfunctions/newtonian.h:133-202) and solves with the "mass_" KSP that CreateKSPMass builds (src/setuplibceed.c:15-93):
  * KSPPREONLY + PCJacobi row sum by default ("lumped"), or e.g. GMRES + PCJacobi diagonal from the options file
- * (examples/taylor_green_vortex.yaml).  PETSc's TSRK and KSPGMRES are not part of this project, so the loop is restated
+ * (examples/taylor_green_vortex.yaml).  With stab = supg the mass operator is the SUPG-stabilized one
+ * (MassFunction_Newtonian, problems/newtonian.c:212-265, 795), linearised at the state of each right-hand side; the Jacobi
+ * preconditioner is set up at the first solve and kept (the MatCEED object PETSc sees never changes state).  PETSc's TSRK and KSPGMRES are not part of this project, so the loop is restated
  * here on device buffers.
  *
  * The right-hand side is the IFunction kernel at q_dot = 0 with the sign reversed: the IFunction integrand
@@ -37,6 +39,18 @@ struct HbExplicitStepper {
   cudaStream_t       s;
   double *q, *y, *f, *zero, *dinv, *K; /* K: stage block [stages][ldv] */
   double *V, *w, *r, *scratch, *d_partial, *d_dots;
+  /* stabilized mass (stab = supg): the state it is linearised at, and whether the Jacobi set-up has run */
+  int           mass_stab, pc_ready;
+  const double *qstate;
+  /* essential DOFs (device indices and values) */
+  int32_t *ess_idx;
+  double  *ess_val, *ess_one;
+  int64_t  ess_n;
+  /* free-stream faces: their flux joins the right-hand side */
+  const HbFaceOp *bc;
+  unsigned char   bc_ctx[sizeof(HbFreestreamContext)];
+  int             bc_flux;
+  const double   *bc_qdata;
 };
 
 #define CUCK(x)                                   \
@@ -75,20 +89,36 @@ static int norm2(HbExplicitStepper *ex, const double *x, double *nrm) {
   return HB_SUCCESS;
 }
 
+/* constrained entries leave the system (DMLocalToGlobal drops them): zero them */
+static int mask(HbExplicitStepper *ex, double *x) { return ex->ess_n ? hb_constrain_set_f64(x, ex->ess_idx, NULL, ex->ess_n, ex->s) : HB_SUCCESS; }
+
+/* w = M x: Mass_5, or the stabilized mass at the current right-hand side's state */
+static int mass(HbExplicitStepper *ex, const double *x, double *w) {
+  if (ex->mass_stab) return hb_mass_stab_apply(ex->op, &ex->ctx, ex->qdata, ex->qstate, x, w, 0, ex->s);
+  return hb_mass_apply(ex->op, ex->qdata, x, w, 0, ex->s);
+}
+
 /* w = D^-1 M x */
 static int pmass(HbExplicitStepper *ex, const double *x, double *w) {
-  HBCK(hb_mass_apply(ex->op, ex->qdata, x, w, 0, ex->s));
+  HBCK(mass(ex, x, w));
+  HBCK(mask(ex, w));
   return hb_vec_pointwise_mult_f64(w, w, ex->dinv, ex->n, ex->s);
 }
 
-/* Jacobi from the mass diagonal or its row sums (M 1), stored inverted */
+/* Jacobi from the mass diagonal or its row sums, stored inverted.  The row sums are those of the free-DOF system (PETSc's
+ * MatGetRowSum multiplies the global, constrained-free matrix by ones); constrained rows get 1 (their residual is zero). */
 static int setup_jacobi(HbExplicitStepper *ex) {
   if (ex->o.mass_pc_rowsum) {
     HBCK(hb_vec_set_f64(ex->r, ex->n, 1.0, ex->s));
-    HBCK(hb_mass_apply(ex->op, ex->qdata, ex->r, ex->dinv, 0, ex->s));
+    HBCK(mask(ex, ex->r));
+    HBCK(mass(ex, ex->r, ex->dinv));
+  } else if (ex->mass_stab) {
+    HBCK(hb_mass_stab_diagonal(ex->op, &ex->ctx, ex->qdata, ex->qstate, ex->dinv, 0, ex->s));
   } else {
     HBCK(hb_mass_diagonal(ex->op, ex->qdata, ex->dinv, 0, ex->s));
   }
+  ex->pc_ready = 1;
+  if (ex->ess_n) HBCK(hb_constrain_set_f64(ex->dinv, ex->ess_idx, ex->ess_one, ex->ess_n, ex->s));
   return hb_vec_reciprocal_f64(ex->dinv, ex->n, ex->s);
 }
 
@@ -169,7 +199,8 @@ static int mass_gmres(HbExplicitStepper *ex, const double *b, double *x, int *it
     HBCK(hb_krylov_multiaxpy_f64(x, ex->V, ex->ldv, k, y, ex->n, ex->s));
     if (done || its >= ex->o.mass_max_it) break;
     /* restart: r = D^-1 (b - M x) */
-    HBCK(hb_mass_apply(ex->op, ex->qdata, x, ex->r, 0, ex->s));
+    HBCK(mass(ex, x, ex->r));
+    HBCK(mask(ex, ex->r));
     HBCK(hb_vec_axpby_f64(ex->r, -1.0, 1.0, b, ex->n, ex->s)); /* r = b - M x */
     HBCK(hb_vec_pointwise_mult_f64(v0, ex->r, ex->dinv, ex->n, ex->s));
     HBCK(norm2(ex, v0, &beta));
@@ -192,6 +223,17 @@ static int neg_rhs(HbExplicitStepper *ex, const double *q, double t, double *out
   ex->ctx.time = t;
   HbIFunctionIO io = {q, ex->zero, ex->qdata, NULL, NULL, ex->f, 0};
   HBCK(hb_ifunction_apply(ex->op, &ex->ctx, &io, ex->s));
+  /* the face flux: the reference's explicit Freestream QFunction returns -wdetJb F (bc_freestream.h:45-48) into the RHS,
+   * so the negated right-hand side gains +wdetJb F */
+  if (ex->bc) {
+    HbFreestreamContext fc;
+    memcpy(&fc, ex->bc_ctx, sizeof fc);
+    fc.newt.time = t;
+    HBCK(hb_freestream_apply(ex->bc, &fc, ex->bc_flux, ex->bc_qdata, q, NULL, ex->f, ex->s));
+  }
+  HBCK(mask(ex, ex->f));
+  ex->qstate = q;
+  if (!ex->pc_ready) HBCK(setup_jacobi(ex)); /* first solve: PCSetUp */
   *its    = 0;
   *reason = 1;
   if (ex->o.mass_ksp == 0) return hb_vec_pointwise_mult_f64(out, ex->f, ex->dinv, ex->n, ex->s);
@@ -204,6 +246,7 @@ int hb_explicit_create(const HbElemOp *op, const void *ctx184, const double *d_q
   if (!op || !ctx184 || !d_qdata || !opts) return HB_ERROR_INVALID;
   if (opts->dt <= 0 || opts->rk_stages < 1 || opts->rk_stages > MAXS || (opts->mass_ksp != 0 && opts->mass_ksp != 1)) return HB_ERROR_INVALID;
   if (opts->mass_ksp == 1 && (opts->mass_restart < 1 || opts->mass_restart + 1 > MAXK || opts->mass_max_it < 1)) return HB_ERROR_INVALID;
+  if (opts->mass_type != 0 && opts->mass_type != 1) return HB_ERROR_INVALID;
   for (int i = 0; i < opts->rk_stages; i++)
     for (int j = i; j < opts->rk_stages; j++)
       if (opts->rk_a[i * MAXS + j] != 0) return HB_ERROR_INVALID; /* explicit tableaux only */
@@ -229,8 +272,9 @@ int hb_explicit_create(const HbElemOp *op, const void *ctx184, const double *d_q
     hb_explicit_destroy(ex);
     return HB_ERROR_NOMEM;
   }
+  ex->mass_stab = opts->mass_type == 0 && ex->ctx.stabilization == HB_STAB_SUPG;
+  ex->pc_ready  = 0; /* the Jacobi set-up runs at the first solve */
   int rc = hb_vec_set_f64(ex->zero, ex->n, 0.0, ex->s);
-  if (!rc) rc = setup_jacobi(ex);
   if (rc) {
     hb_explicit_destroy(ex);
     return rc;
@@ -239,8 +283,49 @@ int hb_explicit_create(const HbElemOp *op, const void *ctx184, const double *d_q
   return HB_SUCCESS;
 }
 
+int hb_explicit_set_essential(HbExplicitStepper *ex, const int32_t *h_idx, const double *h_val, int64_t n) {
+  if (!ex || n < 0 || (n && !h_idx)) return HB_ERROR_INVALID;
+  for (int64_t i = 0; i < n; i++)
+    if (h_idx[i] < 0 || h_idx[i] >= ex->n) return HB_ERROR_INVALID;
+  if (ex->ess_idx) cudaFree(ex->ess_idx);
+  if (ex->ess_val) cudaFree(ex->ess_val);
+  if (ex->ess_one) cudaFree(ex->ess_one);
+  ex->ess_idx = NULL;
+  ex->ess_val = ex->ess_one = NULL;
+  ex->ess_n   = 0;
+  if (n) {
+    if (cudaMalloc((void **)&ex->ess_idx, sizeof(int32_t) * (size_t)n) != cudaSuccess ||
+        cudaMalloc((void **)&ex->ess_val, sizeof(double) * (size_t)n) != cudaSuccess ||
+        cudaMalloc((void **)&ex->ess_one, sizeof(double) * (size_t)n) != cudaSuccess)
+      return HB_ERROR_NOMEM;
+    CUCK(cudaMemcpy(ex->ess_idx, h_idx, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice));
+    if (h_val) CUCK(cudaMemcpy(ex->ess_val, h_val, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice));
+    else CUCK(cudaMemset(ex->ess_val, 0, sizeof(double) * (size_t)n));
+    HBCK(hb_vec_set_f64(ex->ess_one, n, 1.0, ex->s));
+    ex->ess_n = n;
+    HBCK(hb_constrain_set_f64(ex->q, ex->ess_idx, ex->ess_val, n, ex->s));
+  }
+  ex->pc_ready = 0; /* the free-DOF mass system changed: set the preconditioner up again at the next solve */
+  return HB_SUCCESS;
+}
+
+int hb_explicit_set_freestream(HbExplicitStepper *ex, const HbFaceOp *faces, const void *ctx264, int flux_type, const double *qdata_sur) {
+  if (!ex) return HB_ERROR_INVALID;
+  ex->bc = NULL;
+  if (!faces) return HB_SUCCESS;
+  if (!ctx264 || !qdata_sur || (flux_type != 0 && flux_type != 1) || faces->l_size != ex->n) return HB_ERROR_INVALID;
+  memcpy(ex->bc_ctx, ctx264, sizeof ex->bc_ctx);
+  ex->bc       = faces;
+  ex->bc_flux  = flux_type;
+  ex->bc_qdata = qdata_sur;
+  return HB_SUCCESS;
+}
+
 int hb_explicit_destroy(HbExplicitStepper *ex) {
   if (!ex) return HB_SUCCESS;
+  if (ex->ess_idx) cudaFree(ex->ess_idx);
+  if (ex->ess_val) cudaFree(ex->ess_val);
+  if (ex->ess_one) cudaFree(ex->ess_one);
   void *p[] = {ex->q, ex->y, ex->f, ex->zero, ex->dinv, ex->K, ex->V, ex->w, ex->r, ex->scratch, ex->d_partial, ex->d_dots};
   for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
     if (p[i]) cudaFree(p[i]);
@@ -251,6 +336,7 @@ int hb_explicit_destroy(HbExplicitStepper *ex) {
 int hb_explicit_set_state(HbExplicitStepper *ex, const double *d_q, double t) {
   if (!ex || !d_q) return HB_ERROR_INVALID;
   CUCK(cudaMemcpyAsync(ex->q, d_q, sizeof(double) * (size_t)ex->n, cudaMemcpyDeviceToDevice, ex->s));
+  if (ex->ess_n) HBCK(hb_constrain_set_f64(ex->q, ex->ess_idx, ex->ess_val, ex->ess_n, ex->s)); /* boundary values inserted */
   ex->t           = t;
   ex->steps_taken = 0;
   return HB_SUCCESS;

@@ -1413,6 +1413,275 @@ __global__ void __launch_bounds__(kMassThreads) k_mass_diag(const ElemArgs<doubl
   }
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// SUPG-stabilized mass of the explicit path (MassFunction_Newtonian, qfunctions/newtonian.h:44-86; HONEE builds it instead of
+// Mass_5 when stab = supg and the run is explicit, problems/newtonian.c:212-265, 795): for a rate u at the state q,
+//   v = wdetJ u,  grad v = wdetJ dXdx stab(u),  stab = dF(StateFromY_fwd(tau . u)) with tau = Tau_diagPrim(q).
+// One CTA per element of a colour: both fields gathered and interpolated, the point function, then the value and the three
+// gradient transposes grouped by their remaining factors (z: {B v + G gv_z, B gv_y, B gv_x}; y: {B, G, B}; x: {B, B, G}).
+template <typename T>
+__device__ __forceinline__ void mass_stab_point(const PhysConst<T> &c, const T q[5], const T u[5], T wdetJ, const T X[3][3], T v[5], T gv[3][5]) {
+  St<T> s;
+  T inv_rho, etot, eint;
+  state_from_u(c, q, s, inv_rho, etot, eint);
+#pragma unroll
+  for (int i = 0; i < 5; i++) v[i] = wdetJ * u[i];
+  St<T> gs[3];
+  memset(gs, 0, sizeof gs);
+  const T body[5] = {0, 0, 0, 0, 0};
+  T tau[3], stab[5][3];
+  tau_diag(c, s, X, tau);
+  stabilization(c, s, eint, tau, gs, u, body, stab);
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int j = 0; j < 5; j++) gv[k][j] = wdetJ * (stab[j][0] * X[k][0] + stab[j][1] * X[k][1] + stab[j][2] * X[k][2]);
+}
+
+template <int P, int Q>
+struct MassStabPlan {
+  static constexpr int P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q, P2Q = P2 * Q, PQ2 = P * Q2;
+  static constexpr int oN = 0, oA = oN + 5 * P3, oB = oA + 5 * P2Q, oU = oB + 5 * PQ2, oQ = oU + 5 * Q3, oG = oQ + 5 * Q3, oZ = oG + 15 * Q3,
+                       oY = oZ + 15 * PQ2, total = oY + 10 * P2Q;
+  static constexpr size_t bytes = sizeof(double) * (size_t)total;
+};
+
+// interpolate the 5-component field gathered in sN [5][P3] to sOut [5][Q3] (x, y, z passes through sA, sB)
+template <int P, int Q>
+__device__ __forceinline__ void interp5(const double *sB1, const double *sN, double *sA, double *sBt, double *sOut) {
+  using L = MassStabPlan<P, Q>;
+  for (int f = threadIdx.x; f < 5 * L::P2Q; f += kMassThreads) {
+    const int qi = f % Q, pcb = (f / Q) % L::P2, c = f / L::P2Q;
+    double acc = 0;
+#pragma unroll
+    for (int i = 0; i < P; i++) acc += sB1[qi * P + i] * sN[c * L::P3 + pcb * P + i];
+    sA[f] = acc;
+  }
+  __syncthreads();
+  for (int f = threadIdx.x; f < 5 * L::PQ2; f += kMassThreads) {
+    const int qi = f % Q, qj = (f / Q) % Q, pc = (f / L::Q2) % P, c = f / L::PQ2;
+    double acc = 0;
+#pragma unroll
+    for (int j = 0; j < P; j++) acc += sB1[qj * P + j] * sA[c * L::P2Q + (pc * P + j) * Q + qi];
+    sBt[f] = acc;
+  }
+  __syncthreads();
+  for (int f = threadIdx.x; f < 5 * L::Q3; f += kMassThreads) {
+    const int qji = f % L::Q2, qk = (f / L::Q2) % Q, c = f / L::Q3;
+    double acc = 0;
+#pragma unroll
+    for (int k = 0; k < P; k++) acc += sB1[qk * P + k] * sBt[c * L::PQ2 + k * L::Q2 + qji];
+    sOut[f] = acc;
+  }
+}
+
+struct Grad1D {
+  double G[kMaxP * kMaxP];  // reference 1D gradient [Q][P]
+};
+
+template <int P, int Q>
+__global__ void __launch_bounds__(kMassThreads) k_mass_stab(const ElemArgs<double> a, const Grad1D bg, const double *__restrict__ qs,
+                                                            const double *__restrict__ u, double *__restrict__ v) {
+  using L = MassStabPlan<P, Q>;
+  constexpr int P3 = L::P3, Q2 = L::Q2, Q3 = L::Q3, P2Q = L::P2Q, PQ2 = L::PQ2, NT = kMassThreads;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sm = reinterpret_cast<double *>(smem_raw);
+  double *sN = sm + L::oN, *sA = sm + L::oA, *sBt = sm + L::oB, *sU = sm + L::oU, *sQ = sm + L::oQ, *sG = sm + L::oG, *sZ = sm + L::oZ,
+         *sY = sm + L::oY;
+  __shared__ double sB1[Q * P], sG1[Q * P];
+  for (int t = threadIdx.x; t < Q * P; t += NT) {
+    double b = 0, g = 0;
+#pragma unroll
+    for (int i = 0; i < Q * P; i++)  // compile-time indices: the parameter arrays stay in the constant bank
+      if (i == t) {
+        b = a.basis.B[i];
+        g = bg.G[i];
+      }
+    sB1[t] = b;
+    sG1[t] = g;
+  }
+  __syncthreads();
+  for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
+    const int e = a.elems[idx];
+    const int32_t *off = a.offsets + (int64_t)e * P3;
+    // rate and state at the quadrature points
+    for (int i = threadIdx.x; i < 5 * P3; i += NT) sN[(i % 5) * P3 + i / 5] = u[off[i / 5] + i % 5];
+    __syncthreads();
+    interp5<P, Q>(sB1, sN, sA, sBt, sU);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 5 * P3; i += NT) sN[(i % 5) * P3 + i / 5] = qs[off[i / 5] + i % 5];
+    __syncthreads();
+    interp5<P, Q>(sB1, sN, sA, sBt, sQ);
+    __syncthreads();
+    const double *qd = a.qdata + (int64_t)e * 10 * Q3;
+    for (int q = threadIdx.x; q < Q3; q += NT) {
+      double wdetJ, X[3][3], qv[5], uv[5], vv[5], gv[3][5];
+      load_qdata(qd, Q3, q, wdetJ, X);
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        qv[c] = sQ[c * Q3 + q];
+        uv[c] = sU[c * Q3 + q];
+      }
+      mass_stab_point<double>(a.pc, qv, uv, wdetJ, X, vv, gv);
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        sU[c * Q3 + q] = vv[c];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sG[(d * 5 + c) * Q3 + q] = gv[d][c];
+      }
+    }
+    __syncthreads();
+    // z: three arrays [g][c][pc][qj][qi]: g0 = B v + G gv_z, g1 = B gv_y, g2 = B gv_x
+    for (int f = threadIdx.x; f < 15 * PQ2; f += NT) {
+      const int qji = f % Q2, pc = (f / Q2) % P, c = (f / PQ2) % 5, g = f / (5 * PQ2);
+      double acc = 0;
+#pragma unroll
+      for (int k = 0; k < Q; k++) {
+        const int qq = k * Q2 + qji;
+        if (g == 0) acc += sB1[k * P + pc] * sU[c * Q3 + qq] + sG1[k * P + pc] * sG[(10 + c) * Q3 + qq];
+        else acc += sB1[k * P + pc] * sG[((g == 1 ? 5 : 0) + c) * Q3 + qq];
+      }
+      sZ[f] = acc;
+    }
+    __syncthreads();
+    // y: two arrays [h][c][pc][pb][qi]: h0 = B g0 + G g1 (x factor B), h1 = B g2 (x factor G)
+    for (int f = threadIdx.x; f < 10 * P2Q; f += NT) {
+      const int qi = f % Q, pb = (f / Q) % P, pc = (f / (Q * P)) % P, c = (f / P2Q) % 5, h = f / (5 * P2Q);
+      double acc = 0;
+#pragma unroll
+      for (int j = 0; j < Q; j++) {
+        const int zz = c * PQ2 + (pc * Q + j) * Q + qi;
+        if (h == 0) acc += sB1[j * P + pb] * sZ[zz] + sG1[j * P + pb] * sZ[5 * PQ2 + zz];
+        else acc += sB1[j * P + pb] * sZ[10 * PQ2 + zz];
+      }
+      sY[f] = acc;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 5 * P3; f += NT) {  // x and the scatter, components fastest
+      const int c = f % 5, p = f / 5, pa = p % P, pcb = p / P;
+      double acc = 0;
+#pragma unroll
+      for (int i = 0; i < Q; i++) acc += sB1[i * P + pa] * sY[c * P2Q + pcb * Q + i] + sG1[i * P + pa] * sY[5 * P2Q + c * P2Q + pcb * Q + i];
+      v[off[p] + c] += acc;
+    }
+    __syncthreads();
+  }
+}
+
+// Diagonal of the stabilized mass at the state q: for node p and component c, sum over points of phi_p^2 wdetJ plus
+// sum_k phi_p dphi_p/dX_k wdetJ (dXdx stab_c)_k, stab_c the stabilization row c for the unit rate e_c.  Twenty combination
+// arrays per element (5 components x {value, X0, X1, X2}) contracted together in three passes.
+template <int P, int Q>
+struct MassStabDiagPlan {
+  static constexpr int P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q, P2Q = P2 * Q, PQ2 = P * Q2;
+  static constexpr int oN = 0, oTa = oN + 5 * P3, oTb = oTa + 5 * P2Q, oQ = oTb + 5 * PQ2, oA = oQ + 5 * Q3, oY = oA + 20 * Q3,
+                       total = oY + 20 * Q2 * P;
+  static constexpr size_t bytes = sizeof(double) * (size_t)total;
+};
+
+template <int P, int Q>
+__global__ void __launch_bounds__(kMassThreads) k_mass_stab_diag(const ElemArgs<double> a, const Grad1D bg, const double *__restrict__ qs,
+                                                                 double *__restrict__ diag) {
+  using L = MassStabDiagPlan<P, Q>;
+  constexpr int P2 = L::P2, P3 = L::P3, Q2 = L::Q2, Q3 = L::Q3, QP2 = Q * L::P2, NT = kMassThreads;  // QP2: [Q][P][P] after the y pass
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sm = reinterpret_cast<double *>(smem_raw);
+  double *sN = sm + L::oN, *sTa = sm + L::oTa, *sTb = sm + L::oTb, *sQ = sm + L::oQ, *sA = sm + L::oA, *sY = sm + L::oY;
+  __shared__ double sB1[Q * P], sW[3][Q * P];
+  for (int t = threadIdx.x; t < Q * P; t += NT) {
+    double b = 0, g = 0;
+#pragma unroll
+    for (int i = 0; i < Q * P; i++)
+      if (i == t) {
+        b = a.basis.B[i];
+        g = bg.G[i];
+      }
+    sB1[t] = b;
+    sW[0][t] = b * b;
+    sW[1][t] = b * g;
+    sW[2][t] = g * g;
+  }
+  __syncthreads();
+  for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
+    const int e = a.elems[idx];
+    const int32_t *off = a.offsets + (int64_t)e * P3;
+    for (int i = threadIdx.x; i < 5 * P3; i += NT) sN[(i % 5) * P3 + i / 5] = qs[off[i / 5] + i % 5];
+    __syncthreads();
+    interp5<P, Q>(sB1, sN, sTa, sTb, sQ);
+    __syncthreads();
+    const double *qd = a.qdata + (int64_t)e * 10 * Q3;
+    for (int q = threadIdx.x; q < Q3; q += NT) {
+      double wdetJ, X[3][3], qv[5];
+      load_qdata(qd, Q3, q, wdetJ, X);
+#pragma unroll
+      for (int c = 0; c < 5; c++) qv[c] = sQ[c * Q3 + q];
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        double uv[5] = {0, 0, 0, 0, 0}, vv[5], gv[3][5];
+        uv[c] = 1.0;
+        mass_stab_point<double>(a.pc, qv, uv, wdetJ, X, vv, gv);
+        sA[(c * 4 + 0) * Q3 + q] = vv[c];
+#pragma unroll
+        for (int k = 0; k < 3; k++) sA[(c * 4 + 1 + k) * Q3 + q] = gv[k][c];
+      }
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 20 * Q2 * P; f += NT) {  // x: [t][k][j][pa]
+      const int t = f / (Q2 * P), rem = f % (Q2 * P), pa = rem % P, kj = rem / P;
+      const double *W = sW[combo_sel(t % 4, 0)];
+      double acc = 0;
+#pragma unroll
+      for (int i = 0; i < Q; i++) acc += W[i * P + pa] * sA[t * Q3 + kj * Q + i];
+      sY[f] = acc;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 20 * QP2; f += NT) {  // y: [t][k][pb][pa]
+      const int t = f / QP2, rem = f % QP2, pa = rem % P, pb = (rem / P) % P, k = rem / P2;
+      const double *W = sW[combo_sel(t % 4, 1)];
+      double acc = 0;
+#pragma unroll
+      for (int j = 0; j < Q; j++) acc += W[j * P + pb] * sY[t * Q2 * P + (k * Q + j) * P + pa];
+      sA[f] = acc;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 5 * P3; f += NT) {  // z, summed over the four combinations, and the scatter
+      const int c = f % 5, pp = f / 5, pab = pp % P2, pc_ = pp / P2;
+      double acc = 0;
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const double *W = sW[combo_sel(m, 2)];
+#pragma unroll
+        for (int k = 0; k < Q; k++) acc += W[k * P + pc_] * sA[(c * 4 + m) * QP2 + k * P2 + pab];
+      }
+      diag[off[pp] + c] += acc;
+    }
+    __syncthreads();
+  }
+}
+
+template <int P, int Q>
+static int launch_mass_stab(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const double *qs, const double *u, double *v,
+                            bool diagonal, cudaStream_t s) {
+  Grad1D bg;
+  memset(&bg, 0, sizeof bg);
+  for (int i = 0; i < Q * P; i++) bg.G[i] = op->grad1d[i];
+  const size_t sm = diagonal ? MassStabDiagPlan<P, Q>::bytes : MassStabPlan<P, Q>::bytes;
+  if (diagonal) {
+    if (cudaFuncSetAttribute(k_mass_stab_diag<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
+  } else {
+    if (cudaFuncSetAttribute(k_mass_stab<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
+  }
+  for (int c = 0; c < op->num_colors; c++) {
+    ElemArgs<double> a = make_args<double>(op, ctx, qdata, c);
+    if (a.n_elems == 0) continue;
+    if (diagonal)
+      k_mass_stab_diag<P, Q><<<grid_for(op, a.n_elems, k_mass_stab_diag<P, Q>, kMassThreads, sm), kMassThreads, sm, s>>>(a, bg, qs, v);
+    else
+      k_mass_stab<P, Q><<<grid_for(op, a.n_elems, k_mass_stab<P, Q>, kMassThreads, sm), kMassThreads, sm, s>>>(a, bg, qs, u, v);
+  }
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+
 template <int P, int Q>
 static int launch_mass(const HbElemOp *op, const double *qdata, const double *u, double *v, bool diagonal, cudaStream_t s, int block = 0) {
   for (int c = 0; c < op->num_colors; c++) {
@@ -1677,4 +1946,32 @@ extern "C" int hb_mass_point_block_diagonal(const HbElemOp *op, const double *qd
   HB_PQ_LIST(HB_CASE)
 #undef HB_CASE
   return HB_ERROR_UNSUPPORTED;
+}
+
+// SUPG-stabilized mass (MassFunction_Newtonian) at the state qs: v (+)= M_stab(qs) u, and its diagonal
+template <bool DIAG>
+static int mass_stab_dispatch(const HbElemOp *op, const void *ctx184, const double *qdata, const double *qs, const double *u, double *v, int add,
+                              void *stream) {
+  int err = check_op(op);
+  if (err) return err;
+  if (!ctx184 || !qdata || !qs || (!DIAG && !u) || !v) return HB_ERROR_INVALID;
+  HbNewtonianContext ctx;
+  memcpy(&ctx, ctx184, sizeof ctx);
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!add && cudaMemsetAsync(v, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_mass_stab<PP, QQ>(op, ctx, qdata, qs, u, v, DIAG, s);
+  HB_PQ_LIST(HB_CASE)
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+
+extern "C" int hb_mass_stab_apply(const HbElemOp *op, const void *ctx184, const double *qdata, const double *q_state, const double *u, double *v,
+                                  int add, void *stream) {
+  return mass_stab_dispatch<false>(op, ctx184, qdata, q_state, u, v, add, stream);
+}
+extern "C" int hb_mass_stab_diagonal(const HbElemOp *op, const void *ctx184, const double *qdata, const double *q_state, double *diag, int add,
+                                     void *stream) {
+  return mass_stab_dispatch<true>(op, ctx184, qdata, q_state, NULL, diag, add, stream);
 }

@@ -143,20 +143,41 @@ class NewtonianOperators:
         self.op_rhs = ce.Operator(ceed)
         self.op_rhs.set_name("RHS Composite Operator")
         self.op_rhs.add_sub(op_rhs_vol)
-        qf_mass = ce.QFunction(ceed, "mass.h:Mass_5")
-        qf_mass.add_input("u", 5, ce.CEED_EVAL_INTERP)
-        qf_mass.add_input("qdata", 10, ce.CEED_EVAL_NONE)
-        qf_mass.add_output("v", 5, ce.CEED_EVAL_INTERP)
-        self.op_mass = ce.Operator(ceed, qf_mass)
-        self.op_mass.set_name("RHS Mass Operator")
-        self.op_mass.set_field("u", self.rstr_q, self.basis_q, ceed.active)
-        self.op_mass.set_field("qdata", self.rstr_qd, ceed.basis_none, self.q_data)
-        self.op_mass.set_field("v", self.rstr_q, self.basis_q, ceed.active)
+        if self.ctx.stabilization == 2:  # SUPG: CreateKSPMassOperator_NewtonianStabilized (problems/newtonian.c:212-265, 795)
+            self.q_state = ce.Vector(ceed, self.mesh.l_size)  # the state RHS_NS last evaluated at (honee->q_ceed)
+            qf_mass = ce.QFunction(ceed, "newtonian.h:MassFunction_Newtonian_Conserv")
+            qf_mass.add_input("q_dot", 5, ce.CEED_EVAL_INTERP)
+            qf_mass.add_input("q", 5, ce.CEED_EVAL_INTERP)
+            qf_mass.add_input("qdata", 10, ce.CEED_EVAL_NONE)
+            qf_mass.add_output("v", 5, ce.CEED_EVAL_INTERP)
+            qf_mass.add_output("Grad_v", 15, ce.CEED_EVAL_GRAD)
+            qf_mass.set_context(self.qfctx)
+            self.op_mass = ce.Operator(ceed, qf_mass)
+            self.op_mass.set_name("RHS Mass Operator, Newtonian Stabilized")
+            self.op_mass.set_field("q_dot", self.rstr_q, self.basis_q, ceed.active)
+            self.op_mass.set_field("q", self.rstr_q, self.basis_q, self.q_state)
+            self.op_mass.set_field("qdata", self.rstr_qd, ceed.basis_none, self.q_data)
+            self.op_mass.set_field("v", self.rstr_q, self.basis_q, ceed.active)
+            self.op_mass.set_field("Grad_v", self.rstr_q, self.basis_q, ceed.active)
+        else:  # CreateKSPMassOperator_Unstabilized (src/setuplibceed.c:15-53)
+            self.q_state = None
+            qf_mass = ce.QFunction(ceed, "mass.h:Mass_5")
+            qf_mass.add_input("u", 5, ce.CEED_EVAL_INTERP)
+            qf_mass.add_input("qdata", 10, ce.CEED_EVAL_NONE)
+            qf_mass.add_output("v", 5, ce.CEED_EVAL_INTERP)
+            self.op_mass = ce.Operator(ceed, qf_mass)
+            self.op_mass.set_name("RHS Mass Operator")
+            self.op_mass.set_field("u", self.rstr_q, self.basis_q, ceed.active)
+            self.op_mass.set_field("qdata", self.rstr_qd, ceed.basis_none, self.q_data)
+            self.op_mass.set_field("v", self.rstr_q, self.basis_q, ceed.active)
         self._explicit = (op_rhs_vol, qf_rhs, qf_mass)
 
     def rhs(self, q: ce.Vector, g: ce.Vector):
-        """R = RHS(q) before the mass solve (ApplyCeedOperatorLocalToGlobal in RHS_NS, src/setupts.c:50)."""
+        """R = RHS(q) before the mass solve (ApplyCeedOperatorLocalToGlobal in RHS_NS, src/setupts.c:50); the stabilized mass
+        operator then sees the same state (the reference points honee->q_ceed at it, src/setupts.c:54)."""
         self.op_rhs.apply(q, g)
+        if self.q_state is not None:
+            q.copy_to(self.q_state)
 
     # ---- boundary faces
     def add_freestream(self, P_inf, u_inf, T_inf, *, riemann="hllc", sides=None, implicit=True):

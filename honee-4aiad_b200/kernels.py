@@ -126,6 +126,17 @@ class ElemOp:
     def mass_diagonal(self, qdata, diag, add=False, stream=None):
         _chk(_load().hb_mass_diagonal(self.ptr, _addr(qdata), _addr(diag), int(add), _stream(stream)), "hb_mass_diagonal")
 
+    def mass_stab(self, ctx_bytes: bytes, qdata, q_state, u, v, add=False, stream=None):
+        """v (+)= M_stab(q_state) u, the SUPG-stabilized mass of explicit SUPG runs (MassFunction_Newtonian)."""
+        cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        _chk(_load().hb_mass_stab_apply(self.ptr, cb, _addr(qdata), _addr(q_state), _addr(u), _addr(v), int(add), _stream(stream)),
+             "hb_mass_stab_apply")
+
+    def mass_stab_diagonal(self, ctx_bytes: bytes, qdata, q_state, diag, add=False, stream=None):
+        cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
+        _chk(_load().hb_mass_stab_diagonal(self.ptr, cb, _addr(qdata), _addr(q_state), _addr(diag), int(add), _stream(stream)),
+             "hb_mass_stab_diagonal")
+
     def mass_point_block_diagonal(self, qdata, out, add=False, stream=None):
         _chk(_load().hb_mass_point_block_diagonal(self.ptr, _addr(qdata), _addr(out), int(add), _stream(stream)), "hb_mass_point_block_diagonal")
 

@@ -345,6 +345,54 @@ def taylor_green_context(degree: int, *, L=2 * math.pi, Re=1600., Ma=0.1, rho0=1
 
 
 # --------------------------------------------------------------------------------------------------------------------
+# Gaussian wave (problems/gaussianwave.c, qfunctions/gaussianwave.h)
+
+class StateC(C.Structure):
+    """struct State (qfunctions/newtonian_types.h): conservative U then primitive Y."""
+    _fields_ = [("U", C.c_double * 5), ("Y", C.c_double * 5)]
+
+
+class GaussianWaveContext(C.Structure):
+    """struct GaussianWaveContext_ (qfunctions/gaussianwave.h:12-18)."""
+    _fields_ = [("epicenter", C.c_double * 3), ("width", C.c_double), ("amplitude", C.c_double), ("S_infty", StateC),
+                ("newt_ctx", NewtonianContext)]
+
+
+def state_from_primitive(gas: GasProperties, P, u, T):
+    """StateFromPrimitive: (U, Y) of an ideal gas at pressure P, velocity u, temperature T."""
+    U = conservative_from_primitive(gas, np.array([P]), np.asarray(u, dtype=np.float64).reshape(3, 1), np.array([T]))[:, 0]
+    return U, np.array([P, *np.asarray(u, dtype=np.float64), T])
+
+
+def gaussian_wave_context(newt: NewtonianContext, P, u, T, *, epicenter=(0.0, 0.0, 0.0), width=0.002, amplitude=0.1):
+    U, Y = state_from_primitive(newt.gas, P, u, T)
+    ctx = GaussianWaveContext()
+    ctx.epicenter[:] = list(epicenter)
+    ctx.width, ctx.amplitude = width, amplitude
+    ctx.S_infty.U[:] = list(U)
+    ctx.S_infty.Y[:] = list(Y)
+    ctx.newt_ctx = newt
+    return ctx
+
+
+def gaussian_wave_state(mesh: BoxMesh, basis: TensorBasis, gw: GaussianWaveContext) -> np.ndarray:
+    """IC_GaussianWave (qfunctions/gaussianwave.h:20-58) at the nodes: the free-stream density and pressure scaled by
+    1 + amplitude exp(-r^2 / (2 width^2)) in the x-y plane around the epicentre, the free-stream velocity, kinetic energy of the
+    free stream."""
+    X = node_coordinates(mesh, basis)
+    gas = gw.newt_ctx.gas
+    gamma = gas.cp / gas.cv
+    rho_inf, Pinf = gw.S_infty.U[0], gw.S_infty.Y[0]
+    u = np.array(gw.S_infty.Y[1:4])
+    pert = 1 + gw.amplitude * np.exp(-((X[0] - gw.epicenter[0]) ** 2 + (X[1] - gw.epicenter[1]) ** 2) / (2 * gw.width ** 2))
+    q = np.empty((5, X.shape[1]))
+    q[0] = rho_inf * pert
+    q[1:4] = u[:, None] * q[0]
+    q[4] = Pinf / (gamma - 1) * pert + 0.5 * rho_inf * (u @ u)
+    return np.ascontiguousarray(q.T.reshape(-1))
+
+
+# --------------------------------------------------------------------------------------------------------------------
 # channel flow (problems/channel.c:73-150, qfunctions/channel.h): Poiseuille initial state, body force, no-slip walls
 
 class ChannelContext(C.Structure):

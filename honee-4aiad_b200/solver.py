@@ -125,6 +125,10 @@ RK_TABLEAUX = {
     "3": ([[0, 0, 0], [0.5, 0, 0], [-1.0, 2.0, 0]], [1 / 6, 2 / 3, 1 / 6], [0, 0.5, 1.0]),
     "3bs": ([[0, 0, 0, 0], [0.5, 0, 0, 0], [0, 0.75, 0, 0], [2 / 9, 1 / 3, 4 / 9, 0]], [2 / 9, 1 / 3, 4 / 9, 0], [0, 0.5, 0.75, 1.0]),
     "4": ([[0, 0, 0, 0], [0.5, 0, 0, 0], [0, 0.5, 0, 0], [0, 0, 1.0, 0]], [1 / 6, 1 / 3, 1 / 3, 1 / 6], [0, 0.5, 0.5, 1.0]),
+    # Fehlberg's six-stage pair, advanced with its fifth-order weights (TSRK5F, HONEE's explicit default, src/setupts.c:355)
+    "5f": ([[0, 0, 0, 0, 0, 0], [1 / 4, 0, 0, 0, 0, 0], [3 / 32, 9 / 32, 0, 0, 0, 0], [1932 / 2197, -7200 / 2197, 7296 / 2197, 0, 0, 0],
+            [439 / 216, -8, 3680 / 513, -845 / 4104, 0, 0], [-8 / 27, 2, -3544 / 2565, 1859 / 4104, -11 / 40, 0]],
+           [16 / 135, 0, 6656 / 12825, 28561 / 56430, -9 / 50, 2 / 55], [0, 1 / 4, 3 / 8, 12 / 13, 1, 1 / 2]),
 }
 
 
@@ -132,7 +136,7 @@ class HbExplicitOptions(C.Structure):
     _fields_ = [("dt", C.c_double), ("rk_stages", C.c_int), ("rk_a", C.c_double * (RK_MAX_STAGES * RK_MAX_STAGES)),
                 ("rk_b", C.c_double * RK_MAX_STAGES), ("rk_c", C.c_double * RK_MAX_STAGES), ("mass_ksp", C.c_int),
                 ("mass_pc_rowsum", C.c_int), ("mass_rtol", C.c_double), ("mass_atol", C.c_double), ("mass_max_it", C.c_int),
-                ("mass_restart", C.c_int)]
+                ("mass_restart", C.c_int), ("mass_type", C.c_int)]
 
 
 class HbExplicitStats(C.Structure):
@@ -140,7 +144,7 @@ class HbExplicitStats(C.Structure):
 
 
 def explicit_options(*, dt, rk_type="4", mass_ksp="preonly", pc_jacobi="rowsum", rtol=1e-5, atol=1e-50, max_it=10000,
-                     restart=30) -> HbExplicitOptions:
+                     restart=30, mass="auto") -> HbExplicitOptions:
     """Options in HONEE's vocabulary: -ts_rk_type, -mass_ksp_type preonly|gmres, -mass_pc_jacobi_type rowsum|diagonal."""
     o = HbExplicitOptions()
     _load().hb_explicit_default_options(C.byref(o))
@@ -158,6 +162,7 @@ def explicit_options(*, dt, rk_type="4", mass_ksp="preonly", pc_jacobi="rowsum",
     o.mass_ksp = {"preonly": 0, "gmres": 1}[mass_ksp]
     o.mass_pc_rowsum = {"rowsum": 1, "diagonal": 0}[pc_jacobi]
     o.mass_rtol, o.mass_atol, o.mass_max_it, o.mass_restart = rtol, atol, max_it, restart
+    o.mass_type = {"auto": 0, "plain": 1}[mass]  # auto: the SUPG-stabilized mass when stab = supg, as HONEE chooses
     return o
 
 
@@ -194,6 +199,25 @@ class ExplicitStepper:
         its, reason = C.c_int(), C.c_int()
         _chk(_load().hb_explicit_rhs(self.ptr, _addr(q), C.c_double(t), _addr(g), C.byref(its), C.byref(reason)), "hb_explicit_rhs")
         return its.value, reason.value
+
+    def set_essential(self, idx=None, values=None):
+        """Strong Dirichlet DOFs (L-vector indices node * 5 + component, values default 0), or none."""
+        L = _load()
+        if idx is None or len(idx) == 0:
+            _chk(L.hb_explicit_set_essential(self.ptr, None, None, C.c_int64(0)), "hb_explicit_set_essential")
+            return
+        i = np.ascontiguousarray(idx, dtype=np.int32)
+        v = None if values is None else np.ascontiguousarray(values, dtype=np.float64)
+        _chk(L.hb_explicit_set_essential(self.ptr, i.ctypes.data_as(C.POINTER(C.c_int32)), None if v is None else v.ctypes.data_as(C.POINTER(C.c_double)),
+                                         C.c_int64(i.size)), "hb_explicit_set_essential")
+
+    def set_freestream(self, faceop=None, ctx264: bytes = b"", flux_type=1):
+        if faceop is None:
+            _chk(_load().hb_explicit_set_freestream(self.ptr, None, None, 0, None), "hb_explicit_set_freestream")
+            return
+        self._bc = (faceop, C.create_string_buffer(bytes(ctx264), len(ctx264)))
+        _chk(_load().hb_explicit_set_freestream(self.ptr, faceop.ptr, self._bc[1], C.c_int(flux_type), _addr(faceop.qdata)),
+             "hb_explicit_set_freestream")
 
     def step(self) -> ExplicitStats:
         s = HbExplicitStats()

@@ -187,6 +187,13 @@ HB_EXPORT int hb_ts_destroy(HbTimeStepper *ts);
  * diagonal (what MatGetDiagonal_Ceed gives PCJacobi "diagonal"; the row sums of PCJacobi "rowsum" are M applied to ones). */
 HB_EXPORT int hb_mass_apply(const HbElemOp *op, const double *qdata, const double *u, double *v, int add, void *stream);
 HB_EXPORT int hb_mass_diagonal(const HbElemOp *op, const double *qdata, double *diag, int add, void *stream);
+/* The SUPG-stabilized mass HONEE uses instead when stab = supg and the run is explicit (MassFunction_Newtonian,
+ * qfunctions/newtonian.h:44-86; problems/newtonian.c:212-265, 795), at the state q_state: v (+)= M_stab u, with
+ * v = wdetJ u and grad v = wdetJ dXdx stab(u) (the SUPG term of the rate, tau from q_state); and its diagonal. */
+HB_EXPORT int hb_mass_stab_apply(const HbElemOp *op, const void *ctx184, const double *qdata, const double *q_state, const double *u, double *v,
+                                 int add, void *stream);
+HB_EXPORT int hb_mass_stab_diagonal(const HbElemOp *op, const void *ctx184, const double *qdata, const double *q_state, double *diag, int add,
+                                    void *stream);
 /* its point blocks (5 * l_size values, row-major 5 x 5 per node): the diagonal on each block's diagonal, zeros elsewhere */
 HB_EXPORT int hb_mass_point_block_diagonal(const HbElemOp *op, const double *qdata, double *out, int add, void *stream);
 
@@ -202,6 +209,7 @@ typedef struct {
   int    mass_pc_rowsum; /* Jacobi from the row sums (1) or from the diagonal (0, -mass_pc_jacobi_type diagonal) */
   double mass_rtol, mass_atol;
   int    mass_max_it, mass_restart;
+  int    mass_type; /* 0: as HONEE (the SUPG-stabilized mass MassFunction_Newtonian when stab = supg, else Mass_5), 1: Mass_5 */
 } HbExplicitOptions;
 
 typedef struct {
@@ -211,8 +219,11 @@ typedef struct {
 } HbExplicitStats;
 
 typedef struct HbExplicitStepper HbExplicitStepper;
+struct HbFaceOp; /* boundary faces, declared below */
 
-/* Classical 4-stage RK (TSRK4), lumped mass, PETSc's KSP defaults (rtol 1e-5, atol 1e-50, 10000 its, restart 30). */
+/* Classical 4-stage RK (TSRK4), lumped mass, PETSc's KSP defaults (rtol 1e-5, atol 1e-50, 10000 its, restart 30).  The
+ * Jacobi preconditioner of the mass solve is set up at the first solve and kept, as PETSc keeps it (the MatCEED object never
+ * changes state, so PCSetUp runs once): for the stabilized mass that is the state of the first right-hand side. */
 HB_EXPORT void hb_explicit_default_options(HbExplicitOptions *o);
 /* ctx184 is copied; "timestep size" and "solution time" are set per stage like RHS_NS does (src/setupts.c:40-46). */
 HB_EXPORT int hb_explicit_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, const HbExplicitOptions *opts, void *stream,
@@ -223,6 +234,12 @@ HB_EXPORT int hb_explicit_get_state(HbExplicitStepper *ex, double *d_q, double *
  * one call of RHS_NS; *its receives the mass-solve iterations and *converged_reason 1, -1 or -2 (either may be NULL). */
 HB_EXPORT int hb_explicit_rhs(HbExplicitStepper *ex, const double *d_q, double t, double *d_g, int *its, int *converged_reason);
 HB_EXPORT int hb_explicit_step(HbExplicitStepper *ex, HbExplicitStats *stats);
+/* Essential DOFs (as hb_ts_set_essential): the state keeps their values, the right-hand side and the mass solve act on the
+ * free DOFs only (RHS_NS after DMLocalToGlobal). */
+HB_EXPORT int hb_explicit_set_essential(HbExplicitStepper *ex, const int32_t *h_idx, const double *h_val, int64_t n);
+/* Free-stream faces in the explicit right-hand side (the reference's explicit Freestream QFunction contributes -wdetJb F,
+ * bc_freestream.h:45-48); faces == NULL removes them. */
+HB_EXPORT int hb_explicit_set_freestream(HbExplicitStepper *ex, const struct HbFaceOp *faces, const void *ctx264, int flux_type, const double *qdata_sur);
 HB_EXPORT int hb_explicit_destroy(HbExplicitStepper *ex);
 
 /* Krylov block operations (FP64 accumulation): out[i] = V_i . w for i < k (d_partial: 512*HB_GMRES_MAX_BASIS doubles),

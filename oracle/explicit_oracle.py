@@ -4,7 +4,10 @@ RHS_NS (src/setupts.c:31-75): G = M^-1 RHS(q), RHS from the RHSFunction_Newtonia
 Mass_5 operator (oracle.apply_mass) inverted by the "mass_" KSP of CreateKSPMass (src/setuplibceed.c:55-93): KSPPREONLY
 with PCJacobi row sums ("lumped", the default) or KSPGMRES with PCJacobi; PETSc's defaults for GMRES are restated here
 (left preconditioning, preconditioned residual norm, zero initial guess, classical Gram-Schmidt, restart 30, rtol 1e-5,
-atol 1e-50).  PETSc's TSRK tableaux (TSRK1FE, TSRK2A, TSRK3, TSRK3BS, TSRK4) are the published Butcher tables.
+atol 1e-50).  PETSc's TSRK tableaux (TSRK1FE, TSRK2A, TSRK3, TSRK3BS, TSRK4, TSRK5F) are the published Butcher tables (5F: Fehlberg's pair with
+its fifth-order weights).  Essential DOFs are removed from the system as DMPlex constraints do (values in the state, zero rows
+in the right-hand side, the mass solved on the free DOFs); free-stream faces add -wdetJb F (the explicit Freestream QFunction,
+bc_freestream.h:45-48).
 
 PETSc itself is not present here; the restatement is pinned by the reference's own run of this path:
 tests/output/taylorgreen_totalke.csv (kinetic-energy rows at steps 0, 2, 3) and tests/output/taylor-green.bin (the
@@ -22,6 +25,9 @@ TABLEAUX = {  # name -> (A, b, c)
     "3": ([[0, 0, 0], [0.5, 0, 0], [-1.0, 2.0, 0]], [1 / 6, 2 / 3, 1 / 6], [0, 0.5, 1.0]),
     "3bs": ([[0, 0, 0, 0], [0.5, 0, 0, 0], [0, 0.75, 0, 0], [2 / 9, 1 / 3, 4 / 9, 0]], [2 / 9, 1 / 3, 4 / 9, 0], [0, 0.5, 0.75, 1.0]),
     "4": ([[0, 0, 0, 0], [0.5, 0, 0, 0], [0, 0.5, 0, 0], [0, 0, 1.0, 0]], [1 / 6, 1 / 3, 1 / 3, 1 / 6], [0, 0.5, 0.5, 1.0]),
+    "5f": ([[0, 0, 0, 0, 0, 0], [1 / 4, 0, 0, 0, 0, 0], [3 / 32, 9 / 32, 0, 0, 0, 0], [1932 / 2197, -7200 / 2197, 7296 / 2197, 0, 0, 0],
+            [439 / 216, -8, 3680 / 513, -845 / 4104, 0, 0], [-8 / 27, 2, -3544 / 2565, 1859 / 4104, -11 / 40, 0]],
+           [16 / 135, 0, 6656 / 12825, 28561 / 56430, -9 / 50, 2 / 55], [0, 1 / 4, 3 / 8, 12 / 13, 1, 1 / 2]),
 }
 
 
@@ -94,21 +100,52 @@ class Explicit:
     """The explicit loop on one box: q_{n+1} from an explicit RK tableau with G = M^-1 RHS(q)."""
 
     def __init__(self, mesh: O.Mesh, P, Q, ctx_bytes: bytes, qdata, l_size, *, dt, tableau="4", mass_ksp="preonly",
-                 pc_jacobi="rowsum", rtol=1e-5, atol=1e-50, restart=30, x_q=None):
+                 pc_jacobi="rowsum", rtol=1e-5, atol=1e-50, restart=30, x_q=None, essential=None, faces=None, mass="auto"):
+        """faces: optional callable q -> wdetJb F through the free-stream faces (face_oracle.freestream_apply).  mass "auto":
+        the SUPG-stabilized mass (MassFunction_Newtonian, linearised at each right-hand side's state) when the context's
+        stabilization is SUPG, as problems/newtonian.c:795 chooses, else Mass_5; the Jacobi preconditioner is set up at the
+        first solve and kept (PCSetUp runs once: the MatCEED object never changes state)."""
         self.mesh, self.qdata, self.l_size, self.dt, self.x_q = mesh, qdata, l_size, dt, x_q
+        self.ess = np.asarray(essential if essential is not None else [], dtype=np.int64)
+        self.faces = faces
         self.ctx = bytearray(ctx_bytes)
         self.ctx[168:176] = np.float64(dt).tobytes()  # "timestep size" (RHS_NS, src/setupts.c:44-46)
         self.A, self.b, self.c = (np.asarray(v, dtype=np.float64) for v in TABLEAUX[tableau])
         self.mass_ksp, self.rtol, self.atol, self.restart = mass_ksp, rtol, atol, restart
-        M = lambda u: O.apply_mass(mesh, np.ascontiguousarray(u), qdata)  # noqa: E731
+        stab = int(np.frombuffer(bytes(self.ctx)[88:92], dtype=np.int32)[0])  # NewtonianIdealGasContext_.stabilization (offset 88)
+        self.stab_mass = mass == "auto" and stab == 2
+        self.state = None
+
+        def M(u):
+            if self.stab_mass:
+                v = O.apply_mass_stab(mesh, bytes(self.ctx), np.ascontiguousarray(u), self.state, qdata)
+            else:
+                v = O.apply_mass(mesh, np.ascontiguousarray(u), qdata)
+            v[self.ess] = 0.0
+            return v
         self.M = M
-        d = M(np.ones(l_size)) if pc_jacobi == "rowsum" else mass_diagonal(mesh, P, Q, qdata, l_size)
-        self.dinv = 1.0 / d
+        self.P, self.Q, self.pc_jacobi = P, Q, pc_jacobi
+        self.dinv = None
         self.mass_its = []
 
     def rhs(self, q, t):
         self.ctx[64:72] = np.float64(t).tobytes()  # "solution time"
         R = O.apply_rhs(self.mesh, bytes(self.ctx), np.ascontiguousarray(q), self.qdata, self.x_q)
+        if self.faces is not None:
+            R = R - self.faces(q)
+        R[self.ess] = 0.0
+        self.state = np.ascontiguousarray(q)
+        if self.dinv is None:  # PCSetUp at the first solve
+            if self.pc_jacobi == "rowsum":
+                ones = np.ones(self.l_size)
+                ones[self.ess] = 0.0
+                d = self.M(ones)
+            elif self.stab_mass:
+                d = O.mass_stab_diagonal(self.mesh, bytes(self.ctx), self.state, self.qdata, self.l_size)
+            else:
+                d = mass_diagonal(self.mesh, self.P, self.Q, self.qdata, self.l_size)
+            d[self.ess] = 1.0
+            self.dinv = 1.0 / d
         if self.mass_ksp == "preonly":
             return self.dinv * R
         G, its, reason = gmres_left(self.M, self.dinv, R, self.rtol, self.atol, self.restart)

@@ -1115,6 +1115,109 @@ int oracle_apply_mass(const OracleMesh *m, OracleQF qf, const double *u, const d
   return err;
 }
 
+/* Restatement of MassFunction_Newtonian for conservative variables (qfunctions/newtonian.h:44-86): v = wdetJ q_dot and
+ * Grad_v = wdetJ dXdx stab, stab from the stabilization with zero state gradient, zero body force and the rate as U_dot (for
+ * SUPG the strong residual is U_dot; for SU and none the term vanishes). */
+int oracle_qf_mass_stab_conserv(void *ctx_, int Q, const double *const *in, double *const *out) {
+  const HbNewtonianContext *ctx = (const HbNewtonianContext *)ctx_;
+  const HbGasProperties    *gas = &ctx->gas;
+  const double             *qd = in[0], *q = in[1], *qdata = in[2];
+  double                   *v = out[0], *gv = out[1];
+  for (int i = 0; i < Q; i++) {
+    double qi[5], U_dot[5];
+    for (int c = 0; c < 5; c++) {
+      qi[c]    = q[c * Q + i];
+      U_dot[c] = qd[c * Q + i];
+    }
+    const OracleState s = oracle_state_from_q(gas, qi, HB_STATEVAR_CONSERVATIVE);
+    double            wdetJ, dXdx[3][3];
+    unpack_qdata(Q, i, qdata, &wdetJ, dXdx);
+    for (int c = 0; c < 5; c++) v[c * Q + i] = wdetJ * U_dot[c];
+    OracleState grad_s[3];
+    memset(grad_s, 0, sizeof grad_s);
+    const double zero[5] = {0, 0, 0, 0, 0};
+    double       tau_d[3], stab[5][3];
+    tau_diag_prim(&ctx->tau_coeffs, gas, &s, dXdx, ctx->dt, tau_d);
+    stabilization(ctx->stabilization, gas, &s, tau_d, grad_s, U_dot, zero, zero, stab);
+    for (int c = 0; c < 5; c++)
+      for (int k = 0; k < 3; k++) gv[(k * 5 + c) * Q + i] = wdetJ * (stab[c][0] * dXdx[k][0] + stab[c][1] * dXdx[k][1] + stab[c][2] * dXdx[k][2]);
+  }
+  return 0;
+}
+
+/* The SUPG-stabilized mass operator of the explicit path (MassFunction_Newtonian, qfunctions/newtonian.h:44-86; built by
+ * CreateKSPMassOperator_NewtonianStabilized, problems/newtonian.c:212-265, when stab = supg and the run is explicit):
+ * inputs q_dot (active, INTERP), q (passive, INTERP), qdata; outputs v (INTERP) and Grad_v (GRAD). */
+static void mass_stab_elem(const OracleMesh *m, int64_t e, void *user, double *s, int *err) {
+  ApplyArgs *a  = (ApplyArgs *)user;
+  const int  P3 = m->P * m->P * m->P, Q3 = m->Q * m->Q * m->Q;
+  double *ue = s, *qdi = ue + 5 * P3, *qi = qdi + 5 * Q3, *v = qi + 15 * Q3 + 5 * Q3, *gv = v + 5 * Q3, *ve = gv + 15 * Q3;
+  elem_eval(m, e, a->q_dot, ue, qdi, NULL);
+  elem_eval(m, e, a->q, ue, qi, NULL);
+  const double *in[3]  = {qdi, qi, a->qdata + e * 10 * Q3};
+  double       *out[2] = {v, gv};
+  if (a->qf(a->ctx, Q3, in, out)) *err = 1;
+  elem_scatter(m, e, v, gv, ve, a->v);
+}
+
+int oracle_apply_mass_stab(const OracleMesh *m, OracleQF qf, void *ctx, const double *q_dot, const double *q, const double *qdata, double *v,
+                           int64_t l_size) {
+  ApplyArgs a = {qf, ctx, q, q_dot, qdata, NULL, NULL, NULL, v, 14};
+  int       err = 0;
+  memset(v, 0, sizeof(double) * l_size);
+  for_each_elem(m, mass_stab_elem, &a, apply_scratch(m), &err);
+  return err;
+}
+
+/* Diagonal of the stabilized mass at the state q: the QFunction linearised in the rate at each point (unit rates), tested
+ * with the value and the reference gradient of the same basis function (libCEED diagonal assembly semantics). */
+static void mass_stab_diag_elem(const OracleMesh *m, int64_t e, void *user, double *s, int *err) {
+  ApplyArgs    *a = (ApplyArgs *)user;
+  const int     P = m->P, Q = m->Q, P3 = P * P * P, Q3 = Q * Q * Q;
+  const double *B = m->interp1d, *G = m->grad1d;
+  double       *ue = s, *qi = ue + 5 * P3, *de = qi + 5 * Q3;
+  elem_eval(m, e, a->q, ue, qi, NULL);
+  memset(de, 0, sizeof(double) * 5 * P3);
+  for (int qp = 0; qp < Q3; qp++) {
+    const int qx = qp % Q, qy = (qp / Q) % Q, qz = qp / (Q * Q);
+    double    qd[10], qv[5], A[20][5];
+    for (int c = 0; c < 10; c++) qd[c] = a->qdata[(e * 10 + c) * Q3 + qp];
+    for (int c = 0; c < 5; c++) qv[c] = qi[c * Q3 + qp];
+    for (int j = 0; j < 5; j++) {
+      double u[5] = {0}, v[5], gv[15];
+      u[j]                 = 1;
+      const double *in[3]  = {u, qv, qd};
+      double       *out[2] = {v, gv};
+      if (a->qf(a->ctx, 1, in, out)) *err = 1;
+      for (int i = 0; i < 5; i++) A[i][j] = v[i];
+      for (int i = 0; i < 15; i++) A[5 + i][j] = gv[i];
+    }
+    for (int p = 0; p < P3; p++) {
+      const int    pa = p % P, pb = (p / P) % P, pc = p / (P * P);
+      const double bx = B[qx * P + pa], by = B[qy * P + pb], bz = B[qz * P + pc];
+      const double gx = G[qx * P + pa], gy = G[qy * P + pb], gz = G[qz * P + pc];
+      const double phi[4] = {bx * by * bz, gx * by * bz, bx * gy * bz, bx * by * gz};
+      for (int c = 0; c < 5; c++) {
+        double acc = 0;
+        for (int mo = 0; mo < 4; mo++) acc += phi[mo] * A[mo == 0 ? c : 5 + (mo - 1) * 5 + c][c] * phi[0];
+        de[c * P3 + p] += acc;
+      }
+    }
+  }
+  for (int c = 0; c < 5; c++)
+    for (int p = 0; p < P3; p++) a->v[m->offsets[e * P3 + p] + c] += de[c * P3 + p];
+}
+
+int oracle_assemble_mass_stab_diagonal(const OracleMesh *m, OracleQF qf, void *ctx, const double *q, const double *qdata, double *diag,
+                                       int64_t l_size) {
+  ApplyArgs a = {qf, ctx, q, NULL, qdata, NULL, NULL, NULL, diag, 14};
+  int       err = 0;
+  memset(diag, 0, sizeof(double) * l_size);
+  const size_t P3 = (size_t)m->P * m->P * m->P, Q3 = (size_t)m->Q * m->Q * m->Q;
+  for_each_elem(m, mass_stab_diag_elem, &a, 10 * P3 + 5 * Q3, &err);
+  return err;
+}
+
 int oracle_setup_qdata(int num_elem, int Q, const double *x_elem, double *qdata) {
   const int Q3 = Q * Q * Q;
   double    B[32], G[32], w1[16];

@@ -103,6 +103,13 @@ int oracle_qf_rhs_conserv(void *ctx, int Q, const double *const *in, double *con
  * (in: u [5][Q], qdata [10][Q]; out: v [5][Q]) -- oracle_qf_mass or the reference's Mass_5.  v is overwritten. */
 int oracle_apply_mass(const OracleMesh *m, OracleQF qf, const double *u, const double *qdata, double *v, int64_t l_size);
 int oracle_qf_mass(void *ctx, int Q, const double *const *in, double *const *out);
+/* The SUPG-stabilized mass operator (MassFunction_Newtonian: in q_dot [5][Q], q [5][Q], qdata [10][Q]; out v [5][Q],
+ * Grad_v [3][5][Q]), applied to q_dot at the state q.  v is overwritten. */
+int oracle_apply_mass_stab(const OracleMesh *m, OracleQF qf, void *ctx, const double *q_dot, const double *q, const double *qdata, double *v,
+                           int64_t l_size);
+int oracle_qf_mass_stab_conserv(void *ctx, int Q, const double *const *in, double *const *out);
+int oracle_assemble_mass_stab_diagonal(const OracleMesh *m, OracleQF qf, void *ctx, const double *q, const double *qdata, double *diag,
+                                       int64_t l_size);
 
 /* Point-block diagonal of the IJacobian operator (CeedOperatorLinearAssemblePointBlockDiagonal semantics): a row-major
  * 5 x 5 block per node, out[(node * 5 + i) * 5 + j] (5 * l_size values), overwritten. */

@@ -63,6 +63,7 @@ def _declare(L):
     L.oracle_apply_mass.restype = C.c_int
     L.oracle_qf_rhs_conserv.restype = C.c_int
     L.oracle_qf_mass.restype = C.c_int
+    L.oracle_qf_mass_stab_conserv.restype = C.c_int
     L.oracle_apply_ijacobian.restype = C.c_int
     L.oracle_assemble_diagonal.restype = C.c_int
     L.oracle_assemble_point_block.restype = C.c_int
@@ -193,6 +194,31 @@ def assemble_point_block(mesh: Mesh, ctx: bytes, qdata, jac_data, l_size, num_jd
     if L.oracle_assemble_point_block(C.byref(mesh.c), fn, cbuf, ptr(qdata), ptr(jac_data), C.c_int(num_jd), ptr(out), C.c_int64(l_size)):
         raise RuntimeError("oracle point-block assembly failed")
     return out
+
+
+def apply_mass_stab(mesh: Mesh, ctx: bytes, q_dot, q, qdata, use_ref=False):
+    """The SUPG-stabilized mass applied to q_dot at state q (MassFunction_Newtonian: the restatement, or the reference's)."""
+    L = lib()
+    fn = qf("ref_MassFunction_Newtonian_Conserv" if use_ref else "oracle_qf_mass_stab_conserv", use_ref)
+    v = np.zeros_like(q_dot)
+    cbuf = C.create_string_buffer(bytes(ctx), len(ctx))
+    L.oracle_apply_mass_stab.restype = C.c_int
+    if L.oracle_apply_mass_stab(C.byref(mesh.c), fn, cbuf, ptr(np.ascontiguousarray(q_dot)), ptr(np.ascontiguousarray(q)), ptr(qdata), ptr(v),
+                                C.c_int64(v.size)):
+        raise RuntimeError("oracle stabilized mass failed")
+    return v
+
+
+def mass_stab_diagonal(mesh: Mesh, ctx: bytes, q, qdata, l_size, use_ref=False):
+    """Diagonal of the stabilized mass at the state q."""
+    L = lib()
+    fn = qf("ref_MassFunction_Newtonian_Conserv" if use_ref else "oracle_qf_mass_stab_conserv", use_ref)
+    d = np.zeros(l_size)
+    cbuf = C.create_string_buffer(bytes(ctx), len(ctx))
+    L.oracle_assemble_mass_stab_diagonal.restype = C.c_int
+    if L.oracle_assemble_mass_stab_diagonal(C.byref(mesh.c), fn, cbuf, ptr(np.ascontiguousarray(q)), ptr(qdata), ptr(d), C.c_int64(l_size)):
+        raise RuntimeError("oracle stabilized-mass diagonal failed")
+    return d
 
 
 def setup_qdata(num_elem, Q, x_elem):

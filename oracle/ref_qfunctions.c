@@ -10,6 +10,7 @@
 
 #include "bc_freestream.h"
 #include "channel.h"
+#include "gaussianwave.h"
 #include "differential_filter.h"
 #include "grid_anisotropy_tensor.h"
 #include "mass.h"
@@ -34,10 +35,13 @@ EXPORT int ref_IJacobian_Newtonian_Entropy(void *c, CeedInt Q, In in, Out out) {
 EXPORT int ref_Setup(void *c, CeedInt Q, In in, Out out) { return Setup(c, Q, in, out); }
 EXPORT int ref_RHSFunction_Newtonian(void *c, CeedInt Q, In in, Out out) { return RHSFunction_Newtonian(c, Q, in, out); }
 EXPORT int ref_Mass_5(void *c, CeedInt Q, In in, Out out) { return Mass_5(c, Q, in, out); }
+EXPORT int ref_MassFunction_Newtonian_Conserv(void *c, CeedInt Q, In in, Out out) { return MassFunction_Newtonian_Conserv(c, Q, in, out); }
 EXPORT int ref_MonitorTotalKineticEnergy_Conserv(void *c, CeedInt Q, In in, Out out) { return MonitorTotalKineticEnergy_Conserv(c, Q, in, out); }
 EXPORT int ref_ICsTaylorGreen(void *c, CeedInt Q, In in, Out out) { return ICsTaylorGreen(c, Q, in, out); }
 EXPORT int ref_ICsChannel(void *c, CeedInt Q, In in, Out out) { return ICsChannel(c, Q, in, out); }
 EXPORT size_t ref_channel_ctx_size(void) { return sizeof(struct ChannelContext_); }
+EXPORT int ref_IC_GaussianWave_Conserv(void *c, CeedInt Q, In in, Out out) { return IC_GaussianWave_Conserv(c, Q, in, out); }
+EXPORT size_t ref_gaussianwave_ctx_size(void) { return sizeof(struct GaussianWaveContext_); }
 
 /* State helpers: q (5) in state_var -> U (5) and Y (5); forward-mode tangents. */
 EXPORT void ref_StateFromQ(const NewtonianIGProperties *gas, const CeedScalar q[5], int state_var, CeedScalar U[5], CeedScalar Y[5]) {

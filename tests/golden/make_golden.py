@@ -12,6 +12,8 @@ Outputs (committed; the GPU box has no reference tree):
                             reference's StateToQ outputs for every (A, B) pair
   channel_be5.npz           the free DOFs of the final state of the "Channel" run (examples/navierstokes.c:252:
                             examples/channel.yaml, 5 x 5 x 1 faces, 5 backward-Euler steps), tests/output/channel.bin
+  gaussianwave_explicit.npz the free DOFs of the final state of "Gaussian Wave, explicit, supg, IDL" (examples/navierstokes.c:233),
+                            tests/output/gaussianwave-explicit.bin (a 64-bit-index HONEE file)
   taylorgreen_rk4.npz       every row of tests/output/taylorgreen_totalke.csv (steps 0, 2, 3 of the explicit RK4 run of
                             examples/navierstokes.c:222) and the final state of that run, tests/output/taylor-green.bin
                             (HONEE binary format, src/honee-file.c:194-217: int32 token, int32 step, float64 time, then a
@@ -144,6 +146,22 @@ def main():
                         q_extra=np.int64(2), box_hi=np.array([0.01, 0.01, 0.001]), mu=np.float64(0.01), umax=np.float64(40.0),
                         dt=np.float64(5e-6), steps=np.int64(5), essential=np.array("y-:1,2,3 y+:1,2,3 z-:3 z+:3"), compare_atol=np.float64(2e-11),
                         source=np.array("tests/output/channel.bin (examples/navierstokes.c:252, examples/channel.yaml)"))
+
+    # ---- Gaussian wave, explicit, SUPG, IDL (examples/navierstokes.c:233): free DOFs of the final state, a 64-bit-index file
+    #      (token 0x0CEEDF64: int64 step, float64 time, int64 class id, int64 length, values)
+    raw = open(os.path.join(args.ref, "tests/output/gaussianwave-explicit.bin"), "rb").read()
+    assert int(np.frombuffer(raw[:4], dtype=">i4")[0]) == 0x0CEEDF64
+    step = np.frombuffer(raw[4:12], dtype=">i8")[0]
+    t_final = np.frombuffer(raw[12:20], dtype=">f8")[0]
+    classid, length = np.frombuffer(raw[20:36], dtype=">i8")
+    assert int(classid) == 1211214 and len(raw) == 36 + 8 * int(length)
+    np.savez_compressed(os.path.join(HERE, "gaussianwave_explicit.npz"), final_step=np.int64(step), final_time=np.float64(t_final),
+                        free_state=np.frombuffer(raw[36:], dtype=">f8").astype(np.float64), faces=np.array([2, 2, 1]), degree=np.int64(3),
+                        box_hi=np.array([1.0, 1.0, 0.025]), reference_PuT=np.array([71.75, 2.0, 2.0, 0.0, 0.25]),
+                        epicenter=np.array([0.33, 0.75, 0.0]), amplitude=np.float64(2.0), width=np.float64(0.05), mu=np.float64(0.0),
+                        dt=np.float64(2e-3), steps=np.int64(5), rk_type=np.array("5f"), mass_ksp=np.array("gmres"),
+                        mass_pc_jacobi=np.array("diagonal"), idl=np.array([2e-3, 0.0, 0.25, 70.0]), compare_atol=np.float64(1e-8),
+                        source=np.array("tests/output/gaussianwave-explicit.bin (examples/navierstokes.c:233, examples/gaussianwave.yaml)"))
 
     # ---- UnitTests_Newtonian inputs (problems/newtonian.c:947-987) and reference StateToQ outputs
     ctx = prob.newtonian_context(2)

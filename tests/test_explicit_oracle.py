@@ -120,3 +120,88 @@ def test_lumped_mass_is_distinguishable_from_the_reference_run():
     rows, q, _ = run_oracle_tg("preonly", "rowsum")
     ke3 = rows[3][0]
     assert abs(ke3 - G["ke"][2, 0]) > 1e-8 * abs(G["ke"][2, 0])
+
+
+@pytest.mark.parametrize("stab", [prob.STAB_SUPG, prob.STAB_SU, prob.STAB_NONE])
+def test_stabilized_mass_restatement_equals_reference(stab):
+    """MassFunction_Newtonian (qfunctions/newtonian.h:44-86), the mass operator HONEE uses for explicit SUPG runs."""
+    if O.ref() is None:
+        pytest.skip("oracle/_ref not built")
+    mesh, basis, ctx, q, qd = case((2, 2, 1), 4, 4, stab=stab)
+    m = oracle_mesh(mesh, basis)
+    qdata = O.setup_qdata(mesh.num_elem, basis.Q, mesh.x_elem)
+    cb = prob.context_bytes(ctx)
+    np.testing.assert_array_equal(O.apply_mass_stab(m, cb, qd, q, qdata), O.apply_mass_stab(m, cb, qd, q, qdata, use_ref=True))
+
+
+def test_stabilized_mass_diagonal_is_the_operator_diagonal():
+    mesh, basis, ctx, q, _ = case((2, 1, 1), 3, 4, periodic=(1, 0, 0))
+    m = oracle_mesh(mesh, basis)
+    qdata = O.setup_qdata(mesh.num_elem, basis.Q, mesh.x_elem)
+    cb = prob.context_bytes(ctx)
+    d = O.mass_stab_diagonal(m, cb, q, qdata, mesh.l_size)
+    for i in np.random.default_rng(4).choice(mesh.l_size, 25, replace=False):
+        e = np.zeros(mesh.l_size)
+        e[i] = 1.0
+        assert abs(O.apply_mass_stab(m, cb, e, q, qdata)[i] - d[i]) <= 1e-13 * np.abs(d).max()
+
+
+def gaussian_wave_explicit_case():
+    """"Gaussian Wave, explicit, supg, IDL" (examples/navierstokes.c:233, examples/gaussianwave.yaml): degree 3 on 2 x 2 x 1 faces
+    of [0,1]^2 x [0,0.025], free-stream faces (HLLC) on the x and y sides, symmetry planes (z momentum) on the z sides, SUPG,
+    the internal damping layer, TSRK5F with dt 2e-3, GMRES + Jacobi-diagonal solves of the stabilized mass."""
+    import face_oracle as FO
+    G = np.load(os.path.join(GOLD, "gaussianwave_explicit.npz"))
+    hi = tuple(float(v) for v in G["box_hi"])
+    deg = int(G["degree"])
+    P = Q = deg + 1
+    mesh = prob.box_mesh(tuple(int(v) for v in G["faces"]), P, hi=hi)
+    basis = prob.tensor_basis(P, Q)
+    Pr, ux, uy, uz, T = (float(v) for v in G["reference_PuT"])
+    decay, start, length, p_idl = (float(v) for v in G["idl"])
+    newt = prob.newtonian_context(deg, mu=float(G["mu"]), stab=prob.STAB_SUPG, implicit=False, idl=(decay, start, length, p_idl), dt=float(G["dt"]))
+    gw = prob.gaussian_wave_context(newt, Pr, (ux, uy, uz), T, epicenter=tuple(float(v) for v in G["epicenter"]), width=float(G["width"]),
+                                    amplitude=float(G["amplitude"]))
+    q = prob.gaussian_wave_state(mesh, basis, gw)
+    ess = prob.box_essential(mesh, {"z-": (3,), "z+": (3,)})
+    q[ess] = 0.0
+    off, xn, _ = prob.box_faces(mesh, basis, sides=["x-", "x+", "y-", "y+"])
+    fs = prob.freestream_context(newt, Pr, (ux, uy, uz), T)
+    U, Y = prob.state_from_primitive(newt.gas, Pr, (ux, uy, uz), T)
+    return G, mesh, basis, newt, gw, q, ess, off, xn, fs, U, Y, FO
+
+
+def test_gaussian_wave_initial_state_equals_reference():
+    if O.ref() is None:
+        pytest.skip("oracle/_ref not built")
+    G, mesh, basis, newt, gw, q, ess, off, xn, fs, U, Y, FO = gaussian_wave_explicit_case()
+    import ctypes as C
+    assert O.ref().ref_gaussianwave_ctx_size() == C.sizeof(gw)
+    X_ = prob.node_coordinates(mesh, basis)
+    qr = np.zeros((5, X_.shape[1]))
+    O.call_qf(O.ref().ref_IC_GaussianWave_Conserv, bytes(memoryview(gw)), X_.shape[1], [np.ascontiguousarray(X_)], [qr])
+    qr = qr.T.reshape(-1)
+    qr[ess] = 0.0  # the reference's IC has zero z momentum there too
+    np.testing.assert_array_equal(q, qr)
+
+
+def test_oracle_reproduces_reference_gaussian_wave_explicit_run():
+    G, mesh, basis, newt, gw, q, ess, off, xn, fs, U, Y, FO = gaussian_wave_explicit_case()
+    P, Q = basis.P, basis.Q
+    m = oracle_mesh(mesh, basis)
+    qdata = O.setup_qdata(mesh.num_elem, Q, mesh.x_elem)
+    xq = O.coords_at_qpts(mesh.num_elem, Q, mesh.x_elem)
+    qd_sur = FO.face_qdata(basis.interp1d, basis.grad1d, basis.qweight1d, P, Q, xn)
+    gas = newt.gas
+    faces = lambda qq: FO.freestream_apply(off, basis.interp1d, P, Q, qd_sur, qq, U, Y, gas.cv, gas.cp, hllc=True, l_size=mesh.l_size)  # noqa
+    ex = X.Explicit(m, P, Q, prob.context_bytes(newt), qdata, mesh.l_size, dt=float(G["dt"]), tableau=str(G["rk_type"]),
+                    mass_ksp=str(G["mass_ksp"]), pc_jacobi=str(G["mass_pc_jacobi"]), x_q=xq, essential=ess, faces=faces)
+    assert ex.stab_mass
+    t = 0.0
+    for _ in range(int(G["steps"])):
+        q = ex.step(q, t)
+        t += float(G["dt"])
+    free = np.setdiff1d(np.arange(mesh.l_size), ess)
+    ref = G["free_state"]
+    err = np.abs(np.sort(q[free]) - np.sort(ref)).max() / np.abs(ref).max()
+    assert err <= float(G["compare_atol"]), err
