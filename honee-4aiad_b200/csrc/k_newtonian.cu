@@ -58,8 +58,11 @@ __host__ __device__ constexpr int nthreads_for(int Q) {
 }
 // resident CTAs per SM the register budget is tuned for (65536 registers / (threads * CTAs)); the FP32 Jacobian holds
 // half the point-wise state in registers and fits four CTAs (121 registers, no spills at P=4, Q=5)
+#ifndef HB_F32_MIN_BLOCKS
+#define HB_F32_MIN_BLOCKS 4
+#endif
 __host__ __device__ constexpr int min_blocks_for(int Q, bool staged = true, int elem_bytes = 8) {
-  return Q <= 5 ? (elem_bytes == 4 ? 4 : (staged ? 3 : 4)) : (Q == 6 ? 2 : 1);
+  return Q <= 5 ? (elem_bytes == 4 ? HB_F32_MIN_BLOCKS : (staged ? 3 : 4)) : (Q == 6 ? 2 : 1);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------

@@ -14,6 +14,8 @@ Outputs (committed; the GPU box has no reference tree):
                             examples/channel.yaml, 5 x 5 x 1 faces, 5 backward-Euler steps), tests/output/channel.bin
   gaussianwave_explicit.npz the free DOFs of the final state of "Gaussian Wave, explicit, supg, IDL" (examples/navierstokes.c:233),
                             tests/output/gaussianwave-explicit.bin (a 64-bit-index HONEE file)
+  ref_*.bin                 copies of tests/output/{channel,taylor-green,gaussianwave-explicit}.bin, the reference's own
+                            solution files, for the checks of the file-format reader (honee-4aiad_b200/honee_file.py)
   taylorgreen_rk4.npz       every row of tests/output/taylorgreen_totalke.csv (steps 0, 2, 3 of the explicit RK4 run of
                             examples/navierstokes.c:222) and the final state of that run, tests/output/taylor-green.bin
                             (HONEE binary format, src/honee-file.c:194-217: int32 token, int32 step, float64 time, then a
@@ -162,6 +164,11 @@ def main():
                         dt=np.float64(2e-3), steps=np.int64(5), rk_type=np.array("5f"), mass_ksp=np.array("gmres"),
                         mass_pc_jacobi=np.array("diagonal"), idl=np.array([2e-3, 0.0, 0.25, 70.0]), compare_atol=np.float64(1e-8),
                         source=np.array("tests/output/gaussianwave-explicit.bin (examples/navierstokes.c:233, examples/gaussianwave.yaml)"))
+
+    # ---- raw solution files of the reference's runs (32- and 64-bit-index HONEE files) for the file-format reader
+    import shutil
+    for name in ("channel.bin", "taylor-green.bin", "gaussianwave-explicit.bin"):
+        shutil.copyfile(os.path.join(args.ref, "tests/output", name), os.path.join(HERE, "ref_" + name))
 
     # ---- UnitTests_Newtonian inputs (problems/newtonian.c:947-987) and reference StateToQ outputs
     ctx = prob.newtonian_context(2)

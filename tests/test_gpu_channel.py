@@ -63,3 +63,46 @@ def test_channel_run_reproduces_reference(fp32, pc):
     qf = out.cpu().numpy()
     assert np.all(qf[idx] == 0.0)
     assert free_state_error(qf, idx, G) <= float(G["compare_atol"])
+
+
+def test_checkpoint_and_resume_through_a_honee_file(tmp_path):
+    """3 steps, a HONEE solution file (free DOFs, step, time), a fresh stepper resumed from it for 2 more steps: the same
+    state as 5 uninterrupted steps (backward Euler carries no history) and as the reference's channel.bin."""
+    import torch
+    HF = importlib.import_module("honee-4aiad_b200.honee_file")
+    G, mesh, basis, ch, q, idx = channel_case()
+    op = K.ElemOp(mesh, basis)
+    x = torch.from_numpy(np.ascontiguousarray(mesh.x_elem)).to(_dev())
+    qdata = torch.zeros(mesh.num_elem * 10 * basis.Q ** 3, dtype=torch.float64, device=_dev())
+    op.setup_qdata(x, qdata)
+    dt = float(G["dt"])
+
+    def stepper():
+        ts = S.TimeStepper(op, prob.context_bytes(ch.newt_ctx), qdata, dt=dt, bdf_order=1, newton_rtol=1e-8)
+        ts.set_essential(idx)
+        return ts
+
+    ts = stepper()
+    tq = torch.from_numpy(q).to(_dev())
+    ts.set_state(tq, 0.0)
+    for _ in range(5):
+        ts.step()
+    full = torch.empty_like(tq)
+    ts.get_state(full)
+    ts = stepper()
+    ts.set_state(tq, 0.0)
+    for _ in range(3):
+        ts.step()
+    mid = torch.empty_like(tq)
+    t = ts.get_state(mid)
+    path = str(tmp_path / "channel-3.bin")
+    HF.write(path, HF.free_values(mid.cpu().numpy(), idx), step=3, time=t)
+    f = HF.read(path)
+    ts2 = stepper()
+    ts2.set_state(torch.from_numpy(HF.expand(f.values, mesh.l_size, idx)).to(_dev()), f.time)
+    for _ in range(2):
+        ts2.step()
+    out = torch.empty_like(tq)
+    assert abs(ts2.get_state(out) - 5 * dt) < 1e-18
+    np.testing.assert_array_equal(out.cpu().numpy(), full.cpu().numpy())
+    assert free_state_error(out.cpu().numpy(), idx, G) <= float(G["compare_atol"])
