@@ -427,6 +427,33 @@ def channel_state(mesh: BoxMesh, basis: TensorBasis, ch: ChannelContext) -> np.n
     return np.ascontiguousarray(q.T.reshape(-1))
 
 
+def tanh_planes(n: int, lo: float, hi: float, beta: float) -> np.ndarray:
+    """n + 1 vertex planes on [lo, hi] clustered towards both ends: y = c + h tanh(beta (2 j / n - 1)) / tanh(beta) with
+    c, h the centre and half-width (the usual wall-resolved channel grading; beta = 0 gives uniform planes)."""
+    eta = 2 * np.arange(n + 1) / n - 1
+    c, h = 0.5 * (lo + hi), 0.5 * (hi - lo)
+    if beta == 0:
+        return c + h * eta
+    y = c + h * np.tanh(beta * eta) / math.tanh(beta)
+    y[0], y[-1] = lo, hi
+    return y
+
+
+def perturbed_channel_state(mesh: BoxMesh, basis: TensorBasis, ch: ChannelContext, amplitude=0.05, seed=0) -> np.ndarray:
+    """channel_state with seeded uniform velocity perturbations of +-amplitude * umax in every component at every node
+    (the essential DOFs take their wall values when the state is set on a stepper with them)."""
+    X = node_coordinates(mesh, basis)
+    gas = ch.newt_ctx.gas
+    eta = (X[1] - ch.center) / ch.H
+    Pr = gas.mu / (gas.cp * gas.k)
+    Ec = ch.umax ** 2 / (gas.cp * ch.theta0)
+    theta = ch.theta0 * (1 + (Pr * Ec / 3) * (1 - eta ** 4))
+    u = np.stack([ch.umax * (1 - eta ** 2), 0 * eta, 0 * eta])
+    u = u + amplitude * ch.umax * np.random.default_rng(seed).uniform(-1, 1, u.shape)
+    q = conservative_from_primitive(gas, ch.P0 * np.ones_like(eta), u, theta)
+    return np.ascontiguousarray(q.T.reshape(-1))
+
+
 def box_essential(mesh: BoxMesh, sides: dict):
     """Essential DOFs of box sides: {"y-": (1, 2, 3), ...} -> sorted unique L-vector indices node * 5 + component (the
     bc_*_essential_comps of HONEE's options; PETSc's box face sets 1/2 are z-/z+, 3/4 y-/y+, 5/6 x+/x-)."""

@@ -407,6 +407,70 @@ HB_EXPORT int hb_ts_set_essential(HbTimeStepper *ts, const int32_t *h_idx, const
  * tangent every Krylov product (FP32 in mixed precision) and its diagonal the Jacobi preconditioner (FP64). */
 HB_EXPORT int hb_ts_set_freestream(HbTimeStepper *ts, const HbFaceOp *faces, const void *ctx264, int flux_type, const double *qdata_sur);
 
+/* ---- spanwise statistics of turbulence quantities ------------------------------------------------------------------
+ * HONEE's -ts_monitor_spanstats_turbulence (src/spanstats/turbulence.c:152-278, src/spanstats/spanstats.c:343-470):
+ * every step the 22 statistics of qfunctions/spanstats/turbulence.h:8-32 (mean density, pressure, pressure squared,
+ * pressure-velocity, density-temperature and its fluxes, momentum, momentum fluxes, velocity), weighted by w detJ and by
+ * the step's time increment, are summed over the span onto the quadrature points of the 2D parent plane; processing
+ * divides by the duration and the span width, projects onto the parent nodes (B^T) and solves with the parent mass
+ * matrix (CG, point Jacobi, natural norm), giving the time- and span-averaged fields [parent node][22]. */
+#define HB_TURB_NUM_COMPONENTS 22
+
+/* The parent plane: a 2D tensor-product mesh of P^2-node elements whose quadrature points carry the (x, y) of the
+ * child elements' points (DMPlexFilter of the spanwise face, spanstats.c:42-112, with the same P and Q).  Offsets are
+ * node indices into [num_nodes][22] vectors; colours as in HbElemOp. */
+typedef struct HbPlaneOp {
+  int            num_elem, P, Q;
+  int64_t        num_nodes;
+  int32_t       *d_offsets;     /* device [num_elem][P^2] */
+  int            num_colors;
+  int32_t       *h_color_ptr;
+  int32_t       *d_color_elem;
+  double         interp1d[HB_MAX_P * HB_MAX_P];
+  double         qref1d[HB_MAX_P], qweight1d[HB_MAX_P];
+  double        *d_wdetJ;       /* device [num_elem][Q^2] */
+} HbPlaneOp;
+
+/* Parent-point sums of one collection (ChildStatsCollection_Conserv applied and reduced over the span,
+ * turbulence.c:19-108 + spanstats.c:425-443): sums[col][Q^2][22] += sum over the elements d_column_elems[col][*] and their
+ * quadrature planes of w detJ * dt * stats(q).  Each column lists the 3D elements whose first two reference axes
+ * coincide with those of parent element `col`.  Conservative state only. */
+HB_EXPORT int hb_stats_collect(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double dt, int num_columns,
+                               int column_length, const int32_t *d_column_elems, double *sums, void *stream);
+/* Parent mass matrix M (HoneeMassQFunctionCreate on the parent basis, spanstats.c:313-320), 22 components: v (+)= M u */
+HB_EXPORT int hb_plane_mass_apply(const HbPlaneOp *pl, const double *u, double *v, int add, void *stream);
+/* Its diagonal, one value per node (the same for all 22 components). */
+HB_EXPORT int hb_plane_mass_diagonal(const HbPlaneOp *pl, double *diag, int add, void *stream);
+/* Projection right-hand side v (+)= B^T (scale * sums) (the identity QFunction of spanstats.c:302-309). */
+HB_EXPORT int hb_plane_project_rhs(const HbPlaneOp *pl, const double *sums, double scale, double *v, int add, void *stream);
+/* w detJ of the parent points from the bilinear vertex coordinates x_plane [num_elem][3][4] (vertex a + 2b), as
+ * Setup2D_3Dcoords (qfunctions/setupgeo2d.h:136-152) computes it: weight times |dx/dX0 x dx/dX1|.  Device pointers. */
+HB_EXPORT int hb_plane_setup_qdata(int num_elem, int Q, const double *qref1d, const double *qweight1d, const double *x_plane, double *wdetJ,
+                                   void *stream);
+
+/* The statistics monitor: owns the parent plane, the columns, the sums and the projection work space. */
+typedef struct HbSpanStats HbSpanStats;
+/* op: the 3D operator (its P, Q and basis are the parent's); column_elems [num_columns][column_length] host element ids;
+ * parent_offsets [num_columns][P^2] host parent-node indices (< num_parent_nodes); parent_x [num_columns][3][4] host
+ * vertex coordinates; span_width the spanwise extent of the domain (spanstats.c:52-54). */
+HB_EXPORT int hb_spanstats_create(const HbElemOp *op, int num_columns, int column_length, const int32_t *column_elems,
+                                  const int32_t *parent_offsets, int64_t num_parent_nodes, const double *parent_x, double span_width,
+                                  HbSpanStats **st);
+/* Zero the sums and start a new averaging window at initial_time (SpanwiseStatisticsSetupFinalize, spanstats.c:371-389). */
+HB_EXPORT int hb_spanstats_reset(HbSpanStats *st, double initial_time, void *stream);
+/* One collection at solution_time (SpanwiseStatisticsCollect, spanstats.c:392-411): dt = solution_time - previous time. */
+HB_EXPORT int hb_spanstats_collect(HbSpanStats *st, const void *ctx184, const double *q, const double *qdata, double solution_time, void *stream);
+/* Device pointer to the parent-point sums [num_columns][Q^2][22] and the parent plane. */
+HB_EXPORT int hb_spanstats_view(const HbSpanStats *st, const double **d_sums, const HbPlaneOp **plane);
+/* Copy the sums into dst (host or device; synchronous). */
+HB_EXPORT int hb_spanstats_copy_sums(const HbSpanStats *st, double *dst);
+/* Processing at solution_time (SpanwiseStatisticsProcess, spanstats.c:414-458): stats [num_parent_nodes][22] (device)
+ * solves M stats = B^T sums / ((solution_time - initial_time) * span_width); rtol as -ts_monitor_spanstats_turbulence_ksp_rtol
+ * (default 1e-10).  HB_ERROR_INCOMPLETE when max_it iterations do not reach it. */
+HB_EXPORT int hb_spanstats_process(HbSpanStats *st, double solution_time, double rtol, int max_it, double *stats, int *its, double *rel_norm,
+                                   void *stream);
+HB_EXPORT int hb_spanstats_destroy(HbSpanStats *st);
+
 /* Library identification */
 const char *hb_version(void);
 

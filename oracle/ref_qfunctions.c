@@ -18,6 +18,7 @@
 #include "newtonian.h"
 #include "setupgeo.h"
 #include "sgs_dd_model.h"
+#include "spanstats/turbulence.h"
 #include "taylorgreen.h"
 
 #include <stddef.h>
@@ -42,6 +43,8 @@ EXPORT int ref_ICsChannel(void *c, CeedInt Q, In in, Out out) { return ICsChanne
 EXPORT size_t ref_channel_ctx_size(void) { return sizeof(struct ChannelContext_); }
 EXPORT int ref_IC_GaussianWave_Conserv(void *c, CeedInt Q, In in, Out out) { return IC_GaussianWave_Conserv(c, Q, in, out); }
 EXPORT size_t ref_gaussianwave_ctx_size(void) { return sizeof(struct GaussianWaveContext_); }
+EXPORT int ref_ChildStatsCollection_Conserv(void *c, CeedInt Q, In in, Out out) { return ChildStatsCollection_Conserv(c, Q, in, out); }
+EXPORT size_t ref_turb_spanstats_ctx_size(void) { return sizeof(struct Turbulence_SpanStatsContext_); }
 
 /* State helpers: q (5) in state_var -> U (5) and Y (5); forward-mode tangents. */
 EXPORT void ref_StateFromQ(const NewtonianIGProperties *gas, const CeedScalar q[5], int state_var, CeedScalar U[5], CeedScalar Y[5]) {
