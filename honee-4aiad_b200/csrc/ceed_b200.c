@@ -1492,6 +1492,18 @@ static int plan_freestream(CeedOperator op, int jacobian, int flux_type) {
   return CEED_ERROR_SUCCESS;
 }
 
+
+/* The state variable a Newtonian QFunction name selects (newtonian.h:259-269, 313-323): "<prefix>Conserv" 0, "<prefix>Prim" 1,
+ * "<prefix>Entropy" 2, anything else -1. */
+static int newtonian_state_var(const char *k, const char *prefix) {
+  const size_t n = strlen(prefix);
+  if (strncmp(k, prefix, n)) return -1;
+  if (!strcmp(k + n, "Conserv")) return HB_STATEVAR_CONSERVATIVE;
+  if (!strcmp(k + n, "Prim")) return HB_STATEVAR_PRIMITIVE;
+  if (!strcmp(k + n, "Entropy")) return HB_STATEVAR_ENTROPY;
+  return -1;
+}
+
 static int op_plan(CeedOperator op) {
   if (op->plan != PLAN_NONE) return CEED_ERROR_SUCCESS;
   CK(op_check_fields(op));
@@ -1509,7 +1521,8 @@ static int op_plan(CeedOperator op) {
     op->plan = PLAN_SETUP;
     return CEED_ERROR_SUCCESS;
   }
-  if (!strcmp(k, "IFunction_Newtonian_Conserv")) {
+  const int sv_if = newtonian_state_var(k, "IFunction_Newtonian_"), sv_ij = newtonian_state_var(k, "IJacobian_Newtonian_");
+  if (sv_if >= 0) {
     if (qf->nin < 5 || qf->nout != 3 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[1].emode != CEED_EVAL_GRAD ||
         qf->in[2].emode != CEED_EVAL_INTERP || qf->in[3].emode != CEED_EVAL_NONE || qf->out[0].emode != CEED_EVAL_INTERP ||
         qf->out[1].emode != CEED_EVAL_GRAD || qf->out[2].emode != CEED_EVAL_NONE)
@@ -1523,6 +1536,7 @@ static int op_plan(CeedOperator op) {
     if (op->in[0].b != op->in[1].b || op->in[0].b != op->in[2].b || op->in[0].b != op->out[0].b || op->in[0].b != op->out[1].b)
       return plan_fail(op, "state fields must share one basis");
     if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+    if (((const HbNewtonianContext *)qf->ctx->data)->state_var != sv_if) return plan_fail(op, "the context's state_var differs from the QFunction's");
     CK(plan_elemop(op, op->in[0].r, op->in[0].b));
     const int Q3 = op->eop->Q * op->eop->Q * op->eop->Q;
     CK(check_qdata_rstr(op, op->in[3].r, 10, Q3, "qdata"));
@@ -1532,7 +1546,7 @@ static int op_plan(CeedOperator op) {
     op->plan = PLAN_IFUNCTION;
     return CEED_ERROR_SUCCESS;
   }
-  if (!strcmp(k, "IJacobian_Newtonian_Conserv")) {
+  if (sv_ij >= 0) {
     if (qf->nin != 4 || qf->nout != 2 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[1].emode != CEED_EVAL_GRAD ||
         qf->in[2].emode != CEED_EVAL_NONE || qf->in[3].emode != CEED_EVAL_NONE || qf->out[0].emode != CEED_EVAL_INTERP ||
         qf->out[1].emode != CEED_EVAL_GRAD)
@@ -1543,6 +1557,7 @@ static int op_plan(CeedOperator op) {
     if (op->in[0].r != op->in[1].r || op->in[0].r != op->out[0].r || op->in[0].r != op->out[1].r) return plan_fail(op, "shared restriction expected");
     if (op->in[0].b != op->in[1].b || op->in[0].b != op->out[0].b || op->in[0].b != op->out[1].b) return plan_fail(op, "shared basis expected");
     if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+    if (((const HbNewtonianContext *)qf->ctx->data)->state_var != sv_ij) return plan_fail(op, "the context's state_var differs from the QFunction's");
     CK(plan_elemop(op, op->in[0].r, op->in[0].b));
     const int Q3 = op->eop->Q * op->eop->Q * op->eop->Q;
     CK(check_qdata_rstr(op, op->in[2].r, 10, Q3, "qdata"));

@@ -77,8 +77,8 @@ void hb_solver_default_options(HbSolverOptions *o) {
   o->newton_rtol   = 1e-8;
   o->newton_atol   = 1e-30;
   o->newton_max_it = 20;
-  o->ksp_rtol      = 1e-5; /* PETSc's KSP default */
-  o->ksp_max_it    = 200;
+  o->ksp_rtol      = 1e-5;  /* PETSc's KSP defaults: rtol 1e-5, at most 10000 iterations */
+  o->ksp_max_it    = 10000;
   o->gmres_restart = 30;
   o->pc_jacobi     = 1;
   o->jacobian_fp32 = 0;

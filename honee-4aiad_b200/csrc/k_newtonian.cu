@@ -546,7 +546,7 @@ struct IfunctionPtrs {
   int qdata_tma;      // qdata blocks can be bulk-copied (16-byte aligned base)
 };
 
-template <int P, int Q, bool ST, int SGS = 0>
+template <int P, int Q, bool ST, int SGS = 0, int SV = HB_STATEVAR_CONSERVATIVE>
 __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p,
                                                                                                const SgsArg<SGS> sg) {
   constexpr int NT = nthreads_for<double>(Q);
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
           if (jd32) jd32[k * Q3] = float(val);
         }
       };
-      ifunction_point_stream<double>(a.pc, qi, gref, qd, wdetJ, X, x0, v, gv, emit);
+      ifunction_point_stream<double, SV>(a.pc, qi, gref, qd, wdetJ, X, x0, v, gv, emit);
       if constexpr (SGS > 0) sgs_add<SGS>(a.pc, qi, gref, wdetJ, X, sg, gv);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
@@ -715,7 +715,7 @@ struct IjacobianPtrs {
   int qdata_tma, jd_tma;
 };
 
-template <int P, int Q, typename T, bool ST>
+template <int P, int Q, typename T, bool ST, int SV = HB_STATEVAR_CONSERVATIVE>
 __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int)sizeof(T))) k_ijacobian(const ElemArgs<T> a, const IjacobianPtrs<T> p) {
   constexpr int NT = nthreads_for<T>(Q);
   using L = Plan<P, Q, 1, T, true, ST>;
@@ -812,7 +812,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
       wdetJ = T(qdp[q]);
 #pragma unroll
       for (int k = 0; k < 9; k++) X[k / 3][k % 3] = T(qdp[(1 + k) * Q3 + q]);
-      ijacobian_point_stream<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
+      ijacobian_point_stream<T, SV>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
         sU[c * Q3 + q] = v[c];
@@ -865,7 +865,7 @@ struct DiagArgs {
   T G1[kMaxP * kMaxP];  // reference 1D gradient [Q][P]
 };
 
-template <int P, int Q, typename T>
+template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
 __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemArgs<T> a, const DiagArgs<T> p) {
   constexpr int NT = nthreads_for<T>(Q);
   constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
@@ -916,7 +916,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemAr
             for (int d = 0; d < 3; d++)
               if (n == d + 1 && k == c) gref[d][k] = 1;
           }
-          ijacobian_point_stream<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
+          ijacobian_point_stream<T, SV>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
 #pragma unroll
           for (int k = 0; k < 5; k++)
             if (k == c) {
@@ -1014,7 +1014,7 @@ __host__ __device__ constexpr int combo_of(int a, int b) {
                : (a == b ? (a == 0 ? 0 : 3 + a) : (a == 0 ? b : (a == 1 ? (b == 2 ? 7 : 8) : 9)));
 }
 
-template <int P, int Q, typename T>
+template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
 __global__ void __launch_bounds__(nthreads_for<T>(Q), 1) k_blockdiag(const ElemArgs<T> a, const DiagArgs<T> p) {
   constexpr int NT = nthreads_for<T>(Q);
   constexpr int P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q, Q2P = Q2 * P, QP2 = Q * P2;
@@ -1063,7 +1063,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), 1) k_blockdiag(const ElemA
               for (int d = 0; d < 3; d++)
                 if (n == d + 1 && k == jj) gref[d][k] = 1;
             }
-            ijacobian_point_stream<T>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
+            ijacobian_point_stream<T, SV>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
 #pragma unroll
             for (int k = 0; k < 5; k++) {
               if (k < i0 || k >= i0 + NI) continue;
@@ -1222,12 +1222,12 @@ static size_t smem_bytes(int P, int Q) {
   return sizeof(T) * (size_t)(10 * P3 + 10 * P * P * Q + 10 * P * Q * Q + 10 * Q3 + 15 * Q3);
 }
 
-template <int P, int Q, bool ST, int SGS = 0>
+template <int P, int Q, bool ST, int SGS = 0, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s,
                               const SgsArg<SGS> &sg = SgsArg<SGS>{}) {
   using L = Plan<P, Q, 2, double, false, ST>;
   const size_t sm = L::bytes;
-  cudaFuncSetAttribute(k_ifunction<P, Q, ST, SGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_ifunction<P, Q, ST, SGS, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   IfunctionPtrs p;
   p.q = io->q;
   p.q_dot = io->q_dot;
@@ -1239,23 +1239,23 @@ static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx,
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<double> a = make_args<double>(op, ctx, io->qdata, c);
     if (a.n_elems == 0) continue;
-    k_ifunction<P, Q, ST, SGS><<<grid_for(op, a.n_elems, k_ifunction<P, Q, ST, SGS>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p,
+    k_ifunction<P, Q, ST, SGS, SV><<<grid_for(op, a.n_elems, k_ifunction<P, Q, ST, SGS, SV>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p,
                                                                                                                                                sg);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
-template <int P, int Q>
+template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
   // staged per-point data (TMA, 3 CTAs/SM) measured faster than direct loads at 4 CTAs/SM with spills
-  return launch_ifunction_v<P, Q, true>(op, ctx, io, s);
+  return launch_ifunction_v<P, Q, true, 0, SV>(op, ctx, io, s);
 }
 
-template <int P, int Q, typename T, bool ST>
+template <int P, int Q, typename T, bool ST, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_ijacobian_v(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v,
                               cudaStream_t s) {
   using L = Plan<P, Q, 1, T, true, ST>;
   const size_t sm = L::bytes;
-  cudaFuncSetAttribute(k_ijacobian<P, Q, T, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_ijacobian<P, Q, T, ST, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   IjacobianPtrs<T> p;
   p.dq = dq;
   p.jac_data = jd;
@@ -1266,22 +1266,22 @@ static int launch_ijacobian_v(const HbElemOp *op, const HbNewtonianContext &ctx,
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
-    k_ijacobian<P, Q, T, ST><<<grid_for(op, a.n_elems, k_ijacobian<P, Q, T, ST>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
+    k_ijacobian<P, Q, T, ST, SV><<<grid_for(op, a.n_elems, k_ijacobian<P, Q, T, ST, SV>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
-template <int P, int Q, typename T>
+template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v,
                             cudaStream_t s) {
-  return launch_ijacobian_v<P, Q, T, true>(op, ctx, qdata, jd, dq, v, s);
+  return launch_ijacobian_v<P, Q, T, true, SV>(op, ctx, qdata, jd, dq, v, s);
 }
 
-template <int P, int Q, typename T>
+template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_diagonal(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, T *diag, cudaStream_t s) {
   const int P3 = P * P * P, Q3 = Q * Q * Q;
   const size_t sm = sizeof(T) * (size_t)(10 * Q3 + Q * Q * P + Q * P * P + 5 * P3);
-  cudaFuncSetAttribute(k_diagonal<P, Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_diagonal<P, Q, T, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   DiagArgs<T> p;
   p.jac_data = jd;
   p.diag = diag;
@@ -1290,7 +1290,7 @@ static int launch_diagonal(const HbElemOp *op, const HbNewtonianContext &ctx, co
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
-    k_diagonal<P, Q, T><<<grid_for(op, a.n_elems, k_diagonal<P, Q, T>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
+    k_diagonal<P, Q, T, SV><<<grid_for(op, a.n_elems, k_diagonal<P, Q, T, SV>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
@@ -1705,10 +1705,10 @@ static int launch_mass(const HbElemOp *op, const double *qdata, const double *u,
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
-template <int P, int Q, typename T>
+template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_blockdiag(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, T *out, cudaStream_t s) {
   const size_t sm = blockdiag_smem<P, Q, T>();
-  if (cudaFuncSetAttribute(k_blockdiag<P, Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
+  if (cudaFuncSetAttribute(k_blockdiag<P, Q, T, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
   DiagArgs<T> p;
   p.jac_data = jd;
   p.diag = out;
@@ -1717,7 +1717,7 @@ static int launch_blockdiag(const HbElemOp *op, const HbNewtonianContext &ctx, c
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
-    k_blockdiag<P, Q, T><<<grid_for(op, a.n_elems, k_blockdiag<P, Q, T>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
+    k_blockdiag<P, Q, T, SV><<<grid_for(op, a.n_elems, k_blockdiag<P, Q, T, SV>, nthreads_for<T>(Q), sm), nthreads_for<T>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
@@ -1727,6 +1727,8 @@ static int launch_blockdiag(const HbElemOp *op, const HbNewtonianContext &ctx, c
 #define HB_PQ_LIST(X) X(2, 2) X(2, 3) X(2, 4) X(3, 3) X(3, 4) X(3, 5) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7)
 // bases the residual with the fused SGS closure is built for (the coarse LES runs at degree 2 and 3)
 #define HB_SGS_PQ_LIST(X) X(3, 3) X(3, 4) X(4, 5)
+// bases compiled for the primitive and entropy state variables (degree 1-3 with q_extra 0-2 as HONEE's examples use them)
+#define HB_SV_PQ_LIST(X) X(2, 2) X(2, 3) X(2, 4) X(3, 3) X(3, 4) X(3, 5) X(4, 4) X(4, 5)
 
 }  // namespace hb
 
@@ -1737,20 +1739,34 @@ static int check_op(const HbElemOp *op) {
   return HB_SUCCESS;
 }
 
+// (P, Q) dispatch for one state variable: every compiled pair for conservative variables, HB_SV_PQ_LIST for the others
+template <int SV>
+static int ifunction_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_ifunction<PP, QQ, SV>(op, ctx, io, s);
+  if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
+    HB_PQ_LIST(HB_CASE)
+  } else {
+    HB_SV_PQ_LIST(HB_CASE)
+  }
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+
 extern "C" int hb_ifunction_apply(const HbElemOp *op, const void *ctx184, const HbIFunctionIO *io, void *stream) {
   int err = check_op(op);
   if (err) return err;
   HbNewtonianContext ctx;
   memcpy(&ctx, ctx184, sizeof ctx);
-  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE || ctx.divFdiff_method != HB_DIV_DIFF_FLUX_PROJ_NONE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.divFdiff_method != HB_DIV_DIFF_FLUX_PROJ_NONE) return HB_ERROR_UNSUPPORTED;
   if (ctx.idl_enable && !op->d_x_elem) return HB_ERROR_INVALID;
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE && ctx.state_var != HB_STATEVAR_PRIMITIVE && ctx.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   if (!io->add && cudaMemsetAsync(io->v, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
-#define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_ifunction<PP, QQ>(op, ctx, io, s);
-  HB_PQ_LIST(HB_CASE)
-#undef HB_CASE
-  return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return ifunction_pq<HB_STATEVAR_PRIMITIVE>(op, ctx, io, s);
+  if (ctx.state_var == HB_STATEVAR_ENTROPY) return ifunction_pq<HB_STATEVAR_ENTROPY>(op, ctx, io, s);
+  return ifunction_pq<HB_STATEVAR_CONSERVATIVE>(op, ctx, io, s);
 }
 
 template <int SGS>
@@ -1794,20 +1810,32 @@ extern "C" int hb_ifunction_apply_sgs(const HbElemOp *op, const void *ctx184, co
   return HB_ERROR_UNSUPPORTED;
 }
 
+template <typename T, int SV>
+static int ijacobian_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v, cudaStream_t s) {
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_ijacobian<PP, QQ, T, SV>(op, ctx, qdata, jd, dq, v, s);
+  if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
+    HB_PQ_LIST(HB_CASE)
+  } else {
+    HB_SV_PQ_LIST(HB_CASE)
+  }
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+
 extern "C" int hb_ijacobian_apply_f64(const HbElemOp *op, const void *ctx184, const double *qdata, const double *jac_data, const double *dq,
                                       double *v, int add, void *stream) {
   int err = check_op(op);
   if (err) return err;
   HbNewtonianContext ctx;
   memcpy(&ctx, ctx184, sizeof ctx);
-  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE && ctx.state_var != HB_STATEVAR_PRIMITIVE && ctx.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   if (!add && cudaMemsetAsync(v, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
-#define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_ijacobian<PP, QQ, double>(op, ctx, qdata, jac_data, dq, v, s);
-  HB_PQ_LIST(HB_CASE)
-#undef HB_CASE
-  return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return ijacobian_pq<double, HB_STATEVAR_PRIMITIVE>(op, ctx, qdata, jac_data, dq, v, s);
+  if (ctx.state_var == HB_STATEVAR_ENTROPY) return ijacobian_pq<double, HB_STATEVAR_ENTROPY>(op, ctx, qdata, jac_data, dq, v, s);
+  return ijacobian_pq<double, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, dq, v, s);
 }
 
 extern "C" int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, const float *dq,
@@ -1816,12 +1844,24 @@ extern "C" int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, co
   if (err) return err;
   HbNewtonianContext ctx;
   memcpy(&ctx, ctx184, sizeof ctx);
-  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE && ctx.state_var != HB_STATEVAR_PRIMITIVE && ctx.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   if (!add && cudaMemsetAsync(v, 0, sizeof(float) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
+  if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return ijacobian_pq<float, HB_STATEVAR_PRIMITIVE>(op, ctx, qdata, jac_data, dq, v, s);
+  if (ctx.state_var == HB_STATEVAR_ENTROPY) return ijacobian_pq<float, HB_STATEVAR_ENTROPY>(op, ctx, qdata, jac_data, dq, v, s);
+  return ijacobian_pq<float, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, dq, v, s);
+}
+
+template <typename T, int SV>
+static int diagonal_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, T *diag, cudaStream_t s) {
 #define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_ijacobian<PP, QQ, float>(op, ctx, qdata, jac_data, dq, v, s);
-  HB_PQ_LIST(HB_CASE)
+  if (op->P == PP && op->Q == QQ) return launch_diagonal<PP, QQ, T, SV>(op, ctx, qdata, jd, diag, s);
+  if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
+    HB_PQ_LIST(HB_CASE)
+  } else {
+    HB_SV_PQ_LIST(HB_CASE)
+  }
 #undef HB_CASE
   return HB_ERROR_UNSUPPORTED;
 }
@@ -1832,14 +1872,13 @@ extern "C" int hb_diagonal_assemble_f64(const HbElemOp *op, const void *ctx184, 
   if (err) return err;
   HbNewtonianContext ctx;
   memcpy(&ctx, ctx184, sizeof ctx);
-  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE && ctx.state_var != HB_STATEVAR_PRIMITIVE && ctx.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   if (!add && cudaMemsetAsync(diag, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
-#define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_diagonal<PP, QQ, double>(op, ctx, qdata, jac_data, diag, s);
-  HB_PQ_LIST(HB_CASE)
-#undef HB_CASE
-  return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return diagonal_pq<double, HB_STATEVAR_PRIMITIVE>(op, ctx, qdata, jac_data, diag, s);
+  if (ctx.state_var == HB_STATEVAR_ENTROPY) return diagonal_pq<double, HB_STATEVAR_ENTROPY>(op, ctx, qdata, jac_data, diag, s);
+  return diagonal_pq<double, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, diag, s);
 }
 
 extern "C" int hb_diagonal_assemble_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, float *diag, int add,
@@ -1848,14 +1887,13 @@ extern "C" int hb_diagonal_assemble_f32(const HbElemOp *op, const void *ctx184, 
   if (err) return err;
   HbNewtonianContext ctx;
   memcpy(&ctx, ctx184, sizeof ctx);
-  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE && ctx.state_var != HB_STATEVAR_PRIMITIVE && ctx.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   if (!add && cudaMemsetAsync(diag, 0, sizeof(float) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
-#define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_diagonal<PP, QQ, float>(op, ctx, qdata, jac_data, diag, s);
-  HB_PQ_LIST(HB_CASE)
-#undef HB_CASE
-  return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return diagonal_pq<float, HB_STATEVAR_PRIMITIVE>(op, ctx, qdata, jac_data, diag, s);
+  if (ctx.state_var == HB_STATEVAR_ENTROPY) return diagonal_pq<float, HB_STATEVAR_ENTROPY>(op, ctx, qdata, jac_data, diag, s);
+  return diagonal_pq<float, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, diag, s);
 }
 
 extern "C" int hb_setup_qdata(int num_elem, int Q, const double *qref1d, const double *qweight1d, const double *x_elem, double *qdata, void *stream) {
@@ -1911,6 +1949,19 @@ extern "C" int hb_mass_diagonal(const HbElemOp *op, const double *qdata, double 
 
 // Point-block diagonal of the IJacobian operator: out[(node * 5 + i) * 5 + j] (+)= d v_(node,i) / d dq_(node,j), i.e. one
 // row-major 5 x 5 block per node of the node-interleaved L-vector (out holds l_size * 5 values).
+template <typename T, int SV>
+static int pbdiag_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, T *out, cudaStream_t s) {
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_blockdiag<PP, QQ, T, SV>(op, ctx, qdata, jd, out, s);
+  if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
+    HB_PQ_LIST(HB_CASE)
+  } else {
+    HB_SV_PQ_LIST(HB_CASE)
+  }
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+
 template <typename T>
 static int pbdiag_dispatch(const HbElemOp *op, const void *ctx184, const double *qdata, const T *jac_data, T *out, int add, void *stream) {
   int err = check_op(op);
@@ -1918,14 +1969,13 @@ static int pbdiag_dispatch(const HbElemOp *op, const void *ctx184, const double 
   if (!ctx184 || !qdata || !jac_data || !out) return HB_ERROR_INVALID;
   HbNewtonianContext ctx;
   memcpy(&ctx, ctx184, sizeof ctx);
-  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE && ctx.state_var != HB_STATEVAR_PRIMITIVE && ctx.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   if (!add && cudaMemsetAsync(out, 0, sizeof(T) * (size_t)op->l_size * 5, s) != cudaSuccess) return HB_ERROR_CUDA;
-#define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_blockdiag<PP, QQ, T>(op, ctx, qdata, jac_data, out, s);
-  HB_PQ_LIST(HB_CASE)
-#undef HB_CASE
-  return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return pbdiag_pq<T, HB_STATEVAR_PRIMITIVE>(op, ctx, qdata, jac_data, out, s);
+  if (ctx.state_var == HB_STATEVAR_ENTROPY) return pbdiag_pq<T, HB_STATEVAR_ENTROPY>(op, ctx, qdata, jac_data, out, s);
+  return pbdiag_pq<T, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, out, s);
 }
 
 extern "C" int hb_point_block_diagonal_f64(const HbElemOp *op, const void *ctx184, const double *qdata, const double *jac_data, double *out, int add,

@@ -1,10 +1,11 @@
 // newtonian_qf.cuh -- point-wise Newtonian ideal-gas physics for the fused sm_100a kernels.
 //
-// Device restatement of the reference QFunctions, specialised to conservative state variables:
+// Device restatement of the reference QFunctions for the three state variables (conservative, primitive, entropy; a
+// template parameter, so each kernel is compiled for the one it runs):
 //   IFunction_Newtonian / IFunction_Newtonian_Integrand   qfunctions/newtonian.h:205-257, newtonian_integrands.h:87-115
 //   IJacobian_Newtonian / IJacobian_Newtonian_Integrand   qfunctions/newtonian.h:272-311, newtonian_integrands.h:134-166
 //   Tau_diagPrim, Stabilization, StabilizationMatrix      qfunctions/stabilization.h:25-100
-//   state algebra and fluxes                              qfunctions/newtonian_state.h:64-89, 170-184, 425-574
+//   state algebra and fluxes                              qfunctions/newtonian_state.h:64-423, 425-574
 // The arithmetic is reorganised for the GPU: reciprocals of density/cv are formed once and multiplied, only the rows of
 // the linearised flux that are used are formed, and terms known to be zero (time derivative of Y, divergence of the
 // diffusive flux when its projection is off) are dropped.  The result equals the reference to rounding (a few ulp per
@@ -91,6 +92,78 @@ __device__ __forceinline__ void state_from_y_fwd(const PhysConst<T> &c, const St
   const T de_int = c.cv * dY[4];
   ds.E = ds.rho * (e_int + ke) + s.rho * (de_int + dke);
   (void)eint;
+}
+
+// Per-point values the tangents of each state variable reuse (1/rho and the specific energies; the entropy variables).
+template <typename T>
+struct SAux {
+  T inv_rho, etot, eint;
+  T V[5];
+};
+
+// StateFromQ (newtonian_state.h:393-407) for the state variable SV: conservative U (StateFromU), primitive Y = (P, u, T)
+// (StateFromY: StateConservativeFromPrimitive, :159-168) or entropy V (StateFromV: StatePrimitiveFromEntropy and
+// StateConservativeFromEntropy, :122-132, :222-238; log and exp as the reference evaluates them).
+template <int SV, typename T>
+__device__ __forceinline__ void state_from_q(const PhysConst<T> &c, const T q[5], St<T> &s, SAux<T> &a) {
+  if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
+    state_from_u(c, q, s, a.inv_rho, a.etot, a.eint);
+  } else if constexpr (SV == HB_STATEVAR_PRIMITIVE) {
+    s.P = q[0];
+    s.u[0] = q[1];
+    s.u[1] = q[2];
+    s.u[2] = q[3];
+    s.T_ = q[4];
+    s.rho = s.P / (c.Rgas * s.T_);
+    for (int i = 0; i < 3; i++) s.m[i] = s.rho * s.u[i];
+    const T ke = T(.5) * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]);
+    a.eint = c.cv * s.T_;
+    a.etot = a.eint + ke;
+    s.E = s.rho * (a.eint + ke);
+    a.inv_rho = rcp(s.rho);
+  } else {
+    for (int i = 0; i < 5; i++) a.V[i] = q[i];
+    const T inv_v4 = rcp(q[4]);
+    for (int i = 0; i < 3; i++) s.u[i] = -q[1 + i] * inv_v4;
+    s.T_ = T(-1) / (c.Rgas * q[4]);
+    const T g = c.gm1 + T(1);
+    const T ke = T(.5) * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]);
+    const T ent = g - c.gm1 * (q[0] - ke * q[4]);
+    const T l4 = log(-q[4]);
+    s.P = exp(-(ent + g * l4) / c.gm1);
+    s.rho = exp(-(ent + l4) / c.gm1);
+    for (int i = 0; i < 3; i++) s.m[i] = s.rho * s.u[i];
+    a.eint = -c.cv / (c.Rgas * q[4]);
+    a.etot = a.eint + ke;
+    s.E = s.rho * (a.eint + ke);
+    a.inv_rho = rcp(s.rho);
+  }
+}
+
+// StateFromQ_fwd (newtonian_state.h:409-423): the full tangent state of a tangent dq in the state variable SV
+// (StateFromU_fwd; StateFromY_fwd; StateFromV_fwd = StatePrimitiveFromEntropy_fwd and StateConservativeFromEntropy_fwd,
+// :134-146, :240-262).
+template <int SV, typename T>
+__device__ __forceinline__ void state_from_q_fwd(const PhysConst<T> &c, const St<T> &s, const SAux<T> &a, const T dq[5], St<T> &ds) {
+  if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
+    state_from_u_fwd(c, s, a.inv_rho, a.etot, a.eint, dq, ds);
+  } else if constexpr (SV == HB_STATEVAR_PRIMITIVE) {
+    state_from_y_fwd(c, s, a.eint, dq, ds);
+  } else {
+    const T *V = a.V;
+    const T inv_v4 = rcp(V[4]);
+    for (int i = 0; i < 3; i++) ds.u[i] = (-dq[1 + i] - s.u[i] * dq[4]) * inv_v4;
+    const T ke = T(.5) * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]);
+    const T dke = ds.u[0] * s.u[0] + ds.u[1] * s.u[1] + ds.u[2] * s.u[2];
+    const T dent = -c.gm1 * (dq[0] - (dke * V[4] + ke * dq[4]));
+    const T g = c.gm1 + T(1);
+    ds.rho = -s.rho / c.gm1 * (dent + dq[4] * inv_v4);
+    for (int i = 0; i < 3; i++) ds.m[i] = ds.rho * s.u[i] + s.rho * ds.u[i];
+    const T deint = c.cv * dq[4] / (c.Rgas * V[4] * V[4]);
+    ds.E = ds.rho * (a.eint + ke) + s.rho * (deint + dke);
+    ds.T_ = dq[4] / (c.Rgas * V[4] * V[4]);
+    ds.P = s.P * (-dent - g * dq[4] * inv_v4) / c.gm1;
+  }
 }
 
 // Row i of the linearised inviscid flux (newtonian_state.h:433-442): dF_i for components 0..4.
@@ -347,27 +420,43 @@ namespace hb {
 // are handed to `emit` (index, value) as soon as they are known.
 
 // gradient direction j of the state: dq_j = sum_k gref[k][.] X[k][j] -> tangent state
-template <typename T>
-__device__ __forceinline__ void gradient_dir(const PhysConst<T> &c, const St<T> &s, T inv_rho, T etot, T eint, const T gref[3][5], const T X[3][3],
-                                             int j, St<T> &g) {
+template <int SV, typename T>
+__device__ __forceinline__ void gradient_dir(const PhysConst<T> &c, const St<T> &s, const SAux<T> &a, const T gref[3][5], const T X[3][3], int j,
+                                             St<T> &g) {
   T dq[5];
 #pragma unroll
   for (int cc = 0; cc < 5; cc++) dq[cc] = gref[0][cc] * X[0][j] + gref[1][cc] * X[1][j] + gref[2][cc] * X[2][j];
-  state_from_u_fwd(c, s, inv_rho, etot, eint, dq, g);
+  state_from_q_fwd<SV>(c, s, a, dq, g);
 }
 
-template <typename T, typename Emit>
-__device__ __forceinline__ void ifunction_point_stream(const PhysConst<T> &c, const T q[5], const T gref[3][5], const T qdot[5], T wdetJ,
+// SV: the state variable of q, q_dot and the stored q (HbStateVariable); the residual is always the conservation law in
+// conservative form, with the rate dU/dt = (dU/dq) q_dot (newtonian.h:226-230).
+template <typename T, int SV = HB_STATEVAR_CONSERVATIVE, typename Emit>
+__device__ __forceinline__ void ifunction_point_stream(const PhysConst<T> &c, const T q[5], const T gref[3][5], const T qdot_in[5], T wdetJ,
                                                        const T X[3][3], T x0, T v[5], T gv[3][5], Emit emit) {
   St<T> s;
-  T inv_rho, etot, eint;
-  state_from_u(c, q, s, inv_rho, etot, eint);
+  SAux<T> aux;
+  state_from_q<SV>(c, q, s, aux);
+  const T eint = aux.eint;
+  T qdot[5];
+  if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) qdot[k] = qdot_in[k];
+  } else {
+    St<T> sd;
+    state_from_q_fwd<SV>(c, s, aux, qdot_in, sd);
+    qdot[0] = sd.rho;
+    qdot[1] = sd.m[0];
+    qdot[2] = sd.m[1];
+    qdot[3] = sd.m[2];
+    qdot[4] = sd.E;
+  }
   // strong convective residual, velocity gradient G[i][j] = du_i/dx_j, temperature gradient
   T r[5] = {0, 0, 0, 0, 0}, G[3][3], gT[3];
 #pragma unroll
   for (int j = 0; j < 3; j++) {
     St<T> g;
-    gradient_dir(c, s, inv_rho, etot, eint, gref, X, j, g);
+    gradient_dir<SV>(c, s, aux, gref, X, j, g);
     if (c.stab != HB_STAB_NONE) {
       T row[5];
       dflux_row(s, g, j, row);
@@ -455,20 +544,21 @@ __device__ __forceinline__ void ifunction_point_stream(const PhysConst<T> &c, co
   }
 }
 
-template <typename T>
+template <typename T, int SV = HB_STATEVAR_CONSERVATIVE>
 __device__ __forceinline__ void ijacobian_point_stream(const PhysConst<T> &c, const T jd[15], const T dq[5], const T gref[3][5], T wdetJ,
                                                        const T X[3][3], T v[5], T gv[3][5]) {
   St<T> s;
-  T inv_rho, etot, eint;
+  SAux<T> aux;
   const T q[5] = {jd[0], jd[1], jd[2], jd[3], jd[4]};
-  state_from_u(c, q, s, inv_rho, etot, eint);
+  state_from_q<SV>(c, q, s, aux);
+  const T eint = aux.eint;
   St<T> ds;
-  state_from_u_fwd(c, s, inv_rho, etot, eint, dq, ds);
+  state_from_q_fwd<SV>(c, s, aux, dq, ds);
   T r[5] = {0, 0, 0, 0, 0}, G[3][3], gT[3];
 #pragma unroll
   for (int j = 0; j < 3; j++) {
     St<T> g;
-    gradient_dir(c, s, inv_rho, etot, eint, gref, X, j, g);
+    gradient_dir<SV>(c, s, aux, gref, X, j, g);
     if (c.stab != HB_STAB_NONE) {
       T row[5];
       dflux_row(s, g, j, row);

@@ -76,7 +76,8 @@ class NewtonianOperators:
         self.jac_data = ce.Vector(ceed, E * Q3 * njd)
         self.q_dot = ce.Vector(ceed, mesh.l_size)
         # -- IFunction volume operator (src/setuplibceed.c:209-243)
-        qf_if = ce.QFunction(ceed, "newtonian.h:IFunction_Newtonian_Conserv")
+        sv_name = ("Conserv", "Prim", "Entropy")[ctx.state_var]  # problems/newtonian.c:771-787: the QFunctions of the state variable
+        qf_if = ce.QFunction(ceed, f"newtonian.h:IFunction_Newtonian_{sv_name}")
         for name, size, mode in (("q", 5, ce.CEED_EVAL_INTERP), ("Grad_q", 15, ce.CEED_EVAL_GRAD), ("q dot", 5, ce.CEED_EVAL_INTERP),
                                  ("qdata", 10, ce.CEED_EVAL_NONE), ("x", 3, ce.CEED_EVAL_INTERP)):
             qf_if.add_input(name, size, mode)
@@ -95,7 +96,7 @@ class NewtonianOperators:
         op_if.set_field("Grad_v", self.rstr_q, self.basis_q, ceed.active)
         op_if.set_field("jac_data", self.rstr_jd, ceed.basis_none, self.jac_data)
         # -- IJacobian volume operator (src/setuplibceed.c:245-269)
-        qf_ij = ce.QFunction(ceed, "newtonian.h:IJacobian_Newtonian_Conserv")
+        qf_ij = ce.QFunction(ceed, f"newtonian.h:IJacobian_Newtonian_{sv_name}")
         for name, size, mode in (("dq", 5, ce.CEED_EVAL_INTERP), ("Grad_dq", 15, ce.CEED_EVAL_GRAD), ("qdata", 10, ce.CEED_EVAL_NONE),
                                  ("jac_data", njd, ce.CEED_EVAL_NONE)):
             qf_ij.add_input(name, size, mode)

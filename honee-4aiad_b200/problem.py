@@ -97,6 +97,29 @@ def conservative_from_primitive(gas: GasProperties, P, u, T):
     return np.stack([rho, rho * u[0], rho * u[1], rho * u[2], E])
 
 
+def state_to_q(gas: GasProperties, q_cons, state_var: int) -> np.ndarray:
+    """Node-interleaved conservative states -> the same states in `state_var` (StateToQ, newtonian_state.h:371-391):
+    primitive Y = (P, u, T) (StatePrimitiveFromConservative, :64-73), entropy V (StateEntropyFromPrimitive, :91-103)."""
+    U = np.asarray(q_cons, dtype=np.float64).reshape(-1, 5)
+    if state_var == STATEVAR_CONSERVATIVE:
+        return U.reshape(-1).copy()
+    rho = U[:, 0]
+    u = U[:, 1:4] / rho[:, None]
+    ke = 0.5 * np.sum(u * u, axis=1)
+    eint = U[:, 4] / rho - ke
+    T = eint / gas.cv
+    P = (gas.cp / gas.cv - 1) * rho * eint
+    if state_var == STATEVAR_PRIMITIVE:
+        return np.column_stack([P, u, T]).reshape(-1)
+    if state_var != STATEVAR_ENTROPY:
+        raise ValueError(f"unknown state variable {state_var}")
+    g, R = gas.cp / gas.cv, gas.cp - gas.cv
+    rho_y = P / (R * T)
+    ent = np.log(P) - g * np.log(rho_y)
+    rho_p = rho_y / P
+    return np.column_stack([(g - ent) / (g - 1) - rho_p * ke, rho_p[:, None] * u, -rho_p]).reshape(-1)
+
+
 # --------------------------------------------------------------------------------------------------------------------
 # 1D tabulation
 

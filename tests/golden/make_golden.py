@@ -10,11 +10,13 @@ Outputs (committed; the GPU box has no reference tree):
                             it (examples/navierstokes.c:222, examples/taylor_green_vortex.yaml)
   unit_state.json           the UnitTests_Newtonian inputs and tolerances (problems/newtonian.c:947-987) with the
                             reference's StateToQ outputs for every (A, B) pair
+  channel_prim_be5.npz      the same for "Channel, Primitive" (examples/navierstokes.c:253, -state_var primitive),
+                            tests/output/channel-prim.bin
   channel_be5.npz           the free DOFs of the final state of the "Channel" run (examples/navierstokes.c:252:
                             examples/channel.yaml, 5 x 5 x 1 faces, 5 backward-Euler steps), tests/output/channel.bin
   gaussianwave_explicit.npz the free DOFs of the final state of "Gaussian Wave, explicit, supg, IDL" (examples/navierstokes.c:233),
                             tests/output/gaussianwave-explicit.bin (a 64-bit-index HONEE file)
-  ref_*.bin                 copies of tests/output/{channel,taylor-green,gaussianwave-explicit}.bin, the reference's own
+  ref_*.bin                 copies of tests/output/{channel,channel-prim,taylor-green,gaussianwave-explicit}.bin, the reference's own
                             solution files, for the checks of the file-format reader (honee-4aiad_b200/honee_file.py)
   taylorgreen_rk4.npz       every row of tests/output/taylorgreen_totalke.csv (steps 0, 2, 3 of the explicit RK4 run of
                             examples/navierstokes.c:222) and the final state of that run, tests/output/taylor-green.bin
@@ -149,6 +151,19 @@ def main():
                         dt=np.float64(5e-6), steps=np.int64(5), essential=np.array("y-:1,2,3 y+:1,2,3 z-:3 z+:3"), compare_atol=np.float64(2e-11),
                         source=np.array("tests/output/channel.bin (examples/navierstokes.c:252, examples/channel.yaml)"))
 
+    # ---- "Channel, Primitive" (examples/navierstokes.c:253): the same run with -state_var primitive
+    raw = open(os.path.join(args.ref, "tests/output/channel-prim.bin"), "rb").read()
+    token, step = np.frombuffer(raw[:8], dtype=">i4")
+    t_final = np.frombuffer(raw[8:16], dtype=">f8")[0]
+    classid, length = np.frombuffer(raw[16:24], dtype=">i4")
+    assert len(raw) == 24 + 8 * int(length) and int(classid) == 1211214
+    np.savez_compressed(os.path.join(HERE, "channel_prim_be5.npz"), final_step=np.int64(step), final_time=np.float64(t_final),
+                        free_state=np.frombuffer(raw[24:], dtype=">f8").astype(np.float64), faces=np.array([5, 5, 1]), degree=np.int64(1),
+                        q_extra=np.int64(2), box_hi=np.array([0.01, 0.01, 0.001]), mu=np.float64(0.01), umax=np.float64(40.0),
+                        dt=np.float64(5e-6), steps=np.int64(5), essential=np.array("y-:1,2,3 y+:1,2,3 z-:3 z+:3"), compare_atol=np.float64(2e-11),
+                        state_var=np.int64(1),
+                        source=np.array("tests/output/channel-prim.bin (examples/navierstokes.c:253, examples/channel.yaml, -state_var primitive)"))
+
     # ---- Gaussian wave, explicit, SUPG, IDL (examples/navierstokes.c:233): free DOFs of the final state, a 64-bit-index file
     #      (token 0x0CEEDF64: int64 step, float64 time, int64 class id, int64 length, values)
     raw = open(os.path.join(args.ref, "tests/output/gaussianwave-explicit.bin"), "rb").read()
@@ -167,7 +182,7 @@ def main():
 
     # ---- raw solution files of the reference's runs (32- and 64-bit-index HONEE files) for the file-format reader
     import shutil
-    for name in ("channel.bin", "taylor-green.bin", "gaussianwave-explicit.bin"):
+    for name in ("channel.bin", "channel-prim.bin", "taylor-green.bin", "gaussianwave-explicit.bin"):
         shutil.copyfile(os.path.join(args.ref, "tests/output", name), os.path.join(HERE, "ref_" + name))
 
     # ---- UnitTests_Newtonian inputs (problems/newtonian.c:947-987) and reference StateToQ outputs

@@ -17,8 +17,9 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 WALLS = {"y-": (1, 2, 3), "y+": (1, 2, 3), "z-": (3,), "z+": (3,)}
 
 
-def channel_case():
-    G = np.load(os.path.join(GOLD, "channel_be5.npz"))
+def channel_case(golden="channel_be5.npz"):
+    """The "Channel" run (channel_be5.npz) or "Channel, Primitive" (channel_prim_be5.npz: the same in primitive variables)."""
+    G = np.load(os.path.join(GOLD, golden))
     hi = tuple(float(v) for v in G["box_hi"])
     P = int(G["degree"]) + 1
     Q = P + int(G["q_extra"])
@@ -27,6 +28,10 @@ def channel_case():
     newt = prob.newtonian_context(int(G["degree"]), mu=float(G["mu"]), implicit=True)
     ch = prob.channel_context(newt, (0.0, 0.0, 0.0), hi, umax=float(G["umax"]))
     q = prob.channel_state(mesh, basis, ch)
+    sv = int(G["state_var"]) if "state_var" in G else prob.STATEVAR_CONSERVATIVE
+    if sv != prob.STATEVAR_CONSERVATIVE:  # ICsChannel returns the state in the problem's variables (qfunctions/channel.h:68)
+        ch.newt_ctx.state_var = sv
+        q = prob.state_to_q(newt.gas, q, sv)
     idx = prob.box_essential(mesh, WALLS)
     return G, mesh, basis, ch, q, idx
 
@@ -57,8 +62,10 @@ def test_essential_dofs_match_the_reference_global_vector():
     assert np.all(q[idx] == 0.0)
 
 
-def test_oracle_reproduces_reference_channel_run():
-    G, mesh, basis, ch, q, idx = channel_case()
+@pytest.mark.parametrize("golden", ["channel_be5.npz", "channel_prim_be5.npz"])
+def test_oracle_reproduces_reference_channel_run(golden):
+    G, mesh, basis, ch, q, idx = channel_case(golden)
+    tag = ("conserv", "prim", "entropy")[ch.newt_ctx.state_var]
     free = np.setdiff1d(np.arange(mesh.l_size), idx)
     m = oracle_mesh(mesh, basis)
     Q = basis.Q
@@ -75,7 +82,7 @@ def test_oracle_reproduces_reference_channel_run():
         for it in range(10):
             qdot = (qk - qn) / dt
             qdot[idx] = 0.0
-            r = O.apply_ifunction(m, cb, qk, qdot, qdata, jd)
+            r = O.apply_ifunction(m, cb, qk, qdot, qdata, jd, qf_name=f"oracle_qf_ifunction_{tag}")
             r[idx] = 0.0
             rn = np.linalg.norm(r)
             r0 = rn if it == 0 else r0
@@ -85,7 +92,7 @@ def test_oracle_reproduces_reference_channel_run():
             for k, j in enumerate(free):
                 e = np.zeros(mesh.l_size)
                 e[j] = 1.0
-                J[:, k] = O.apply_ijacobian(m, cb, e, qdata, jd)[free]
+                J[:, k] = O.apply_ijacobian(m, cb, e, qdata, jd, qf_name=f"oracle_qf_ijacobian_{tag}")[free]
             qk[free] += np.linalg.solve(J, -r[free])
         assert rn <= 1e-8 * r0
         qn = qk

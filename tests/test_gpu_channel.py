@@ -1,8 +1,9 @@
 """GPU run of the reference's "Channel" test (examples/navierstokes.c:252, examples/channel.yaml): degree 1 with q_extra 2 on
 5 x 5 x 1 faces, body force, no-slip walls and symmetry planes as essential DOFs, 5 backward-Euler steps through the time
-loop (hb_ts_* with hb_ts_set_essential), FP64 and mixed precision, point Jacobi and point-block Jacobi.  The final state must
-meet the reference's own regression bound against tests/output/channel.bin (max |Q - Q_ref| / max |Q_ref| <= 2e-11, over the
-free DOFs as a sorted multiset), and the fused operators at this (P, Q) = (2, 4) must equal the oracle."""
+loop (hb_ts_* with hb_ts_set_essential), FP64 and mixed precision, point Jacobi and point-block Jacobi, in conservative
+variables and as "Channel, Primitive" (examples/navierstokes.c:253).  The final state must meet the reference's own regression
+bound against tests/output/channel.bin / channel-prim.bin (max |Q - Q_ref| / max |Q_ref| <= 2e-11, over the free DOFs as a
+sorted multiset), and the fused operators at this (P, Q) = (2, 4) must equal the oracle."""
 import importlib
 
 import numpy as np
@@ -42,10 +43,15 @@ def test_channel_operators_match_oracle():
     assert rel_l2(jv.cpu().numpy(), O.apply_ijacobian(m, cb, dq, qdata, jd_ref)) < 1e-12
 
 
-@pytest.mark.parametrize("fp32,pc", [(0, 1), (1, 1), (0, 2), (1, 2)])
-def test_channel_run_reproduces_reference(fp32, pc):
+@pytest.mark.parametrize("golden,fp32,pc", [("channel_be5.npz", 0, 1), ("channel_be5.npz", 1, 1), ("channel_be5.npz", 0, 2), ("channel_be5.npz", 1, 2),
+                                             ("channel_prim_be5.npz", 0, 2), ("channel_prim_be5.npz", 1, 2)])
+def test_channel_run_reproduces_reference(fp32, pc, golden):
+    """Conservative ("Channel") and primitive ("Channel, Primitive", tests/output/channel-prim.bin) variables.  In primitive
+    variables the rate term couples the five components of every node (dU/dY is a full 5 x 5 block), so point Jacobi leaves
+    GMRES stagnating (10000 iterations per Newton step without reaching rtol 1e-5); the point-block Jacobi (-pc_type
+    vpbjacobi) inverts that coupling and converges in 2 Newton / 14 GMRES iterations per step."""
     import torch
-    G, mesh, basis, ch, q, idx = channel_case()
+    G, mesh, basis, ch, q, idx = channel_case(golden)
     op = K.ElemOp(mesh, basis)
     x = torch.from_numpy(np.ascontiguousarray(mesh.x_elem)).to(_dev())
     qdata = torch.zeros(mesh.num_elem * 10 * basis.Q ** 3, dtype=torch.float64, device=_dev())

@@ -1,0 +1,140 @@
+"""GPU parity of the fused operators in primitive and entropy state variables (IFunction_Newtonian_Prim/_Entropy and
+IJacobian_Newtonian_Prim/_Entropy, qfunctions/newtonian.h:263-269, 317-323; the state algebra of newtonian_state.h:64-423)
+against the oracle's QFunctions of the same state variable (oracle/honee_oracle.c, pinned bit for bit to the reference's).
+
+Tolerances: residual, stored Jacobian data, Jacobian action, diagonal and point blocks 1e-12 relative L2 in FP64, or 10x the
+change the oracle itself shows when the state is perturbed by one ulp, whichever is larger.  That floor matters for entropy
+variables only: pressure and density are rebuilt through exp(log(...)) of arguments of size ~10, so the last-bit differences
+between the device's and the C library's exp/log reach the residual, amplified where its flux terms nearly cancel (a
+periodic multi-mode state).  The FP32 Jacobian action: 1e-6 for primitive variables; 2e-5 for entropy variables (the
+same rebuild in FP32: ~10 FP32 ulp in pressure and density)."""
+import importlib
+
+import numpy as np
+import pytest
+
+from helpers import O, case, prob, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+K = importlib.import_module("honee-4aiad_b200.kernels")
+NAMES = {prob.STATEVAR_PRIMITIVE: "prim", prob.STATEVAR_ENTROPY: "entropy"}
+
+CASES = {
+    "prim_P3Q3_supg": (prob.STATEVAR_PRIMITIVE, dict(n=(3, 3, 2), P=3, Q=3)),
+    "prim_P2Q4_none_gravity": (prob.STATEVAR_PRIMITIVE, dict(n=(3, 2, 2), P=2, Q=4, stab=prob.STAB_NONE, g=(0.0, -9.81, 0.0))),
+    "prim_P4Q5_su_idl_modes": (prob.STATEVAR_PRIMITIVE, dict(n=(2, 2, 2), P=4, Q=5, stab=prob.STAB_SU, idl=(2e-3, 0.2, 0.5, 101000.0),
+                                                              state="modes")),
+    "entropy_P3Q4_supg": (prob.STATEVAR_ENTROPY, dict(n=(3, 2, 2), P=3, Q=4)),
+    "entropy_P2Q3_none_idl": (prob.STATEVAR_ENTROPY, dict(n=(3, 3, 2), P=2, Q=3, stab=prob.STAB_NONE, idl=(2e-3, 0.2, 0.5, 101000.0))),
+    "entropy_P4Q5_supg_modes_periodic": (prob.STATEVAR_ENTROPY, dict(n=(2, 2, 2), P=4, Q=5, periodic=(1, 1, 1), state="modes")),
+}
+
+
+def _dev():
+    import torch
+    return torch.device("cuda:0")
+
+
+def sv_case(sv, **kw):
+    mesh, basis, ctx, q, _ = case(**kw)
+    ctx.state_var = sv
+    qv = prob.state_to_q(ctx.gas, q, sv)
+    qdv = qv * 1e-3 * np.random.default_rng(7).uniform(-1, 1, qv.shape)
+    return mesh, basis, ctx, qv, qdv
+
+
+def _oracle_mesh(mesh, basis):
+    return O.Mesh(mesh.num_elem, basis.P, basis.Q, mesh.offsets, basis.interp1d, basis.grad1d, basis.qweight1d, colors=mesh.colors)
+
+
+def _oracle_all(mesh, basis, ctx, q, qd, dq):
+    """Residual, stored data, Jacobian action, diagonal and point blocks of the oracle for the state q."""
+    tag = NAMES[ctx.state_var]
+    cb = prob.context_bytes(ctx)
+    m = _oracle_mesh(mesh, basis)
+    qdata = O.setup_qdata(mesh.num_elem, basis.Q, mesh.x_elem)
+    njd = 15 if ctx.idl_enable else 14
+    jd = np.zeros(mesh.num_elem * njd * basis.Q ** 3)
+    xq = O.coords_at_qpts(mesh.num_elem, basis.Q, mesh.x_elem)
+    v = O.apply_ifunction(m, cb, q, qd, qdata, jd, num_jd=njd, x_q=xq, qf_name=f"oracle_qf_ifunction_{tag}")
+    jv = O.apply_ijacobian(m, cb, dq, qdata, jd, num_jd=njd, qf_name=f"oracle_qf_ijacobian_{tag}")
+    d = O.assemble_diagonal(m, cb, qdata, jd, mesh.l_size, num_jd=njd, qf_name=f"oracle_qf_ijacobian_{tag}")
+    pb = O.assemble_point_block(m, cb, qdata, jd, mesh.l_size, num_jd=njd, qf_name=f"oracle_qf_ijacobian_{tag}")
+    return dict(v=v, jd=jd, jv=jv, d=d, pb=pb, qdata=qdata)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_operators_match_oracle(name):
+    import torch
+    sv, kw = CASES[name]
+    mesh, basis, ctx, q, qd = sv_case(sv, **kw)
+    cb = prob.context_bytes(ctx)
+    dq = q * 1e-4 * np.random.default_rng(1).normal(size=q.shape)
+    ref = _oracle_all(mesh, basis, ctx, q, qd, dq)
+    # the oracle's own sensitivity to a one-ulp perturbation of the state
+    q1 = q * (1 + np.finfo(np.float64).eps * np.random.default_rng(3).uniform(-1, 1, q.shape))
+    ref1 = _oracle_all(mesh, basis, ctx, q1, qd, dq)
+    bound = {k: max(1e-12, 10 * rel_l2(ref1[k], ref[k])) for k in ("v", "jd", "jv", "d", "pb")}
+    op = K.ElemOp(mesh, basis)
+    if ctx.idl_enable:
+        op.set_vertex_coords(np.ascontiguousarray(mesh.x_elem))
+    dev = _dev()
+    tq, tqd, tqdata = (torch.from_numpy(a).to(dev) for a in (q, qd, ref["qdata"]))
+    v = torch.zeros_like(tq)
+    jd = torch.zeros(ref["jd"].size, dtype=torch.float64, device=dev)
+    op.ifunction(cb, tq, tqd, tqdata, v, jac_data=jd)
+    assert rel_l2(v.cpu().numpy(), ref["v"]) < bound["v"], bound
+    assert rel_l2(jd.cpu().numpy(), ref["jd"]) < bound["jd"], bound
+    # Jacobian action, FP64 and FP32
+    jv = torch.zeros_like(tq)
+    tdq = torch.from_numpy(dq).to(dev)
+    op.ijacobian(cb, tqdata, jd, tdq, jv)
+    assert rel_l2(jv.cpu().numpy(), ref["jv"]) < bound["jv"], bound
+    jv32 = torch.zeros(q.size, dtype=torch.float32, device=dev)
+    op.ijacobian(cb, tqdata, jd.float(), tdq.float(), jv32, fp32=True)
+    assert rel_l2(jv32.double().cpu().numpy(), ref["jv"]) < (2e-5 if sv == prob.STATEVAR_ENTROPY else 1e-6)
+    # diagonal and point blocks
+    d = torch.zeros_like(tq)
+    op.diagonal(cb, tqdata, jd, d)
+    assert rel_l2(d.cpu().numpy(), ref["d"]) < bound["d"], bound
+    pb = torch.zeros(5 * mesh.l_size, dtype=torch.float64, device=dev)
+    op.point_block_diagonal(cb, tqdata, jd, pb)
+    assert rel_l2(pb.cpu().numpy(), ref["pb"]) < bound["pb"], bound
+
+
+def test_state_variable_outside_the_compiled_bases_is_refused():
+    import torch
+    mesh, basis, ctx, q, qd = sv_case(prob.STATEVAR_PRIMITIVE, n=(2, 1, 1), P=5, Q=6)
+    op = K.ElemOp(mesh, basis)
+    qdata = torch.zeros(mesh.num_elem * 10 * basis.Q ** 3, dtype=torch.float64, device=_dev())
+    tq = torch.from_numpy(q).to(_dev())
+    with pytest.raises(K.HbError):
+        op.ifunction(prob.context_bytes(ctx), tq, tq, qdata, torch.zeros_like(tq))
+
+
+@pytest.mark.parametrize("resource", ["/gpu/b200", "/gpu/b200/mixed"])
+def test_primitive_operators_through_the_ceed_api(resource):
+    """HONEE's operator set-up with -state_var primitive (IFunction_Newtonian_Prim / IJacobian_Newtonian_Prim) through the
+    libCEED API: residual and Jacobi diagonal equal the oracle's."""
+    ce = importlib.import_module("honee-4aiad_b200.ceed")
+    hon = importlib.import_module("honee-4aiad_b200.honee")
+    mesh, basis, ctx, q, qd = sv_case(prob.STATEVAR_PRIMITIVE, n=(3, 2, 2), P=3, Q=4)
+    ceed = ce.Ceed(resource)
+    ops = hon.NewtonianOperators(ceed, mesh, basis, ctx)
+    qv = ce.Vector(ceed, mesh.l_size)
+    qv.set_array_host(q)
+    ops.q_dot.set_array_host(qd)
+    out = ce.Vector(ceed, mesh.l_size)
+    ops.ifunction(qv, ops.q_dot, out)
+    cb = prob.context_bytes(ctx)
+    m = _oracle_mesh(mesh, basis)
+    qdata = O.setup_qdata(mesh.num_elem, basis.Q, mesh.x_elem)
+    jd_ref = np.zeros(mesh.num_elem * 14 * basis.Q ** 3)
+    xq = O.coords_at_qpts(mesh.num_elem, basis.Q, mesh.x_elem)
+    v_ref = O.apply_ifunction(m, cb, q, qd, qdata, jd_ref, x_q=xq, qf_name="oracle_qf_ifunction_prim")
+    assert rel_l2(out.to_numpy(), v_ref) < 1e-12
+    d = ce.Vector(ceed, mesh.l_size)
+    ops.diagonal(d)
+    d_ref = O.assemble_diagonal(m, cb, qdata, jd_ref, mesh.l_size, qf_name="oracle_qf_ijacobian_prim")
+    assert rel_l2(d.to_numpy(), d_ref) < (1e-12 if resource == "/gpu/b200" else 2e-6)
