@@ -45,6 +45,11 @@ struct Ceed_private {
   double          *d_scratch; /* 1024 doubles for reductions */
   HbElemOp        *ops[64];   /* element operators whose kernel status words are checked at host synchronisation */
   int              nops;
+  /* host <-> device copies of host-backed vectors run on their own streams, ordered against the compute stream by
+   * events, so an input copy overlaps the kernels before it and an output read-back the kernels after its producer */
+  cudaStream_t     s_h2d, s_d2h;
+  cudaEvent_t      ev_tmp;
+  int              copy_streams;
 };
 
 struct CeedVector_private {
@@ -56,6 +61,9 @@ struct CeedVector_private {
   float   *d_f32;      /* FP32 shadow (mixed-precision jac_data) */
   int      f32_valid;  /* shadow holds the current values */
   int      f64_stale;  /* FP64 copies are out of date: rebuild from the shadow on access */
+  cudaEvent_t ev_h2d;  /* end of the last host-to-device copy (on the Ceed's copy stream) */
+  cudaEvent_t ev_use;  /* recorded on the compute stream after the last operator that used the device array */
+  int      events, h2d_pending, use_known; /* use_known: ev_use covers every use of d handed out so far */
 };
 
 struct CeedElemRestriction_private {
@@ -288,6 +296,11 @@ int CeedDestroy(Ceed *ceed) {
     return CEED_ERROR_SUCCESS;
   }
   cudaFree((*ceed)->d_scratch);
+  if ((*ceed)->copy_streams) {
+    cudaStreamDestroy((*ceed)->s_h2d);
+    cudaStreamDestroy((*ceed)->s_d2h);
+    cudaEventDestroy((*ceed)->ev_tmp);
+  }
   free(*ceed);
   *ceed = NULL;
   return CEED_ERROR_SUCCESS;
@@ -365,14 +378,51 @@ static int vec_unstale(CeedVector v) {
   v->h_valid   = 0;
   return CEED_ERROR_SUCCESS;
 }
+static int ceed_copy_streams(Ceed c) {
+  if (c->copy_streams) return CEED_ERROR_SUCCESS;
+  CUDA_CK(c, cudaStreamCreateWithFlags(&c->s_h2d, cudaStreamNonBlocking));
+  CUDA_CK(c, cudaStreamCreateWithFlags(&c->s_d2h, cudaStreamNonBlocking));
+  CUDA_CK(c, cudaEventCreateWithFlags(&c->ev_tmp, cudaEventDisableTiming));
+  c->copy_streams = 1;
+  return CEED_ERROR_SUCCESS;
+}
+static int vec_events(CeedVector v) {
+  if (v->events) return CEED_ERROR_SUCCESS;
+  CUDA_CK(v->ceed, cudaEventCreateWithFlags(&v->ev_h2d, cudaEventDisableTiming));
+  CUDA_CK(v->ceed, cudaEventCreateWithFlags(&v->ev_use, cudaEventDisableTiming));
+  v->events = 1;
+  return CEED_ERROR_SUCCESS;
+}
+/* A host array handed over with CEED_USE_POINTER is read by an asynchronous copy: wait for it before the host array is
+ * given back, replaced, overwritten or freed. */
+static int vec_wait_h2d(CeedVector v) {
+  if (v->h2d_pending) {
+    CUDA_CK(v->ceed, cudaEventSynchronize(v->ev_h2d));
+    v->h2d_pending = 0;
+  }
+  return CEED_ERROR_SUCCESS;
+}
+/* Host -> device on the copy stream, after every earlier use of the device array on the compute stream (ev_use when an
+ * operator recorded it, else everything enqueued so far); later compute work waits for the copy. */
 static int vec_sync_dev(CeedVector v) {
   CK(vec_unstale(v));
   CK(vec_alloc_dev(v));
   if (!v->d_valid) {
     if (!v->h_valid) return CeedError(v->ceed, CEED_ERROR_INCOMPLETE, "vector has no valid data");
-    CUDA_CK(v->ceed, cudaMemcpyAsync(v->d, v->h, sizeof(double) * (size_t)v->length, cudaMemcpyHostToDevice, v->ceed->stream));
-    CUDA_CK(v->ceed, cudaStreamSynchronize(v->ceed->stream));
-    v->d_valid = 1;
+    Ceed c = v->ceed;
+    CK(ceed_copy_streams(c));
+    CK(vec_events(v));
+    CK(vec_wait_h2d(v));
+    if (v->use_known) CUDA_CK(c, cudaStreamWaitEvent(c->s_h2d, v->ev_use, 0));
+    else {
+      CUDA_CK(c, cudaEventRecord(c->ev_tmp, c->stream));
+      CUDA_CK(c, cudaStreamWaitEvent(c->s_h2d, c->ev_tmp, 0));
+    }
+    CUDA_CK(c, cudaMemcpyAsync(v->d, v->h, sizeof(double) * (size_t)v->length, cudaMemcpyHostToDevice, c->s_h2d));
+    CUDA_CK(c, cudaEventRecord(v->ev_h2d, c->s_h2d));
+    CUDA_CK(c, cudaStreamWaitEvent(c->stream, v->ev_h2d, 0));
+    v->h2d_pending = 1;
+    v->d_valid     = 1;
   }
   return CEED_ERROR_SUCCESS;
 }
@@ -400,13 +450,24 @@ static void ceed_unregister_op(Ceed ceed, HbElemOp *op) {
     }
 }
 
+/* Device -> host.  When the last operator that touched the vector recorded ev_use, the read-back waits only for that
+ * operator (on the copy stream), so it overlaps kernels enqueued after it; otherwise it follows the compute stream. */
 static int vec_sync_host(CeedVector v) {
   CK(vec_unstale(v));
   CK(vec_alloc_host(v));
+  CK(vec_wait_h2d(v));
   if (!v->h_valid) {
     if (!v->d_valid) return CeedError(v->ceed, CEED_ERROR_INCOMPLETE, "vector has no valid data");
-    CUDA_CK(v->ceed, cudaMemcpyAsync(v->h, v->d, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToHost, v->ceed->stream));
-    CUDA_CK(v->ceed, cudaStreamSynchronize(v->ceed->stream));
+    Ceed c = v->ceed;
+    if (v->use_known) {
+      CK(ceed_copy_streams(c));
+      CUDA_CK(c, cudaStreamWaitEvent(c->s_d2h, v->ev_use, 0));
+      CUDA_CK(c, cudaMemcpyAsync(v->h, v->d, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToHost, c->s_d2h));
+      CUDA_CK(c, cudaStreamSynchronize(c->s_d2h));
+    } else {
+      CUDA_CK(c, cudaMemcpyAsync(v->h, v->d, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToHost, c->stream));
+      CUDA_CK(c, cudaStreamSynchronize(c->stream));
+    }
     v->h_valid = 1;
     CK(ceed_check_status(v->ceed));
   }
@@ -415,11 +476,13 @@ static int vec_sync_host(CeedVector v) {
 /* device array for a kernel that reads the vector */
 static int vec_dev_read(CeedVector v, const double **d) {
   CK(vec_sync_dev(v));
+  v->use_known = 0; /* a new use of d: ev_use no longer covers it */
   *d = v->d;
   return CEED_ERROR_SUCCESS;
 }
 /* device array for a kernel that writes (write_only: contents may be discarded) */
 static int vec_dev_write(CeedVector v, double **d, int write_only) {
+  v->use_known = 0;
   if (write_only) {
     v->f64_stale = 0;
     CK(vec_alloc_dev(v));
@@ -432,6 +495,7 @@ static int vec_dev_write(CeedVector v, double **d, int write_only) {
 }
 
 int CeedVectorSetArray(CeedVector v, CeedMemType mem_type, CeedCopyMode copy_mode, CeedScalar *array) {
+  CK(vec_wait_h2d(v));
   v->f64_stale = 0;
   v->f32_valid = 0;
   if (mem_type == CEED_MEM_HOST) {
@@ -470,6 +534,7 @@ int CeedVectorSetValue(CeedVector v, CeedScalar value) {
 int CeedVectorSyncArray(CeedVector v, CeedMemType mem_type) { return mem_type == CEED_MEM_HOST ? vec_sync_host(v) : vec_sync_dev(v); }
 
 int CeedVectorTakeArray(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
+  CK(vec_wait_h2d(v));
   if (mem_type == CEED_MEM_HOST) {
     if (v->h && !v->h_valid && (v->d_valid || v->f64_stale)) CK(vec_sync_host(v));
     *array     = v->h;
@@ -498,6 +563,7 @@ int CeedVectorGetArrayRead(CeedVector v, CeedMemType mem_type, const CeedScalar 
 }
 
 int CeedVectorGetArray(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
+  CK(vec_wait_h2d(v));
   if (mem_type == CEED_MEM_HOST) {
     CK(vec_sync_host(v));
     v->d_valid = 0;
@@ -512,6 +578,7 @@ int CeedVectorGetArray(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
 }
 
 int CeedVectorGetArrayWrite(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
+  CK(vec_wait_h2d(v));
   v->f64_stale = 0;
   v->f32_valid = 0;
   if (mem_type == CEED_MEM_HOST) {
@@ -614,9 +681,14 @@ int CeedVectorDestroy(CeedVector *vec) {
     *vec = NULL;
     return CEED_ERROR_SUCCESS;
   }
+  vec_wait_h2d(v);
   if (v->h_own) free(v->h);
   if (v->d_own) cudaFree(v->d);
   if (v->d_f32) cudaFree(v->d_f32);
+  if (v->events) {
+    cudaEventDestroy(v->ev_h2d);
+    cudaEventDestroy(v->ev_use);
+  }
   Ceed ceed = v->ceed;
   free(v);
   *vec = NULL;
@@ -1857,6 +1929,30 @@ static int op_apply_add(CeedOperator op, CeedVector in, CeedVector out) {
   return op_apply_add_single(op, in, out);
 }
 
+/* After an operator's kernels are enqueued, record on the compute stream that every vector it touched has been used up
+ * to here: later copies into or out of those vectors wait for this point only, not for work enqueued after it. */
+static int vec_mark_used(CeedVector v) {
+  if (!v || v == CEED_VECTOR_ACTIVE || v == CEED_VECTOR_NONE || !v->d) return CEED_ERROR_SUCCESS;
+  CK(vec_events(v));
+  CUDA_CK(v->ceed, cudaEventRecord(v->ev_use, v->ceed->stream));
+  v->use_known = 1;
+  return CEED_ERROR_SUCCESS;
+}
+static int op_mark_used(CeedOperator op) {
+  for (int i = 0; i < MAX_FIELDS; i++) {
+    CK(vec_mark_used(op->in[i].v));
+    CK(vec_mark_used(op->out[i].v));
+  }
+  for (int i = 0; i < op->nsub; i++) CK(op_mark_used(op->subs[i]));
+  return CEED_ERROR_SUCCESS;
+}
+static int op_apply_marked(CeedOperator op, CeedVector in, CeedVector out) {
+  CK(op_apply_add(op, in, out));
+  CK(op_mark_used(op));
+  CK(vec_mark_used(in));
+  return vec_mark_used(out);
+}
+
 int CeedOperatorApply(CeedOperator op, CeedVector in, CeedVector out, CeedRequest *request) {
   (void)request;
   if (out && out != CEED_VECTOR_NONE) {
@@ -1864,12 +1960,12 @@ int CeedOperatorApply(CeedOperator op, CeedVector in, CeedVector out, CeedReques
     int only_setup = !op->composite && (op_plan(op) == 0) && (op->plan == PLAN_SETUP || op->plan == PLAN_SETUP_SUR);
     if (!only_setup) CK(CeedVectorSetValue(out, 0.0));
   }
-  return op_apply_add(op, in, out);
+  return op_apply_marked(op, in, out);
 }
 
 int CeedOperatorApplyAdd(CeedOperator op, CeedVector in, CeedVector out, CeedRequest *request) {
   (void)request;
-  return op_apply_add(op, in, out);
+  return op_apply_marked(op, in, out);
 }
 
 static int op_diag_add_single(CeedOperator op, CeedVector assembled) {
