@@ -1515,24 +1515,25 @@ static int gather_coords(CeedOperator op, OpField *fx, CeedVector xvec, double *
  * qfunctions/bc_freestream.h:54-138).  Inputs "q"/"dq" (INTERP), "Grad_q"/"Grad_dq" (GRAD, unused by the flux),
  * "surface qdata" (NONE, 10), "x" (INTERP, unused); IFunction outputs "v" (INTERP) and, for implicit runs, "surface
  * jacobian data" (NONE, 5); the IJacobian reads that data as its fifth input.  Returns the flux type through the name. */
-static int freestream_kernel(const char *k, int *jacobian, int *flux_type) {
-  static const struct {
-    const char *name;
-    int         jac, flux;
-  } tab[] = {{"Freestream_Conserv_HLL", 0, 0},
-             {"Freestream_Conserv_HLLC", 0, 1},
-             {"Freestream_Jacobian_Conserv_HLL", 1, 0},
-             {"Freestream_Jacobian_Conserv_HLLC", 1, 1}};
-  for (size_t i = 0; i < sizeof tab / sizeof tab[0]; i++)
-    if (!strcmp(k, tab[i].name)) {
-      *jacobian  = tab[i].jac;
-      *flux_type = tab[i].flux;
-      return 1;
-    }
+/* "Freestream[_Jacobian]_{Conserv,Prim,Entropy}_{HLL,HLLC}" (qfunctions/bc_freestream.h:54-76, 116-138) */
+static int freestream_kernel(const char *k, int *jacobian, int *flux_type, int *state_var) {
+  static const char *sv_names[3] = {"Conserv", "Prim", "Entropy"};
+  for (int jac = 0; jac < 2; jac++)
+    for (int sv = 0; sv < 3; sv++)
+      for (int flux = 0; flux < 2; flux++) {
+        char name[64];
+        snprintf(name, sizeof name, "Freestream_%s%s_%s", jac ? "Jacobian_" : "", sv_names[sv], flux ? "HLLC" : "HLL");
+        if (!strcmp(k, name)) {
+          *jacobian  = jac;
+          *flux_type = flux;
+          *state_var = sv;
+          return 1;
+        }
+      }
   return 0;
 }
 
-static int plan_freestream(CeedOperator op, int jacobian, int flux_type) {
+static int plan_freestream(CeedOperator op, int jacobian, int flux_type, int state_var) {
   CeedQFunction qf = op->qf;
   const int     nin = jacobian ? 5 : 4, nout = jacobian ? 1 : (qf->nout == 2 ? 2 : 1);
   if (qf->nin != nin || qf->nout != nout || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[0].size != 5 || qf->in[1].emode != CEED_EVAL_GRAD ||
@@ -1549,8 +1550,8 @@ static int plan_freestream(CeedOperator op, int jacobian, int flux_type) {
     return plan_fail(op, "face restriction must be 5 node-interleaved components (comp_stride 1) with offsets");
   if (!is_tensor2(b, 5) || r->elem_size != b->P1d * b->P1d) return plan_fail(op, "face basis must be a 2D tensor H1 basis with 5 components");
   if (!qf->ctx || qf->ctx->size != sizeof(HbFreestreamContext)) return plan_fail(op, "context must be the 264-byte FreestreamContext_");
-  if (((const HbFreestreamContext *)qf->ctx->data)->newt.state_var != HB_STATEVAR_CONSERVATIVE)
-    return plan_fail(op, "free-stream context must use conservative variables");
+  if (((const HbFreestreamContext *)qf->ctx->data)->newt.state_var != state_var)
+    return plan_fail(op, "the free-stream context's state_var differs from the QFunction's");
   const int Q2 = b->Q1d * b->Q1d;
   CK(check_qdata_rstr(op, op->in[2].r, 10, Q2, "surface qdata"));
   if (jacobian) CK(check_qdata_rstr(op, op->in[4].r, 5, Q2, "surface jacobian data"));
@@ -1701,8 +1702,8 @@ static int op_plan(CeedOperator op) {
     op->plan = PLAN_SETUP_SUR;
     return CEED_ERROR_SUCCESS;
   }
-  int jacobian, flux_type;
-  if (freestream_kernel(k, &jacobian, &flux_type)) return plan_freestream(op, jacobian, flux_type);
+  int jacobian, flux_type, fs_sv;
+  if (freestream_kernel(k, &jacobian, &flux_type, &fs_sv)) return plan_freestream(op, jacobian, flux_type, fs_sv);
   return plan_fail(op, "no fused kernel for this QFunction (no CPU fallback on /gpu/b200)");
 }
 

@@ -26,6 +26,7 @@ struct Exterior {
   double cv, gamma, gm1;
   double U[5], Y[5];  // free-stream State: conservative (rho, m, E) and primitive (P, u, T)
   int hllc;
+  int sv;             // state variable of q and of the stored face state (HbStateVariable)
 };
 
 inline int rc() { return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA; }
@@ -74,6 +75,19 @@ __device__ __forceinline__ void exterior_state(const Exterior &x, hb::St<double>
   s.T_ = x.Y[4];
 }
 
+// StateFromQ / StateFromQ_fwd for the face's state variable (a run-time switch: boundary work is O(E^(2/3)))
+__device__ __forceinline__ void face_state(int sv, const hb::PhysConst<double> &pc, const double q[5], hb::St<double> &s, hb::SAux<double> &a) {
+  if (sv == HB_STATEVAR_PRIMITIVE) hb::state_from_q<HB_STATEVAR_PRIMITIVE>(pc, q, s, a);
+  else if (sv == HB_STATEVAR_ENTROPY) hb::state_from_q<HB_STATEVAR_ENTROPY>(pc, q, s, a);
+  else hb::state_from_q<HB_STATEVAR_CONSERVATIVE>(pc, q, s, a);
+}
+__device__ __forceinline__ void face_state_fwd(int sv, const hb::PhysConst<double> &pc, const hb::St<double> &s, const hb::SAux<double> &a,
+                                               const double dq[5], hb::St<double> &ds) {
+  if (sv == HB_STATEVAR_PRIMITIVE) hb::state_from_q_fwd<HB_STATEVAR_PRIMITIVE>(pc, s, a, dq, ds);
+  else if (sv == HB_STATEVAR_ENTROPY) hb::state_from_q_fwd<HB_STATEVAR_ENTROPY>(pc, s, a, dq, ds);
+  else hb::state_from_q_fwd<HB_STATEVAR_CONSERVATIVE>(pc, s, a, dq, ds);
+}
+
 // v += wdetJb * F_riemann(q, S_infty, n) integrated against the face basis; jac_sur [F][5][Q^2] = q at the points
 // (Freestream, bc_freestream.h:14-48)
 __global__ void k_freestream(int P, int Q, const int32_t *__restrict__ offsets, const int32_t *__restrict__ faces, FaceBasis b,
@@ -91,8 +105,8 @@ __global__ void k_freestream(int P, int Q, const int32_t *__restrict__ offsets, 
       for (int c = 0; c < 5; c++) U[c] += w * sN[c][p];
     }
     hb::St<double> s, sx;
-    double inv_rho, etot, eint;
-    hb::state_from_u(pc, U, s, inv_rho, etot, eint);
+    hb::SAux<double> aux;
+    face_state(ex.sv, pc, U, s, aux);
     exterior_state(ex, sx);
     const double *qf = qd + (int64_t)f * 10 * Q2;
     const double wdetJb = qf[t], n[3] = {qf[Q2 + t], qf[2 * Q2 + t], qf[3 * Q2 + t]};
@@ -131,9 +145,9 @@ __global__ void k_freestream_jac(int P, int Q, const int32_t *__restrict__ offse
     }
     for (int c = 0; c < 5; c++) U[c] = jac[((int64_t)f * 5 + c) * Q2 + t];
     hb::St<double> s, ds, sx, dsx;
-    double inv_rho, etot, eint;
-    hb::state_from_u(pc, U, s, inv_rho, etot, eint);
-    hb::state_from_u_fwd(pc, s, inv_rho, etot, eint, dU, ds);
+    hb::SAux<double> aux;
+    face_state(ex.sv, pc, U, s, aux);
+    face_state_fwd(ex.sv, pc, s, aux, dU, ds);
     exterior_state(ex, sx);
     memset(&dsx, 0, sizeof dsx);
     const double *qf = qd + (int64_t)f * 10 * Q2;
@@ -166,8 +180,8 @@ __global__ void k_freestream_diag(int P, int Q, const int32_t *__restrict__ offs
     double U[5];
     for (int c = 0; c < 5; c++) U[c] = jac[((int64_t)f * 5 + c) * Q2 + t];
     hb::St<double> s, sx, dsx;
-    double inv_rho, etot, eint;
-    hb::state_from_u(pc, U, s, inv_rho, etot, eint);
+    hb::SAux<double> aux;
+    face_state(ex.sv, pc, U, s, aux);
     exterior_state(ex, sx);
     memset(&dsx, 0, sizeof dsx);
     const double *qf = qd + (int64_t)f * 10 * Q2;
@@ -177,7 +191,7 @@ __global__ void k_freestream_diag(int P, int Q, const int32_t *__restrict__ offs
       double dU[5] = {0, 0, 0, 0, 0}, dF[5];
       dU[c] = 1.0;
       hb::St<double> ds;
-      hb::state_from_u_fwd(pc, s, inv_rho, etot, eint, dU, ds);
+      face_state_fwd(ex.sv, pc, s, aux, dU, ds);
       if (ex.hllc) hb::riemann::hllc_flux_fwd(ex.gamma, ex.cv, s, ds, sx, dsx, n, dF);
       else hb::riemann::hll_flux_fwd(ex.gamma, ex.cv, s, ds, sx, dsx, n, dF);
       if (FULL) {
@@ -218,8 +232,10 @@ int nthreads(const HbFaceOp *op) {
 int unpack_ctx(const void *ctx264, hb::PhysConst<double> &pc, Exterior &ex) {
   HbFreestreamContext c;
   memcpy(&c, ctx264, sizeof c);
-  if (c.newt.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  if (c.newt.state_var != HB_STATEVAR_CONSERVATIVE && c.newt.state_var != HB_STATEVAR_PRIMITIVE && c.newt.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   memset(&pc, 0, sizeof pc);
+  ex.sv = c.newt.state_var;
   pc.cv = c.newt.gas.cv;
   pc.inv_cv = 1.0 / c.newt.gas.cv;
   pc.gm1 = c.newt.gas.cp / c.newt.gas.cv - 1;

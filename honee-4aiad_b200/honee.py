@@ -183,7 +183,7 @@ class NewtonianOperators:
     # ---- boundary faces
     def add_freestream(self, P_inf, u_inf, T_inf, *, riemann="hllc", sides=None, implicit=True):
         """Free-stream condition on the non-periodic box sides: face restriction and 2D basis of the state, the bilinear
-        face coordinate field, surface qdata from ``SetupBoundary``, and the ``Freestream_[Jacobian_]Conserv_HLL[C]`` sub-
+        face coordinate field, surface qdata from ``SetupBoundary``, and the ``Freestream_[Jacobian_]{Conserv,Prim,Entropy}_HLL[C]`` sub-
         operators joined to the IFunction and IJacobian composites (num_comps_jac_data 5 for implicit runs,
         problems/bc_freestream.c:175)."""
         ceed, mesh, basis = self.ceed, self.mesh, self.basis
@@ -192,6 +192,7 @@ class NewtonianOperators:
         F = off.shape[0]
         Q2 = Q * Q
         flux = {"hll": "HLL", "hllc": "HLLC"}[riemann]
+        sv_name = ("Conserv", "Prim", "Entropy")[self.ctx.state_var]  # the QFunctions of the state variable
         # -- face restriction and basis of the state (DMPlexCeedElemRestrictionCreate / DMPlexCeedBasisCreate at the face height)
         rstr_q = ce.ElemRestriction(ceed, F, P * P, 5, 1, mesh.l_size, offsets=off)
         basis_q = ce.Basis(ceed, 2, 5, P, Q, basis.interp1d, basis.grad1d, basis.qref1d, basis.qweight1d)
@@ -222,7 +223,7 @@ class NewtonianOperators:
         rstr_jd = ce.ElemRestriction(ceed, F, Q2, 5, 0, F * Q2 * 5) if njd else None
         jac_data = ce.Vector(ceed, F * Q2 * 5) if njd else None
         # -- IFunction face sub-operator
-        qf_if = ce.QFunction(ceed, f"bc_freestream.h:Freestream_Conserv_{flux}")
+        qf_if = ce.QFunction(ceed, f"bc_freestream.h:Freestream_{sv_name}_{flux}")
         for name, size, mode in (("q", 5, ce.CEED_EVAL_INTERP), ("Grad_q", 10, ce.CEED_EVAL_GRAD), ("surface qdata", 10, ce.CEED_EVAL_NONE),
                                  ("x", 3, ce.CEED_EVAL_INTERP)):
             qf_if.add_input(name, size, mode)
@@ -242,7 +243,7 @@ class NewtonianOperators:
         self.op_ifunction.add_sub(op_if)
         op_ij = None
         if njd:
-            qf_ij = ce.QFunction(ceed, f"bc_freestream.h:Freestream_Jacobian_Conserv_{flux}")
+            qf_ij = ce.QFunction(ceed, f"bc_freestream.h:Freestream_Jacobian_{sv_name}_{flux}")
             for name, size, mode in (("dq", 5, ce.CEED_EVAL_INTERP), ("Grad_dq", 10, ce.CEED_EVAL_GRAD),
                                      ("surface qdata", 10, ce.CEED_EVAL_NONE), ("x", 3, ce.CEED_EVAL_INTERP),
                                      ("surface jacobian data", njd, ce.CEED_EVAL_NONE)):

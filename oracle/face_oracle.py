@@ -37,6 +37,51 @@ def state_from_U_fwd(s, dU, cv, cp):
     return St(drho, dm, dE, (cp / cv - 1) * (drho * e + s.rho * de), du, de / cv)
 
 
+def state_from_q(q, sv, cv, cp):
+    """StateFromQ (newtonian_state.h:393-407) over points: conservative U, primitive Y = (P, u, T) (StateFromY, :159-168),
+    entropy V (StateFromV: StatePrimitiveFromEntropy :122-132, StateConservativeFromEntropy :222-238)."""
+    q = np.asarray(q, dtype=np.float64)
+    if sv == 0:
+        return state_from_U(q, cv, cp)
+    R, g = cp - cv, cp / cv
+    if sv == 1:
+        P, u, T = q[0], q[1:4], q[4]
+        rho = P / (R * T)
+        return St(rho, rho * u, rho * (cv * T + 0.5 * (u * u).sum(0)), P, u, T)
+    V = q
+    u = -V[1:4] / V[4]
+    T = -1 / (R * V[4])
+    ke = 0.5 * (u * u).sum(0)
+    ent = g - (g - 1) * (V[0] - ke * V[4])
+    P = np.exp(-(ent + g * np.log(-V[4])) / (g - 1))
+    rho = np.exp(-(ent + np.log(-V[4])) / (g - 1))
+    return St(rho, rho * u, rho * (-cv / (R * V[4]) + ke), P, u, T)
+
+
+def state_from_q_fwd(s, dq, sv, cv, cp):
+    """StateFromQ_fwd (newtonian_state.h:409-423) over points for the state variable sv."""
+    dq = np.asarray(dq, dtype=np.float64)
+    if sv == 0:
+        return state_from_U_fwd(s, dq, cv, cp)
+    R, g = cp - cv, cp / cv
+    ke = 0.5 * (s.u * s.u).sum(0)
+    if sv == 1:  # StateFromY_fwd (:170-184)
+        dP, du, dT = dq[0], dq[1:4], dq[4]
+        drho = (dP * s.T - s.P * dT) / (R * s.T * s.T)
+        dke = (du * s.u).sum(0)
+        return St(drho, drho * s.u + s.rho * du, drho * (cv * s.T + ke) + s.rho * (cv * dT + dke), dP, du, dT)
+    V4 = -1 / (R * s.T)  # the entropy variable V4 of the state (StateEntropyFromPrimitive, :91-103)
+    du = (-dq[1:4] - s.u * dq[4]) / V4
+    dke = (du * s.u).sum(0)
+    dent = -(g - 1) * (dq[0] - (dke * V4 + ke * dq[4]))
+    drho = -s.rho / (g - 1) * (dent + dq[4] / V4)
+    deint = cv * dq[4] / (R * V4 * V4)
+    dE = drho * (-cv / (R * V4) + ke) + s.rho * (deint + dke)
+    dT = dq[4] / (R * V4 * V4)
+    dP = s.P * (-dent - g * dq[4] / V4) / (g - 1)
+    return St(drho, drho * s.u + s.rho * du, dE, dP, du, dT)
+
+
 def flux_n(s, n):
     mn = (s.m * n).sum(0)
     un = (s.u * n).sum(0)
@@ -175,8 +220,9 @@ def face_qdata(interp1d, grad1d, qweight1d, P, Q, x_nodes):
     return out
 
 
-def freestream_apply(offsets, interp1d, P, Q, qdata_sur, q, U_inf, Y_inf, cv, cp, hllc=True, dq=None, jac=None, l_size=None):
-    """Residual contribution (dq None) or Jacobian action (dq given, jac = q at the face points) as an L-vector."""
+def freestream_apply(offsets, interp1d, P, Q, qdata_sur, q, U_inf, Y_inf, cv, cp, hllc=True, dq=None, jac=None, l_size=None, sv=0):
+    """Residual contribution (dq None) or Jacobian action (dq given, jac = q at the face points) as an L-vector; q, dq and
+    jac in the state variable sv (Freestream_{Conserv,Prim,Entropy}, bc_freestream.h:54-76)."""
     B = np.asarray(interp1d).reshape(Q, P)
     Bq = np.einsum("jb,ia->jiba", B, B).reshape(Q * Q, P * P)
     F = offsets.shape[0]
@@ -188,11 +234,11 @@ def freestream_apply(offsets, interp1d, P, Q, qdata_sur, q, U_inf, Y_inf, cv, cp
         Uq = (Bq @ src).T                                                 # [5][Q2]
         n = qdata_sur[f, 1:4]
         if dq is None:
-            s = state_from_U(Uq, cv, cp)
+            s = state_from_q(Uq, sv, cv, cp)
             flux = riemann(s, exterior(U_inf, Y_inf, Q * Q), n, cv, cp, hllc)
         else:
-            s = state_from_U(jac[f], cv, cp)
-            ds = state_from_U_fwd(s, Uq, cv, cp)
+            s = state_from_q(jac[f], sv, cv, cp)
+            ds = state_from_q_fwd(s, Uq, sv, cv, cp)
             zero = St(*(np.zeros(Q * Q) if k not in (1, 4) else np.zeros((3, Q * Q)) for k in range(6)))
             flux = riemann(s, exterior(U_inf, Y_inf, Q * Q), n, cv, cp, hllc, dL=ds, dR=zero)
         v = qdata_sur[f, 0][None] * flux
@@ -202,7 +248,7 @@ def freestream_apply(offsets, interp1d, P, Q, qdata_sur, q, U_inf, Y_inf, cv, cp
     return out
 
 
-def freestream_diagonal(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, cv, cp, hllc=True, l_size=None):
+def freestream_diagonal(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, cv, cp, hllc=True, l_size=None, sv=0):
     """Diagonal of the free-stream Jacobian as an L-vector: for face node p and component c, the sum over the face's
     points of B_p^2 wdetJb dF_c/dU_c, the column of the point Jacobian taken by the forward tangent with dU = e_c (the
     libCEED diagonal assembly of the Freestream_Jacobian operator, bc_freestream.h:75-114, summed over faces)."""
@@ -212,13 +258,13 @@ def freestream_diagonal(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, c
     out = np.zeros(l_size if l_size is not None else int(offsets.max()) + 5)
     zero = St(*(np.zeros(Q * Q) if k not in (1, 4) else np.zeros((3, Q * Q)) for k in range(6)))
     for f in range(F):
-        s = state_from_U(jac[f], cv, cp)
+        s = state_from_q(jac[f], sv, cv, cp)
         n = qdata_sur[f, 1:4]
         D = np.zeros((5, Q * Q))
         for c in range(5):
             dU = np.zeros((5, Q * Q))
             dU[c] = 1.0
-            ds = state_from_U_fwd(s, dU, cv, cp)
+            ds = state_from_q_fwd(s, dU, sv, cv, cp)
             D[c] = qdata_sur[f, 0] * riemann(s, exterior(U_inf, Y_inf, Q * Q), n, cv, cp, hllc, dL=ds, dR=zero)[c]
         contrib = (Bq.T ** 2) @ D.T                                          # [P2][5]
         for p in range(P * P):
@@ -226,7 +272,7 @@ def freestream_diagonal(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, c
     return out
 
 
-def freestream_point_block(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, cv, cp, hllc=True, l_size=None):
+def freestream_point_block(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf, cv, cp, hllc=True, l_size=None, sv=0):
     """5 x 5 point blocks of the free-stream Jacobian, out[(node * 5 + i) * 5 + j] = sum over a node's face points of
     B_p^2 wdetJb dF_i/dU_j (the point-block assembly of the Freestream_Jacobian operator, summed over faces)."""
     B = np.asarray(interp1d).reshape(Q, P)
@@ -235,13 +281,13 @@ def freestream_point_block(offsets, interp1d, P, Q, qdata_sur, jac, U_inf, Y_inf
     out = np.zeros(5 * n_l)
     zero = St(*(np.zeros(Q * Q) if k not in (1, 4) else np.zeros((3, Q * Q)) for k in range(6)))
     for f in range(offsets.shape[0]):
-        s = state_from_U(jac[f], cv, cp)
+        s = state_from_q(jac[f], sv, cv, cp)
         n = qdata_sur[f, 1:4]
         D = np.zeros((5, 5, Q * Q))                                             # [i][j][point]
         for j in range(5):
             dU = np.zeros((5, Q * Q))
             dU[j] = 1.0
-            ds = state_from_U_fwd(s, dU, cv, cp)
+            ds = state_from_q_fwd(s, dU, sv, cv, cp)
             D[:, j] = qdata_sur[f, 0] * riemann(s, exterior(U_inf, Y_inf, Q * Q), n, cv, cp, hllc, dL=ds, dR=zero)
         contrib = np.einsum("kp,ijk->pij", Bq ** 2, D)                          # [P2][5][5]
         for p in range(P * P):

@@ -113,5 +113,9 @@ EXPORT int ref_Freestream_Conserv_HLL(void *c, CeedInt Q, In in, Out out) { retu
 EXPORT int ref_Freestream_Conserv_HLLC(void *c, CeedInt Q, In in, Out out) { return Freestream_Conserv_HLLC(c, Q, in, out); }
 EXPORT int ref_Freestream_Jacobian_Conserv_HLL(void *c, CeedInt Q, In in, Out out) { return Freestream_Jacobian_Conserv_HLL(c, Q, in, out); }
 EXPORT int ref_Freestream_Jacobian_Conserv_HLLC(void *c, CeedInt Q, In in, Out out) { return Freestream_Jacobian_Conserv_HLLC(c, Q, in, out); }
+EXPORT int ref_Freestream_Prim_HLLC(void *c, CeedInt Q, In in, Out out) { return Freestream_Prim_HLLC(c, Q, in, out); }
+EXPORT int ref_Freestream_Entropy_HLL(void *c, CeedInt Q, In in, Out out) { return Freestream_Entropy_HLL(c, Q, in, out); }
+EXPORT int ref_Freestream_Jacobian_Prim_HLLC(void *c, CeedInt Q, In in, Out out) { return Freestream_Jacobian_Prim_HLLC(c, Q, in, out); }
+EXPORT int ref_Freestream_Jacobian_Entropy_HLL(void *c, CeedInt Q, In in, Out out) { return Freestream_Jacobian_Entropy_HLL(c, Q, in, out); }
 EXPORT int ref_SetupBoundary(void *c, CeedInt Q, In in, Out out) { return SetupBoundary(c, Q, in, out); }
 EXPORT int ref_freestream_ctx_size(void) { return (int)sizeof(struct FreestreamContext_); }

@@ -105,3 +105,37 @@ def test_face_diagonal_is_the_oracle_jacobian_diagonal(hllc):
         e[i] = 1.0
         col = FO.freestream_apply(off, basis.interp1d, 3, 3, qd, q, U, Y, cv, cp, hllc=hllc, dq=e, jac=jac)
         assert abs(col[i] - d[i]) <= 1e-12 * np.abs(d).max()
+
+
+@pytest.mark.parametrize("sv,flux", [(1, "HLLC"), (2, "HLL")])
+def test_state_variables_match_reference(sv, flux):
+    """The oracle's free-stream flux and tangent in primitive (Freestream_Prim_HLLC) and entropy (Freestream_Entropy_HLL)
+    variables against the reference's QFunctions compiled in oracle/_ref, on the fixture's points converted to those
+    variables (the stored face state is the state in its own variables)."""
+    import importlib
+    import oracle as O
+    if O.ref() is None:
+        pytest.skip("oracle/_ref not built")
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    U, Y, cv, cp = _ext()
+    name = ("Conserv", "Prim", "Entropy")[sv]
+    qd = np.ascontiguousarray(G["qdata"])
+    n = qd.shape[1]
+    newt = prob.newtonian_context(2, cv=cv, cp=cp)
+    newt.state_var = sv
+    ctx = prob.freestream_context(newt, float(G["P_inf"]), np.asarray(G["u_inf"]), float(G["T_inf"]))
+    qv = np.ascontiguousarray(prob.state_to_q(newt.gas, G["q"].T.reshape(-1), sv).reshape(-1, 5).T)
+    v, jac = np.zeros((5, n)), np.zeros((5, n))
+    grad, x = np.zeros((10, n)), np.zeros((3, n))
+    assert O.call_qf(getattr(O.ref(), f"ref_Freestream_{name}_{flux}"), ctx, n, [qv, grad, qd, x], [v, jac]) == 0
+    np.testing.assert_array_equal(jac, qv)
+    s = FO.state_from_q(qv, sv, cv, cp)
+    F = FO.riemann(s, FO.exterior(U, Y, n), qd[1:4], cv, cp, hllc=flux == "HLLC")
+    np.testing.assert_allclose(qd[0] * F, v, rtol=1e-11, atol=1e-11 * np.abs(v).max())
+    dq = qv * 1e-3 * np.random.default_rng(sv).normal(size=qv.shape)
+    dv = np.zeros((5, n))
+    assert O.call_qf(getattr(O.ref(), f"ref_Freestream_Jacobian_{name}_{flux}"), ctx, n, [dq, grad, qd, x, jac], [dv]) == 0
+    ds = FO.state_from_q_fwd(s, dq, sv, cv, cp)
+    zero = FO.St(np.zeros(n), np.zeros((3, n)), np.zeros(n), np.zeros(n), np.zeros((3, n)), np.zeros(n))
+    dF = FO.riemann(s, FO.exterior(U, Y, n), qd[1:4], cv, cp, hllc=flux == "HLLC", dL=ds, dR=zero)
+    np.testing.assert_allclose(qd[0] * dF, dv, rtol=1e-9, atol=1e-9 * np.abs(dv).max())
