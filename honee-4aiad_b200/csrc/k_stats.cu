@@ -18,6 +18,7 @@
 #include <string.h>
 
 #include "honee_b200.h"
+#include "newtonian_qf.cuh"
 
 namespace hbs {
 
@@ -37,6 +38,7 @@ struct CollectArgs {
   const double *qdata;          // [E][10][Q^3], component 0 = w detJ
   double dt;                    // solution_time - previous_time
   double cv, gm1;               // cv and cp / cv - 1
+  hb::PhysConst<double> pc;     // gas constants for primitive / entropy states (state_from_q)
   double *sums;                 // [num_columns][Q^2][22]
 };
 
@@ -73,7 +75,26 @@ __device__ __forceinline__ void turb_stats(const double U[5], double w, double c
   for (int i = 0; i < 3; i++) v[19 + i] = w * u[i];
 }
 
-template <int P, int Q>
+// The same statistics from a state given in any of the three variables (ChildStatsCollection_Prim / _Entropy,
+// turbulence.h:85-91: StateFromQ first), products in the reference's order.
+__device__ __forceinline__ void turb_stats_state(const hb::St<double> &s, double w, double v[NS]) {
+  v[0] = w * s.rho;
+  v[1] = w * s.P;
+  v[2] = w * (s.P * s.P);
+  for (int i = 0; i < 3; i++) v[3 + i] = w * s.P * s.u[i];
+  v[6] = w * s.rho * s.T_;
+  for (int i = 0; i < 3; i++) v[7 + i] = w * s.rho * s.T_ * s.u[i];
+  for (int i = 0; i < 3; i++) v[10 + i] = w * s.m[i];
+  v[13] = w * s.m[0] * s.u[0];
+  v[14] = w * s.m[1] * s.u[1];
+  v[15] = w * s.m[2] * s.u[2];
+  v[16] = w * s.m[1] * s.u[2];
+  v[17] = w * s.m[0] * s.u[2];
+  v[18] = w * s.m[0] * s.u[1];
+  for (int i = 0; i < 3; i++) v[19 + i] = w * s.u[i];
+}
+
+template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
 __global__ void __launch_bounds__(kThreads) k_stats_collect(const CollectArgs a, const Interp1D bas) {
   using L = CollectPlan<P, Q>;
   constexpr int NT = kThreads, P2 = P * P, P3 = L::P3, Q2 = L::Q2, Q3 = L::Q3, P2Q = P2 * Q, PQ2 = P * Q2;
@@ -116,7 +137,14 @@ __global__ void __launch_bounds__(kThreads) k_stats_collect(const CollectArgs a,
         double U[5], v[NS];
 #pragma unroll
         for (int c = 0; c < 5; c++) U[c] = sY[c * Q3 + qp];
-        turb_stats(U, __ldg(wq + qp) * a.dt, a.cv, a.gm1, v);
+        if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
+          turb_stats(U, __ldg(wq + qp) * a.dt, a.cv, a.gm1, v);
+        } else {
+          hb::St<double> st;
+          hb::SAux<double> aux;
+          hb::state_from_q<SV>(a.pc, U, st, aux);
+          turb_stats_state(st, __ldg(wq + qp) * a.dt, v);
+        }
 #pragma unroll
         for (int s = 0; s < NS; s++) sS[s * Q3 + qp] = v[s];
       }
@@ -281,12 +309,18 @@ static int grid_for(int n_items, const void *fn, size_t smem) {
   return n_items < g ? (n_items > 0 ? n_items : 1) : g;
 }
 
-template <int P, int Q>
-static int launch_collect(const CollectArgs &a, const Interp1D &b, cudaStream_t s) {
+template <int P, int Q, int SV>
+static int launch_collect_sv(const CollectArgs &a, const Interp1D &b, cudaStream_t s) {
   const size_t sm = CollectPlan<P, Q>::bytes;
-  if (cudaFuncSetAttribute(k_stats_collect<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
-  k_stats_collect<P, Q><<<grid_for(a.num_columns, (const void *)k_stats_collect<P, Q>, sm), kThreads, sm, s>>>(a, b);
+  if (cudaFuncSetAttribute(k_stats_collect<P, Q, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
+  k_stats_collect<P, Q, SV><<<grid_for(a.num_columns, (const void *)k_stats_collect<P, Q, SV>, sm), kThreads, sm, s>>>(a, b);
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+template <int P, int Q>
+static int launch_collect(const CollectArgs &a, const Interp1D &b, int sv, cudaStream_t s) {
+  if (sv == HB_STATEVAR_PRIMITIVE) return launch_collect_sv<P, Q, HB_STATEVAR_PRIMITIVE>(a, b, s);
+  if (sv == HB_STATEVAR_ENTROPY) return launch_collect_sv<P, Q, HB_STATEVAR_ENTROPY>(a, b, s);
+  return launch_collect_sv<P, Q, HB_STATEVAR_CONSERVATIVE>(a, b, s);
 }
 
 // kind 0: mass apply (u -> v), 1: projection right-hand side (sums -> v), 2: mass diagonal (-> v[node])
@@ -331,8 +365,10 @@ extern "C" int hb_stats_collect(const HbElemOp *op, const void *ctx184, const do
   if (num_columns == 0) return HB_SUCCESS;
   HbNewtonianContext ctx;
   memcpy(&ctx, ctx184, sizeof ctx);
-  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE && ctx.state_var != HB_STATEVAR_PRIMITIVE && ctx.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   CollectArgs a;
+  memset(&a, 0, sizeof a);
   a.offsets = op->d_offsets;
   a.column_elems = d_column_elems;
   a.num_columns = num_columns;
@@ -342,11 +378,15 @@ extern "C" int hb_stats_collect(const HbElemOp *op, const void *ctx184, const do
   a.dt = dt;
   a.cv = ctx.gas.cv;
   a.gm1 = ctx.gas.cp / ctx.gas.cv - 1;
+  a.pc.cv = ctx.gas.cv;
+  a.pc.inv_cv = 1.0 / ctx.gas.cv;
+  a.pc.gm1 = a.gm1;
+  a.pc.Rgas = ctx.gas.cp - ctx.gas.cv;
   a.sums = sums;
   const Interp1D b = interp_of(op->interp1d, op->P, op->Q);
   cudaStream_t s = (cudaStream_t)stream;
 #define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_collect<PP, QQ>(a, b, s);
+  if (op->P == PP && op->Q == QQ) return launch_collect<PP, QQ>(a, b, ctx.state_var, s);
   HB_STATS_PQ_LIST(HB_CASE)
 #undef HB_CASE
   return HB_ERROR_UNSUPPORTED;

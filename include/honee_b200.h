@@ -83,11 +83,12 @@ typedef struct {
   int           add;       /* 0: v = F(q), 1: v += F(q) */
 } HbIFunctionIO;
 
-/* Fused IFunction_Newtonian_Conserv operator (qfunctions/newtonian.h:205-261 inside the volume operator of
- * src/setuplibceed.c:209-243), called where HONEE calls CeedOperatorApply(op_ifunction) (src/setupts.c:109). */
+/* Fused IFunction_Newtonian_Conserv / _Prim / _Entropy operator, the variable taken from the context's state_var
+ * (qfunctions/newtonian.h:205-269 inside the volume operator of src/setuplibceed.c:209-243), called where HONEE calls
+ * CeedOperatorApply(op_ifunction) (src/setupts.c:109).  Primitive and entropy variables for degree 1-3. */
 HB_EXPORT int hb_ifunction_apply(const HbElemOp *op, const void *ctx184, const HbIFunctionIO *io, void *stream);
 
-/* Fused IJacobian_Newtonian_Conserv action (qfunctions/newtonian.h:272-315, operator src/setuplibceed.c:245-269),
+/* Fused IJacobian_Newtonian_Conserv / _Prim / _Entropy action (qfunctions/newtonian.h:272-323, operator src/setuplibceed.c:245-269),
  * called where MatMult_Ceed calls CeedOperatorApplyAdd (src/mat-ceed.c:1669).  FP64 and FP32 variants; the FP32 one
  * reads the FP32 shadow of jac_data and FP32 L-vectors, qdata stays FP64 and is rounded on load. */
 HB_EXPORT int hb_ijacobian_apply_f64(const HbElemOp *op, const void *ctx184, const double *qdata, const double *jac_data, const double *dq, double *v,
@@ -434,7 +435,7 @@ typedef struct HbPlaneOp {
 /* Parent-point sums of one collection (ChildStatsCollection_Conserv applied and reduced over the span,
  * turbulence.c:19-108 + spanstats.c:425-443): sums[col][Q^2][22] += sum over the elements d_column_elems[col][*] and their
  * quadrature planes of w detJ * dt * stats(q).  Each column lists the 3D elements whose first two reference axes
- * coincide with those of parent element `col`.  Conservative state only. */
+ * coincide with those of parent element `col`.  q in the context's state variable (ChildStatsCollection_Conserv/_Prim/_Entropy). */
 HB_EXPORT int hb_stats_collect(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double dt, int num_columns,
                                int column_length, const int32_t *d_column_elems, double *sums, void *stream);
 /* Parent mass matrix M (HoneeMassQFunctionCreate on the parent basis, spanstats.c:313-320), 22 components: v (+)= M u */

@@ -44,6 +44,8 @@ EXPORT size_t ref_channel_ctx_size(void) { return sizeof(struct ChannelContext_)
 EXPORT int ref_IC_GaussianWave_Conserv(void *c, CeedInt Q, In in, Out out) { return IC_GaussianWave_Conserv(c, Q, in, out); }
 EXPORT size_t ref_gaussianwave_ctx_size(void) { return sizeof(struct GaussianWaveContext_); }
 EXPORT int ref_ChildStatsCollection_Conserv(void *c, CeedInt Q, In in, Out out) { return ChildStatsCollection_Conserv(c, Q, in, out); }
+EXPORT int ref_ChildStatsCollection_Prim(void *c, CeedInt Q, In in, Out out) { return ChildStatsCollection_Prim(c, Q, in, out); }
+EXPORT int ref_ChildStatsCollection_Entropy(void *c, CeedInt Q, In in, Out out) { return ChildStatsCollection_Entropy(c, Q, in, out); }
 EXPORT size_t ref_turb_spanstats_ctx_size(void) { return sizeof(struct Turbulence_SpanStatsContext_); }
 
 /* State helpers: q (5) in state_var -> U (5) and Y (5); forward-mode tangents. */

@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import numpy as np
 
+import face_oracle as FaceO
 import filter_oracle as FO
 import oracle as O
 
@@ -57,8 +58,32 @@ def stats_weighted(U, w, cv, cp):
     return v
 
 
-def collect_child(mesh, basis, qdata, q, cv, cp, dt, child=None):
-    """child [E][Q^3][22] (+)= w detJ * dt * stats(B q_e) (the collocated child restriction is [elem][qpt][comp])."""
+def stats_state(s, w):
+    """ChildStatsCollection_Prim / _Entropy (turbulence.h:85-91): the statistics of a state already converted (StateFromQ)."""
+    v = np.empty((NS, np.asarray(s.rho).size))
+    v[0] = w * s.rho
+    v[1] = w * s.P
+    v[2] = w * (s.P * s.P)
+    for i in range(3):
+        v[3 + i] = w * s.P * s.u[i]
+    v[6] = w * s.rho * s.T
+    for i in range(3):
+        v[7 + i] = w * s.rho * s.T * s.u[i]
+        v[10 + i] = w * s.m[i]
+    v[13] = w * s.m[0] * s.u[0]
+    v[14] = w * s.m[1] * s.u[1]
+    v[15] = w * s.m[2] * s.u[2]
+    v[16] = w * s.m[1] * s.u[2]
+    v[17] = w * s.m[0] * s.u[2]
+    v[18] = w * s.m[0] * s.u[1]
+    for i in range(3):
+        v[19 + i] = w * s.u[i]
+    return v
+
+
+def collect_child(mesh, basis, qdata, q, cv, cp, dt, child=None, sv=0):
+    """child [E][Q^3][22] (+)= w detJ * dt * stats(B q_e) (the collocated child restriction is [elem][qpt][comp]); q in the
+    state variable sv."""
     P, Q = basis.P, basis.Q
     Q3 = Q ** 3
     Bq, _ = FO.tensor_ops(basis.interp1d, basis.grad1d, P, Q)
@@ -70,7 +95,10 @@ def collect_child(mesh, basis, qdata, q, cv, cp, dt, child=None):
     for e in range(mesh.num_elem):
         Uq = Bq @ qn[nodes[e]]                # [Q3][5]
         wdt = qd[e, 0] * dt
-        child[e] += stats_weighted(Uq.T, wdt, cv, cp).T
+        if sv == 0:
+            child[e] += stats_weighted(Uq.T, wdt, cv, cp).T
+        else:
+            child[e] += stats_state(FaceO.state_from_q(Uq.T, sv, cv, cp), wdt).T
     return child
 
 

@@ -148,7 +148,37 @@ def test_errors_are_reported():
     with pytest.raises(K.HbError):
         SP.SpanStats(op, bad)
     ctx = prob.newtonian_context(2)
-    ctx.state_var = 1  # primitive
+    ctx.state_var = 7  # not a state variable
     qdata = torch.zeros(mesh.num_elem * 10 * 64, dtype=torch.float64, device=_dev())
     with pytest.raises(K.HbError):
         st.collect(prob.context_bytes(ctx), torch.from_numpy(q0).to(_dev()), qdata, 1.5)
+
+
+@pytest.mark.parametrize("sv", [prob.STATEVAR_PRIMITIVE, prob.STATEVAR_ENTROPY])
+def test_collection_in_other_state_variables_matches_oracle(sv):
+    """ChildStatsCollection_Prim / _Entropy: the state handed over in primitive or entropy variables (interpolated in
+    those variables, then converted at each point)."""
+    import torch
+    mesh, basis, ch, q0 = channel_case((3, 3, 2), 3, 4)
+    ctx = ch.newt_ctx
+    ctx.state_var = sv
+    cb = prob.context_bytes(ctx)
+    op = K.ElemOp(mesh, basis)
+    qdata = O.setup_qdata(mesh.num_elem, 4, mesh.x_elem)
+    tqd = torch.from_numpy(qdata).to(_dev())
+    lay = SP.box_span_layout(mesh)
+    rng = np.random.default_rng(6)
+    states = [prob.state_to_q(ctx.gas, q0 * (1 + 0.01 * rng.uniform(-1, 1, q0.shape)), sv) for _ in range(2)]
+    times = [0.0, 2e-3, 3e-3]
+    st = SP.SpanStats(op, lay, initial_time=times[0])
+    for k, qk in enumerate(states):
+        st.collect(cb, torch.from_numpy(qk).to(_dev()), tqd, times[k + 1])
+    xy_p, wdetJ_p = SO.parent_points(lay.parent_x, basis.Q, basis.qref1d, basis.qweight1d)
+    match = SO.star_forest(SO.child_points_xy(mesh, basis.Q), xy_p)
+    child = None
+    for k, qk in enumerate(states):
+        child = SO.collect_child(mesh, basis, qdata, qk, ctx.gas.cv, ctx.gas.cp, times[k + 1] - times[k], child, sv=sv)
+    parent = SO.reduce_to_parent(child, match, xy_p.shape[0] * xy_p.shape[1])
+    got = st.sums().reshape(-1, 22)
+    for c in range(22):
+        assert rel_l2(got[:, c], parent[:, c]) < 1e-12, (c, SP.COMPONENTS[c])

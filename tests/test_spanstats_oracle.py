@@ -104,3 +104,30 @@ def test_average_of_steady_polynomial_field_is_exact():
     np.testing.assert_allclose(stats[:, 19], 3 + 2 * yn - yn ** 2, rtol=1e-12, atol=1e-13)
     np.testing.assert_allclose(stats[:, 20], 0.5 * yn, rtol=1e-12, atol=1e-14)
     np.testing.assert_allclose(stats[:, 12], rho0 * 0.25, rtol=1e-12)
+
+
+@pytest.mark.parametrize("sv", [1, 2])
+def test_statistics_in_other_state_variables_match_reference(sv):
+    """ChildStatsCollection_Prim / _Entropy (compiled in oracle/_ref) against the oracle's StateFromQ + statistics."""
+    if O.ref() is None:
+        pytest.skip("oracle/_ref not built")
+    ctx = _ctx()
+    ctx.state_var = sv
+    cb = prob.context_bytes(ctx)
+    rng = np.random.default_rng(5)
+    n = 129
+    rho = rng.uniform(0.8, 1.4, n)
+    u = rng.normal(0, 30, (3, n))
+    T = rng.uniform(250, 350, n)
+    U = np.vstack([rho, rho * u, rho * (ctx.gas.cv * T + 0.5 * (u * u).sum(0))])
+    qv = np.ascontiguousarray(prob.state_to_q(ctx.gas, U.T.reshape(-1), sv).reshape(-1, 5).T)
+    qdata = np.zeros((10, n))
+    qdata[0] = rng.uniform(1e-6, 1e-3, n)
+    v = np.zeros((22, n))
+    name = ("Conserv", "Prim", "Entropy")[sv]
+    ctx_stats = np.array([0.5 + 1e-3, 0.5]).tobytes() + cb
+    assert O.call_qf(getattr(O.ref(), f"ref_ChildStatsCollection_{name}"), ctx_stats, n, [qv, qdata, np.zeros((3, n))], [v]) == 0
+    import face_oracle as FaceO
+    mine = SO.stats_state(FaceO.state_from_q(qv, sv, ctx.gas.cv, ctx.gas.cp), qdata[0] * 1e-3)
+    for c in range(22):
+        np.testing.assert_allclose(mine[c], v[c], rtol=1e-12, atol=1e-14 * np.abs(v[c]).max(), err_msg=SP.COMPONENTS[c])
