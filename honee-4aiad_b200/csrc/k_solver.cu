@@ -265,9 +265,28 @@ __device__ void eval_point(const double *sN, int P, int Q, const MonBasis &b, in
       }
 }
 
-// per-element partial sums of the five kinetic-energy integrands [num_elem][5]
+// StateFromQ / StateFromQ_fwd for the monitors' state variable (run-time switch: the monitors are not on the hot path)
+__device__ __forceinline__ void mon_state(int sv, const hb::PhysConst<double> &pc, const double q[5], hb::St<double> &s, hb::SAux<double> &a) {
+  if (sv == HB_STATEVAR_PRIMITIVE) hb::state_from_q<HB_STATEVAR_PRIMITIVE>(pc, q, s, a);
+  else if (sv == HB_STATEVAR_ENTROPY) hb::state_from_q<HB_STATEVAR_ENTROPY>(pc, q, s, a);
+  else hb::state_from_q<HB_STATEVAR_CONSERVATIVE>(pc, q, s, a);
+}
+// physical gradient of the state (StatePhysicalGradientFromReference, newtonian_state.h:581-593) in the state variable sv
+__device__ __forceinline__ void mon_gradient(int sv, const hb::PhysConst<double> &pc, const hb::St<double> &s, const hb::SAux<double> &a,
+                                             const double gref[3][5], const double X[3][3], hb::St<double> gs[3]) {
+  for (int j = 0; j < 3; j++) {
+    double dq[5];
+    for (int c = 0; c < 5; c++) dq[c] = gref[0][c] * X[0][j] + gref[1][c] * X[1][j] + gref[2][c] * X[2][j];
+    if (sv == HB_STATEVAR_PRIMITIVE) hb::state_from_q_fwd<HB_STATEVAR_PRIMITIVE>(pc, s, a, dq, gs[j]);
+    else if (sv == HB_STATEVAR_ENTROPY) hb::state_from_q_fwd<HB_STATEVAR_ENTROPY>(pc, s, a, dq, gs[j]);
+    else hb::state_from_q_fwd<HB_STATEVAR_CONSERVATIVE>(pc, s, a, dq, gs[j]);
+  }
+}
+
+// per-element partial sums of the five kinetic-energy integrands [num_elem][5] (MonitorTotalKineticEnergy_Conserv/_Prim/
+// _Entropy, qfunctions/monitor_totalkineticenergy.h:8-51)
 __global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, const double *__restrict__ q, const double *__restrict__ qdata,
-                             hb::PhysConst<double> pc, MonBasis b, double *__restrict__ elem_sums) {
+                             hb::PhysConst<double> pc, int sv, MonBasis b, double *__restrict__ elem_sums) {
   extern __shared__ double sm[];
   const int e = blockIdx.x, P3 = P * P * P, Q3 = Q * Q * Q;
   double *sN = sm, *red = sm + 5 * P3;
@@ -281,10 +300,10 @@ __global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, 
     const double wdetJ = qd[qp];
     for (int kk = 0; kk < 9; kk++) X[kk / 3][kk % 3] = qd[(1 + kk) * Q3 + qp];
     hb::St<double> s;
-    double inv_rho, etot, eint;
-    hb::state_from_u(pc, qi, s, inv_rho, etot, eint);
+    hb::SAux<double> aux;
+    mon_state(sv, pc, qi, s, aux);
     hb::St<double> gs[3];
-    hb::physical_gradient(pc, s, inv_rho, etot, eint, gref, X, gs);
+    mon_gradient(sv, pc, s, aux, gref, X, gs);
     double e6[6], S[3][3];
     hb::km_strain(gs, e6);
     const double w = 1.0 / 1.4142135623730951;
@@ -314,9 +333,10 @@ __global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, 
   }
 }
 
-// per-element min/max over points of sqrt(u . g u) with g = 0.25 dXdx^T dXdx
+// per-element min/max over points of sqrt(u . g u) with g = 0.25 dXdx^T dXdx (MonitorCFL_3D_Conserv/_Prim/_Entropy,
+// qfunctions/monitor_cfl.h:9-58)
 __global__ void k_monitor_cfl(int P, int Q, const int32_t *__restrict__ offsets, const double *__restrict__ q, const double *__restrict__ qdata,
-                              hb::PhysConst<double> pc, MonBasis b, double *__restrict__ elem_minmax) {
+                              hb::PhysConst<double> pc, int sv, MonBasis b, double *__restrict__ elem_minmax) {
   extern __shared__ double sm[];
   const int e = blockIdx.x, P3 = P * P * P, Q3 = Q * Q * Q;
   double *sN = sm, *red = sm + 5 * P3;
@@ -329,8 +349,8 @@ __global__ void k_monitor_cfl(int P, int Q, const int32_t *__restrict__ offsets,
     const double *qd = qdata + (int64_t)e * 10 * Q3;
     for (int kk = 0; kk < 9; kk++) X[kk / 3][kk % 3] = qd[(1 + kk) * Q3 + qp];
     hb::St<double> s;
-    double inv_rho, etot, eint;
-    hb::state_from_u(pc, qi, s, inv_rho, etot, eint);
+    hb::SAux<double> aux;
+    mon_state(sv, pc, qi, s, aux);
     for (int a = 0; a < 3; a++)
       for (int c = 0; c < 3; c++) g[a][c] = 0.25 * (X[0][a] * X[0][c] + X[1][a] * X[1][c] + X[2][a] * X[2][c]);
     double ugu = 0;
@@ -572,11 +592,21 @@ static MonBasis mon_basis(const HbElemOp *op) {
 }
 
 // Kinetic-energy monitor sums (not divided by the volume); d_scratch >= 5 * num_elem doubles; synchronises the stream.
+static int state_var_of(const void *ctx184, int *sv) {
+  HbNewtonianContext c;
+  memcpy(&c, ctx184, sizeof c);
+  if (c.state_var != HB_STATEVAR_CONSERVATIVE && c.state_var != HB_STATEVAR_PRIMITIVE && c.state_var != HB_STATEVAR_ENTROPY) return HB_ERROR_UNSUPPORTED;
+  *sv = c.state_var;
+  return HB_SUCCESS;
+}
+
 int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *d_scratch, double sums[5], void *s) {
+  int sv = 0;
+  if (state_var_of(ctx184, &sv)) return HB_ERROR_UNSUPPORTED;
   const int P3 = op->P * op->P * op->P;
   const int nt = 128;
   const size_t sm = sizeof(double) * (5 * P3 + 5 * nt);
-  k_monitor_ke<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), mon_basis(op), d_scratch);
+  k_monitor_ke<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), d_scratch);
   if (rc()) return HB_ERROR_CUDA;
   double *h = (double *)malloc(sizeof(double) * 5 * (size_t)op->num_elem);
   if (!h) return HB_ERROR_NOMEM;
@@ -592,10 +622,12 @@ int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double *q, const
 // CFL monitor: min and max over points of dt * sqrt(u . g u); d_scratch >= 2 * num_elem doubles; synchronises.
 int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double dt, double *d_scratch, double minmax[2],
                    void *s) {
+  int sv = 0;
+  if (state_var_of(ctx184, &sv)) return HB_ERROR_UNSUPPORTED;
   const int P3 = op->P * op->P * op->P;
   const int nt = 128;
   const size_t sm = sizeof(double) * (5 * P3 + 2 * nt);
-  k_monitor_cfl<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), mon_basis(op), d_scratch);
+  k_monitor_cfl<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), d_scratch);
   if (rc()) return HB_ERROR_CUDA;
   double *h = (double *)malloc(sizeof(double) * 2 * (size_t)op->num_elem);
   if (!h) return HB_ERROR_NOMEM;

@@ -215,3 +215,43 @@ def test_bdf2_with_freestream_faces_in_primitive_variables():
     assert rel_l2(prim32 - y0, prim64 - y0) < 1e-6
     cons_as_prim = prob.state_to_q(ctx.gas, finals[(prob.STATEVAR_CONSERVATIVE, 0)], prob.STATEVAR_PRIMITIVE)
     assert rel_l2(prim64 - y0, cons_as_prim - y0) < 1e-2
+
+
+def test_monitors_read_the_state_variable():
+    """MonitorTotalKineticEnergy / MonitorCFL in all three variables (qfunctions/monitor_totalkineticenergy.h:41-51,
+    monitor_cfl.h:48-58).  A uniform-pressure, uniform-temperature shear u = (a + b y, 0, 0) is exactly quadratic in each
+    representation, so at degree 2 every monitor integral is exact: kinetic energy 1/2 rho int (a + b y)^2, strain
+    dissipation -mu b^2 V, vorticity mu b^2 V, divergence terms 0; the CFL extremes are those of |u| on the quadrature grid."""
+    import torch
+    S = importlib.import_module("honee-4aiad_b200.solver")
+    n, P, Q = (2, 3, 2), 3, 4
+    mesh = prob.box_mesh(n, P, hi=(1.0, 2.0, 0.5))
+    basis = prob.tensor_basis(P, Q)
+    ctx = prob.newtonian_context(P - 1, cv=717.5, cp=1004.5, mu=1.8e-2)
+    X = prob.node_coordinates(mesh, basis)
+    a, b, Pr, T = 3.0, 4.0, 1.0e5, 300.0
+    u = np.stack([a + b * X[1], 0 * X[1], 0 * X[1]])
+    q_cons = prob.conservative_from_primitive(ctx.gas, Pr + 0 * X[1], u, T + 0 * X[1]).T.reshape(-1)
+    rho = Pr / ((ctx.gas.cp - ctx.gas.cv) * T)
+    V = 1.0 * 2.0 * 0.5
+    ke = 0.5 * rho * 1.0 * 0.5 * ((a + 2 * b) ** 3 - a ** 3) / (3 * b)
+    expect = np.array([ke, -ctx.gas.mu * b * b * V, 0.0, 0.0, ctx.gas.mu * b * b * V])
+    op = K.ElemOp(mesh, basis)
+    x = torch.from_numpy(np.ascontiguousarray(mesh.x_elem)).to(_dev())
+    qdata = torch.zeros(mesh.num_elem * 10 * Q ** 3, dtype=torch.float64, device=_dev())
+    op.setup_qdata(x, qdata)
+    scratch = torch.zeros(5 * mesh.num_elem, dtype=torch.float64, device=_dev())
+    cfl = {}
+    for sv in (prob.STATEVAR_CONSERVATIVE, prob.STATEVAR_PRIMITIVE, prob.STATEVAR_ENTROPY):
+        ctx.state_var = sv
+        cb = prob.context_bytes(ctx)
+        tq = torch.from_numpy(prob.state_to_q(ctx.gas, q_cons, sv)).to(_dev())
+        sums = S.monitor_ke(op, cb, tq, qdata, scratch)
+        np.testing.assert_allclose(sums[[0, 1, 4]], expect[[0, 1, 4]], rtol=1e-11)
+        assert abs(sums[2]) < 1e-10 * abs(expect[1]) and abs(sums[3]) < 1e-10 * Pr * V
+        cfl[sv] = S.monitor_cfl(op, cb, tq, qdata, 1e-3, scratch)
+    for sv in (prob.STATEVAR_PRIMITIVE, prob.STATEVAR_ENTROPY):
+        np.testing.assert_allclose(cfl[sv], cfl[prob.STATEVAR_CONSERVATIVE], rtol=1e-12)
+    ctx.state_var = 9
+    with pytest.raises(K.HbError):
+        S.monitor_ke(op, prob.context_bytes(ctx), tq, qdata, scratch)
