@@ -75,19 +75,6 @@ __device__ __forceinline__ void exterior_state(const Exterior &x, hb::St<double>
   s.T_ = x.Y[4];
 }
 
-// StateFromQ / StateFromQ_fwd for the face's state variable (a run-time switch: boundary work is O(E^(2/3)))
-__device__ __forceinline__ void face_state(int sv, const hb::PhysConst<double> &pc, const double q[5], hb::St<double> &s, hb::SAux<double> &a) {
-  if (sv == HB_STATEVAR_PRIMITIVE) hb::state_from_q<HB_STATEVAR_PRIMITIVE>(pc, q, s, a);
-  else if (sv == HB_STATEVAR_ENTROPY) hb::state_from_q<HB_STATEVAR_ENTROPY>(pc, q, s, a);
-  else hb::state_from_q<HB_STATEVAR_CONSERVATIVE>(pc, q, s, a);
-}
-__device__ __forceinline__ void face_state_fwd(int sv, const hb::PhysConst<double> &pc, const hb::St<double> &s, const hb::SAux<double> &a,
-                                               const double dq[5], hb::St<double> &ds) {
-  if (sv == HB_STATEVAR_PRIMITIVE) hb::state_from_q_fwd<HB_STATEVAR_PRIMITIVE>(pc, s, a, dq, ds);
-  else if (sv == HB_STATEVAR_ENTROPY) hb::state_from_q_fwd<HB_STATEVAR_ENTROPY>(pc, s, a, dq, ds);
-  else hb::state_from_q_fwd<HB_STATEVAR_CONSERVATIVE>(pc, s, a, dq, ds);
-}
-
 // v += wdetJb * F_riemann(q, S_infty, n) integrated against the face basis; jac_sur [F][5][Q^2] = q at the points
 // (Freestream, bc_freestream.h:14-48)
 __global__ void k_freestream(int P, int Q, const int32_t *__restrict__ offsets, const int32_t *__restrict__ faces, FaceBasis b,
@@ -106,7 +93,7 @@ __global__ void k_freestream(int P, int Q, const int32_t *__restrict__ offsets, 
     }
     hb::St<double> s, sx;
     hb::SAux<double> aux;
-    face_state(ex.sv, pc, U, s, aux);
+    hb::state_from_q_rt(ex.sv, pc, U, s, aux);
     exterior_state(ex, sx);
     const double *qf = qd + (int64_t)f * 10 * Q2;
     const double wdetJb = qf[t], n[3] = {qf[Q2 + t], qf[2 * Q2 + t], qf[3 * Q2 + t]};
@@ -146,8 +133,8 @@ __global__ void k_freestream_jac(int P, int Q, const int32_t *__restrict__ offse
     for (int c = 0; c < 5; c++) U[c] = jac[((int64_t)f * 5 + c) * Q2 + t];
     hb::St<double> s, ds, sx, dsx;
     hb::SAux<double> aux;
-    face_state(ex.sv, pc, U, s, aux);
-    face_state_fwd(ex.sv, pc, s, aux, dU, ds);
+    hb::state_from_q_rt(ex.sv, pc, U, s, aux);
+    hb::state_from_q_fwd_rt(ex.sv, pc, s, aux, dU, ds);
     exterior_state(ex, sx);
     memset(&dsx, 0, sizeof dsx);
     const double *qf = qd + (int64_t)f * 10 * Q2;
@@ -181,7 +168,7 @@ __global__ void k_freestream_diag(int P, int Q, const int32_t *__restrict__ offs
     for (int c = 0; c < 5; c++) U[c] = jac[((int64_t)f * 5 + c) * Q2 + t];
     hb::St<double> s, sx, dsx;
     hb::SAux<double> aux;
-    face_state(ex.sv, pc, U, s, aux);
+    hb::state_from_q_rt(ex.sv, pc, U, s, aux);
     exterior_state(ex, sx);
     memset(&dsx, 0, sizeof dsx);
     const double *qf = qd + (int64_t)f * 10 * Q2;
@@ -191,7 +178,7 @@ __global__ void k_freestream_diag(int P, int Q, const int32_t *__restrict__ offs
       double dU[5] = {0, 0, 0, 0, 0}, dF[5];
       dU[c] = 1.0;
       hb::St<double> ds;
-      face_state_fwd(ex.sv, pc, s, aux, dU, ds);
+      hb::state_from_q_fwd_rt(ex.sv, pc, s, aux, dU, ds);
       if (ex.hllc) hb::riemann::hllc_flux_fwd(ex.gamma, ex.cv, s, ds, sx, dsx, n, dF);
       else hb::riemann::hll_flux_fwd(ex.gamma, ex.cv, s, ds, sx, dsx, n, dF);
       if (FULL) {

@@ -165,10 +165,10 @@ __global__ void k_filter_diag(int P, int Q, const int32_t *__restrict__ offsets,
   }
 }
 
-// b += int phi f(q) with f = (P, u, T, uu_xx, uu_yy, uu_zz, uu_yz, uu_xz, uu_xy) of the conservative state q, b
-// node-interleaved [node][11] (DifferentialFilter_RHS_Conserv)
+// b += int phi f(q) with f = (P, u, T, uu_xx, uu_yy, uu_zz, uu_yz, uu_xz, uu_xy) of the state q in the variable sv, b
+// node-interleaved [node][11] (DifferentialFilter_RHS_Conserv / _Prim / _Entropy, qfunctions/differential_filter.h:29-68)
 __global__ void k_filter_rhs(int P, int Q, const int32_t *__restrict__ offsets, const int32_t *__restrict__ elems, const double *__restrict__ qdata,
-                             FBasis b, hb::PhysConst<double> pc, const double *__restrict__ q, double *__restrict__ rhs) {
+                             FBasis b, hb::PhysConst<double> pc, int sv, const double *__restrict__ q, double *__restrict__ rhs) {
   __shared__ double sN[5][kMaxP3], sF[11][kMaxQ3];
   const int e = elems[blockIdx.x], P3 = P * P * P, Q3 = Q * Q * Q, t = threadIdx.x;
   for (int p = t; p < 5 * P3; p += blockDim.x) sN[p % 5][p / 5] = q[offsets[(int64_t)e * P3 + p / 5] + p % 5];
@@ -181,8 +181,8 @@ __global__ void k_filter_rhs(int P, int Q, const int32_t *__restrict__ offsets, 
       eval_pt(sN[c], P, b, i, j, k, U[c], g);
     }
     hb::St<double> s;
-    double inv_rho, etot, eint;
-    hb::state_from_u(pc, U, s, inv_rho, etot, eint);
+    hb::SAux<double> aux;
+    hb::state_from_q_rt(sv, pc, U, s, aux);
     const double w = qdata[(int64_t)e * 10 * Q3 + t];
     const double f[11] = {s.P, s.u[0], s.u[1], s.u[2], s.T_, s.u[0] * s.u[0], s.u[1] * s.u[1], s.u[2] * s.u[2], s.u[1] * s.u[2], s.u[0] * s.u[2], s.u[0] * s.u[1]};
     for (int c = 0; c < 11; c++) sF[c][t] = w * f[c];
@@ -243,15 +243,27 @@ __global__ void k_sgs_pairs(int P, int Q, const int32_t *__restrict__ offsets, c
 }
 
 // conservative state (rho, rho u, E) of filtered fields (P, u, T, ...) [node][11], rho = P / (R T)
-__global__ void k_filtered_state(const double *__restrict__ f, int64_t nodes, double cv, double R, double *__restrict__ q) {
+// the state of the filtered primitive fields (P, u, T) in the variable sv: conservative (StateConservativeFromPrimitive,
+// newtonian_state.h:159-168), primitive as is, entropy (StateEntropyFromPrimitive, :91-103)
+__global__ void k_filtered_state(const double *__restrict__ f, int64_t nodes, double cv, double R, int sv, double *__restrict__ q) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
     const double *g = f + i * 11;
     const double rho = g[0] / (R * g[4]);
-    q[i * 5 + 0] = rho;
-    q[i * 5 + 1] = rho * g[1];
-    q[i * 5 + 2] = rho * g[2];
-    q[i * 5 + 3] = rho * g[3];
-    q[i * 5 + 4] = rho * (cv * g[4] + 0.5 * (g[1] * g[1] + g[2] * g[2] + g[3] * g[3]));
+    const double ke = 0.5 * (g[1] * g[1] + g[2] * g[2] + g[3] * g[3]);
+    if (sv == HB_STATEVAR_PRIMITIVE) {
+      for (int c = 0; c < 5; c++) q[i * 5 + c] = g[c];
+    } else if (sv == HB_STATEVAR_ENTROPY) {
+      const double gamma = (cv + R) / cv, ent = log(g[0]) - gamma * log(rho), rho_p = rho / g[0];
+      q[i * 5 + 0] = (gamma - ent) / (gamma - 1) - rho_p * ke;
+      for (int c = 1; c < 4; c++) q[i * 5 + c] = rho_p * g[c];
+      q[i * 5 + 4] = -rho_p;
+    } else {
+      q[i * 5 + 0] = rho;
+      q[i * 5 + 1] = rho * g[1];
+      q[i * 5 + 2] = rho * g[2];
+      q[i * 5 + 3] = rho * g[3];
+      q[i * 5 + 4] = rho * (cv * g[4] + ke);
+    }
   }
 }
 
@@ -320,6 +332,7 @@ int hb_filter_rhs(const HbElemOp *op, const void *ctx184, const double *qdata, c
   if (cudaMemsetAsync(rhs, 0, sizeof(double) * (op->l_size / 5) * 11, s) != cudaSuccess) return HB_ERROR_CUDA;
   HbNewtonianContext c;
   memcpy(&c, ctx184, sizeof c);
+  if (c.state_var != HB_STATEVAR_CONSERVATIVE && c.state_var != HB_STATEVAR_PRIMITIVE && c.state_var != HB_STATEVAR_ENTROPY) return HB_ERROR_UNSUPPORTED;
   hb::PhysConst<double> pc;
   memset(&pc, 0, sizeof pc);
   pc.cv = c.gas.cv;
@@ -329,7 +342,7 @@ int hb_filter_rhs(const HbElemOp *op, const void *ctx184, const double *qdata, c
   const FBasis b = fbasis(op);
   for (int k = 0; k < op->num_colors; k++) {
     const int n = op->h_color_ptr[k + 1] - op->h_color_ptr[k];
-    if (n) k_filter_rhs<<<n, nthreads(op), 0, s>>>(op->P, op->Q, op->d_offsets, op->d_color_elem + op->h_color_ptr[k], qdata, b, pc, q, rhs);
+    if (n) k_filter_rhs<<<n, nthreads(op), 0, s>>>(op->P, op->Q, op->d_offsets, op->d_color_elem + op->h_color_ptr[k], qdata, b, pc, c.state_var, q, rhs);
   }
   return rc();
 }
@@ -344,7 +357,8 @@ int hb_filtered_state(const double *filtered, int64_t nodes, const void *ctx184,
   if (!filtered || !ctx184 || !q || nodes < 0) return HB_ERROR_INVALID;
   HbNewtonianContext c;
   memcpy(&c, ctx184, sizeof c);
-  if (nodes) k_filtered_state<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(filtered, nodes, c.gas.cv, c.gas.cp - c.gas.cv, q);
+  if (c.state_var != HB_STATEVAR_CONSERVATIVE && c.state_var != HB_STATEVAR_PRIMITIVE && c.state_var != HB_STATEVAR_ENTROPY) return HB_ERROR_UNSUPPORTED;
+  if (nodes) k_filtered_state<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(filtered, nodes, c.gas.cv, c.gas.cp - c.gas.cv, c.state_var, q);
   return rc();
 }
 

@@ -265,21 +265,13 @@ __device__ void eval_point(const double *sN, int P, int Q, const MonBasis &b, in
       }
 }
 
-// StateFromQ / StateFromQ_fwd for the monitors' state variable (run-time switch: the monitors are not on the hot path)
-__device__ __forceinline__ void mon_state(int sv, const hb::PhysConst<double> &pc, const double q[5], hb::St<double> &s, hb::SAux<double> &a) {
-  if (sv == HB_STATEVAR_PRIMITIVE) hb::state_from_q<HB_STATEVAR_PRIMITIVE>(pc, q, s, a);
-  else if (sv == HB_STATEVAR_ENTROPY) hb::state_from_q<HB_STATEVAR_ENTROPY>(pc, q, s, a);
-  else hb::state_from_q<HB_STATEVAR_CONSERVATIVE>(pc, q, s, a);
-}
 // physical gradient of the state (StatePhysicalGradientFromReference, newtonian_state.h:581-593) in the state variable sv
 __device__ __forceinline__ void mon_gradient(int sv, const hb::PhysConst<double> &pc, const hb::St<double> &s, const hb::SAux<double> &a,
                                              const double gref[3][5], const double X[3][3], hb::St<double> gs[3]) {
   for (int j = 0; j < 3; j++) {
     double dq[5];
     for (int c = 0; c < 5; c++) dq[c] = gref[0][c] * X[0][j] + gref[1][c] * X[1][j] + gref[2][c] * X[2][j];
-    if (sv == HB_STATEVAR_PRIMITIVE) hb::state_from_q_fwd<HB_STATEVAR_PRIMITIVE>(pc, s, a, dq, gs[j]);
-    else if (sv == HB_STATEVAR_ENTROPY) hb::state_from_q_fwd<HB_STATEVAR_ENTROPY>(pc, s, a, dq, gs[j]);
-    else hb::state_from_q_fwd<HB_STATEVAR_CONSERVATIVE>(pc, s, a, dq, gs[j]);
+    hb::state_from_q_fwd_rt(sv, pc, s, a, dq, gs[j]);
   }
 }
 
@@ -301,7 +293,7 @@ __global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, 
     for (int kk = 0; kk < 9; kk++) X[kk / 3][kk % 3] = qd[(1 + kk) * Q3 + qp];
     hb::St<double> s;
     hb::SAux<double> aux;
-    mon_state(sv, pc, qi, s, aux);
+    hb::state_from_q_rt(sv, pc, qi, s, aux);
     hb::St<double> gs[3];
     mon_gradient(sv, pc, s, aux, gref, X, gs);
     double e6[6], S[3][3];
@@ -350,7 +342,7 @@ __global__ void k_monitor_cfl(int P, int Q, const int32_t *__restrict__ offsets,
     for (int kk = 0; kk < 9; kk++) X[kk / 3][kk % 3] = qd[(1 + kk) * Q3 + qp];
     hb::St<double> s;
     hb::SAux<double> aux;
-    mon_state(sv, pc, qi, s, aux);
+    hb::state_from_q_rt(sv, pc, qi, s, aux);
     for (int a = 0; a < 3; a++)
       for (int c = 0; c < 3; c++) g[a][c] = 0.25 * (X[0][a] * X[0][c] + X[1][a] * X[1][c] + X[2][a] * X[2][c]);
     double ugu = 0;

@@ -166,6 +166,20 @@ __device__ __forceinline__ void state_from_q_fwd(const PhysConst<T> &c, const St
   }
 }
 
+// The same with the state variable chosen at run time, for kernels off the hot path (faces, monitors, filter).
+template <typename T>
+__device__ __forceinline__ void state_from_q_rt(int sv, const PhysConst<T> &c, const T q[5], St<T> &s, SAux<T> &a) {
+  if (sv == HB_STATEVAR_PRIMITIVE) state_from_q<HB_STATEVAR_PRIMITIVE>(c, q, s, a);
+  else if (sv == HB_STATEVAR_ENTROPY) state_from_q<HB_STATEVAR_ENTROPY>(c, q, s, a);
+  else state_from_q<HB_STATEVAR_CONSERVATIVE>(c, q, s, a);
+}
+template <typename T>
+__device__ __forceinline__ void state_from_q_fwd_rt(int sv, const PhysConst<T> &c, const St<T> &s, const SAux<T> &a, const T dq[5], St<T> &ds) {
+  if (sv == HB_STATEVAR_PRIMITIVE) state_from_q_fwd<HB_STATEVAR_PRIMITIVE>(c, s, a, dq, ds);
+  else if (sv == HB_STATEVAR_ENTROPY) state_from_q_fwd<HB_STATEVAR_ENTROPY>(c, s, a, dq, ds);
+  else state_from_q_fwd<HB_STATEVAR_CONSERVATIVE>(c, s, a, dq, ds);
+}
+
 // Row i of the linearised inviscid flux (newtonian_state.h:433-442): dF_i for components 0..4.
 template <typename T>
 __device__ __forceinline__ void dflux_row(const St<T> &s, const St<T> &ds, int i, T r[5]) {

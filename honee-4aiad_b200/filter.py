@@ -58,7 +58,7 @@ class DifferentialFilter:
         return its.value, rel.value
 
     def filter_state(self, q, rtol=1e-10, max_it=500):
-        """Filtered (P, u, T, u_i u_j) [node][11] of the conservative state q, with the CG statistics."""
+        """Filtered (P, u, T, u_i u_j) [node][11] of the state q (in the context's state variable), with the CG statistics."""
         b = self.torch.empty(self.nodes * 11, dtype=self.torch.float64, device=self.device)
         x = self.torch.empty_like(b)
         self.rhs(q, b)
@@ -66,7 +66,7 @@ class DifferentialFilter:
         return x, its, rel
 
     def conservative(self, filtered, q):
-        """Conservative state [node][5] of filtered fields (to run the monitors on the filtered solution)."""
+        """State [node][5] of filtered fields in the context's state variable (to run the monitors on the filtered solution)."""
         _chk(_load().hb_filtered_state(_addr(filtered), C.c_int64(self.nodes), self.ctx, _addr(q), _stream(self.stream)), "hb_filtered_state")
 
     def training_pairs(self, filtered, width_scale, X, Y):

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import numpy as np
 
+import face_oracle as FaceO
 import sgs_oracle as SO
 
 
@@ -74,8 +75,8 @@ def apply(mesh, basis, qdata, x, nc, grid_based=False, width_scaling=(1, 1, 1), 
     return y.reshape(-1)
 
 
-def rhs(mesh, basis, qdata, q, gas):
-    """[node][11] = int phi (P, u, T, u_i u_j) of the conservative state q."""
+def rhs(mesh, basis, qdata, q, gas, sv=0):
+    """[node][11] = int phi (P, u, T, u_i u_j) of the state q, given in the state variable sv (0 conservative)."""
     P, Q = basis.P, basis.Q
     Q3 = Q ** 3
     Bq, _ = tensor_ops(basis.interp1d, basis.grad1d, P, Q)
@@ -83,10 +84,16 @@ def rhs(mesh, basis, qdata, q, gas):
     qe = np.asarray(q).reshape(-1, 5)[nodes]
     U = np.einsum("qp,epc->eqc", Bq, qe)                          # [E][Q3][5]
     R, cv = gas.cp - gas.cv, gas.cv
-    rho, m, E = U[..., 0], U[..., 1:4], U[..., 4]
-    u = m / rho[..., None]
-    T = (E / rho - 0.5 * (u ** 2).sum(-1)) / cv
-    Pr = rho * R * T
+    if sv == 0:
+        rho, m, E = U[..., 0], U[..., 1:4], U[..., 4]
+        u = m / rho[..., None]
+        T = (E / rho - 0.5 * (u ** 2).sum(-1)) / cv
+        Pr = rho * R * T
+    else:  # StateFromQ (newtonian_state.h:393-407) at every point
+        s = FaceO.state_from_q(U.reshape(-1, 5).T, sv, cv, gas.cp)
+        shp = U.shape[:2]
+        Pr, T = s.P.reshape(shp), s.T.reshape(shp)
+        u = np.moveaxis(s.u, 0, -1).reshape(shp + (3,))
     f = np.stack([Pr, u[..., 0], u[..., 1], u[..., 2], T, u[..., 0] ** 2, u[..., 1] ** 2, u[..., 2] ** 2, u[..., 1] * u[..., 2],
                   u[..., 0] * u[..., 2], u[..., 0] * u[..., 1]], -1)
     w = np.asarray(qdata).reshape(mesh.num_elem, 10, Q3)[:, 0, :]

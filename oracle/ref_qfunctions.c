@@ -80,6 +80,8 @@ EXPORT int ref_ComputeSgsDDNodal_Conserv(void *c, CeedInt Q, In in, Out out) { r
 EXPORT int ref_AnisotropyTensorCollocate(void *c, CeedInt Q, In in, Out out) { return AnisotropyTensorCollocate(c, Q, in, out); }
 EXPORT int ref_IFunction_NodalSgs_Conserv(void *c, CeedInt Q, In in, Out out) { return IFunction_NodalSgs_Conserv(c, Q, in, out); }
 EXPORT int ref_DifferentialFilter_RHS_Conserv(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_RHS_Conserv(c, Q, in, out); }
+EXPORT int ref_DifferentialFilter_RHS_Prim(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_RHS_Prim(c, Q, in, out); }
+EXPORT int ref_DifferentialFilter_RHS_Entropy(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_RHS_Entropy(c, Q, in, out); }
 EXPORT int ref_DifferentialFilter_LHS_11(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_LHS_11(c, Q, in, out); }
 EXPORT int ref_DifferentialFilter_LHS_1(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_LHS_1(c, Q, in, out); }
 /* ComputeSgsDDInputs / ComputeSgsDDOutputs / DataDrivenInference on single points */

@@ -16,6 +16,7 @@ import pytest
 from helpers import O, case, prob, rel_l2
 
 import face_oracle as FO  # noqa: E402
+import filter_oracle as FIL  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -255,3 +256,29 @@ def test_monitors_read_the_state_variable():
     ctx.state_var = 9
     with pytest.raises(K.HbError):
         S.monitor_ke(op, prob.context_bytes(ctx), tq, qdata, scratch)
+
+
+@pytest.mark.parametrize("sv", [prob.STATEVAR_PRIMITIVE, prob.STATEVAR_ENTROPY])
+def test_filter_rhs_and_filtered_state_in_other_variables(sv):
+    """The differential filter's right-hand side from a primitive / entropy state (DifferentialFilter_RHS_Prim/_Entropy)
+    against the oracle, and the state rebuilt from filtered (P, u, T) fields in that variable."""
+    import torch
+    F = importlib.import_module("honee-4aiad_b200.filter")
+    mesh, basis, ctx, q, _ = sv_case(sv, n=(3, 3, 2), P=3, Q=4, state="modes")
+    op = K.ElemOp(mesh, basis)
+    x = torch.from_numpy(np.ascontiguousarray(mesh.x_elem)).to(_dev())
+    qdata = torch.zeros(mesh.num_elem * 10 * basis.Q ** 3, dtype=torch.float64, device=_dev())
+    op.setup_qdata(x, qdata)
+    filt = F.DifferentialFilter(op, qdata, prob.context_bytes(ctx), grid_based_width=True, width_scaling=(1.0, 1.0, 1.0), kernel_scaling=0.1)
+    b = torch.empty(mesh.num_nodes * 11, dtype=torch.float64, device=_dev())
+    filt.rhs(torch.from_numpy(q).to(_dev()), b)
+    assert rel_l2(b.cpu().numpy(), FIL.rhs(mesh, basis, qdata.cpu().numpy(), q, ctx.gas, sv=sv)) < 1e-12
+    rng = np.random.default_rng(9)
+    n = mesh.num_nodes
+    Pn, Tn, un = 101325 * (1 + 0.01 * rng.uniform(-1, 1, n)), 288 * (1 + 0.01 * rng.uniform(-1, 1, n)), rng.uniform(-20, 20, (3, n))
+    fields = np.zeros((n, 11))
+    fields[:, 0], fields[:, 1:4], fields[:, 4] = Pn, un.T, Tn
+    out = torch.empty(5 * n, dtype=torch.float64, device=_dev())
+    filt.conservative(torch.from_numpy(fields.reshape(-1)).to(_dev()), out)
+    expect = prob.state_to_q(ctx.gas, prob.conservative_from_primitive(ctx.gas, Pn, un, Tn).T.reshape(-1), sv)
+    assert rel_l2(out.cpu().numpy(), expect) < 1e-14

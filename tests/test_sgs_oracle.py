@@ -167,3 +167,32 @@ def test_filter_pointwise_forms_match_reference(grid_based):
     w = qdata[0]
     np.testing.assert_allclose(v0, w * np.stack([P, u[0], u[1], u[2], T]), rtol=1e-12)
     np.testing.assert_allclose(v1, w * np.stack([u[0] ** 2, u[1] ** 2, u[2] ** 2, u[1] * u[2], u[0] * u[2], u[0] * u[1]]), rtol=1e-11)
+
+
+@pytest.mark.parametrize("sv", [1, 2])
+def test_filter_rhs_in_other_state_variables_matches_reference(sv):
+    """DifferentialFilter_RHS_Prim / _Entropy (qfunctions/differential_filter.h:62-68): the same integrand w (P, u, T, u_i u_j)
+    from the state given in primitive or entropy variables."""
+    import oracle as O
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    R = O.ref()
+    if R is None:
+        pytest.skip("oracle/_ref not built")
+    ctx = prob.newtonian_context(2)
+    ctx.state_var = sv
+    cb = _filter_ctx(R, prob.context_bytes(ctx), False, (1.0, 1.0, 1.0), 0.1)
+    rng = np.random.default_rng(8)
+    n = 64
+    qdata = np.zeros((10, n))
+    qdata[0] = rng.uniform(1e-4, 1e-2, n)
+    P = 101325 * (1 + 0.01 * rng.uniform(-1, 1, n))
+    T = 288 * (1 + 0.01 * rng.uniform(-1, 1, n))
+    u = rng.uniform(-20, 20, (3, n))
+    qc = prob.conservative_from_primitive(ctx.gas, P, u, T)
+    qv = np.ascontiguousarray(prob.state_to_q(ctx.gas, qc.T.reshape(-1), sv).reshape(-1, 5).T)
+    v0, v1 = np.zeros((5, n)), np.zeros((6, n))
+    name = ("Conserv", "Prim", "Entropy")[sv]
+    O.call_qf(getattr(R, f"ref_DifferentialFilter_RHS_{name}"), cb, n, [qv, np.ascontiguousarray(qdata)], [v0, v1])
+    w = qdata[0]
+    np.testing.assert_allclose(v0, w * np.stack([P, u[0], u[1], u[2], T]), rtol=1e-11)
+    np.testing.assert_allclose(v1, w * np.stack([u[0] ** 2, u[1] ** 2, u[2] ** 2, u[1] * u[2], u[0] * u[2], u[0] * u[1]]), rtol=1e-10)
