@@ -490,14 +490,16 @@ struct SgsArg<2> {
   int clamp, no_backscatter;
 };
 
-template <int SGS>
+template <int SGS, int SV = HB_STATEVAR_CONSERVATIVE>
 __device__ __forceinline__ void sgs_add(const PhysConst<double> &c, const double q[5], const double gref[3][5], double wdetJ, const double X[3][3],
                                         const SgsArg<SGS> &sg, double gv[3][5]) {
   St<double> st;
-  double inv_rho, etot, eint;
-  state_from_u(c, q, st, inv_rho, etot, eint);
+  SAux<double> aux;
+  state_from_q<SV>(c, q, st, aux);
+  const double inv_rho = aux.inv_rho;
   St<double> gs[3];
-  physical_gradient(c, st, inv_rho, etot, eint, gref, X, gs);
+#pragma unroll
+  for (int j = 0; j < 3; j++) gradient_dir<SV>(c, st, aux, gref, X, j, gs[j]);
   double G[3][3];
 #pragma unroll
   for (int i = 0; i < 3; i++)
@@ -656,7 +658,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
         }
       };
       ifunction_point_stream<double, SV>(a.pc, qi, gref, qd, wdetJ, X, x0, v, gv, emit);
-      if constexpr (SGS > 0) sgs_add<SGS>(a.pc, qi, gref, wdetJ, X, sg, gv);
+      if constexpr (SGS > 0) sgs_add<SGS, SV>(a.pc, qi, gref, wdetJ, X, sg, gv);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
         sU[c * Q3 + q] = v[c];
@@ -1781,6 +1783,21 @@ static int fill_sgs(const HbMlpDesc *d, const float *w, SgsArg<SGS> &sg) {
   return HB_SUCCESS;
 }
 
+template <int SGS, int SV>
+static int ifunction_sgs_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, const SgsArg<SGS> &sg, cudaStream_t s) {
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return launch_ifunction_v<PP, QQ, true, SGS, SV>(op, ctx, io, s, sg);
+  HB_SGS_PQ_LIST(HB_CASE)
+#undef HB_CASE
+  return HB_ERROR_UNSUPPORTED;
+}
+template <int SGS>
+static int ifunction_sgs_sv(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, const SgsArg<SGS> &sg, cudaStream_t s) {
+  if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return ifunction_sgs_pq<SGS, HB_STATEVAR_PRIMITIVE>(op, ctx, io, sg, s);
+  if (ctx.state_var == HB_STATEVAR_ENTROPY) return ifunction_sgs_pq<SGS, HB_STATEVAR_ENTROPY>(op, ctx, io, sg, s);
+  return ifunction_sgs_pq<SGS, HB_STATEVAR_CONSERVATIVE>(op, ctx, io, sg, s);
+}
+
 extern "C" int hb_ifunction_apply_sgs(const HbElemOp *op, const void *ctx184, const HbIFunctionIO *io, const HbMlpDesc *d, const float *h_weights,
                                       void *stream) {
   int err = check_op(op);
@@ -1788,26 +1805,20 @@ extern "C" int hb_ifunction_apply_sgs(const HbElemOp *op, const void *ctx184, co
   if (!d || !h_weights || d->hidden1 != 20 || (d->hidden2 != 0 && d->hidden2 != 20)) return HB_ERROR_INVALID;
   HbNewtonianContext ctx;
   memcpy(&ctx, ctx184, sizeof ctx);
-  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE || ctx.divFdiff_method != HB_DIV_DIFF_FLUX_PROJ_NONE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.divFdiff_method != HB_DIV_DIFF_FLUX_PROJ_NONE) return HB_ERROR_UNSUPPORTED;
+  if (ctx.state_var != HB_STATEVAR_CONSERVATIVE && ctx.state_var != HB_STATEVAR_PRIMITIVE && ctx.state_var != HB_STATEVAR_ENTROPY)
+    return HB_ERROR_UNSUPPORTED;
   if (ctx.idl_enable && !op->d_x_elem) return HB_ERROR_INVALID;
   cudaStream_t s = (cudaStream_t)stream;
   if (!io->add && cudaMemsetAsync(io->v, 0, sizeof(double) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
   if (d->hidden2 == 20) {
     SgsArg<2> sg;
     if ((err = fill_sgs<2>(d, h_weights, sg))) return err;
-#define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_ifunction_v<PP, QQ, true, 2>(op, ctx, io, s, sg);
-    HB_SGS_PQ_LIST(HB_CASE)
-#undef HB_CASE
-  } else {
-    SgsArg<1> sg;
-    if ((err = fill_sgs<1>(d, h_weights, sg))) return err;
-#define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_ifunction_v<PP, QQ, true, 1>(op, ctx, io, s, sg);
-    HB_SGS_PQ_LIST(HB_CASE)
-#undef HB_CASE
+    return ifunction_sgs_sv<2>(op, ctx, io, sg, s);
   }
-  return HB_ERROR_UNSUPPORTED;
+  SgsArg<1> sg;
+  if ((err = fill_sgs<1>(d, h_weights, sg))) return err;
+  return ifunction_sgs_sv<1>(op, ctx, io, sg, s);
 }
 
 template <typename T, int SV>

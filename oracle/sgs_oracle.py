@@ -187,10 +187,12 @@ def reference_layout_to_flat(b1, b2, w1_file, w2_file):
     return np.concatenate([W1.reshape(-1), np.asarray(b1)[:20], W2.reshape(-1), np.asarray(b2)[:6]])
 
 
-def residual_contribution(mesh, basis, qdata, q, gas, params, h1, h2, bounds, alpha=0.0, float32_net=True):
+def residual_contribution(mesh, basis, qdata, q, gas, params, h1, h2, bounds, alpha=0.0, float32_net=True, sv=0):
     """Nodal residual contribution of the closure's flux (IFunction_NodalSgs, sgs_dd_model.h:219-241, with the stress of
     ComputeSgsDD_Fused evaluated at the quadrature points).  float32_net rounds the network's inputs, weights and
-    outputs to float32 the way the CUDA kernel evaluates it (FP64 everywhere else)."""
+    outputs to float32 the way the CUDA kernel evaluates it (FP64 everywhere else).  q in the state variable sv
+    (StateFromQ and its tangent give the density, velocity and velocity gradient at each point)."""
+    import face_oracle as FaceO
     import filter_oracle as FO
     P, Q = basis.P, basis.Q
     Q3 = Q ** 3
@@ -206,9 +208,14 @@ def residual_contribution(mesh, basis, qdata, q, gas, params, h1, h2, bounds, al
         gv = np.zeros((Q3, 3, 5))
         for k in range(Q3):
             X = qd[e, 1:, k].reshape(3, 3)
-            rho, m = U[e, k, 0], U[e, k, 1:4]
-            u = m / rho
-            du_ref = (Gr[e, k][:, 1:4] - np.outer(Gr[e, k][:, 0], u)) / rho   # [dir][comp] d u / d xi
+            if sv == 0:
+                rho, m = U[e, k, 0], U[e, k, 1:4]
+                u = m / rho
+                du_ref = (Gr[e, k][:, 1:4] - np.outer(Gr[e, k][:, 0], u)) / rho   # [dir][comp] d u / d xi
+            else:
+                st = FaceO.state_from_q(U[e, k][:, None], sv, gas.cv, gas.cp)
+                rho, u = st.rho[0], st.u[:, 0]
+                du_ref = np.stack([FaceO.state_from_q_fwd(st, Gr[e, k][r][:, None], sv, gas.cv, gas.cp).u[:, 0] for r in range(3)])
             G = du_ref.T @ X
             kmA, delta = anisotropy(X)
             x, E, g = inputs(G, kmA, delta, gas.mu / rho)

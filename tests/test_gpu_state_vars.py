@@ -282,3 +282,42 @@ def test_filter_rhs_and_filtered_state_in_other_variables(sv):
     filt.conservative(torch.from_numpy(fields.reshape(-1)).to(_dev()), out)
     expect = prob.state_to_q(ctx.gas, prob.conservative_from_primitive(ctx.gas, Pn, un, Tn).T.reshape(-1), sv)
     assert rel_l2(out.cpu().numpy(), expect) < 1e-14
+
+
+@pytest.mark.parametrize("sv", [prob.STATEVAR_PRIMITIVE, prob.STATEVAR_ENTROPY])
+def test_fused_closure_in_other_state_variables(sv):
+    """The learned closure fused into the residual with the state in primitive / entropy variables (the reference's
+    data-driven SGS runs use -state_var primitive): its residual contribution against the oracle's, which rebuilds
+    density, velocity and velocity gradient through StateFromQ and its tangent; 1e-5 (FP32 network)."""
+    import math
+    import torch
+    SG = importlib.import_module("honee-4aiad_b200.sgs")
+    import sgs_oracle as SO
+    import os
+    L = 2 * math.pi
+    mesh = prob.box_mesh((3, 3, 3), 3, periodic=(1, 1, 1), hi=(L, L, L))
+    basis = prob.tensor_basis(3, 4)
+    tg = prob.taylor_green_context(2)
+    tg.u[0], tg.u[1], tg.u[2] = 0.2, 0.1, 0.3
+    q = prob.taylor_green_state(mesh, basis, tg)
+    ctx = tg.newt_ctx
+    ctx.dt, ctx.ijacobian_time_shift = 0.01, 150.0
+    ctx.state_var = sv
+    qv = prob.state_to_q(ctx.gas, q, sv)
+    cb = prob.context_bytes(ctx)
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "sgs_points.npz"))
+    d, w = SG.desc(20, 0, 0.0, g["bounds"]), g["weights"].astype(np.float32)
+    op = K.ElemOp(mesh, basis)
+    x = torch.from_numpy(np.ascontiguousarray(mesh.x_elem)).to(_dev())
+    qdata = torch.zeros(mesh.num_elem * 10 * basis.Q ** 3, dtype=torch.float64, device=_dev())
+    op.setup_qdata(x, qdata)
+    tq = torch.from_numpy(qv).to(_dev())
+    tqd = torch.zeros_like(tq)
+    v0, v1 = torch.empty_like(tq), torch.empty_like(tq)
+    op.ifunction(cb, tq, tqd, qdata, v0)
+    op.ifunction_sgs(cb, tq, tqd, qdata, v1, d, w)
+    torch.cuda.synchronize()
+    got = (v1 - v0).cpu().numpy()
+    ref = SO.residual_contribution(mesh, basis, qdata.cpu().numpy(), qv, ctx.gas, w, d.hidden1, d.hidden2, np.array(d.out_bounds[:]), sv=sv)
+    assert np.linalg.norm(ref) > 0
+    assert rel_l2(got, ref) < 1e-5, rel_l2(got, ref)
