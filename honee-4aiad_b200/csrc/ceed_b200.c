@@ -1713,7 +1713,19 @@ static int vec_f32_shadow(CeedVector v) {
 }
 
 /* apply one non-composite operator, adding into out (out already holds what should be kept) */
+/* An operator over zero elements (a partition that owns none, libCEED's CeedElemRestrictionCreate with num_elem 0)
+ * contributes nothing: its apply, diagonal and point-block diagonal add zero, and no plan (no kernel) is built. */
+static int op_empty(CeedOperator op) {
+  if (op->composite) return 0;
+  for (int i = 0; i < MAX_FIELDS; i++) {
+    const CeedElemRestriction r = op->in[i].r;
+    if (r && r != CEED_ELEMRESTRICTION_NONE) return r->num_elem == 0;
+  }
+  return 0;
+}
+
 static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
+  if (op_empty(op)) return CEED_ERROR_SUCCESS;
   CK(op_plan(op));
   Ceed         ceed = op->ceed;
   cudaStream_t s    = ceed->stream;
@@ -1958,7 +1970,7 @@ int CeedOperatorApply(CeedOperator op, CeedVector in, CeedVector out, CeedReques
   (void)request;
   if (out && out != CEED_VECTOR_NONE) {
     /* Setup overwrites; everything else accumulates after zeroing */
-    int only_setup = !op->composite && (op_plan(op) == 0) && (op->plan == PLAN_SETUP || op->plan == PLAN_SETUP_SUR);
+    int only_setup = !op->composite && !op_empty(op) && (op_plan(op) == 0) && (op->plan == PLAN_SETUP || op->plan == PLAN_SETUP_SUR);
     if (!only_setup) CK(CeedVectorSetValue(out, 0.0));
   }
   return op_apply_marked(op, in, out);
@@ -1970,6 +1982,7 @@ int CeedOperatorApplyAdd(CeedOperator op, CeedVector in, CeedVector out, CeedReq
 }
 
 static int op_diag_add_single(CeedOperator op, CeedVector assembled) {
+  if (op_empty(op)) return CEED_ERROR_SUCCESS;
   CK(op_plan(op));
   if (op->plan == PLAN_FREESTREAM_JAC) {
     CK(need_len(op, assembled, op->fop->l_size, "diagonal"));
@@ -2292,6 +2305,7 @@ static int pb_rstr(CeedOperator op, CeedElemRestriction *r) {
 }
 
 static int op_pbdiag_add_single(CeedOperator op, CeedVector assembled) {
+  if (op_empty(op)) return CEED_ERROR_SUCCESS;
   CK(op_plan(op));
   Ceed         ceed = op->ceed;
   cudaStream_t s    = ceed->stream;

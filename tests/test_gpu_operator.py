@@ -29,6 +29,10 @@ CASES = {
     "su_gravity_P4Q4": dict(n=(3, 3, 3), P=4, Q=4, stab=prob.STAB_SU, g=(0.5, -9.81, 0.2)),
     "nostab_P3Q4": dict(n=(3, 4, 2), P=3, Q=4, stab=prob.STAB_NONE),
     "idl_P3Q3": dict(n=(6, 3, 3), P=3, Q=3, idl=(2e-3, 0.2, 0.5, 101000.0)),
+    # edge sizes: one element (one colour, the other launches empty), the smallest and the largest compiled bases
+    "single_elem_P4Q5": dict(n=(1, 1, 1), P=4, Q=5, state="modes"),
+    "min_basis_P2Q2": dict(n=(5, 3, 4), P=2, Q=2),
+    "max_basis_P6Q7": dict(n=(2, 2, 1), P=6, Q=7, state="modes"),
 }
 
 
@@ -220,3 +224,48 @@ def test_host_backed_vectors_across_steps_match_the_device_path():
         torch.cuda.synchronize()
         np.testing.assert_array_equal(h_g, tv.cpu().numpy(), err_msg=f"step {step}")
         np.testing.assert_array_equal(h_j, tj.cpu().numpy(), err_msg=f"step {step}")
+
+
+def test_operator_over_zero_elements_contributes_nothing():
+    """A partition may own no elements: libCEED accepts restrictions with num_elem 0 and an operator over them adds zero.
+    HONEE's operators built over zero elements (same L-vector) give a zero residual with Apply, leave the output of
+    ApplyAdd unchanged, assemble zero (point-block) diagonals, and change nothing, bit for bit, as sub-operators of the
+    real composites."""
+    from types import SimpleNamespace
+    mesh, basis, ctx, q, qd, ceed, ops, qv, g = _setup("cfg2_P4Q5")
+    empty = SimpleNamespace(num_elem=0, l_size=mesh.l_size, offsets=np.zeros(0, np.int32), x_elem=np.zeros((0, 3, 8)))
+    eops = hon.NewtonianOperators(ceed, empty, basis, ctx)
+    assert eops.q_data.to_numpy().size == 0
+    rng = np.random.default_rng(5)
+    dq = q * 1e-4 * rng.normal(size=q.shape)
+    dv = ce.Vector(ceed, mesh.l_size)
+    dv.set_array_host(dq)
+    out = ce.Vector(ceed, mesh.l_size)
+    out.set_array_host(np.full(mesh.l_size, 7.0))
+    eops.op_ifunction.apply(qv, out)
+    np.testing.assert_array_equal(out.to_numpy(), 0.0)
+    out.set_array_host(np.full(mesh.l_size, 7.0))
+    eops.op_ijacobian.apply(dv, out, add=True)
+    np.testing.assert_array_equal(out.to_numpy(), 7.0)
+    eops.op_ijacobian.assemble_diagonal(out)
+    np.testing.assert_array_equal(out.to_numpy(), 0.0)
+    pb = ce.Vector(ceed, 5 * mesh.l_size)
+    eops.op_ijacobian.assemble_point_block_diagonal(pb)
+    np.testing.assert_array_equal(pb.to_numpy(), 0.0)
+    # reference results of the real composites, then the same composites with an empty sub-operator joined
+    ops.ifunction(qv, ops.q_dot, g)
+    v_ref = g.to_numpy()
+    jv = ce.Vector(ceed, mesh.l_size)
+    ops.ijacobian(dv, jv)
+    j_ref = jv.to_numpy()
+    d = ce.Vector(ceed, mesh.l_size)
+    ops.diagonal(d)
+    d_ref = d.to_numpy()
+    ops.op_ifunction.add_sub(eops.op_ifunction_volume)
+    ops.op_ijacobian.add_sub(eops.op_ijacobian_volume)
+    ops.ifunction(qv, ops.q_dot, g)
+    ops.ijacobian(dv, jv)
+    ops.diagonal(d)
+    np.testing.assert_array_equal(g.to_numpy(), v_ref)
+    np.testing.assert_array_equal(jv.to_numpy(), j_ref)
+    np.testing.assert_array_equal(d.to_numpy(), d_ref)
