@@ -1,4 +1,4 @@
-"""End-to-end GPU test of the learned closure (the BASELINE learned-closure workflow at reduced size): a fine plain run,
+"""End-to-end GPU test of the learned closure at reduced size: a fine plain run,
 differential filter, training pairs, GPU training of the 6-20-20-6 network, and two coarse runs from the filtered
 initial state.  The closure must beat the closure-free coarse run against the filtered fine solution on the kinetic
 energy decay and on the resolved dissipation, at lower GPU cost than the fine run."""

@@ -1,6 +1,6 @@
 """GPU parity: the fused sm_100a operators, reached through the libCEED C API, against the CPU oracle.
 
-Tolerances (BASELINE north star): restriction maps bit-exact; FP64 residual, Jacobian action and diagonal within
+Tolerances: restriction maps bit-exact; FP64 residual, Jacobian action and diagonal within
 1e-12 relative L2 of the oracle; geometric factors within 1e-14; the FP32 (mixed-precision) Jacobian action and
 diagonal within 2e-6 relative L2 (single-precision arithmetic on FP64 geometry).
 """
