@@ -2,7 +2,7 @@
 
   python tests/golden/make_golden.py [--ref /root/reference]
 
-Outputs (committed; the GPU box has no reference tree):
+Outputs (committed, so the tests need no reference tree):
   pointwise_newtonian.npz   seeded quadrature-point inputs and the outputs of the reference's own
                             IFunction_Newtonian_* / IJacobian_Newtonian_* QFunctions (qfunctions/newtonian.h:205-315),
                             compiled unchanged into oracle/_ref/libhonee_ref.so by oracle/Makefile
