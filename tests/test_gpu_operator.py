@@ -79,7 +79,7 @@ def test_ifunction_ijacobian_diagonal_fp64(name):
         assert rel_l2(d.to_numpy(), d_ref) < TOL64, rel_l2(d.to_numpy(), d_ref)
 
 
-@pytest.mark.parametrize("name", ["cfg1_P3Q3", "cfg2_P4Q5", "cfg3_P5Q6_periodic"])
+@pytest.mark.parametrize("name", ["cfg1_P3Q3", "cfg2_P4Q5", "cfg3_P5Q6_periodic", "single_elem_P4Q5", "max_basis_P6Q7"])
 def test_mixed_precision_jacobian(name):
     mesh, basis, ctx, q, qd, ceed, ops, qv, g = _setup(name, "/gpu/b200/mixed")
     v_ref, jd_ref, qdata_ref, m = oracle_ifunction(mesh, basis, ctx, q, qd)
