@@ -494,10 +494,14 @@ static int vec_dev_write(CeedVector v, double **d, int write_only) {
   return CEED_ERROR_SUCCESS;
 }
 
+/* Any call that hands the device array out (GetArray*, TakeArray) or replaces or writes it outside an operator (SetArray,
+ * including a device-to-device copy on the compute stream) clears use_known: ev_use then no longer covers every use of
+ * d, so the next copy between host and device follows the whole compute stream instead of the last operator's event. */
 int CeedVectorSetArray(CeedVector v, CeedMemType mem_type, CeedCopyMode copy_mode, CeedScalar *array) {
   CK(vec_wait_h2d(v));
   v->f64_stale = 0;
   v->f32_valid = 0;
+  v->use_known = 0;
   if (mem_type == CEED_MEM_HOST) {
     if (copy_mode == CEED_COPY_VALUES) {
       CK(vec_alloc_host(v));
@@ -535,6 +539,7 @@ int CeedVectorSyncArray(CeedVector v, CeedMemType mem_type) { return mem_type ==
 
 int CeedVectorTakeArray(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
   CK(vec_wait_h2d(v));
+  v->use_known = 0;
   if (mem_type == CEED_MEM_HOST) {
     if (v->h && !v->h_valid && (v->d_valid || v->f64_stale)) CK(vec_sync_host(v));
     *array     = v->h;
@@ -557,6 +562,7 @@ int CeedVectorGetArrayRead(CeedVector v, CeedMemType mem_type, const CeedScalar 
     *array = v->h;
   } else {
     CK(vec_sync_dev(v));
+    v->use_known = 0;
     *array = v->d;
   }
   return CEED_ERROR_SUCCESS;
@@ -570,8 +576,9 @@ int CeedVectorGetArray(CeedVector v, CeedMemType mem_type, CeedScalar **array) {
     *array     = v->h;
   } else {
     CK(vec_sync_dev(v));
-    v->h_valid = 0;
-    *array     = v->d;
+    v->use_known = 0;
+    v->h_valid   = 0;
+    *array       = v->d;
   }
   v->f32_valid = 0;
   return CEED_ERROR_SUCCESS;
@@ -588,9 +595,10 @@ int CeedVectorGetArrayWrite(CeedVector v, CeedMemType mem_type, CeedScalar **arr
     *array     = v->h;
   } else {
     CK(vec_alloc_dev(v));
-    v->d_valid = 1;
-    v->h_valid = 0;
-    *array     = v->d;
+    v->use_known = 0;
+    v->d_valid   = 1;
+    v->h_valid   = 0;
+    *array       = v->d;
   }
   return CEED_ERROR_SUCCESS;
 }

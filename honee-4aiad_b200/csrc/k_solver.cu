@@ -382,7 +382,8 @@ std::atomic<double *> g_multidot_scratch_addr[kMaxDevices];
 
 // Address of g_multidot_scratch on the current device, looked up once per device (with that device current) on the first
 // call there.  The lookup may load this module on the device, so the first call on each device belongs before any
-// stream capture starts.
+// stream capture starts.  The cached address does not survive cudaDeviceReset (the reloaded module may place the array
+// elsewhere); the header states that the entry point is not for a device whose context was reset.
 int multidot_scratch(double **p) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) return HB_ERROR_CUDA;

@@ -252,7 +252,9 @@ HB_EXPORT int hb_krylov_multidot_f32(const float *V, int64_t ldv, int k, const f
  * No counterpart in the reference (PETSc's VecMDot owns its work space); it exists for callers that cannot hand over a
  * device buffer, such as a vector-library inner-product callback.  The first call on each device looks the array up
  * and belongs before any stream capture; calls that overlap on one device (different streams or host threads) race on
- * the shared array and must be serialised by the caller. */
+ * the shared array and must be serialised by the caller.  The looked-up address is kept per device ordinal for the life
+ * of the process: after cudaDeviceReset (or any teardown of the device's primary context) the module is loaded anew and
+ * the array may move, so this entry point must not be called on a device after its context was reset. */
 HB_EXPORT int hb_krylov_multidot_f64_static(const double *V, int64_t ldv, int k, const double *w, int64_t n, double *d_out, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);

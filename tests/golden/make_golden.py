@@ -1,6 +1,6 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself (run in a container that has the reference).
 
-  python tests/golden/make_golden.py [--ref /root/reference]
+  python tests/golden/make_golden.py [--ref REFERENCE_TREE]
 
 Outputs (committed, so the tests need no reference tree):
   pointwise_newtonian.npz   seeded quadrature-point inputs and the outputs of the reference's own
@@ -75,9 +75,12 @@ def seeded_points(rng, gas, Q, state_var):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("HONEE_REFERENCE_DIR"),
+                    help="the reference tree (default: HONEE_REFERENCE_DIR, else the tree oracle/_ref was built from)")
     args = ap.parse_args()
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={args.ref}"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")] + ([f"REF={args.ref}"] if args.ref else []), check=True)
+    if not args.ref:
+        args.ref = open(os.path.join(ROOT, "oracle", "_ref", "reference_dir.txt")).read().strip()
     import oracle as O
     R = O.ref()
     assert R is not None, "reference QFunctions were not built"

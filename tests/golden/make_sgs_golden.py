@@ -1,6 +1,6 @@
 """Generate tests/golden/sgs_points.npz from the reference itself (run in a container that has the reference).
 
-  python tests/golden/make_sgs_golden.py [--ref /root/reference]
+  python tests/golden/make_sgs_golden.py [--ref REFERENCE_TREE]
 
 Seeded quadrature-point data run through the reference's own data-driven SGS QFunctions, compiled unchanged into
 oracle/_ref/libhonee_ref.so (oracle/Makefile):
@@ -49,7 +49,8 @@ def sgs_ctx_bytes(R, newt_ctx: bytes, flat_ref_layout: np.ndarray) -> bytes:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("HONEE_REFERENCE_DIR"),
+                    help="the reference tree (default: HONEE_REFERENCE_DIR, else the tree oracle/_ref was built from)")
     args = ap.parse_args()
     import oracle as O
     O.build()
@@ -61,6 +62,8 @@ def main():
     n = 256
 
     # weights: the reference's files, in its data-blob layout (b1 | b2 (20 slots) | W1 [20][6] | W2 [6][20] | bounds)
+    if not args.ref:
+        args.ref = open(os.path.join(os.path.dirname(O.__file__), "_ref", "reference_dir.txt")).read().strip()
     dd = os.path.join(args.ref, "examples", "dd_sgs_data")
     b1, b2 = sgs.read_dat(os.path.join(dd, "b1.dat")), sgs.read_dat(os.path.join(dd, "b2.dat"))
     w1, w2 = sgs.read_dat(os.path.join(dd, "w1.dat")), sgs.read_dat(os.path.join(dd, "w2.dat"))

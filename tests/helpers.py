@@ -12,6 +12,16 @@ import oracle as O  # noqa: E402
 prob = importlib.import_module("honee-4aiad_b200.problem")
 
 
+def reference_dir():
+    """The reference source tree, or None: HONEE_REFERENCE_DIR when set, else the tree oracle/Makefile built oracle/_ref
+    from (recorded in oracle/_ref/reference_dir.txt).  Tests that read reference sources skip when it is None."""
+    d = os.environ.get("HONEE_REFERENCE_DIR")
+    if not d:
+        rec = os.path.join(ROOT, "oracle", "_ref", "reference_dir.txt")
+        d = open(rec).read().strip() if os.path.exists(rec) else None
+    return d if d and os.path.isdir(os.path.join(d, "qfunctions")) else None
+
+
 def rel_l2(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)

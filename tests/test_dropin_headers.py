@@ -5,13 +5,14 @@ import subprocess
 import textwrap
 
 import pytest
+from helpers import reference_dir
 
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
-REF = "/root/reference"
 INC = os.path.join(ROOT, "include")
+REF = reference_dir()
 
 
-@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "qfunctions")), reason="reference sources not present")
+@pytest.mark.skipif(REF is None, reason="reference sources not present (set HONEE_REFERENCE_DIR)")
 @pytest.mark.parametrize("header", ["newtonian.h", "setupgeo.h", "taylorgreen.h", "monitor_totalkineticenergy.h"])
 def test_reference_qfunctions_compile_against_our_headers(tmp_path, header):
     src = tmp_path / "t.c"

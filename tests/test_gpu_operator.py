@@ -224,6 +224,14 @@ def test_host_backed_vectors_across_steps_match_the_device_path():
         torch.cuda.synchronize()
         np.testing.assert_array_equal(h_g, tv.cpu().numpy(), err_msg=f"step {step}")
         np.testing.assert_array_equal(h_j, tj.cpu().numpy(), err_msg=f"step {step}")
+    # An operator marks g's device array used; a device-to-device copy into it (SetArray DEVICE, COPY_VALUES) is enqueued
+    # on the compute stream after that.  The read-back must wait for the copy, not only for the operator's event.
+    ops.op_ifunction.apply(qv, g)
+    src = torch.from_numpy(q * 3.0 + 1.0).to(dev)
+    torch.cuda.synchronize()
+    g.set_array_device(src.data_ptr(), copy=True)
+    ce.L().CeedVectorSyncArray(g.ptr, ce.CEED_MEM_HOST)
+    np.testing.assert_array_equal(h_g, src.cpu().numpy())
 
 
 def test_operator_over_zero_elements_contributes_nothing():

@@ -85,9 +85,11 @@ def test_backprop_matches_finite_differences(h2, alpha):
 
 def test_reference_weight_files_load_into_the_fixture_layout():
     sgs = importlib.import_module("honee-4aiad_b200.sgs")
-    dd = "/root/reference/examples/dd_sgs_data"
-    if not os.path.isdir(dd):
-        pytest.skip("reference tree not present")
+    from helpers import reference_dir
+    ref = reference_dir()
+    if ref is None:
+        pytest.skip("reference tree not present (set HONEE_REFERENCE_DIR)")
+    dd = os.path.join(ref, "examples", "dd_sgs_data")
     d, flat = sgs.load_reference_model(dd)
     np.testing.assert_array_equal(flat, GOLD["weights"])
     assert (d.hidden1, d.hidden2) == (20, 0)
