@@ -858,122 +858,149 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
 // Diagonal of the IJacobian operator (libCEED CeedOperatorLinearAssembleDiagonal semantics): at every quadrature point
 // linearise the point-wise Jacobian for each component c with unit inputs in the four eval modes (interp, grad x/y/z),
 // keep the 4x4 block A_c[m][n] = d out(m,c) / d in(n,c), and contract sum_q phi_m(q,p) A_c[m][n](q) phi_n(q,p) by sum
-// factorisation with products of 1D basis rows.  The 16 (m,n) pairs share 10 distinct product triples.
+// factorisation with products of 1D basis rows.  The 16 (m,n) pairs share 10 distinct product triples (combinations).
+//
+// The point blocks come from the explicit linearisation of the point function (diag_point_blocks: per component one
+// value tangent and three physical-gradient tangents with their unit inputs folded in, the reference-direction blocks
+// assembled as X R X^T), so a point costs about four Jacobian evaluations, not twenty.  The per-point Jacobian data and
+// qdata are read once per element.  The 50 combination arrays [5][10][Q^3] are contracted in three batched passes whose
+// partial sums are grouped by the basis factors still to apply: after the x pass the ten combinations of a component
+// collapse into six (y, z) groups, after the y pass into three z groups.
 
 template <typename T>
 struct DiagArgs {
   const T *jac_data;
   T *diag;
-  T G1[kMaxP * kMaxP];  // reference 1D gradient [Q][P]
+  T G1[kMaxP * kMaxP];        // reference 1D gradient [Q][P]
+  T W[3][kMaxP * kMaxP];      // squared basis rows [Q][P]: B*B, B*G, G*G
+};
+
+// combination order: II, IGx, IGy, IGz, GxGx, GyGy, GzGz, GxGy, GxGz, GyGz.  The six x-pass groups by their (y, z)
+// factors, each member given as (combination, x factor): (0,0): II/BB, IGx/BG, GxGx/GG; (1,0): IGy/BB, GxGy/BG;
+// (0,1): IGz/BB, GxGz/BG; (2,0): GyGy/BB; (0,2): GzGz/BB; (1,1): GyGz/BB.  The three y-pass groups by their z factor,
+// members (x group, y factor): z=0: (0,0)/BB, (1,0)/BG, (2,0)/GG; z=1: (0,1)/BB, (1,1)/BG; z=2: (0,2)/BB.
+__host__ __device__ constexpr int diag_xgroup_size(int g) { return g == 0 ? 3 : (g < 3 ? 2 : 1); }
+__host__ __device__ constexpr int diag_xmember(int g, int i) {
+  return g == 0 ? (i == 0 ? 0 : (i == 1 ? 1 : 4)) : g == 1 ? (i == 0 ? 2 : 7) : g == 2 ? (i == 0 ? 3 : 8) : g == 3 ? 5 : (g == 4 ? 6 : 9);
+}
+__host__ __device__ constexpr int diag_xfactor(int g, int i) { return g < 3 ? i : 0; }
+__host__ __device__ constexpr int diag_ygroup_size(int h) { return 3 - h; }
+__host__ __device__ constexpr int diag_ymember(int h, int i) { return h == 0 ? (i == 0 ? 0 : (i == 1 ? 1 : 3)) : h == 1 ? (i == 0 ? 2 : 5) : 4; }
+__host__ __device__ constexpr int diag_yfactor(int h, int i) { return i; }
+
+template <int P, int Q>
+struct DiagPlan {
+  // FP64 at Q = 5: 74 KB, three CTAs per SM
+  static constexpr int P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q, PX = P;  // PX: pa stride of the x-pass output
+  static constexpr int nA = 50 * Q3;                                               // [5][10][Q3]; after the y pass: T2 [5][3][Q][P][P]
+  static constexpr int nT1 = 5 * 6 * Q2 * PX;                                      // [5][6][Q][Q][PX]
+  static constexpr int nT2 = 5 * 3 * Q * P2;
+  static_assert(nT2 <= nA, "the y-pass output fits in the combination arrays");
+  template <typename T>
+  static constexpr size_t bytes() { return sizeof(T) * (size_t)(nA + nT1); }
 };
 
 template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
-__global__ void __launch_bounds__(nthreads_for<T>(Q), 2) k_diagonal(const ElemArgs<T> a, const DiagArgs<T> p) {
+__global__ void __launch_bounds__(nthreads_for<T>(Q), (Q <= 5 ? 3 : 1)) k_diagonal(const ElemArgs<T> a, const DiagArgs<T> p) {
   constexpr int NT = nthreads_for<T>(Q);
-  constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
+  using L = DiagPlan<P, Q>;
+  constexpr int P2 = L::P2, P3 = L::P3, Q2 = L::Q2, Q3 = L::Q3, PX = L::PX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *smem = reinterpret_cast<T *>(smem_raw);
-  T *sA = smem;                // [10][Q3]
-  T *sT1 = sA + 10 * Q3;       // [Q][Q][P]  after x contraction
-  T *sT2 = sT1 + Q2 * P;       // [Q][P][P]  after y contraction
-  T *sOut = sT2 + Q * P * P;   // [5][P3]
-  // squared basis rows: W[s][i][p] for s = 0: B*B, 1: B*G, 2: G*G (shared copies: no parameter arrays indexed at run time)
-  __shared__ T sW[3][kMaxP * kMaxP];
-  for (int t = threadIdx.x; t < Q * P; t += NT) {
-    T b = 0, g = 0;
-#pragma unroll
-    for (int i = 0; i < Q * P; i++)
-      if (i == t) {
-        b = a.basis.B[i];
-        g = p.G1[i];
-      }
-    sW[0][t] = b * b;
-    sW[1][t] = b * g;
-    sW[2][t] = g * g;
-  }
-  __syncthreads();
-  // combo order: II, IGx, IGy, IGz, GxGx, GyGy, GzGz, GxGy, GxGz, GyGz; selectors = number of derivatives per direction
-  constexpr int cx[10] = {0, 1, 0, 0, 2, 0, 0, 1, 1, 0};
-  constexpr int cy[10] = {0, 0, 1, 0, 0, 2, 0, 1, 0, 1};
-  constexpr int cz[10] = {0, 0, 0, 1, 0, 0, 2, 0, 1, 1};
+  T *sA = reinterpret_cast<T *>(smem_raw);  // [5][10][Q3]
+  T *sT1 = sA + L::nA;                      // [5][6][Q2][PX]
+  T *sT2 = sA;                              // [5][3][Q][P][P]
+  const int njd = a.num_jd;
   for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
     const int e = a.elems[idx];
-    for (int c = 0; c < 5; c++) {
-      const int q = threadIdx.x;
-      if (q < Q3) {
-        T jd[15], wdetJ, X[3][3];
-        const T *jdp = p.jac_data + (int64_t)e * a.num_jd * Q3 + q;
+    if (threadIdx.x == 0 && idx + (int)gridDim.x < a.n_elems) {  // warm L2 with the next element's point data
+      const int en = a.elems[idx + gridDim.x];
+      prefetch_l2_bulk(p.jac_data + (int64_t)en * njd * Q3, sizeof(T) * njd * Q3);
+      prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, sizeof(double) * 10 * Q3);
+    }
+    const int q = threadIdx.x;
+    if (q < Q3) {
+      T jd[15], wdetJ, X[3][3];
+      const T *jdp = p.jac_data + (int64_t)e * njd * Q3 + q;
 #pragma unroll
-        for (int k = 0; k < 14; k++) jd[k] = jdp[k * Q3];
-        jd[14] = a.num_jd > 14 ? jdp[14 * Q3] : T(0);
-        load_qdata(a.qdata + (int64_t)e * 10 * Q3, Q3, q, wdetJ, X);
-        T A[4][4];
+      for (int k = 0; k < 14; k++) jd[k] = jdp[k * Q3];
+      jd[14] = njd > 14 ? jdp[14 * Q3] : T(0);
+      load_qdata(a.qdata + (int64_t)e * 10 * Q3, Q3, q, wdetJ, X);
+      T *sAq = sA + q;
+      diag_point_blocks<SV>(a.pc, jd, wdetJ, X, [&](int c, int m, T v) { sAq[(c * 10 + m) * Q3] = v; });
+    }
+    __syncthreads();
+    // x pass, one (component, k j) fibre per work item and x group: T1[c][g][kj][pa] = sum_members sum_i W(i,pa) A[c][m][kj][i]
 #pragma unroll
-        for (int n = 0; n < 4; n++) {
-          T dq[5] = {0, 0, 0, 0, 0}, gref[3][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}}, v[5], gv[3][5];
+    for (int g = 0; g < 6; g++) {
+      for (int t = threadIdx.x; t < 5 * Q2; t += NT) {
+        const int c = t / Q2, kj = t % Q2;
+        T acc[P];
 #pragma unroll
-          for (int k = 0; k < 5; k++) {
-            if (n == 0 && k == c) dq[k] = 1;
+        for (int pa = 0; pa < P; pa++) acc[pa] = 0;
 #pragma unroll
-            for (int d = 0; d < 3; d++)
-              if (n == d + 1 && k == c) gref[d][k] = 1;
-          }
-          ijacobian_point_stream<T, SV>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
+        for (int mi = 0; mi < diag_xgroup_size(g); mi++) {
+          const T *src = sA + (c * 10 + diag_xmember(g, mi)) * Q3 + kj * Q;
+          T in[Q];
 #pragma unroll
-          for (int k = 0; k < 5; k++)
-            if (k == c) {
-              A[0][n] = v[k];
-              A[1][n] = gv[0][k];
-              A[2][n] = gv[1][k];
-              A[3][n] = gv[2][k];
-            }
+          for (int i = 0; i < Q; i++) in[i] = src[i];
+#pragma unroll
+          for (int pa = 0; pa < P; pa++)
+#pragma unroll
+            for (int i = 0; i < Q; i++) acc[pa] += p.W[diag_xfactor(g, mi)][i * P + pa] * in[i];
         }
-        sA[0 * Q3 + q] = A[0][0];
-        sA[1 * Q3 + q] = A[0][1] + A[1][0];
-        sA[2 * Q3 + q] = A[0][2] + A[2][0];
-        sA[3 * Q3 + q] = A[0][3] + A[3][0];
-        sA[4 * Q3 + q] = A[1][1];
-        sA[5 * Q3 + q] = A[2][2];
-        sA[6 * Q3 + q] = A[3][3];
-        sA[7 * Q3 + q] = A[1][2] + A[2][1];
-        sA[8 * Q3 + q] = A[1][3] + A[3][1];
-        sA[9 * Q3 + q] = A[2][3] + A[3][2];
-      }
-      for (int t = threadIdx.x; t < P3; t += NT) sOut[c * P3 + t] = 0;
-      __syncthreads();
+        T *dst = sT1 + ((c * 6 + g) * Q2 + kj) * PX;
 #pragma unroll
-      for (int m = 0; m < 10; m++) {
-        const T *Wx = sW[cx[m]], *Wy = sW[cy[m]], *Wz = sW[cz[m]];
-        for (int f = threadIdx.x; f < Q2 * P; f += NT) {  // x: T1[k][j][pa] = sum_i Wx(i,pa) A[k][j][i]
-          const int pa = f % P, kj = f / P;
-          T s = 0;
-#pragma unroll
-          for (int i = 0; i < Q; i++) s += Wx[i * P + pa] * sA[m * Q3 + kj * Q + i];
-          sT1[kj * P + pa] = s;
-        }
-        __syncthreads();
-        for (int f = threadIdx.x; f < Q * P * P; f += NT) {
-          const int pa = f % P, pb = (f / P) % P, k = f / (P * P);
-          T s = 0;
-#pragma unroll
-          for (int j = 0; j < Q; j++) s += Wy[j * P + pb] * sT1[(k * Q + j) * P + pa];
-          sT2[(k * P + pb) * P + pa] = s;
-        }
-        __syncthreads();
-        for (int f = threadIdx.x; f < P3; f += NT) {
-          const int pab = f % (P * P), pc_ = f / (P * P);
-          T s = 0;
-#pragma unroll
-          for (int k = 0; k < Q; k++) s += Wz[k * P + pc_] * sT2[k * P * P + pab];
-          sOut[c * P3 + f] += s;
-        }
-        __syncthreads();
+        for (int pa = 0; pa < P; pa++) dst[pa] = acc[pa];
       }
     }
+    __syncthreads();
+    // y pass, one (component, k, pa) fibre per work item and y group: T2[c][h][k][pb][pa]
+#pragma unroll
+    for (int h = 0; h < 3; h++) {
+      for (int t = threadIdx.x; t < 5 * Q * P; t += NT) {
+        const int c = t / (Q * P), k = (t / P) % Q, pa = t % P;
+        T acc[P];
+#pragma unroll
+        for (int pb = 0; pb < P; pb++) acc[pb] = 0;
+#pragma unroll
+        for (int mi = 0; mi < diag_ygroup_size(h); mi++) {
+          const T *src = sT1 + ((c * 6 + diag_ymember(h, mi)) * Q2 + k * Q) * PX + pa;
+          T in[Q];
+#pragma unroll
+          for (int j = 0; j < Q; j++) in[j] = src[j * PX];
+#pragma unroll
+          for (int pb = 0; pb < P; pb++)
+#pragma unroll
+            for (int j = 0; j < Q; j++) acc[pb] += p.W[diag_yfactor(h, mi)][j * P + pb] * in[j];
+        }
+        T *dst = sT2 + ((c * 3 + h) * Q + k) * P2 + pa;
+#pragma unroll
+        for (int pb = 0; pb < P; pb++) dst[pb * P] = acc[pb];
+      }
+    }
+    __syncthreads();
+    // z pass over the three z groups, then the scatter: elements of one colour share no node
     const int32_t *off = a.offsets + (int64_t)e * P3;
-    for (int t = threadIdx.x; t < P3 * 5; t += NT) {
-      const int pp = t / 5, c = t % 5;
-      p.diag[__ldg(off + pp) + c] += sOut[c * P3 + pp];
+    for (int t = threadIdx.x; t < 5 * P2; t += NT) {
+      const int c = t / P2, pab = t % P2;
+      T acc[P];
+#pragma unroll
+      for (int pc = 0; pc < P; pc++) acc[pc] = 0;
+#pragma unroll
+      for (int h = 0; h < 3; h++) {
+        T in[Q];
+#pragma unroll
+        for (int k = 0; k < Q; k++) in[k] = sT2[((c * 3 + h) * Q + k) * P2 + pab];
+#pragma unroll
+        for (int pc = 0; pc < P; pc++)
+#pragma unroll
+          for (int k = 0; k < Q; k++) acc[pc] += p.W[h][k * P + pc] * in[k];
+      }
+#pragma unroll
+      for (int pc = 0; pc < P; pc++) {
+        T *d = p.diag + __ldg(off + pc * P2 + pab) + c;
+        *d += acc[pc];
+      }
     }
     __syncthreads();
   }
@@ -1281,14 +1308,19 @@ static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, c
 
 template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_diagonal(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, T *diag, cudaStream_t s) {
-  const int P3 = P * P * P, Q3 = Q * Q * Q;
-  const size_t sm = sizeof(T) * (size_t)(10 * Q3 + Q * Q * P + Q * P * P + 5 * P3);
+  const size_t sm = DiagPlan<P, Q>::template bytes<T>();
   cudaFuncSetAttribute(k_diagonal<P, Q, T, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   DiagArgs<T> p;
+  memset(&p, 0, sizeof p);
   p.jac_data = jd;
   p.diag = diag;
-  memset(p.G1, 0, sizeof p.G1);
-  for (int i = 0; i < Q * P; i++) p.G1[i] = T(op->grad1d[i]);
+  for (int i = 0; i < Q * P; i++) {
+    const double b = op->interp1d[i], g = op->grad1d[i];
+    p.G1[i] = T(g);
+    p.W[0][i] = T(b * b);
+    p.W[1][i] = T(b * g);
+    p.W[2][i] = T(g * g);
+  }
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<T> a = make_args<T>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
@@ -1726,11 +1758,24 @@ static int launch_blockdiag(const HbElemOp *op, const HbNewtonianContext &ctx, c
 
 // (P, Q) pairs compiled: polynomial degree 1..5 with q_extra 0 or 1 (Q = P or P + 1), and q_extra 2 for degrees 1 and 2
 // (the channel example's q_extra 2); the benchmark configurations use (3,3), (4,5) and (5,6).
+// The compiled (P, Q) lists.  A build with -DHB_BASES_P4Q5_ONLY compiles the degree-3 basis with q_extra 1 alone (every
+// kernel, conservative variables only): a quick build for kernel work, not a product configuration.
+#ifdef HB_BASES_P4Q5_ONLY
+#define HB_PQ_LIST(X) X(4, 5)
+#define HB_SGS_PQ_LIST(X)
+#define HB_SV_PQ_LIST(X)
+#endif
+#ifndef HB_PQ_LIST
 #define HB_PQ_LIST(X) X(2, 2) X(2, 3) X(2, 4) X(3, 3) X(3, 4) X(3, 5) X(4, 4) X(4, 5) X(5, 5) X(5, 6) X(6, 6) X(6, 7)
+#endif
 // bases the residual with the fused SGS closure is built for (the coarse LES runs at degree 2 and 3)
+#ifndef HB_SGS_PQ_LIST
 #define HB_SGS_PQ_LIST(X) X(3, 3) X(3, 4) X(4, 5)
+#endif
 // bases compiled for the primitive and entropy state variables (degree 1-3 with q_extra 0-2 as HONEE's examples use them)
+#ifndef HB_SV_PQ_LIST
 #define HB_SV_PQ_LIST(X) X(2, 2) X(2, 3) X(2, 4) X(3, 3) X(3, 4) X(3, 5) X(4, 4) X(4, 5)
+#endif
 
 }  // namespace hb
 

@@ -653,3 +653,162 @@ __device__ __forceinline__ void ijacobian_point_stream(const PhysConst<T> &c, co
 }
 
 }  // namespace hb
+
+namespace hb {
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Component-diagonal blocks of the linearised IJacobian point function, the point-wise input of the Jacobi diagonal
+// (CeedOperatorLinearAssembleDiagonal on the IJacobian operator).  For component C the 4 x 4 block
+// A[m][n] = d out(m, C) / d in(n, C), m, n in {value, reference gradient 0..2}, of ijacobian_point_stream decomposes by
+// linearity:
+//   A[0][0]     = v_C of the value tangent dq = e_C;   A[0][1 + d] = 0 (the value output does not see gradients)
+//   A[1+k][0]   = wdetJ sum_j X[k][j] V_j              V_j    flux column j, component C, of the value tangent
+//   A[1+k][1+d] = wdetJ sum_j sum_i X[k][j] R[j][i] X[d][i]
+//                                                      R[j][i] flux column j, component C, of a unit physical gradient
+//                                                              e_C in direction i (a reference gradient e_C in direction d
+//                                                              is the physical gradient X[d][i] e_C in direction i)
+// so each component costs one value tangent and three physical-gradient tangents, each folded for its unit input, instead
+// of four reference-gradient evaluations of the full point function.  The set-up (state, stress, 1 / (R T^2)) is formed
+// once per point.  `out(m, value)` receives the ten symmetric combinations in the order II, IGx, IGy, IGz, GxGx, GyGy,
+// GzGz, GxGy, GxGz, GyGz (A[m][n] + A[n][m], one term on the diagonal).
+template <int C, int SV, typename T, typename Out>
+__device__ __forceinline__ void diag_point_component(const PhysConst<T> &c, const St<T> &s, const SAux<T> &aux, T inv_RT2, const T sig[3][3],
+                                                     const T jd[15], T wdetJ, const T X[3][3], Out out) {
+  const bool stab = c.stab != HB_STAB_NONE;
+  const T tau[3] = {jd[11], jd[12], jd[13]};
+  const T ke = T(.5) * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]);
+  // state_from_y_fwd with the reciprocal 1 / (R T^2) formed once per point
+  auto y_fwd = [&](const T dY[5], St<T> &ds) {
+    ds.P = dY[0];
+    ds.u[0] = dY[1];
+    ds.u[1] = dY[2];
+    ds.u[2] = dY[3];
+    ds.T_ = dY[4];
+    ds.rho = (dY[0] * s.T_ - s.P * dY[4]) * inv_RT2;
+#pragma unroll
+    for (int i = 0; i < 3; i++) ds.m[i] = ds.rho * s.u[i] + s.rho * ds.u[i];
+    const T dke = ds.u[0] * s.u[0] + ds.u[1] * s.u[1] + ds.u[2] * s.u[2];
+    ds.E = ds.rho * (c.cv * s.T_ + ke) + s.rho * (c.cv * dY[4] + dke);
+  };
+  // component C of flux row j of a tangent state (dflux_row)
+  auto frow = [&](const St<T> &ds, int j) -> T {
+    if (C == 0) return ds.m[j];
+    if (C == 4) return (ds.E + ds.P) * s.u[j] + (s.E + s.P) * ds.u[j];
+    return ds.m[j] * s.u[C - 1] + s.m[j] * ds.u[C - 1] + (j == C - 1 ? ds.P : T(0));
+  };
+  // the stabilisation state of a strong residual r: d = StateFromY_fwd(tau . r)
+  auto stab_state = [&](const T r[5], St<T> &d) {
+    const T dY[5] = {tau[0] * r[0], tau[1] * r[1], tau[1] * r[2], tau[1] * r[3], tau[2] * r[4]};
+    y_fwd(dY, d);
+  };
+  St<T> dS;  // unit tangent of component C
+  {
+    T e[5] = {0, 0, 0, 0, 0};
+    e[C] = T(1);
+    state_from_q_fwd<SV>(c, s, aux, e, dS);
+  }
+  // value tangent
+  T V[3], A00;
+  {
+    const T dU[5] = {dS.rho, dS.m[0], dS.m[1], dS.m[2], dS.E};
+    const T dbody[5] = {T(0), dS.rho * c.g[0], dS.rho * c.g[1], dS.rho * c.g[2], dS.m[0] * c.g[0] + dS.m[1] * c.g[1] + dS.m[2] * c.g[2]};
+    T vi = c.shift * dU[C] - dbody[C];
+    if (c.idl_enable) {
+      const T dY[5] = {dS.P * jd[14], T(0), T(0), T(0), T(0)};
+      St<T> di;
+      y_fwd(dY, di);
+      const T dUi[5] = {di.rho, di.m[0], di.m[1], di.m[2], di.E};
+      vi += dUi[C];
+    }
+    A00 = wdetJ * vi;
+    St<T> d;
+    const bool supg = c.stab == HB_STAB_SUPG;
+    if (supg) {
+      T r[5];
+#pragma unroll
+      for (int k = 0; k < 5; k++) r[k] = c.shift * dU[k] - dbody[k];
+      stab_state(r, d);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      T col = -frow(dS, j);
+      if (C == 4) col += dS.u[0] * sig[0][j] + dS.u[1] * sig[1][j] + dS.u[2] * sig[2][j];  // -dFe with dsig = 0, gT = 0
+      if (supg) col += frow(d, j);
+      V[j] = col;
+    }
+  }
+  // physical-gradient tangents: R[j][i]
+  T R[3][3];
+  const T w = T(1.0 / 1.4142135623730951);
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    St<T> d;
+    if (stab) {
+      T r[5];
+      r[0] = dS.m[i];
+#pragma unroll
+      for (int k = 0; k < 3; k++) r[1 + k] = dS.m[i] * s.u[k] + s.m[i] * dS.u[k] + (i == k ? dS.P : T(0));
+      r[4] = (dS.E + dS.P) * s.u[i] + (s.E + s.P) * dS.u[i];
+      stab_state(r, d);
+    }
+    // strain of a velocity gradient with only column i = dS.u
+    T de[6] = {0, 0, 0, 0, 0, 0};
+    de[i] = dS.u[i];
+    if (i == 0) {
+      de[4] = w * dS.u[2];
+      de[5] = w * dS.u[1];
+    } else if (i == 1) {
+      de[3] = w * dS.u[2];
+      de[5] = w * dS.u[0];
+    } else {
+      de[3] = w * dS.u[1];
+      de[4] = w * dS.u[0];
+    }
+    T dsig[3][3];
+    stress_full(c, de, dsig);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      T col = 0;
+      if (C >= 1 && C <= 3) col = dsig[C - 1][j];
+      if (C == 4) col = s.u[0] * dsig[0][j] + s.u[1] * dsig[1][j] + s.u[2] * dsig[2][j] + (j == i ? c.k * dS.T_ : T(0));
+      if (stab) col += frow(d, j);
+      R[j][i] = col;
+    }
+  }
+  // reference-direction blocks
+  T XR[3][3];  // XR[k][i] = sum_j X[k][j] R[j][i]
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) XR[k][i] = X[k][0] * R[0][i] + X[k][1] * R[1][i] + X[k][2] * R[2][i];
+  auto AGG = [&](int k, int d) { return wdetJ * (XR[k][0] * X[d][0] + XR[k][1] * X[d][1] + XR[k][2] * X[d][2]); };
+  out(0, A00);
+#pragma unroll
+  for (int k = 0; k < 3; k++) out(1 + k, wdetJ * (X[k][0] * V[0] + X[k][1] * V[1] + X[k][2] * V[2]));
+  out(4, AGG(0, 0));
+  out(5, AGG(1, 1));
+  out(6, AGG(2, 2));
+  out(7, AGG(0, 1) + AGG(1, 0));
+  out(8, AGG(0, 2) + AGG(2, 0));
+  out(9, AGG(1, 2) + AGG(2, 1));
+}
+
+// Shared per-point set-up of diag_point_component and the five components.
+template <int SV, typename T, typename Out>
+__device__ __forceinline__ void diag_point_blocks(const PhysConst<T> &c, const T jd[15], T wdetJ, const T X[3][3], Out out) {
+  St<T> s;
+  SAux<T> aux;
+  const T q[5] = {jd[0], jd[1], jd[2], jd[3], jd[4]};
+  state_from_q<SV>(c, q, s, aux);
+  const T e[6] = {jd[5], jd[6], jd[7], jd[8], jd[9], jd[10]};
+  T sig[3][3];
+  stress_full(c, e, sig);
+  const T inv_RT2 = rcp(c.Rgas * s.T_ * s.T_);
+  diag_point_component<0, SV>(c, s, aux, inv_RT2, sig, jd, wdetJ, X, [&](int m, T v) { out(0, m, v); });
+  diag_point_component<1, SV>(c, s, aux, inv_RT2, sig, jd, wdetJ, X, [&](int m, T v) { out(1, m, v); });
+  diag_point_component<2, SV>(c, s, aux, inv_RT2, sig, jd, wdetJ, X, [&](int m, T v) { out(2, m, v); });
+  diag_point_component<3, SV>(c, s, aux, inv_RT2, sig, jd, wdetJ, X, [&](int m, T v) { out(3, m, v); });
+  diag_point_component<4, SV>(c, s, aux, inv_RT2, sig, jd, wdetJ, X, [&](int m, T v) { out(4, m, v); });
+}
+
+}  // namespace hb

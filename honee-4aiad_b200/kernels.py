@@ -190,3 +190,26 @@ class FaceOp:
         cb = C.create_string_buffer(bytes(ctx264), len(ctx264))
         _chk(_load().hb_freestream_jacobian_apply(self.ptr, cb, C.c_int(flux_type), _addr(self.qdata), _addr(self.jac), _addr(dq), _addr(v),
                                                   _stream(stream)), "hb_freestream_jacobian_apply")
+
+
+def fma_peak(fp64=True, iters=4096, reps=5, device=None):
+    """Measured FMA throughput of the FP64 (or FP32) pipe in FMA/s: the best of `reps` launches of the library's probe
+    (independent FMA chains over 8 CTAs per SM), timed with CUDA events on torch's current stream after one warm-up."""
+    import torch
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    n = 2048 * torch.cuda.get_device_properties(dev).multi_processor_count
+    sink = torch.empty(n, dtype=torch.float64 if fp64 else torch.float32, device=dev)
+    s = torch.cuda.current_stream(dev)
+    cnt = C.c_int64()
+    fn = _load().hb_fma_peak_probe
+    _chk(fn(int(fp64), iters, _addr(sink), C.c_int64(n), C.byref(cnt), _stream(s)), "hb_fma_peak_probe")
+    best = None
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        _chk(fn(int(fp64), iters, _addr(sink), C.c_int64(n), C.byref(cnt), _stream(s)), "hb_fma_peak_probe")
+        b.record(s)
+        b.synchronize()
+        t = a.elapsed_time(b) * 1e-3
+        best = t if best is None else min(best, t)
+    return cnt.value / best

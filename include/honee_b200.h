@@ -474,6 +474,12 @@ HB_EXPORT int hb_spanstats_process(HbSpanStats *st, double solution_time, double
                                    void *stream);
 HB_EXPORT int hb_spanstats_destroy(HbSpanStats *st);
 
+/* Arithmetic-pipe throughput probe (no reference counterpart; the pipe-side denominator of the operator roofline): one
+ * launch of 8 x SMs CTAs of 256 threads, each thread running eight independent FMA chains of `iters` steps in FP64
+ * (fp64 != 0) or FP32.  d_sink: device scratch of at least 2048 x SMs elements of that type (written only on an
+ * impossible value); *fma_per_launch receives the FMA count, to be divided by the caller's event time on `stream`. */
+HB_EXPORT int hb_fma_peak_probe(int fp64, int iters, void *d_sink, int64_t sink_elems, int64_t *fma_per_launch, void *stream);
+
 /* Library identification */
 const char *hb_version(void);
 

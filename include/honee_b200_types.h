@@ -109,6 +109,28 @@ typedef struct {
   double             u[3];
 } HbTaylorGreenContext;
 
+/* qfunctions/newtonian_types.h (State: conservative then primitive values, 80 bytes) */
+typedef struct {
+  double density, momentum[3], E_total;
+  HbStatePrimitive Y;
+} HbState;
+
+/* qfunctions/channel.h:12-21 (struct ChannelContext_, 240 bytes) */
+typedef struct {
+  bool               implicit;
+  double             theta0, P0, umax, center, H, B;
+  HbNewtonianContext newt_ctx;
+} HbChannelContext;
+
+/* qfunctions/gaussianwave.h:11-18 (struct GaussianWaveContext_, 304 bytes) */
+typedef struct {
+  double             epicenter[3];
+  double             width;
+  double             amplitude;
+  HbState            S_infty;
+  HbNewtonianContext newt_ctx;
+} HbGaussianWaveContext;
+
 /* Number of stored Jacobian components per quadrature point: q (5), Kelvin-Mandel strain rate (6), diagonal tau (3),
  * plus the IDL ramp coefficient when enabled (problems/newtonian.c:756-757; qfunctions/newtonian.h:251-254). */
 #define HB_JAC_DATA_COMPS 14
@@ -128,5 +150,11 @@ HB_STATIC_ASSERT(offsetof(HbNewtonianContext, time) == 64, "solution time offset
 HB_STATIC_ASSERT(offsetof(HbNewtonianContext, ijacobian_time_shift) == 72, "ijacobian time shift offset");
 HB_STATIC_ASSERT(offsetof(HbNewtonianContext, dt) == 168, "timestep size offset");
 HB_STATIC_ASSERT(sizeof(HbSetupContext) == 304, "SetupContext_ layout");
+HB_STATIC_ASSERT(sizeof(HbTaylorGreenContext) == 272, "TaylorGreenContext_ layout");
+HB_STATIC_ASSERT(sizeof(HbState) == 80, "State layout");
+HB_STATIC_ASSERT(sizeof(HbChannelContext) == 240, "ChannelContext_ layout");
+HB_STATIC_ASSERT(offsetof(HbChannelContext, newt_ctx) == 56, "ChannelContext_ newt_ctx offset");
+HB_STATIC_ASSERT(sizeof(HbGaussianWaveContext) == 304, "GaussianWaveContext_ layout");
+HB_STATIC_ASSERT(offsetof(HbGaussianWaveContext, newt_ctx) == 120, "GaussianWaveContext_ newt_ctx offset");
 
 #endif
