@@ -127,7 +127,21 @@ typedef struct {
   int                 set;
 } OpField;
 
-enum { PLAN_NONE = 0, PLAN_SETUP, PLAN_IFUNCTION, PLAN_IJACOBIAN, PLAN_SETUP_SUR, PLAN_FREESTREAM, PLAN_FREESTREAM_JAC, PLAN_RHS, PLAN_MASS, PLAN_MASS_STAB };
+enum {
+  PLAN_NONE = 0,
+  PLAN_SETUP,
+  PLAN_IFUNCTION,
+  PLAN_IJACOBIAN,
+  PLAN_SETUP_SUR,
+  PLAN_FREESTREAM,
+  PLAN_FREESTREAM_JAC,
+  PLAN_RHS,
+  PLAN_MASS,
+  PLAN_MASS_STAB,
+  PLAN_ICS,     /* initial condition at the solution nodes (src/setuplibceed.c:143-175) */
+  PLAN_MON_KE,  /* MonitorTotalKineticEnergy_* per-point integrands (src/monitor_totalkineticenergy.c:80-103) */
+  PLAN_MON_CFL  /* MonitorCFL_3D_* per-point CFL numbers (src/monitor_cfl.c:60-110) */
+};
 
 struct CeedOperator_private {
   Ceed          ceed;
@@ -148,6 +162,8 @@ struct CeedOperator_private {
   double   *d_zero, *d_tmp_rhs;       /* explicit right-hand side: zero rate and the residual it is negated from */
   float    *d_tmp_pb32;               /* mixed-precision point blocks before they are widened into the FP64 output */
   int       flux_type;                /* 0 HLL, 1 HLLC */
+  double   *d_tmp_e2;                 /* output E-vector of the initial-condition and monitor operators */
+  int       ic_kind, ic_state_var;    /* initial-condition QFunction (HB_IC_*) and the state variable it writes */
 };
 
 struct CeedContextFieldLabel_private {
@@ -1015,9 +1031,58 @@ int CeedBasisCreateH1(Ceed ceed, CeedElemTopology topo, CeedInt num_comp, CeedIn
   (void)topo, (void)num_comp, (void)num_nodes, (void)nqpts, (void)interp, (void)grad, (void)q_ref, (void)q_weights, (void)basis;
   return CeedError(ceed, CEED_ERROR_UNSUPPORTED, "non-tensor H1 bases are outside the B200 backend's hex-element scope");
 }
+/* libCEED's CeedBasisCreateProjection, which SetupLibceed calls for its initial-condition operator
+ * (src/setuplibceed.c:150): a basis from the nodes of basis_from to the nodes of basis_to with interp = B_to^+ B_from
+ * and grad = B_to^+ G_from, B_to^+ the least-squares pseudo-inverse over the quadrature both bases share, so a field
+ * given at basis_from's nodes is evaluated (value and reference gradient) at basis_to's nodes.  Tensor bases take the
+ * 1D rule per direction; the new basis has P = P_from, Q = P_to and no quadrature weights.  The pseudo-inverse comes
+ * from the normal equations solved by Cholesky in long double (B_to has full column rank for Q >= P_to); when the
+ * from-space lies in the to-space (a trilinear coordinate field projected onto a higher-degree solution basis) the
+ * result is the from-basis evaluated at the to-nodes, to rounding. */
 int CeedBasisCreateProjection(CeedBasis basis_from, CeedBasis basis_to, CeedBasis *basis_project) {
-  (void)basis_to, (void)basis_project;
-  return CeedError(basis_from->ceed, CEED_ERROR_UNSUPPORTED, "projection bases (initial-condition operators) are outside the backend scope");
+  Ceed ceed = basis_from->ceed;
+  if (!basis_from->tensor || !basis_to->tensor || basis_from->dim != basis_to->dim)
+    return CeedError(ceed, CEED_ERROR_UNSUPPORTED, "projection bases need two tensor H1 bases of the same dimension");
+  if (basis_from->Q1d != basis_to->Q1d) return CeedError(ceed, CEED_ERROR_DIMENSION, "bases for a projection must share their quadrature points");
+  const int Q = basis_to->Q1d, Pt = basis_to->P1d, Pf = basis_from->P1d;
+  if (Pt > Q) return CeedError(ceed, CEED_ERROR_DIMENSION, "projection needs at least as many quadrature points as target nodes");
+  long double M[HB_MAX_P][HB_MAX_P], L[HB_MAX_P][HB_MAX_P];
+  for (int a = 0; a < Pt; a++)
+    for (int b = 0; b < Pt; b++) {
+      long double s = 0;
+      for (int q = 0; q < Q; q++) s += (long double)basis_to->interp1d[q * Pt + a] * basis_to->interp1d[q * Pt + b];
+      M[a][b] = s;
+    }
+  for (int a = 0; a < Pt; a++)
+    for (int b = 0; b <= a; b++) {
+      long double s = M[a][b];
+      for (int k = 0; k < b; k++) s -= L[a][k] * L[b][k];
+      if (a == b) {
+        if (s <= 0) return CeedError(ceed, CEED_ERROR_DIMENSION, "target basis is rank deficient on the shared quadrature");
+        L[a][a] = sqrtl(s);
+      } else L[a][b] = s / L[b][b];
+    }
+  double interp[HB_MAX_P * HB_MAX_P], grad[HB_MAX_P * HB_MAX_P], zeros[HB_MAX_P] = {0};
+  for (int m = 0; m < 2; m++) {
+    const double *src = m ? basis_from->grad1d : basis_from->interp1d;
+    double       *dst = m ? grad : interp;
+    for (int j = 0; j < Pf; j++) {
+      long double y[HB_MAX_P], x[HB_MAX_P];
+      for (int a = 0; a < Pt; a++) {  /* rhs = B_to^T src[:, j], then forward and back substitution */
+        long double r = 0;
+        for (int q = 0; q < Q; q++) r += (long double)basis_to->interp1d[q * Pt + a] * src[q * Pf + j];
+        for (int k = 0; k < a; k++) r -= L[a][k] * y[k];
+        y[a] = r / L[a][a];
+      }
+      for (int a = Pt - 1; a >= 0; a--) {
+        long double r = y[a];
+        for (int k = a + 1; k < Pt; k++) r -= L[k][a] * x[k];
+        x[a] = r / L[a][a];
+      }
+      for (int a = 0; a < Pt; a++) dst[a * Pf + j] = (double)x[a];
+    }
+  }
+  return CeedBasisCreateTensorH1(ceed, basis_from->dim, basis_from->num_comp, Pf, Pt, interp, grad, zeros, zeros, basis_project);
 }
 
 int CeedBasisReferenceCopy(CeedBasis basis, CeedBasis *basis_copy) {
@@ -1336,8 +1401,9 @@ int CeedOperatorSetField(CeedOperator op, const char *field_name, CeedElemRestri
   cudaFree(op->d_tmp_out32);
   cudaFree(op->d_tmp_e);
   cudaFree(op->d_tmp_pb32);
+  cudaFree(op->d_tmp_e2);
   op->d_tmp_pb32 = NULL;
-  op->d_zero = op->d_tmp_rhs = op->d_tmp_e = NULL;
+  op->d_zero = op->d_tmp_rhs = op->d_tmp_e = op->d_tmp_e2 = NULL;
   op->d_tmp_in32 = op->d_tmp_out32 = NULL;
   return CEED_ERROR_SUCCESS;
 }
@@ -1574,6 +1640,57 @@ static int plan_freestream(CeedOperator op, int jacobian, int flux_type, int sta
 }
 
 
+/* Initial-condition operator: the coordinates' restriction (3 components, trilinear) with the projection basis onto the
+ * solution nodes, the IC QFunction's context, and the output through the solution's node restriction. */
+static int plan_ics(CeedOperator op, int kind, int sv) {
+  CeedQFunction qf = op->qf;
+  if (qf->nin > 2) return plan_fail(op, "initial conditions from the wall distance (ics_use_wall_distance) are not supported");
+  if (qf->nin != 2 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[0].size != 3 || qf->in[1].emode != CEED_EVAL_GRAD ||
+      qf->out[0].emode != CEED_EVAL_NONE || qf->out[0].size != 5)
+    return plan_fail(op, "unexpected initial-condition field layout (src/setuplibceed.c:153-166)");
+  if (op->in[0].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "the coordinates and q0 must be active");
+  CeedBasis bx = op->in[0].b;
+  if (!is_tensor3(bx, 3) || bx->P1d != 2 || op->in[1].b != bx || op->in[1].r != op->in[0].r)
+    return plan_fail(op, "x and dx must share the trilinear coordinate restriction and its projection basis");
+  CeedElemRestriction rq = op->out[0].r;
+  if (!rq || rq == CEED_ELEMRESTRICTION_NONE || rq->strided || rq->num_comp != 5 || rq->elem_size != bx->Q1d * bx->Q1d * bx->Q1d ||
+      rq->num_elem != op->in[0].r->num_elem)
+    return plan_fail(op, "q0 must use a 5-component node restriction with one entry per projected node");
+  static const size_t sizes[4] = {sizeof(HbSetupContext), sizeof(HbTaylorGreenContext), sizeof(HbChannelContext), sizeof(HbGaussianWaveContext)};
+  if (!qf->ctx || qf->ctx->size != sizes[kind]) return plan_fail(op, "the initial-condition context has an unexpected size");
+  if (kind == HB_IC_TAYLOR_GREEN) sv = ((const HbTaylorGreenContext *)qf->ctx->data)->newt_ctx.state_var;
+  if (kind == HB_IC_CHANNEL) sv = ((const HbChannelContext *)qf->ctx->data)->newt_ctx.state_var;
+  op->ic_kind      = kind;
+  op->ic_state_var = sv;
+  op->plan         = PLAN_ICS;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* Monitor operators: the state (INTERP, and GRAD for the kinetic energy) and qdata -> per-point values through a strided
+ * collocated restriction (CreateElemRestrColloc_CompMajor, src/monitor_totalkineticenergy.c:35-47). */
+static int plan_monitor(CeedOperator op, int ke, int sv) {
+  CeedQFunction qf = op->qf;
+  const int     nin = ke ? 3 : 2, ncomp = ke ? 5 : 1;
+  if (qf->nin != nin || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[0].size != 5 ||
+      (ke && qf->in[1].emode != CEED_EVAL_GRAD) || qf->in[nin - 1].emode != CEED_EVAL_NONE || qf->in[nin - 1].size != 10 ||
+      qf->out[0].emode != CEED_EVAL_NONE || qf->out[0].size != ncomp)
+    return plan_fail(op, ke ? "unexpected kinetic-energy monitor field layout (src/monitor_totalkineticenergy.c:96-105)"
+                            : "unexpected CFL monitor field layout (src/monitor_cfl.c:100-107)");
+  if (op->in[0].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE || (ke && op->in[1].v != CEED_VECTOR_ACTIVE))
+    return plan_fail(op, "the state and the monitor values must be active");
+  if (ke && (op->in[1].r != op->in[0].r || op->in[1].b != op->in[0].b)) return plan_fail(op, "q and Grad_q must share restriction and basis");
+  if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+  if (((const HbNewtonianContext *)qf->ctx->data)->state_var != sv) return plan_fail(op, "the context's state_var differs from the QFunction's");
+  CK(plan_elemop(op, op->in[0].r, op->in[0].b));
+  const int           Q3 = op->eop->Q * op->eop->Q * op->eop->Q;
+  CeedElemRestriction ro = op->out[0].r;
+  CK(check_qdata_rstr(op, op->in[nin - 1].r, 10, Q3, "qdata"));
+  if (!ro || ro == CEED_ELEMRESTRICTION_NONE || !ro->strided || ro->num_comp != ncomp || ro->elem_size != Q3 || ro->num_elem != op->eop->num_elem)
+    return plan_fail(op, "monitor values must use a strided restriction with one entry per quadrature point and component");
+  op->plan = ke ? PLAN_MON_KE : PLAN_MON_CFL;
+  return CEED_ERROR_SUCCESS;
+}
+
 /* The state variable a Newtonian QFunction name selects (newtonian.h:259-269, 313-323): "<prefix>Conserv" 0, "<prefix>Prim" 1,
  * "<prefix>Entropy" 2, anything else -1. */
 static int newtonian_state_var(const char *k, const char *prefix) {
@@ -1710,6 +1827,17 @@ static int op_plan(CeedOperator op) {
     op->plan = PLAN_SETUP_SUR;
     return CEED_ERROR_SUCCESS;
   }
+  {  /* initial conditions (src/setuplibceed.c:143-175): "x" (INTERP) and "dx" (GRAD) of the coordinates through the
+      * projection basis onto the solution nodes -> "q0" (NONE) through the state restriction */
+    int kind = -1, sv = -1;
+    if ((sv = newtonian_state_var(k, "ICsNewtonianIG_")) >= 0) kind = HB_IC_NEWTONIAN;
+    else if ((sv = newtonian_state_var(k, "IC_GaussianWave_")) >= 0) kind = HB_IC_GAUSSIAN_WAVE;
+    else if (!strcmp(k, "ICsTaylorGreen")) kind = HB_IC_TAYLOR_GREEN;
+    else if (!strcmp(k, "ICsChannel")) kind = HB_IC_CHANNEL;
+    if (kind >= 0) return plan_ics(op, kind, sv);
+  }
+  const int sv_ke = newtonian_state_var(k, "MonitorTotalKineticEnergy_"), sv_cfl = newtonian_state_var(k, "MonitorCFL_3D_");
+  if (sv_ke >= 0 || sv_cfl >= 0) return plan_monitor(op, sv_ke >= 0, sv_ke >= 0 ? sv_ke : sv_cfl);
   int jacobian, flux_type, fs_sv;
   if (freestream_kernel(k, &jacobian, &flux_type, &fs_sv)) return plan_freestream(op, jacobian, flux_type, fs_sv);
   return plan_fail(op, "no fused kernel for this QFunction (no CPU fallback on /gpu/b200)");
@@ -1843,6 +1971,42 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
       CK(vec_dev_read(op->in[2].v, &qd));
       CK(vec_dev_write(out, &v, 0));
       HB_CK(ceed, hb_mass_stab_apply(op->eop, op->qf->ctx->data, qd, qs, u, v, 1, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_ICS: {
+      CeedBasis           bx = op->in[0].b;
+      CeedElemRestriction rq = op->out[0].r;
+      CK(need_len(op, out, rq->l_size, "initial state"));
+      CK(gather_coords(op, &op->in[0], in, &op->d_tmp_e));
+      const size_t ne = (size_t)rq->num_elem * 5 * rq->elem_size;
+      if (!op->d_tmp_e2) CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_e2, sizeof(double) * (ne ? ne : 1)));
+      HB_CK(ceed, hb_ics_apply(op->ic_kind, op->ic_state_var, op->qf->ctx->data, op->qf->ctx->size, rq->num_elem, bx->Q1d, bx->interp1d, op->d_tmp_e,
+                               op->d_tmp_e2, s));
+      CK(rstr_upload(rq));
+      CK(rstr_build_transpose(rq));
+      double *v;
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_restrict_apply_t_csr(rq->l_size, rq->d_tptr, rq->d_teidx, op->d_tmp_e2, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_MON_KE:
+    case PLAN_MON_CFL: {
+      const int           ke = op->plan == PLAN_MON_KE, iq = ke ? 2 : 1;
+      CeedElemRestriction ro = op->out[0].r;
+      CK(need_len(op, in, op->eop->l_size, "state"));
+      CK(need_len(op, out, ro->l_size, "monitor values"));
+      CK(need_len(op, op->in[iq].v, op->in[iq].r->l_size, "qdata"));
+      const size_t ne = (size_t)ro->num_elem * ro->num_comp * ro->elem_size;
+      if (!op->d_tmp_e2) CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_e2, sizeof(double) * (ne ? ne : 1)));
+      const double *q, *qd;
+      CK(vec_dev_read(in, &q));
+      CK(vec_dev_read(op->in[iq].v, &qd));
+      if (ke) HB_CK(ceed, hb_monitor_ke_points(op->eop, op->qf->ctx->data, q, qd, op->d_tmp_e2, s));
+      else HB_CK(ceed, hb_monitor_cfl_points(op->eop, op->qf->ctx->data, q, qd, op->d_tmp_e2, s));
+      CK(rstr_upload(ro));
+      double *v;
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_restrict_apply_t_strided(ro->num_elem, ro->elem_size, ro->num_comp, ro->d_strides, op->d_tmp_e2, v, s));
       return CEED_ERROR_SUCCESS;
     }
     case PLAN_MASS: {
@@ -2135,6 +2299,7 @@ int CeedOperatorDestroy(CeedOperator *op) {
   cudaFree(o->d_tmp_in32);
   cudaFree(o->d_tmp_out32);
   cudaFree(o->d_tmp_e);
+  cudaFree(o->d_tmp_e2);
   Ceed ceed = o->ceed;
   free(o);
   *op = NULL;

@@ -277,8 +277,10 @@ __device__ __forceinline__ void mon_gradient(int sv, const hb::PhysConst<double>
 
 // per-element partial sums of the five kinetic-energy integrands [num_elem][5] (MonitorTotalKineticEnergy_Conserv/_Prim/
 // _Entropy, qfunctions/monitor_totalkineticenergy.h:8-51)
+// point_out (may be null): the five integrands at every point, E-vector [elem][5][Q^3], the output of the Ceed-bound
+// MonitorTotalKineticEnergy_* operator (src/monitor_totalkineticenergy.c:80-103); elem_sums (may be null): their sums.
 __global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, const double *__restrict__ q, const double *__restrict__ qdata,
-                             hb::PhysConst<double> pc, int sv, MonBasis b, double *__restrict__ elem_sums) {
+                             hb::PhysConst<double> pc, int sv, MonBasis b, double *__restrict__ elem_sums, double *__restrict__ point_out) {
   extern __shared__ double sm[];
   const int e = blockIdx.x, P3 = P * P * P, Q3 = Q * Q * Q;
   double *sN = sm, *red = sm + 5 * P3;
@@ -310,12 +312,13 @@ __global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, 
     for (int a = 0; a < 3; a++)
       for (int c = 0; c < 3; c++) SS += S[a][c] * S[a][c];
     const double w0 = gs[2].u[1] - gs[1].u[2], w1 = gs[0].u[2] - gs[2].u[0], w2 = gs[1].u[0] - gs[0].u[1];
-    acc[0] += wdetJ * 0.5 * s.rho * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]);
-    acc[1] += wdetJ * -2 * pc.mu * SS;
-    acc[2] += wdetJ * -pc.lambda * pc.mu * div * div;
-    acc[3] += wdetJ * s.P * div;
-    acc[4] += wdetJ * pc.mu * (w0 * w0 + w1 * w1 + w2 * w2);
+    const double v[5] = {wdetJ * 0.5 * s.rho * (s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2]), wdetJ * -2 * pc.mu * SS,
+                         wdetJ * -pc.lambda * pc.mu * div * div, wdetJ * s.P * div, wdetJ * pc.mu * (w0 * w0 + w1 * w1 + w2 * w2)};
+    for (int c = 0; c < 5; c++) acc[c] += v[c];
+    if (point_out)
+      for (int c = 0; c < 5; c++) point_out[((int64_t)e * 5 + c) * Q3 + qp] = v[c];
   }
+  if (!elem_sums) return;
   for (int c = 0; c < 5; c++) red[c * blockDim.x + threadIdx.x] = acc[c];
   __syncthreads();
   if (threadIdx.x < 5) {
@@ -327,8 +330,10 @@ __global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, 
 
 // per-element min/max over points of sqrt(u . g u) with g = 0.25 dXdx^T dXdx (MonitorCFL_3D_Conserv/_Prim/_Entropy,
 // qfunctions/monitor_cfl.h:9-58)
+// point_out (may be null): sqrt(u . g u) at every point, E-vector [elem][Q^3] (the Ceed-bound MonitorCFL_3D_* operator,
+// src/monitor_cfl.c:100-110); elem_minmax (may be null): its per-element extremes.
 __global__ void k_monitor_cfl(int P, int Q, const int32_t *__restrict__ offsets, const double *__restrict__ q, const double *__restrict__ qdata,
-                              hb::PhysConst<double> pc, int sv, MonBasis b, double *__restrict__ elem_minmax) {
+                              hb::PhysConst<double> pc, int sv, MonBasis b, double *__restrict__ elem_minmax, double *__restrict__ point_out) {
   extern __shared__ double sm[];
   const int e = blockIdx.x, P3 = P * P * P, Q3 = Q * Q * Q;
   double *sN = sm, *red = sm + 5 * P3;
@@ -350,7 +355,9 @@ __global__ void k_monitor_cfl(int P, int Q, const int32_t *__restrict__ offsets,
     const double cfl = sqrt(ugu);
     mn = fmin(mn, cfl);
     mx = fmax(mx, cfl);
+    if (point_out) point_out[(int64_t)e * Q3 + qp] = cfl;
   }
+  if (!elem_minmax) return;
   red[threadIdx.x] = mn;
   red[blockDim.x + threadIdx.x] = mx;
   __syncthreads();
@@ -599,7 +606,7 @@ int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double *q, const
   const int P3 = op->P * op->P * op->P;
   const int nt = 128;
   const size_t sm = sizeof(double) * (5 * P3 + 5 * nt);
-  k_monitor_ke<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), d_scratch);
+  k_monitor_ke<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), d_scratch, nullptr);
   if (rc()) return HB_ERROR_CUDA;
   double *h = (double *)malloc(sizeof(double) * 5 * (size_t)op->num_elem);
   if (!h) return HB_ERROR_NOMEM;
@@ -620,7 +627,7 @@ int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, cons
   const int P3 = op->P * op->P * op->P;
   const int nt = 128;
   const size_t sm = sizeof(double) * (5 * P3 + 2 * nt);
-  k_monitor_cfl<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), d_scratch);
+  k_monitor_cfl<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), d_scratch, nullptr);
   if (rc()) return HB_ERROR_CUDA;
   double *h = (double *)malloc(sizeof(double) * 2 * (size_t)op->num_elem);
   if (!h) return HB_ERROR_NOMEM;
@@ -635,6 +642,26 @@ int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, cons
   minmax[0] = mn * dt;
   minmax[1] = mx * dt;
   return err ? HB_ERROR_CUDA : HB_SUCCESS;
+}
+
+// Per-point monitor values (the Ceed-bound monitor operators): asynchronous on s.
+int hb_monitor_ke_points(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *e_out, void *s) {
+  int sv = 0;
+  if (state_var_of(ctx184, &sv)) return HB_ERROR_UNSUPPORTED;
+  if (op->num_elem == 0) return HB_SUCCESS;
+  const int P3 = op->P * op->P * op->P, nt = 128;
+  const size_t sm = sizeof(double) * (5 * P3 + 5 * nt);
+  k_monitor_ke<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), nullptr, e_out);
+  return rc();
+}
+int hb_monitor_cfl_points(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *e_out, void *s) {
+  int sv = 0;
+  if (state_var_of(ctx184, &sv)) return HB_ERROR_UNSUPPORTED;
+  if (op->num_elem == 0) return HB_SUCCESS;
+  const int P3 = op->P * op->P * op->P, nt = 128;
+  const size_t sm = sizeof(double) * (5 * P3 + 2 * nt);
+  k_monitor_cfl<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), nullptr, e_out);
+  return rc();
 }
 
 int hb_pb_invert_f64(const double *blocks, double *inv, int64_t nodes, int *d_singular, int *h_singular, void *s) {

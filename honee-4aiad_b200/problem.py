@@ -48,7 +48,27 @@ class TaylorGreenContext(C.Structure):
                 ("lz", C.c_double), ("u", C.c_double * 3)]
 
 
+class ICBoundaryLayer(C.Structure):
+    _fields_ = [("wall", StatePrimitive), ("height", C.c_double)]
+
+
+class SetupContext(C.Structure):
+    """struct SetupContext_ (qfunctions/newtonian_types.h:66-75): the context of ICsNewtonianIG_*, with "evaluation time"."""
+    _fields_ = [("reference", StatePrimitive), ("ic_boundary_layer", ICBoundaryLayer), ("newt_ctx", NewtonianContext), ("lx", C.c_double),
+                ("ly", C.c_double), ("lz", C.c_double), ("time", C.c_double)]
+
+
+def setup_context(newt, P, u, T, lengths=(1.0, 1.0, 1.0)):
+    """A SetupContext with the reference (P, u, T), as NS_NEWTONIAN_IG fills it (problems/newtonian.c:660-700)."""
+    ctx = SetupContext()
+    ctx.reference = StatePrimitive(P, (C.c_double * 3)(*u), T)
+    ctx.newt_ctx = newt
+    ctx.lx, ctx.ly, ctx.lz = lengths
+    return ctx
+
+
 assert C.sizeof(NewtonianContext) == 184
+assert C.sizeof(SetupContext) == 304
 assert NewtonianContext.time.offset == 64 and NewtonianContext.ijacobian_time_shift.offset == 72 and NewtonianContext.dt.offset == 168
 
 # Field offsets HONEE registers with CeedQFunctionContextRegisterDouble (problems/newtonian.c:747-753)

@@ -279,6 +279,11 @@ HB_EXPORT int hb_vec_combine_f64(const double *q1, const double *q2, double a, d
 /* Monitors (src/monitor_totalkineticenergy.c:134-163, src/monitor_cfl.c:140-164): kinetic-energy integrand sums (not divided
  * by the volume; d_scratch >= 5*num_elem doubles) and dt * min/max CFL (d_scratch >= 2*num_elem doubles).  Synchronise. */
 HB_EXPORT int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *d_scratch, double sums[5], void *s);
+/* The same integrands at every quadrature point, E-vector e_out [elem][5][Q^3] (the Ceed-bound MonitorTotalKineticEnergy_*
+ * operator, src/monitor_totalkineticenergy.c:80-103, before VecStrideSum); and sqrt(u . g u) at every point, e_out
+ * [elem][Q^3] (MonitorCFL_3D_*, src/monitor_cfl.c:100-110, before the min / max and the time-step factor).  Asynchronous. */
+HB_EXPORT int hb_monitor_ke_points(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *e_out, void *s);
+HB_EXPORT int hb_monitor_cfl_points(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *e_out, void *s);
 HB_EXPORT int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double dt, double *d_scratch,
                              double minmax[2], void *s);
 
@@ -473,6 +478,19 @@ HB_EXPORT int hb_spanstats_copy_sums(const HbSpanStats *st, double *dst);
 HB_EXPORT int hb_spanstats_process(HbSpanStats *st, double solution_time, double rtol, int max_it, double *stats, int *its, double *rel_norm,
                                    void *stream);
 HB_EXPORT int hb_spanstats_destroy(HbSpanStats *st);
+
+/* Initial condition at the solution nodes (SetupLibceed's op_ics, src/setuplibceed.c:143-175): one thread per node of
+ * each element evaluates the coordinates through proj1d ([P_to][2], the 1D CeedBasisCreateProjection of the trilinear
+ * coordinate basis onto the solution basis) from x_e ([elem][3][8] vertex coordinates) and the IC QFunction `kind` with
+ * its context bytes (HbSetupContext, HbTaylorGreenContext, HbChannelContext or HbGaussianWaveContext; ctx_size checked),
+ * writing q0_e [elem][5][P_to^3].  state_var: the QFunction's state variable for ICsNewtonianIG_* and IC_GaussianWave_*
+ * (the Taylor-Green and channel ICs use their context's). */
+#define HB_IC_NEWTONIAN 0     /* ICsNewtonianIG_{Conserv,Prim,Entropy}, qfunctions/newtonian.h:17-42 */
+#define HB_IC_TAYLOR_GREEN 1  /* ICsTaylorGreen, qfunctions/taylorgreen.h:23-51 */
+#define HB_IC_CHANNEL 2       /* ICsChannel, qfunctions/channel.h:58-73 */
+#define HB_IC_GAUSSIAN_WAVE 3 /* IC_GaussianWave_{Conserv,Prim,Entropy}, qfunctions/gaussianwave.h:20-71 */
+HB_EXPORT int hb_ics_apply(int kind, int state_var, const void *ctx, size_t ctx_size, int num_elem, int P_to, const double *proj1d, const double *x_e,
+                           double *q0_e, void *stream);
 
 /* Arithmetic-pipe throughput probe (no reference counterpart; the pipe-side denominator of the operator roofline): one
  * launch of 8 x SMs CTAs of 256 threads, each thread running eight independent FMA chains of `iters` steps in FP64

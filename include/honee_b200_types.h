@@ -109,7 +109,7 @@ typedef struct {
   double             u[3];
 } HbTaylorGreenContext;
 
-/* qfunctions/newtonian_types.h (State: conservative then primitive values, 80 bytes) */
+/* qfunctions/newtonian_state.h:11-22 (State: conservative then primitive values, 80 bytes) */
 typedef struct {
   double density, momentum[3], E_total;
   HbStatePrimitive Y;

@@ -14,6 +14,7 @@
 #include "differential_filter.h"
 #include "grid_anisotropy_tensor.h"
 #include "mass.h"
+#include "monitor_cfl.h"
 #include "monitor_totalkineticenergy.h"
 #include "newtonian.h"
 #include "setupgeo.h"
@@ -39,6 +40,16 @@ EXPORT int ref_Mass_5(void *c, CeedInt Q, In in, Out out) { return Mass_5(c, Q, 
 EXPORT int ref_MassFunction_Newtonian_Conserv(void *c, CeedInt Q, In in, Out out) { return MassFunction_Newtonian_Conserv(c, Q, in, out); }
 EXPORT int ref_MonitorTotalKineticEnergy_Conserv(void *c, CeedInt Q, In in, Out out) { return MonitorTotalKineticEnergy_Conserv(c, Q, in, out); }
 EXPORT int ref_ICsTaylorGreen(void *c, CeedInt Q, In in, Out out) { return ICsTaylorGreen(c, Q, in, out); }
+EXPORT int ref_ICsNewtonianIG_Conserv(void *c, CeedInt Q, In in, Out out) { return ICsNewtonianIG_Conserv(c, Q, in, out); }
+EXPORT int ref_ICsNewtonianIG_Prim(void *c, CeedInt Q, In in, Out out) { return ICsNewtonianIG_Prim(c, Q, in, out); }
+EXPORT int ref_ICsNewtonianIG_Entropy(void *c, CeedInt Q, In in, Out out) { return ICsNewtonianIG_Entropy(c, Q, in, out); }
+EXPORT int ref_IC_GaussianWave_Prim(void *c, CeedInt Q, In in, Out out) { return IC_GaussianWave_Prim(c, Q, in, out); }
+EXPORT int ref_IC_GaussianWave_Entropy(void *c, CeedInt Q, In in, Out out) { return IC_GaussianWave_Entropy(c, Q, in, out); }
+EXPORT int ref_MonitorCFL_3D_Conserv(void *c, CeedInt Q, In in, Out out) { return MonitorCFL_3D_Conserv(c, Q, in, out); }
+EXPORT int ref_MonitorCFL_3D_Prim(void *c, CeedInt Q, In in, Out out) { return MonitorCFL_3D_Prim(c, Q, in, out); }
+EXPORT int ref_MonitorCFL_3D_Entropy(void *c, CeedInt Q, In in, Out out) { return MonitorCFL_3D_Entropy(c, Q, in, out); }
+EXPORT int ref_MonitorTotalKineticEnergy_Prim(void *c, CeedInt Q, In in, Out out) { return MonitorTotalKineticEnergy_Prim(c, Q, in, out); }
+EXPORT int ref_MonitorTotalKineticEnergy_Entropy(void *c, CeedInt Q, In in, Out out) { return MonitorTotalKineticEnergy_Entropy(c, Q, in, out); }
 EXPORT int ref_ICsChannel(void *c, CeedInt Q, In in, Out out) { return ICsChannel(c, Q, in, out); }
 EXPORT size_t ref_channel_ctx_size(void) { return sizeof(struct ChannelContext_); }
 EXPORT int ref_IC_GaussianWave_Conserv(void *c, CeedInt Q, In in, Out out) { return IC_GaussianWave_Conserv(c, Q, in, out); }
