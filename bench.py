@@ -283,7 +283,12 @@ def run_gpu(args, rank, world):
 
     pk, pk_kind = peaks()
     b_if, b_ij = algorithmic_bytes(N_L, N_q, E, P)
+    _, b_ij32 = algorithmic_bytes(N_L, N_q, E, P, f32=True)
+    b_diag = 8 * N_L + 8 * N_q * 24 + 4 * E * P ** 3
     achieved_if = b_if / (ms_if * 1e-3) / 1e9
+    fma64, fma32 = kern.fma_peak(True), kern.fma_peak(False)
+    sides = two_sided_roofline({"ifunction": ms_if, "ijacobian": ms_ij, "ijacobian_f32": ms_ij32, "diagonal_f64": ms_diag},
+                               {"ifunction": b_if, "ijacobian": b_ij, "ijacobian_f32": b_ij32, "diagonal_f64": b_diag}, E, pk, fma64, fma32)
     launches = 2 * op.num_colors * args.steps
     line = {
         "metric": METRIC, "value": job_gdofs(world, N_L, ms64), "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
@@ -300,10 +305,14 @@ def run_gpu(args, rank, world):
         "roofline": {"bound": "hbm", "kernel": "k_ifunction (fused IFunction, one launch per colour)", "achieved": achieved_if,
                      "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved_if / pk["hbm_gbs"], "peak_source": pk_kind,
                      "algorithmic_bytes_per_apply": b_if, "algorithmic_bytes_per_launch": b_if / op.num_colors,
-                     "traffic": IF_DRAM_BYTES_PER_ELEM * E / op.num_colors,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 4096-element k_ifunction launch "
-                                       "(32^3, P=4 Q=5), scaled by the elements of one launch here",
-                     "ijacobian": {"achieved": b_ij / (ms_ij * 1e-3) / 1e9, "frac": b_ij / (ms_ij * 1e-3) / 1e9 / pk["hbm_gbs"]}},
+                     "traffic": KERNEL_COUNTERS["ifunction"]["dram_per_elem"] * E / op.num_colors,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean of the 8 colour launches of one 64^3 apply "
+                                       "(--cache-control none, steady state), per launch",
+                     "ijacobian": {"achieved": b_ij / (ms_ij * 1e-3) / 1e9, "frac": b_ij / (ms_ij * 1e-3) / 1e9 / pk["hbm_gbs"]},
+                     "pipe_peaks": {"fp64_fma_per_s": fma64, "fp32_fma_per_s": fma32, "fp64_tflops": 2 * fma64 / 1e12,
+                                    "fp32_tflops": 2 * fma32 / 1e12,
+                                    "source": "hb_fma_peak_probe (independent FMA chains, 8 CTAs/SM), best of 5 launches, CUDA events, this run"},
+                     "two_sided": sides},
         "e2e": {"value": job_gdofs(world, N_L, ms_e2e), "unit": "GDoF/s", "h2d_bytes_per_step": 3 * 8 * N_L, "d2h_bytes_per_step": 2 * 8 * N_L,
                 "api": "CeedVectorSetArray(HOST, USE_POINTER) + CeedOperatorApply x2 + CeedVectorSyncArray(HOST)", "jacobian_rel_l2_vs_kernel": err_e2e},
         "gpu_launches": launches,
@@ -315,6 +324,93 @@ def run_gpu(args, rank, world):
         line["cpu_baseline"] = cpu_full
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_gpu_partitioned(args, rank, world):
+    """N > 1: the operator partitioned into z-slabs (weak scaling: rank r holds a size^3 slab of a size x size x (N size) box),
+    each step one ghost-plane exchange of q and q_dot, the IFunction, the ghost contributions summed into their owners, the
+    same for the Jacobian action on dq -- the exchanges of HONEE's DMGlobalToLocal / DMLocalToGlobal around every apply,
+    over NCCL point-to-point between neighbouring ranks.  value = DOF of the whole box / the slowest rank's step time."""
+    import torch
+    import torch.distributed as dist
+    kern = importlib.import_module("honee-4aiad_b200.kernels")
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    part = importlib.import_module("honee-4aiad_b200.partition")
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    n = args.size
+    slab = part.partition_box((n, n, n * world), 4, rank, world)
+    mesh, basis = slab.local, prob.tensor_basis(4, 5)
+    ctx = prob.newtonian_context(3, cv=717.5, cp=1004.5, mu=1.8e-5, k=0.0257, stab=prob.STAB_SUPG, dt=1e-5, ijacobian_time_shift=1.5e5)
+    q = prob.multimode_state(mesh, basis, ctx.gas, seed=0)
+    rng = np.random.default_rng(1 + rank)
+    q_dot, dq = q * 1e-3 * rng.uniform(-1, 1, q.shape), q * 1e-4 * rng.uniform(-1, 1, q.shape)
+    E, Q, NL, no = mesh.num_elem, basis.Q, mesh.l_size, slab.owned_size
+    cb = prob.context_bytes(ctx)
+    op = kern.ElemOp(mesh, basis)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    t_q, t_qd, t_dq = T(q), T(q_dot), T(dq)
+    t_v, t_jv = torch.empty_like(t_q), torch.empty_like(t_q)
+    t_qdata = torch.empty(E * 10 * Q ** 3, dtype=torch.float64, device=dev)
+    op.setup_qdata(T(mesh.x_elem), t_qdata)
+    t_jd = torch.empty(E * 14 * Q ** 3, dtype=torch.float64, device=dev)
+    ex = part.HaloExchange(slab, dist)
+    own_v, own_jv = torch.empty(no, dtype=torch.float64, device=dev), torch.empty(no, dtype=torch.float64, device=dev)
+
+    def step():
+        ex.global_to_local(t_q[:no], t_q)
+        ex.global_to_local(t_qd[:no], t_qd)
+        op.ifunction(cb, t_q, t_qd, t_qdata, t_v, jac_data=t_jd)
+        ex.local_to_global(t_v, own_v)
+        ex.global_to_local(t_dq[:no], t_dq)
+        op.ijacobian(cb, t_qdata, t_jd, t_dq, t_jv)
+        ex.local_to_global(t_jv, own_jv)
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        dist.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(k):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(a.elapsed_time(b) / k, world, dev)
+
+    with ClockSampler(dev.index) as clk:
+        ms = timed(step, args.steps)
+    clocks = clk.summary()
+    # end to end: this rank's owned state from pinned host memory, the exchanged step, both owned results back to the host
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a[:no])).pin_memory()  # noqa: E731
+    h_q, h_qd, h_dq = pin(q), pin(q_dot), pin(dq)
+    h_v, h_j = torch.empty(no, dtype=torch.float64).pin_memory(), torch.empty(no, dtype=torch.float64).pin_memory()
+
+    def e2e():
+        t_q[:no].copy_(h_q, non_blocking=True)
+        t_qd[:no].copy_(h_qd, non_blocking=True)
+        t_dq[:no].copy_(h_dq, non_blocking=True)
+        step()
+        h_v.copy_(own_v, non_blocking=True)
+        h_j.copy_(own_jv, non_blocking=True)
+
+    ms_e2e = timed(e2e, max(1, min(args.steps, 5)))
+    dofs = torch.tensor([float(no)], dtype=torch.float64, device=dev)
+    dist.all_reduce(dofs)
+    total = dofs.item()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": total / (ms * 1e-3) / 1e9, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: background + 8 seeded sinusoidal modes (|k|<=8, 1e-3 relative)",
+            "config": {"workload": f"{n}x{n}x{n * world} hex box in {world} z-slabs of {n}^3 elements, P=4 Q=5, Newtonian IFunction + IJacobian "
+                                   "(SUPG, conservative, FP64) with the ghost-plane exchanges of every apply", "dofs": total,
+                       "parallelism": f"z-slab element partition over {world} GPUs (NCCL point-to-point halo planes)",
+                       "l2": "inputs larger than L2 per GPU; no flush"},
+            "e2e": {"value": total / (ms_e2e * 1e-3) / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": 3 * 8 * no * world,
+                    "d2h_bytes_per_step": 2 * 8 * no * world, "api": "pinned host owned vectors -> exchange + ElemOp applies -> host"},
+            "gpu_launches": 2 * op.num_colors * args.steps, "clocks": clocks}), flush=True)
 
 
 def timeloop_leg(steps):
@@ -337,9 +433,36 @@ def timeloop_leg(steps):
     return out
 
 
-# DRAM bytes (read + write) per element of one k_ifunction<4,5> launch, from an ncu capture of a 4,096-element colour
-# launch at 32^3: 90.25 MB read + 28.65 MB written.
-IF_DRAM_BYTES_PER_ELEM = (90.252032e6 + 28.651008e6) / 4096
+# Per-element counters of the fused kernels at P=4, Q=5 (profiles/roofline_counters_64cube_P4Q5.md has the commands):
+#   pipe ops: FP64 (DFMA + DADD + DMUL) or FP32 (FFMA + FADD + FMUL) thread instructions, ncu
+#             smsp__sass_thread_inst_executed_op_{d,f}{fma,add,mul}_pred_on.sum over one apply at 32^3 / elements;
+#   dram:     dram__bytes_read.sum + dram__bytes_write.sum per element over the 8 colour launches of one apply at 64^3
+#             with --cache-control none (steady state: each launch pays for the dirty lines the previous one left).
+KERNEL_COUNTERS = {
+    "ifunction": {"pipe": "fp64", "ops_per_elem": 99330, "dram_per_elem": 39034},
+    "ijacobian": {"pipe": "fp64", "ops_per_elem": 90820, "dram_per_elem": 35388},
+    "ijacobian_f32": {"pipe": "fp32", "ops_per_elem": 88695, "dram_per_elem": 23315},
+    "diagonal_f64": {"pipe": "fp64", "ops_per_elem": 197120, "dram_per_elem": 31853},
+}
+
+
+def two_sided_roofline(ms, bytes_alg, E, pk, fma64, fma32):
+    """Per kernel: the HBM floor (algorithmic bytes / measured copy bandwidth), the arithmetic-pipe floor (thread
+    instructions / measured FMA-pipe rate; DFMA, DADD and DMUL each take one pipe slot), the binding (larger) floor and
+    the measured time's fraction of it.  fma64 / fma32: measured pipe rates in thread instructions per second."""
+    out = {}
+    for name, t_ms in ms.items():
+        k = KERNEL_COUNTERS[name]
+        t = t_ms * 1e-3
+        t_hbm = bytes_alg[name] / (pk["hbm_gbs"] * 1e9)
+        rate = fma64 if k["pipe"] == "fp64" else fma32
+        t_pipe = k["ops_per_elem"] * E / rate
+        out[name] = {"ms": t_ms, "algorithmic_bytes": bytes_alg[name], "hbm_floor_ms": t_hbm * 1e3, "hbm_frac": t_hbm / t,
+                     f"{k['pipe']}_pipe_floor_ms": t_pipe * 1e3, "pipe_frac": t_pipe / t, "pipe_ops_per_elem": k["ops_per_elem"],
+                     "binding": "hbm" if t_hbm >= t_pipe else f"{k['pipe']} pipe", "binding_floor_ms": max(t_hbm, t_pipe) * 1e3,
+                     "frac_of_binding": max(t_hbm, t_pipe) / t, "dram_traffic_per_elem": k["dram_per_elem"],
+                     "dram_traffic_over_algorithmic": k["dram_per_elem"] * E / bytes_alg[name]}
+    return out
 
 
 def parity_full(prob, mesh, basis, ctx, q, q_dot, dq, gpu, n):
@@ -425,6 +548,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank)
+        elif world > 1:
+            run_gpu_partitioned(args, rank, world)
         else:
             run_gpu(args, rank, world)
     finally:

@@ -18,6 +18,7 @@
 
 #include "honee_b200.h"
 #include "newtonian_qf.cuh"
+#include "pair_f32.cuh"
 #include "pipeline.cuh"
 #include "sgs.cuh"
 
@@ -855,6 +856,199 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
+// Mixed-precision Jacobian action on element pairs with packed FP32 arithmetic (pair_f32.cuh).  Each CTA pass takes two
+// elements of the colour (list positions 2i and 2i + 1; an odd count leaves the last pair with one element, whose second
+// lane recomputes the first and is not stored): the node values of both are gathered into the two lanes of one 8-byte
+// slot, every basis pass and the point-wise tangent run once for both lanes, and the scatter stores each lane at its own
+// element's nodes.  Same arithmetic per lane as k_ijacobian<float> (FP32 values and Jacobian data, FP64 qdata rounded to
+// FP32 at the point), half the instructions.  qdata of both elements is staged by TMA; their Jacobian data are read at
+// the point from global memory (coalesced per component, warmed in L2 one pair ahead), which keeps three CTAs per SM.
+
+struct IjacobianPairPtrs {
+  const float *dq;
+  const float *jac_data;  // [E][num_jd][Q3]
+  float *v;
+};
+
+// node gathers into one lane (byte offset 0 or 4) of the pair slots: sN [5][P][P][PX], sV [P3][5]
+template <int P, int NT>
+__device__ __forceinline__ void gather_lane_async(const EntryOffsets<P, NT> &eo, const float *l, f2 *sN, int lane) {
+  constexpr int P3 = P * P * P, PX = padded_row<P>(), PS = P * P * PX;
+#pragma unroll
+  for (int j = 0; j < EntryOffsets<P, NT>::NJ; j++) {
+    const int t = threadIdx.x + j * NT;
+    if (t < 5 * P3) {
+      const int pp = t / 5, c = t % 5, srow = (pp / P) * PX + pp % P;
+      cp_async4(reinterpret_cast<float *>(&sN[c * PS + srow]) + lane, l + eo.o[j] + c);
+    }
+  }
+}
+template <int P, int NT>
+__device__ __forceinline__ void gather_out_lane_async(const int32_t *sO, const float *l_out, f2 *sV, int lane) {
+  constexpr int P3 = P * P * P;
+  for (int t = threadIdx.x; t < 5 * P3; t += NT) cp_async4(reinterpret_cast<float *>(&sV[t]) + lane, l_out + sO[t]);
+}
+
+template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
+__global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ijacobian_pair(const ElemArgs<f2> a, const IjacobianPairPtrs p) {
+  constexpr int NT = nthreads_for<float>(Q);
+  using L = Plan<P, Q, 1, f2, false, false>;
+  constexpr int Q3 = L::Q3, P3 = L::P3;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  f2 *sm = reinterpret_cast<f2 *>(smem_raw);
+  f2 *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
+  f2 *sW1 = sU + 5 * Q3;
+  double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);  // [2][10][Q3]: the pair's qdata
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + 2 * sizeof(double) * 10 * Q3);
+  __shared__ int s_bail;
+  __shared__ int32_t sO[2][2][5 * P3];  // entry offsets of the current / next pair, per lane
+  const unsigned qd_bytes = sizeof(double) * 10 * Q3;
+  const int njd = a.num_jd;
+  const int npairs = (a.n_elems + 1) / 2;
+  // element ids of pair i: list positions 2i and 2i + 1 (the second repeats the first when the count is odd)
+  auto pair_elems = [&](int i, int &eA, int &eB, int &hasB) {
+    eA = a.elems[2 * i];
+    hasB = 2 * i + 1 < a.n_elems;
+    eB = hasB ? a.elems[2 * i + 1] : eA;
+  };
+  auto stage_qdata = [&](int eA, int eB) {  // thread 0: both elements' qdata by TMA on one mbarrier phase
+    mbar_arrive_expect_tx(mbar, 2 * qd_bytes);
+    tma_load_1d(sQD, a.qdata + (int64_t)eA * 10 * Q3, qd_bytes, mbar);
+    tma_load_1d(sQD + 10 * Q3, a.qdata + (int64_t)eB * 10 * Q3, qd_bytes, mbar);
+  };
+  auto warm_jd = [&](int eA, int eB) {
+    prefetch_l2_bulk(p.jac_data + (int64_t)eA * njd * Q3, sizeof(float) * njd * Q3);
+    prefetch_l2_bulk(p.jac_data + (int64_t)eB * njd * Q3, sizeof(float) * njd * Q3);
+  };
+
+  if (threadIdx.x == 0) {
+    mbar_init(mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_bail = 0;
+  }
+  __syncthreads();
+  int idx = blockIdx.x;
+  if (idx >= npairs) return;
+  const int G = gridDim.x;
+  int buf = 0;
+  int eA, eB, hasB;
+  pair_elems(idx, eA, eB, hasB);
+  {  // prologue: stage the first pair
+    EntryOffsets<P, NT> oa, ob;
+    oa.load(a.offsets, eA);
+    ob.load(a.offsets, eB);
+    oa.store(sO[0][0]);
+    ob.store(sO[0][1]);
+    gather_lane_async<P, NT>(oa, p.dq, sN, 0);
+    gather_lane_async<P, NT>(ob, p.dq, sN, 1);
+    if (threadIdx.x == 0) {
+      stage_qdata(eA, eB);
+      warm_jd(eA, eB);
+    }
+    cp_async_commit();
+    __syncthreads();
+    gather_out_lane_async<P, NT>(sO[0][0], p.v, sV, 0);
+    gather_out_lane_async<P, NT>(sO[0][1], p.v, sV, 1);
+    cp_async_commit();
+  }
+  unsigned phase = 0;
+  int nA = -1, nB = -1, nhasB = 0;
+  if (idx + G < npairs) pair_elems(idx + G, nA, nB, nhasB);
+  EntryOffsets<P, NT> nxa, nxb;
+  if (nA >= 0) {
+    nxa.load(a.offsets, nA);
+    nxb.load(a.offsets, nB);
+  }
+  for (; idx < npairs; idx += G) {
+    const int cA = eA, cB = eB, chasB = hasB;
+    cp_async_wait_group<1>();
+    if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
+      s_bail = 1;
+      atomicOr(a.status, 1);
+    }
+    __syncthreads();
+    if (s_bail) break;
+    phase ^= 1;
+    if (nA >= 0 && threadIdx.x == 0) warm_jd(nA, nB);
+    pass_x_staged<P, Q, 5, NT, f2>(a.basis, sN, s1);
+    __syncthreads();
+    if (nA >= 0) {
+      gather_lane_async<P, NT>(nxa, p.dq, sN, 0);
+      gather_lane_async<P, NT>(nxb, p.dq, sN, 1);
+      cp_async_commit();
+      nxa.store(sO[buf ^ 1][0]);
+      nxb.store(sO[buf ^ 1][1]);
+    }
+    forward_yz<P, Q, 5, NT, f2>(a.basis, s1, s2, sU, sG);
+    const int q = threadIdx.x;
+    if (q < Q3) {
+      f2 dq[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5], jd[15];
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        dq[c] = sU[c * Q3 + q];
+#pragma unroll
+        for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
+      }
+      const float *jA = p.jac_data + (int64_t)cA * njd * Q3 + q, *jB = p.jac_data + (int64_t)cB * njd * Q3 + q;
+#pragma unroll
+      for (int c = 0; c < 14; c++) jd[c] = f2(__ldg(jA + c * Q3), __ldg(jB + c * Q3));
+      jd[14] = njd > 14 ? f2(__ldg(jA + 14 * Q3), __ldg(jB + 14 * Q3)) : f2(0.0);
+      const double *qA = sQD + q, *qB = sQD + 10 * Q3 + q;
+      wdetJ = f2(float(qA[0]), float(qB[0]));
+#pragma unroll
+      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = f2(float(qA[(1 + k) * Q3]), float(qB[(1 + k) * Q3]));
+      ijacobian_point_stream<f2, SV>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        sU[c * Q3 + q] = v[c];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sG[(d * 5 + c) * Q3 + q] = gv[d][c];
+      }
+    }
+    __syncthreads();
+    if (nA >= 0) {
+      if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        stage_qdata(nA, nB);
+      }
+      cp_async_commit();
+    }
+    transpose_passes<P, Q, NT, f2>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
+    if (nA >= 0) cp_async_wait_group<2>();
+    else cp_async_wait_group<0>();
+    __syncthreads();
+    {  // scatter: elements of one colour share no node; each lane to its own element
+      const int32_t *oA = sO[buf][0], *oB = sO[buf][1];
+      for (int t = threadIdx.x; t < 5 * P3; t += NT) {
+        const f2 r = sV[t] + s2[t];
+        p.v[oA[t]] = r.x();
+        if (chasB) p.v[oB[t]] = r.y();
+      }
+    }
+    __syncthreads();
+    buf ^= 1;
+    if (nA >= 0) {
+      gather_out_lane_async<P, NT>(sO[buf][0], p.v, sV, 0);
+      gather_out_lane_async<P, NT>(sO[buf][1], p.v, sV, 1);
+      cp_async_commit();
+    }
+    eA = nA;
+    eB = nB;
+    hasB = nhasB;
+    if (idx + 2 * G < npairs) {
+      pair_elems(idx + 2 * G, nA, nB, nhasB);
+      nxa.load(a.offsets, nA);
+      nxb.load(a.offsets, nB);
+    } else {
+      nA = nB = -1;
+      nhasB = 0;
+    }
+  }
+  cp_async_wait_all();
+  if (s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
 // Diagonal of the IJacobian operator (libCEED CeedOperatorLinearAssembleDiagonal semantics): at every quadrature point
 // linearise the point-wise Jacobian for each component c with unit inputs in the four eval modes (interp, grad x/y/z),
 // keep the 4x4 block A_c[m][n] = d out(m,c) / d in(n,c), and contract sum_q phi_m(q,p) A_c[m][n](q) phi_n(q,p) by sum
@@ -1304,6 +1498,32 @@ template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v,
                             cudaStream_t s) {
   return launch_ijacobian_v<P, Q, T, true, SV>(op, ctx, qdata, jd, dq, v, s);
+}
+
+// The paired FP32 Jacobian (two elements of a colour per CTA pass, packed FP32): needs qdata 16-byte aligned (TMA).
+template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
+static int launch_ijacobian_pair(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *jd, const float *dq, float *v,
+                                 cudaStream_t s) {
+  using L = Plan<P, Q, 1, f2, false, false>;
+  const size_t sm = L::qd_offset_bytes + 2 * sizeof(double) * 10 * L::Q3 + 16;
+  if (cudaFuncSetAttribute(k_ijacobian_pair<P, Q, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
+  IjacobianPairPtrs p;
+  p.dq = dq;
+  p.jac_data = jd;
+  p.v = v;
+  for (int c = 0; c < op->num_colors; c++) {
+    ElemArgs<f2> a = make_args<f2>(op, ctx, qdata, c);
+    if (a.n_elems == 0) continue;
+    const int npairs = (a.n_elems + 1) / 2;
+    k_ijacobian_pair<P, Q, SV><<<grid_for(op, npairs, k_ijacobian_pair<P, Q, SV>, nthreads_for<float>(Q), sm), nthreads_for<float>(Q), sm, s>>>(a, p);
+  }
+  return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
+}
+
+template <int P, int Q, int SV>
+static int pair_case(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *jd, const float *dq, float *v, cudaStream_t s) {
+  if constexpr (Q <= 6) return launch_ijacobian_pair<P, Q, SV>(op, ctx, qdata, jd, dq, v, s);
+  return launch_ijacobian<P, Q, float, SV>(op, ctx, qdata, jd, dq, v, s);
 }
 
 template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
@@ -1868,6 +2088,14 @@ extern "C" int hb_ifunction_apply_sgs(const HbElemOp *op, const void *ctx184, co
 
 template <typename T, int SV>
 static int ijacobian_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4 && SV == HB_STATEVAR_CONSERVATIVE) {  // FP32: element pairs in packed FP32 where the basis allows
+    if (((uintptr_t)qdata % 16) == 0 && op->Q <= 6) {
+#define HB_CASE(PP, QQ) \
+  if (op->P == PP && op->Q == QQ) return pair_case<PP, QQ, SV>(op, ctx, qdata, (const float *)jd, (const float *)dq, (float *)v, s);
+      HB_PQ_LIST(HB_CASE)
+#undef HB_CASE
+    }
+  }
 #define HB_CASE(PP, QQ) \
   if (op->P == PP && op->Q == QQ) return launch_ijacobian<PP, QQ, T, SV>(op, ctx, qdata, jd, dq, v, s);
   if constexpr (SV == HB_STATEVAR_CONSERVATIVE) {
