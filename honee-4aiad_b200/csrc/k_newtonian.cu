@@ -444,7 +444,7 @@ __device__ __forceinline__ void scatter_store(const int32_t *sO, const T *sV, co
 //   sU  [10][Q3]        interpolated values (q, then q_dot or w1); point-wise outputs v in place
 //   sG  [15][Q3]        reference gradients; point-wise fluxes in place; later sT1
 //   sJD [15][Q3]        staged stored Jacobian data (IJacobian only)
-//   sQD [10][Q3] double staged qdata
+//   sQD [10][Q3] double staged qdata (the residual keeps two: element i and element i + 1)
 template <int P, int Q, int NV, typename T, bool JD, bool ST = true>
 struct Plan {
   static constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
@@ -458,7 +458,8 @@ struct Plan {
   static constexpr int oN = 0, oV = pad(oN + nN), o1 = pad(oV + nV), o2 = pad(o1 + n1), oU = pad(o2 + n2), oG = pad(oU + nU),
                        oJD = pad(oG + nG), end_T = pad(oJD + nJD);
   static constexpr size_t qd_offset_bytes = ((size_t)end_T * sizeof(T) + 15) & ~(size_t)15;
-  static constexpr size_t mbar_offset = qd_offset_bytes + (ST ? sizeof(double) * 10 * Q3 : 0);  // staged qdata precedes it
+  // staged qdata precedes the mbarriers: two buffers for the residual (NV == 2), one for the Jacobian
+  static constexpr size_t mbar_offset = qd_offset_bytes + (ST ? (NV == 2 ? 2 : 1) * sizeof(double) * 10 * Q3 : 0);
   static constexpr size_t bytes = mbar_offset + 16;
   static_assert(5 * P * Q2 <= n1, "sT2 fits in s1");
   static_assert(5 * Q3 <= n2, "w2 fits in s2");
@@ -568,6 +569,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
 
   if (threadIdx.x == 0) {
     mbar_init(mbar, 1);
+    mbar_init(mbar + 1, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_bail = 0;
   }
@@ -585,16 +587,20 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     eo.load(a.offsets, e0);
     eo.store(sO[0]);
     gather_async<P, 2, NT, double>(eo, p.q, p.q_dot, sN);
-    if constexpr (ST) {
+    if constexpr (ST) {  // qdata of the first two elements, one buffer each
       if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
       stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+      if (idx + (int)gridDim.x < a.n_elems) {
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar + 1, p.qdata_tma ? qd_bytes : 0);
+        stage_block<double, NT>(sQD + 10 * Q3, a.qdata + (int64_t)a.elems[idx + gridDim.x] * 10 * Q3, 10 * Q3, p.qdata_tma, mbar + 1);
+      }
     } else if (threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)e0 * 10 * Q3, qd_bytes);
     cp_async_commit();
     __syncthreads();
     gather_out_async<P, NT, double>(sO[0], p.v, sV);
     cp_async_commit();
   }
-  unsigned phase = 0;
+  unsigned kit = 0;  // elements done by this CTA: qdata buffer kit & 1, its mbarrier phase parity (kit >> 1) & 1
   // element ids and entry offsets are read two elements ahead so no global load latency sits on the critical path
   const int G = gridDim.x;
   int ecur = a.elems[idx];
@@ -612,16 +618,15 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     // everything but the most recent group (the output gather, only needed at the scatter) has landed
     cp_async_wait_group<1>();
     HB_PT(8)
-    if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
+    if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar + (kit & 1), (kit >> 1) & 1)) {
       s_bail = 1;
       atomicOr(a.status, 1);
     }
     HB_PT(9)
     __syncthreads();
     if (s_bail) break;
-    phase ^= 1;
     HB_PT(0)
-    if (en >= 0 && threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, qd_bytes);
+    if (en2 >= 0 && threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)en2 * 10 * Q3, qd_bytes);
     pass_x_staged<P, Q, 10, NT, double>(a.basis, sN, s1);
     __syncthreads();
     HB_PT(1)
@@ -642,7 +647,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
 #pragma unroll
         for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
-      const double *qdp = ST ? sQD : a.qdata + (int64_t)e * 10 * Q3;
+      const double *qdp = ST ? sQD + (kit & 1) * 10 * Q3 : a.qdata + (int64_t)e * 10 * Q3;
       wdetJ = qdp[q];
 #pragma unroll
       for (int k = 0; k < 9; k++) X[k / 3][k % 3] = qdp[(1 + k) * Q3 + q];
@@ -669,13 +674,26 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     }
     __syncthreads();
     HB_PT(3)
-    if (en >= 0) {  // sQD consumed: stage the next element's qdata
-      if constexpr (ST) {
-        if (threadIdx.x == 0) {
-          fence_proxy_async_smem();
-          mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
+    if (en2 >= 0) {  // warm L2 for the element after next: its node rows of q, q_dot and v (its qdata follows below)
+#pragma unroll
+      for (int j = 0; j < EntryOffsets<P, NT>::NJ; j++) {
+        const int t = threadIdx.x + j * NT;
+        if (t < 5 * L::P3 && t % 5 == 0) {
+          prefetch_l2(p.q + nxt2.o[j]);
+          prefetch_l2(p.q_dot + nxt2.o[j]);
+          prefetch_l2(p.v + nxt2.o[j]);
         }
-        stage_block<double, NT>(sQD, a.qdata + (int64_t)en * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
+      }
+    }
+    if (en >= 0) {  // this qdata buffer consumed: stage the qdata of the element after next into it
+      if constexpr (ST) {
+        if (en2 >= 0) {
+          if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(mbar + (kit & 1), p.qdata_tma ? qd_bytes : 0);
+          }
+          stage_block<double, NT>(sQD + (kit & 1) * 10 * Q3, a.qdata + (int64_t)en2 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar + (kit & 1));
+        }
       }
       cp_async_commit();
     }
@@ -700,11 +718,15 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     en = en2;
     en2 = en3;
     nxt = nxt2;
+    kit++;
     HB_PT(6)
   }
   HB_PT_FLUSH(0)
   cp_async_wait_all();
-  if (ST && s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);  // let an outstanding bulk copy land before exit
+  if (ST && s_bail && threadIdx.x == 0) {  // let outstanding bulk copies land before exit (bounded waits)
+    mbar_wait_bounded(mbar + (kit & 1), (kit >> 1) & 1);
+    mbar_wait_bounded(mbar + ((kit + 1) & 1), ((kit + 1) >> 1) & 1);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -786,9 +808,9 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
     __syncthreads();
     if (s_bail) break;
     phase ^= 1;
-    if (en >= 0 && threadIdx.x == 0) {
-      prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, qd_bytes);
-      prefetch_l2_bulk(p.jac_data + (int64_t)en * njd * Q3, jd_bytes);
+    if (en2 >= 0 && threadIdx.x == 0) {  // warm L2 for the element after next (its own staging follows the next point phase)
+      prefetch_l2_bulk(a.qdata + (int64_t)en2 * 10 * Q3, qd_bytes);
+      prefetch_l2_bulk(p.jac_data + (int64_t)en2 * njd * Q3, jd_bytes);
     }
     pass_x_staged<P, Q, 5, NT, T>(a.basis, sN, s1);
     __syncthreads();
@@ -824,6 +846,16 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
       }
     }
     __syncthreads();
+    if (en2 >= 0) {  // and the node rows of dq and v of the element after next
+#pragma unroll
+      for (int j = 0; j < EntryOffsets<P, NT>::NJ; j++) {
+        const int t = threadIdx.x + j * NT;
+        if (t < 5 * L::P3 && t % 5 == 0) {
+          prefetch_l2(p.dq + nxt2.o[j]);
+          prefetch_l2(p.v + nxt2.o[j]);
+        }
+      }
+    }
     if (en >= 0) {
       if constexpr (ST) {
         if (threadIdx.x == 0) {

@@ -32,16 +32,8 @@ struct f2 {
     r = (unsigned long long)ua | ((unsigned long long)ub << 32);
 #endif
   }
-  __device__ __forceinline__ float x() const {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-    return a;
-  }
-  __device__ __forceinline__ float y() const {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-    return b;
-  }
+  __device__ __forceinline__ float x() const { return __uint_as_float((unsigned)(r & 0xffffffffull)); }
+  __device__ __forceinline__ float y() const { return __uint_as_float((unsigned)(r >> 32)); }
 };
 
 __device__ __forceinline__ f2 f2_raw(unsigned long long r) {

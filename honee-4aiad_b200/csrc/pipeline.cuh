@@ -61,6 +61,9 @@ __device__ __forceinline__ void tma_load_1d(void *dst, const void *src, unsigned
                : "memory");
 }
 
+// warm L2 with the 128-byte line holding p
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ void prefetch_l2_bulk(const void *p, size_t bytes) {
   const uintptr_t a = (uintptr_t)p, lo = (a + 15) & ~(uintptr_t)15, hi = (a + bytes) & ~(uintptr_t)15;
   if (hi > lo) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");

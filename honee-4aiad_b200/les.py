@@ -95,22 +95,28 @@ def run_steps(m: TGMesh, dt, n_steps, every, mixed=True, sgs=None, on_snapshot=N
     return rows, seconds
 
 
-def _max_rel_err(rows, ref, key, scale, from_start=False):
-    """max over the monitored times after t = 0 of |a - b| / scale; from_start compares the changes since t = 0."""
-    n = min(len(rows), len(ref))
+def _max_rel_err(rows, ref, key, scale, from_start=False, upto=None):
+    """max over the monitored times after t = 0 (up to row `upto`) of |a - b| / scale; from_start compares the changes
+    since t = 0."""
+    n = min(len(rows), len(ref), (upto + 1) if upto else 1 << 30)
     a0, b0 = (rows[0][key], ref[0][key]) if from_start else (0.0, 0.0)
     return max(abs((rows[k][key] - a0) - (ref[k][key] - b0)) for k in range(1, n)) / scale
 
 
 def study(fine_faces=96, coarse_faces=24, degree=2, t_end=2.0, snaps=4, cfl=1.0, train_steps=4000, batch=65536, lr=1e-3, seed=0,
-          clip=1e-3, implicit_closure=False, coarse_substeps=1, cache=None, clamp_outputs=False, no_backscatter=True, log=None):
+          clip=1e-3, implicit_closure=False, coarse_substeps=1, cache=None, clamp_outputs=False, no_backscatter=True, log=None, scales=None):
     """implicit_closure: the closure inside Newton with matrix-free Krylov products (FP64); by default it is evaluated once
     per step at the previous state (explicit, mixed-precision Krylov).  coarse_substeps divides the coarse step of both
     coarse runs.  cache: a directory where the fine-run products (filtered monitors, injected initial state, trained
     model) are stored after stages 1-3 and reused by later calls with the same fine configuration.  clamp_outputs and
     no_backscatter select the inference limiters of the fused closure (HbMlpDesc; both off = the reference's evaluation).
     Backscatter limiting is on by default: without it the trained closure fed energy into the resolved scales of the 24^3
-    Taylor-Green run and the run diverged near t = 1.5 at every time step tried."""
+    Taylor-Green run and the run diverged near t = 1.5 at every time step tried.
+
+    scales: candidate stress scales gamma (each multiplies the de-normalisation bounds, so the modelled stress scales by
+    gamma).  With candidates, every scale runs the coarse closure and the one whose worst error ratio to the plain coarse
+    run is smallest on the first half of the snapshots (validation) is kept; the reported errors cover all snapshots.
+    Without, the trained model is used as it is (gamma = 1)."""
     import os
     import torch
 
@@ -148,22 +154,54 @@ def study(fine_faces=96, coarse_faces=24, degree=2, t_end=2.0, snaps=4, cfl=1.0,
             np.savez(cpath, meta=json.dumps(meta), weights=weights, bounds=bounds, q_inject=q_inject[0].cpu().numpy())
     out["weights"] = np.asarray(weights).tolist()
 
-    d = SG.desc(20, 20, 0.0, bounds, clamp_outputs=clamp_outputs, no_backscatter=no_backscatter)
     out["limiters"] = {"clamp_outputs": bool(clamp_outputs), "no_backscatter": bool(no_backscatter)}
 
     # 4. coarse runs without and with the closure (same step, from the same filtered initial state)
     dt_cs, n_cs, every_cs = dt_c / coarse_substeps, n_c * coarse_substeps, every_c * coarse_substeps
     out["coarse_dt"], out["coarse_steps"] = dt_cs, n_cs
     rows_c0, sec_c0 = run_steps(coarse, dt_cs, n_cs, every_cs, mixed=True, q0=q_inject[0])
-    try:
-        rows_c1, sec_c1 = run_steps(coarse, dt_cs, n_cs, every_cs, mixed=not implicit_closure, sgs=(d, np.asarray(weights, dtype=np.float32)),
-                                    q0=q_inject[0], jfnk=int(implicit_closure))
-        diverged = None
-    except RuntimeError as e:
-        rows_c1, sec_c1, diverged = [], float("nan"), str(e)
     out["coarse_plain"] = {"gpu_seconds": sec_c0, "rows": rows_c0}
+
+    def closure_run(gamma):
+        d = SG.desc(20, 20, 0.0, np.asarray(bounds) * gamma, clamp_outputs=clamp_outputs, no_backscatter=no_backscatter)
+        try:
+            rows, sec = run_steps(coarse, dt_cs, n_cs, every_cs, mixed=not implicit_closure, sgs=(d, np.asarray(weights, dtype=np.float32)),
+                                  q0=q_inject[0], jfnk=int(implicit_closure))
+            return rows, sec, None
+        except RuntimeError as e:
+            return [], float("nan"), str(e)
+
+    half = max(1, snaps // 2)
+    if scales:
+        cands = []
+        for g in scales:
+            rows, sec, div = closure_run(float(g))
+            score = None
+            if div is None:
+                ev = _errors(ref_rows, rows, upto=half)
+                e0 = _errors(ref_rows, rows_c0, upto=half)
+                score = max(ev[k] / e0[k] for k in ev)
+            cands.append({"gamma": float(g), "diverged": div, "validation_worst_error_ratio": score, "rows": rows, "gpu_seconds": sec})
+            say(stage="closure scale", gamma=g, diverged=div, score=score)
+        ok = [c for c in cands if c["diverged"] is None]
+        best = min(ok, key=lambda c: c["validation_worst_error_ratio"]) if ok else cands[-1]
+        out["scale_selection"] = {"validation_snapshots": half, "candidates": [{k: v for k, v in c.items() if k != "rows"} for c in cands],
+                                  "chosen_gamma": best["gamma"]}
+        rows_c1, sec_c1, diverged = best["rows"], best["gpu_seconds"], best["diverged"]
+    else:
+        rows_c1, sec_c1, diverged = closure_run(1.0)
     out["coarse_closure"] = {"gpu_seconds": sec_c1, "rows": rows_c1, "diverged": diverged, "implicit": bool(implicit_closure)}
     return _compare(out, ref_rows, rows_c0, rows_c1, sec_f, sec_c1)
+
+
+def _errors(ref_rows, rows, upto=None):
+    """KE, KE-decay and resolved-dissipation errors of a coarse run against the filtered fine rows."""
+    ke0 = ref_rows[0]["TotalKineticEnergy"]
+    eps_scale = max(abs(r["StrainDissipation"]) for r in ref_rows)
+    return {"ke_err": _max_rel_err(rows, ref_rows, "TotalKineticEnergy", ke0, upto=upto),
+            "ke_decay_err": _max_rel_err(rows, ref_rows, "TotalKineticEnergy", max(ke0 - r["TotalKineticEnergy"] for r in ref_rows),
+                                         from_start=True, upto=upto),
+            "dissipation_err": _max_rel_err(rows, ref_rows, "StrainDissipation", eps_scale, upto=upto)}
 
 
 def _fine_and_train(out, coarse, fine_faces, degree, ratio, dt_f, n_f, every_f, clip, seed, batch, lr, train_steps, say):
@@ -233,16 +271,11 @@ def _fine_and_train(out, coarse, fine_faces, degree, ratio, dt_f, n_f, every_f, 
 
 def _compare(out, ref_rows, rows_c0, rows_c1, sec_f, sec_c1):
     """errors of both coarse runs against the filtered fine solution at the snapshot times"""
-    ke0 = ref_rows[0]["TotalKineticEnergy"]
-    eps_scale = max(abs(r["StrainDissipation"]) for r in ref_rows)
     res = {}
     for name, rows in (("plain", rows_c0), ("closure", rows_c1)):
         if len(rows) < 2:
             continue
-        res[name] = {"ke_err": _max_rel_err(rows, ref_rows, "TotalKineticEnergy", ke0),
-                     "ke_decay_err": _max_rel_err(rows, ref_rows, "TotalKineticEnergy", max(ke0 - r["TotalKineticEnergy"] for r in ref_rows),
-                                                  from_start=True),
-                     "dissipation_err": _max_rel_err(rows, ref_rows, "StrainDissipation", eps_scale)}
+        res[name] = _errors(ref_rows, rows)
     out["errors_vs_filtered_fine"] = res
     out["cost_ratio_fine_over_closure"] = sec_f / sec_c1 if sec_c1 == sec_c1 and sec_c1 > 0 else None
     return out
@@ -266,14 +299,16 @@ def main(argv=None):
     ap.add_argument("--clamp-outputs", action="store_true", help="limit the network outputs to the training range")
     ap.add_argument("--backscatter", action="store_true", help="keep the model's stress where tau : S > 0 (the reference's evaluation)")
     ap.add_argument("--out", default=None, help="write the full result (monitor rows, loss history, weights) as JSON here")
+    ap.add_argument("--scales", default=None, help="comma-separated candidate stress scales, chosen on the first half of the snapshots")
     a = ap.parse_args(argv)
     res = study(a.fine_faces, a.coarse_faces, a.degree, a.t_end, a.snaps, a.cfl, a.train_steps, a.batch, a.lr, a.seed,
                 implicit_closure=a.implicit_closure, coarse_substeps=a.coarse_substeps, cache=a.cache, clamp_outputs=a.clamp_outputs,
-                no_backscatter=not a.backscatter, log=sys.stderr)
+                no_backscatter=not a.backscatter, log=sys.stderr, scales=[float(v) for v in a.scales.split(",")] if a.scales else None)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(res, f)
     summary = {k: v for k, v in res.items() if k not in ("weights", "fine", "coarse_plain", "coarse_closure", "filtered_fine", "training")}
+    summary["cost_ratio_fine_over_plain"] = res["fine"]["gpu_seconds"] / res["coarse_plain"]["gpu_seconds"]
     summary["fine_gpu_seconds"] = res["fine"]["gpu_seconds"]
     summary["coarse_plain_gpu_seconds"] = res["coarse_plain"]["gpu_seconds"]
     summary["coarse_closure_gpu_seconds"] = res["coarse_closure"]["gpu_seconds"]

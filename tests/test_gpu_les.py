@@ -1,7 +1,7 @@
 """End-to-end GPU test of the learned closure at reduced size: a fine plain run,
 differential filter, training pairs, GPU training of the 6-20-20-6 network, and two coarse runs from the filtered
 initial state.  The closure must beat the closure-free coarse run against the filtered fine solution on the kinetic
-energy decay and on the resolved dissipation, at lower GPU cost than the fine run."""
+energy, its decay and the resolved dissipation, at no more than a fifth of the fine run's GPU time."""
 import importlib
 
 import pytest
@@ -19,4 +19,4 @@ def test_learned_closure_beats_the_plain_coarse_run():
     assert e["closure"]["ke_err"] < e["plain"]["ke_err"], e
     assert e["closure"]["dissipation_err"] < e["plain"]["dissipation_err"], e
     assert r["training"]["loss"][-1][1] < 0.1 * r["training"]["loss"][0][1]
-    assert r["fine"]["gpu_seconds"] > r["coarse_closure"]["gpu_seconds"]
+    assert r["fine"]["gpu_seconds"] >= 5 * r["coarse_closure"]["gpu_seconds"], (r["fine"]["gpu_seconds"], r["coarse_closure"]["gpu_seconds"])
