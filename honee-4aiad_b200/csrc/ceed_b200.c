@@ -140,7 +140,13 @@ enum {
   PLAN_MASS_STAB,
   PLAN_ICS,     /* initial condition at the solution nodes (src/setuplibceed.c:143-175) */
   PLAN_MON_KE,  /* MonitorTotalKineticEnergy_* per-point integrands (src/monitor_totalkineticenergy.c:80-103) */
-  PLAN_MON_CFL  /* MonitorCFL_3D_* per-point CFL numbers (src/monitor_cfl.c:60-110) */
+  PLAN_MON_CFL, /* MonitorCFL_3D_* per-point CFL numbers (src/monitor_cfl.c:60-110) */
+  PLAN_MASS_N,  /* Mass_N on N != 5 node-interleaved fields (src/honee-mass.c:20-60) */
+  PLAN_VELGRAD, /* VelocityGradientProjectionRHS_* (src/velocity_gradient_projection.c:61-103) */
+  PLAN_ANISO,   /* AnisotropyTensorProjection (src/grid_anisotropy_tensor.c:49-69) */
+  PLAN_INV_MULT,/* InverseMultiplicity (src/inverse_multiplicity.c:63-73) */
+  PLAN_SGS_NODAL, /* ComputeSgsDDNodal_* (problems/sgs_dd_model.c:149-185) */
+  PLAN_SGS_IF   /* IFunction_NodalSgs_* (problems/sgs_dd_model.c:533-550) */
 };
 
 struct CeedOperator_private {
@@ -164,6 +170,8 @@ struct CeedOperator_private {
   int       flux_type;                /* 0 HLL, 1 HLLC */
   double   *d_tmp_e2;                 /* output E-vector of the initial-condition and monitor operators */
   int       ic_kind, ic_state_var;    /* initial-condition QFunction (HB_IC_*) and the state variable it writes */
+  int       nc, state_var;            /* fields of a Mass_N operator; state variable of the nodal SGS operators */
+  double   *d_node_w;                 /* per-node weight of the nodal SGS closure (transposed inverse multiplicity) */
 };
 
 struct CeedContextFieldLabel_private {
@@ -1402,6 +1410,8 @@ int CeedOperatorSetField(CeedOperator op, const char *field_name, CeedElemRestri
   cudaFree(op->d_tmp_e);
   cudaFree(op->d_tmp_pb32);
   cudaFree(op->d_tmp_e2);
+  cudaFree(op->d_node_w);
+  op->d_node_w = NULL;
   op->d_tmp_pb32 = NULL;
   op->d_zero = op->d_tmp_rhs = op->d_tmp_e = op->d_tmp_e2 = NULL;
   op->d_tmp_in32 = op->d_tmp_out32 = NULL;
@@ -1691,6 +1701,186 @@ static int plan_monitor(CeedOperator op, int ke, int sv) {
   return CEED_ERROR_SUCCESS;
 }
 
+/* ---- nodal data-driven SGS pipeline (problems/sgs_dd_model.c:98-200, 508-560, 645-737) ----------------------------------
+ * Every field of these operators lives on one node set: the state (5 fields), the velocity gradient (9), the anisotropy
+ * tensor (7) and the SGS stress (6) each come from a clone of the solution DM (DMSetupByOrder_FEM with the solution's
+ * degree, src/velocity_gradient_projection.c:12-36, src/grid_anisotropy_tensor.c:23-45, problems/sgs_dd_model.c:75-96), so
+ * their restrictions number the nodes alike and differ only in the fields per node.  The plans check exactly that. */
+
+/* a node restriction of nc node-interleaved fields: offsets node * nc (comp_stride 1) */
+static int node_rstr(CeedElemRestriction r, int nc) {
+  return r && r != CEED_ELEMRESTRICTION_NONE && !r->strided && r->num_comp == nc && r->comp_stride == 1 && r->l_size % nc == 0;
+}
+
+/* 1 when restrictions a (na fields) and b (nb fields) put every element node on the same node */
+static int same_nodes(CeedElemRestriction a, int na, CeedElemRestriction b, int nb) {
+  if (a->num_elem != b->num_elem || a->elem_size != b->elem_size || a->l_size / na != b->l_size / nb) return 0;
+  const int64_t n = (int64_t)a->num_elem * a->elem_size;
+  for (int64_t i = 0; i < n; i++)
+    if (a->h_off[i] % na || b->h_off[i] % nb || a->h_off[i] / na != b->h_off[i] / nb) return 0;
+  return 1;
+}
+
+/* the element operator of an nc-field node restriction and its basis: offsets rewritten as node * 5 */
+static int plan_elemop_nc(CeedOperator op, CeedElemRestriction r, CeedBasis b, int nc, const char *what) {
+  if (nc == 5) {
+    if (!is_tensor3(b, 5)) return plan_fail(op, "state basis must be a 3D tensor H1 basis with 5 components");
+    return plan_elemop(op, r, b);
+  }
+  char why[160];
+  snprintf(why, sizeof why, "%s needs a %d-component node restriction (comp_stride 1) and a 3D tensor basis with %d components", what, nc, nc);
+  if (!node_rstr(r, nc) || !is_tensor3(b, nc) || r->elem_size != b->P1d * b->P1d * b->P1d) return plan_fail(op, why);
+  if (op->eop) return CEED_ERROR_SUCCESS;
+  const int64_t n   = (int64_t)r->num_elem * r->elem_size;
+  int32_t      *off = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n ? n : 1));
+  if (!off) return CeedError(op->ceed, CEED_ERROR_BACKEND, "out of host memory");
+  for (int64_t i = 0; i < n; i++) {
+    if (r->h_off[i] % nc) {
+      free(off);
+      return plan_fail(op, why);
+    }
+    off[i] = (r->h_off[i] / nc) * 5;
+  }
+  const int rc = hb_elemop_create(r->num_elem, b->P1d, b->Q1d, off, (r->l_size / nc) * 5, b->interp1d, b->grad1d, b->qref1d, b->qweight1d, &op->eop);
+  free(off);
+  HB_CK(op->ceed, rc);
+  ceed_register_op(op->ceed, op->eop);
+  return CEED_ERROR_SUCCESS;
+}
+
+/* "Mass_<N>" (src/honee-mass.c:20-60): u (INTERP, N) and qdata (NONE) -> v (INTERP, N) */
+static int plan_mass_n(CeedOperator op, int nc) {
+  CeedQFunction qf = op->qf;
+  if (qf->nin != 2 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[0].size != nc || qf->in[1].emode != CEED_EVAL_NONE ||
+      qf->in[1].size != 10 || qf->out[0].emode != CEED_EVAL_INTERP || qf->out[0].size != nc)
+    return plan_fail(op, "unexpected Mass_N field layout (src/honee-mass.c:58-60)");
+  if (op->in[0].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "u and v must be active");
+  if (op->in[0].r != op->out[0].r || op->in[0].b != op->out[0].b) return plan_fail(op, "u and v must share restriction and basis");
+  CK(plan_elemop_nc(op, op->in[0].r, op->in[0].b, nc, "the mass operator"));
+  CK(check_qdata_rstr(op, op->in[1].r, 10, op->eop->Q * op->eop->Q * op->eop->Q, "qdata"));
+  op->nc   = nc;
+  op->plan = PLAN_MASS_N;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* "VelocityGradientProjectionRHS_*": q (INTERP), Grad_q (GRAD), qdata (NONE), x (INTERP, unused by the point function)
+ * -> velocity gradient (INTERP, 9) */
+static int plan_velgrad(CeedOperator op, int sv) {
+  CeedQFunction qf = op->qf;
+  if (qf->nin != 4 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[0].size != 5 || qf->in[1].emode != CEED_EVAL_GRAD ||
+      qf->in[2].emode != CEED_EVAL_NONE || qf->in[2].size != 10 || qf->in[3].emode != CEED_EVAL_INTERP || qf->out[0].emode != CEED_EVAL_INTERP ||
+      qf->out[0].size != 9)
+    return plan_fail(op, "unexpected velocity-gradient projection field layout (src/velocity_gradient_projection.c:86-97)");
+  if (op->in[0].v != CEED_VECTOR_ACTIVE || op->in[1].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE)
+    return plan_fail(op, "q, Grad_q and the velocity gradient must be active");
+  if (op->in[1].r != op->in[0].r || op->in[1].b != op->in[0].b) return plan_fail(op, "q and Grad_q must share restriction and basis");
+  if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+  CK(plan_elemop(op, op->in[0].r, op->in[0].b));
+  CeedElemRestriction ro = op->out[0].r;
+  CeedBasis           bo = op->out[0].b;
+  if (!node_rstr(ro, 9) || !is_tensor3(bo, 9) || bo->P1d != op->eop->P || bo->Q1d != op->eop->Q || !same_nodes(op->in[0].r, 5, ro, 9))
+    return plan_fail(op, "the velocity gradient must use the solution's nodes with 9 fields and the solution's basis");
+  CK(check_qdata_rstr(op, op->in[2].r, 10, op->eop->Q * op->eop->Q * op->eop->Q, "qdata"));
+  op->state_var = sv;
+  op->plan      = PLAN_VELGRAD;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* "AnisotropyTensorProjection": qdata (NONE) -> v (INTERP, 7) */
+static int plan_aniso(CeedOperator op) {
+  CeedQFunction qf = op->qf;
+  if (qf->nin != 1 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_NONE || qf->in[0].size != 10 || qf->out[0].emode != CEED_EVAL_INTERP ||
+      qf->out[0].size != 7)
+    return plan_fail(op, "unexpected anisotropy-tensor projection field layout (src/grid_anisotropy_tensor.c:56-62)");
+  if (op->out[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "the projected tensor must be active");
+  CK(plan_elemop_nc(op, op->out[0].r, op->out[0].b, 7, "the anisotropy tensor"));
+  CK(check_qdata_rstr(op, op->in[0].r, 10, op->eop->Q * op->eop->Q * op->eop->Q, "qdata"));
+  op->plan = PLAN_ANISO;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* "InverseMultiplicity": multiplicity (NONE, any fields, node restriction) -> inverse multiplicity (NONE, 1, strided) */
+static int plan_inv_mult(CeedOperator op) {
+  CeedQFunction qf = op->qf;
+  if (qf->nin != 1 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_NONE || qf->out[0].emode != CEED_EVAL_NONE || qf->out[0].size != 1)
+    return plan_fail(op, "unexpected inverse-multiplicity field layout (src/inverse_multiplicity.c:63-71)");
+  if (op->in[0].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "multiplicity and its inverse must be active");
+  CeedElemRestriction ri = op->in[0].r, ro = op->out[0].r;
+  if (!ri || ri == CEED_ELEMRESTRICTION_NONE || ri->strided || ri->num_comp != qf->in[0].size)
+    return plan_fail(op, "the multiplicity must come through a node restriction");
+  CK(check_qdata_rstr(op, ro, 1, ri->elem_size, "the inverse multiplicity"));
+  if (ro->num_elem != ri->num_elem) return plan_fail(op, "both restrictions must cover the same elements");
+  op->plan = PLAN_INV_MULT;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* "ComputeSgsDDNodal_*": q (NONE, 5), x (INTERP, unused), gradient velocity (NONE, 9), anisotropy tensor (NONE, 7),
+ * inverse multiplicity (NONE, 1, strided) -> km_sgs (NONE, 6); context SgsDDContext_ */
+static int plan_sgs_nodal(CeedOperator op, int sv) {
+  CeedQFunction qf = op->qf;
+  static const int sizes[5] = {5, 3, 9, 7, 1};
+  int              ok       = qf->nin == 5 && qf->nout == 1 && qf->out[0].emode == CEED_EVAL_NONE && qf->out[0].size == 6;
+  for (int i = 0; ok && i < 5; i++) ok = qf->in[i].size == sizes[i] && qf->in[i].emode == (i == 1 ? CEED_EVAL_INTERP : CEED_EVAL_NONE);
+  if (!ok) return plan_fail(op, "unexpected nodal SGS field layout (problems/sgs_dd_model.c:168-173)");
+  if (op->in[2].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "the velocity gradient and km_sgs must be active");
+  for (int i = 0; i < 5; i++)
+    if (i != 2 && (!op->in[i].v || op->in[i].v == CEED_VECTOR_ACTIVE || op->in[i].v == CEED_VECTOR_NONE))
+      return plan_fail(op, "q, x, the anisotropy tensor and the inverse multiplicity must be passive vectors");
+  if (!qf->ctx || qf->ctx->size < sizeof(HbSgsDDContext)) return plan_fail(op, "context must be an SgsDDContext_ with its network data");
+  const HbSgsDDContext *c = (const HbSgsDDContext *)qf->ctx->data;
+  if (c->num_inputs != 6 || c->num_outputs != 6 || c->num_neurons != 20)
+    return plan_fail(op, "the fused nodal closure is built for the 6-20-6 network of SgsDDSetup (problems/sgs_dd_model.c:665-671)");
+  if (c->newt_ctx.state_var != sv) return plan_fail(op, "the context's state_var differs from the QFunction's");
+  CeedElemRestriction rs = op->out[0].r;
+  if (!node_rstr(rs, 6)) return plan_fail(op, "km_sgs must use a 6-field node restriction");
+  if (!node_rstr(op->in[0].r, 5) || !same_nodes(rs, 6, op->in[0].r, 5) || !node_rstr(op->in[2].r, 9) || !same_nodes(rs, 6, op->in[2].r, 9) ||
+      !node_rstr(op->in[3].r, 7) || !same_nodes(rs, 6, op->in[3].r, 7))
+    return plan_fail(op, "q, the velocity gradient, the anisotropy tensor and km_sgs must number the nodes alike");
+  CK(check_qdata_rstr(op, op->in[4].r, 1, rs->elem_size, "the inverse multiplicity"));
+  CeedBasis bx = op->in[1].b;
+  if (!is_tensor3(bx, 3) || bx->Q1d * bx->Q1d * bx->Q1d != rs->elem_size) return plan_fail(op, "x must be projected onto the solution nodes");
+  /* the node weights are summed per element colour: an element operator on the stress nodes (its basis is not used) */
+  if (!op->eop) {
+    const int P = (int)(cbrt((double)rs->elem_size) + 0.5);
+    if (P * P * P != rs->elem_size) return plan_fail(op, "km_sgs elements must be tensor-product node sets");
+    double        I[HB_MAX_P * HB_MAX_P] = {0}, w[HB_MAX_P] = {0};
+    const int64_t n                      = (int64_t)rs->num_elem * rs->elem_size;
+    int32_t      *off                    = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n ? n : 1));
+    if (!off) return CeedError(op->ceed, CEED_ERROR_BACKEND, "out of host memory");
+    for (int64_t i = 0; i < n; i++) off[i] = (rs->h_off[i] / 6) * 5;
+    for (int i = 0; i < P; i++) I[i * P + i] = 1;
+    const int rc = hb_elemop_create(rs->num_elem, P, P, off, (rs->l_size / 6) * 5, I, I, NULL, w, &op->eop);
+    free(off);
+    HB_CK(op->ceed, rc);
+    ceed_register_op(op->ceed, op->eop);
+  }
+  op->state_var = sv;
+  op->plan      = PLAN_SGS_NODAL;
+  return CEED_ERROR_SUCCESS;
+}
+
+/* "IFunction_NodalSgs_*": q (INTERP, 5), qdata (NONE), km_sgs (INTERP, 6) -> Grad_v (GRAD) */
+static int plan_sgs_if(CeedOperator op, int sv) {
+  CeedQFunction qf = op->qf;
+  if (qf->nin != 3 || qf->nout != 1 || qf->in[0].emode != CEED_EVAL_INTERP || qf->in[0].size != 5 || qf->in[1].emode != CEED_EVAL_NONE ||
+      qf->in[1].size != 10 || qf->in[2].emode != CEED_EVAL_INTERP || qf->in[2].size != 6 || qf->out[0].emode != CEED_EVAL_GRAD || qf->out[0].size != 15)
+    return plan_fail(op, "unexpected nodal SGS residual field layout (problems/sgs_dd_model.c:533-545)");
+  if (op->in[0].v != CEED_VECTOR_ACTIVE || op->out[0].v != CEED_VECTOR_ACTIVE) return plan_fail(op, "q and Grad_v must be active");
+  if (!op->in[2].v || op->in[2].v == CEED_VECTOR_ACTIVE || op->in[2].v == CEED_VECTOR_NONE) return plan_fail(op, "km_sgs must be a passive vector");
+  if (op->out[0].r != op->in[0].r || op->out[0].b != op->in[0].b) return plan_fail(op, "q and Grad_v must share restriction and basis");
+  if (!qf->ctx || qf->ctx->size != sizeof(HbNewtonianContext)) return plan_fail(op, "context must be the 184-byte NewtonianIdealGasContext_");
+  if (((const HbNewtonianContext *)qf->ctx->data)->state_var != sv) return plan_fail(op, "the context's state_var differs from the QFunction's");
+  CK(plan_elemop(op, op->in[0].r, op->in[0].b));
+  CeedElemRestriction rk = op->in[2].r;
+  CeedBasis           bk = op->in[2].b;
+  if (!node_rstr(rk, 6) || !is_tensor3(bk, 6) || bk->P1d != op->eop->P || bk->Q1d != op->eop->Q || !same_nodes(op->in[0].r, 5, rk, 6))
+    return plan_fail(op, "km_sgs must use the solution's nodes with 6 fields and the solution's basis");
+  CK(check_qdata_rstr(op, op->in[1].r, 10, op->eop->Q * op->eop->Q * op->eop->Q, "qdata"));
+  op->state_var = sv;
+  op->plan      = PLAN_SGS_IF;
+  return CEED_ERROR_SUCCESS;
+}
+
 /* The state variable a Newtonian QFunction name selects (newtonian.h:259-269, 313-323): "<prefix>Conserv" 0, "<prefix>Prim" 1,
  * "<prefix>Entropy" 2, anything else -1. */
 static int newtonian_state_var(const char *k, const char *prefix) {
@@ -1835,6 +2025,18 @@ static int op_plan(CeedOperator op) {
     else if (!strcmp(k, "ICsTaylorGreen")) kind = HB_IC_TAYLOR_GREEN;
     else if (!strcmp(k, "ICsChannel")) kind = HB_IC_CHANNEL;
     if (kind >= 0) return plan_ics(op, kind, sv);
+  }
+  {
+    int nc = 0, used = 0;
+    if (sscanf(k, "Mass_%d%n", &nc, &used) == 1 && k[used] == 0 && nc != 5 && nc >= 1 && nc <= 64) return plan_mass_n(op, nc);
+  }
+  {
+    int sv;
+    if ((sv = newtonian_state_var(k, "VelocityGradientProjectionRHS_")) >= 0) return plan_velgrad(op, sv);
+    if ((sv = newtonian_state_var(k, "ComputeSgsDDNodal_")) >= 0) return plan_sgs_nodal(op, sv);
+    if ((sv = newtonian_state_var(k, "IFunction_NodalSgs_")) >= 0) return plan_sgs_if(op, sv);
+    if (!strcmp(k, "AnisotropyTensorProjection")) return plan_aniso(op);
+    if (!strcmp(k, "InverseMultiplicity")) return plan_inv_mult(op);
   }
   const int sv_ke = newtonian_state_var(k, "MonitorTotalKineticEnergy_"), sv_cfl = newtonian_state_var(k, "MonitorCFL_3D_");
   if (sv_ke >= 0 || sv_cfl >= 0) return plan_monitor(op, sv_ke >= 0, sv_ke >= 0 ? sv_ke : sv_cfl);
@@ -2009,6 +2211,94 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
       HB_CK(ceed, hb_restrict_apply_t_strided(ro->num_elem, ro->elem_size, ro->num_comp, ro->d_strides, op->d_tmp_e2, v, s));
       return CEED_ERROR_SUCCESS;
     }
+    case PLAN_MASS_N: {
+      const int64_t n = op->in[0].r->l_size;
+      CK(need_len(op, in, n, "input"));
+      CK(need_len(op, out, n, "output"));
+      CK(need_len(op, op->in[1].v, op->in[1].r->l_size, "qdata"));
+      const double *u, *qd;
+      double       *v;
+      CK(vec_dev_read(in, &u));
+      CK(vec_dev_read(op->in[1].v, &qd));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_mass_n_apply(op->eop, op->nc, qd, u, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_VELGRAD: {
+      CK(need_len(op, in, op->eop->l_size, "state"));
+      CK(need_len(op, out, op->out[0].r->l_size, "velocity gradient"));
+      CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "qdata"));
+      const double *q, *qd;
+      double       *v;
+      CK(vec_dev_read(in, &q));
+      CK(vec_dev_read(op->in[2].v, &qd));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_velocity_gradient_rhs(op->eop, op->qf->ctx->data, op->state_var, qd, q, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_ANISO: {
+      CK(need_len(op, out, op->out[0].r->l_size, "anisotropy tensor"));
+      CK(need_len(op, op->in[0].v, op->in[0].r->l_size, "qdata"));
+      const double *qd;
+      double       *v;
+      CK(vec_dev_read(op->in[0].v, &qd));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_anisotropy_rhs(op->eop, qd, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_INV_MULT: {
+      CeedElemRestriction ri = op->in[0].r, ro = op->out[0].r;
+      CK(need_len(op, in, ri->l_size, "multiplicity"));
+      CK(need_len(op, out, ro->l_size, "inverse multiplicity"));
+      CK(rstr_upload(ri));
+      CK(rstr_upload(ro));
+      const size_t ne = (size_t)ro->num_elem * ro->elem_size;
+      if (!op->d_tmp_e2) CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_e2, sizeof(double) * (ne ? ne : 1)));
+      const double *m;
+      double       *v;
+      CK(vec_dev_read(in, &m));
+      CUDA_CK(ceed, cudaMemsetAsync(op->d_tmp_e2, 0, sizeof(double) * ne, s));
+      HB_CK(ceed, hb_inverse_multiplicity((int64_t)ne, ri->d_off, m, op->d_tmp_e2, s));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_restrict_apply_t_strided(ro->num_elem, ro->elem_size, 1, ro->d_strides, op->d_tmp_e2, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_SGS_NODAL: {
+      CeedElemRestriction rs = op->out[0].r;
+      const int64_t       nodes = rs->l_size / 6;
+      CK(need_len(op, in, op->in[2].r->l_size, "velocity gradient"));
+      CK(need_len(op, out, rs->l_size, "km_sgs"));
+      CK(need_len(op, op->in[0].v, op->in[0].r->l_size, "q"));
+      CK(need_len(op, op->in[3].v, op->in[3].r->l_size, "anisotropy tensor"));
+      CK(need_len(op, op->in[4].v, op->in[4].r->l_size, "inverse multiplicity"));
+      if (!op->d_node_w) CUDA_CK(ceed, cudaMalloc((void **)&op->d_node_w, sizeof(double) * (size_t)(nodes ? nodes : 1)));
+      const double *q, *G, *A, *im;
+      double       *v;
+      CK(vec_dev_read(op->in[0].v, &q));
+      CK(vec_dev_read(in, &G));
+      CK(vec_dev_read(op->in[3].v, &A));
+      CK(vec_dev_read(op->in[4].v, &im));
+      /* the inverse multiplicity arrives in the backend E-vector order [elem][node] (strided, one field) */
+      CUDA_CK(ceed, cudaMemsetAsync(op->d_node_w, 0, sizeof(double) * (size_t)nodes, s));
+      HB_CK(ceed, hb_node_weight_sum(op->eop, im, op->d_node_w, s));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_sgs_nodal_closure(nodes, op->qf->ctx->data, op->qf->ctx->size, op->state_var, q, G, A, op->d_node_w, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
+    case PLAN_SGS_IF: {
+      CK(need_len(op, in, op->eop->l_size, "state"));
+      CK(need_len(op, out, op->eop->l_size, "residual"));
+      CK(need_len(op, op->in[1].v, op->in[1].r->l_size, "qdata"));
+      CK(need_len(op, op->in[2].v, op->in[2].r->l_size, "km_sgs"));
+      const double *q, *qd, *km;
+      double       *v;
+      CK(vec_dev_read(in, &q));
+      CK(vec_dev_read(op->in[1].v, &qd));
+      CK(vec_dev_read(op->in[2].v, &km));
+      CK(vec_dev_write(out, &v, 0));
+      HB_CK(ceed, hb_sgs_nodal_ifunction(op->eop, op->qf->ctx->data, op->state_var, qd, q, km, v, s));
+      return CEED_ERROR_SUCCESS;
+    }
     case PLAN_MASS: {
       const int64_t n = op->eop->l_size;
       CK(need_len(op, in, n, "input"));
@@ -2180,6 +2470,16 @@ static int op_diag_add_single(CeedOperator op, CeedVector assembled) {
     HB_CK(op->ceed, hb_mass_stab_diagonal(op->eop, op->qf->ctx->data, qd, qs, y, 1, op->ceed->stream));
     return CEED_ERROR_SUCCESS;
   }
+  if (op->plan == PLAN_MASS_N) {
+    CK(need_len(op, assembled, op->in[0].r->l_size, "diagonal"));
+    CK(need_len(op, op->in[1].v, op->in[1].r->l_size, "qdata"));
+    const double *qd;
+    double       *y;
+    CK(vec_dev_read(op->in[1].v, &qd));
+    CK(vec_dev_write(assembled, &y, 0));
+    HB_CK(op->ceed, hb_mass_n_diagonal(op->eop, op->nc, qd, y, op->ceed->stream));
+    return CEED_ERROR_SUCCESS;
+  }
   if (op->plan == PLAN_MASS) {
     CK(need_len(op, assembled, op->eop->l_size, "diagonal"));
     CK(need_len(op, op->in[1].v, op->in[1].r->l_size, "qdata"));
@@ -2263,6 +2563,11 @@ int CeedOperatorGetFlopsEstimate(CeedOperator op, CeedSize *flops) {
   if (op->plan == PLAN_IFUNCTION || op->plan == PLAN_RHS) *flops = E * (5 * (2 * (interp + deriv)) + 5 * interp + 700 * Q3);
   else if (op->plan == PLAN_MASS) *flops = E * (5 * 2 * interp + 5 * Q3);
   else if (op->plan == PLAN_IJACOBIAN) *flops = E * (5 * (2 * (interp + deriv)) + 520 * Q3);
+  else if (op->plan == PLAN_MASS_N) *flops = E * (op->nc * (2 * interp + Q3));
+  else if (op->plan == PLAN_VELGRAD) *flops = E * (5 * (interp + deriv) + 9 * interp + 150 * Q3);
+  else if (op->plan == PLAN_ANISO) *flops = E * (7 * interp + 400 * Q3);
+  else if (op->plan == PLAN_SGS_IF) *flops = E * (11 * interp + 5 * (interp + deriv) + 90 * Q3);
+  else if (op->plan == PLAN_SGS_NODAL) *flops = (op->out[0].r->l_size / 6) * 1500;
   return CEED_ERROR_SUCCESS;
 }
 
@@ -2425,6 +2730,12 @@ static void op_view(CeedOperator op, FILE *stream, int terse, int depth) {
           : op->plan == PLAN_RHS       ? "explicit right-hand side"
           : op->plan == PLAN_MASS      ? "mass"
           : op->plan == PLAN_MASS_STAB ? "stabilized mass"
+          : op->plan == PLAN_MASS_N    ? "mass (N fields)"
+          : op->plan == PLAN_VELGRAD   ? "velocity-gradient projection right-hand side"
+          : op->plan == PLAN_ANISO     ? "anisotropy-tensor projection right-hand side"
+          : op->plan == PLAN_INV_MULT  ? "inverse multiplicity"
+          : op->plan == PLAN_SGS_NODAL ? "nodal data-driven SGS closure"
+          : op->plan == PLAN_SGS_IF    ? "nodal SGS residual"
                                        : "not planned");
   if (terse) return;
   for (int o = 0; o < 2; o++)

@@ -236,8 +236,8 @@ HB_HD void inputs(const T G[3][3], const T km_A[6], T delta, T nu, T E[3][3], T 
 
 // Model outputs (normalised to [0, 1] by min-max bounds b[c] = {lo, hi}) -> physical SGS stress in KM notation:
 // de-normalise, scale by delta^2 |G A|^2, rotate from the eigenframe: tau = E^T S E.
-template <typename T>
-HB_HD void outputs_to_stress(const T out_n[6], T delta, const T E[3][3], const float (&b)[6][2], T gmag, T km_tau[6]) {
+template <typename T, typename TB>
+HB_HD void outputs_to_stress(const T out_n[6], T delta, const T E[3][3], const TB (&b)[6][2], T gmag, T km_tau[6]) {
   T o[6];
   const T sc = delta * delta * gmag * gmag;
 #pragma unroll

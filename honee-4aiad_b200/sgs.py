@@ -63,6 +63,28 @@ def load_reference_model(data_dir, alpha=0.0):
     return desc(20, 0, alpha, bounds), flat
 
 
+def sgs_dd_context(newt_ctx_bytes: bytes, flat_params, bounds, alpha=0.0):
+    """The SgsDDContext_ blob of a 6-20-6 network (qfunctions/sgs_dd_model.h:16-31) as SgsDDContextFill lays it out
+    (problems/sgs_dd_model.c:598-651): num_inputs, num_outputs, num_layers (1), num_neurons, alpha, the Newtonian context,
+    the data offsets bias1 0, bias2 20, weight1 40, weight2 160, out_scaling 280 (in doubles; bias2 gets num_neurons
+    slots), total_bytes, then data = b1 | b2 | W1 [20][6] | W2 [6][20] | bounds [6][2].  flat_params in the layout of
+    load_reference_model.  Returns a ctypes char array (what CeedQFunctionContextSetData is given)."""
+    p = np.asarray(flat_params, dtype=np.float64)
+    W1, b1, W2, b2 = p[:120], p[120:140], p[140:260], p[260:266]
+    data = np.concatenate([b1, np.pad(b2, (0, 14)), W1, W2, np.asarray(bounds, dtype=np.float64).reshape(12)])
+    o_data = 256
+    total = o_data + 8 * data.size
+    buf = bytearray(total)
+    np.frombuffer(buf, dtype=np.int32, count=4, offset=0)[:] = [6, 6, 1, 20]
+    np.frombuffer(buf, dtype=np.float64, count=1, offset=16)[:] = alpha
+    if len(newt_ctx_bytes) != 184:
+        raise ValueError("the Newtonian context must be the 184-byte NewtonianIdealGasContext_")
+    buf[24:208] = newt_ctx_bytes
+    np.frombuffer(buf, dtype=np.uint64, count=6, offset=208)[:] = [0, 20, 40, 160, 280, total]
+    np.frombuffer(buf, dtype=np.float64, count=data.size, offset=o_data)[:] = data
+    return (C.c_char * total).from_buffer_copy(bytes(buf))
+
+
 def xavier_init(d: HbMlpDesc, seed=0) -> np.ndarray:
     """Glorot-uniform weights U(-a, a), a = sqrt(6 / (fan_in + fan_out)), zero biases, from a seeded generator."""
     rng = np.random.default_rng(seed)

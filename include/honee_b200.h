@@ -284,6 +284,32 @@ HB_EXPORT int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double
  * [elem][Q^3] (MonitorCFL_3D_*, src/monitor_cfl.c:100-110, before the min / max and the time-step factor).  Asynchronous. */
 HB_EXPORT int hb_monitor_ke_points(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *e_out, void *s);
 HB_EXPORT int hb_monitor_cfl_points(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *e_out, void *s);
+
+/* ---- Nodal data-driven SGS pipeline (problems/sgs_dd_model.c:98-200, 508-560, 645-737; src/velocity_gradient_projection.c;
+ *      src/grid_anisotropy_tensor.c; src/inverse_multiplicity.c).  Element operators take an HbElemOp whose offsets are
+ *      node * 5 (the node numbering every field of the pipeline shares); node-interleaved L-vectors of nc fields are
+ *      addressed [node][nc].  All outputs are added to. ---- */
+/* v [node][9] += int phi wdetJ du_i/dx_j (row-major i, j) of the state q in state_var (VelocityGradientProjectionRHS_*,
+ * qfunctions/velocity_gradient_projection.h:9-37). */
+HB_EXPORT int hb_velocity_gradient_rhs(const HbElemOp *op, const void *ctx184, int state_var, const double *qdata, const double *q, double *v, void *s);
+/* v [node][7] += int phi wdetJ (KM anisotropy tensor (6), delta) (AnisotropyTensorProjection, grid_anisotropy_tensor.h:35-55). */
+HB_EXPORT int hb_anisotropy_rhs(const HbElemOp *op, const double *qdata, double *v, void *s);
+/* v [node][nc] += M u, the mass matrix on nc fields (Mass_N, src/honee-mass.c:20-60); its diagonal, the same in every field. */
+HB_EXPORT int hb_mass_n_apply(const HbElemOp *op, int nc, const double *qdata, const double *u, double *v, void *s);
+HB_EXPORT int hb_mass_n_diagonal(const HbElemOp *op, int nc, const double *qdata, double *diag, void *s);
+/* e_out[i] = 1 / mult[offsets[i]] for the n entries of an element vector (InverseMultiplicity, qfunctions/inverse_multiplicity.h). */
+HB_EXPORT int hb_inverse_multiplicity(int64_t n, const int32_t *offsets, const double *mult, double *e_out, void *s);
+/* w [node] += the entries of the element vector e_vec [elem][P^3] at that node (transposed restriction of one field). */
+HB_EXPORT int hb_node_weight_sum(const HbElemOp *op, const double *e_vec, double *w, void *s);
+/* km_sgs [node][6] += w [node] tau(node): the data-driven closure at every node with w != 0 (ComputeSgsDDNodal_*,
+ * qfunctions/sgs_dd_model.h:69-96) from q [node][5] in state_var, the velocity gradient G [node][9] and the anisotropy
+ * tensor with width A [node][7]; sgs_ctx is the SgsDDContext_ blob of ctx_bytes bytes (6-20-6 network, FP64 weights). */
+HB_EXPORT int hb_sgs_nodal_closure(int64_t nodes, const void *sgs_ctx, size_t ctx_bytes, int state_var, const double *q, const double *G, const double *A,
+                                   const double *w, double *km_sgs, void *s);
+/* v [node][5] += int grad phi . (-wdetJ dXdx F_sgs), F_sgs the flux of the interpolated nodal stress km_sgs [node][6]
+ * (IFunction_NodalSgs_*, qfunctions/sgs_dd_model.h:205-243). */
+HB_EXPORT int hb_sgs_nodal_ifunction(const HbElemOp *op, const void *ctx184, int state_var, const double *qdata, const double *q, const double *km_sgs,
+                                     double *v, void *s);
 HB_EXPORT int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double dt, double *d_scratch,
                              double minmax[2], void *s);
 

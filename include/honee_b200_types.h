@@ -12,9 +12,11 @@
 
 #ifdef __cplusplus
 #include <cstddef>
+#include <cstdint>
 #else
 #include <stdbool.h>
 #include <stddef.h>
+#include <stdint.h>
 #endif
 
 #ifdef __cplusplus
@@ -131,6 +133,24 @@ typedef struct {
   HbNewtonianContext newt_ctx;
 } HbGaussianWaveContext;
 
+/* qfunctions/sgs_dd_model.h:16-31 (struct SgsDDContext_, 264 bytes with one data entry): the network's shape, the leaky
+ * ReLU slope, the Newtonian context, the offsets (in doubles) of the biases, weights and output bounds inside data[],
+ * the total size in bytes of the context with its data (problems/sgs_dd_model.c:605-620). */
+typedef struct {
+  int32_t            num_inputs, num_outputs;
+  int32_t            num_layers;
+  int32_t            num_neurons;
+  double             alpha;
+  HbNewtonianContext newt_ctx;
+  struct {
+    size_t bias1, bias2;
+    size_t weight1, weight2;
+    size_t out_scaling;
+  } offsets;
+  size_t total_bytes;
+  double data[1];
+} HbSgsDDContext;
+
 /* Number of stored Jacobian components per quadrature point: q (5), Kelvin-Mandel strain rate (6), diagonal tau (3),
  * plus the IDL ramp coefficient when enabled (problems/newtonian.c:756-757; qfunctions/newtonian.h:251-254). */
 #define HB_JAC_DATA_COMPS 14
@@ -156,5 +176,9 @@ HB_STATIC_ASSERT(sizeof(HbChannelContext) == 240, "ChannelContext_ layout");
 HB_STATIC_ASSERT(offsetof(HbChannelContext, newt_ctx) == 56, "ChannelContext_ newt_ctx offset");
 HB_STATIC_ASSERT(sizeof(HbGaussianWaveContext) == 304, "GaussianWaveContext_ layout");
 HB_STATIC_ASSERT(offsetof(HbGaussianWaveContext, newt_ctx) == 120, "GaussianWaveContext_ newt_ctx offset");
+HB_STATIC_ASSERT(sizeof(HbSgsDDContext) == 264, "SgsDDContext_ layout");
+HB_STATIC_ASSERT(offsetof(HbSgsDDContext, newt_ctx) == 24, "SgsDDContext_ newt_ctx offset");
+HB_STATIC_ASSERT(offsetof(HbSgsDDContext, offsets) == 208, "SgsDDContext_ offsets offset");
+HB_STATIC_ASSERT(offsetof(HbSgsDDContext, data) == 256, "SgsDDContext_ data offset");
 
 #endif

@@ -21,6 +21,8 @@
 #include "sgs_dd_model.h"
 #include "spanstats/turbulence.h"
 #include "taylorgreen.h"
+#include "velocity_gradient_projection.h"
+#include "inverse_multiplicity.h"
 
 #include <stddef.h>
 
@@ -90,6 +92,17 @@ EXPORT int ref_setup_context_size(void) { return (int)sizeof(struct SetupContext
 EXPORT int ref_ComputeSgsDDNodal_Conserv(void *c, CeedInt Q, In in, Out out) { return ComputeSgsDDNodal_Conserv(c, Q, in, out); }
 EXPORT int ref_AnisotropyTensorCollocate(void *c, CeedInt Q, In in, Out out) { return AnisotropyTensorCollocate(c, Q, in, out); }
 EXPORT int ref_IFunction_NodalSgs_Conserv(void *c, CeedInt Q, In in, Out out) { return IFunction_NodalSgs_Conserv(c, Q, in, out); }
+EXPORT int ref_IFunction_NodalSgs_Prim(void *c, CeedInt Q, In in, Out out) { return IFunction_NodalSgs_Prim(c, Q, in, out); }
+EXPORT int ref_IFunction_NodalSgs_Entropy(void *c, CeedInt Q, In in, Out out) { return IFunction_NodalSgs_Entropy(c, Q, in, out); }
+EXPORT int ref_ComputeSgsDDNodal_Prim(void *c, CeedInt Q, In in, Out out) { return ComputeSgsDDNodal_Prim(c, Q, in, out); }
+EXPORT int ref_ComputeSgsDDNodal_Entropy(void *c, CeedInt Q, In in, Out out) { return ComputeSgsDDNodal_Entropy(c, Q, in, out); }
+EXPORT int ref_AnisotropyTensorProjection(void *c, CeedInt Q, In in, Out out) { return AnisotropyTensorProjection(c, Q, in, out); }
+EXPORT int ref_InverseMultiplicity(void *c, CeedInt Q, In in, Out out) { return InverseMultiplicity(c, Q, in, out); }
+EXPORT int ref_VelocityGradientProjectionRHS_Conserv(void *c, CeedInt Q, In in, Out out) { return VelocityGradientProjectionRHS_Conserv(c, Q, in, out); }
+EXPORT int ref_VelocityGradientProjectionRHS_Prim(void *c, CeedInt Q, In in, Out out) { return VelocityGradientProjectionRHS_Prim(c, Q, in, out); }
+EXPORT int ref_VelocityGradientProjectionRHS_Entropy(void *c, CeedInt Q, In in, Out out) { return VelocityGradientProjectionRHS_Entropy(c, Q, in, out); }
+EXPORT int ref_Mass_7(void *c, CeedInt Q, In in, Out out) { return Mass_7(c, Q, in, out); }
+EXPORT int ref_Mass_9(void *c, CeedInt Q, In in, Out out) { return Mass_9(c, Q, in, out); }
 EXPORT int ref_DifferentialFilter_RHS_Conserv(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_RHS_Conserv(c, Q, in, out); }
 EXPORT int ref_DifferentialFilter_RHS_Prim(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_RHS_Prim(c, Q, in, out); }
 EXPORT int ref_DifferentialFilter_RHS_Entropy(void *c, CeedInt Q, In in, Out out) { return DifferentialFilter_RHS_Entropy(c, Q, in, out); }
