@@ -183,6 +183,9 @@ class Vector(_Obj):
     def pointwise_mult(self, x: "Vector", y: "Vector"):
         self.ceed.chk(L().CeedVectorPointwiseMult(self.ptr, x.ptr, y.ptr))
 
+    def reciprocal(self):
+        self.ceed.chk(L().CeedVectorReciprocal(self.ptr))
+
 
 class ElemRestriction(_Obj):
     _destroy = "CeedElemRestrictionDestroy"
@@ -209,6 +212,10 @@ class ElemRestriction(_Obj):
         n_e = self.num_elem * self.elem_size * self.num_comp
         return Vector.wrap(self.ceed, lv.value, self.l_size), Vector.wrap(self.ceed, ev.value, n_e)
 
+    def multiplicity(self, mult: Vector):
+        """CeedElemRestrictionGetMultiplicity: mult = the number of element nodes at each L-vector entry."""
+        self.ceed.chk(L().CeedElemRestrictionGetMultiplicity(self.ptr, mult.ptr))
+
     def apply(self, transpose: bool, u: Vector, ru: Vector):
         self.ceed.chk(L().CeedElemRestrictionApply(self.ptr, CEED_TRANSPOSE if transpose else CEED_NOTRANSPOSE, u.ptr, ru.ptr,
                                                    self.ceed.request_immediate))
@@ -225,6 +232,15 @@ class Basis(_Obj):
             return
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (interp1d, grad1d, qref1d, qweight1d)]
         ceed.chk(L().CeedBasisCreateTensorH1(ceed.ptr, dim, num_comp, P, Q, *[a.ctypes.data_as(_dp) for a in arrs], C.byref(self.ptr)))
+
+    @classmethod
+    def projection(cls, basis_from: "Basis", basis_to: "Basis"):
+        """CeedBasisCreateProjection(basis_from, basis_to): interpolation from one basis's nodes onto the other's."""
+        b = cls.__new__(cls)
+        _Obj.__init__(b, basis_from.ceed)
+        b.dim, b.num_comp, b.P, b.Q = basis_from.dim, basis_from.num_comp, basis_from.P, basis_to.P
+        basis_from.ceed.chk(L().CeedBasisCreateProjection(basis_from.ptr, basis_to.ptr, C.byref(b.ptr)))
+        return b
 
     def apply(self, num_elem, transpose, emode, u: Optional[Vector], v: Vector):
         self.ceed.chk(L().CeedBasisApply(self.ptr, num_elem, CEED_TRANSPOSE if transpose else CEED_NOTRANSPOSE, emode,

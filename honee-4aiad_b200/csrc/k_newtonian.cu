@@ -893,14 +893,37 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
 // lane recomputes the first and is not stored): the node values of both are gathered into the two lanes of one 8-byte
 // slot, every basis pass and the point-wise tangent run once for both lanes, and the scatter stores each lane at its own
 // element's nodes.  Same arithmetic per lane as k_ijacobian<float> (FP32 values and Jacobian data, FP64 qdata rounded to
-// FP32 at the point), half the instructions.  qdata of both elements is staged by TMA; their Jacobian data are read at
-// the point from global memory (coalesced per component, warmed in L2 one pair ahead), which keeps three CTAs per SM.
+// FP32 at the point), half the instructions.
+//   Q32 = false: qdata of both elements (FP64) is staged by TMA; their Jacobian data are read at the point from global
+//                memory (coalesced per component, warmed in L2 one pair ahead), which keeps three CTAs per SM.
+//   Q32 = true:  qdata comes already rounded to FP32 ([E][10][Q3], the values every point rounds it to anyway), so the
+//                pair's qdata and Jacobian data (24 KB) both fit in shared memory at three CTAs per SM: both are staged
+//                by cp.async for the next pair while this pair finishes, and no global load is left in the point-wise
+//                phase.  Half the qdata bytes, bit-identical results.
 
 struct IjacobianPairPtrs {
   const float *dq;
   const float *jac_data;  // [E][num_jd][Q3]
   float *v;
+  const float *qdata32;   // [E][10][Q3] FP32 qdata (Q32 kernels)
+  int jd8, qd8;           // the Jacobian data / FP32 qdata of every element can be copied in 8-byte chunks
 };
+
+constexpr int kPairJdMax = 15;  // Jacobian-data components staged per element (14, or 15 with the IDL)
+// floats between the two lanes' staged Jacobian data: 15 Q^3 rounded up to a multiple of 4, so the second lane's buffer
+// starts 16-byte aligned (8-byte cp.async needs an 8-byte aligned shared-memory destination)
+__host__ __device__ constexpr int pair_jd_stride(int Q3) { return (kPairJdMax * Q3 + 3) & ~3; }
+
+// copy a contiguous block of n floats into shared memory with cp.async (8-byte chunks when both ends are 8-byte aligned
+// and n is even, else 4-byte)
+template <int NT>
+__device__ __forceinline__ void stage_floats_async(float *dst, const float *src, int n, bool by8) {
+  if (by8) {
+    for (int i = threadIdx.x; i < n / 2; i += NT) cp_async8(dst + 2 * i, src + 2 * i);
+  } else {
+    for (int i = threadIdx.x; i < n; i += NT) cp_async4(dst + i, src + i);
+  }
+}
 
 // node gathers into one lane (byte offset 0 or 4) of the pair slots: sN [5][P][P][PX], sV [P3][5]
 template <int P, int NT>
@@ -921,17 +944,33 @@ __device__ __forceinline__ void gather_out_lane_async(const int32_t *sO, const f
   for (int t = threadIdx.x; t < 5 * P3; t += NT) cp_async4(reinterpret_cast<float *>(&sV[t]) + lane, l_out + sO[t]);
 }
 
-template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
+template <int P, int Q, bool Q32>
+struct PairPlan {
+  using L = Plan<P, Q, 1, f2, false, false>;
+  static constexpr int Q3 = L::Q3;
+  // staged point data after the basis buffers: FP64 qdata [2][10][Q3] (Q32 = false) or FP32 qdata [2][10][Q3] and
+  // Jacobian data [2][kPairJdMax][Q3] (Q32 = true); then the mbarrier
+  static constexpr size_t stage_bytes = Q32 ? sizeof(float) * (2 * 10 * Q3 + 2 * pair_jd_stride(Q3)) : sizeof(double) * 2 * 10 * Q3;
+  static_assert((sizeof(float) * 10 * Q3) % 8 == 0, "second lane's qdata 8-byte aligned");
+  static_assert((sizeof(float) * pair_jd_stride(Q3)) % 16 == 0, "second lane's Jacobian data 16-byte aligned");
+  static constexpr size_t mbar_offset = (L::qd_offset_bytes + stage_bytes + 15) & ~(size_t)15;
+  static constexpr size_t bytes = mbar_offset + 16;
+};
+
+template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE, bool Q32 = false>
 __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ijacobian_pair(const ElemArgs<f2> a, const IjacobianPairPtrs p) {
   constexpr int NT = nthreads_for<float>(Q);
   using L = Plan<P, Q, 1, f2, false, false>;
+  using PL = PairPlan<P, Q, Q32>;
   constexpr int Q3 = L::Q3, P3 = L::P3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   f2 *sm = reinterpret_cast<f2 *>(smem_raw);
   f2 *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
   f2 *sW1 = sU + 5 * Q3;
-  double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);  // [2][10][Q3]: the pair's qdata
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + 2 * sizeof(double) * 10 * Q3);
+  double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);  // [2][10][Q3]: the pair's qdata (Q32 = false)
+  float *sQ32 = reinterpret_cast<float *>(smem_raw + L::qd_offset_bytes);   // [2][10][Q3]: the pair's FP32 qdata (Q32)
+  float *sJD = sQ32 + 2 * 10 * Q3;                                          // [2][pair_jd_stride]: its Jacobian data (Q32)
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + PL::mbar_offset);
   __shared__ int s_bail;
   __shared__ int32_t sO[2][2][5 * P3];  // entry offsets of the current / next pair, per lane
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
@@ -948,9 +987,19 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
     tma_load_1d(sQD, a.qdata + (int64_t)eA * 10 * Q3, qd_bytes, mbar);
     tma_load_1d(sQD + 10 * Q3, a.qdata + (int64_t)eB * 10 * Q3, qd_bytes, mbar);
   };
+  auto stage_points32 = [&](int eA, int eB) {  // all threads: both elements' FP32 qdata and Jacobian data by cp.async
+    stage_floats_async<NT>(sQ32, p.qdata32 + (int64_t)eA * 10 * Q3, 10 * Q3, p.qd8);
+    stage_floats_async<NT>(sQ32 + 10 * Q3, p.qdata32 + (int64_t)eB * 10 * Q3, 10 * Q3, p.qd8);
+    stage_floats_async<NT>(sJD, p.jac_data + (int64_t)eA * njd * Q3, njd * Q3, p.jd8);
+    stage_floats_async<NT>(sJD + pair_jd_stride(Q3), p.jac_data + (int64_t)eB * njd * Q3, njd * Q3, p.jd8);
+  };
   auto warm_jd = [&](int eA, int eB) {
     prefetch_l2_bulk(p.jac_data + (int64_t)eA * njd * Q3, sizeof(float) * njd * Q3);
     prefetch_l2_bulk(p.jac_data + (int64_t)eB * njd * Q3, sizeof(float) * njd * Q3);
+    if constexpr (Q32) {
+      prefetch_l2_bulk(p.qdata32 + (int64_t)eA * 10 * Q3, sizeof(float) * 10 * Q3);
+      prefetch_l2_bulk(p.qdata32 + (int64_t)eB * 10 * Q3, sizeof(float) * 10 * Q3);
+    }
   };
 
   if (threadIdx.x == 0) {
@@ -973,7 +1022,9 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
     ob.store(sO[0][1]);
     gather_lane_async<P, NT>(oa, p.dq, sN, 0);
     gather_lane_async<P, NT>(ob, p.dq, sN, 1);
-    if (threadIdx.x == 0) {
+    if constexpr (Q32) {
+      stage_points32(eA, eB);
+    } else if (threadIdx.x == 0) {
       stage_qdata(eA, eB);
       warm_jd(eA, eB);
     }
@@ -993,8 +1044,8 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
   }
   for (; idx < npairs; idx += G) {
     const int cA = eA, cB = eB, chasB = hasB;
-    cp_async_wait_group<1>();
-    if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
+    cp_async_wait_group<1>();  // the pair's node values (and with Q32 its point data) have landed
+    if (!Q32 && threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
       s_bail = 1;
       atomicOr(a.status, 1);
     }
@@ -1021,14 +1072,25 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
 #pragma unroll
         for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
-      const float *jA = p.jac_data + (int64_t)cA * njd * Q3 + q, *jB = p.jac_data + (int64_t)cB * njd * Q3 + q;
+      if constexpr (Q32) {
+        const float *jA = sJD + q, *jB = sJD + pair_jd_stride(Q3) + q;
 #pragma unroll
-      for (int c = 0; c < 14; c++) jd[c] = f2(__ldg(jA + c * Q3), __ldg(jB + c * Q3));
-      jd[14] = njd > 14 ? f2(__ldg(jA + 14 * Q3), __ldg(jB + 14 * Q3)) : f2(0.0);
-      const double *qA = sQD + q, *qB = sQD + 10 * Q3 + q;
-      wdetJ = f2(float(qA[0]), float(qB[0]));
+        for (int c = 0; c < 14; c++) jd[c] = f2(jA[c * Q3], jB[c * Q3]);
+        jd[14] = njd > 14 ? f2(jA[14 * Q3], jB[14 * Q3]) : f2(0.0);
+        const float *qA = sQ32 + q, *qB = sQ32 + 10 * Q3 + q;
+        wdetJ = f2(qA[0], qB[0]);
 #pragma unroll
-      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = f2(float(qA[(1 + k) * Q3]), float(qB[(1 + k) * Q3]));
+        for (int k = 0; k < 9; k++) X[k / 3][k % 3] = f2(qA[(1 + k) * Q3], qB[(1 + k) * Q3]);
+      } else {
+        const float *jA = p.jac_data + (int64_t)cA * njd * Q3 + q, *jB = p.jac_data + (int64_t)cB * njd * Q3 + q;
+#pragma unroll
+        for (int c = 0; c < 14; c++) jd[c] = f2(__ldg(jA + c * Q3), __ldg(jB + c * Q3));
+        jd[14] = njd > 14 ? f2(__ldg(jA + 14 * Q3), __ldg(jB + 14 * Q3)) : f2(0.0);
+        const double *qA = sQD + q, *qB = sQD + 10 * Q3 + q;
+        wdetJ = f2(float(qA[0]), float(qB[0]));
+#pragma unroll
+        for (int k = 0; k < 9; k++) X[k / 3][k % 3] = f2(float(qA[(1 + k) * Q3]), float(qB[(1 + k) * Q3]));
+      }
       ijacobian_point_stream<f2, SV>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
@@ -1038,8 +1100,10 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
       }
     }
     __syncthreads();
-    if (nA >= 0) {
-      if (threadIdx.x == 0) {
+    if (nA >= 0) {  // this pair's point data consumed: stage the next pair's
+      if constexpr (Q32) {
+        stage_points32(nA, nB);
+      } else if (threadIdx.x == 0) {
         fence_proxy_async_smem();
         stage_qdata(nA, nB);
       }
@@ -1077,7 +1141,7 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
     }
   }
   cp_async_wait_all();
-  if (s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);
+  if (!Q32 && s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -1116,14 +1180,22 @@ __host__ __device__ constexpr int diag_yfactor(int h, int i) { return i; }
 
 template <int P, int Q>
 struct DiagPlan {
-  // FP64 at Q = 5: 74 KB, three CTAs per SM
+  // FP64 at Q = 5: 75 KB, three CTAs per SM
   static constexpr int P2 = P * P, P3 = P2 * P, Q2 = Q * Q, Q3 = Q2 * Q, PX = P;  // PX: pa stride of the x-pass output
   static constexpr int nA = 50 * Q3;                                               // [5][10][Q3]; after the y pass: T2 [5][3][Q][P][P]
   static constexpr int nT1 = 5 * 6 * Q2 * PX;                                      // [5][6][Q][Q][PX]
   static constexpr int nT2 = 5 * 3 * Q * P2;
   static_assert(nT2 <= nA, "the y-pass output fits in the combination arrays");
+  // The x-pass output region also holds, between the y pass of one element and the x pass of the next, the next
+  // element's staged point data: qdata [10][Q3] (FP64) then its Jacobian data [15][Q3] (T)
   template <typename T>
-  static constexpr size_t bytes() { return sizeof(T) * (size_t)(nA + nT1); }
+  static constexpr size_t stage_bytes() { return sizeof(double) * 10 * Q3 + sizeof(T) * 15 * Q3; }
+  template <typename T>
+  static constexpr size_t t1_bytes() {
+    return ((sizeof(T) * nT1 > stage_bytes<T>() ? sizeof(T) * nT1 : stage_bytes<T>()) + 15) & ~(size_t)15;
+  }
+  template <typename T>
+  static constexpr size_t bytes() { return ((sizeof(T) * nA + 15) & ~(size_t)15) + t1_bytes<T>(); }
 };
 
 template <int P, int Q, typename T, int SV = HB_STATEVAR_CONSERVATIVE>
@@ -1132,25 +1204,39 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), (Q <= 5 ? 3 : 1)) k_diagon
   using L = DiagPlan<P, Q>;
   constexpr int P2 = L::P2, P3 = L::P3, Q2 = L::Q2, Q3 = L::Q3, PX = L::PX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *sA = reinterpret_cast<T *>(smem_raw);  // [5][10][Q3]
-  T *sT1 = sA + L::nA;                      // [5][6][Q2][PX]
-  T *sT2 = sA;                              // [5][3][Q][P][P]
+  T *sA = reinterpret_cast<T *>(smem_raw);                                        // [5][10][Q3]
+  unsigned char *t1_raw = smem_raw + ((sizeof(T) * L::nA + 15) & ~(size_t)15);
+  T *sT1 = reinterpret_cast<T *>(t1_raw);                                         // [5][6][Q2][PX]
+  T *sT2 = sA;                                                                    // [5][3][Q][P][P]
+  double *sQD = reinterpret_cast<double *>(t1_raw);                               // staged qdata [10][Q3] (in the sT1 region)
+  T *sJD = reinterpret_cast<T *>(t1_raw + sizeof(double) * 10 * Q3);              // staged Jacobian data [njd][Q3]
   const int njd = a.num_jd;
+  // the element's point data (qdata and Jacobian data) are staged by cp.async into the x-pass region: for the first
+  // element here, for the next one as soon as this one's y pass has consumed that region
+  auto stage = [&](int e) {
+    stage_block<double, NT>(sQD, a.qdata + (int64_t)e * 10 * Q3, 10 * Q3, false, nullptr);
+    stage_block<T, NT>(sJD, p.jac_data + (int64_t)e * njd * Q3, njd * Q3, false, nullptr);
+    cp_async_commit();
+  };
+  if (blockIdx.x < a.n_elems) stage(a.elems[blockIdx.x]);
   for (int idx = blockIdx.x; idx < a.n_elems; idx += gridDim.x) {
     const int e = a.elems[idx];
-    if (threadIdx.x == 0 && idx + (int)gridDim.x < a.n_elems) {  // warm L2 with the next element's point data
-      const int en = a.elems[idx + gridDim.x];
+    const int en = idx + (int)gridDim.x < a.n_elems ? a.elems[idx + gridDim.x] : -1;
+    if (threadIdx.x == 0 && en >= 0) {  // warm L2 with the next element's point data before it is staged
       prefetch_l2_bulk(p.jac_data + (int64_t)en * njd * Q3, sizeof(T) * njd * Q3);
       prefetch_l2_bulk(a.qdata + (int64_t)en * 10 * Q3, sizeof(double) * 10 * Q3);
     }
+    cp_async_wait_group<0>();
+    __syncthreads();
     const int q = threadIdx.x;
     if (q < Q3) {
       T jd[15], wdetJ, X[3][3];
-      const T *jdp = p.jac_data + (int64_t)e * njd * Q3 + q;
 #pragma unroll
-      for (int k = 0; k < 14; k++) jd[k] = jdp[k * Q3];
-      jd[14] = njd > 14 ? jdp[14 * Q3] : T(0);
-      load_qdata(a.qdata + (int64_t)e * 10 * Q3, Q3, q, wdetJ, X);
+      for (int k = 0; k < 14; k++) jd[k] = sJD[k * Q3 + q];
+      jd[14] = njd > 14 ? sJD[14 * Q3 + q] : T(0);
+      wdetJ = T(sQD[q]);
+#pragma unroll
+      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = T(sQD[(1 + k) * Q3 + q]);
       T *sAq = sA + q;
       diag_point_blocks<SV>(a.pc, jd, wdetJ, X, [&](int c, int m, T v) { sAq[(c * 10 + m) * Q3] = v; });
     }
@@ -1205,7 +1291,9 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), (Q <= 5 ? 3 : 1)) k_diagon
       }
     }
     __syncthreads();
-    // z pass over the three z groups, then the scatter: elements of one colour share no node
+    if (en >= 0) stage(en);  // the x-pass region is free until the next element's x pass
+    // z pass over the three z groups, then the scatter: elements of one colour share no node, so each entry receives one
+    // addition per launch; a reduction without return (red.global.add) leaves no thread waiting for the old value
     const int32_t *off = a.offsets + (int64_t)e * P3;
     for (int t = threadIdx.x; t < 5 * P2; t += NT) {
       const int c = t / P2, pab = t % P2;
@@ -1223,13 +1311,11 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), (Q <= 5 ? 3 : 1)) k_diagon
           for (int k = 0; k < Q; k++) acc[pc] += p.W[h][k * P + pc] * in[k];
       }
 #pragma unroll
-      for (int pc = 0; pc < P; pc++) {
-        T *d = p.diag + __ldg(off + pc * P2 + pab) + c;
-        *d += acc[pc];
-      }
+      for (int pc = 0; pc < P; pc++) atomicAdd(p.diag + __ldg(off + pc * P2 + pab) + c, acc[pc]);
     }
     __syncthreads();
   }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -1533,28 +1619,36 @@ static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, c
 }
 
 // The paired FP32 Jacobian (two elements of a colour per CTA pass, packed FP32): needs qdata 16-byte aligned (TMA).
-template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
-static int launch_ijacobian_pair(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *jd, const float *dq, float *v,
-                                 cudaStream_t s) {
-  using L = Plan<P, Q, 1, f2, false, false>;
-  const size_t sm = L::qd_offset_bytes + 2 * sizeof(double) * 10 * L::Q3 + 16;
-  if (cudaFuncSetAttribute(k_ijacobian_pair<P, Q, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
+template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE, bool Q32 = false>
+static int launch_ijacobian_pair(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *qdata32, const float *jd,
+                                 const float *dq, float *v, cudaStream_t s) {
+  const size_t sm = PairPlan<P, Q, Q32>::bytes;
+  auto kern = k_ijacobian_pair<P, Q, SV, Q32>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
   IjacobianPairPtrs p;
   p.dq = dq;
   p.jac_data = jd;
   p.v = v;
+  p.qdata32 = qdata32;
+  const int Q3 = Q * Q * Q, njd = HB_JAC_DATA_COMPS + (ctx.idl_enable ? 1 : 0);
+  p.jd8 = (njd * Q3) % 2 == 0 && ((uintptr_t)jd % 8) == 0;
+  p.qd8 = ((uintptr_t)qdata32 % 8) == 0;
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<f2> a = make_args<f2>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
     const int npairs = (a.n_elems + 1) / 2;
-    k_ijacobian_pair<P, Q, SV><<<grid_for(op, npairs, k_ijacobian_pair<P, Q, SV>, nthreads_for<float>(Q), sm), nthreads_for<float>(Q), sm, s>>>(a, p);
+    kern<<<grid_for(op, npairs, kern, nthreads_for<float>(Q), sm), nthreads_for<float>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
 template <int P, int Q, int SV>
-static int pair_case(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *jd, const float *dq, float *v, cudaStream_t s) {
-  if constexpr (Q <= 6) return launch_ijacobian_pair<P, Q, SV>(op, ctx, qdata, jd, dq, v, s);
+static int pair_case(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *qdata32, const float *jd, const float *dq,
+                     float *v, cudaStream_t s) {
+  if constexpr (Q <= 6) {
+    if (qdata32) return launch_ijacobian_pair<P, Q, SV, true>(op, ctx, qdata, qdata32, jd, dq, v, s);
+    return launch_ijacobian_pair<P, Q, SV, false>(op, ctx, qdata, nullptr, jd, dq, v, s);
+  }
   return launch_ijacobian<P, Q, float, SV>(op, ctx, qdata, jd, dq, v, s);
 }
 
@@ -2119,11 +2213,12 @@ extern "C" int hb_ifunction_apply_sgs(const HbElemOp *op, const void *ctx184, co
 }
 
 template <typename T, int SV>
-static int ijacobian_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v, cudaStream_t s) {
+static int ijacobian_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v, cudaStream_t s,
+                        const float *qdata32 = nullptr) {
   if constexpr (sizeof(T) == 4 && SV == HB_STATEVAR_CONSERVATIVE) {  // FP32: element pairs in packed FP32 where the basis allows
     if (((uintptr_t)qdata % 16) == 0 && op->Q <= 6) {
 #define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return pair_case<PP, QQ, SV>(op, ctx, qdata, (const float *)jd, (const float *)dq, (float *)v, s);
+  if (op->P == PP && op->Q == QQ) return pair_case<PP, QQ, SV>(op, ctx, qdata, qdata32, (const float *)jd, (const float *)dq, (float *)v, s);
       HB_PQ_LIST(HB_CASE)
 #undef HB_CASE
     }
@@ -2154,8 +2249,8 @@ extern "C" int hb_ijacobian_apply_f64(const HbElemOp *op, const void *ctx184, co
   return ijacobian_pq<double, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, dq, v, s);
 }
 
-extern "C" int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, const float *dq,
-                                      float *v, int add, void *stream) {
+extern "C" int hb_ijacobian_apply_f32x(const HbElemOp *op, const void *ctx184, const double *qdata, const float *qdata_f32, const float *jac_data,
+                                       const float *dq, float *v, int add, void *stream) {
   int err = check_op(op);
   if (err) return err;
   HbNewtonianContext ctx;
@@ -2166,7 +2261,12 @@ extern "C" int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, co
   if (!add && cudaMemsetAsync(v, 0, sizeof(float) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
   if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return ijacobian_pq<float, HB_STATEVAR_PRIMITIVE>(op, ctx, qdata, jac_data, dq, v, s);
   if (ctx.state_var == HB_STATEVAR_ENTROPY) return ijacobian_pq<float, HB_STATEVAR_ENTROPY>(op, ctx, qdata, jac_data, dq, v, s);
-  return ijacobian_pq<float, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, dq, v, s);
+  return ijacobian_pq<float, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, dq, v, s, qdata_f32);
+}
+
+extern "C" int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, const float *dq,
+                                      float *v, int add, void *stream) {
+  return hb_ijacobian_apply_f32x(op, ctx184, qdata, nullptr, jac_data, dq, v, add, stream);
 }
 
 template <typename T, int SV>

@@ -265,6 +265,138 @@ class NewtonianOperators:
         self.boundaries.append(bc)
         return bc
 
+    # ---- data-driven SGS model, fused nodal implementation (problems/sgs_dd_model.c:645-737)
+    def add_sgs_dd(self, flat_params, bounds, alpha=0.0, aniso_rtol=1e-10):
+        """SgsDDSetup for a box mesh: the velocity-gradient projection (src/velocity_gradient_projection.c:44-140: right-hand
+        side ``VelocityGradientProjectionRHS_*`` and ``Mass_9``, solved by one row-sum Jacobi step), the anisotropy tensor
+        projected once (src/grid_anisotropy_tensor.c:10-118: ``AnisotropyTensorProjection``, ``Mass_7``, CG with Jacobi to
+        ``aniso_rtol`` in the natural norm), the local inverse multiplicity (src/inverse_multiplicity.c:24-80), the nodal
+        closure ``ComputeSgsDDNodal_*`` with the network's ``SgsDDContext_`` (flat_params and bounds in the layout of
+        sgs.load_reference_model) and the residual term ``IFunction_NodalSgs_*``.  Afterwards :meth:`ifunction` adds the SGS
+        term as IFunction_NS does through SgsDDApplyIFunction (problems/sgs_dd_model.c:559-587)."""
+        from .sgs import sgs_dd_context
+        ceed, mesh, basis = self.ceed, self.mesh, self.basis
+        P, Q, E, N = basis.P, basis.Q, mesh.num_elem, mesh.num_nodes
+        a, none_b = ceed.active, ceed.basis_none
+        sv_name = ("Conserv", "Prim", "Entropy")[self.ctx.state_var]
+        keep = []
+
+        def rstr(nc):  # DMPlexCeedElemRestrictionCreate on the nc-field clone of the solution DM
+            return ce.ElemRestriction(ceed, E, P ** 3, nc, 1, N * nc, offsets=(mesh.offsets // 5) * nc)
+
+        def bas(nc):
+            return ce.Basis(ceed, 3, nc, P, Q, basis.interp1d, basis.grad1d, basis.qref1d, basis.qweight1d)
+
+        def qfunction(name, ins, outs, ctx=None):
+            q = ce.QFunction(ceed, name)
+            for nm, size, mode in ins:
+                q.add_input(nm, size, mode)
+            for nm, size, mode in outs:
+                q.add_output(nm, size, mode)
+            if ctx is not None:
+                q.set_context(ctx)
+            keep.append(q)
+            return q
+
+        def operator(qf, fields, name):
+            op = ce.Operator(ceed, qf)
+            op.set_name(name)
+            for nm, r, b, v in fields:
+                op.set_field(nm, r, b, v)
+            keep.append(op)
+            return op
+
+        def mass(nc, r, b):
+            qf = qfunction(f"mass.h:Mass_{nc}", [("u", nc, ce.CEED_EVAL_INTERP), ("qdata", 10, ce.CEED_EVAL_NONE)], [("v", nc, ce.CEED_EVAL_INTERP)])
+            return operator(qf, [("u", r, b, a), ("qdata", self.rstr_qd, none_b, self.q_data), ("v", r, b, a)], f"Mass_{nc}")
+
+        r9, r7, r6, b9, b7, b6 = rstr(9), rstr(7), rstr(6), bas(9), bas(7), bas(6)
+        keep += [r9, r7, r6, b9, b7, b6]
+        # -- velocity-gradient projection
+        qf = qfunction(f"velocity_gradient_projection.h:VelocityGradientProjectionRHS_{sv_name}",
+                       [("q", 5, ce.CEED_EVAL_INTERP), ("Grad_q", 15, ce.CEED_EVAL_GRAD), ("qdata", 10, ce.CEED_EVAL_NONE), ("x", 3, ce.CEED_EVAL_INTERP)],
+                       [("velocity gradient", 9, ce.CEED_EVAL_INTERP)], self.qfctx)
+        self.op_sgs_velgrad = operator(qf, [("q", self.rstr_q, self.basis_q, a), ("Grad_q", self.rstr_q, self.basis_q, a),
+                                            ("qdata", self.rstr_qd, none_b, self.q_data), ("x", self.rstr_x, self.basis_x, self.x_coord),
+                                            ("velocity gradient", r9, b9, a)], "velocity gradient projection RHS")
+        op_m9 = mass(9, r9, b9)
+        ones, self.sgs_rowsum_inv = ce.Vector(ceed, N * 9), ce.Vector(ceed, N * 9)
+        ones.set_value(1.0)
+        op_m9.apply(ones, self.sgs_rowsum_inv)  # PC_JACOBI_ROWSUM: MatGetRowSum = M 1
+        self.sgs_rowsum_inv.reciprocal()
+        # -- anisotropy tensor, projected once
+        qf = qfunction("grid_anisotropy_tensor.h:AnisotropyTensorProjection", [("qdata", 10, ce.CEED_EVAL_NONE)], [("v", 7, ce.CEED_EVAL_INTERP)])
+        op_a = operator(qf, [("qdata", self.rstr_qd, none_b, self.q_data), ("v", r7, b7, a)], "anisotropy tensor projection RHS")
+        op_m7 = mass(7, r7, b7)
+        rhs, diag, tmp = ce.Vector(ceed, N * 7), ce.Vector(ceed, N * 7), ce.Vector(ceed, N * 7)
+        op_a.apply(None, rhs)
+        op_m7.assemble_diagonal(diag)
+        b_h, dinv = rhs.to_numpy(), 1.0 / diag.to_numpy()
+
+        def m7(x):
+            tmp.set_array_host(x)
+            out = ce.Vector(ceed, N * 7)
+            op_m7.apply(tmp, out)
+            return out.to_numpy()
+
+        x = np.zeros_like(b_h)
+        r = b_h.copy()
+        z = dinv * r
+        p = z.copy()
+        rz = rz0 = float(r @ z)
+        for _ in range(1000):  # KSPCG, KSP_NORM_NATURAL, PCJACOBI diagonal (src/grid_anisotropy_tensor.c:84-95)
+            if rz <= aniso_rtol * aniso_rtol * rz0:
+                break
+            Ap = m7(p)
+            al = rz / float(p @ Ap)
+            x += al * p
+            r -= al * Ap
+            z = dinv * r
+            rz_new = float(r @ z)
+            p = z + (rz_new / rz) * p
+            rz = rz_new
+        self.sgs_aniso = ce.Vector(ceed, N * 7)
+        self.sgs_aniso.set_array_host(x)
+        # -- inverse multiplicity (local)
+        r_inv = ce.ElemRestriction(ceed, E, P ** 3, 1, None, E * P ** 3)
+        mult = ce.Vector(ceed, N * 6)
+        mult.set_value(0.0)
+        r6.multiplicity(mult)
+        qf = qfunction("inverse_multiplicity.h:InverseMultiplicity", [("multiplicity", 6, ce.CEED_EVAL_NONE)], [("inverse multiplicity", 1, ce.CEED_EVAL_NONE)])
+        op_im = operator(qf, [("multiplicity", r6, none_b, a), ("inverse multiplicity", r_inv, none_b, a)], "InverseMultiplicity")
+        self.sgs_inv_mult = ce.Vector(ceed, E * P ** 3)
+        op_im.apply(mult, self.sgs_inv_mult)
+        keep += [r_inv, mult]
+        # -- nodal closure
+        self.sgs_ctx_blob = sgs_dd_context(context_bytes(self.ctx), flat_params, bounds, alpha)
+        self.sgs_qfctx = ce.QFunctionContext(ceed, self.sgs_ctx_blob)
+        basis_x_to_q = ce.Basis.projection(self.basis_x, self.basis_q)
+        keep.append(basis_x_to_q)
+        self.sgs_q, self.sgs_grad_velo, self.sgs_km = ce.Vector(ceed, mesh.l_size), ce.Vector(ceed, N * 9), ce.Vector(ceed, N * 6)
+        qf = qfunction(f"sgs_dd_model.h:ComputeSgsDDNodal_{sv_name}",
+                       [("q", 5, ce.CEED_EVAL_NONE), ("x", 3, ce.CEED_EVAL_INTERP), ("gradient velocity", 9, ce.CEED_EVAL_NONE),
+                        ("anisotropy tensor", 7, ce.CEED_EVAL_NONE), ("inverse multiplicity", 1, ce.CEED_EVAL_NONE)],
+                       [("km_sgs", 6, ce.CEED_EVAL_NONE)], self.sgs_qfctx)
+        self.op_sgs_nodal = operator(qf, [("q", self.rstr_q, none_b, self.sgs_q), ("x", self.rstr_x, basis_x_to_q, self.x_coord),
+                                          ("gradient velocity", r9, none_b, a), ("anisotropy tensor", r7, none_b, self.sgs_aniso),
+                                          ("inverse multiplicity", r_inv, none_b, self.sgs_inv_mult), ("km_sgs", r6, none_b, a)],
+                                     "nodal data-driven SGS")
+        # -- SGS residual term
+        qf = qfunction(f"sgs_dd_model.h:IFunction_NodalSgs_{sv_name}",
+                       [("q", 5, ce.CEED_EVAL_INTERP), ("qdata", 10, ce.CEED_EVAL_NONE), ("km_sgs", 6, ce.CEED_EVAL_INTERP)],
+                       [("Grad_v", 15, ce.CEED_EVAL_GRAD)], self.qfctx)
+        self.op_sgs_apply = operator(qf, [("q", self.rstr_q, self.basis_q, a), ("qdata", self.rstr_qd, none_b, self.q_data),
+                                          ("km_sgs", r6, b6, self.sgs_km), ("Grad_v", self.rstr_q, self.basis_q, a)], "SGS residual")
+        self._sgs_keep = keep
+
+    def sgs_stress(self, q: ce.Vector) -> ce.Vector:
+        """The nodal SGS stress (KM, [node][6]) of the state q: VelocityGradientProjectionApply, then the nodal closure."""
+        self.op_sgs_velgrad.apply(q, self.sgs_grad_velo)
+        self.sgs_grad_velo.pointwise_mult(self.sgs_grad_velo, self.sgs_rowsum_inv)
+        q.copy_to(self.sgs_q)  # q_ceed is the closure's implicit input (problems/sgs_dd_model.c:105)
+        self.op_sgs_nodal.apply(self.sgs_grad_velo, self.sgs_km)
+        return self.sgs_km
+
     # ---- context updates (src/setupts.c:91-93, :141)
     def set_time(self, t):
         self.op_ifunction.set_context_double("solution time", [t])
@@ -280,6 +412,9 @@ class NewtonianOperators:
         """G = F(q, q_dot): HONEE points its q_dot CeedVector at the PETSc array, then applies (src/setupts.c:102-109)."""
         q_dot.copy_to(self.q_dot) if q_dot is not self.q_dot else None
         self.op_ifunction.apply(q, g)
+        if getattr(self, "op_sgs_apply", None) is not None:  # SgsDDApplyIFunction (src/setupts.c:118-120)
+            self.sgs_stress(q)
+            self.op_sgs_apply.apply(q, g, add=True)
 
     def ijacobian(self, dq: ce.Vector, out: ce.Vector, add=False):
         self.op_ijacobian.apply(dq, out, add=add)

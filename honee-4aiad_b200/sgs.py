@@ -162,6 +162,14 @@ def point_inputs(G, kmA, delta, nu, inputs, E, gmag, stream=None):
                                _stream(stream)), "hb_sgs_inputs")
 
 
+def nodal_closure(ctx_blob, state_var, q, G, A, w, km_sgs, stream=None):
+    """km_sgs [n][6] += w [n] tau: the closure of an SgsDDContext_ blob at n nodes (hb_sgs_nodal_closure) from q [n][5] in
+    state_var, the velocity gradient G [n][9] and the anisotropy tensor with width A [n][7] (device tensors)."""
+    n = w.shape[0]
+    _chk(_load().hb_sgs_nodal_closure(C.c_int64(n), C.cast(C.pointer(ctx_blob), C.c_void_p), C.c_size_t(C.sizeof(ctx_blob)), C.c_int(state_var),
+                                      _addr(q), _addr(G), _addr(A), _addr(w), _addr(km_sgs), _stream(stream)), "hb_sgs_nodal_closure")
+
+
 def point_stress(out_n, delta, E, gmag, bounds, km_tau, stream=None):
     b = (C.c_float * 12)(*[float(x) for x in np.asarray(bounds).reshape(12)])
     _chk(_load().hb_sgs_stress(C.c_int64(out_n.shape[0]), _addr(out_n), _addr(delta), _addr(E), _addr(gmag), b, _addr(km_tau),

@@ -111,3 +111,35 @@ def test_sgs_dd_context_blob_runs_the_reference_closure():
     O.call_qf(R.ref_ComputeSgsDDNodal_Conserv, blob, n, [GOLD["q_Conserv"], GOLD["x"], np.ascontiguousarray(GOLD["G"].transpose(1, 2, 0)),
                                                          GOLD["Aij_delta"], GOLD["inv_mult"]], [out])
     np.testing.assert_array_equal(out, GOLD["km_sgs_Conserv"])
+
+
+def test_nodal_pipeline_closure_matches_reference_on_a_mesh():
+    """SN.sgs_nodal on a small mesh with a generic state (all velocity components perturbed) equals the reference's
+    ComputeSgsDDNodal_Prim at every node (skipped without oracle/_ref).  At degenerate states (v = w = 0: repeated
+    strain-rate eigenvalues, an eigenframe orthogonal to the vorticity) the reference's own result depends on rounding."""
+    import oracle as O
+    R = O.ref()
+    if R is None:
+        pytest.skip("oracle/_ref not built")
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    sgs = importlib.import_module("honee-4aiad_b200.sgs")
+    mesh = prob.box_mesh((2, 2, 1), 3, periodic=(True, False, False))
+    basis = prob.tensor_basis(3, 4)
+    ctx = prob.newtonian_context(2, cv=717.5, cp=1004.5, mu=1.8e-5, k=0.0257, state_var=1)
+    gas = ctx.gas
+    q = prob.multimode_state(mesh, basis, gas, seed=4).reshape(-1, 5).copy()
+    rng = np.random.default_rng(8)
+    q[:, 2:4] += q[:, 0:1] * rng.normal(0, 2.0, (q.shape[0], 2))
+    q = prob.state_to_q(gas, q.reshape(-1), 1)
+    qdata = O.setup_qdata(mesh.num_elem, basis.Q, mesh.x_elem)
+    A7 = SN.project_cg(mesh, basis, qdata, SN.aniso_rhs(mesh, basis, qdata), 7, rtol=1e-12)
+    G9 = SN.project_rowsum(mesh, basis, qdata, SN.velgrad_rhs(mesh, basis, qdata, q, 1, gas.cv, gas.cp), 9)
+    km = SN.sgs_nodal(mesh, SN.Net(SGS["weights"], SGS["bounds"]), q, G9, A7, SN.inverse_multiplicity(mesh), 1, gas.mu, gas.cv, gas.cp)
+    N = mesh.num_nodes
+    blob = bytes(sgs.sgs_dd_context(prob.context_bytes(ctx), SGS["weights"], SGS["bounds"]))
+    out = np.zeros((6, N))
+    O.call_qf(R.ref_ComputeSgsDDNodal_Prim, blob, N, [np.ascontiguousarray(q.reshape(N, 5).T), np.zeros((3, N)),
+                                                      np.ascontiguousarray(G9.reshape(N, 3, 3).transpose(1, 2, 0)),
+                                                      np.ascontiguousarray(A7.reshape(N, 7).T), np.ones(N)], [out])
+    ref = out.T.reshape(-1)
+    assert np.linalg.norm(km - ref) / np.linalg.norm(ref) < 1e-13
