@@ -2375,19 +2375,12 @@ static int op_apply_add_single(CeedOperator op, CeedVector in, CeedVector out) {
           CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_in32, sizeof(float) * (size_t)n));
           CUDA_CK(ceed, cudaMalloc((void **)&op->d_tmp_out32, sizeof(float) * (size_t)n));
         }
-        /* qdata rounded to FP32 once (its shadow, refreshed whenever qdata is written): the FP32 action reads half the bytes */
-        CeedVector qv = op->in[2].v;
-        if (!qv->f32_valid) {
-          CK(vec_f32_shadow(qv));
-          HB_CK(ceed, hb_vec_f64_to_f32(qd, qv->d_f32, qv->length, 0, s));
-          qv->f32_valid = 1;
-        }
         const double *x;
         double       *y;
         CK(vec_dev_read(in, &x));
         CK(vec_dev_write(out, &y, 0));
         HB_CK(ceed, hb_vec_f64_to_f32(x, op->d_tmp_in32, n, 0, s));
-        HB_CK(ceed, hb_ijacobian_apply_f32x(op->eop, ctx, qd, qv->d_f32, jd->d_f32, op->d_tmp_in32, op->d_tmp_out32, 0, s));
+        HB_CK(ceed, hb_ijacobian_apply_f32(op->eop, ctx, qd, jd->d_f32, op->d_tmp_in32, op->d_tmp_out32, 0, s));
         HB_CK(ceed, hb_vec_f32_to_f64(op->d_tmp_out32, y, n, 1, s));
       } else {
         const double *j64, *x;

@@ -26,7 +26,6 @@ struct HbTimeStepper {
   const HbElemOp    *op;
   HbNewtonianContext ctx;
   const double      *qdata;
-  float             *qdata32;   /* qdata rounded to FP32 once at creation (mixed precision: the FP32 Jacobian reads it) */
   HbSolverOptions    o;
   int64_t            n, ldv; /* ldv: row stride of the Krylov basis, n rounded up so every row starts 16-byte aligned */
   int                njd, steps_taken;
@@ -116,9 +115,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
   err |= cudaMalloc((void **)&ts->scratch, sizeof(double) * 1024);
   err |= cudaMalloc(&ts->V, ksz(ts) * (size_t)ts->ldv * (m + 1)) | cudaMalloc(&ts->w, ksz(ts) * (size_t)ts->n);
   err |= cudaMalloc(&ts->zvec, ksz(ts) * (size_t)ts->n) | cudaMalloc(&ts->diag, ksz(ts) * (size_t)ts->n);
-  if (ts->o.jacobian_fp32)
-    err |= cudaMalloc(&ts->jd32, sizeof(float) * njd) | cudaMalloc((void **)&ts->res32, sizeof(float) * (size_t)ts->n) |
-           cudaMalloc((void **)&ts->qdata32, sizeof(float) * 10 * Q3 * (size_t)op->num_elem);
+  if (ts->o.jacobian_fp32) err |= cudaMalloc(&ts->jd32, sizeof(float) * njd) | cudaMalloc((void **)&ts->res32, sizeof(float) * (size_t)ts->n);
   else err |= cudaMalloc((void **)&ts->jd64, sizeof(double) * njd);
   if (ts->o.jfnk) err |= cudaMalloc((void **)&ts->qp, nb) | cudaMalloc((void **)&ts->qdp, nb) | cudaMalloc((void **)&ts->rp, nb);
   if (ts->o.pc_jacobi == 2) {
@@ -129,10 +126,6 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
     hb_ts_destroy(ts);
     return HB_ERROR_NOMEM;
   }
-  if (ts->qdata32 && (err = hb_vec_f64_to_f32(d_qdata, ts->qdata32, (int64_t)(10 * Q3 * (size_t)op->num_elem), 0, ts->s))) {
-    hb_ts_destroy(ts);
-    return err;
-  }
   *out = ts;
   return HB_SUCCESS;
 }
@@ -140,8 +133,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
 int hb_ts_destroy(HbTimeStepper *ts) {
   if (!ts) return HB_SUCCESS;
   void *p[] = {ts->q, ts->q_prev, ts->q_prev2, ts->z, ts->qdot, ts->res, ts->delta, ts->d_partial, ts->d_dots, ts->scratch,
-               ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64, ts->qp, ts->qdp, ts->rp, ts->pb64, ts->pb32, ts->d_sing,
-               ts->qdata32};
+               ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64, ts->qp, ts->qdp, ts->rp, ts->pb64, ts->pb32, ts->d_sing};
   for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
     if (p[i]) cudaFree(p[i]);
   free(ts->sgs_w);
@@ -275,7 +267,7 @@ static int jac_fd(HbTimeStepper *ts, const double *x, double *y) {
 static int kv_jac(HbTimeStepper *ts, const void *x, void *y) {
   if (ts->o.jfnk) return jac_fd(ts, (const double *)x, (double *)y);
   if (ts->o.jacobian_fp32) {
-    HBCK(hb_ijacobian_apply_f32x(ts->op, &ts->ctx, ts->qdata, ts->qdata32, (const float *)ts->jd32, (const float *)x, (float *)y, 0, ts->s));
+    HBCK(hb_ijacobian_apply_f32(ts->op, &ts->ctx, ts->qdata, (const float *)ts->jd32, (const float *)x, (float *)y, 0, ts->s));
     if (ts->bc) HBCK(hb_freestream_jacobian_apply_f32(ts->bc, ts->bc_ctx, ts->bc_flux, ts->bc_qdata, ts->bc_jac, (const float *)x, (float *)y, ts->s));
     if (ts->ess_n) HBCK(hb_constrain_set_f32((float *)y, ts->ess_idx, NULL, ts->ess_n, ts->s));
     return HB_SUCCESS;

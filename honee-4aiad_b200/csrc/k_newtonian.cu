@@ -165,9 +165,9 @@ struct QRef {
 //   * its node values (state, time derivative) by cp.async, issued once the first fibre pass has consumed e's values
 //   * its per-point blocks (qdata, stored Jacobian data) by TMA bulk copies on an mbarrier, issued after e's point-wise
 //     phase has consumed e's blocks
-//   * the current values of the output L-vector at its nodes by cp.async, issued after e's scatter
-// so each element starts with all its inputs resident.  Elements of one colour share no node, so the output values
-// gathered ahead are still current when the element scatters (a plain store of old + contribution, no atomics).
+// so each element starts with all its inputs resident.  The element's contribution is added to the output L-vector by
+// reductions without return (scatter_add): elements of one colour share no node, so each entry receives one addition per
+// launch and the result equals a load-add-store, with no output values staged and no thread waiting on them.
 
 // Offsets of the entries a thread handles in a 5-component node gather/scatter: entries t = threadIdx.x + j*NT
 // (node t/5, component t%5).  They are loaded into registers one element ahead (so no gather waits on them) and kept in
@@ -217,17 +217,6 @@ __device__ __forceinline__ void gather_async(const EntryOffsets<P, NT> &eo, cons
         else cp_async4(&sN[(5 + c) * PS + srow], l1 + o);
       }
     }
-  }
-}
-
-// Gather the output L-vector at one element's nodes, node-major sV [P3][5] (the layout of the scatter); sO holds the
-// element's entry offsets (EntryOffsets::store).
-template <int P, int NT, typename T>
-__device__ __forceinline__ void gather_out_async(const int32_t *sO, const T *l_out, T *sV) {
-  constexpr int P3 = P * P * P;
-  for (int t = threadIdx.x; t < 5 * P3; t += NT) {
-    if (sizeof(T) == 8) cp_async8(&sV[t], l_out + sO[t]);
-    else cp_async4(&sV[t], l_out + sO[t]);
   }
 }
 
@@ -429,16 +418,17 @@ __device__ __forceinline__ void transpose_passes(const Basis1D<T> &bas, const T 
   __syncthreads();
 }
 
-// out[o] = old + contribution; elements of one colour share no node, so `old` (gathered ahead) is current.
+// out[o] += contribution, node-major sF [P3][5] at the element's entry offsets sO.  Elements of one colour share no node,
+// so every entry receives exactly one addition per launch: a reduction without return (red.global.add, performed at L2)
+// gives the same sum as a load-add-store, in any order, and leaves no thread waiting for the old value.
 template <int P, int NT, typename T>
-__device__ __forceinline__ void scatter_store(const int32_t *sO, const T *sV, const T *sF, T *l_out) {
+__device__ __forceinline__ void scatter_add(const int32_t *sO, const T *sF, T *l_out) {
   constexpr int P3 = P * P * P;
-  for (int t = threadIdx.x; t < 5 * P3; t += NT) l_out[sO[t]] = sV[t] + sF[t];
+  for (int t = threadIdx.x; t < 5 * P3; t += NT) atomicAdd(l_out + sO[t], sF[t]);
 }
 
 // Shared-memory plan (in units of T unless noted):
 //   sN  [NV*5][P][P][PX] staged node values (x rows padded to odd PX) of the element being computed / the next one
-//   sV  [P3][5]         staged output values at the element's nodes
 //   s1  [NV*5][P][P][Q] x-pass output; later sT2 (transpose scratch)
 //   s2  [NV*5][P][Q][Q] y-pass output; later w2 and the final node values
 //   sU  [10][Q3]        interpolated values (q, then q_dot or w1); point-wise outputs v in place
@@ -449,13 +439,13 @@ template <int P, int Q, int NV, typename T, bool JD, bool ST = true>
 struct Plan {
   static constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
   static constexpr int cmax(int x, int y) { return x > y ? x : y; }
-  static constexpr int nN = NV * 5 * P * P * padded_row<P>(), nV = 5 * P3, nU = 10 * Q3, nG = 15 * Q3;
+  static constexpr int nN = NV * 5 * P * P * padded_row<P>(), nU = 10 * Q3, nG = 15 * Q3;
   static constexpr int n1 = cmax(NV * 5 * P * P * Q, 5 * P * Q2);          // x-pass output, then sT2
   static constexpr int n2 = cmax(cmax(NV * 5 * P * Q2, 5 * Q3), 5 * P3);   // y-pass output, then w2 and node values
   static constexpr int nJD = (JD && ST) ? 15 * Q3 : 0;
   static constexpr int kAl = 16 / (int)sizeof(T);
   static constexpr int pad(int n) { return (n + kAl - 1) / kAl * kAl; }  // every buffer 16-byte aligned (bulk copies)
-  static constexpr int oN = 0, oV = pad(oN + nN), o1 = pad(oV + nV), o2 = pad(o1 + n1), oU = pad(o2 + n2), oG = pad(oU + nU),
+  static constexpr int oN = 0, o1 = pad(oN + nN), o2 = pad(o1 + n1), oU = pad(o2 + n2), oG = pad(oU + nU),
                        oJD = pad(oG + nG), end_T = pad(oJD + nJD);
   static constexpr size_t qd_offset_bytes = ((size_t)end_T * sizeof(T) + 15) & ~(size_t)15;
   // staged qdata precedes the mbarriers: two buffers for the residual (NV == 2), one for the Jacobian
@@ -558,7 +548,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
   constexpr int Q3 = L::Q3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sm = reinterpret_cast<double *>(smem_raw);
-  double *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
+  double *sN = sm + L::oN, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
   double *sD = sU + 5 * Q3;
   double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::mbar_offset);
@@ -596,9 +586,6 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
       }
     } else if (threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)e0 * 10 * Q3, qd_bytes);
     cp_async_commit();
-    __syncthreads();
-    gather_out_async<P, NT, double>(sO[0], p.v, sV);
-    cp_async_commit();
   }
   unsigned kit = 0;  // elements done by this CTA: qdata buffer kit & 1, its mbarrier phase parity (kit >> 1) & 1
   // element ids and entry offsets are read two elements ahead so no global load latency sits on the critical path
@@ -615,8 +602,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     if (idx + 3 * G < a.n_elems) en3 = __ldg(a.elems + idx + 3 * G);
     if (en2 >= 0) nxt2.load(a.offsets, en2);
     HB_PT(7)
-    // everything but the most recent group (the output gather, only needed at the scatter) has landed
-    cp_async_wait_group<1>();
+    cp_async_wait_group<0>();  // this element's node values have landed
     HB_PT(8)
     if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar + (kit & 1), (kit >> 1) & 1)) {
       s_bail = 1;
@@ -701,19 +687,10 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     HB_PT(4)
     transpose_passes<P, Q, NT, double>(a.basis, sU, sG, sD, s2, s1, sG, s2);
     HB_PT(5)
-    if (en >= 0) cp_async_wait_group<2>();  // the output gather, committed before this element's two stagings
-    else cp_async_wait_group<0>();
-    HB_PT(10)
-    __syncthreads();
-    HB_PT(11)
-    scatter_store<P, NT, double>(sO[buf], sV, s2, p.v);
+    scatter_add<P, NT, double>(sO[buf], s2, p.v);
     HB_PT(12)
     __syncthreads();
     buf ^= 1;
-    if (en >= 0) {
-      gather_out_async<P, NT, double>(sO[buf], p.v, sV);
-      cp_async_commit();
-    }
     ecur = en;
     en = en2;
     en2 = en3;
@@ -747,7 +724,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
   constexpr int Q3 = L::Q3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
-  T *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG, *sJD = sm + L::oJD;
+  T *sN = sm + L::oN, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG, *sJD = sm + L::oJD;
   T *sW1 = sU + 5 * Q3;
   double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::mbar_offset);
@@ -782,9 +759,6 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
       prefetch_l2_bulk(p.jac_data + (int64_t)e0 * njd * Q3, jd_bytes);
     }
     cp_async_commit();
-    __syncthreads();
-    gather_out_async<P, NT, T>(sO[0], p.v, sV);
-    cp_async_commit();
   }
   unsigned phase = 0;
   // element ids and entry offsets are read two elements ahead so no global load latency sits on the critical path
@@ -799,8 +773,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
     int en3 = -1;  // used one iteration later: a predicated load, so nothing waits for it here
     if (idx + 3 * G < a.n_elems) en3 = __ldg(a.elems + idx + 3 * G);
     if (en2 >= 0) nxt2.load(a.offsets, en2);
-    // everything but the most recent group (the output gather, only needed at the scatter) has landed
-    cp_async_wait_group<1>();
+    cp_async_wait_group<0>();  // this element's node values (and point data staged by cp.async) have landed
     if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
       s_bail = 1;
       atomicOr(a.status, 1);
@@ -868,16 +841,9 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
       cp_async_commit();
     }
     transpose_passes<P, Q, NT, T>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
-    if (en >= 0) cp_async_wait_group<2>();
-    else cp_async_wait_group<0>();
-    __syncthreads();
-    scatter_store<P, NT, T>(sO[buf], sV, s2, p.v);
+    scatter_add<P, NT, T>(sO[buf], s2, p.v);
     __syncthreads();
     buf ^= 1;
-    if (en >= 0) {
-      gather_out_async<P, NT, T>(sO[buf], p.v, sV);
-      cp_async_commit();
-    }
     ecur = en;
     en = en2;
     en2 = en3;
@@ -893,39 +859,16 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
 // lane recomputes the first and is not stored): the node values of both are gathered into the two lanes of one 8-byte
 // slot, every basis pass and the point-wise tangent run once for both lanes, and the scatter stores each lane at its own
 // element's nodes.  Same arithmetic per lane as k_ijacobian<float> (FP32 values and Jacobian data, FP64 qdata rounded to
-// FP32 at the point), half the instructions.
-//   Q32 = false: qdata of both elements (FP64) is staged by TMA; their Jacobian data are read at the point from global
-//                memory (coalesced per component, warmed in L2 one pair ahead), which keeps three CTAs per SM.
-//   Q32 = true:  qdata comes already rounded to FP32 ([E][10][Q3], the values every point rounds it to anyway), so the
-//                pair's qdata and Jacobian data (24 KB) both fit in shared memory at three CTAs per SM: both are staged
-//                by cp.async for the next pair while this pair finishes, and no global load is left in the point-wise
-//                phase.  Half the qdata bytes, bit-identical results.
+// FP32 at the point), half the instructions.  qdata of both elements is staged by TMA; their Jacobian data are read at
+// the point from global memory (coalesced per component, warmed in L2 one pair ahead), which keeps three CTAs per SM.
 
 struct IjacobianPairPtrs {
   const float *dq;
   const float *jac_data;  // [E][num_jd][Q3]
   float *v;
-  const float *qdata32;   // [E][10][Q3] FP32 qdata (Q32 kernels)
-  int jd8, qd8;           // the Jacobian data / FP32 qdata of every element can be copied in 8-byte chunks
 };
 
-constexpr int kPairJdMax = 15;  // Jacobian-data components staged per element (14, or 15 with the IDL)
-// floats between the two lanes' staged Jacobian data: 15 Q^3 rounded up to a multiple of 4, so the second lane's buffer
-// starts 16-byte aligned (8-byte cp.async needs an 8-byte aligned shared-memory destination)
-__host__ __device__ constexpr int pair_jd_stride(int Q3) { return (kPairJdMax * Q3 + 3) & ~3; }
-
-// copy a contiguous block of n floats into shared memory with cp.async (8-byte chunks when both ends are 8-byte aligned
-// and n is even, else 4-byte)
-template <int NT>
-__device__ __forceinline__ void stage_floats_async(float *dst, const float *src, int n, bool by8) {
-  if (by8) {
-    for (int i = threadIdx.x; i < n / 2; i += NT) cp_async8(dst + 2 * i, src + 2 * i);
-  } else {
-    for (int i = threadIdx.x; i < n; i += NT) cp_async4(dst + i, src + i);
-  }
-}
-
-// node gathers into one lane (byte offset 0 or 4) of the pair slots: sN [5][P][P][PX], sV [P3][5]
+// node gathers into one lane (byte offset 0 or 4) of the pair slots: sN [5][P][P][PX]
 template <int P, int NT>
 __device__ __forceinline__ void gather_lane_async(const EntryOffsets<P, NT> &eo, const float *l, f2 *sN, int lane) {
   constexpr int P3 = P * P * P, PX = padded_row<P>(), PS = P * P * PX;
@@ -938,39 +881,18 @@ __device__ __forceinline__ void gather_lane_async(const EntryOffsets<P, NT> &eo,
     }
   }
 }
-template <int P, int NT>
-__device__ __forceinline__ void gather_out_lane_async(const int32_t *sO, const float *l_out, f2 *sV, int lane) {
-  constexpr int P3 = P * P * P;
-  for (int t = threadIdx.x; t < 5 * P3; t += NT) cp_async4(reinterpret_cast<float *>(&sV[t]) + lane, l_out + sO[t]);
-}
 
-template <int P, int Q, bool Q32>
-struct PairPlan {
-  using L = Plan<P, Q, 1, f2, false, false>;
-  static constexpr int Q3 = L::Q3;
-  // staged point data after the basis buffers: FP64 qdata [2][10][Q3] (Q32 = false) or FP32 qdata [2][10][Q3] and
-  // Jacobian data [2][kPairJdMax][Q3] (Q32 = true); then the mbarrier
-  static constexpr size_t stage_bytes = Q32 ? sizeof(float) * (2 * 10 * Q3 + 2 * pair_jd_stride(Q3)) : sizeof(double) * 2 * 10 * Q3;
-  static_assert((sizeof(float) * 10 * Q3) % 8 == 0, "second lane's qdata 8-byte aligned");
-  static_assert((sizeof(float) * pair_jd_stride(Q3)) % 16 == 0, "second lane's Jacobian data 16-byte aligned");
-  static constexpr size_t mbar_offset = (L::qd_offset_bytes + stage_bytes + 15) & ~(size_t)15;
-  static constexpr size_t bytes = mbar_offset + 16;
-};
-
-template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE, bool Q32 = false>
+template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
 __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ijacobian_pair(const ElemArgs<f2> a, const IjacobianPairPtrs p) {
   constexpr int NT = nthreads_for<float>(Q);
   using L = Plan<P, Q, 1, f2, false, false>;
-  using PL = PairPlan<P, Q, Q32>;
   constexpr int Q3 = L::Q3, P3 = L::P3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   f2 *sm = reinterpret_cast<f2 *>(smem_raw);
-  f2 *sN = sm + L::oN, *sV = sm + L::oV, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
+  f2 *sN = sm + L::oN, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
   f2 *sW1 = sU + 5 * Q3;
-  double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);  // [2][10][Q3]: the pair's qdata (Q32 = false)
-  float *sQ32 = reinterpret_cast<float *>(smem_raw + L::qd_offset_bytes);   // [2][10][Q3]: the pair's FP32 qdata (Q32)
-  float *sJD = sQ32 + 2 * 10 * Q3;                                          // [2][pair_jd_stride]: its Jacobian data (Q32)
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + PL::mbar_offset);
+  double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);  // [2][10][Q3]: the pair's qdata
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + 2 * sizeof(double) * 10 * Q3);
   __shared__ int s_bail;
   __shared__ int32_t sO[2][2][5 * P3];  // entry offsets of the current / next pair, per lane
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
@@ -987,19 +909,9 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
     tma_load_1d(sQD, a.qdata + (int64_t)eA * 10 * Q3, qd_bytes, mbar);
     tma_load_1d(sQD + 10 * Q3, a.qdata + (int64_t)eB * 10 * Q3, qd_bytes, mbar);
   };
-  auto stage_points32 = [&](int eA, int eB) {  // all threads: both elements' FP32 qdata and Jacobian data by cp.async
-    stage_floats_async<NT>(sQ32, p.qdata32 + (int64_t)eA * 10 * Q3, 10 * Q3, p.qd8);
-    stage_floats_async<NT>(sQ32 + 10 * Q3, p.qdata32 + (int64_t)eB * 10 * Q3, 10 * Q3, p.qd8);
-    stage_floats_async<NT>(sJD, p.jac_data + (int64_t)eA * njd * Q3, njd * Q3, p.jd8);
-    stage_floats_async<NT>(sJD + pair_jd_stride(Q3), p.jac_data + (int64_t)eB * njd * Q3, njd * Q3, p.jd8);
-  };
   auto warm_jd = [&](int eA, int eB) {
     prefetch_l2_bulk(p.jac_data + (int64_t)eA * njd * Q3, sizeof(float) * njd * Q3);
     prefetch_l2_bulk(p.jac_data + (int64_t)eB * njd * Q3, sizeof(float) * njd * Q3);
-    if constexpr (Q32) {
-      prefetch_l2_bulk(p.qdata32 + (int64_t)eA * 10 * Q3, sizeof(float) * 10 * Q3);
-      prefetch_l2_bulk(p.qdata32 + (int64_t)eB * 10 * Q3, sizeof(float) * 10 * Q3);
-    }
   };
 
   if (threadIdx.x == 0) {
@@ -1022,16 +934,10 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
     ob.store(sO[0][1]);
     gather_lane_async<P, NT>(oa, p.dq, sN, 0);
     gather_lane_async<P, NT>(ob, p.dq, sN, 1);
-    if constexpr (Q32) {
-      stage_points32(eA, eB);
-    } else if (threadIdx.x == 0) {
+    if (threadIdx.x == 0) {
       stage_qdata(eA, eB);
       warm_jd(eA, eB);
     }
-    cp_async_commit();
-    __syncthreads();
-    gather_out_lane_async<P, NT>(sO[0][0], p.v, sV, 0);
-    gather_out_lane_async<P, NT>(sO[0][1], p.v, sV, 1);
     cp_async_commit();
   }
   unsigned phase = 0;
@@ -1044,8 +950,8 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
   }
   for (; idx < npairs; idx += G) {
     const int cA = eA, cB = eB, chasB = hasB;
-    cp_async_wait_group<1>();  // the pair's node values (and with Q32 its point data) have landed
-    if (!Q32 && threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
+    cp_async_wait_group<0>();  // the pair's node values have landed
+    if (threadIdx.x == 0 && !mbar_wait_bounded(mbar, phase)) {
       s_bail = 1;
       atomicOr(a.status, 1);
     }
@@ -1072,25 +978,14 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
 #pragma unroll
         for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
-      if constexpr (Q32) {
-        const float *jA = sJD + q, *jB = sJD + pair_jd_stride(Q3) + q;
+      const float *jA = p.jac_data + (int64_t)cA * njd * Q3 + q, *jB = p.jac_data + (int64_t)cB * njd * Q3 + q;
 #pragma unroll
-        for (int c = 0; c < 14; c++) jd[c] = f2(jA[c * Q3], jB[c * Q3]);
-        jd[14] = njd > 14 ? f2(jA[14 * Q3], jB[14 * Q3]) : f2(0.0);
-        const float *qA = sQ32 + q, *qB = sQ32 + 10 * Q3 + q;
-        wdetJ = f2(qA[0], qB[0]);
+      for (int c = 0; c < 14; c++) jd[c] = f2(__ldg(jA + c * Q3), __ldg(jB + c * Q3));
+      jd[14] = njd > 14 ? f2(__ldg(jA + 14 * Q3), __ldg(jB + 14 * Q3)) : f2(0.0);
+      const double *qA = sQD + q, *qB = sQD + 10 * Q3 + q;
+      wdetJ = f2(float(qA[0]), float(qB[0]));
 #pragma unroll
-        for (int k = 0; k < 9; k++) X[k / 3][k % 3] = f2(qA[(1 + k) * Q3], qB[(1 + k) * Q3]);
-      } else {
-        const float *jA = p.jac_data + (int64_t)cA * njd * Q3 + q, *jB = p.jac_data + (int64_t)cB * njd * Q3 + q;
-#pragma unroll
-        for (int c = 0; c < 14; c++) jd[c] = f2(__ldg(jA + c * Q3), __ldg(jB + c * Q3));
-        jd[14] = njd > 14 ? f2(__ldg(jA + 14 * Q3), __ldg(jB + 14 * Q3)) : f2(0.0);
-        const double *qA = sQD + q, *qB = sQD + 10 * Q3 + q;
-        wdetJ = f2(float(qA[0]), float(qB[0]));
-#pragma unroll
-        for (int k = 0; k < 9; k++) X[k / 3][k % 3] = f2(float(qA[(1 + k) * Q3]), float(qB[(1 + k) * Q3]));
-      }
+      for (int k = 0; k < 9; k++) X[k / 3][k % 3] = f2(float(qA[(1 + k) * Q3]), float(qB[(1 + k) * Q3]));
       ijacobian_point_stream<f2, SV>(a.pc, jd, dq, gref, wdetJ, X, v, gv);
 #pragma unroll
       for (int c = 0; c < 5; c++) {
@@ -1100,34 +995,24 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
       }
     }
     __syncthreads();
-    if (nA >= 0) {  // this pair's point data consumed: stage the next pair's
-      if constexpr (Q32) {
-        stage_points32(nA, nB);
-      } else if (threadIdx.x == 0) {
+    if (nA >= 0) {
+      if (threadIdx.x == 0) {
         fence_proxy_async_smem();
         stage_qdata(nA, nB);
       }
       cp_async_commit();
     }
     transpose_passes<P, Q, NT, f2>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
-    if (nA >= 0) cp_async_wait_group<2>();
-    else cp_async_wait_group<0>();
-    __syncthreads();
-    {  // scatter: elements of one colour share no node; each lane to its own element
+    {  // scatter: each lane to its own element's nodes, by reductions (scatter_add)
       const int32_t *oA = sO[buf][0], *oB = sO[buf][1];
       for (int t = threadIdx.x; t < 5 * P3; t += NT) {
-        const f2 r = sV[t] + s2[t];
-        p.v[oA[t]] = r.x();
-        if (chasB) p.v[oB[t]] = r.y();
+        const f2 r = s2[t];
+        atomicAdd(p.v + oA[t], r.x());
+        if (chasB) atomicAdd(p.v + oB[t], r.y());
       }
     }
     __syncthreads();
     buf ^= 1;
-    if (nA >= 0) {
-      gather_out_lane_async<P, NT>(sO[buf][0], p.v, sV, 0);
-      gather_out_lane_async<P, NT>(sO[buf][1], p.v, sV, 1);
-      cp_async_commit();
-    }
     eA = nA;
     eB = nB;
     hasB = nhasB;
@@ -1141,7 +1026,7 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
     }
   }
   cp_async_wait_all();
-  if (!Q32 && s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);
+  if (s_bail && threadIdx.x == 0) mbar_wait_bounded(mbar, phase);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -1619,36 +1504,28 @@ static int launch_ijacobian(const HbElemOp *op, const HbNewtonianContext &ctx, c
 }
 
 // The paired FP32 Jacobian (two elements of a colour per CTA pass, packed FP32): needs qdata 16-byte aligned (TMA).
-template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE, bool Q32 = false>
-static int launch_ijacobian_pair(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *qdata32, const float *jd,
-                                 const float *dq, float *v, cudaStream_t s) {
-  const size_t sm = PairPlan<P, Q, Q32>::bytes;
-  auto kern = k_ijacobian_pair<P, Q, SV, Q32>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
+template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
+static int launch_ijacobian_pair(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *jd, const float *dq, float *v,
+                                 cudaStream_t s) {
+  using L = Plan<P, Q, 1, f2, false, false>;
+  const size_t sm = L::qd_offset_bytes + 2 * sizeof(double) * 10 * L::Q3 + 16;
+  if (cudaFuncSetAttribute(k_ijacobian_pair<P, Q, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
   IjacobianPairPtrs p;
   p.dq = dq;
   p.jac_data = jd;
   p.v = v;
-  p.qdata32 = qdata32;
-  const int Q3 = Q * Q * Q, njd = HB_JAC_DATA_COMPS + (ctx.idl_enable ? 1 : 0);
-  p.jd8 = (njd * Q3) % 2 == 0 && ((uintptr_t)jd % 8) == 0;
-  p.qd8 = ((uintptr_t)qdata32 % 8) == 0;
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<f2> a = make_args<f2>(op, ctx, qdata, c);
     if (a.n_elems == 0) continue;
     const int npairs = (a.n_elems + 1) / 2;
-    kern<<<grid_for(op, npairs, kern, nthreads_for<float>(Q), sm), nthreads_for<float>(Q), sm, s>>>(a, p);
+    k_ijacobian_pair<P, Q, SV><<<grid_for(op, npairs, k_ijacobian_pair<P, Q, SV>, nthreads_for<float>(Q), sm), nthreads_for<float>(Q), sm, s>>>(a, p);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 
 template <int P, int Q, int SV>
-static int pair_case(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *qdata32, const float *jd, const float *dq,
-                     float *v, cudaStream_t s) {
-  if constexpr (Q <= 6) {
-    if (qdata32) return launch_ijacobian_pair<P, Q, SV, true>(op, ctx, qdata, qdata32, jd, dq, v, s);
-    return launch_ijacobian_pair<P, Q, SV, false>(op, ctx, qdata, nullptr, jd, dq, v, s);
-  }
+static int pair_case(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const float *jd, const float *dq, float *v, cudaStream_t s) {
+  if constexpr (Q <= 5) return launch_ijacobian_pair<P, Q, SV>(op, ctx, qdata, jd, dq, v, s);
   return launch_ijacobian<P, Q, float, SV>(op, ctx, qdata, jd, dq, v, s);
 }
 
@@ -2213,12 +2090,11 @@ extern "C" int hb_ifunction_apply_sgs(const HbElemOp *op, const void *ctx184, co
 }
 
 template <typename T, int SV>
-static int ijacobian_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v, cudaStream_t s,
-                        const float *qdata32 = nullptr) {
+static int ijacobian_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const double *qdata, const T *jd, const T *dq, T *v, cudaStream_t s) {
   if constexpr (sizeof(T) == 4 && SV == HB_STATEVAR_CONSERVATIVE) {  // FP32: element pairs in packed FP32 where the basis allows
-    if (((uintptr_t)qdata % 16) == 0 && op->Q <= 6) {
+    if (((uintptr_t)qdata % 16) == 0 && op->Q <= 5) {  // three CTAs per SM; at Q = 6 the pair kernel would run one
 #define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return pair_case<PP, QQ, SV>(op, ctx, qdata, qdata32, (const float *)jd, (const float *)dq, (float *)v, s);
+  if (op->P == PP && op->Q == QQ) return pair_case<PP, QQ, SV>(op, ctx, qdata, (const float *)jd, (const float *)dq, (float *)v, s);
       HB_PQ_LIST(HB_CASE)
 #undef HB_CASE
     }
@@ -2249,8 +2125,8 @@ extern "C" int hb_ijacobian_apply_f64(const HbElemOp *op, const void *ctx184, co
   return ijacobian_pq<double, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, dq, v, s);
 }
 
-extern "C" int hb_ijacobian_apply_f32x(const HbElemOp *op, const void *ctx184, const double *qdata, const float *qdata_f32, const float *jac_data,
-                                       const float *dq, float *v, int add, void *stream) {
+extern "C" int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, const float *dq,
+                                      float *v, int add, void *stream) {
   int err = check_op(op);
   if (err) return err;
   HbNewtonianContext ctx;
@@ -2261,12 +2137,7 @@ extern "C" int hb_ijacobian_apply_f32x(const HbElemOp *op, const void *ctx184, c
   if (!add && cudaMemsetAsync(v, 0, sizeof(float) * op->l_size, s) != cudaSuccess) return HB_ERROR_CUDA;
   if (ctx.state_var == HB_STATEVAR_PRIMITIVE) return ijacobian_pq<float, HB_STATEVAR_PRIMITIVE>(op, ctx, qdata, jac_data, dq, v, s);
   if (ctx.state_var == HB_STATEVAR_ENTROPY) return ijacobian_pq<float, HB_STATEVAR_ENTROPY>(op, ctx, qdata, jac_data, dq, v, s);
-  return ijacobian_pq<float, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, dq, v, s, qdata_f32);
-}
-
-extern "C" int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, const float *dq,
-                                      float *v, int add, void *stream) {
-  return hb_ijacobian_apply_f32x(op, ctx184, qdata, nullptr, jac_data, dq, v, add, stream);
+  return ijacobian_pq<float, HB_STATEVAR_CONSERVATIVE>(op, ctx, qdata, jac_data, dq, v, s);
 }
 
 template <typename T, int SV>

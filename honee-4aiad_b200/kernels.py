@@ -103,15 +103,10 @@ class ElemOp:
         _chk(_load().hb_ifunction_apply_sgs(self.ptr, cb, C.byref(io), C.byref(desc), w.ctypes.data_as(C.POINTER(C.c_float)), _stream(stream)),
              "hb_ifunction_apply_sgs")
 
-    def ijacobian(self, ctx_bytes: bytes, qdata, jac_data, dq, v, add=False, fp32=False, stream=None, qdata_f32=None):
-        """v (+)= J dq.  fp32: FP32 jac_data, dq and v; qdata_f32 (optional) is qdata rounded to FP32 (hb_ijacobian_apply_f32x)."""
+    def ijacobian(self, ctx_bytes: bytes, qdata, jac_data, dq, v, add=False, fp32=False, stream=None):
         cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))
-        if fp32:
-            _chk(_load().hb_ijacobian_apply_f32x(self.ptr, cb, _addr(qdata), _addr(qdata_f32), _addr(jac_data), _addr(dq), _addr(v), int(add),
-                                                 _stream(stream)), "hb_ijacobian_apply_f32x")
-            return
-        _chk(_load().hb_ijacobian_apply_f64(self.ptr, cb, _addr(qdata), _addr(jac_data), _addr(dq), _addr(v), int(add), _stream(stream)),
-             "hb_ijacobian_apply_f64")
+        fn = _load().hb_ijacobian_apply_f32 if fp32 else _load().hb_ijacobian_apply_f64
+        _chk(fn(self.ptr, cb, _addr(qdata), _addr(jac_data), _addr(dq), _addr(v), int(add), _stream(stream)), "hb_ijacobian_apply")
 
     def diagonal(self, ctx_bytes: bytes, qdata, jac_data, diag, add=False, fp32=False, stream=None):
         cb = C.create_string_buffer(bytes(ctx_bytes), len(ctx_bytes))

@@ -95,11 +95,6 @@ HB_EXPORT int hb_ijacobian_apply_f64(const HbElemOp *op, const void *ctx184, con
                            int add, void *stream);
 HB_EXPORT int hb_ijacobian_apply_f32(const HbElemOp *op, const void *ctx184, const double *qdata, const float *jac_data, const float *dq, float *v,
                            int add, void *stream);
-/* The FP32 action with qdata also given rounded to FP32 (qdata_f32 [E][10][Q^3], e.g. from hb_vec_f64_to_f32; NULL: as
- * hb_ijacobian_apply_f32).  The FP32 action rounds qdata to FP32 at every point anyway, so the results are bit-identical;
- * the conservative-variable kernel then moves half the qdata bytes and stages all its point data in shared memory. */
-HB_EXPORT int hb_ijacobian_apply_f32x(const HbElemOp *op, const void *ctx184, const double *qdata, const float *qdata_f32, const float *jac_data,
-                                      const float *dq, float *v, int add, void *stream);
 
 /* Point-wise diagonal of the IJacobian operator, where MatGetDiagonal_Ceed calls CeedOperatorLinearAssembleDiagonal
  * (src/mat-ceed.c:1603-1630). */
@@ -177,9 +172,7 @@ typedef struct {
 typedef struct HbTimeStepper HbTimeStepper;
 
 HB_EXPORT void hb_solver_default_options(HbSolverOptions *o);
-/* ctx184 is copied; its dt / ijacobian_time_shift / time fields are set every step like HONEE's context labels.  d_qdata
- * is read at every residual; with jacobian_fp32 the stepper also keeps an FP32 copy made here for the Jacobian action, so
- * qdata must not change during the stepper's life (the mesh does not move). */
+/* ctx184 is copied; its dt / ijacobian_time_shift / time fields are set every step like HONEE's context labels. */
 HB_EXPORT int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, const HbSolverOptions *opts, void *stream,
                            HbTimeStepper **ts);
 HB_EXPORT int hb_ts_set_state(HbTimeStepper *ts, const double *d_q, double t);

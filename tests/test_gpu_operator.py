@@ -278,25 +278,3 @@ def test_operator_over_zero_elements_contributes_nothing():
     np.testing.assert_array_equal(jv.to_numpy(), j_ref)
     np.testing.assert_array_equal(d.to_numpy(), d_ref)
 
-
-@pytest.mark.parametrize("name", ["cfg1_P3Q3", "cfg2_P4Q5", "cfg3_P5Q6_periodic", "idl_P3Q3", "single_elem_P4Q5"])
-def test_fp32_jacobian_reading_fp32_qdata_is_bit_identical(name):
-    """hb_ijacobian_apply_f32x with qdata rounded to FP32 (the element-pair kernel staging both elements' qdata and Jacobian
-    data by cp.async, 8-byte chunks, or 4-byte ones for the 15 IDL components at odd Q^3) equals the FP32 action that
-    rounds FP64 qdata at every point, bit for bit; odd element counts leave a pair with one element."""
-    import torch
-    kern = importlib.import_module("honee-4aiad_b200.kernels")
-    mesh, basis, ctx, q, qd, ceed, ops, qv, g = _setup(name)
-    ops.ifunction(qv, ops.q_dot, g)
-    dev = torch.device("cuda:0")
-    op = kern.ElemOp(mesh, basis)
-    cb = prob.context_bytes(ctx)
-    qdata = torch.from_numpy(ops.q_data.to_numpy()).to(dev)
-    jd = torch.from_numpy(ops.jac_data.to_numpy()).to(dev).float()
-    dq = torch.from_numpy(np.random.default_rng(6).normal(size=q.shape) * np.abs(q) * 1e-4).to(dev).float()
-    v1, v2 = torch.zeros_like(dq), torch.zeros_like(dq)
-    op.ijacobian(cb, qdata, jd, dq, v1, fp32=True)
-    op.ijacobian(cb, qdata, jd, dq, v2, fp32=True, qdata_f32=qdata.float())
-    torch.cuda.synchronize()
-    assert torch.equal(v1, v2)
-    assert v1.abs().max().item() > 0
