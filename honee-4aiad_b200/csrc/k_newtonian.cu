@@ -8,7 +8,9 @@
 //   -> point-wise IFunction / IJacobian / linearised diagonal (newtonian_qf.cuh), one thread per quadrature point, with
 //      qdata read and jac_data written coalesced in the [elem][comp][qpt] layout
 //   -> transpose gradient + interpolation back to the element nodes
-//   -> scatter-add into the L-vector without atomics: elements of one colour share no node, colours run in stream order.
+//   -> scatter-add into the L-vector through element colouring: elements of one colour share no node and colours run in
+//      stream order, so every entry receives one uncontended addition per launch (issued as a reduction without return,
+//      performed in L2; deterministic, the same sum as a load-add-store).
 // Reference semantics: libCEED CeedOperatorApply / CeedOperatorLinearAssembleDiagonal as called from src/setupts.c:109,
 // src/mat-ceed.c:1618,1669 on the operators built in src/setuplibceed.c:209-269.
 #include <cuda_runtime.h>
@@ -435,7 +437,7 @@ __device__ __forceinline__ void scatter_add(const int32_t *sO, const T *sF, T *l
 //   sG  [15][Q3]        reference gradients; point-wise fluxes in place; later sT1
 //   sJD [15][Q3]        staged stored Jacobian data (IJacobian only)
 //   sQD [10][Q3] double staged qdata (the residual keeps two: element i and element i + 1)
-template <int P, int Q, int NV, typename T, bool JD, bool ST = true>
+template <int P, int Q, int NV, typename T, bool JD, bool ST = true, int NQB = (NV == 2 ? 2 : 1)>
 struct Plan {
   static constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
   static constexpr int cmax(int x, int y) { return x > y ? x : y; }
@@ -448,8 +450,9 @@ struct Plan {
   static constexpr int oN = 0, o1 = pad(oN + nN), o2 = pad(o1 + n1), oU = pad(o2 + n2), oG = pad(oU + nU),
                        oJD = pad(oG + nG), end_T = pad(oJD + nJD);
   static constexpr size_t qd_offset_bytes = ((size_t)end_T * sizeof(T) + 15) & ~(size_t)15;
-  // staged qdata precedes the mbarriers: two buffers for the residual (NV == 2), one for the Jacobian
-  static constexpr size_t mbar_offset = qd_offset_bytes + (ST ? (NV == 2 ? 2 : 1) * sizeof(double) * 10 * Q3 : 0);
+  // staged qdata precedes the mbarriers: NQB buffers (the residual double-buffers where the occupancy allows, the
+  // Jacobian uses one)
+  static constexpr size_t mbar_offset = qd_offset_bytes + (ST ? NQB * sizeof(double) * 10 * Q3 : 0);
   static constexpr size_t bytes = mbar_offset + 16;
   static_assert(5 * P * Q2 <= n1, "sT2 fits in s1");
   static_assert(5 * Q3 <= n2, "w2 fits in s2");
@@ -531,6 +534,14 @@ __device__ __forceinline__ void sgs_add(const PhysConst<double> &c, const double
 // ---------------------------------------------------------------------------------------------------------------------
 // IFunction
 
+// qdata buffers of the residual kernel: two (the element after next is staged while this one computes) where both fit at
+// the kernel's resident CTAs per SM, else one (e.g. P = 5, Q = 6: 111 KB with two buffers would leave one CTA per SM)
+template <int P, int Q, bool ST>
+__host__ __device__ constexpr int ifunction_qdata_buffers() {
+  constexpr size_t static_bytes = sizeof(int32_t) * 2 * 5 * P * P * P + sizeof(double) * kMaxP + 16, reserved = 1024, per_sm = 233472;
+  return (size_t)min_blocks_for(Q, ST) * (Plan<P, Q, 2, double, false, ST, 2>::bytes + static_bytes + reserved) <= per_sm ? 2 : 1;
+}
+
 struct IfunctionPtrs {
   const double *q, *q_dot;
   double *jac_data;   // [E][num_jd][Q3], may be null
@@ -544,7 +555,8 @@ template <int P, int Q, bool ST, int SGS = 0, int SV = HB_STATEVAR_CONSERVATIVE>
 __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p,
                                                                                                const SgsArg<SGS> sg) {
   constexpr int NT = nthreads_for<double>(Q);
-  using L = Plan<P, Q, 2, double, false, ST>;
+  constexpr int NB = ifunction_qdata_buffers<P, Q, ST>();  // qdata buffers: element k uses buffer and mbarrier k % NB
+  using L = Plan<P, Q, 2, double, false, ST, NB>;
   constexpr int Q3 = L::Q3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sm = reinterpret_cast<double *>(smem_raw);
@@ -577,17 +589,17 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     eo.load(a.offsets, e0);
     eo.store(sO[0]);
     gather_async<P, 2, NT, double>(eo, p.q, p.q_dot, sN);
-    if constexpr (ST) {  // qdata of the first two elements, one buffer each
+    if constexpr (ST) {  // qdata of the first NB elements, one buffer each
       if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
       stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
-      if (idx + (int)gridDim.x < a.n_elems) {
+      if (NB == 2 && idx + (int)gridDim.x < a.n_elems) {
         if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar + 1, p.qdata_tma ? qd_bytes : 0);
         stage_block<double, NT>(sQD + 10 * Q3, a.qdata + (int64_t)a.elems[idx + gridDim.x] * 10 * Q3, 10 * Q3, p.qdata_tma, mbar + 1);
       }
     } else if (threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)e0 * 10 * Q3, qd_bytes);
     cp_async_commit();
   }
-  unsigned kit = 0;  // elements done by this CTA: qdata buffer kit & 1, its mbarrier phase parity (kit >> 1) & 1
+  unsigned kit = 0;  // elements done by this CTA: qdata buffer kit % NB, its mbarrier's phase parity (kit / NB) & 1
   // element ids and entry offsets are read two elements ahead so no global load latency sits on the critical path
   const int G = gridDim.x;
   int ecur = a.elems[idx];
@@ -604,7 +616,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     HB_PT(7)
     cp_async_wait_group<0>();  // this element's node values have landed
     HB_PT(8)
-    if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar + (kit & 1), (kit >> 1) & 1)) {
+    if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar + kit % NB, (kit / NB) & 1)) {
       s_bail = 1;
       atomicOr(a.status, 1);
     }
@@ -633,7 +645,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
 #pragma unroll
         for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
-      const double *qdp = ST ? sQD + (kit & 1) * 10 * Q3 : a.qdata + (int64_t)e * 10 * Q3;
+      const double *qdp = ST ? sQD + (kit % NB) * 10 * Q3 : a.qdata + (int64_t)e * 10 * Q3;
       wdetJ = qdp[q];
 #pragma unroll
       for (int k = 0; k < 9; k++) X[k / 3][k % 3] = qdp[(1 + k) * Q3 + q];
@@ -671,14 +683,15 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
         }
       }
     }
-    if (en >= 0) {  // this qdata buffer consumed: stage the qdata of the element after next into it
+    if (en >= 0) {  // this qdata buffer consumed: stage the qdata of the element NB ahead into it
       if constexpr (ST) {
-        if (en2 >= 0) {
+        const int ea = NB == 2 ? en2 : en;
+        if (ea >= 0) {
           if (threadIdx.x == 0) {
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(mbar + (kit & 1), p.qdata_tma ? qd_bytes : 0);
+            mbar_arrive_expect_tx(mbar + kit % NB, p.qdata_tma ? qd_bytes : 0);
           }
-          stage_block<double, NT>(sQD + (kit & 1) * 10 * Q3, a.qdata + (int64_t)en2 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar + (kit & 1));
+          stage_block<double, NT>(sQD + (kit % NB) * 10 * Q3, a.qdata + (int64_t)ea * 10 * Q3, 10 * Q3, p.qdata_tma, mbar + kit % NB);
         }
       }
       cp_async_commit();
@@ -701,8 +714,8 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
   HB_PT_FLUSH(0)
   cp_async_wait_all();
   if (ST && s_bail && threadIdx.x == 0) {  // let outstanding bulk copies land before exit (bounded waits)
-    mbar_wait_bounded(mbar + (kit & 1), (kit >> 1) & 1);
-    mbar_wait_bounded(mbar + ((kit + 1) & 1), ((kit + 1) >> 1) & 1);
+    mbar_wait_bounded(mbar + kit % NB, (kit / NB) & 1);
+    if (NB == 2) mbar_wait_bounded(mbar + (kit + 1) % NB, ((kit + 1) / NB) & 1);
   }
 }
 
@@ -1451,7 +1464,7 @@ static size_t smem_bytes(int P, int Q) {
 template <int P, int Q, bool ST, int SGS = 0, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s,
                               const SgsArg<SGS> &sg = SgsArg<SGS>{}) {
-  using L = Plan<P, Q, 2, double, false, ST>;
+  using L = Plan<P, Q, 2, double, false, ST, ifunction_qdata_buffers<P, Q, ST>()>;
   const size_t sm = L::bytes;
   cudaFuncSetAttribute(k_ifunction<P, Q, ST, SGS, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   IfunctionPtrs p;
