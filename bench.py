@@ -267,27 +267,45 @@ def run_gpu(args, rank, world):
     gpu_out = {"v": t_v.cpu().numpy(), "jac_data": t_jd.cpu().numpy(), "jv": jv64.cpu().numpy(), "jv32": t_jv32.double().cpu().numpy()}
     del jv64, t_jd32, t_dq32, t_jv32
 
-    # e2e through the libCEED API with host (pinned) buffers: H2D of q, q_dot, dq and D2H of both results every step
+    # e2e through the libCEED API with host (pinned) buffers: H2D of q, q_dot, dq and D2H of both results every step.
+    # Two steps in flight: the results of step k are read back (CeedVectorSyncArray) after step k+1 is enqueued, into a
+    # second pair of output vectors, so step k's read-back (device->host) shares the bus with step k+1's upload
+    # (host->device); the serial variant reads each step back before enqueuing the next.
     ceed = ce.Ceed("/gpu/b200")
     ops = hon.NewtonianOperators(ceed, mesh, basis, ctx)
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
     h_q, h_qd, h_dq = pin(q), pin(q_dot), pin(dq)
-    h_g, h_j = pin(np.zeros(N_L)), pin(np.zeros(N_L))
-    qv, dv, gv, jvv = (ce.Vector(ceed, N_L) for _ in range(4))
+    h_g, h_j = [pin(np.zeros(N_L)) for _ in range(2)], [pin(np.zeros(N_L)) for _ in range(2)]
+    qv, dv = ce.Vector(ceed, N_L), ce.Vector(ceed, N_L)
+    gv, jvv = [ce.Vector(ceed, N_L) for _ in range(2)], [ce.Vector(ceed, N_L) for _ in range(2)]
 
-    def e2e_step():
+    def e2e_enqueue(s):
         qv.set_array_host(h_q, copy=False)
         ops.q_dot.set_array_host(h_qd, copy=False)
         dv.set_array_host(h_dq, copy=False)
-        gv.set_array_host(h_g, copy=False)
-        jvv.set_array_host(h_j, copy=False)
-        ops.op_ifunction.apply(qv, gv)
-        ops.op_ijacobian.apply(dv, jvv)
-        ce.L().CeedVectorSyncArray(gv.ptr, ce.CEED_MEM_HOST)
-        ce.L().CeedVectorSyncArray(jvv.ptr, ce.CEED_MEM_HOST)
+        gv[s].set_array_host(h_g[s], copy=False)
+        jvv[s].set_array_host(h_j[s], copy=False)
+        ops.op_ifunction.apply(qv, gv[s])
+        ops.op_ijacobian.apply(dv, jvv[s])
 
-    ms_e2e = timed(e2e_step, max(1, min(args.steps, 5)))
-    err_e2e = float(np.linalg.norm(h_j - gpu_out["jv"]) / np.linalg.norm(gpu_out["jv"]))
+    def e2e_read(s):
+        ce.L().CeedVectorSyncArray(gv[s].ptr, ce.CEED_MEM_HOST)
+        ce.L().CeedVectorSyncArray(jvv[s].ptr, ce.CEED_MEM_HOST)
+
+    def e2e_steps(k, in_flight):
+        for i in range(k):
+            e2e_enqueue(i % 2)
+            if in_flight == 1:
+                e2e_read(i % 2)
+            elif i:
+                e2e_read((i - 1) % 2)
+        if in_flight == 2:
+            e2e_read((k - 1) % 2)
+
+    k_e2e = max(2, min(args.steps, 10))
+    ms_e2e_serial = timed(lambda: e2e_steps(1, 1), k_e2e)
+    ms_e2e = timed(lambda: e2e_steps(k_e2e, 2), 1) / k_e2e
+    err_e2e = max(float(np.linalg.norm(h_j[s] - gpu_out["jv"]) / np.linalg.norm(gpu_out["jv"])) for s in range(2))
 
     # parity against the CPU oracle: the benchmarked outputs themselves (full size), and a small case of the same operator
     acc, cpu_full = parity_full(prob, mesh, basis, ctx, q, q_dot, dq, gpu_out, args.size) if rank == 0 and not args.no_cpu else ({}, None)
@@ -327,7 +345,8 @@ def run_gpu(args, rank, world):
                                     "source": "hb_fma_peak_probe (independent FMA chains, 8 CTAs/SM), best of 5 launches, CUDA events, this run"},
                      "two_sided": sides},
         "e2e": {"value": job_gdofs(world, N_L, ms_e2e), "unit": "GDoF/s", "h2d_bytes_per_step": 3 * 8 * N_L, "d2h_bytes_per_step": 2 * 8 * N_L,
-                "api": "CeedVectorSetArray(HOST, USE_POINTER) + CeedOperatorApply x2 + CeedVectorSyncArray(HOST)", "jacobian_rel_l2_vs_kernel": err_e2e},
+                "api": "CeedVectorSetArray(HOST, USE_POINTER) + CeedOperatorApply x2 + CeedVectorSyncArray(HOST)", "steps_in_flight": 2,
+                "steps": k_e2e, "serial_value": job_gdofs(world, N_L, ms_e2e_serial), "jacobian_rel_l2_vs_kernel": err_e2e},
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -540,6 +559,33 @@ def parity_sample(prob, kern, torch, dev):
             "ijacobian_f32_rel_l2": r(tj32.double().cpu().numpy(), j_ref)}
 
 
+def run_contraction_ab(args):
+    """A/B of the basis-contraction mechanism on one GPU (hb_contraction_probe): 32 rounds of the in-plane collocated
+    derivatives of five FP64 components at Q = 5 on 65,536 elements (328 MB in, 328 MB out), by shared-memory fibre passes
+    (the operator kernels' mechanism) and by warp shuffles, each at its own occupancy limit and at the operator kernels'
+    three CTAs per SM; best of 5 CUDA-event-timed launches.  Prints one JSON line; no part of the benchmark step."""
+    import torch
+    kern = importlib.import_module("honee-4aiad_b200.kernels")
+    prob = importlib.import_module("honee-4aiad_b200.problem")
+    qx, _ = prob.gauss_legendre(5)
+    _, D = prob.lagrange_tabulate(qx, qx)
+    D = D / np.abs(D).sum(1).max()
+    E, reps = 65536, 32
+    u = torch.from_numpy(np.random.default_rng(0).normal(size=(E, 5, 125))).cuda()
+    fma64 = kern.fma_peak(True)
+    res, outs = {}, {}
+    for variant, name in ((0, "shared_fibre_passes"), (1, "warp_shuffles")):
+        for ctas in (0, 3):
+            ms, fmas, out = kern.contraction_probe(variant, D, u, reps, ctas_per_sm=ctas)
+            res[f"{name}_{'max_occupancy' if ctas == 0 else '3_ctas_per_sm'}"] = {
+                "ms": ms, "ns_per_element_round": ms * 1e6 / (E * reps), "fp64_pipe_fraction": fmas / (ms * 1e-3) / fma64}
+            outs[(variant, ctas)] = out
+        del out
+    same = all(torch.equal(o, outs[(0, 0)]) for o in outs.values())
+    print(json.dumps({"contraction_ab": "in-plane collocated derivatives, 5 FP64 components, Q=5", "elements": E, "rounds": reps,
+                      "fma_per_element_round": 6250, "fp64_fma_peak_per_s": fma64, "bit_identical": same, "variants": res}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -552,6 +598,8 @@ def main():
     ap.add_argument("--profile-apply", action="store_true",
                     help="run two applies of every operator kernel (IFunction, IJacobian FP64/FP32, diagonal FP64/FP32) and exit: "
                          "the launches an ncu capture selects with -k/-s/-c")
+    ap.add_argument("--contraction-ab", action="store_true",
+                    help="time the basis-contraction A/B probe (shared-memory fibre passes against warp shuffles) and exit")
     ap.add_argument("--no-timeloop", action="store_true", help="skip the implicit time-loop leg")
     ap.add_argument("--timeloop-steps", type=int, default=5)
     args = ap.parse_args()
@@ -566,6 +614,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank)
+        elif args.contraction_ab:
+            run_contraction_ab(args)
         elif world > 1:
             run_gpu_partitioned(args, rank, world)
         else:

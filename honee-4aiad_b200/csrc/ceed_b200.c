@@ -50,6 +50,7 @@ struct Ceed_private {
   cudaStream_t     s_h2d, s_d2h;
   cudaEvent_t      ev_tmp;
   int              copy_streams;
+  int             *h_status; /* pinned: the status words read back beside an output read-back on s_d2h */
 };
 
 struct CeedVector_private {
@@ -324,6 +325,7 @@ int CeedDestroy(Ceed *ceed) {
     cudaStreamDestroy((*ceed)->s_h2d);
     cudaStreamDestroy((*ceed)->s_d2h);
     cudaEventDestroy((*ceed)->ev_tmp);
+    cudaFreeHost((*ceed)->h_status);
   }
   free(*ceed);
   *ceed = NULL;
@@ -341,7 +343,7 @@ int CeedGetPreferredMemType(Ceed ceed, CeedMemType *type) {
 }
 int CeedIsDeterministic(Ceed ceed, bool *is_deterministic) {
   (void)ceed;
-  *is_deterministic = true; /* coloured scatters, no atomics */
+  *is_deterministic = true; /* coloured scatters: one addition per output entry and launch, colours in stream order */
   return CEED_ERROR_SUCCESS;
 }
 int CeedSetStream(Ceed ceed, void *handle) {
@@ -397,6 +399,7 @@ static int vec_unstale(CeedVector v) {
   if (!v->f64_stale) return CEED_ERROR_SUCCESS;
   CK(vec_alloc_dev(v));
   HB_CK(v->ceed, hb_vec_f32_to_f64(v->d_f32, v->d, v->length, 0, v->ceed->stream));
+  v->use_known = 0; /* d written on the compute stream after the last operator's ev_use */
   v->f64_stale = 0;
   v->d_valid   = 1;
   v->h_valid   = 0;
@@ -407,6 +410,7 @@ static int ceed_copy_streams(Ceed c) {
   CUDA_CK(c, cudaStreamCreateWithFlags(&c->s_h2d, cudaStreamNonBlocking));
   CUDA_CK(c, cudaStreamCreateWithFlags(&c->s_d2h, cudaStreamNonBlocking));
   CUDA_CK(c, cudaEventCreateWithFlags(&c->ev_tmp, cudaEventDisableTiming));
+  CUDA_CK(c, cudaMallocHost((void **)&c->h_status, sizeof(int) * 64));
   c->copy_streams = 1;
   return CEED_ERROR_SUCCESS;
 }
@@ -450,17 +454,31 @@ static int vec_sync_dev(CeedVector v) {
   }
   return CEED_ERROR_SUCCESS;
 }
+static int ceed_status_error(Ceed ceed, int i, int st) {
+  cudaMemset(ceed->ops[i]->d_status, 0, sizeof(int));
+  return CeedError(ceed, CEED_ERROR_BACKEND, "a fused kernel abandoned a bounded wait (status %d); its output is incomplete", st);
+}
 /* Kernels never trap: a bounded wait that gives up sets a status word.  Surface it at the next host synchronisation. */
 static int ceed_check_status(Ceed ceed) {
   for (int i = 0; i < ceed->nops; i++) {
     int st = 0;
     if (cudaMemcpy(&st, ceed->ops[i]->d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
       return CeedError(ceed, CEED_ERROR_BACKEND, "could not read the kernel status word");
-    if (st) {
-      cudaMemset(ceed->ops[i]->d_status, 0, sizeof(int));
-      return CeedError(ceed, CEED_ERROR_BACKEND, "a fused kernel abandoned a bounded wait (status %d); its output is incomplete", st);
-    }
+    if (st) return ceed_status_error(ceed, i, st);
   }
+  return CEED_ERROR_SUCCESS;
+}
+/* The same check beside a read-back on the copy stream s_d2h, after the producer's ev_use: the words are read in that
+ * stream's order, so the check covers the producer and does not wait for kernels enqueued after it (a blocking
+ * cudaMemcpy would, on the legacy default stream, and so serialise a pipelined host loop).  A word that a later kernel
+ * is still writing reads as 0 or as its error; the error is then reported here or at a later synchronisation. */
+static int ceed_check_status_d2h(Ceed ceed) {
+  const int n = ceed->nops;
+  for (int i = 0; i < n; i++)
+    CUDA_CK(ceed, cudaMemcpyAsync(ceed->h_status + i, ceed->ops[i]->d_status, sizeof(int), cudaMemcpyDeviceToHost, ceed->s_d2h));
+  CUDA_CK(ceed, cudaStreamSynchronize(ceed->s_d2h));
+  for (int i = 0; i < n; i++)
+    if (ceed->h_status[i]) return ceed_status_error(ceed, i, ceed->h_status[i]);
   return CEED_ERROR_SUCCESS;
 }
 static void ceed_register_op(Ceed ceed, HbElemOp *op) {
@@ -487,13 +505,14 @@ static int vec_sync_host(CeedVector v) {
       CK(ceed_copy_streams(c));
       CUDA_CK(c, cudaStreamWaitEvent(c->s_d2h, v->ev_use, 0));
       CUDA_CK(c, cudaMemcpyAsync(v->h, v->d, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToHost, c->s_d2h));
-      CUDA_CK(c, cudaStreamSynchronize(c->s_d2h));
+      v->h_valid = 1;
+      CK(ceed_check_status_d2h(c));
     } else {
       CUDA_CK(c, cudaMemcpyAsync(v->h, v->d, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToHost, c->stream));
       CUDA_CK(c, cudaStreamSynchronize(c->stream));
+      v->h_valid = 1;
+      CK(ceed_check_status(v->ceed));
     }
-    v->h_valid = 1;
-    CK(ceed_check_status(v->ceed));
   }
   return CEED_ERROR_SUCCESS;
 }
@@ -518,14 +537,15 @@ static int vec_dev_write(CeedVector v, double **d, int write_only) {
   return CEED_ERROR_SUCCESS;
 }
 
-/* Any call that hands the device array out (GetArray*, TakeArray) or replaces or writes it outside an operator (SetArray,
- * including a device-to-device copy on the compute stream) clears use_known: ev_use then no longer covers every use of
- * d, so the next copy between host and device follows the whole compute stream instead of the last operator's event. */
+/* Any call that hands the device array out (GetArray*, TakeArray) or replaces or writes it outside an operator (SetArray
+ * on the device, including a device-to-device copy on the compute stream) clears use_known: ev_use then no longer covers
+ * every use of d, so the next copy between host and device follows the whole compute stream instead of the last
+ * operator's event.  SetArray on the host leaves d untouched, so ev_use still covers it: the upload of the new host array
+ * waits only for the last operator that used the vector, and overlaps the kernels enqueued after that one. */
 int CeedVectorSetArray(CeedVector v, CeedMemType mem_type, CeedCopyMode copy_mode, CeedScalar *array) {
   CK(vec_wait_h2d(v));
   v->f64_stale = 0;
   v->f32_valid = 0;
-  v->use_known = 0;
   if (mem_type == CEED_MEM_HOST) {
     if (copy_mode == CEED_COPY_VALUES) {
       CK(vec_alloc_host(v));
@@ -538,6 +558,7 @@ int CeedVectorSetArray(CeedVector v, CeedMemType mem_type, CeedCopyMode copy_mod
     v->h_valid = array != NULL;
     v->d_valid = 0;
   } else {
+    v->use_known = 0;
     if (copy_mode == CEED_COPY_VALUES) {
       CK(vec_alloc_dev(v));
       if (array) CUDA_CK(v->ceed, cudaMemcpyAsync(v->d, array, sizeof(double) * (size_t)v->length, cudaMemcpyDeviceToDevice, v->ceed->stream));

@@ -192,6 +192,33 @@ class FaceOp:
                                                   _stream(stream)), "hb_freestream_jacobian_apply")
 
 
+def contraction_probe(variant, D, u, reps, ctas_per_sm=0, launches=5):
+    """Run the library's contraction A/B probe (hb_contraction_probe) on u, a CUDA float64 tensor [E][5][125]: returns
+    (best CUDA-event milliseconds of `launches` timed launches after one warm-up, FMA count per launch, output tensor).
+    variant 0 = shared-memory fibre passes, 1 = warp shuffles."""
+    import torch
+    assert u.is_cuda and u.dtype == torch.float64 and u.is_contiguous() and u.numel() % 625 == 0
+    E = u.numel() // 625
+    out = torch.empty_like(u)
+    Dh = np.ascontiguousarray(np.asarray(D, dtype=np.float64).reshape(5, 5))
+    s = torch.cuda.current_stream(u.device)
+    cnt = C.c_int64()
+    fn = _load().hb_contraction_probe
+    args = lambda: (int(variant), Dh.ctypes.data_as(C.POINTER(C.c_double)), C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr()),  # noqa: E731
+                    int(E), int(reps), int(ctas_per_sm), C.byref(cnt), _stream(s))
+    _chk(fn(*args()), "hb_contraction_probe")
+    best = None
+    for _ in range(launches):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        _chk(fn(*args()), "hb_contraction_probe")
+        b.record(s)
+        b.synchronize()
+        t = a.elapsed_time(b)
+        best = t if best is None else min(best, t)
+    return best, cnt.value, out
+
+
 def fma_peak(fp64=True, iters=4096, reps=5, device=None):
     """Measured FMA throughput of the FP64 (or FP32) pipe in FMA/s: the best of `reps` launches of the library's probe
     (independent FMA chains over 8 CTAs per SM), timed with CUDA events on torch's current stream after one warm-up."""

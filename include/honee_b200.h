@@ -524,6 +524,15 @@ HB_EXPORT int hb_ics_apply(int kind, int state_var, const void *ctx, size_t ctx_
  * impossible value); *fma_per_launch receives the FMA count, to be divided by the caller's event time on `stream`. */
 HB_EXPORT int hb_fma_peak_probe(int fp64, int iters, void *d_sink, int64_t sink_elems, int64_t *fma_per_launch, void *stream);
 
+/* Basis-contraction mechanism A/B probe (no reference counterpart): `reps` rounds of u <- D_x u + D_y u, the in-plane
+ * collocated derivatives of five FP64 components at the Q = 5 points of each element (d_u, d_out: [num_elem][5][125],
+ * x fastest; D: host 5 x 5 row-major), by shared-memory fibre passes (variant 0, the operator kernels' mechanism, 128
+ * threads per element) or warp shuffles (variant 1, one z-plane per warp, 160 threads per element).  Results are
+ * bit-identical between the variants.  ctas_per_sm = 0: each variant at its own occupancy limit.  *fma_per_launch
+ * receives the FMA count (num_elem x reps x 6250). */
+HB_EXPORT int hb_contraction_probe(int variant, const double *D, const double *d_u, double *d_out, int num_elem, int reps, int ctas_per_sm,
+                                   int64_t *fma_per_launch, void *stream);
+
 /* Library identification */
 const char *hb_version(void);
 

@@ -85,6 +85,9 @@ def test_mixed_precision_jacobian(name):
     v_ref, jd_ref, qdata_ref, m = oracle_ifunction(mesh, basis, ctx, q, qd)
     ops.ifunction(qv, ops.q_dot, g)
     assert rel_l2(g.to_numpy(), v_ref) < TOL64  # the residual stays FP64
+    # the stored Jacobian data is written in FP32 only; reading it on the host widens it on the compute stream first, and
+    # the read-back must wait for that conversion, not only for the operator that wrote the FP32 copy
+    assert rel_l2(ops.jac_data.to_numpy(), jd_ref) < 1e-7
     cb = prob.context_bytes(ctx)
     dq = np.random.default_rng(4).normal(size=q.shape) * np.abs(q) * 1e-4
     dv = ce.Vector(ceed, mesh.l_size)
@@ -232,6 +235,60 @@ def test_host_backed_vectors_across_steps_match_the_device_path():
     g.set_array_device(src.data_ptr(), copy=True)
     ce.L().CeedVectorSyncArray(g.ptr, ce.CEED_MEM_HOST)
     np.testing.assert_array_equal(h_g, src.cpu().numpy())
+
+
+def test_host_backed_vectors_with_two_steps_in_flight():
+    """Two steps in flight through the libCEED API, as a pipelined host loop runs them: step k+1's host inputs are handed
+    over (CEED_USE_POINTER) and its operators enqueued before step k's outputs are read back, into a second pair of output
+    vectors.  The input vectors are shared by both steps, so step k+1's upload may start only after step k's operator has
+    read the device array (its last-use event), and each step's inputs differ: any overlap of the two would change step k's
+    results.  Every step equals the kernel ABI on device buffers, bit for bit."""
+    import torch
+    kern = importlib.import_module("honee-4aiad_b200.kernels")
+    mesh, basis, ctx, q, qd, ceed, ops, qv, _ = _setup("cfg2_P4Q5")
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    rng = np.random.default_rng(6)
+    K = 5
+    h_q = [pin(q * (1 + 1e-3 * rng.uniform(-1, 1, q.shape))) for _ in range(K)]
+    h_qd = [pin(qd * (1 + 0.1 * rng.uniform(-1, 1, q.shape))) for _ in range(K)]
+    h_dq = [pin(q * 1e-4 * rng.normal(size=q.shape)) for _ in range(K)]
+    h_g, h_j = [pin(q * 0) for _ in range(2)], [pin(q * 0) for _ in range(2)]
+    dv = ce.Vector(ceed, mesh.l_size)
+    gv, jv = [ce.Vector(ceed, mesh.l_size) for _ in range(2)], [ce.Vector(ceed, mesh.l_size) for _ in range(2)]
+    op = kern.ElemOp(mesh, basis)
+    dev = torch.device("cuda:0")
+    tqdata = torch.from_numpy(ops.q_data.to_numpy()).to(dev)
+    cb = prob.context_bytes(ctx)
+
+    def expected(k):
+        tq, tqd, tdq = (torch.from_numpy(a[k].copy()).to(dev) for a in (h_q, h_qd, h_dq))
+        tv, tj = torch.zeros_like(tq), torch.zeros_like(tq)
+        tjd = torch.zeros(mesh.num_elem * 14 * basis.Q ** 3, dtype=torch.float64, device=dev)
+        op.ifunction(cb, tq, tqd, tqdata, tv, jac_data=tjd)
+        op.ijacobian(cb, tqdata, tjd, tdq, tj)
+        torch.cuda.synchronize()
+        return tv.cpu().numpy(), tj.cpu().numpy()
+
+    def read_and_check(k):
+        s = k % 2
+        ce.L().CeedVectorSyncArray(gv[s].ptr, ce.CEED_MEM_HOST)
+        ce.L().CeedVectorSyncArray(jv[s].ptr, ce.CEED_MEM_HOST)
+        v_exp, j_exp = expected(k)
+        np.testing.assert_array_equal(h_g[s], v_exp, err_msg=f"residual of step {k}")
+        np.testing.assert_array_equal(h_j[s], j_exp, err_msg=f"Jacobian action of step {k}")
+
+    for k in range(K):
+        s = k % 2
+        qv.set_array_host(h_q[k], copy=False)
+        ops.q_dot.set_array_host(h_qd[k], copy=False)
+        dv.set_array_host(h_dq[k], copy=False)
+        gv[s].set_array_host(h_g[s], copy=False)
+        jv[s].set_array_host(h_j[s], copy=False)
+        ops.op_ifunction.apply(qv, gv[s])
+        ops.op_ijacobian.apply(dv, jv[s])
+        if k:
+            read_and_check(k - 1)
+    read_and_check(K - 1)
 
 
 def test_operator_over_zero_elements_contributes_nothing():
