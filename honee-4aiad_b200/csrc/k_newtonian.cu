@@ -436,8 +436,8 @@ __device__ __forceinline__ void scatter_add(const int32_t *sO, const T *sF, T *l
 //   sU  [10][Q3]        interpolated values (q, then q_dot or w1); point-wise outputs v in place
 //   sG  [15][Q3]        reference gradients; point-wise fluxes in place; later sT1
 //   sJD [15][Q3]        staged stored Jacobian data (IJacobian only)
-//   sQD [10][Q3] double staged qdata (the residual keeps two: element i and element i + 1)
-template <int P, int Q, int NV, typename T, bool JD, bool ST = true, int NQB = (NV == 2 ? 2 : 1)>
+//   sQD [10][Q3] double staged qdata (IJacobian only; the residual reads qdata at the point)
+template <int P, int Q, int NV, typename T, bool JD, bool ST = true>
 struct Plan {
   static constexpr int P3 = P * P * P, Q2 = Q * Q, Q3 = Q2 * Q;
   static constexpr int cmax(int x, int y) { return x > y ? x : y; }
@@ -450,9 +450,7 @@ struct Plan {
   static constexpr int oN = 0, o1 = pad(oN + nN), o2 = pad(o1 + n1), oU = pad(o2 + n2), oG = pad(oU + nU),
                        oJD = pad(oG + nG), end_T = pad(oJD + nJD);
   static constexpr size_t qd_offset_bytes = ((size_t)end_T * sizeof(T) + 15) & ~(size_t)15;
-  // staged qdata precedes the mbarriers: NQB buffers (the residual double-buffers where the occupancy allows, the
-  // Jacobian uses one)
-  static constexpr size_t mbar_offset = qd_offset_bytes + (ST ? NQB * sizeof(double) * 10 * Q3 : 0);
+  static constexpr size_t mbar_offset = qd_offset_bytes + (ST ? sizeof(double) * 10 * Q3 : 0);  // staged qdata, then the mbarrier
   static constexpr size_t bytes = mbar_offset + 16;
   static_assert(5 * P * Q2 <= n1, "sT2 fits in s1");
   static_assert(5 * Q3 <= n2, "w2 fits in s2");
@@ -534,47 +532,31 @@ __device__ __forceinline__ void sgs_add(const PhysConst<double> &c, const double
 // ---------------------------------------------------------------------------------------------------------------------
 // IFunction
 
-// qdata buffers of the residual kernel: two (the element after next is staged while this one computes) where both fit at
-// the kernel's resident CTAs per SM, else one (e.g. P = 5, Q = 6: 111 KB with two buffers would leave one CTA per SM)
-template <int P, int Q, bool ST>
-__host__ __device__ constexpr int ifunction_qdata_buffers() {
-  constexpr size_t static_bytes = sizeof(int32_t) * 2 * 5 * P * P * P + sizeof(double) * kMaxP + 16, reserved = 1024, per_sm = 233472;
-  return (size_t)min_blocks_for(Q, ST) * (Plan<P, Q, 2, double, false, ST, 2>::bytes + static_bytes + reserved) <= per_sm ? 2 : 1;
-}
-
 struct IfunctionPtrs {
   const double *q, *q_dot;
   double *jac_data;   // [E][num_jd][Q3], may be null
   float *jac_f32;     // [E][num_jd][Q3] single-precision shadow for the mixed-precision Jacobian, may be null
   double *v;
   QRef qref;
-  int qdata_tma;      // qdata blocks can be bulk-copied (16-byte aligned base)
 };
 
-template <int P, int Q, bool ST, int SGS = 0, int SV = HB_STATEVAR_CONSERVATIVE>
-__global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p,
-                                                                                               const SgsArg<SGS> sg) {
+// qdata is read at the point (coalesced: thread q reads entry q of each of the element's ten [Q3] rows) after an L2
+// prefetch two elements ahead; staging it in shared memory by TMA measured slower (3.75 against 3.64 ms per 64^3 apply
+// at P = 4, Q = 5; 1.25 against 1.21 ms per 32^3 apply at P = 5, Q = 6), so the kernel has no bulk copies and no waits.
+template <int P, int Q, int SGS = 0, int SV = HB_STATEVAR_CONSERVATIVE>
+__global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_ifunction(const ElemArgs<double> a, const IfunctionPtrs p,
+                                                                                           const SgsArg<SGS> sg) {
   constexpr int NT = nthreads_for<double>(Q);
-  constexpr int NB = ifunction_qdata_buffers<P, Q, ST>();  // qdata buffers: element k uses buffer and mbarrier k % NB
-  using L = Plan<P, Q, 2, double, false, ST, NB>;
+  using L = Plan<P, Q, 2, double, false, false>;
   constexpr int Q3 = L::Q3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sm = reinterpret_cast<double *>(smem_raw);
   double *sN = sm + L::oN, *s1 = sm + L::o1, *s2 = sm + L::o2, *sU = sm + L::oU, *sG = sm + L::oG;
   double *sD = sU + 5 * Q3;
-  double *sQD = reinterpret_cast<double *>(smem_raw + L::qd_offset_bytes);
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::mbar_offset);
-  __shared__ int s_bail;
   __shared__ double s_qref[kMaxP];
   __shared__ int32_t sO[2][5 * L::P3];  // entry offsets of the current / next element
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
 
-  if (threadIdx.x == 0) {
-    mbar_init(mbar, 1);
-    mbar_init(mbar + 1, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_bail = 0;
-  }
   if (threadIdx.x == 0) {  // constant indices: indexing the parameter array with threadIdx would copy it to local memory
 #pragma unroll
     for (int i = 0; i < kMaxP; i++) s_qref[i] = p.qref.x[i];
@@ -589,17 +571,12 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     eo.load(a.offsets, e0);
     eo.store(sO[0]);
     gather_async<P, 2, NT, double>(eo, p.q, p.q_dot, sN);
-    if constexpr (ST) {  // qdata of the first NB elements, one buffer each
-      if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar, p.qdata_tma ? qd_bytes : 0);
-      stage_block<double, NT>(sQD, a.qdata + (int64_t)e0 * 10 * Q3, 10 * Q3, p.qdata_tma, mbar);
-      if (NB == 2 && idx + (int)gridDim.x < a.n_elems) {
-        if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar + 1, p.qdata_tma ? qd_bytes : 0);
-        stage_block<double, NT>(sQD + 10 * Q3, a.qdata + (int64_t)a.elems[idx + gridDim.x] * 10 * Q3, 10 * Q3, p.qdata_tma, mbar + 1);
-      }
-    } else if (threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)e0 * 10 * Q3, qd_bytes);
+    if (threadIdx.x == 0) {
+      prefetch_l2_bulk(a.qdata + (int64_t)e0 * 10 * Q3, qd_bytes);
+      if (idx + (int)gridDim.x < a.n_elems) prefetch_l2_bulk(a.qdata + (int64_t)a.elems[idx + gridDim.x] * 10 * Q3, qd_bytes);
+    }
     cp_async_commit();
   }
-  unsigned kit = 0;  // elements done by this CTA: qdata buffer kit % NB, its mbarrier's phase parity (kit / NB) & 1
   // element ids and entry offsets are read two elements ahead so no global load latency sits on the critical path
   const int G = gridDim.x;
   int ecur = a.elems[idx];
@@ -616,13 +593,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     HB_PT(7)
     cp_async_wait_group<0>();  // this element's node values have landed
     HB_PT(8)
-    if (ST && threadIdx.x == 0 && !mbar_wait_bounded(mbar + kit % NB, (kit / NB) & 1)) {
-      s_bail = 1;
-      atomicOr(a.status, 1);
-    }
-    HB_PT(9)
     __syncthreads();
-    if (s_bail) break;
     HB_PT(0)
     if (en2 >= 0 && threadIdx.x == 0) prefetch_l2_bulk(a.qdata + (int64_t)en2 * 10 * Q3, qd_bytes);
     pass_x_staged<P, Q, 10, NT, double>(a.basis, sN, s1);
@@ -645,7 +616,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
 #pragma unroll
         for (int d = 0; d < 3; d++) gref[d][c] = sG[(d * 5 + c) * Q3 + q];
       }
-      const double *qdp = ST ? sQD + (kit % NB) * 10 * Q3 : a.qdata + (int64_t)e * 10 * Q3;
+      const double *qdp = a.qdata + (int64_t)e * 10 * Q3;
       wdetJ = qdp[q];
 #pragma unroll
       for (int k = 0; k < 9; k++) X[k / 3][k % 3] = qdp[(1 + k) * Q3 + q];
@@ -683,19 +654,6 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
         }
       }
     }
-    if (en >= 0) {  // this qdata buffer consumed: stage the qdata of the element NB ahead into it
-      if constexpr (ST) {
-        const int ea = NB == 2 ? en2 : en;
-        if (ea >= 0) {
-          if (threadIdx.x == 0) {
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx(mbar + kit % NB, p.qdata_tma ? qd_bytes : 0);
-          }
-          stage_block<double, NT>(sQD + (kit % NB) * 10 * Q3, a.qdata + (int64_t)ea * 10 * Q3, 10 * Q3, p.qdata_tma, mbar + kit % NB);
-        }
-      }
-      cp_async_commit();
-    }
     // transpose scratch: w1 in the q_dot slot, w2 and the node values in s2, sT2 in s1, sT1 in sG
     HB_PT(4)
     transpose_passes<P, Q, NT, double>(a.basis, sU, sG, sD, s2, s1, sG, s2);
@@ -708,15 +666,10 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q, ST)
     en = en2;
     en2 = en3;
     nxt = nxt2;
-    kit++;
     HB_PT(6)
   }
   HB_PT_FLUSH(0)
   cp_async_wait_all();
-  if (ST && s_bail && threadIdx.x == 0) {  // let outstanding bulk copies land before exit (bounded waits)
-    mbar_wait_bounded(mbar + kit % NB, (kit / NB) & 1);
-    if (NB == 2) mbar_wait_bounded(mbar + (kit + 1) % NB, ((kit + 1) / NB) & 1);
-  }
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -1461,12 +1414,12 @@ static size_t smem_bytes(int P, int Q) {
   return sizeof(T) * (size_t)(10 * P3 + 10 * P * P * Q + 10 * P * Q * Q + 10 * Q3 + 15 * Q3);
 }
 
-template <int P, int Q, bool ST, int SGS = 0, int SV = HB_STATEVAR_CONSERVATIVE>
+template <int P, int Q, int SGS = 0, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s,
                               const SgsArg<SGS> &sg = SgsArg<SGS>{}) {
-  using L = Plan<P, Q, 2, double, false, ST, ifunction_qdata_buffers<P, Q, ST>()>;
+  using L = Plan<P, Q, 2, double, false, false>;
   const size_t sm = L::bytes;
-  cudaFuncSetAttribute(k_ifunction<P, Q, ST, SGS, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_ifunction<P, Q, SGS, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   IfunctionPtrs p;
   p.q = io->q;
   p.q_dot = io->q_dot;
@@ -1474,19 +1427,16 @@ static int launch_ifunction_v(const HbElemOp *op, const HbNewtonianContext &ctx,
   p.jac_f32 = io->jac_data_f32;
   p.v = io->v;
   for (int i = 0; i < kMaxP; i++) p.qref.x[i] = i < Q ? op->qref1d[i] : 0;
-  p.qdata_tma = ((uintptr_t)io->qdata % 16) == 0;
   for (int c = 0; c < op->num_colors; c++) {
     ElemArgs<double> a = make_args<double>(op, ctx, io->qdata, c);
     if (a.n_elems == 0) continue;
-    k_ifunction<P, Q, ST, SGS, SV><<<grid_for(op, a.n_elems, k_ifunction<P, Q, ST, SGS, SV>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p,
-                                                                                                                                               sg);
+    k_ifunction<P, Q, SGS, SV><<<grid_for(op, a.n_elems, k_ifunction<P, Q, SGS, SV>, nthreads_for<double>(Q), sm), nthreads_for<double>(Q), sm, s>>>(a, p, sg);
   }
   return cudaGetLastError() == cudaSuccess ? HB_SUCCESS : HB_ERROR_CUDA;
 }
 template <int P, int Q, int SV = HB_STATEVAR_CONSERVATIVE>
 static int launch_ifunction(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, cudaStream_t s) {
-  // staged per-point data (TMA, 3 CTAs/SM) measured faster than direct loads at 4 CTAs/SM with spills
-  return launch_ifunction_v<P, Q, true, 0, SV>(op, ctx, io, s);
+  return launch_ifunction_v<P, Q, 0, SV>(op, ctx, io, s);
 }
 
 template <int P, int Q, typename T, bool ST, int SV = HB_STATEVAR_CONSERVATIVE>
@@ -2067,7 +2017,7 @@ static int fill_sgs(const HbMlpDesc *d, const float *w, SgsArg<SGS> &sg) {
 template <int SGS, int SV>
 static int ifunction_sgs_pq(const HbElemOp *op, const HbNewtonianContext &ctx, const HbIFunctionIO *io, const SgsArg<SGS> &sg, cudaStream_t s) {
 #define HB_CASE(PP, QQ) \
-  if (op->P == PP && op->Q == QQ) return launch_ifunction_v<PP, QQ, true, SGS, SV>(op, ctx, io, s, sg);
+  if (op->P == PP && op->Q == QQ) return launch_ifunction_v<PP, QQ, SGS, SV>(op, ctx, io, s, sg);
   HB_SGS_PQ_LIST(HB_CASE)
 #undef HB_CASE
   return HB_ERROR_UNSUPPORTED;
