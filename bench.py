@@ -610,7 +610,12 @@ def main():
         import datetime
 
         import torch
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        # the reference arm is CPU work on rank 0 alone (minutes at full size) while the other ranks wait at the final
+        # barrier: a CPU process group with a long timeout; the GPU arm's ranks exchange over NCCL with a short one
+        if args.impl == "reference":
+            torch.distributed.init_process_group("gloo", timeout=datetime.timedelta(seconds=3600))
+        else:
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
         if args.impl == "reference":
             run_reference(args, rank)

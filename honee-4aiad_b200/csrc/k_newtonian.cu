@@ -658,9 +658,8 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
     HB_PT(4)
     transpose_passes<P, Q, NT, double>(a.basis, sU, sG, sD, s2, s1, sG, s2);
     HB_PT(5)
-    scatter_add<P, NT, double>(sO[buf], s2, p.v);
-    HB_PT(12)
-    __syncthreads();
+    scatter_add<P, NT, double>(sO[buf], s2, p.v);  // no barrier after it: nothing writes shared memory before the next
+    HB_PT(12)                                       // iteration's top barrier
     buf ^= 1;
     ecur = en;
     en = en2;
@@ -807,8 +806,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
       cp_async_commit();
     }
     transpose_passes<P, Q, NT, T>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
-    scatter_add<P, NT, T>(sO[buf], s2, p.v);
-    __syncthreads();
+    scatter_add<P, NT, T>(sO[buf], s2, p.v);  // the next iteration's top barrier orders it before any shared-memory write
     buf ^= 1;
     ecur = en;
     en = en2;

@@ -205,8 +205,11 @@ __device__ __forceinline__ void tau_diag(const PhysConst<T> &c, const St<T> &s, 
   }
   const T tsum = s.rho * s.rho * (T(4) * c.dts * c.dts + ugu) + c.Ctau_v * c.mu * c.mu * g2;
   const T f = sqrt(tsum);
-  const T inv_f = rcp(f);
-  tau[0] = c.Ctau_C * f / (s.rho * (g[0][0] + g[1][1] + g[2][2])) * T(0.125);
+  // one reciprocal for both divisions: 1/f = rt / (f rt) and f / rt = f^2 / (f rt)
+  const T rt = s.rho * (g[0][0] + g[1][1] + g[2][2]);
+  const T r = rcp(f * rt);
+  const T inv_f = rt * r;
+  tau[0] = c.Ctau_C * (f * f * r) * T(0.125);
   tau[1] = c.Ctau_M * inv_f;
   tau[2] = c.Ctau_E * inv_f * c.inv_cv;
 }

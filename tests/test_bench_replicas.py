@@ -55,3 +55,19 @@ def test_single_rank_is_unchanged():
     import bench
     assert bench.max_over_ranks(4.0, 1, None) == 4.0
     assert bench.job_gdofs(1, 2_000_000, 2.0) == pytest.approx(1.0)
+
+
+def test_reference_arm_under_torchrun_prints_one_line_from_rank_zero():
+    """`bench.py --impl reference` launched as the driver launches every arm for N > 1 (torchrun, one process per GPU):
+    rank 0 alone runs the reference's CPU path and prints the JSON line, the other ranks exit 0 without work.  The arm's
+    process group is a CPU (gloo) one, so this runs here; a small box keeps it short."""
+    import json
+    import subprocess
+    port = _free_port()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+           "--master-port", str(port), "bench.py", "--impl", "reference", "--gpus", "2", "--size", "3", "--steps", "1", "--warmup", "1"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    assert lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2 and lines[0]["value"] > 0
