@@ -974,8 +974,7 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
         atomicAdd(p.v + oA[t], r.x());
         if (chasB) atomicAdd(p.v + oB[t], r.y());
       }
-    }
-    __syncthreads();
+    }  // no barrier: the next iteration's top barrier orders the scatter before any shared-memory write
     buf ^= 1;
     eA = nA;
     eB = nB;

@@ -193,30 +193,72 @@ inline bool vec_ok(const T *V, int64_t ldv, const void *w) {
   return ((uintptr_t)V % 16 == 0) && ((uintptr_t)w % 16 == 0) && ((ldv * (int64_t)sizeof(T)) % 16 == 0);
 }
 
-// out[i] = V_i . w for i < k through the per-block partials (kRedBlocks x kMaxK doubles)
+// Blocks of one full wave of a grid-stride kernel at kBS threads: the SMs times the blocks resident per SM, lowered to a
+// whole multiple of the SM count when that exceeds `cap`.  Every block then starts at once and carries the same share, where
+// a fixed grid that is not a whole number of waves leaves a small, slow last wave (the multi-dot's 512 blocks were 1.15 or
+// 1.73 waves at three or two resident blocks per SM).
+template <typename F>
+unsigned full_wave(F kernel, unsigned cap) {
+  int dev = 0, sms = 0, occ = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kBS, 0) != cudaSuccess || sms <= 0 || occ <= 0)
+    return cap;
+  const unsigned per = (unsigned)sms, g = (unsigned)occ * per;
+  if (g <= cap) return g;
+  return cap >= per ? cap / per * per : cap;
+}
+
+// Full-wave grids of the multi-dot and multi-axpy for every basis size, read on the first call for the element type (so
+// before any stream capture that follows a first call; the devices of one process are alike).
+template <typename T>
+struct Waves {
+  unsigned dot[kMaxK + 1], axpy[kMaxK + 1];
+  Waves() {
+#define HB_WAVE(KK)                                                  \
+  dot[KK] = full_wave(k_multidot_vec<T, KK>, kRedBlocks);            \
+  axpy[KK] = full_wave(k_multiaxpy_vec<T, KK>, 148 * 16);
+    HB_BASIS_SIZES(HB_WAVE)
+#undef HB_WAVE
+  }
+};
+template <typename T>
+const Waves<T> &waves() {
+  static const Waves<T> w;
+  return w;
+}
+
+// out[i] = V_i . w for i < k through the per-block partials (at most kRedBlocks x kMaxK doubles)
 template <typename T>
 void launch_multidot(const T *V, int64_t ldv, int k, const T *w, int64_t n, double *partial, double *out, cudaStream_t s) {
+  unsigned nblk = kRedBlocks;
   if (vec_ok(V, ldv, w)) {
+    const Waves<T> &wv = waves<T>();
     switch (k) {
-#define HB_MDOT_CASE(KK) \
-  case KK: k_multidot_vec<T, KK><<<kRedBlocks, kBS, 0, s>>>(V, ldv, w, n, partial); break;
+#define HB_MDOT_CASE(KK)                                                       \
+  case KK:                                                                     \
+    nblk = wv.dot[KK];                                                         \
+    k_multidot_vec<T, KK><<<nblk, kBS, 0, s>>>(V, ldv, w, n, partial);         \
+    break;
       HB_BASIS_SIZES(HB_MDOT_CASE)
 #undef HB_MDOT_CASE
     }
   } else {
     k_multidot<T><<<kRedBlocks, kBS, 0, s>>>(V, ldv, k, w, n, partial);
   }
-  k_multidot_final<<<k, kBS, 0, s>>>(partial, kRedBlocks, k, out);
+  k_multidot_final<<<k, kBS, 0, s>>>(partial, (int)nblk, k, out);
 }
 
 template <typename T>
 void launch_multiaxpy(T *w, const T *V, int64_t ldv, int k, const Coefs &c, int64_t n, cudaStream_t s) {
   if (vec_ok(V, ldv, w)) {
     const int64_t nv = n / (16 / (int64_t)sizeof(T));
-    const unsigned g = (unsigned)(nv / kBS + 1 > 148 * 16 ? 148 * 16 : nv / kBS + 1);
+    const unsigned work = (unsigned)(nv / kBS + 1 > 148 * 16 ? 148 * 16 : nv / kBS + 1);
+    const Waves<T> &wv = waves<T>();
     switch (k) {
-#define HB_MAXPY_CASE(KK) \
-  case KK: k_multiaxpy_vec<T, KK><<<g, kBS, 0, s>>>(w, V, ldv, c, n); break;
+#define HB_MAXPY_CASE(KK)                                                                         \
+  case KK:                                                                                        \
+    k_multiaxpy_vec<T, KK><<<work < wv.axpy[KK] ? work : wv.axpy[KK], kBS, 0, s>>>(w, V, ldv, c, n); \
+    break;
       HB_BASIS_SIZES(HB_MAXPY_CASE)
 #undef HB_MAXPY_CASE
     }
