@@ -72,6 +72,128 @@ __global__ void k_reduce(const T *x, const T *y, int64_t n, int type, double *pa
   if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
 }
 
+// 16-byte vector forms of the kernels in the Krylov inner loop (scale, point-wise multiply, reductions): VW entries per
+// load and store where every pointer is 16-byte aligned (checked by the caller), the last n mod VW entries by block 0.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using V = float4;
+  static constexpr int W = 4;
+  static __device__ __forceinline__ void get(const V &v, float (&x)[4]) { x[0] = v.x, x[1] = v.y, x[2] = v.z, x[3] = v.w; }
+  static __device__ __forceinline__ V make(const float (&x)[4]) { return make_float4(x[0], x[1], x[2], x[3]); }
+};
+template <>
+struct Vec16<double> {
+  using V = double2;
+  static constexpr int W = 2;
+  static __device__ __forceinline__ void get(const V &v, double (&x)[2]) { x[0] = v.x, x[1] = v.y; }
+  static __device__ __forceinline__ V make(const double (&x)[2]) { return make_double2(x[0], x[1]); }
+};
+
+template <typename T>
+__global__ void k_scale_v(T *x, int64_t n, T a) {
+  using H = Vec16<T>;
+  const int64_t nv = n / H::W;
+  typename H::V *xv = reinterpret_cast<typename H::V *>(x);
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nv; j += (int64_t)gridDim.x * blockDim.x) {
+    T u[H::W];
+    H::get(xv[j], u);
+#pragma unroll
+    for (int k = 0; k < H::W; k++) u[k] *= a;
+    xv[j] = H::make(u);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - nv * H::W) x[nv * H::W + threadIdx.x] *= a;
+}
+template <typename T>
+__global__ void k_pmult_v(T *w, const T *x, const T *y, int64_t n) {
+  using H = Vec16<T>;
+  const int64_t nv = n / H::W;
+  const typename H::V *xv = reinterpret_cast<const typename H::V *>(x), *yv = reinterpret_cast<const typename H::V *>(y);
+  typename H::V *wv = reinterpret_cast<typename H::V *>(w);
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nv; j += (int64_t)gridDim.x * blockDim.x) {
+    T a[H::W], b[H::W];
+    H::get(xv[j], a);
+    H::get(yv[j], b);
+#pragma unroll
+    for (int k = 0; k < H::W; k++) a[k] *= b[k];
+    wv[j] = H::make(a);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - nv * H::W) {
+    const int64_t i = nv * H::W + threadIdx.x;
+    w[i] = x[i] * y[i];
+  }
+}
+template <typename T>
+__global__ void k_reduce_v(const T *x, const T *y, int64_t n, int type, double *partial) {
+  using H = Vec16<T>;
+  __shared__ double sh[kBS];
+  const int64_t nv = n / H::W;
+  const typename H::V *xv = reinterpret_cast<const typename H::V *>(x), *yv = reinterpret_cast<const typename H::V *>(y);
+  double acc = 0;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nv; j += (int64_t)gridDim.x * blockDim.x) {
+    T a[H::W], b[H::W];
+    H::get(xv[j], a);
+    if (type == 3) H::get(yv[j], b);
+#pragma unroll
+    for (int k = 0; k < H::W; k++) {
+      const double v = (double)a[k];
+      if (type == 0) acc += fabs(v);
+      else if (type == 1) acc += v * v;
+      else if (type == 2) acc = fmax(acc, fabs(v));
+      else acc += v * (double)b[k];
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - nv * H::W) {
+    const int64_t i = nv * H::W + threadIdx.x;
+    const double v = (double)x[i];
+    if (type == 0) acc += fabs(v);
+    else if (type == 1) acc += v * v;
+    else if (type == 2) acc = fmax(acc, fabs(v));
+    else acc += v * (double)y[i];
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] = type == 2 ? fmax(sh[threadIdx.x], sh[threadIdx.x + s]) : sh[threadIdx.x] + sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+inline bool al16(const void *p) { return p == nullptr || ((uintptr_t)p % 16) == 0; }
+
+// One full wave of a grid-stride kernel at kBS threads (resident blocks per SM x SMs), lowered to a whole multiple of the
+// SM count when that exceeds `cap`.
+template <typename F>
+unsigned wave_blocks(F kernel, unsigned cap) {
+  int dev = 0, sms = 0, occ = 0;
+  unsigned g = cap;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kBS, 0) == cudaSuccess && sms > 0 && occ > 0) {
+    const unsigned w = (unsigned)occ * (unsigned)sms;
+    g = w <= cap ? w : (cap >= (unsigned)sms ? cap / sms * sms : cap);
+  }
+  return g;
+}
+template <typename T>
+struct VecWaves {
+  unsigned scale, pmult, reduce;
+  VecWaves()
+      : scale(wave_blocks(k_scale_v<T>, 148 * 64)), pmult(wave_blocks(k_pmult_v<T>, 148 * 64)), reduce(wave_blocks(k_reduce_v<T>, 1024)) {}
+};
+template <typename T>
+const VecWaves<T> &vec_waves() {
+  static const VecWaves<T> w;
+  return w;
+}
+// blocks for n entries: the full wave, or fewer when n needs fewer (block 0 always exists for the tail)
+template <typename T>
+unsigned capped(unsigned wave, int64_t n) {
+  const int64_t need = (n / Vec16<T>::W + kBS - 1) / kBS;
+  return need < 1 ? 1u : (need < (int64_t)wave ? (unsigned)need : wave);
+}
+
 __global__ void k_reduce_final(double *partial, int n, int type) {
   __shared__ double sh[kBS];
   double acc = 0;
@@ -196,11 +318,13 @@ int hb_vec_set_f32(float *x, int64_t n, float v, void *s) {
   return rc();
 }
 int hb_vec_scale_f64(double *x, int64_t n, double a, void *s) {
-  k_scale<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(x, n, a);
+  if (al16(x)) k_scale_v<<<capped<double>(vec_waves<double>().scale, n), kBS, 0, (cudaStream_t)s>>>(x, n, a);
+  else k_scale<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(x, n, a);
   return rc();
 }
 int hb_vec_scale_f32(float *x, int64_t n, float a, void *s) {
-  k_scale<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(x, n, a);
+  if (al16(x)) k_scale_v<<<capped<float>(vec_waves<float>().scale, n), kBS, 0, (cudaStream_t)s>>>(x, n, a);
+  else k_scale<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(x, n, a);
   return rc();
 }
 int hb_vec_axpy_f64(double *y, double a, const double *x, int64_t n, void *s) {
@@ -220,11 +344,13 @@ int hb_vec_axpby_f32(float *y, float a, float b, const float *x, int64_t n, void
   return rc();
 }
 int hb_vec_pointwise_mult_f64(double *w, const double *x, const double *y, int64_t n, void *s) {
-  k_pmult<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, x, y, n);
+  if (al16(w) && al16(x) && al16(y)) k_pmult_v<<<capped<double>(vec_waves<double>().pmult, n), kBS, 0, (cudaStream_t)s>>>(w, x, y, n);
+  else k_pmult<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, x, y, n);
   return rc();
 }
 int hb_vec_pointwise_mult_f32(float *w, const float *x, const float *y, int64_t n, void *s) {
-  k_pmult<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, x, y, n);
+  if (al16(w) && al16(x) && al16(y)) k_pmult_v<<<capped<float>(vec_waves<float>().pmult, n), kBS, 0, (cudaStream_t)s>>>(w, x, y, n);
+  else k_pmult<<<nblocks(n), kBS, 0, (cudaStream_t)s>>>(w, x, y, n);
   return rc();
 }
 int hb_vec_reciprocal_f64(double *x, int64_t n, void *s) {
@@ -250,13 +376,15 @@ static int reduce_common(int type, double *scratch, double *result, void *s) {
 int hb_vec_reduce_f64(const double *x, const double *y, int64_t n, int type, double *scratch, double *result, void *s) {
   cudaStream_t st = (cudaStream_t)s;
   cudaMemsetAsync(scratch, 0, 1024 * sizeof(double), st);
-  k_reduce<<<1024, kBS, 0, st>>>(x, y, n, type, scratch);
+  if (al16(x) && al16(y)) k_reduce_v<<<capped<double>(vec_waves<double>().reduce, n), kBS, 0, st>>>(x, y, n, type, scratch);
+  else k_reduce<<<1024, kBS, 0, st>>>(x, y, n, type, scratch);
   return reduce_common(type, scratch, result, s);
 }
 int hb_vec_reduce_f32(const float *x, const float *y, int64_t n, int type, double *scratch, double *result, void *s) {
   cudaStream_t st = (cudaStream_t)s;
   cudaMemsetAsync(scratch, 0, 1024 * sizeof(double), st);
-  k_reduce<<<1024, kBS, 0, st>>>(x, y, n, type, scratch);
+  if (al16(x) && al16(y)) k_reduce_v<<<capped<float>(vec_waves<float>().reduce, n), kBS, 0, st>>>(x, y, n, type, scratch);
+  else k_reduce<<<1024, kBS, 0, st>>>(x, y, n, type, scratch);
   return reduce_common(type, scratch, result, s);
 }
 
