@@ -32,7 +32,8 @@ struct HbTimeStepper {
   double             t;
   cudaStream_t       s;
   /* FP64 state */
-  double *q, *q_prev, *q_prev2, *z, *qdot, *res, *jd64, *d_partial, *d_dots, *scratch;
+  double *q, *q_prev, *q_prev2, *z, *qdot, *res, *jd64, *d_partial, *d_dots, *d_dots2, *scratch;
+  double *h_dots; /* pinned host copies of the Gram-Schmidt coefficients: [0, MAXK) first pass, [MAXK, 2 MAXK) refinement */
   /* Krylov (FP32 or FP64) */
   void  *V, *w, *zvec, *diag, *jd32, *y_work;
   float *res32;
@@ -112,6 +113,7 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
   err |= cudaMalloc((void **)&ts->q, nb) | cudaMalloc((void **)&ts->q_prev, nb) | cudaMalloc((void **)&ts->q_prev2, nb);
   err |= cudaMalloc((void **)&ts->z, nb) | cudaMalloc((void **)&ts->qdot, nb) | cudaMalloc((void **)&ts->res, nb) | cudaMalloc((void **)&ts->delta, nb);
   err |= cudaMalloc((void **)&ts->d_partial, sizeof(double) * 512 * MAXK) | cudaMalloc((void **)&ts->d_dots, sizeof(double) * MAXK);
+  err |= cudaMalloc((void **)&ts->d_dots2, sizeof(double) * MAXK) | cudaMallocHost((void **)&ts->h_dots, sizeof(double) * 2 * MAXK);
   err |= cudaMalloc((void **)&ts->scratch, sizeof(double) * 1024);
   err |= cudaMalloc(&ts->V, ksz(ts) * (size_t)ts->ldv * (m + 1)) | cudaMalloc(&ts->w, ksz(ts) * (size_t)ts->n);
   err |= cudaMalloc(&ts->zvec, ksz(ts) * (size_t)ts->n) | cudaMalloc(&ts->diag, ksz(ts) * (size_t)ts->n);
@@ -132,10 +134,11 @@ int hb_ts_create(const HbElemOp *op, const void *ctx184, const double *d_qdata, 
 
 int hb_ts_destroy(HbTimeStepper *ts) {
   if (!ts) return HB_SUCCESS;
-  void *p[] = {ts->q, ts->q_prev, ts->q_prev2, ts->z, ts->qdot, ts->res, ts->delta, ts->d_partial, ts->d_dots, ts->scratch,
+  void *p[] = {ts->q, ts->q_prev, ts->q_prev2, ts->z, ts->qdot, ts->res, ts->delta, ts->d_partial, ts->d_dots, ts->d_dots2, ts->scratch,
                ts->V, ts->w, ts->zvec, ts->diag, ts->jd32, ts->res32, ts->jd64, ts->qp, ts->qdp, ts->rp, ts->pb64, ts->pb32, ts->d_sing};
   for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
     if (p[i]) cudaFree(p[i]);
+  if (ts->h_dots) cudaFreeHost(ts->h_dots);
   free(ts->sgs_w);
   if (ts->sgs_res) cudaFree(ts->sgs_res);
   if (ts->bc_jac) cudaFree(ts->bc_jac);
@@ -287,16 +290,16 @@ static int kv_pc(HbTimeStepper *ts, const void *x, void *z) {
   if (ts->o.jacobian_fp32) return hb_vec_pointwise_mult_f32((float *)z, (const float *)ts->diag, (const float *)x, ts->n, ts->s);
   return hb_vec_pointwise_mult_f64((double *)z, (const double *)ts->diag, (const double *)x, ts->n, ts->s);
 }
-static int kv_multidot(HbTimeStepper *ts, int k, const void *w, double *h) {
-  if (ts->o.jacobian_fp32) HBCK(hb_krylov_multidot_f32((const float *)ts->V, ts->ldv, k, (const float *)w, ts->n, ts->d_partial, ts->d_dots, ts->s));
-  else HBCK(hb_krylov_multidot_f64((const double *)ts->V, ts->ldv, k, (const double *)w, ts->n, ts->d_partial, ts->d_dots, ts->s));
-  CUCK(cudaMemcpyAsync(h, ts->d_dots, sizeof(double) * k, cudaMemcpyDeviceToHost, ts->s));
-  CUCK(cudaStreamSynchronize(ts->s));
+/* d_h = V[:, :k]^T w, left on the device */
+static int kv_multidot_dev(HbTimeStepper *ts, int k, const void *w, double *d_h) {
+  if (ts->o.jacobian_fp32) HBCK(hb_krylov_multidot_f32((const float *)ts->V, ts->ldv, k, (const float *)w, ts->n, ts->d_partial, d_h, ts->s));
+  else HBCK(hb_krylov_multidot_f64((const double *)ts->V, ts->ldv, k, (const double *)w, ts->n, ts->d_partial, d_h, ts->s));
   return HB_SUCCESS;
 }
-static int kv_multiaxpy(HbTimeStepper *ts, void *w, int k, const double *c) {
-  if (ts->o.jacobian_fp32) return hb_krylov_multiaxpy_f32((float *)w, (const float *)ts->V, ts->ldv, k, c, ts->n, ts->s);
-  return hb_krylov_multiaxpy_f64((double *)w, (const double *)ts->V, ts->ldv, k, c, ts->n, ts->s);
+/* w -= V[:, :k] d_h with the coefficients read on the device */
+static int kv_multiaxpy_dev(HbTimeStepper *ts, void *w, int k, const double *d_h) {
+  if (ts->o.jacobian_fp32) return hb_krylov_multiaxpy_dev_f32((float *)w, (const float *)ts->V, ts->ldv, k, d_h, -1.0, ts->n, ts->s);
+  return hb_krylov_multiaxpy_dev_f64((double *)w, (const double *)ts->V, ts->ldv, k, d_h, -1.0, ts->n, ts->s);
 }
 
 /* Jacobi diagonal (or point blocks) at the current linearisation point, stored inverted; *failed: a point block had no
@@ -340,7 +343,7 @@ static int assemble_pc(HbTimeStepper *ts, int *failed) {
  * (res FP64) to relative tolerance ksp_rtol.  delta (FP64) receives the solution. */
 static int gmres(HbTimeStepper *ts, int *its_out, double *rnorm_out) {
   const int m = ts->o.gmres_restart;
-  double    H[MAXK + 1][MAXK], cs[MAXK], sn[MAXK], g[MAXK + 1], hcol[MAXK], h2[MAXK], y[MAXK];
+  double    H[MAXK + 1][MAXK], cs[MAXK], sn[MAXK], g[MAXK + 1], y[MAXK];
   int       its = 0;
   HBCK(hb_vec_set_f64(ts->delta, ts->n, 0.0, ts->s));
   /* r0 = -res (x0 = 0) */
@@ -363,28 +366,26 @@ static int gmres(HbTimeStepper *ts, int *its_out, double *rnorm_out) {
     g[0]  = beta;
     int k = 0;
     for (; k < m && its < ts->o.ksp_max_it; k++, its++) {
+      /* the operator writes the next basis vector in place; it is orthogonalised and normalised there */
+      void *wk = kv_col(ts, k + 1);
       HBCK(kv_pc(ts, kv_col(ts, k), ts->zvec));
-      HBCK(kv_jac(ts, ts->zvec, ts->w));
-      /* classical Gram-Schmidt, optionally with one refinement pass (CGS2) */
-      HBCK(kv_multidot(ts, k + 1, ts->w, hcol));
-      for (int i = 0; i <= k; i++) y[i] = -hcol[i];
-      HBCK(kv_multiaxpy(ts, ts->w, k + 1, y));
+      HBCK(kv_jac(ts, ts->zvec, wk));
+      /* classical Gram-Schmidt, optionally with one refinement pass (CGS2).  The coefficients stay on the device for the
+       * update and reach the host by asynchronous copies into pinned memory, complete once the norm has synchronised the
+       * stream: one host round trip per iteration */
+      HBCK(kv_multidot_dev(ts, k + 1, wk, ts->d_dots));
+      HBCK(kv_multiaxpy_dev(ts, wk, k + 1, ts->d_dots));
+      CUCK(cudaMemcpyAsync(ts->h_dots, ts->d_dots, sizeof(double) * (size_t)(k + 1), cudaMemcpyDeviceToHost, ts->s));
       if (ts->o.cgs_refine) {
-        HBCK(kv_multidot(ts, k + 1, ts->w, h2));
-        for (int i = 0; i <= k; i++) {
-          y[i] = -h2[i];
-          hcol[i] += h2[i];
-        }
-        HBCK(kv_multiaxpy(ts, ts->w, k + 1, y));
+        HBCK(kv_multidot_dev(ts, k + 1, wk, ts->d_dots2));
+        HBCK(kv_multiaxpy_dev(ts, wk, k + 1, ts->d_dots2));
+        CUCK(cudaMemcpyAsync(ts->h_dots + MAXK, ts->d_dots2, sizeof(double) * (size_t)(k + 1), cudaMemcpyDeviceToHost, ts->s));
       }
       double hn;
-      HBCK(kv_norm2(ts, ts->w, &hn));
-      for (int i = 0; i <= k; i++) H[i][k] = hcol[i];
+      HBCK(kv_norm2(ts, wk, &hn));
+      for (int i = 0; i <= k; i++) H[i][k] = ts->o.cgs_refine ? ts->h_dots[i] + ts->h_dots[MAXK + i] : ts->h_dots[i];
       H[k + 1][k] = hn;
-      if (hn > 0) {
-        HBCK(kv_copy(ts, kv_col(ts, k + 1), ts->w));
-        HBCK(kv_scale(ts, kv_col(ts, k + 1), 1.0 / hn));
-      }
+      if (hn > 0) HBCK(kv_scale(ts, wk, 1.0 / hn));
       /* apply the previous Givens rotations, then a new one */
       for (int i = 0; i < k; i++) {
         const double a = H[i][k], b = H[i + 1][k];

@@ -183,6 +183,50 @@ __global__ void __launch_bounds__(kBS) k_multiaxpy_vec(T *__restrict__ w, const 
   }
 }
 
+// The same with the coefficients read from device memory, times `sign` (the Gram-Schmidt step passes the multi-dot's
+// result, so no host round trip separates the two); sign * c[i] is formed exactly as the host path's negated copy.
+template <typename T, int K>
+__global__ void __launch_bounds__(kBS) k_multiaxpy_vec_dev(T *__restrict__ w, const T *__restrict__ V, int64_t ldv, const double *__restrict__ dc,
+                                                           double sign, int64_t n) {
+  constexpr int VW = 16 / sizeof(T);
+  double c[K];
+#pragma unroll
+  for (int i = 0; i < K; i++) c[i] = sign * dc[i];
+  const int64_t nv = n / VW;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nv; j += (int64_t)gridDim.x * blockDim.x) {
+    T wv[VW];
+    ld16(w + j * VW, wv);
+    double s[VW];
+#pragma unroll
+    for (int u = 0; u < VW; u++) s[u] = (double)wv[u];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+      T x[VW];
+      ld16(V + i * ldv + j * VW, x);
+#pragma unroll
+      for (int u = 0; u < VW; u++) s[u] += c[i] * (double)x[u];
+    }
+#pragma unroll
+    for (int u = 0; u < VW; u++) wv[u] = T(s[u]);
+    st16(w + j * VW, wv);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - nv * VW) {
+    const int64_t e = nv * VW + threadIdx.x;
+    double s = (double)w[e];
+#pragma unroll
+    for (int i = 0; i < K; i++) s += c[i] * (double)V[i * ldv + e];
+    w[e] = T(s);
+  }
+}
+template <typename T>
+__global__ void k_multiaxpy_dev(T *w, const T *V, int64_t ldv, int k, const double *dc, double sign, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    double s = (double)w[e];
+    for (int i = 0; i < k; i++) s += (sign * dc[i]) * (double)V[i * ldv + e];
+    w[e] = T(s);
+  }
+}
+
 #define HB_BASIS_SIZES(X)                                                                                               \
   X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20) X(21) \
   X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29) X(30) X(31) X(32)
@@ -212,11 +256,12 @@ unsigned full_wave(F kernel, unsigned cap) {
 // before any stream capture that follows a first call; the devices of one process are alike).
 template <typename T>
 struct Waves {
-  unsigned dot[kMaxK + 1], axpy[kMaxK + 1];
+  unsigned dot[kMaxK + 1], axpy[kMaxK + 1], axpy_dev[kMaxK + 1];
   Waves() {
 #define HB_WAVE(KK)                                                  \
   dot[KK] = full_wave(k_multidot_vec<T, KK>, kRedBlocks);            \
-  axpy[KK] = full_wave(k_multiaxpy_vec<T, KK>, 148 * 16);
+  axpy[KK] = full_wave(k_multiaxpy_vec<T, KK>, 148 * 16);            \
+  axpy_dev[KK] = full_wave(k_multiaxpy_vec_dev<T, KK>, 148 * 16);
     HB_BASIS_SIZES(HB_WAVE)
 #undef HB_WAVE
   }
@@ -264,6 +309,25 @@ void launch_multiaxpy(T *w, const T *V, int64_t ldv, int k, const Coefs &c, int6
     }
   } else {
     k_multiaxpy<T, T><<<nblocks(n), kBS, 0, s>>>(w, V, ldv, k, c, n);
+  }
+}
+
+template <typename T>
+void launch_multiaxpy_dev(T *w, const T *V, int64_t ldv, int k, const double *dc, double sign, int64_t n, cudaStream_t s) {
+  if (vec_ok(V, ldv, w)) {
+    const int64_t nv = n / (16 / (int64_t)sizeof(T));
+    const unsigned work = (unsigned)(nv / kBS + 1 > 148 * 16 ? 148 * 16 : nv / kBS + 1);
+    const Waves<T> &wv = waves<T>();
+    switch (k) {
+#define HB_MAXPY_DEV_CASE(KK)                                                                                          \
+  case KK:                                                                                                             \
+    k_multiaxpy_vec_dev<T, KK><<<work < wv.axpy_dev[KK] ? work : wv.axpy_dev[KK], kBS, 0, s>>>(w, V, ldv, dc, sign, n); \
+    break;
+      HB_BASIS_SIZES(HB_MAXPY_DEV_CASE)
+#undef HB_MAXPY_DEV_CASE
+    }
+  } else {
+    k_multiaxpy_dev<T><<<nblocks(n), kBS, 0, s>>>(w, V, ldv, k, dc, sign, n);
   }
 }
 
@@ -591,6 +655,16 @@ int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const 
   memset(&cf, 0, sizeof cf);
   memcpy(cf.c, c, sizeof(double) * k);
   launch_multiaxpy<float>(w, V, ldv, k, cf, n, (cudaStream_t)s);
+  return rc();
+}
+int hb_krylov_multiaxpy_dev_f64(double *w, const double *V, int64_t ldv, int k, const double *d_c, double sign, int64_t n, void *s) {
+  if (k < 1 || k > kMaxK || !d_c) return HB_ERROR_INVALID;
+  launch_multiaxpy_dev<double>(w, V, ldv, k, d_c, sign, n, (cudaStream_t)s);
+  return rc();
+}
+int hb_krylov_multiaxpy_dev_f32(float *w, const float *V, int64_t ldv, int k, const double *d_c, double sign, int64_t n, void *s) {
+  if (k < 1 || k > kMaxK || !d_c) return HB_ERROR_INVALID;
+  launch_multiaxpy_dev<float>(w, V, ldv, k, d_c, sign, n, (cudaStream_t)s);
   return rc();
 }
 int hb_krylov_multiaxpy_f32_to_f64(double *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s) {

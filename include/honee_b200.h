@@ -250,7 +250,8 @@ HB_EXPORT int hb_krylov_multidot_f32(const float *V, int64_t ldv, int k, const f
 /* hb_krylov_multidot_f64 that allocates nothing and takes no work buffer: the partial sums live in a fixed 128 KiB device
  * array inside this library (room for k <= HB_GMRES_MAX_BASIS; larger k returns HB_ERROR_INVALID, nothing launched).
  * No counterpart in the reference (PETSc's VecMDot owns its work space); it exists for callers that cannot hand over a
- * device buffer, such as a vector-library inner-product callback.  The first call on each device looks the array up
+ * device buffer, such as a vector-library inner-product callback.  The first call on each device looks the array up (and
+ * reads the block kernels' occupancy, which sizes their grids)
  * and belongs before any stream capture; calls that overlap on one device (different streams or host threads) race on
  * the shared array and must be serialised by the caller.  The looked-up address is kept per device ordinal for the life
  * of the process: after cudaDeviceReset (or any teardown of the device's primary context) the module is loaded anew and
@@ -259,6 +260,10 @@ HB_EXPORT int hb_krylov_multidot_f64_static(const double *V, int64_t ldv, int k,
 HB_EXPORT int hb_krylov_multiaxpy_f64(double *w, const double *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f32(float *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
 HB_EXPORT int hb_krylov_multiaxpy_f32_to_f64(double *w, const float *V, int64_t ldv, int k, const double *c, int64_t n, void *s);
+/* w += sign * sum_{i<k} d_c[i] V_i with the k coefficients in device memory (e.g. a multi-dot's d_out, sign -1 for the
+ * Gram-Schmidt step), so no host synchronisation separates the multi-dot and the update; FP64 sums as above. */
+HB_EXPORT int hb_krylov_multiaxpy_dev_f64(double *w, const double *V, int64_t ldv, int k, const double *d_c, double sign, int64_t n, void *s);
+HB_EXPORT int hb_krylov_multiaxpy_dev_f32(float *w, const float *V, int64_t ldv, int k, const double *d_c, double sign, int64_t n, void *s);
 /* Point-block Jacobi (PCVPBJACOBI on 5 x 5 node blocks, row-major, as hb_point_block_diagonal_* writes them): invert every
  * block in FP64 with partial pivoting (inv may equal blocks for the FP64 form); blocks with a vanishing pivot become the
  * identity and are counted in *d_singular (a device int), copied to *h_singular when that is not NULL (synchronises s).
