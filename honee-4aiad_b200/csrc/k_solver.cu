@@ -219,11 +219,11 @@ __global__ void __launch_bounds__(kBS) k_multiaxpy_vec_dev(T *__restrict__ w, co
   }
 }
 template <typename T>
-__global__ void k_multiaxpy_dev(T *w, const T *V, int64_t ldv, int k, const double *dc, double sign, int64_t n) {
+__global__ void k_multiaxpy_dev(T *w, const T *V, int64_t ldv, int k, const double *dc, double sign, int64_t n) {  // as k_multiaxpy
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    double s = (double)w[e];
+    double s = 0;
     for (int i = 0; i < k; i++) s += (sign * dc[i]) * (double)V[i * ldv + e];
-    w[e] = T(s);
+    w[e] = T((double)w[e] + s);
   }
 }
 

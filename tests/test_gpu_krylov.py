@@ -44,3 +44,30 @@ def test_multidot_and_multiaxpy_match_torch(dtype, k, n, ldv):
     ref_w = w0 + (torch.tensor(c, dtype=torch.float64, device=dev)[:, None] * V[:, :n].double()).sum(0)
     tol = 1e-14 if dtype == "f64" else 2e-7  # FP64 sum rounded once to the storage precision
     torch.testing.assert_close(w.double(), ref_w, rtol=tol, atol=tol * float(ref_w.abs().max()))
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("k,n,ldv", [(1, 10, 12), (7, 100_001, 100_004), (30, 65_537, 65_537), (3, 7, 7)])
+def test_multiaxpy_with_device_coefficients_equals_the_host_form(dtype, k, n, ldv):
+    """hb_krylov_multiaxpy_dev_* (coefficients in device memory times a sign, as the GMRES loop passes the multi-dot's
+    result with sign -1) gives the host-coefficient multi-axpy's result bit for bit, on the vectorised and element-wise
+    paths."""
+    import torch
+    L = _lib()
+    for name in ("hb_krylov_multiaxpy_dev_f64", "hb_krylov_multiaxpy_dev_f32"):
+        getattr(L, name).argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_double, C.c_int64, C.c_void_p]
+    dev = torch.device("cuda:0")
+    tt = torch.float64 if dtype == "f64" else torch.float32
+    g = torch.Generator().manual_seed(k * 11 + n)
+    V = torch.randn(k, ldv, generator=g, dtype=torch.float64).to(dev, tt)
+    w = torch.randn(n, generator=g, dtype=torch.float64).to(dev, tt)
+    h = torch.randn(k, generator=g, dtype=torch.float64)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    w_host, w_dev = w.clone(), w.clone()
+    neg = (C.c_double * k)(*[-float(x) for x in h])
+    assert getattr(L, f"hb_krylov_multiaxpy_{dtype}")(w_host.data_ptr(), V.data_ptr(), ldv, k, neg, n, s) == 0
+    d_h = h.to(dev)
+    assert getattr(L, f"hb_krylov_multiaxpy_dev_{dtype}")(w_dev.data_ptr(), V.data_ptr(), ldv, k, d_h.data_ptr(), -1.0, n, s) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(w_dev, w_host)
+    assert getattr(L, f"hb_krylov_multiaxpy_dev_{dtype}")(w_dev.data_ptr(), V.data_ptr(), ldv, 0, d_h.data_ptr(), -1.0, n, s) != 0
