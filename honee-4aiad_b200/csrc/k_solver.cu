@@ -343,33 +343,11 @@ __global__ void k_combine(const double *__restrict__ q1, const double *__restric
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
-// Monitors: one CTA per element (not a hot path), direct tensor evaluation of q and its reference gradient at each point.
+// Monitors: one CTA per element, q and its reference gradient tabulated at the points by sum factorisation (mon_tabulate).
 
 struct MonBasis {
   double B[HB_MAX_P * HB_MAX_P], G[HB_MAX_P * HB_MAX_P];
 };
-
-__device__ void eval_point(const double *sN, int P, int Q, const MonBasis &b, int qp, double qi[5], double gref[3][5]) {
-  const int i = qp % Q, j = (qp / Q) % Q, k = qp / (Q * Q);
-  for (int c = 0; c < 5; c++) {
-    qi[c] = 0;
-    gref[0][c] = gref[1][c] = gref[2][c] = 0;
-  }
-  for (int pc = 0; pc < P; pc++)
-    for (int pb = 0; pb < P; pb++)
-      for (int pa = 0; pa < P; pa++) {
-        const int p = (pc * P + pb) * P + pa;
-        const double bx = b.B[i * P + pa], by = b.B[j * P + pb], bz = b.B[k * P + pc];
-        const double gx = b.G[i * P + pa], gy = b.G[j * P + pb], gz = b.G[k * P + pc];
-        for (int c = 0; c < 5; c++) {
-          const double u = sN[p * 5 + c];
-          qi[c] += bx * by * bz * u;
-          gref[0][c] += gx * by * bz * u;
-          gref[1][c] += bx * gy * bz * u;
-          gref[2][c] += bx * by * gz * u;
-        }
-      }
-}
 
 // physical gradient of the state (StatePhysicalGradientFromReference, newtonian_state.h:581-593) in the state variable sv
 __device__ __forceinline__ void mon_gradient(int sv, const hb::PhysConst<double> &pc, const hb::St<double> &s, const hb::SAux<double> &a,
@@ -381,6 +359,71 @@ __device__ __forceinline__ void mon_gradient(int sv, const hb::PhysConst<double>
   }
 }
 
+// q (and, with grads, its reference gradient) at the Q^3 points of one element by sum factorisation in shared memory:
+// an x pass (B, and G with grads), a y pass and a z pass, one thread per 1D output fibre: the tensor-product sums
+// sum_{pa,pb,pc} B_i B_j B_k u (and G in one direction) evaluated in O(P) instead of O(P^3) operations per point.  sN [P^3][5] node-major; work: T1B, T1G
+// [5][P][P][Q], T2BB, T2BG, T2GB [5][P][Q][Q]; out [1 or 4][5][Q^3]: the values, then d/dX0, d/dX1, d/dX2.
+__device__ void mon_tabulate(const double *sN, int P, int Q, const MonBasis &b, bool grads, double *work, double *out) {
+  const int P2Q = P * P * Q, PQ2 = P * Q * Q, Q2 = Q * Q, Q3 = Q2 * Q;
+  double *T1B = work, *T1G = T1B + 5 * P2Q, *T2BB = T1G + (grads ? 5 * P2Q : 0), *T2BG = T2BB + 5 * PQ2, *T2GB = T2BG + 5 * PQ2;
+  for (int t = threadIdx.x; t < 5 * P2Q; t += blockDim.x) {  // x pass: [c][pc][pb][i]
+    const int c = t / P2Q, r = t % P2Q, pcb = r / Q, i = r % Q;
+    const double *u = sN + (pcb * P) * 5 + c;
+    double sb = 0, sg = 0;
+    for (int pa = 0; pa < P; pa++) {
+      sb += b.B[i * P + pa] * u[pa * 5];
+      sg += b.G[i * P + pa] * u[pa * 5];
+    }
+    T1B[t] = sb;
+    if (grads) T1G[t] = sg;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 5 * PQ2; t += blockDim.x) {  // y pass: [c][pc][j][i]
+    const int c = t / PQ2, r = t % PQ2, pc = r / Q2, j = (r / Q) % Q, i = r % Q;
+    const int base = ((c * P + pc) * P) * Q + i;
+    double bb = 0, bg = 0, gb = 0;
+    for (int pb = 0; pb < P; pb++) {
+      const double x = T1B[base + pb * Q];
+      bb += b.B[j * P + pb] * x;
+      if (grads) {
+        bg += b.G[j * P + pb] * x;
+        gb += b.B[j * P + pb] * T1G[base + pb * Q];
+      }
+    }
+    T2BB[t] = bb;
+    if (grads) {
+      T2BG[t] = bg;
+      T2GB[t] = gb;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 5 * Q3; t += blockDim.x) {  // z pass: [c][k][j][i]
+    const int c = t / Q3, r = t % Q3, k = r / Q2, ji = r % Q2;
+    const int base = (c * P) * Q2 + ji;
+    double v = 0, dx = 0, dy = 0, dz = 0;
+    for (int pc = 0; pc < P; pc++) {
+      const double bz = b.B[k * P + pc], x = T2BB[base + pc * Q2];
+      v += bz * x;
+      if (grads) {
+        dz += b.G[k * P + pc] * x;
+        dy += bz * T2BG[base + pc * Q2];
+        dx += bz * T2GB[base + pc * Q2];
+      }
+    }
+    out[c * Q3 + r] = v;
+    if (grads) {
+      out[(5 + c) * Q3 + r] = dx;
+      out[(10 + c) * Q3 + r] = dy;
+      out[(15 + c) * Q3 + r] = dz;
+    }
+  }
+  __syncthreads();
+}
+__host__ __device__ inline size_t mon_smem_doubles(int P, int Q, bool grads, int nt, int nred) {
+  const size_t P3 = (size_t)P * P * P, P2Q = (size_t)P * P * Q, PQ2 = (size_t)P * Q * Q, Q3 = (size_t)Q * Q * Q;
+  return 5 * P3 + (grads ? 2 : 1) * 5 * P2Q + (grads ? 3 : 1) * 5 * PQ2 + (grads ? 4 : 1) * 5 * Q3 + (size_t)nred * nt;
+}
+
 // per-element partial sums of the five kinetic-energy integrands [num_elem][5] (MonitorTotalKineticEnergy_Conserv/_Prim/
 // _Entropy, qfunctions/monitor_totalkineticenergy.h:8-51)
 // point_out (may be null): the five integrands at every point, E-vector [elem][5][Q^3], the output of the Ceed-bound
@@ -389,13 +432,17 @@ __global__ void k_monitor_ke(int P, int Q, const int32_t *__restrict__ offsets, 
                              hb::PhysConst<double> pc, int sv, MonBasis b, double *__restrict__ elem_sums, double *__restrict__ point_out) {
   extern __shared__ double sm[];
   const int e = blockIdx.x, P3 = P * P * P, Q3 = Q * Q * Q;
-  double *sN = sm, *red = sm + 5 * P3;
+  double *sN = sm, *sW = sN + 5 * P3, *sQ = sW + 2 * 5 * P * P * Q + 3 * 5 * P * Q * Q, *red = sQ + 4 * 5 * Q3;
   for (int t = threadIdx.x; t < 5 * P3; t += blockDim.x) sN[t] = q[offsets[(int64_t)e * P3 + t / 5] + t % 5];
   __syncthreads();
+  mon_tabulate(sN, P, Q, b, true, sW, sQ);
   double acc[5] = {0, 0, 0, 0, 0};
   for (int qp = threadIdx.x; qp < Q3; qp += blockDim.x) {
     double qi[5], gref[3][5], X[3][3];
-    eval_point(sN, P, Q, b, qp, qi, gref);
+    for (int c = 0; c < 5; c++) {
+      qi[c] = sQ[c * Q3 + qp];
+      for (int d = 0; d < 3; d++) gref[d][c] = sQ[((1 + d) * 5 + c) * Q3 + qp];
+    }
     const double *qd = qdata + (int64_t)e * 10 * Q3;
     const double wdetJ = qd[qp];
     for (int kk = 0; kk < 9; kk++) X[kk / 3][kk % 3] = qd[(1 + kk) * Q3 + qp];
@@ -442,13 +489,14 @@ __global__ void k_monitor_cfl(int P, int Q, const int32_t *__restrict__ offsets,
                               hb::PhysConst<double> pc, int sv, MonBasis b, double *__restrict__ elem_minmax, double *__restrict__ point_out) {
   extern __shared__ double sm[];
   const int e = blockIdx.x, P3 = P * P * P, Q3 = Q * Q * Q;
-  double *sN = sm, *red = sm + 5 * P3;
+  double *sN = sm, *sW = sN + 5 * P3, *sQ = sW + 5 * P * P * Q + 5 * P * Q * Q, *red = sQ + 5 * Q3;
   for (int t = threadIdx.x; t < 5 * P3; t += blockDim.x) sN[t] = q[offsets[(int64_t)e * P3 + t / 5] + t % 5];
   __syncthreads();
+  mon_tabulate(sN, P, Q, b, false, sW, sQ);
   double mn = 1e300, mx = -1e300;
   for (int qp = threadIdx.x; qp < Q3; qp += blockDim.x) {
-    double qi[5], gref[3][5], X[3][3], g[3][3];
-    eval_point(sN, P, Q, b, qp, qi, gref);
+    double qi[5], X[3][3], g[3][3];
+    for (int c = 0; c < 5; c++) qi[c] = sQ[c * Q3 + qp];
     const double *qd = qdata + (int64_t)e * 10 * Q3;
     for (int kk = 0; kk < 9; kk++) X[kk / 3][kk % 3] = qd[(1 + kk) * Q3 + qp];
     hb::St<double> s;
@@ -719,9 +767,9 @@ static int state_var_of(const void *ctx184, int *sv) {
 int hb_monitor_ke(const HbElemOp *op, const void *ctx184, const double *q, const double *qdata, double *d_scratch, double sums[5], void *s) {
   int sv = 0;
   if (state_var_of(ctx184, &sv)) return HB_ERROR_UNSUPPORTED;
-  const int P3 = op->P * op->P * op->P;
   const int nt = 128;
-  const size_t sm = sizeof(double) * (5 * P3 + 5 * nt);
+  const size_t sm = sizeof(double) * mon_smem_doubles(op->P, op->Q, true, nt, 5);
+  if (cudaFuncSetAttribute(k_monitor_ke, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
   k_monitor_ke<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), d_scratch, nullptr);
   if (rc()) return HB_ERROR_CUDA;
   double *h = (double *)malloc(sizeof(double) * 5 * (size_t)op->num_elem);
@@ -740,9 +788,9 @@ int hb_monitor_cfl(const HbElemOp *op, const void *ctx184, const double *q, cons
                    void *s) {
   int sv = 0;
   if (state_var_of(ctx184, &sv)) return HB_ERROR_UNSUPPORTED;
-  const int P3 = op->P * op->P * op->P;
   const int nt = 128;
-  const size_t sm = sizeof(double) * (5 * P3 + 2 * nt);
+  const size_t sm = sizeof(double) * mon_smem_doubles(op->P, op->Q, false, nt, 2);
+  if (cudaFuncSetAttribute(k_monitor_cfl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
   k_monitor_cfl<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), d_scratch, nullptr);
   if (rc()) return HB_ERROR_CUDA;
   double *h = (double *)malloc(sizeof(double) * 2 * (size_t)op->num_elem);
@@ -765,8 +813,9 @@ int hb_monitor_ke_points(const HbElemOp *op, const void *ctx184, const double *q
   int sv = 0;
   if (state_var_of(ctx184, &sv)) return HB_ERROR_UNSUPPORTED;
   if (op->num_elem == 0) return HB_SUCCESS;
-  const int P3 = op->P * op->P * op->P, nt = 128;
-  const size_t sm = sizeof(double) * (5 * P3 + 5 * nt);
+  const int nt = 128;
+  const size_t sm = sizeof(double) * mon_smem_doubles(op->P, op->Q, true, nt, 5);
+  if (cudaFuncSetAttribute(k_monitor_ke, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
   k_monitor_ke<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), nullptr, e_out);
   return rc();
 }
@@ -774,8 +823,9 @@ int hb_monitor_cfl_points(const HbElemOp *op, const void *ctx184, const double *
   int sv = 0;
   if (state_var_of(ctx184, &sv)) return HB_ERROR_UNSUPPORTED;
   if (op->num_elem == 0) return HB_SUCCESS;
-  const int P3 = op->P * op->P * op->P, nt = 128;
-  const size_t sm = sizeof(double) * (5 * P3 + 2 * nt);
+  const int nt = 128;
+  const size_t sm = sizeof(double) * mon_smem_doubles(op->P, op->Q, false, nt, 2);
+  if (cudaFuncSetAttribute(k_monitor_cfl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return HB_ERROR_CUDA;
   k_monitor_cfl<<<op->num_elem, nt, sm, (cudaStream_t)s>>>(op->P, op->Q, op->d_offsets, q, qdata, phys_of(ctx184), sv, mon_basis(op), nullptr, e_out);
   return rc();
 }
