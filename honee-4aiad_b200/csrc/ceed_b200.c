@@ -325,8 +325,8 @@ int CeedDestroy(Ceed *ceed) {
     cudaStreamDestroy((*ceed)->s_h2d);
     cudaStreamDestroy((*ceed)->s_d2h);
     cudaEventDestroy((*ceed)->ev_tmp);
-    cudaFreeHost((*ceed)->h_status);
   }
+  if ((*ceed)->h_status) cudaFreeHost((*ceed)->h_status);
   free(*ceed);
   *ceed = NULL;
   return CEED_ERROR_SUCCESS;
@@ -407,10 +407,10 @@ static int vec_unstale(CeedVector v) {
 }
 static int ceed_copy_streams(Ceed c) {
   if (c->copy_streams) return CEED_ERROR_SUCCESS;
+  if (!c->h_status) CUDA_CK(c, cudaMallocHost((void **)&c->h_status, sizeof(int) * 64));
   CUDA_CK(c, cudaStreamCreateWithFlags(&c->s_h2d, cudaStreamNonBlocking));
   CUDA_CK(c, cudaStreamCreateWithFlags(&c->s_d2h, cudaStreamNonBlocking));
   CUDA_CK(c, cudaEventCreateWithFlags(&c->ev_tmp, cudaEventDisableTiming));
-  CUDA_CK(c, cudaMallocHost((void **)&c->h_status, sizeof(int) * 64));
   c->copy_streams = 1;
   return CEED_ERROR_SUCCESS;
 }
