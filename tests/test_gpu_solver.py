@@ -196,3 +196,29 @@ def test_matrix_free_jacobian_newton_reaches_the_same_state():
     assert rel_l2(qb - q0, qa - q0) < 1e-6
     with pytest.raises(K.HbError):
         S.TimeStepper(op, prob.context_bytes(ctx), qdata, jfnk=1, jacobian_fp32=1)
+
+
+@pytest.mark.parametrize("P,Q,n", [(2, 2, (3, 2, 2)), (4, 5, (2, 2, 1)), (6, 7, (2, 1, 1)), (8, 8, (1, 1, 2))])
+def test_monitors_tabulate_every_basis_size(P, Q, n):
+    """The monitors tabulate q and its gradient by sum factorisation in shared memory sized from P and Q (205 KB at the
+    largest basis the library accepts, P = Q = 8): the kinetic-energy sums equal the oracle's direct evaluation to 1e-12,
+    and the CFL monitor of a uniform flow is exact, at the smallest, the benchmarked and the largest bases."""
+    import torch
+    mesh = prob.box_mesh(n, P)
+    basis = prob.tensor_basis(P, Q)
+    ctx = prob.newtonian_context(P - 1, cv=717.5, cp=1004.5, mu=1.8e-5, k=0.0257)
+    cb = prob.context_bytes(ctx)
+    q = prob.multimode_state(mesh, basis, ctx.gas, seed=P)
+    op = K.ElemOp(mesh, basis)
+    qdata = torch.zeros(mesh.num_elem * 10 * basis.Q ** 3, dtype=torch.float64, device=_dev())
+    op.setup_qdata(torch.from_numpy(np.ascontiguousarray(mesh.x_elem)).to(_dev()), qdata)
+    scratch = torch.empty(5 * mesh.num_elem, dtype=torch.float64, device=_dev())
+    sums = S.monitor_ke(op, cb, torch.from_numpy(q).to(_dev()), qdata, scratch)
+    ref = O.monitor_ke(oracle_mesh(mesh, basis), cb, q, O.setup_qdata(mesh.num_elem, basis.Q, mesh.x_elem))
+    np.testing.assert_allclose(sums, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    X = prob.node_coordinates(mesh, basis)
+    u = np.array([10.0, -5.0, 2.0])
+    qn = prob.conservative_from_primitive(ctx.gas, 101325.0 * np.ones(X.shape[1]), u[:, None] * np.ones((1, X.shape[1])), 288.0 * np.ones(X.shape[1]))
+    mn, mx = S.monitor_cfl(op, cb, torch.from_numpy(np.ascontiguousarray(qn.T.reshape(-1))).to(_dev()), qdata, 1e-3, scratch)
+    expect = 1e-3 * np.sqrt(np.sum((u * np.array(n)) ** 2))
+    assert mn == pytest.approx(expect, rel=1e-12) and mx == pytest.approx(expect, rel=1e-12)
