@@ -38,7 +38,8 @@ struct HbExplicitStepper {
   int                steps_taken;
   cudaStream_t       s;
   double *q, *y, *f, *zero, *dinv, *K; /* K: stage block [stages][ldv] */
-  double *V, *w, *r, *scratch, *d_partial, *d_dots;
+  double *V, *r, *scratch, *d_partial, *d_dots;
+  double *h_dots; /* pinned host copy of the Gram-Schmidt coefficients */
   /* stabilized mass (stab = supg): the state it is linearised at, and whether the Jacobi set-up has run */
   int           mass_stab, pc_ready;
   const double *qstate;
@@ -125,7 +126,7 @@ static int setup_jacobi(HbExplicitStepper *ex) {
 /* x = M^-1 b by left-preconditioned GMRES(m); x must not alias b */
 static int mass_gmres(HbExplicitStepper *ex, const double *b, double *x, int *its_out, int *reason) {
   const int m = ex->o.mass_restart;
-  double    H[MAXK + 1][MAXK], cs[MAXK], sn[MAXK], g[MAXK + 1], hcol[MAXK], y[MAXK];
+  double    H[MAXK + 1][MAXK], cs[MAXK], sn[MAXK], g[MAXK + 1], y[MAXK];
   int       its = 0;
   *reason       = -2;
   HBCK(hb_vec_set_f64(x, ex->n, 0.0, ex->s));
@@ -151,20 +152,18 @@ static int mass_gmres(HbExplicitStepper *ex, const double *b, double *x, int *it
     int k     = 0;
     int done  = 0;
     while (k < m && its < ex->o.mass_max_it) {
-      HBCK(pmass(ex, col(ex->V, ex->ldv, k), ex->w));
-      HBCK(hb_krylov_multidot_f64(ex->V, ex->ldv, k + 1, ex->w, ex->n, ex->d_partial, ex->d_dots, ex->s));
-      CUCK(cudaMemcpyAsync(hcol, ex->d_dots, sizeof(double) * (k + 1), cudaMemcpyDeviceToHost, ex->s));
-      CUCK(cudaStreamSynchronize(ex->s));
-      for (int i = 0; i <= k; i++) y[i] = -hcol[i];
-      HBCK(hb_krylov_multiaxpy_f64(ex->w, ex->V, ex->ldv, k + 1, y, ex->n, ex->s));
+      /* the operator writes the next basis vector in place; classical Gram-Schmidt with the coefficients kept on the
+       * device, their host copy (pinned, asynchronous) complete once the norm has synchronised the stream */
+      double *wk = col(ex->V, ex->ldv, k + 1);
+      HBCK(pmass(ex, col(ex->V, ex->ldv, k), wk));
+      HBCK(hb_krylov_multidot_f64(ex->V, ex->ldv, k + 1, wk, ex->n, ex->d_partial, ex->d_dots, ex->s));
+      HBCK(hb_krylov_multiaxpy_dev_f64(wk, ex->V, ex->ldv, k + 1, ex->d_dots, -1.0, ex->n, ex->s));
+      CUCK(cudaMemcpyAsync(ex->h_dots, ex->d_dots, sizeof(double) * (size_t)(k + 1), cudaMemcpyDeviceToHost, ex->s));
       double hn;
-      HBCK(norm2(ex, ex->w, &hn));
-      for (int i = 0; i <= k; i++) H[i][k] = hcol[i];
+      HBCK(norm2(ex, wk, &hn));
+      for (int i = 0; i <= k; i++) H[i][k] = ex->h_dots[i];
       H[k + 1][k] = hn;
-      if (hn > 0) {
-        CUCK(cudaMemcpyAsync(col(ex->V, ex->ldv, k + 1), ex->w, sizeof(double) * (size_t)ex->n, cudaMemcpyDeviceToDevice, ex->s));
-        HBCK(hb_vec_scale_f64(col(ex->V, ex->ldv, k + 1), ex->n, 1.0 / hn, ex->s));
-      }
+      if (hn > 0) HBCK(hb_vec_scale_f64(wk, ex->n, 1.0 / hn, ex->s));
       for (int i = 0; i < k; i++) {
         const double a = H[i][k], c = H[i + 1][k];
         H[i][k]     = cs[i] * a + sn[i] * c;
@@ -265,8 +264,9 @@ int hb_explicit_create(const HbElemOp *op, const void *ctx184, const double *d_q
   err |= cudaMalloc((void **)&ex->zero, nb) | cudaMalloc((void **)&ex->dinv, nb) | cudaMalloc((void **)&ex->r, nb);
   err |= cudaMalloc((void **)&ex->K, lb * opts->rk_stages) | cudaMalloc((void **)&ex->scratch, sizeof(double) * 1024);
   if (opts->mass_ksp == 1) {
-    err |= cudaMalloc((void **)&ex->V, lb * (opts->mass_restart + 1)) | cudaMalloc((void **)&ex->w, nb);
+    err |= cudaMalloc((void **)&ex->V, lb * (opts->mass_restart + 1));
     err |= cudaMalloc((void **)&ex->d_partial, sizeof(double) * 512 * MAXK) | cudaMalloc((void **)&ex->d_dots, sizeof(double) * MAXK);
+    err |= cudaMallocHost((void **)&ex->h_dots, sizeof(double) * MAXK);
   }
   if (err) {
     hb_explicit_destroy(ex);
@@ -326,9 +326,10 @@ int hb_explicit_destroy(HbExplicitStepper *ex) {
   if (ex->ess_idx) cudaFree(ex->ess_idx);
   if (ex->ess_val) cudaFree(ex->ess_val);
   if (ex->ess_one) cudaFree(ex->ess_one);
-  void *p[] = {ex->q, ex->y, ex->f, ex->zero, ex->dinv, ex->K, ex->V, ex->w, ex->r, ex->scratch, ex->d_partial, ex->d_dots};
+  void *p[] = {ex->q, ex->y, ex->f, ex->zero, ex->dinv, ex->K, ex->V, ex->r, ex->scratch, ex->d_partial, ex->d_dots};
   for (size_t i = 0; i < sizeof p / sizeof p[0]; i++)
     if (p[i]) cudaFree(p[i]);
+  if (ex->h_dots) cudaFreeHost(ex->h_dots);
   free(ex);
   return HB_SUCCESS;
 }
