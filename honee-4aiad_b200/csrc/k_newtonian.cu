@@ -59,13 +59,16 @@ template <typename T>
 __host__ __device__ constexpr int nthreads_for(int Q) {
   return ((Q * Q * Q + 31) / 32) * 32;
 }
-// resident CTAs per SM the register budget is tuned for (65536 registers / (threads * CTAs)); the FP32 Jacobian holds
-// half the point-wise state in registers and fits four CTAs (121 registers, no spills at P=4, Q=5)
+// resident CTAs per SM the register budget is tuned for (65536 registers / (threads * CTAs), and at most 16384 per SM
+// sub-partition for the warps placed on it); the FP32 Jacobian holds half the point-wise state in registers and fits four
+// CTAs (121 registers, no spills at P=4, Q=5).  At Q = 6 a CTA is seven warps: two CTAs put four warps on a sub-partition,
+// 128 registers, which spills the FP64 point-wise phase (188-260 bytes); one CTA per SM without spills measured faster
+// (IFunction 1.19 -> 1.10 ms, IJacobian 1.10 -> 1.04 ms per 32^3 apply at P = 5), while the FP32 Jacobian keeps two.
 #ifndef HB_F32_MIN_BLOCKS
 #define HB_F32_MIN_BLOCKS 4
 #endif
 __host__ __device__ constexpr int min_blocks_for(int Q, bool staged = true, int elem_bytes = 8) {
-  return Q <= 5 ? (elem_bytes == 4 ? HB_F32_MIN_BLOCKS : (staged ? 3 : 4)) : (Q == 6 ? 2 : 1);
+  return Q <= 5 ? (elem_bytes == 4 ? HB_F32_MIN_BLOCKS : (staged ? 3 : 4)) : (Q == 6 && elem_bytes == 4 ? 2 : 1);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
