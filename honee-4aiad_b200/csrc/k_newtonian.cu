@@ -254,10 +254,24 @@ __device__ __forceinline__ void pass_x_staged(const Basis1D<T> &bas, const T *sN
   }
 }
 
+// The x/y-derivative fibres of one element, [2][5][Q2] (direction x then y, component, position on the other two
+// directions), as (direction << 16) | (component * Q3 + first point); the stride along the fibre is 1 (x) or Q (y).  A
+// kernel that keeps this table in shared memory (FT below) reads one int per fibre where the others divide and take
+// remainders per fibre and element: the IFunction at Q <= 5 (3.60 -> 3.47 ms per 64^3 apply at P = 4) and the FP32 pair
+// kernel (1.88 -> 1.80 ms) gain; the FP64 IJacobian (3.08 -> 3.10) and the IFunction at Q = 6 (1.10 -> 1.11) do not.
+template <int Q, int NT>
+__device__ __forceinline__ void fill_fibres(int *tab) {
+  constexpr int Q2 = Q * Q, Q3 = Q2 * Q, NXY = 2 * 5 * Q2;
+  for (int f = threadIdx.x; f < NXY; f += NT) {
+    const int dir = f / (5 * Q2), r = f % (5 * Q2), c = r / Q2, rem = r % Q2;
+    tab[f] = (dir << 16) | (c * Q3 + (dir == 0 ? rem * Q : (rem / Q) * Q2 + rem % Q));
+  }
+}
+
 // Forward passes after the x pass: s1 -> (y) s2 -> (z) interp sU [NC][Q3] and, for the first vector, the z
 // derivative; then x/y derivatives of the first vector on the quadrature grid.  Two fibres per thread and round.
-template <int P, int Q, int NC, int NT, typename T>
-__device__ __forceinline__ void forward_yz(const Basis1D<T> &bas, const T *s1, T *s2, T *sU, T *sG) {
+template <int P, int Q, int NC, int NT, typename T, bool FT = false>
+__device__ __forceinline__ void forward_yz(const Basis1D<T> &bas, const T *s1, T *s2, T *sU, T *sG, const int *fib = nullptr) {
   constexpr int Q2 = Q * Q, Q3 = Q2 * Q;
   pass1<NC, P, Q, P, Q, false, NT>(s1, s2, bas.B, P);
   __syncthreads();
@@ -314,12 +328,28 @@ __device__ __forceinline__ void forward_yz(const Basis1D<T> &bas, const T *s1, T
   for (int f0 = threadIdx.x; f0 < NXY; f0 += (TWO_XY ? 2 : 1) * NT) {
     const bool h1 = TWO_XY && f0 + NT < NXY;
     const int f1 = h1 ? f0 + NT : f0;
-    const int dir0 = f0 / (5 * Q2), r0 = f0 % (5 * Q2), cc0 = r0 / Q2, rem0 = r0 % Q2;
-    const int dir1 = f1 / (5 * Q2), r1 = f1 % (5 * Q2), cc1 = r1 / Q2, rem1 = r1 % Q2;
-    const int base0 = dir0 == 0 ? rem0 * Q : (rem0 / Q) * Q2 + (rem0 % Q), st0 = dir0 == 0 ? 1 : Q;
-    const int base1 = dir1 == 0 ? rem1 * Q : (rem1 / Q) * Q2 + (rem1 % Q), st1 = dir1 == 0 ? 1 : Q;
-    const T *src0 = sU + cc0 * Q3 + base0, *src1 = sU + cc1 * Q3 + base1;
-    T *dst0 = sG + (dir0 * 5 + cc0) * Q3 + base0, *dst1 = sG + (dir1 * 5 + cc1) * Q3 + base1;
+    const T *src0, *src1;
+    T *dst0, *dst1;
+    int st0, st1;
+    if constexpr (FT) {
+      const int t0 = fib[f0], t1 = fib[f1], dir0 = t0 >> 16, cb0 = t0 & 0xffff, dir1 = t1 >> 16, cb1 = t1 & 0xffff;
+      st0 = dir0 == 0 ? 1 : Q;
+      st1 = dir1 == 0 ? 1 : Q;
+      src0 = sU + cb0;
+      src1 = sU + cb1;
+      dst0 = sG + dir0 * 5 * Q3 + cb0;
+      dst1 = sG + dir1 * 5 * Q3 + cb1;
+    } else {
+      const int dir0 = f0 / (5 * Q2), r0 = f0 % (5 * Q2), cc0 = r0 / Q2, rem0 = r0 % Q2;
+      const int dir1 = f1 / (5 * Q2), r1 = f1 % (5 * Q2), cc1 = r1 / Q2, rem1 = r1 % Q2;
+      const int base0 = dir0 == 0 ? rem0 * Q : (rem0 / Q) * Q2 + (rem0 % Q), base1 = dir1 == 0 ? rem1 * Q : (rem1 / Q) * Q2 + (rem1 % Q);
+      st0 = dir0 == 0 ? 1 : Q;
+      st1 = dir1 == 0 ? 1 : Q;
+      src0 = sU + cc0 * Q3 + base0;
+      src1 = sU + cc1 * Q3 + base1;
+      dst0 = sG + (dir0 * 5 + cc0) * Q3 + base0;
+      dst1 = sG + (dir1 * 5 + cc1) * Q3 + base1;
+    }
     T v0[Q], v1[Q];
 #pragma unroll
     for (int l = 0; l < Q; l++) {
@@ -345,22 +375,44 @@ __device__ __forceinline__ void forward_yz(const Basis1D<T> &bas, const T *s1, T
 // nodes, node-major sF [P3][5].  Scratch: sW1 [5][Q3], sW2 [5][Q3], sT2 [5][P][Q][Q], sT1 [5][P][P][Q]; sT1 may alias
 // sG (free once the z pass is done), sF may alias sW2.  Two fibres per thread and round where a pass has more fibres
 // than threads.
-template <int P, int Q, int NT, typename T>
-__device__ __forceinline__ void transpose_passes(const Basis1D<T> &bas, const T *sU, const T *sG, T *sW1, T *sW2, T *sT2, T *sT1, T *sF) {
+template <int P, int Q, int NT, typename T, bool FT = false>
+__device__ __forceinline__ void transpose_passes(const Basis1D<T> &bas, const T *sU, const T *sG, T *sW1, T *sW2, T *sT2, T *sT1, T *sF,
+                                                 const int *fib = nullptr) {
   constexpr int Q2 = Q * Q, Q3 = Q2 * Q, NXY = 2 * 5 * Q2;
   constexpr bool TWO = NXY > NT;
 #pragma unroll 1
   for (int f0 = threadIdx.x; f0 < NXY; f0 += (TWO ? 2 : 1) * NT) {
     const bool h1 = TWO && f0 + NT < NXY;
     const int f1 = h1 ? f0 + NT : f0;
-    const int dir0 = f0 / (5 * Q2), r0 = f0 % (5 * Q2), c0 = r0 / Q2, rem0 = r0 % Q2;
-    const int dir1 = f1 / (5 * Q2), r1 = f1 % (5 * Q2), c1 = r1 / Q2, rem1 = r1 % Q2;
-    const int base0 = dir0 == 0 ? rem0 * Q : (rem0 / Q) * Q2 + (rem0 % Q), st0 = dir0 == 0 ? 1 : Q;
-    const int base1 = dir1 == 0 ? rem1 * Q : (rem1 / Q) * Q2 + (rem1 % Q), st1 = dir1 == 0 ? 1 : Q;
-    const T *g0 = sG + (dir0 * 5 + c0) * Q3 + base0, *g1 = sG + (dir1 * 5 + c1) * Q3 + base1;
     // x direction adds the point values (w1 = v + D^T g_x); y direction starts from zero (w2 = D^T g_y)
-    const T *v0 = sU + c0 * Q3 + base0, *v1 = sU + c1 * Q3 + base1;
-    T *w0 = (dir0 == 0 ? sW1 : sW2) + c0 * Q3 + base0, *w1 = (dir1 == 0 ? sW1 : sW2) + c1 * Q3 + base1;
+    const T *g0, *g1, *v0, *v1;
+    T *w0, *w1;
+    int dir0, dir1, st0, st1;
+    if constexpr (FT) {
+      const int t0 = fib[f0], t1 = fib[f1], cb0 = t0 & 0xffff, cb1 = t1 & 0xffff;
+      dir0 = t0 >> 16;
+      dir1 = t1 >> 16;
+      g0 = sG + dir0 * 5 * Q3 + cb0;
+      g1 = sG + dir1 * 5 * Q3 + cb1;
+      v0 = sU + cb0;
+      v1 = sU + cb1;
+      w0 = (dir0 == 0 ? sW1 : sW2) + cb0;
+      w1 = (dir1 == 0 ? sW1 : sW2) + cb1;
+    } else {
+      dir0 = f0 / (5 * Q2);
+      dir1 = f1 / (5 * Q2);
+      const int r0 = f0 % (5 * Q2), c0 = r0 / Q2, rem0 = r0 % Q2;
+      const int r1 = f1 % (5 * Q2), c1 = r1 / Q2, rem1 = r1 % Q2;
+      const int base0 = dir0 == 0 ? rem0 * Q : (rem0 / Q) * Q2 + (rem0 % Q), base1 = dir1 == 0 ? rem1 * Q : (rem1 / Q) * Q2 + (rem1 % Q);
+      g0 = sG + (dir0 * 5 + c0) * Q3 + base0;
+      g1 = sG + (dir1 * 5 + c1) * Q3 + base1;
+      v0 = sU + c0 * Q3 + base0;
+      v1 = sU + c1 * Q3 + base1;
+      w0 = (dir0 == 0 ? sW1 : sW2) + c0 * Q3 + base0;
+      w1 = (dir1 == 0 ? sW1 : sW2) + c1 * Q3 + base1;
+    }
+    st0 = dir0 == 0 ? 1 : Q;
+    st1 = dir1 == 0 ? 1 : Q;
     T gv0[Q], gv1[Q], b0[Q], b1[Q];
 #pragma unroll
     for (int l = 0; l < Q; l++) {
@@ -558,7 +610,10 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
   double *sD = sU + 5 * Q3;
   __shared__ double s_qref[kMaxP];
   __shared__ int32_t sO[2][5 * L::P3];  // entry offsets of the current / next element
+  constexpr bool FT = Q <= 5;           // x/y-derivative fibre table
+  __shared__ int sFib[FT ? 2 * 5 * Q * Q : 1];
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
+  if constexpr (FT) fill_fibres<Q, NT>(sFib);
 
   if (threadIdx.x == 0) {  // constant indices: indexing the parameter array with threadIdx would copy it to local memory
 #pragma unroll
@@ -607,7 +662,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
       cp_async_commit();
       nxt.store(sO[buf ^ 1]);
     }
-    forward_yz<P, Q, 10, NT, double>(a.basis, s1, s2, sU, sG);
+    forward_yz<P, Q, 10, NT, double, FT>(a.basis, s1, s2, sU, sG, sFib);
     HB_PT(2)
     const int q = threadIdx.x;
     if (q < Q3) {
@@ -659,7 +714,7 @@ __global__ void __launch_bounds__(nthreads_for<double>(Q), min_blocks_for(Q)) k_
     }
     // transpose scratch: w1 in the q_dot slot, w2 and the node values in s2, sT2 in s1, sT1 in sG
     HB_PT(4)
-    transpose_passes<P, Q, NT, double>(a.basis, sU, sG, sD, s2, s1, sG, s2);
+    transpose_passes<P, Q, NT, double, FT>(a.basis, sU, sG, sD, s2, s1, sG, s2, sFib);
     HB_PT(5)
     scatter_add<P, NT, double>(sO[buf], s2, p.v);  // no barrier after it: nothing writes shared memory before the next
     HB_PT(12)                                       // iteration's top barrier
@@ -862,6 +917,8 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::qd_offset_bytes + 2 * sizeof(double) * 10 * Q3);
   __shared__ int s_bail;
   __shared__ int32_t sO[2][2][5 * P3];  // entry offsets of the current / next pair, per lane
+  __shared__ int sFib[2 * 5 * Q * Q];   // x/y-derivative fibre table
+  fill_fibres<Q, NT>(sFib);
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
   const int njd = a.num_jd;
   const int npairs = (a.n_elems + 1) / 2;
@@ -935,7 +992,7 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
       nxa.store(sO[buf ^ 1][0]);
       nxb.store(sO[buf ^ 1][1]);
     }
-    forward_yz<P, Q, 5, NT, f2>(a.basis, s1, s2, sU, sG);
+    forward_yz<P, Q, 5, NT, f2, true>(a.basis, s1, s2, sU, sG, sFib);
     const int q = threadIdx.x;
     if (q < Q3) {
       f2 dq[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5], jd[15];
@@ -969,7 +1026,7 @@ __global__ void __launch_bounds__(nthreads_for<float>(Q), (Q <= 5 ? 3 : 1)) k_ij
       }
       cp_async_commit();
     }
-    transpose_passes<P, Q, NT, f2>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
+    transpose_passes<P, Q, NT, f2, true>(a.basis, sU, sG, sW1, s2, s1, sG, s2, sFib);
     {  // scatter: each lane to its own element's nodes, by reductions (scatter_add)
       const int32_t *oA = sO[buf][0], *oB = sO[buf][1];
       for (int t = threadIdx.x; t < 5 * P3; t += NT) {
