@@ -254,18 +254,53 @@ __device__ __forceinline__ void pass_x_staged(const Basis1D<T> &bas, const T *sN
   }
 }
 
-// The x/y-derivative fibres of one element, [2][5][Q2] (direction x then y, component, position on the other two
-// directions), as (direction << 16) | (component * Q3 + first point); the stride along the fibre is 1 (x) or Q (y).  A
-// kernel that keeps this table in shared memory (FT below) reads one int per fibre where the others divide and take
+// The x/y-derivative fibres of one element: 2 x 5 x Q2 of them (direction x or y, component, position on the other two
+// directions), each as (direction << 16) | (component * Q3 + first point); the stride along the fibre is 1 (x) or Q (y).
+// A kernel that keeps this table in shared memory (FT below) reads one int per fibre where the others divide and take
 // remainders per fibre and element: the IFunction at Q <= 5 (3.60 -> 3.47 ms per 64^3 apply at P = 4) and the FP32 pair
 // kernel (1.88 -> 1.80 ms) gain; the FP64 IJacobian (3.08 -> 3.10) and the IFunction at Q = 6 (1.10 -> 1.11) do not.
+//
+// The table also fixes which thread takes which fibre (thread t takes entries t and t + NT), and that order sets the
+// shared-memory bank conflicts of the pass: an 8-byte access of 16 threads is one wavefront when their 16 offsets differ
+// modulo 16.  The x fibres start Q apart, which is conflict-free for odd Q.  The y fibres start at c Q3 + z Q2 + x; in
+// that natural order, at Q = 5, groups of 16 repeat offsets modulo 16 (0-4, 25-29, 50-54, ...) and take two wavefronts.
+// So the x fibres keep their order and each y fibre goes, first fit, to the next slot whose 16-slot group holds no
+// offset equal to it modulo 16 (the first one left when none fits).  At Q = 5 every group is then conflict-free.
+template <int Q>
+struct FibreOrder {
+  int v[2 * 5 * Q * Q];
+};
+
+template <int Q>
+constexpr FibreOrder<Q> make_fibre_order() {
+  constexpr int Q2 = Q * Q, Q3 = Q2 * Q, NX = 5 * Q2;
+  FibreOrder<Q> o{};
+  bool taken[NX] = {};
+  for (int f = 0; f < NX; f++) o.v[f] = (f / Q2) * Q3 + (f % Q2) * Q;
+  for (int p = NX; p < 2 * NX; p++) {
+    const int g0 = p - p % 16;
+    int pick = -1, first = -1;
+    for (int r = 0; r < NX && pick < 0; r++) {
+      if (taken[r]) continue;
+      if (first < 0) first = r;
+      const int cb = (r / Q2) * Q3 + ((r % Q2) / Q) * Q2 + (r % Q2) % Q;
+      bool clash = false;
+      for (int i = g0; i < p; i++) clash = clash || ((o.v[i] & 0xffff) - cb) % 16 == 0;
+      if (!clash) pick = r;
+    }
+    if (pick < 0) pick = first;
+    taken[pick] = true;
+    o.v[p] = (1 << 16) | ((pick / Q2) * Q3 + ((pick % Q2) / Q) * Q2 + (pick % Q2) % Q);
+  }
+  return o;
+}
+
+template <int Q>
+__constant__ FibreOrder<Q> c_fibre_order = make_fibre_order<Q>();
+
 template <int Q, int NT>
 __device__ __forceinline__ void fill_fibres(int *tab) {
-  constexpr int Q2 = Q * Q, Q3 = Q2 * Q, NXY = 2 * 5 * Q2;
-  for (int f = threadIdx.x; f < NXY; f += NT) {
-    const int dir = f / (5 * Q2), r = f % (5 * Q2), c = r / Q2, rem = r % Q2;
-    tab[f] = (dir << 16) | (c * Q3 + (dir == 0 ? rem * Q : (rem / Q) * Q2 + rem % Q));
-  }
+  for (int f = threadIdx.x; f < 2 * 5 * Q * Q; f += NT) tab[f] = c_fibre_order<Q>.v[f];
 }
 
 // Forward passes after the x pass: s1 -> (y) s2 -> (z) interp sU [NC][Q3] and, for the first vector, the z
