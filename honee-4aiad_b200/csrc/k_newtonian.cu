@@ -257,8 +257,9 @@ __device__ __forceinline__ void pass_x_staged(const Basis1D<T> &bas, const T *sN
 // The x/y-derivative fibres of one element: 2 x 5 x Q2 of them (direction x or y, component, position on the other two
 // directions), each as (direction << 16) | (component * Q3 + first point); the stride along the fibre is 1 (x) or Q (y).
 // A kernel that keeps this table in shared memory (FT below) reads one int per fibre where the others divide and take
-// remainders per fibre and element: the IFunction at Q <= 5 (3.60 -> 3.47 ms per 64^3 apply at P = 4) and the FP32 pair
-// kernel (1.88 -> 1.80 ms) gain; the FP64 IJacobian (3.08 -> 3.10) and the IFunction at Q = 6 (1.10 -> 1.11) do not.
+// remainders per fibre and element.  At Q <= 5 the IFunction, the IJacobian and the FP32 pair kernel use it (per 64^3
+// apply at P = 4, in the natural order: IFunction 3.60 -> 3.47 ms, pair 1.88 -> 1.80 ms, FP64 IJacobian 3.08 -> 3.10;
+// in the order below: 3.42, 1.78 and 3.04 ms).  At Q = 6 the kernels compute the fibre in place.
 //
 // The table also fixes which thread takes which fibre (thread t takes entries t and t + NT), and that order sets the
 // shared-memory bank conflicts of the pass: an 8-byte access of 16 threads is one wavefront when their 16 offsets differ
@@ -788,6 +789,9 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::mbar_offset);
   __shared__ int s_bail;
   __shared__ int32_t sO[2][5 * L::P3];  // entry offsets of the current / next element
+  constexpr bool FT = Q <= 5;
+  __shared__ int sFib[FT ? 2 * 5 * Q * Q : 1];
+  if constexpr (FT) fill_fibres<Q, NT>(sFib);
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
   const int njd = a.num_jd;
   const unsigned jd_bytes = (unsigned)(sizeof(T) * njd * Q3);
@@ -850,7 +854,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
       cp_async_commit();
       nxt.store(sO[buf ^ 1]);
     }
-    forward_yz<P, Q, 5, NT, T>(a.basis, s1, s2, sU, sG);
+    forward_yz<P, Q, 5, NT, T, FT>(a.basis, s1, s2, sU, sG, sFib);
     const int q = threadIdx.x;
     if (q < Q3) {
       T dq[5], gref[3][5], wdetJ, X[3][3], v[5], gv[3][5], jd[15];
@@ -898,7 +902,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
       }
       cp_async_commit();
     }
-    transpose_passes<P, Q, NT, T>(a.basis, sU, sG, sW1, s2, s1, sG, s2);
+    transpose_passes<P, Q, NT, T, FT>(a.basis, sU, sG, sW1, s2, s1, sG, s2, sFib);
     scatter_add<P, NT, T>(sO[buf], s2, p.v);  // the next iteration's top barrier orders it before any shared-memory write
     buf ^= 1;
     ecur = en;
