@@ -259,7 +259,8 @@ __device__ __forceinline__ void pass_x_staged(const Basis1D<T> &bas, const T *sN
 // A kernel that keeps this table in shared memory (FT below) reads one int per fibre where the others divide and take
 // remainders per fibre and element.  At Q <= 5 the IFunction, the IJacobian and the FP32 pair kernel use it (per 64^3
 // apply at P = 4, in the natural order: IFunction 3.60 -> 3.47 ms, pair 1.88 -> 1.80 ms, FP64 IJacobian 3.08 -> 3.10;
-// in the order below: 3.42, 1.78 and 3.04 ms).  At Q = 6 the kernels compute the fibre in place.
+// in the order below: 3.42, 1.78 and 3.04 ms).  At Q = 6 only the FP64 IJacobian uses it (1.038 -> 1.031 ms per 32^3
+// apply at P = 5; the IFunction measured the same and the FP32 Jacobian 0.582 -> 0.587 ms).
 //
 // The table also fixes which thread takes which fibre (thread t takes entries t and t + NT), and that order sets the
 // shared-memory bank conflicts of the pass: an 8-byte access of 16 threads is one wavefront when their 16 offsets differ
@@ -789,7 +790,7 @@ __global__ void __launch_bounds__(nthreads_for<T>(Q), min_blocks_for(Q, ST, (int
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw + L::mbar_offset);
   __shared__ int s_bail;
   __shared__ int32_t sO[2][5 * L::P3];  // entry offsets of the current / next element
-  constexpr bool FT = Q <= 5;
+  constexpr bool FT = Q <= 5 || (Q == 6 && sizeof(T) == 8);  // x/y-derivative fibre table (FP32 at Q = 6: slower with it)
   __shared__ int sFib[FT ? 2 * 5 * Q * Q : 1];
   if constexpr (FT) fill_fibres<Q, NT>(sFib);
   const unsigned qd_bytes = sizeof(double) * 10 * Q3;
